@@ -1,0 +1,354 @@
+#!/usr/bin/env python
+"""Benchmark: CG-SENSE reconstructions per second on one B200 per rank.
+
+Workload (one "step" = one reconstruction): 3-D koosh-ball radial, 128^3
+image on a 256^3 grid (oversampling 2), 4096 spokes x 256 samples, 16 coils,
+CG-SENSE with 30 CG updates (bmSensa with one outer iteration and nCGD = 30:
+32 forward and 30 adjoint operator applications).  Inputs are seeded
+synthetic data with these shapes; the k-space data are simulated from an
+ellipsoid phantom by the forward operator.
+
+Every rank runs its own reconstruction (replicas: one recon does not span
+GPUs), so `value` = (ranks x steps) / max-over-ranks time.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+The reference arm times the reference's CPU path on the host cores: its own
+C++ sparse-matrix kernel (compiled from source into oracle/_ref; the plain-C
+restatement when that is absent) inside the numpy/scipy restatement of the
+MATLAB operators, on a bounded sample (one forward + one adjoint operator
+application) extrapolated to a full reconstruction.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "recons/sec & p50/p99 latency vs plain GPU at ≤1e-3 rel err; gridding HBM GB/s"
+UNIT = "recons/s"
+
+
+def _peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.rows = []
+        self._p = None
+        self._t = None
+
+    def start(self):
+        try:
+            self._p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                        "-lms", "200", "-i", str(self.dev)], stdout=subprocess.PIPE,
+                                       stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except Exception:
+            self._p = None
+
+    def _read(self):
+        for line in self._p.stdout:
+            parts = [s.strip() for s in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self._p is not None:
+            self._p.terminate()
+            try:
+                self._p.wait(timeout=5)
+            except Exception:
+                self._p.kill()
+        if self._t is not None:
+            self._t.join(timeout=2)
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def algorithmic_bytes(w, Gu, Gut, nCh):
+    """Bytes each stage must move at least (the per-unit figures of the
+    design notes), for one operator application."""
+    nnz = Gu.nnz
+    nPt = Gu.l_size
+    Nu = int(np.prod(w.N_u))
+    nu = int(np.prod(w.n_u))
+    touched, _ = Gut.row_stats()
+    return {
+        "pre": nu * 8 + nu * nCh * 8 + Nu * nCh * 8,
+        "gu": nnz * 8 + 4 * (nPt + 1) + touched * nCh * 8 + nPt * nCh * 8,
+        "gut": nnz * 8 + 4 * (Nu + 1) + nPt * nCh * 8 + 4 * nPt + Nu * nCh * 8,
+        "post": nu * nCh * 8 + nu * nCh * 8 + nu * 8,
+        "fft": 2 * Nu * nCh * 8,
+    }
+
+
+def run_gpu(args):
+    import torch
+    import torch.distributed as dist
+
+    ws, rank, local = _dist()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    import monalisa_b200 as mb
+    from monalisa_b200 import _native as N
+    from monalisa_b200.workloads import koosh3d
+
+    t0 = time.time()
+    w = koosh3d()
+    Gu, Gut = mb.bmTraj2SparseMat(w.t, w.ve, w.N_u, w.dK_u, w.kernelType, w.nWin, w.kernelParam)
+    rec = mb.SensaRecon(Gu, Gut, w.C, w.n_u)
+    dev = torch.device("cuda", local)
+    x_true = torch.from_numpy(w.x_true).to(dev)
+    y = rec.plan.shanna(x_true)
+    gen = torch.Generator(device=dev).manual_seed(1234)
+    noise = torch.randn(y.shape, dtype=torch.complex64, device=dev, generator=gen)
+    y += noise * (y.abs().mean() * 1e-3)
+    ve = torch.from_numpy(np.ascontiguousarray(w.ve, np.float32)).to(dev)
+    nu = int(np.prod(w.n_u))
+    x = torch.zeros(nu, dtype=torch.complex64, device=dev)
+    torch.cuda.synchronize()
+    setup_s = time.time() - t0
+
+    def step():
+        x.zero_()
+        rec.run_dev(y, ve, x, nIter=1, nCGD=w.nCGD)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    # accuracy of the reconstruction against the phantom (reported, not gated)
+    err = float((x - x_true).norm() / x_true.norm())
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    l0 = N.launch_count()
+    stream = torch.cuda.current_stream()
+    if ws > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if ws > 1:
+        dist.barrier()
+    launches = N.launch_count() - l0
+    ms = e0.elapsed_time(e1)
+    clk = clocks.stop()
+    if ws > 1:
+        tt = torch.tensor([ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    value = ws * args.steps / (ms / 1e3)
+
+    # end to end through the C ABI with host buffers (pinned), copies inside
+    ypin = torch.empty((w.nPt, w.nCh), dtype=torch.complex64, pin_memory=True)
+    ypin.copy_(y)
+    yR = np.ascontiguousarray(ypin.numpy().real.T)
+    yI = np.ascontiguousarray(ypin.numpy().imag.T)
+    yR_p = torch.empty(yR.shape, dtype=torch.float32, pin_memory=True).numpy()
+    yI_p = torch.empty(yI.shape, dtype=torch.float32, pin_memory=True).numpy()
+    yR_p[...] = yR
+    yI_p[...] = yI
+    ve_h = torch.empty(w.nPt, dtype=torch.float32, pin_memory=True).numpy()
+    ve_h[...] = w.ve
+    xR = torch.empty(nu, dtype=torch.float32, pin_memory=True).numpy()
+    xI = torch.empty(nu, dtype=torch.float32, pin_memory=True).numpy()
+    res = np.zeros(1)
+
+    def e2e_step():
+        xR[...] = 0
+        xI[...] = 0
+        N.call("mlg_sensa", rec.plan.handle, N.fptr(yR_p), N.fptr(yI_p), N.fptr(ve_h), 0.0, 1, w.nCGD, N.fptr(xR),
+               N.fptr(xI), N.dptr(res))
+
+    e2e_step()
+    if ws > 1:
+        dist.barrier()
+    ta = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    e2e_s = time.perf_counter() - ta
+    if ws > 1:
+        tt = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_s = float(tt.item())
+    e2e = {"value": ws * args.steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(yR_p.nbytes + yI_p.nbytes +
+                                                                                     ve_h.nbytes + xR.nbytes +
+                                                                                     xI.nbytes),
+           "d2h_bytes_per_step": int(xR.nbytes + xI.nbytes + res.nbytes)}
+
+    # per-stage live timing of the operator kernels (CUDA events on the
+    # plan's stream) -> roofline of the dominant kernel of this library
+    st = np.zeros(6)
+    N.call("mlg_plan_profile", rec.plan.handle, 5, N.dptr(st))
+    stage_names = ["pre", "fft_fwd", "gu", "gut", "fft_inv", "post"]
+    B = algorithmic_bytes(w, Gu, Gut, w.nCh)
+    peak, peak_kind = _peaks()
+    stages = {}
+    for i, nm in enumerate(stage_names):
+        b = B["fft"] if nm.startswith("fft") else B[nm]
+        gbs = b / (st[i] * 1e-3) / 1e9
+        stages[nm] = {"ms": round(float(st[i]), 4), "algorithmic_bytes": int(b), "GBps": round(gbs, 1),
+                      "frac": round(gbs / peak, 4), "library": nm.startswith("fft")}
+    ours = [k for k in stage_names if not k.startswith("fft")]
+    dom = max(ours, key=lambda k: stages[k]["ms"])
+    traffic_file = os.path.join(ROOT, "profiles", "traffic.json")
+    traffic = None
+    if os.path.exists(traffic_file):
+        with open(traffic_file) as f:
+            traffic = json.load(f).get(dom)
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": stages[dom]["GBps"], "peak": peak,
+                "peak_kind": peak_kind, "unit": "GB/s", "frac": stages[dom]["frac"], "traffic": traffic,
+                "stages": stages}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(w, _to_oracle(w, Gu), _to_oracle(w, Gut), y.cpu().numpy())
+
+    out = {
+        "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "c64 (fp32 data, fp64 CG scalars)",
+        "data": "synthetic (seeded koosh-ball trajectory, random coil maps, ellipsoid phantom)",
+        "config": {"workload": "3D koosh-ball CG-SENSE: 128^3 image, 256^3 grid, 4096x256 samples, 16 coils, "
+                               "30 CG iterations", "parallelism": f"replicas x{ws}",
+                   "l2": "working set (2.1 GB grid) larger than L2 each step", **w.info},
+        "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
+        "recon_rel_err_vs_phantom": round(err, 5), "setup_s": round(setup_s, 2),
+    }
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    rec.plan.close()
+    if ws > 1:
+        dist.destroy_process_group()
+
+
+def _oracle():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    return oracle
+
+
+def _to_oracle(w, D):
+    """A device matrix as the oracle's jump-format matrix (input transfer)."""
+    oracle = _oracle()
+    b = D.download()
+    return oracle.SparseMat(r_size=b.r_size, l_size=b.l_size, r_nJump=b.r_nJump, m_val=b.m_val, r_jump=b.r_jump,
+                            l_jump=b.l_jump, l_nJump=b.l_nJump, N_u=w.N_u, d_u=w.dK_u, kernel_type=w.kernelType,
+                            nWin=w.nWin, kernelParam=np.array(w.kernelParam))
+
+
+def cpu_baseline(w, gu, gut, y):
+    """The reference CPU path on a bounded sample: one forward and one
+    adjoint operator application at full size (reference SpMV kernel +
+    scipy FFT with all host threads), extrapolated to one reconstruction of
+    (nCGD+2) forward and nCGD adjoint applications."""
+    oracle = _oracle()
+    kind = "reference" if oracle.ref_available() else "port"
+    cores = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    KFC = oracle.bmKF(w.C, w.N_u, w.n_u, w.dK_u, w.nCh, w.kernelType, w.nWin, w.kernelParam)
+    KFCc = oracle.bmKF_conj(np.conj(w.C), w.N_u, w.n_u, w.dK_u, w.nCh, w.kernelType, w.nWin, w.kernelParam)
+    spm = oracle.SpMV(kind)
+    x0 = w.x_true
+    t0 = time.perf_counter()
+    oracle.bmShanna(x0, gu, KFC, w.n_u, spm, workers=cores)
+    t1 = time.perf_counter()
+    oracle.bmNakatsha(y, gut, KFCc, True, w.n_u, spm, workers=cores)
+    t2 = time.perf_counter()
+    fwd, adj = t1 - t0, t2 - t1
+    recon_s = (w.nCGD + 2) * fwd + w.nCGD * adj
+    return {"value": round(1.0 / recon_s, 6), "unit": UNIT, "cores": cores, "kind": kind,
+            "sample": f"1 forward ({fwd:.2f} s) + 1 adjoint ({adj:.2f} s) operator application at full size, "
+                      f"extrapolated to {w.nCGD + 2} forward + {w.nCGD} adjoint per recon; SpMV = "
+                      f"{'reference bmSparseMat_cC_oBlock_omp_mex compiled from source' if kind == 'reference' else 'C restatement'}"
+                      f", FFT = scipy.fft (workers={cores})"}
+
+
+def run_reference(args):
+    ws, rank, local = _dist()
+    if rank != 0:
+        return
+    from monalisa_b200.workloads import koosh3d
+
+    oracle = _oracle()
+    w = koosh3d()
+    G = oracle.traj2sparsemat(w.t, w.ve, w.N_u, w.dK_u, w.kernelType, w.nWin, w.kernelParam)
+    rng = np.random.default_rng(5)
+    y = (rng.standard_normal((w.nPt, w.nCh)) + 1j * rng.standard_normal((w.nPt, w.nCh))).astype(np.complex64)
+    samples = []
+    for i in range(args.warmup + args.steps):
+        c = cpu_baseline(w, G["Gu"], G["Gut"], y)
+        if i >= args.warmup:
+            samples.append(c)
+    value = statistics.median(s["value"] for s in samples)
+    out = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": round(1e3 / value, 1), "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "c64", "data": "synthetic",
+           "config": {"workload": "3D koosh-ball CG-SENSE: 128^3 image, 256^3 grid, 4096x256 samples, 16 coils, "
+                                  "30 CG iterations", **w.info},
+           "cpu_baseline": {"value": value, "unit": UNIT, "kind": samples[0]["kind"], "cores": samples[0]["cores"],
+                            "sample": samples[0]["sample"]},
+           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,251 @@
+/*
+ * monalisa_gpu.h -- C ABI of libmonalisa_gpu.so, the B200 (sm_100a)
+ * implementation of Monalisa's non-Cartesian gridding hot path.
+ *
+ * Conventions
+ *  - Every function returns an int status: MLG_OK (0) or a negative
+ *    MLG_ERR_* code.  mlg_last_error() gives a message for the calling
+ *    thread's last failure.  Invalid arguments are rejected before any launch.
+ *  - Host-buffer entry points ("MEX equivalents") take and return the exact
+ *    argument layouts of the reference MEX kernels they replace: MATLAB
+ *    column-major arrays, complex values as separate real/imaginary float
+ *    arrays, int32 indices, and outputs written into caller-owned buffers.
+ *    They are synchronous, like a MEX call.
+ *  - Device-resident objects sit behind opaque handles (mlg_matrix_t,
+ *    mlg_plan_t).  *_dev entry points take device pointers and a cudaStream_t
+ *    (passed as void*, NULL = default stream) and are stream-ordered.  A
+ *    handle may be used by one host thread at a time.
+ *  - Device data layouts: complex64 = interleaved float2.  Images are
+ *    [prod(n_u)] with x fastest (MATLAB column order).  Gridded data are
+ *    coil-major [nCh][prod(N_u)].  k-space data on the device are
+ *    coil-fastest [nPt][nCh] ("point layout").
+ *
+ * Reference paths in the comments are relative to the Monalisa source tree.
+ */
+#ifndef MONALISA_GPU_H
+#define MONALISA_GPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* exported even when the library is compiled with -fvisibility=hidden */
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+#define MLG_OK 0
+#define MLG_ERR_ARG -1         /* invalid argument (sizes, NULL, bad matrix)   */
+#define MLG_ERR_OOM -2         /* device memory could not be obtained           */
+#define MLG_ERR_CUDA -3        /* a CUDA / cuFFT call failed                    */
+#define MLG_ERR_TIMEOUT -4     /* a bounded device wait gave up                 */
+#define MLG_ERR_STATE -5       /* handle used in a wrong state                  */
+#define MLG_ERR_UNSUPPORTED -6 /* configuration not implemented                 */
+#define MLG_ERR_NO_DEVICE -7   /* no CUDA device visible                        */
+
+#define MLG_KERNEL_GAUSS 0
+#define MLG_KERNEL_KAISER 1
+
+typedef struct mlg_matrix_s* mlg_matrix_t;
+typedef struct mlg_plan_s* mlg_plan_t;
+
+/* ---- library ------------------------------------------------------------ */
+int mlg_version(void);
+const char* mlg_status_string(int status);
+const char* mlg_last_error(void);
+/* Device used by subsequent calls of this host thread (default: current). */
+int mlg_set_device(int device);
+/* Number of launches of this library's kernels since load (all threads). */
+long long mlg_kernel_launch_count(void);
+
+/* ---- adjoint gridding, host buffers (MEX equivalents) ------------------- */
+
+/* Replaces bmGridder_n2u_leight{1,2,3}_mex
+ * (src/gridding123/mex/bmGridder_n2u_leight3/bmGridder_n2u_leight3_mex.cpp:39
+ * gateway, :116 kernel; leight2 :36/:108; leight1 :34/:100), as called by
+ * src/gridding123/m/bmGridder_n2u_leight.m:125-131.
+ * aReal/aImag [nCh, nPt]; tx,ty,tz [nPt] 1-based grid coordinates (ty/tz
+ * ignored below imDim); Dn [nPt]; out bReal/bImag [nCh, Nx*Ny*Nz].
+ * Gaussian window sigma = kernelParam_1; kernelParam_2 is unused, as in the
+ * reference. */
+int mlg_gridder_n2u_leight(int imDim, const float* aReal, const float* aImag,
+                           const float* tx, const float* ty, const float* tz,
+                           const float* Dn, int nCh, int nPt, int Nx, int Ny,
+                           int Nz, int nWin, float kernelParam_1,
+                           float kernelParam_2, float* bReal, float* bImag);
+
+/* Replaces bmGridder_n2u_mex
+ * (src/gridding123/mex/bmGridder_n2u/bmGridder_n2u_mex.cpp:23 gateway, :72
+ * kernel), as called by src/gridding123/m/bmGridder_n2u.m:203.
+ * w [nNb*nPt] weights; nJump [nNb*nPt] jump-coded 0-based target cells (first
+ * entry absolute); out [nCh, Nu_tot]. */
+int mlg_gridder_n2u(const float* aReal, const float* aImag, const float* w,
+                    const int* nJump, int nCh, int nNb, int nPt, int Nu_tot,
+                    float* bReal, float* bImag);
+
+/* ---- sparse gridding matrices ------------------------------------------- */
+
+/* Replaces bmSparseMat_cC_oBlock_omp_mex / bmSparseMat_cC_oBlock_mex
+ * (src/sparseMat/mex/bmSparseMat_vec/bmSparseMat_cC_oBlock_omp/
+ * bmSparseMat_cC_oBlock_omp_mex.cpp:26 gateway, :106 kernel), as dispatched
+ * by src/sparseMat/m/bmSparseMat_vec.m:183-240.
+ * The matrix is the cpp_prepared 'one_block' jump format of
+ * src/sparseMat/m/bmSparseMat.m:100-188; l_jump == NULL means no row
+ * squeezing.  v [r_size, nVec] -> w [l_size, nVec] (column layout). */
+int mlg_sparsemat_vec_cC(int r_size, const int* r_jump, const int* r_nJump,
+                         const float* m_val, int l_size, const int* l_jump,
+                         int l_nJump, const float* vReal, const float* vImag,
+                         int nVec, float* wReal, float* wImag);
+
+/* Replaces bmSparseMat_cR_oBlock_mex (…/bmSparseMat_cR_oBlock_mex.cpp:14
+ * gateway, :82 kernel): row layout v [nVec, r_size] -> w [nVec, l_size]. */
+int mlg_sparsemat_vec_cR(int r_size, const int* r_jump, const int* r_nJump,
+                         const float* m_val, int l_size, const int* l_jump,
+                         int l_nJump, const float* vReal, const float* vImag,
+                         int nVec, float* wReal, float* wImag);
+
+/* Replaces bmSparseMat_rC_oBlock(_omp)_mex (…/bmSparseMat_rC_oBlock_mex.cpp):
+ * real column layout. */
+int mlg_sparsemat_vec_rC(int r_size, const int* r_jump, const int* r_nJump,
+                         const float* m_val, int l_size, const int* l_jump,
+                         int l_nJump, const float* v, int nVec, float* w);
+
+/* Replaces bmSparseMat_r_nJump2index_mex
+ * (…/bmSparseMat_r_nJump2index/bmSparseMat_r_nJump2index_mex.cpp:12,70):
+ * out[out_length] = 0-based row index of every stored entry. */
+int mlg_sparsemat_r_nJump2index(int l_size, const int* r_nJump,
+                                long long out_length, int* out);
+
+/* Uploads a cpp_prepared bmSparseMat (host arrays, jump format of
+ * bmSparseMat.m:100-188) to the device as absolute-index CSR with a dense
+ * row pointer over l_size.  Column and row indices are validated. */
+int mlg_matrix_create(int r_size, const int* r_jump, const int* r_nJump,
+                      const float* m_val, int l_size, const int* l_jump,
+                      int l_nJump, mlg_matrix_t* out);
+int mlg_matrix_destroy(mlg_matrix_t m);
+int mlg_matrix_info(mlg_matrix_t m, long long* nnz, int* r_size, int* l_size);
+/* Rows holding at least one entry, and rows handled by the split long-row
+ * kernel (more than 256 entries). */
+int mlg_matrix_row_stats(mlg_matrix_t m, int* nonempty_rows, int* long_rows);
+/* Downloads the matrix back to jump format (sizes from mlg_matrix_info;
+ * l_nJump_out receives the number of non-empty rows written to r_nJump). */
+int mlg_matrix_download(mlg_matrix_t m, int* r_jump, int* r_nJump,
+                        float* m_val, int* l_jump, int* l_nJump_out);
+
+/* w = M v on the device, complex64 point layout: v [r_size][nVec],
+ * w [l_size][nVec]. */
+int mlg_matrix_spmm_dev(mlg_matrix_t m, const void* v, int nVec, void* w,
+                        void* stream);
+
+/* GPU form of src/gridding123/m/bmTraj2SparseMat.m:12-314 (Gu and Gut):
+ * t [imDim, nPt] (column-major, physical units), ve [nPt], N_u [imDim],
+ * dK_u [imDim]; kernelType MLG_KERNEL_GAUSS (params sigma, K_max) or
+ * MLG_KERNEL_KAISER (tau, alpha, K_max).  Rows normalised to sum 1, periodic
+ * wrap, samples outside the grid keep empty rows; Gut = Gu^T with empty rows
+ * squeezed.  Either output pointer may be NULL. */
+int mlg_traj2sparsemat(int imDim, int nPt, const double* t, const double* ve,
+                       const int* N_u, const double* dK_u, int kernelType,
+                       int nWin, const double* kernelParam, mlg_matrix_t* Gu,
+                       mlg_matrix_t* Gut);
+
+/* ---- deapodisation ------------------------------------------------------ */
+
+/* src/fourier123/prep_function/bmK.m:6-156 for one coil: K [prod(N_u)]
+ * (column order), computed in FP64 and rounded to single. */
+int mlg_deapodization(int imDim, const int* N_u, const double* dK_u,
+                      int kernelType, int nWin, const double* kernelParam,
+                      float* K);
+
+/* ---- fused operators (NUFFT plan) --------------------------------------- */
+
+/* A plan holds cuFFT plans, the sign-folded copies of Gu/Gut used by the
+ * fused operators, KFC and KFC_conj ([nCh, prod(n_u)] coil-major, host
+ * arrays as produced by src/fourier123/prep_function/bmKF.m and
+ * bmKF_conj.m) and work buffers.  N_u and n_u must be even; n_u <= N_u.
+ * Gu / Gut stay owned by the caller and must outlive the plan. */
+int mlg_plan_create(int imDim, const int* N_u, const int* n_u, int nCh,
+                    mlg_matrix_t Gu, mlg_matrix_t Gut, const float* KFC_re,
+                    const float* KFC_im, const float* KFCc_re,
+                    const float* KFCc_im, mlg_plan_t* out);
+int mlg_plan_destroy(mlg_plan_t p);
+/* k-space grid step dK_u [imDim] (default 1): sets the image-space volume
+ * element HX = prod((1/dK_u)/N_u) used by the solvers
+ * (src/fourier123/solver_function/imDim/nonCartesian/bmSensa.m:26-27). */
+int mlg_plan_set_dk(mlg_plan_t p, const double* dK_u);
+/* Device bytes held by the plan (excluding the caller's matrices). */
+int mlg_plan_device_bytes(mlg_plan_t p, long long* bytes);
+
+/* bmShanna (src/fourier123/map_function/nonCartesian/bmShanna_MATLAB.m:6-56)
+ * on device buffers: x [prod(n_u)] (or [nCh][prod(n_u)] if x_per_coil) ->
+ * y [nPt][nCh]. */
+int mlg_shanna_dev(mlg_plan_t p, const void* x, int x_per_coil, void* y,
+                   void* stream);
+/* bmNakatsha with C_flag = true (bmNakatsha_MATLAB.m:6-58): y [nPt][nCh] ->
+ * x [prod(n_u)] (coil-summed).  Optional row weights HY [nPt] (NULL = 1) are
+ * applied to y first and the result is multiplied by `scale`. */
+int mlg_nakatsha_dev(mlg_plan_t p, const void* y, const float* HY, float scale,
+                     void* x, void* stream);
+
+/* Host-buffer fused operators with the argument layouts fixed by the
+ * reference's call sites of its (absent) CUFFT MEX files:
+ * bmShanna{1,2,3}_CUFFT_omp_mex
+ * (src/fourier123/map_function/nonCartesian/bmShanna_CUFFT_omp.m:15-35) and
+ * bmNakatsha{1,2,3}_CUFFT_omp_mex (…/bmNakatsha_CUFFT_omp.m:17-36).
+ * x [prod(n_u), x_nCol] with x_nCol = 1 or nCh, KFC [prod(n_u), nCh],
+ * y [nPt, nCh]; G is the cpp_prepared jump format.  n_u == NULL means
+ * n_u = N_u (the reference's only supported case); otherwise zero-filling and
+ * cropping are fused. */
+int mlg_shanna(int imDim, const int* N_u, const int* n_u, int nCh,
+               const float* xR, const float* xI, int x_nCol,
+               const float* KFC_R, const float* KFC_I, int r_size,
+               const int* r_jump, const int* r_nJump, const float* m_val,
+               int l_size, const int* l_jump, int l_nJump, float* yR,
+               float* yI);
+int mlg_nakatsha(int imDim, const int* N_u, const int* n_u, int nCh,
+                 const float* yR, const float* yI, const float* KFCc_R,
+                 const float* KFCc_I, int r_size, const int* r_jump,
+                 const int* r_nJump, const float* m_val, int l_size,
+                 const int* l_jump, int l_nJump, float* xR, float* xI);
+
+/* bmIDF{1,2,3}_CUFFT_mex (called at
+ * src/fourier123/map_function/nonCartesian/bmMathilda.m:85-102):
+ * fftshift(ifft(ifftshift(x))) * prod(N_u)*prod(dK_u) over the first imDim
+ * dimensions of x [N_u..., nCol]. */
+int mlg_idf(int imDim, const int* N_u, const float* dK_u, int nCol,
+            const float* xR, const float* xI, float* yR, float* yI);
+
+/* Times the stages of one Shanna and one Nakatsha on the plan's stream with
+ * CUDA events, averaged over `iters` repetitions after one warm-up:
+ * ms[0] pre-FFT kernel, ms[1] forward cuFFT, ms[2] Gu product,
+ * ms[3] Gut product, ms[4] inverse cuFFT, ms[5] post-FFT kernel.
+ * Measurement helper; no reference counterpart. */
+int mlg_plan_profile(mlg_plan_t p, int iters, double* ms);
+
+/* ---- reconstructions ---------------------------------------------------- */
+
+/* CG-SENSE, src/fourier123/solver_function/imDim/nonCartesian/bmSensa.m:6-96:
+ * nIter outer iterations (the convergence condition's iteration cap), each
+ * a CG run of at most nCGD x-updates restarted from the current x.
+ * y [nPt][nCh] k-space (device, point layout), ve [nPt] (device), ve_max <=
+ * 0 means max(ve).  x [prod(n_u)] device image, in: initial guess, out:
+ * reconstruction.  residual (host, may be NULL) receives nIter values of
+ * ||y - Mx||^2_HY.  Dot products, norms and step sizes are FP64. */
+int mlg_sensa_dev(mlg_plan_t p, const void* y, const float* ve, float ve_max,
+                  int nIter, int nCGD, void* x, double* residual,
+                  void* stream);
+/* Same with host buffers in MATLAB layouts: yR/yI [nPt, nCh], ve [nPt],
+ * xR/xI [prod(n_u)] in/out.  Copies in and out are part of the call. */
+int mlg_sensa(mlg_plan_t p, const float* yR, const float* yI, const float* ve,
+              float ve_max, int nIter, int nCGD, float* xR, float* xI,
+              double* residual);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MONALISA_GPU_H */

@@ -1,0 +1,20 @@
+"""monalisa_b200 -- B200 (sm_100a) implementation of Monalisa's
+non-Cartesian gridding hot path: adjoint/forward gridding, the Gu/Gut
+gridding-matrix products, the fused Shanna/Nakatsha operators around cuFFT
+and the CG-SENSE reconstruction that calls them.
+
+The compute runs in libmonalisa_gpu.so (include/monalisa_gpu.h); this package
+mirrors the reference's MATLAB interface on top of it.
+"""
+from ._native import MonalisaError, launch_count  # noqa: F401
+from .gridding import bmGridder_n2u, bmGridder_n2u_leight  # noqa: F401
+from .operators import (NufftPlan, bmCoilSense_pinv, bmIDF, bmK, bmKF, bmKF_conj, bmMathilda,  # noqa: F401
+                        bmNakatsha, bmShanna)
+from .solvers import SensaRecon, bmSensa  # noqa: F401
+from .sparsemat import DeviceMatrix, bmSparseMat, bmSparseMat_vec, bmTraj2SparseMat  # noqa: F401
+
+__all__ = [
+    "MonalisaError", "bmGridder_n2u", "bmGridder_n2u_leight", "NufftPlan", "bmIDF", "bmK", "bmKF", "bmKF_conj",
+    "bmMathilda", "bmNakatsha", "bmShanna", "bmCoilSense_pinv", "SensaRecon", "bmSensa", "DeviceMatrix",
+    "bmSparseMat", "bmSparseMat_vec", "bmTraj2SparseMat", "launch_count",
+]

@@ -1,0 +1,217 @@
+// Error plumbing, device selection, stream-ordered allocation, CSR upload
+// from the jump format, and the deterministic FP64 reduction used by the
+// solvers.
+#include <cstdarg>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "mlg_internal.cuh"
+
+namespace mlg {
+
+std::atomic<long long> g_launches{0};
+static thread_local std::string t_last_error;
+static thread_local int t_device = -1;
+
+void set_error(const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  t_last_error = buf;
+}
+
+int fail(int status, const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  t_last_error = buf;
+  return status;
+}
+
+int ensure_device() {
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    return fail(MLG_ERR_NO_DEVICE, "no CUDA device visible (%s)", cudaGetErrorString(e));
+  }
+  if (t_device >= 0) MLG_CUDA(cudaSetDevice(t_device));
+  int dev = 0;
+  MLG_CUDA(cudaGetDevice(&dev));
+  static std::mutex mu;
+  static std::vector<bool> pool_ready;
+  std::lock_guard<std::mutex> lk(mu);
+  if ((int)pool_ready.size() <= dev) pool_ready.resize(dev + 1, false);
+  if (!pool_ready[dev]) {
+    // Keep freed blocks in the default pool: repeated per-call work buffers
+    // then cost no cudaMalloc after the first call.
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+      uint64_t thr = UINT64_MAX;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+    cudaGetLastError();
+    pool_ready[dev] = true;
+  }
+  return MLG_OK;
+}
+
+int dev_alloc(void** p, size_t bytes, cudaStream_t s) {
+  *p = nullptr;
+  cudaError_t e = cudaMallocAsync(p, bytes, s);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    *p = nullptr;
+    return fail(e == cudaErrorMemoryAllocation ? MLG_ERR_OOM : MLG_ERR_CUDA,
+                "device allocation of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
+  }
+  return MLG_OK;
+}
+
+void dev_free(void* p, cudaStream_t s) {
+  if (p) cudaFreeAsync(p, s);
+}
+
+void csr_free(Csr& c) {
+  cudaFree(c.row_ptr);
+  cudaFree(c.col);
+  cudaFree(c.val);
+  cudaFree(c.long_rows);
+  c = Csr();
+}
+
+// Decodes the jump format on the host (one pass, 64-bit running indices,
+// every index range-checked), then uploads.  bmSparseMat.m:135-166 defines
+// the format: r_jump/l_jump hold deltas whose first entry is absolute.
+int csr_from_jump(int r_size, const int* r_jump, const int* r_nJump, const float* m_val, int l_size,
+                  const int* l_jump, int l_nJump, Csr& out, cudaStream_t s) {
+  MLG_CHECK(r_size > 0 && l_size > 0, "matrix sizes must be positive (r_size=%d l_size=%d)", r_size, l_size);
+  MLG_CHECK(l_nJump >= 0 && r_nJump != nullptr, "r_nJump missing");
+  MLG_CHECK(l_jump != nullptr || l_nJump == l_size,
+            "without l_jump the matrix must store every row (l_nJump=%d, l_size=%d)", l_nJump, l_size);
+  long long nnz = 0;
+  for (int i = 0; i < l_nJump; ++i) {
+    MLG_CHECK(r_nJump[i] >= 0, "negative r_nJump at row %d", i);
+    nnz += r_nJump[i];
+  }
+  MLG_CHECK(nnz < (1LL << 32) - 1, "nnz=%lld exceeds the 32-bit row pointer", nnz);
+  MLG_CHECK(nnz == 0 || (r_jump && m_val), "r_jump / m_val missing");
+
+  std::vector<uint32_t> row_ptr((size_t)l_size + 1, 0);
+  long long row = -1;
+  for (int i = 0; i < l_nJump; ++i) {
+    // the first l_jump is the absolute 0-based row, later ones are deltas
+    long long r = l_jump ? (i == 0 ? (long long)l_jump[0] : row + l_jump[i]) : i;
+    MLG_CHECK(r > row && r < l_size, "row index %lld out of order or range at stored row %d", r, i);
+    row = r;
+    row_ptr[(size_t)r + 1] = (uint32_t)r_nJump[i];
+  }
+  for (int r = 0; r < l_size; ++r) row_ptr[(size_t)r + 1] += row_ptr[r];
+
+  std::vector<int> col((size_t)nnz);
+  long long c = 0;
+  for (long long e = 0; e < nnz; ++e) {
+    c += r_jump[e];
+    MLG_CHECK(c >= 0 && c < r_size, "column index %lld out of range [0,%d) at entry %lld", c, r_size, e);
+    col[(size_t)e] = (int)c;
+  }
+
+  Csr m;
+  m.r_size = r_size;
+  m.l_size = l_size;
+  m.nnz = nnz;
+  cudaError_t e1 = cudaMalloc(&m.row_ptr, sizeof(uint32_t) * ((size_t)l_size + 1));
+  cudaError_t e2 = cudaMalloc(&m.col, sizeof(int) * (size_t)(nnz ? nnz : 1));
+  cudaError_t e3 = cudaMalloc(&m.val, sizeof(float) * (size_t)(nnz ? nnz : 1));
+  if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess) {
+    cudaGetLastError();
+    csr_free(m);
+    return fail(MLG_ERR_OOM, "matrix upload: device allocation failed (nnz=%lld)", nnz);
+  }
+  MLG_CUDA(cudaMemcpyAsync(m.row_ptr, row_ptr.data(), sizeof(uint32_t) * row_ptr.size(), cudaMemcpyHostToDevice, s));
+  if (nnz) {
+    MLG_CUDA(cudaMemcpyAsync(m.col, col.data(), sizeof(int) * (size_t)nnz, cudaMemcpyHostToDevice, s));
+    MLG_CUDA(cudaMemcpyAsync(m.val, m_val, sizeof(float) * (size_t)nnz, cudaMemcpyHostToDevice, s));
+  }
+  std::vector<int> longs;
+  int nonempty = 0;
+  for (int r = 0; r < l_size; ++r) {
+    uint32_t len = row_ptr[(size_t)r + 1] - row_ptr[r];
+    nonempty += len > 0;
+    if (len > (uint32_t)kLongRow) longs.push_back(r);
+  }
+  m.n_long = (int)longs.size();
+  m.n_nonempty = nonempty;
+  if (!longs.empty()) {
+    MLG_CUDA(cudaMalloc(&m.long_rows, sizeof(int) * longs.size()));
+    MLG_CUDA(cudaMemcpyAsync(m.long_rows, longs.data(), sizeof(int) * longs.size(), cudaMemcpyHostToDevice, s));
+  }
+  MLG_CUDA(cudaStreamSynchronize(s));  // host vectors go out of scope
+  out = m;
+  return MLG_OK;
+}
+
+// ---- deterministic reduction ---------------------------------------------
+__global__ void reduce_partials_kernel(const double* __restrict__ partial, int n, double* out) {
+  // One CTA; fixed per-thread strided order, fixed tree: bitwise
+  // reproducible for a given n.
+  __shared__ double sh[256];
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) acc += partial[i];
+  sh[threadIdx.x] = acc;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[0] = sh[0];
+}
+
+int reduce_partials(const double* partial, int n, double* out, cudaStream_t s) {
+  reduce_partials_kernel<<<1, 256, 0, s>>>(partial, n, out);
+  MLG_LAUNCHED();
+  return MLG_OK;
+}
+
+}  // namespace mlg
+
+// ---- C ABI: library ---------------------------------------------------------
+extern "C" {
+
+int mlg_version(void) { return 10000; }
+
+const char* mlg_status_string(int status) {
+  switch (status) {
+    case MLG_OK: return "ok";
+    case MLG_ERR_ARG: return "invalid argument";
+    case MLG_ERR_OOM: return "out of device memory";
+    case MLG_ERR_CUDA: return "CUDA error";
+    case MLG_ERR_TIMEOUT: return "timeout";
+    case MLG_ERR_STATE: return "invalid state";
+    case MLG_ERR_UNSUPPORTED: return "unsupported";
+    case MLG_ERR_NO_DEVICE: return "no CUDA device";
+    default: return "unknown status";
+  }
+}
+
+const char* mlg_last_error(void) { return mlg::t_last_error.c_str(); }
+
+int mlg_set_device(int device) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) {
+    cudaGetLastError();
+    return mlg::fail(MLG_ERR_ARG, "device %d not available (%d visible)", device, n);
+  }
+  mlg::t_device = device;
+  MLG_CUDA(cudaSetDevice(device));
+  return MLG_OK;
+}
+
+long long mlg_kernel_launch_count(void) { return mlg::g_launches.load(); }
+
+}  // extern "C"

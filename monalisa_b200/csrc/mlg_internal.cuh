@@ -1,0 +1,182 @@
+// Internal declarations shared by the libmonalisa_gpu translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cufft.h>
+
+#include <atomic>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+
+#include "../../include/monalisa_gpu.h"
+
+namespace mlg {
+
+// ---- status / error plumbing ----------------------------------------------
+void set_error(const char* fmt, ...);
+int fail(int status, const char* fmt, ...);
+const char* cuda_name(cudaError_t e);
+
+extern std::atomic<long long> g_launches;
+inline void count_launch(long long n = 1) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+#define MLG_CUDA(call)                                                                  \
+  do {                                                                                  \
+    cudaError_t e_ = (call);                                                            \
+    if (e_ != cudaSuccess) {                                                            \
+      return ::mlg::fail(e_ == cudaErrorMemoryAllocation ? MLG_ERR_OOM : MLG_ERR_CUDA,  \
+                         "%s:%d %s: %s", __FILE__, __LINE__, #call, cudaGetErrorString(e_)); \
+    }                                                                                   \
+  } while (0)
+
+#define MLG_CUFFT(call)                                                                 \
+  do {                                                                                  \
+    cufftResult r_ = (call);                                                            \
+    if (r_ != CUFFT_SUCCESS) {                                                          \
+      return ::mlg::fail(r_ == CUFFT_ALLOC_FAILED ? MLG_ERR_OOM : MLG_ERR_CUDA,         \
+                         "%s:%d %s: cufft status %d", __FILE__, __LINE__, #call, (int)r_); \
+    }                                                                                   \
+  } while (0)
+
+#define MLG_CHECK(cond, ...)                              \
+  do {                                                    \
+    if (!(cond)) return ::mlg::fail(MLG_ERR_ARG, __VA_ARGS__); \
+  } while (0)
+
+#define MLG_TRY(expr)            \
+  do {                           \
+    int s_ = (expr);             \
+    if (s_ != MLG_OK) return s_; \
+  } while (0)
+
+// After a launch: records a launch and checks the launch configuration.
+#define MLG_LAUNCHED()                                                   \
+  do {                                                                   \
+    ::mlg::count_launch();                                               \
+    cudaError_t e_ = cudaGetLastError();                                 \
+    if (e_ != cudaSuccess)                                               \
+      return ::mlg::fail(MLG_ERR_CUDA, "%s:%d launch: %s", __FILE__, __LINE__, \
+                         cudaGetErrorString(e_));                        \
+  } while (0)
+
+int ensure_device();  // MLG_ERR_NO_DEVICE if no usable GPU
+
+// ---- device buffers -------------------------------------------------------
+// Stream-ordered allocation from the device's default memory pool (kept
+// warm: the release threshold is raised once per device).
+int dev_alloc(void** p, size_t bytes, cudaStream_t s);
+void dev_free(void* p, cudaStream_t s);
+
+template <typename T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  cudaStream_t s = nullptr;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { reset(); }
+  int alloc(size_t count, cudaStream_t stream) {
+    reset();
+    s = stream;
+    n = count;
+    if (count == 0) return MLG_OK;
+    return dev_alloc(reinterpret_cast<void**>(&p), count * sizeof(T), stream);
+  }
+  void reset() {
+    if (p) dev_free(p, s);
+    p = nullptr;
+    n = 0;
+  }
+  T* release() {
+    T* q = p;
+    p = nullptr;
+    n = 0;
+    return q;
+  }
+};
+
+// ---- device CSR -----------------------------------------------------------
+// Absolute-index CSR with a dense row pointer over all l_size rows (rows the
+// jump format squeezes out are empty).  Long rows (more than kLongRow
+// entries) are listed separately so that one CTA can split them.
+constexpr int kLongRow = 256;
+
+struct Csr {
+  int r_size = 0;         // number of columns
+  int l_size = 0;         // number of rows
+  long long nnz = 0;
+  uint32_t* row_ptr = nullptr;  // [l_size + 1]
+  int* col = nullptr;           // [nnz]
+  float* val = nullptr;         // [nnz]
+  int* long_rows = nullptr;     // rows with > kLongRow entries
+  int n_long = 0;
+  int n_nonempty = 0;
+};
+
+void csr_free(Csr& c);
+
+}  // namespace mlg
+
+struct mlg_matrix_s {
+  mlg::Csr csr;
+  int device = 0;
+};
+
+namespace mlg {
+
+// Builds a Csr from host jump-format arrays (validated).
+int csr_from_jump(int r_size, const int* r_jump, const int* r_nJump, const float* m_val, int l_size,
+                  const int* l_jump, int l_nJump, Csr& out, cudaStream_t s);
+// Finishes a Csr whose row_ptr/col/val are already on the device: lists the
+// long rows and counts the non-empty ones.
+int csr_index_long_rows(Csr& c, cudaStream_t s);
+// Copies `src` with each value multiplied by +1/-1 per row (row_sign) or per
+// column (col_sign), sign(i) = (-1)^(x+y+z) of linear cell index i on grid N.
+int csr_sign_copy(const Csr& src, bool by_row, int imDim, const int* N, float global_sign, Csr& dst,
+                  cudaStream_t s);
+// Frees a copy made by csr_sign_copy (only its values are owned).
+void csr_free_sign_copy(Csr& c);
+
+// ---- SpMM kernels (mlg_sparsemat.cu) ---------------------------------------
+// Element layouts of the dense operands.
+enum class Layout : int {
+  kPointC64 = 0,   // float2 [rows][nCh]          (coil fastest, interleaved)
+  kCoilC64 = 1,    // float2 [nCh][rows]          (coil major, interleaved)
+  kCoilSplit = 2,  // float re[nCh][rows], im[...] (MATLAB column layout)
+  kPointSplit = 3, // float re[rows][nCh], im[...] (MATLAB point layout)
+  kCoilReal = 4,   // float [nCh][rows]           (real, column layout)
+};
+
+struct Operand {
+  Layout layout = Layout::kPointC64;
+  void* a = nullptr;        // float2* or float* (re)
+  void* b = nullptr;        // im (split layouts)
+  long long rows = 0;       // leading dimension for coil-major layouts
+};
+
+struct SpmmArgs {
+  const Csr* m = nullptr;
+  int nCh = 1;
+  Operand in;
+  Operand out;
+  const float* in_row_scale = nullptr;  // multiplies input row j (e.g. HY)
+  float out_scale = 1.0f;
+  // Optional per-row normalisation (bmGridder_n2u): divides each output row
+  // by the sum of its weights, 1 if that sum is < 1e-5.
+  bool normalize = false;
+  // Optional FP64 partial sums of sum_rows w_row * |out|^2 (w = row weight,
+  // NULL = 1): one double per CTA written to partial[], count in *n_partial.
+  const float* sqn_row_weight = nullptr;
+  double* partial = nullptr;
+};
+
+int spmm(const SpmmArgs& a, cudaStream_t s);
+// Number of FP64 partial sums spmm writes for this matrix / mapping.
+int spmm_partial_count(const SpmmArgs& a);
+
+// Deterministic final reduction of partial sums: out[0] = sum partial[0..n).
+int reduce_partials(const double* partial, int n, double* out, cudaStream_t s);
+
+}  // namespace mlg

@@ -1,0 +1,418 @@
+// CG-SENSE on the device: the semantics of
+// src/fourier123/solver_function/imDim/nonCartesian/bmSensa.m:6-96.
+//
+// All step sizes live in device memory as FP64 and every dot product is an
+// FP64 sum of per-CTA partials reduced in a fixed order, so one CG step is a
+// fixed sequence of launches with no host synchronisation: it is captured
+// once into a CUDA graph and replayed.  The reference's early exit
+// (sqn < 10*eps('single'), bmSensa.m:54) becomes a device flag that freezes
+// the updates of x for the rest of the inner loop.
+#include <algorithm>
+#include <cfloat>
+#include <vector>
+
+#include "mlg_plan.cuh"
+
+namespace mlg {
+
+// device scalar slots
+enum : int {
+  S_SQN_CURR = 0,  // sqn_dagM_res_curr
+  S_SQN_MP = 1,
+  S_A = 2,
+  S_B = 3,
+  S_R = 4,         // monitoring residual
+  S_DONE = 5,      // 1.0 once sqn_curr < eps (inner loop stopped)
+  S_COUNT = 8
+};
+
+constexpr int kT = 256;
+
+static int grid1(long long n) {
+  return (int)std::max<long long>(1, std::min<long long>((n + kT - 1) / kT, 148LL * 16));
+}
+
+__device__ __forceinline__ double block_reduce(double v, double* sh) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (threadIdx.x == 0)
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += sh[i];
+  return t;
+}
+
+// fixed-order sum of n partials (one CTA)
+__device__ double sum_partials(const double* __restrict__ partial, int n, double* sh) {
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) acc += partial[i];
+  __shared__ double sh2[kT];
+  sh2[threadIdx.x] = acc;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) sh2[threadIdx.x] += sh2[threadIdx.x + w];
+    __syncthreads();
+  }
+  (void)sh;
+  return sh2[0];
+}
+
+// HY = min(ve, ve_max)   (bmSensa.m:29-32)
+__global__ void hy_kernel(const float* __restrict__ ve, int n, float ve_max, float* __restrict__ HY) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) HY[i] = fminf(ve[i], ve_max);
+}
+
+__global__ void max_kernel(const float* __restrict__ v, int n, float* out) {
+  __shared__ float sh[kT];
+  float m = -FLT_MAX;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) m = fmaxf(m, v[i]);
+  sh[threadIdx.x] = m;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) sh[threadIdx.x] = fmaxf(sh[threadIdx.x], sh[threadIdx.x + w]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[0] = sh[0];
+}
+
+// res = y - Mx (k-space), optional partials of sum HY |res|^2
+__global__ void residual_kernel(const float2* __restrict__ y, const float2* __restrict__ Mx, long long n, int nCh,
+                                const float* __restrict__ HY, float2* __restrict__ res, double* partial) {
+  __shared__ double sh[kT / 32];
+  double sq = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const float2 a = y[i], b = Mx[i];
+    const float2 r = make_float2(__fsub_rn(a.x, b.x), __fsub_rn(a.y, b.y));
+    if (res) res[i] = r;
+    sq += (double)HY[i / nCh] * ((double)r.x * r.x + (double)r.y * r.y);
+  }
+  if (partial) {
+    const double t = block_reduce(sq, sh);
+    if (threadIdx.x == 0) partial[blockIdx.x] = t;
+  }
+}
+
+// sqn_curr = HX * sum(partials); done = sqn_curr < eps   (bmSensa.m:45,54)
+__global__ void cg_init_kernel(const double* __restrict__ partial, int n, double HX, double eps, double* sc) {
+  __shared__ double sh[kT / 32];
+  const double s = sum_partials(partial, n, sh);
+  if (threadIdx.x == 0) {
+    sc[S_SQN_CURR] = HX * s;
+    sc[S_DONE] = (HX * s < eps) ? 1.0 : 0.0;
+  }
+}
+
+// sqn_Mp = sum(partials); a = sqn_curr / sqn_Mp   (bmSensa.m:59-61)
+__global__ void cg_alpha_kernel(const double* __restrict__ partial, int n, double* sc) {
+  __shared__ double sh[kT / 32];
+  const double s = sum_partials(partial, n, sh);
+  if (threadIdx.x == 0) {
+    sc[S_SQN_MP] = s;
+    sc[S_A] = sc[S_DONE] != 0.0 ? 0.0 : sc[S_SQN_CURR] / s;
+  }
+}
+
+// sqn_next = HX * sum; b = sqn_next / sqn_curr; sqn_curr = sqn_next;
+// done once sqn_curr < eps   (bmSensa.m:72-75 and the check of :54)
+__global__ void cg_beta_kernel(const double* __restrict__ partial, int n, double HX, double eps, double* sc) {
+  __shared__ double sh[kT / 32];
+  const double s = sum_partials(partial, n, sh);
+  if (threadIdx.x == 0) {
+    const double next = HX * s;
+    if (sc[S_DONE] == 0.0) {
+      sc[S_B] = next / sc[S_SQN_CURR];
+      sc[S_SQN_CURR] = next;
+      if (next < eps) sc[S_DONE] = 1.0;
+    }
+  }
+}
+
+__global__ void sum_to_slot_kernel(const double* __restrict__ partial, int n, double* sc, int slot) {
+  __shared__ double sh[kT / 32];
+  const double s = sum_partials(partial, n, sh);
+  if (threadIdx.x == 0) sc[slot] = s;
+}
+
+// x += a p   (bmSensa.m:63)
+__global__ void cg_update_x_kernel(float2* __restrict__ x, const float2* __restrict__ p, long long n,
+                                   const double* __restrict__ sc) {
+  if (sc[S_DONE] != 0.0) return;
+  const float a = (float)sc[S_A];
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const float2 pv = p[i];
+    float2 xv = x[i];
+    xv.x = __fadd_rn(xv.x, __fmul_rn(a, pv.x));
+    xv.y = __fadd_rn(xv.y, __fmul_rn(a, pv.y));
+    x[i] = xv;
+  }
+}
+
+// res -= a Mp   (bmSensa.m:71)
+__global__ void cg_update_res_kernel(float2* __restrict__ res, const float2* __restrict__ Mp, long long n,
+                                     const double* __restrict__ sc) {
+  if (sc[S_DONE] != 0.0) return;
+  const float a = (float)sc[S_A];
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const float2 m = Mp[i];
+    float2 r = res[i];
+    r.x = __fsub_rn(r.x, __fmul_rn(a, m.x));
+    r.y = __fsub_rn(r.y, __fmul_rn(a, m.y));
+    res[i] = r;
+  }
+}
+
+// p = dagM + b p   (bmSensa.m:77)
+__global__ void cg_update_p_kernel(float2* __restrict__ p, const float2* __restrict__ dagM, long long n,
+                                   const double* __restrict__ sc) {
+  if (sc[S_DONE] != 0.0) return;
+  const float b = (float)sc[S_B];
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const float2 d = dagM[i], pv = p[i];
+    p[i] = make_float2(__fadd_rn(d.x, __fmul_rn(b, pv.x)), __fadd_rn(d.y, __fmul_rn(b, pv.y)));
+  }
+}
+
+static int ensure_solver_buffers(mlg_plan_s* p) {
+  if (p->x_p && p->solver_nPt == p->nPt) return MLG_OK;
+  cudaFree(p->x_p);
+  cudaFree(p->x_dagM);
+  cudaFree(p->k_res);
+  cudaFree(p->k_Mp);
+  cudaFree(p->HY);
+  const size_t ni = sizeof(float2) * (size_t)p->nu_tot, nk = sizeof(float2) * (size_t)p->nPt * p->nCh;
+  if (cudaMalloc(&p->x_p, ni) != cudaSuccess || cudaMalloc(&p->x_dagM, ni) != cudaSuccess ||
+      cudaMalloc(&p->k_res, nk) != cudaSuccess || cudaMalloc(&p->k_Mp, nk) != cudaSuccess ||
+      cudaMalloc(&p->HY, sizeof(float) * (size_t)std::max(1, p->nPt)) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(MLG_ERR_OOM, "solver work buffers: device allocation failed");
+  }
+  p->solver_nPt = p->nPt;
+  p->bytes += 2 * ni + 2 * nk + sizeof(float) * (size_t)p->nPt;
+  return MLG_OK;
+}
+
+// One inner CG step i < nCGD (bmSensa.m:50-77 without the final break).
+static int cg_step(mlg_plan_s* p, float2* x, double HX, double eps, cudaStream_t s) {
+  const long long nk = (long long)p->nPt * p->nCh;
+  int np = 0;
+  MLG_TRY(shanna_run(p, p->x_p, false, p->k_Mp, p->HY, p->partial, &np, s));
+  cg_alpha_kernel<<<1, kT, 0, s>>>(p->partial, np, p->scalars);
+  MLG_LAUNCHED();
+  cg_update_x_kernel<<<grid1(p->nu_tot), kT, 0, s>>>(x, p->x_p, p->nu_tot, p->scalars);
+  MLG_LAUNCHED();
+  cg_update_res_kernel<<<grid1(nk), kT, 0, s>>>(p->k_res, p->k_Mp, nk, p->scalars);
+  MLG_LAUNCHED();
+  MLG_TRY(nakatsha_run(p, p->k_res, p->HY, (float)(1.0 / HX), p->x_dagM, p->partial, &np, s));
+  cg_beta_kernel<<<1, kT, 0, s>>>(p->partial, np, HX, eps, p->scalars);
+  MLG_LAUNCHED();
+  cg_update_p_kernel<<<grid1(p->nu_tot), kT, 0, s>>>(p->x_p, p->x_dagM, p->nu_tot, p->scalars);
+  MLG_LAUNCHED();
+  return MLG_OK;
+}
+
+int sensa_run(mlg_plan_s* p, const float2* y, const float* ve, float ve_max, int nIter, int nCGD, float2* x,
+              double* residual, bool use_graph, cudaStream_t s) {
+  MLG_CHECK(p->Gu && p->Gut, "CG-SENSE needs a plan with both Gu and Gut");
+  MLG_CHECK(nIter >= 0 && nCGD >= 0, "nIter / nCGD must be >= 0");
+  MLG_TRY(ensure_solver_buffers(p));
+  const long long nk = (long long)p->nPt * p->nCh;
+  const double HX = p->HX;
+  const double eps = 10.0 * (double)FLT_EPSILON;  // bmSensa.m:11
+  // HY = min(ve, ve_max), ve_max = max(ve) when not given (bmSensa.m:29-32)
+  float vmax = ve_max;
+  if (!(vmax > 0.f)) {
+    float* dmax = (float*)(p->scalars + S_COUNT);
+    max_kernel<<<1, kT, 0, s>>>(ve, p->nPt, dmax);
+    MLG_LAUNCHED();
+    MLG_CUDA(cudaMemcpyAsync(&vmax, dmax, sizeof(float), cudaMemcpyDeviceToHost, s));
+    MLG_CUDA(cudaStreamSynchronize(s));
+  }
+  hy_kernel<<<grid1(p->nPt), kT, 0, s>>>(ve, p->nPt, vmax, p->HY);
+  MLG_LAUNCHED();
+
+  const int full = std::max(0, nCGD - 1);  // inner steps that run to p_next
+  if (use_graph && full > 0 && (!p->cg_graph || p->cg_graph_x != x)) {
+    if (p->cg_graph) cudaGraphExecDestroy(p->cg_graph);
+    p->cg_graph = nullptr;
+    cudaGraph_t graph;
+    MLG_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    const long long before = g_launches.load();
+    const int st = cg_step(p, x, HX, eps, s);
+    const cudaError_t ce = cudaStreamEndCapture(s, &graph);
+    p->cg_graph_kernels = g_launches.load() - before;
+    g_launches.fetch_sub(p->cg_graph_kernels);  // captured, not launched
+    if (st != MLG_OK) return st;
+    if (ce != cudaSuccess) return fail(MLG_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(ce));
+    const cudaError_t ie = cudaGraphInstantiate(&p->cg_graph, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ie != cudaSuccess) return fail(MLG_ERR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(ie));
+    p->cg_graph_x = x;
+  }
+
+  DevBuf<double> hist;
+  MLG_TRY(hist.alloc(std::max(1, nIter), s));
+  for (int it = 0; it < nIter; ++it) {
+    // res = y - M x; dagM = (1/HX) M*(HY res); sqn = HX |dagM|^2; p = dagM
+    int np = 0;
+    MLG_TRY(shanna_run(p, x, false, p->k_Mp, nullptr, nullptr, nullptr, s));
+    residual_kernel<<<grid1(nk), kT, 0, s>>>(y, p->k_Mp, nk, p->nCh, p->HY, p->k_res, nullptr);
+    MLG_LAUNCHED();
+    MLG_TRY(nakatsha_run(p, p->k_res, p->HY, (float)(1.0 / HX), p->x_dagM, p->partial, &np, s));
+    cg_init_kernel<<<1, kT, 0, s>>>(p->partial, np, HX, eps, p->scalars);
+    MLG_LAUNCHED();
+    MLG_CUDA(cudaMemcpyAsync(p->x_p, p->x_dagM, sizeof(float2) * (size_t)p->nu_tot, cudaMemcpyDeviceToDevice, s));
+    for (int i = 0; i < full; ++i) {
+      if (use_graph) {
+        MLG_CUDA(cudaGraphLaunch(p->cg_graph, s));
+        count_launch(p->cg_graph_kernels);
+      } else {
+        MLG_TRY(cg_step(p, x, HX, eps, s));
+      }
+    }
+    if (nCGD > 0) {  // the last step stops after x += a p (bmSensa.m:67-69)
+      MLG_TRY(shanna_run(p, p->x_p, false, p->k_Mp, p->HY, p->partial, &np, s));
+      cg_alpha_kernel<<<1, kT, 0, s>>>(p->partial, np, p->scalars);
+      MLG_LAUNCHED();
+      cg_update_x_kernel<<<grid1(p->nu_tot), kT, 0, s>>>(x, p->x_p, p->nu_tot, p->scalars);
+      MLG_LAUNCHED();
+    }
+    // monitoring: R = |y - Mx|^2_HY   (bmSensa.m:82-83)
+    MLG_TRY(shanna_run(p, x, false, p->k_Mp, nullptr, nullptr, nullptr, s));
+    const int g = grid1(nk);
+    residual_kernel<<<g, kT, 0, s>>>(y, p->k_Mp, nk, p->nCh, p->HY, nullptr, p->partial);
+    MLG_LAUNCHED();
+    sum_to_slot_kernel<<<1, kT, 0, s>>>(p->partial, g, hist.p, it);
+    MLG_LAUNCHED();
+  }
+  if (residual && nIter > 0) {
+    MLG_CUDA(cudaMemcpyAsync(residual, hist.p, sizeof(double) * nIter, cudaMemcpyDeviceToHost, s));
+    MLG_CUDA(cudaStreamSynchronize(s));
+  }
+  return MLG_OK;
+}
+
+}  // namespace mlg
+
+using namespace mlg;
+
+extern "C" {
+
+int mlg_plan_set_dk(mlg_plan_t p, const double* dK_u) {
+  MLG_CHECK(p && dK_u, "NULL argument");
+  double hx = 1.0;
+  for (int d = 0; d < p->imDim; ++d) {
+    MLG_CHECK(dK_u[d] > 0, "dK_u must be > 0");
+    // single-precision arithmetic of bmSensa.m:26-27
+    const float dx = (1.0f / (float)dK_u[d]) / (float)p->N[d];
+    hx = (double)((float)hx * dx);
+  }
+  p->HX = hx;
+  return MLG_OK;
+}
+
+int mlg_sensa_dev(mlg_plan_t p, const void* y, const float* ve, float ve_max, int nIter, int nCGD, void* x,
+                  double* residual, void* stream) {
+  MLG_CHECK(p && y && ve && x, "NULL argument");
+  MLG_CUDA(cudaSetDevice(p->device));
+  cudaStream_t user = (cudaStream_t)stream;
+  MLG_CUDA(cudaEventRecord(p->ev_in, user));
+  MLG_CUDA(cudaStreamWaitEvent(p->stream, p->ev_in, 0));
+  int st = sensa_run(p, (const float2*)y, ve, ve_max, nIter, nCGD, (float2*)x, residual, true, p->stream);
+  cudaEventRecord(p->ev_out, p->stream);
+  cudaStreamWaitEvent(user, p->ev_out, 0);
+  return st;
+}
+
+int mlg_sensa(mlg_plan_t p, const float* yR, const float* yI, const float* ve, float ve_max, int nIter, int nCGD,
+              float* xR, float* xI, double* residual) {
+  MLG_CHECK(p && yR && yI && ve && xR && xI, "NULL argument");
+  MLG_CUDA(cudaSetDevice(p->device));
+  cudaStream_t s = p->stream;
+  const long long nk = (long long)p->nPt * p->nCh, nx = p->nu_tot;
+  DevBuf<float> dy, dve, dx;
+  DevBuf<float2> y2, x2;
+  MLG_TRY(dy.alloc(2 * nk, s));
+  MLG_TRY(dve.alloc(p->nPt, s));
+  MLG_TRY(dx.alloc(2 * nx, s));
+  MLG_TRY(y2.alloc(nk, s));
+  MLG_TRY(x2.alloc(nx, s));
+  MLG_CUDA(cudaMemcpyAsync(dy.p, yR, sizeof(float) * nk, cudaMemcpyHostToDevice, s));
+  MLG_CUDA(cudaMemcpyAsync(dy.p + nk, yI, sizeof(float) * nk, cudaMemcpyHostToDevice, s));
+  MLG_CUDA(cudaMemcpyAsync(dve.p, ve, sizeof(float) * p->nPt, cudaMemcpyHostToDevice, s));
+  MLG_CUDA(cudaMemcpyAsync(dx.p, xR, sizeof(float) * nx, cudaMemcpyHostToDevice, s));
+  MLG_CUDA(cudaMemcpyAsync(dx.p + nx, xI, sizeof(float) * nx, cudaMemcpyHostToDevice, s));
+  MLG_TRY(mlg::pack_col_to_point(dy.p, dy.p + nk, p->nPt, p->nCh, y2.p, s));
+  MLG_TRY(mlg::interleave(dx.p, dx.p + nx, nx, x2.p, s));
+  MLG_TRY(sensa_run(p, y2.p, dve.p, ve_max, nIter, nCGD, x2.p, residual, true, s));
+  MLG_TRY(mlg::deinterleave(x2.p, nx, dx.p, dx.p + nx, s));
+  MLG_CUDA(cudaMemcpyAsync(xR, dx.p, sizeof(float) * nx, cudaMemcpyDeviceToHost, s));
+  MLG_CUDA(cudaMemcpyAsync(xI, dx.p + nx, sizeof(float) * nx, cudaMemcpyDeviceToHost, s));
+  MLG_CUDA(cudaStreamSynchronize(s));
+  return MLG_OK;
+}
+
+}  // extern "C"
+
+// ---- stage timing -------------------------------------------------------------
+namespace mlg {
+namespace {
+
+struct Timer {
+  cudaEvent_t a = nullptr, b = nullptr;
+  Timer() {
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+  }
+  ~Timer() {
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+  }
+};
+
+}  // namespace
+}  // namespace mlg
+
+extern "C" int mlg_plan_profile(mlg_plan_t p, int iters, double* ms) {
+  using namespace mlg;
+  MLG_CHECK(p && ms && iters >= 1, "invalid argument");
+  MLG_CHECK(p->Gu && p->Gut, "profiling needs a plan with both Gu and Gut");
+  MLG_CUDA(cudaSetDevice(p->device));
+  MLG_TRY(ensure_solver_buffers(p));
+  cudaStream_t s = p->stream;
+  const long long nk = (long long)p->nPt * p->nCh;
+  MLG_CUDA(cudaMemsetAsync(p->x_p, 0, sizeof(float2) * (size_t)p->nu_tot, s));
+  MLG_CUDA(cudaMemsetAsync(p->k_res, 0, sizeof(float2) * (size_t)nk, s));
+  Timer t[6];
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  for (int it = 0; it <= iters; ++it) {
+    // Shanna stages
+    cudaEventRecord(t[0].a, s);
+    MLG_TRY(shanna_pre(p, p->x_p, false, s));
+    cudaEventRecord(t[0].b, s);
+    cudaEventRecord(t[1].a, s);
+    MLG_TRY(fft_exec(p, true, s));
+    cudaEventRecord(t[1].b, s);
+    cudaEventRecord(t[2].a, s);
+    MLG_TRY(shanna_spmm(p, p->k_Mp, nullptr, nullptr, nullptr, s));
+    cudaEventRecord(t[2].b, s);
+    // Nakatsha stages
+    cudaEventRecord(t[3].a, s);
+    MLG_TRY(nakatsha_spmm(p, p->k_res, nullptr, s));
+    cudaEventRecord(t[3].b, s);
+    cudaEventRecord(t[4].a, s);
+    MLG_TRY(fft_exec(p, false, s));
+    cudaEventRecord(t[4].b, s);
+    cudaEventRecord(t[5].a, s);
+    MLG_TRY(nakatsha_post(p, 1.0f, p->x_dagM, nullptr, nullptr, s));
+    cudaEventRecord(t[5].b, s);
+    MLG_CUDA(cudaStreamSynchronize(s));
+    if (it == 0) continue;  // warm-up
+    for (int k = 0; k < 6; ++k) {
+      float v = 0.f;
+      cudaEventElapsedTime(&v, t[k].a, t[k].b);
+      acc[k] += v;
+    }
+  }
+  for (int k = 0; k < 6; ++k) ms[k] = acc[k] / iters;
+  return MLG_OK;
+}

@@ -1,0 +1,465 @@
+// Sparse gridding-matrix products on the device (Gu / Gut / Gn and the
+// generic bmSparseMat_vec family).
+//
+// The reference (bmSparseMat_cC_oBlock_omp_mex.cpp:106-260) streams the whole
+// matrix once per coil and per real/imaginary part.  Here one launch covers
+// every coil: a thread owns one (row, coil) output and walks the row's
+// entries in stored order with explicit round-to-nearest multiply and add
+// (no FMA contraction), so short rows reproduce the reference's
+// floating-point result bit for bit.  Rows longer than kLongRow entries (the
+// k-space centre of Gut, which every radial spoke crosses) get a whole CTA
+// that splits the entries over thread groups and reduces the partial sums in
+// a fixed order.
+//
+// Two thread mappings: coil-fastest (lanes of a warp = coils of one row;
+// used when the output is coil-fastest, e.g. Gu -> k-space) and row-fastest
+// (lanes = consecutive rows of one coil; used when the output is coil-major,
+// e.g. Gut -> grid), so the output side is always coalesced.
+#include <algorithm>
+#include <vector>
+
+#include "mlg_internal.cuh"
+
+namespace mlg {
+
+struct SpmmParams {
+  const uint32_t* row_ptr;
+  const int* col;
+  const float* val;
+  int l_size;
+  int nCh;
+  int rows_per_block;
+  const int* long_rows;
+  int n_long;
+  Operand in;
+  Operand out;
+  const float* in_row_scale;
+  float out_scale;
+  int normalize;
+  const float* sqn_w;
+  double* partial;
+  int partial_long_offset;
+};
+
+template <Layout L>
+__device__ __forceinline__ float2 ld(const Operand& o, long long row, int c, int nCh) {
+  if constexpr (L == Layout::kPointC64) {
+    return __ldg(reinterpret_cast<const float2*>(o.a) + row * nCh + c);
+  } else if constexpr (L == Layout::kCoilC64) {
+    return __ldg(reinterpret_cast<const float2*>(o.a) + (long long)c * o.rows + row);
+  } else if constexpr (L == Layout::kCoilSplit) {
+    const long long i = (long long)c * o.rows + row;
+    return make_float2(__ldg(reinterpret_cast<const float*>(o.a) + i), __ldg(reinterpret_cast<const float*>(o.b) + i));
+  } else if constexpr (L == Layout::kPointSplit) {
+    const long long i = row * nCh + c;
+    return make_float2(__ldg(reinterpret_cast<const float*>(o.a) + i), __ldg(reinterpret_cast<const float*>(o.b) + i));
+  } else {
+    return make_float2(__ldg(reinterpret_cast<const float*>(o.a) + (long long)c * o.rows + row), 0.f);
+  }
+}
+
+template <Layout L>
+__device__ __forceinline__ void st(const Operand& o, long long row, int c, int nCh, float2 v) {
+  if constexpr (L == Layout::kPointC64) {
+    reinterpret_cast<float2*>(o.a)[row * nCh + c] = v;
+  } else if constexpr (L == Layout::kCoilC64) {
+    reinterpret_cast<float2*>(o.a)[(long long)c * o.rows + row] = v;
+  } else if constexpr (L == Layout::kCoilSplit) {
+    const long long i = (long long)c * o.rows + row;
+    reinterpret_cast<float*>(o.a)[i] = v.x;
+    reinterpret_cast<float*>(o.b)[i] = v.y;
+  } else if constexpr (L == Layout::kPointSplit) {
+    const long long i = row * nCh + c;
+    reinterpret_cast<float*>(o.a)[i] = v.x;
+    reinterpret_cast<float*>(o.b)[i] = v.y;
+  } else {
+    reinterpret_cast<float*>(o.a)[(long long)c * o.rows + row] = v.x;
+  }
+}
+
+// Accumulates entries [b, e) with stride `step` of one row for coil c.
+template <Layout IN>
+__device__ __forceinline__ void accumulate(const SpmmParams& p, uint32_t b, uint32_t e, uint32_t step, int c,
+                                           float& ax, float& ay, float& ws) {
+  const bool scale = p.in_row_scale != nullptr;
+#pragma unroll 4
+  for (uint32_t k = b; k < e; k += step) {
+    const int j = __ldg(p.col + k);
+    const float m = __ldg(p.val + k);
+    float2 v = ld<IN>(p.in, j, c, p.nCh);
+    if (scale) {
+      const float h = __ldg(p.in_row_scale + j);
+      v.x = __fmul_rn(h, v.x);
+      v.y = __fmul_rn(h, v.y);
+    }
+    ax = __fadd_rn(ax, __fmul_rn(m, v.x));
+    ay = __fadd_rn(ay, __fmul_rn(m, v.y));
+    ws = __fadd_rn(ws, m);
+  }
+}
+
+template <Layout OUT>
+__device__ __forceinline__ double finish(const SpmmParams& p, long long r, int c, float ax, float ay, float ws) {
+  if (p.normalize) {
+    // bmGridder_n2u_mex.cpp:178-191: divide by the weight sum, 1 if < 1e-5
+    const float s = ws < 1e-5f ? 1.0f : ws;
+    ax = __fdiv_rn(ax, s);
+    ay = __fdiv_rn(ay, s);
+  }
+  if (p.out_scale != 1.0f) {
+    ax = __fmul_rn(ax, p.out_scale);
+    ay = __fmul_rn(ay, p.out_scale);
+  }
+  st<OUT>(p.out, r, c, p.nCh, make_float2(ax, ay));
+  if (p.partial) {
+    const double w = p.sqn_w ? (double)__ldg(p.sqn_w + r) : 1.0;
+    return w * ((double)ax * ax + (double)ay * ay);
+  }
+  return 0.0;
+}
+
+__device__ __forceinline__ double block_sum(double v, double* sh) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) sh[wid] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += sh[i];
+  }
+  return t;
+}
+
+template <Layout IN, Layout OUT, bool ROW_FAST>
+__global__ void __launch_bounds__(256) spmm_short_kernel(SpmmParams p) {
+  __shared__ double sh[32];
+  const long long r0 = (long long)blockIdx.x * p.rows_per_block;
+  const int nrows = (int)min((long long)p.rows_per_block, (long long)p.l_size - r0);
+  const int items = nrows * p.nCh;
+  double sq = 0.0;
+  for (int it = threadIdx.x; it < items; it += blockDim.x) {
+    int lr, c;
+    if (ROW_FAST) {
+      lr = it % nrows;
+      c = it / nrows;
+    } else {
+      c = it % p.nCh;
+      lr = it / p.nCh;
+    }
+    const long long r = r0 + lr;
+    const uint32_t b = __ldg(p.row_ptr + r), e = __ldg(p.row_ptr + r + 1);
+    if (e - b > (uint32_t)kLongRow) continue;  // owned by spmm_long_kernel
+    float ax = 0.f, ay = 0.f, ws = 0.f;
+    accumulate<IN>(p, b, e, 1u, c, ax, ay, ws);
+    sq += finish<OUT>(p, r, c, ax, ay, ws);
+  }
+  if (p.partial) {
+    const double t = block_sum(sq, sh);
+    if (threadIdx.x == 0) p.partial[blockIdx.x] = t;
+  }
+}
+
+template <Layout IN, Layout OUT>
+__global__ void __launch_bounds__(256) spmm_long_kernel(SpmmParams p) {
+  __shared__ float3 part[256];
+  __shared__ double sh[32];
+  const long long r = __ldg(p.long_rows + blockIdx.x);
+  const uint32_t b = __ldg(p.row_ptr + r), e = __ldg(p.row_ptr + r + 1);
+  const int cper = min(p.nCh, (int)blockDim.x);   // coils per pass
+  const int groups = (int)blockDim.x / cper;      // entry groups per coil
+  double sq = 0.0;
+  for (int c0 = 0; c0 < p.nCh; c0 += cper) {
+    const int cl = threadIdx.x % cper, g = threadIdx.x / cper;
+    const int c = c0 + cl;
+    float ax = 0.f, ay = 0.f, ws = 0.f;
+    if (g < groups && c < p.nCh) accumulate<IN>(p, b + g, e, (uint32_t)groups, c, ax, ay, ws);
+    __syncthreads();
+    part[threadIdx.x] = make_float3(ax, ay, ws);
+    __syncthreads();
+    if ((int)threadIdx.x < cper && c0 + (int)threadIdx.x < p.nCh) {
+      float sx = 0.f, sy = 0.f, sw = 0.f;
+      for (int gg = 0; gg < groups; ++gg) {  // fixed order: deterministic
+        const float3 q = part[gg * cper + threadIdx.x];
+        sx = __fadd_rn(sx, q.x);
+        sy = __fadd_rn(sy, q.y);
+        sw = __fadd_rn(sw, q.z);
+      }
+      sq += finish<OUT>(p, r, c0 + threadIdx.x, sx, sy, sw);
+    }
+  }
+  if (p.partial) {
+    const double t = block_sum(sq, sh);
+    if (threadIdx.x == 0) p.partial[p.partial_long_offset + blockIdx.x] = t;
+  }
+}
+
+static int rows_per_block(const SpmmArgs& a) { return std::max(1, 1024 / std::max(1, a.nCh)); }
+
+int spmm_partial_count(const SpmmArgs& a) {
+  const int rpb = rows_per_block(a);
+  return (int)((a.m->l_size + (long long)rpb - 1) / rpb) + a.m->n_long;
+}
+
+template <Layout IN, Layout OUT, bool ROW_FAST>
+static int launch(const SpmmParams& p, int grid_short, cudaStream_t s) {
+  if (grid_short > 0) {
+    spmm_short_kernel<IN, OUT, ROW_FAST><<<grid_short, 256, 0, s>>>(p);
+    MLG_LAUNCHED();
+  }
+  if (p.n_long > 0) {
+    spmm_long_kernel<IN, OUT><<<p.n_long, 256, 0, s>>>(p);
+    MLG_LAUNCHED();
+  }
+  return MLG_OK;
+}
+
+int spmm(const SpmmArgs& a, cudaStream_t s) {
+  const Csr& m = *a.m;
+  MLG_CHECK(a.nCh >= 1, "nCh must be >= 1");
+  SpmmParams p;
+  p.row_ptr = m.row_ptr;
+  p.col = m.col;
+  p.val = m.val;
+  p.l_size = m.l_size;
+  p.nCh = a.nCh;
+  p.rows_per_block = rows_per_block(a);
+  p.long_rows = m.long_rows;
+  p.n_long = m.n_long;
+  p.in = a.in;
+  p.out = a.out;
+  p.in_row_scale = a.in_row_scale;
+  p.out_scale = a.out_scale;
+  p.normalize = a.normalize ? 1 : 0;
+  p.sqn_w = a.sqn_row_weight;
+  p.partial = a.partial;
+  const int grid_short = (int)((m.l_size + (long long)p.rows_per_block - 1) / p.rows_per_block);
+  p.partial_long_offset = grid_short;
+  using L = Layout;
+  const L i = a.in.layout, o = a.out.layout;
+  if (i == L::kCoilC64 && o == L::kPointC64) return launch<L::kCoilC64, L::kPointC64, false>(p, grid_short, s);
+  if (i == L::kPointC64 && o == L::kCoilC64) return launch<L::kPointC64, L::kCoilC64, true>(p, grid_short, s);
+  if (i == L::kPointC64 && o == L::kPointC64) return launch<L::kPointC64, L::kPointC64, false>(p, grid_short, s);
+  if (i == L::kCoilSplit && o == L::kCoilSplit) return launch<L::kCoilSplit, L::kCoilSplit, true>(p, grid_short, s);
+  if (i == L::kPointSplit && o == L::kPointSplit) return launch<L::kPointSplit, L::kPointSplit, false>(p, grid_short, s);
+  if (i == L::kCoilReal && o == L::kCoilReal) return launch<L::kCoilReal, L::kCoilReal, true>(p, grid_short, s);
+  return fail(MLG_ERR_UNSUPPORTED, "spmm: layout pair (%d,%d) not instantiated", (int)i, (int)o);
+}
+
+// ---- sign-folded copies (fftshift as a (-1)^(x+y+z) modulation) ------------
+__device__ __forceinline__ float cell_sign(long long i, int imDim, int Nx, int Ny) {
+  long long x = i % Nx;
+  long long s = x;
+  if (imDim > 1) {
+    const long long q = i / Nx;
+    s += q % Ny;
+    if (imDim > 2) s += q / Ny;
+  }
+  return (s & 1) ? -1.0f : 1.0f;
+}
+
+__global__ void sign_by_col_kernel(const int* __restrict__ col, const float* __restrict__ val, float* out,
+                                   long long nnz, int imDim, int Nx, int Ny, float gs) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nnz; k += (long long)gridDim.x * blockDim.x)
+    out[k] = val[k] * (gs * cell_sign(col[k], imDim, Nx, Ny));
+}
+
+__global__ void sign_by_row_kernel(const uint32_t* __restrict__ row_ptr, const float* __restrict__ val, float* out,
+                                   int l_size, int imDim, int Nx, int Ny, float gs) {
+  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < l_size; r += (long long)gridDim.x * blockDim.x) {
+    const float sg = gs * cell_sign(r, imDim, Nx, Ny);
+    for (uint32_t k = row_ptr[r]; k < row_ptr[r + 1]; ++k) out[k] = val[k] * sg;
+  }
+}
+
+void csr_free_sign_copy(Csr& c) {
+  cudaFree(c.val);
+  c = Csr();
+}
+
+int csr_sign_copy(const Csr& src, bool by_row, int imDim, const int* N, float global_sign, Csr& dst,
+                  cudaStream_t s) {
+  dst = src;  // shares row_ptr / col / long_rows with src (not owned)
+  dst.val = nullptr;
+  MLG_CUDA(cudaMalloc(&dst.val, sizeof(float) * (size_t)std::max<long long>(1, src.nnz)));
+  const int Nx = N[0], Ny = imDim > 1 ? N[1] : 1;
+  if (by_row) {
+    sign_by_row_kernel<<<std::max(1, std::min(65535, (src.l_size + 255) / 256)), 256, 0, s>>>(
+        src.row_ptr, src.val, dst.val, src.l_size, imDim, Nx, Ny, global_sign);
+  } else {
+    sign_by_col_kernel<<<(int)std::max<long long>(1, std::min<long long>(65535, (src.nnz + 255) / 256)), 256, 0, s>>>(
+        src.col, src.val, dst.val, src.nnz, imDim, Nx, Ny, global_sign);
+  }
+  MLG_LAUNCHED();
+  return MLG_OK;
+}
+
+// ---- host-buffer SpMV entry points ------------------------------------------
+namespace {
+
+struct HostCall {
+  cudaStream_t s = nullptr;
+  Csr m;
+  ~HostCall() { csr_free(m); }
+};
+
+int vec_call(int r_size, const int* r_jump, const int* r_nJump, const float* m_val, int l_size,
+             const int* l_jump, int l_nJump, const float* vR, const float* vI, int nVec, float* wR,
+             float* wI, Layout layout) {
+  MLG_TRY(ensure_device());
+  MLG_CHECK(nVec >= 1, "n_vec must be >= 1");
+  MLG_CHECK(vR && wR && (layout == Layout::kCoilReal || (vI && wI)), "NULL vector buffer");
+  HostCall hc;
+  MLG_TRY(csr_from_jump(r_size, r_jump, r_nJump, m_val, l_size, l_jump, l_nJump, hc.m, hc.s));
+  const bool cplx = layout != Layout::kCoilReal;
+  const size_t nin = (size_t)r_size * nVec, nout = (size_t)l_size * nVec;
+  DevBuf<float> din, dout;
+  MLG_TRY(din.alloc(nin * (cplx ? 2 : 1), hc.s));
+  MLG_TRY(dout.alloc(nout * (cplx ? 2 : 1), hc.s));
+  MLG_CUDA(cudaMemcpyAsync(din.p, vR, nin * sizeof(float), cudaMemcpyHostToDevice, hc.s));
+  if (cplx) MLG_CUDA(cudaMemcpyAsync(din.p + nin, vI, nin * sizeof(float), cudaMemcpyHostToDevice, hc.s));
+  SpmmArgs a;
+  a.m = &hc.m;
+  a.nCh = nVec;
+  a.in.layout = a.out.layout = layout;
+  a.in.a = din.p;
+  a.in.b = cplx ? din.p + nin : nullptr;
+  a.in.rows = r_size;
+  a.out.a = dout.p;
+  a.out.b = cplx ? dout.p + nout : nullptr;
+  a.out.rows = l_size;
+  MLG_TRY(spmm(a, hc.s));
+  MLG_CUDA(cudaMemcpyAsync(wR, dout.p, nout * sizeof(float), cudaMemcpyDeviceToHost, hc.s));
+  if (cplx) MLG_CUDA(cudaMemcpyAsync(wI, dout.p + nout, nout * sizeof(float), cudaMemcpyDeviceToHost, hc.s));
+  MLG_CUDA(cudaStreamSynchronize(hc.s));
+  return MLG_OK;
+}
+
+}  // namespace
+}  // namespace mlg
+
+using namespace mlg;
+
+extern "C" {
+
+int mlg_sparsemat_vec_cC(int r_size, const int* r_jump, const int* r_nJump, const float* m_val, int l_size,
+                         const int* l_jump, int l_nJump, const float* vReal, const float* vImag, int nVec,
+                         float* wReal, float* wImag) {
+  return vec_call(r_size, r_jump, r_nJump, m_val, l_size, l_jump, l_nJump, vReal, vImag, nVec, wReal, wImag,
+                  Layout::kCoilSplit);
+}
+
+int mlg_sparsemat_vec_cR(int r_size, const int* r_jump, const int* r_nJump, const float* m_val, int l_size,
+                         const int* l_jump, int l_nJump, const float* vReal, const float* vImag, int nVec,
+                         float* wReal, float* wImag) {
+  return vec_call(r_size, r_jump, r_nJump, m_val, l_size, l_jump, l_nJump, vReal, vImag, nVec, wReal, wImag,
+                  Layout::kPointSplit);
+}
+
+int mlg_sparsemat_vec_rC(int r_size, const int* r_jump, const int* r_nJump, const float* m_val, int l_size,
+                         const int* l_jump, int l_nJump, const float* v, int nVec, float* w) {
+  return vec_call(r_size, r_jump, r_nJump, m_val, l_size, l_jump, l_nJump, v, nullptr, nVec, w, nullptr,
+                  Layout::kCoilReal);
+}
+
+int mlg_sparsemat_r_nJump2index(int l_size, const int* r_nJump, long long out_length, int* out) {
+  // bmSparseMat_r_nJump2index_mex.cpp:70-80.  A setup-time helper of the
+  // matrix builder: runs on the host (there is no device work to amortise).
+  MLG_CHECK(l_size >= 0 && (l_size == 0 || r_nJump), "r_nJump missing");
+  MLG_CHECK(out || out_length == 0, "NULL output");
+  long long n = 0;
+  for (int i = 0; i < l_size; ++i) {
+    MLG_CHECK(r_nJump[i] >= 0, "negative r_nJump");
+    MLG_CHECK(n + r_nJump[i] <= out_length, "out_length %lld smaller than sum(r_nJump)", out_length);
+    for (int j = 0; j < r_nJump[i]; ++j) out[n++] = i;
+  }
+  MLG_CHECK(n == out_length, "out_length %lld differs from sum(r_nJump)=%lld", out_length, n);
+  return MLG_OK;
+}
+
+int mlg_matrix_create(int r_size, const int* r_jump, const int* r_nJump, const float* m_val, int l_size,
+                      const int* l_jump, int l_nJump, mlg_matrix_t* out) {
+  MLG_CHECK(out, "NULL output handle");
+  *out = nullptr;
+  MLG_TRY(ensure_device());
+  mlg_matrix_s* h = new mlg_matrix_s();
+  cudaGetDevice(&h->device);
+  int st = csr_from_jump(r_size, r_jump, r_nJump, m_val, l_size, l_jump, l_nJump, h->csr, nullptr);
+  if (st != MLG_OK) {
+    delete h;
+    return st;
+  }
+  *out = h;
+  return MLG_OK;
+}
+
+int mlg_matrix_destroy(mlg_matrix_t m) {
+  if (!m) return MLG_OK;
+  cudaSetDevice(m->device);
+  csr_free(m->csr);
+  delete m;
+  return MLG_OK;
+}
+
+int mlg_matrix_info(mlg_matrix_t m, long long* nnz, int* r_size, int* l_size) {
+  MLG_CHECK(m, "NULL matrix");
+  if (nnz) *nnz = m->csr.nnz;
+  if (r_size) *r_size = m->csr.r_size;
+  if (l_size) *l_size = m->csr.l_size;
+  return MLG_OK;
+}
+
+int mlg_matrix_row_stats(mlg_matrix_t m, int* nonempty_rows, int* long_rows) {
+  MLG_CHECK(m, "NULL matrix");
+  if (nonempty_rows) *nonempty_rows = m->csr.n_nonempty;
+  if (long_rows) *long_rows = m->csr.n_long;
+  return MLG_OK;
+}
+
+int mlg_matrix_download(mlg_matrix_t m, int* r_jump, int* r_nJump, float* m_val, int* l_jump, int* l_nJump_out) {
+  MLG_CHECK(m && r_jump && r_nJump && m_val, "NULL argument");
+  const Csr& c = m->csr;
+  MLG_CUDA(cudaSetDevice(m->device));
+  std::vector<uint32_t> rp((size_t)c.l_size + 1);
+  std::vector<int> col((size_t)c.nnz);
+  MLG_CUDA(cudaMemcpy(rp.data(), c.row_ptr, sizeof(uint32_t) * rp.size(), cudaMemcpyDeviceToHost));
+  if (c.nnz) {
+    MLG_CUDA(cudaMemcpy(col.data(), c.col, sizeof(int) * (size_t)c.nnz, cudaMemcpyDeviceToHost));
+    MLG_CUDA(cudaMemcpy(m_val, c.val, sizeof(float) * (size_t)c.nnz, cudaMemcpyDeviceToHost));
+  }
+  long long prevc = 0;
+  for (long long e = 0; e < c.nnz; ++e) {
+    r_jump[e] = (int)(col[(size_t)e] - prevc);
+    prevc = col[(size_t)e];
+  }
+  // l_jump != NULL: squeezed form (non-empty rows only, bmSparseMat.m:62-94)
+  int n = 0;
+  long long prevr = 0;
+  for (int r = 0; r < c.l_size; ++r) {
+    const int len = (int)(rp[(size_t)r + 1] - rp[r]);
+    if (l_jump) {
+      if (len == 0) continue;
+      l_jump[n] = (int)(r - prevr);
+      prevr = r;
+    }
+    r_nJump[n++] = len;
+  }
+  if (l_nJump_out) *l_nJump_out = n;
+  return MLG_OK;
+}
+
+int mlg_matrix_spmm_dev(mlg_matrix_t m, const void* v, int nVec, void* w, void* stream) {
+  MLG_CHECK(m && v && w && nVec >= 1, "invalid argument");
+  MLG_CUDA(cudaSetDevice(m->device));
+  SpmmArgs a;
+  a.m = &m->csr;
+  a.nCh = nVec;
+  a.in.layout = a.out.layout = Layout::kPointC64;
+  a.in.a = const_cast<void*>(v);
+  a.in.rows = m->csr.r_size;
+  a.out.a = w;
+  a.out.rows = m->csr.l_size;
+  return spmm(a, (cudaStream_t)stream);
+}
+
+}  // extern "C"

@@ -1,0 +1,242 @@
+"""Non-Cartesian Fourier operators.
+
+bmK / bmKF / bmKF_conj: src/fourier123/prep_function/bmK.m, bmKF.m, bmKF_conj.m
+bmShanna:   src/fourier123/map_function/nonCartesian/bmShanna.m (forward)
+bmNakatsha: src/fourier123/map_function/nonCartesian/bmNakatsha.m (adjoint)
+bmIDF:      src/fourier3/bmIDF3.m (and 1/2-D)
+bmMathilda: src/fourier123/map_function/nonCartesian/bmMathilda.m
+
+Array conventions follow the reference: images are column vectors
+[prod(n_u), nCol] in MATLAB (x fastest) order, k-space data [nPt, nCh].
+NufftPlan is the device-resident form used by the solvers and the serving
+loop; the bmShanna / bmNakatsha functions take host arrays like the MATLAB
+functions and run through the stateless CUDA entry points.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _native as N
+from .gridding import bmGridder_n2u, bmGridder_n2u_leight
+from .sparsemat import DeviceMatrix, bmSparseMat, kernel_code, kernel_defaults
+
+
+def _ints(v):
+    return np.ascontiguousarray(np.ravel(v), np.int32)
+
+
+def bmK(N_u, dK_u, nCh, kernelType=None, nWin=None, kernelParam=None):
+    """Deapodisation [prod(N_u), nCh] float32 (bmK.m:6-156)."""
+    kernelType, nWin, kp = kernel_defaults(kernelType, nWin, kernelParam)
+    Nu = _ints(N_u)
+    dK = np.ascontiguousarray(np.ravel(dK_u), np.float64)
+    kp3 = np.zeros(3)
+    kp3[:kp.size] = kp
+    K = np.zeros(int(np.prod(Nu)), np.float32)
+    N.call("mlg_deapodization", Nu.size, N.iptr(Nu), N.dptr(dK), kernel_code(kernelType), nWin, N.dptr(kp3),
+           N.fptr(K))
+    return np.repeat(K[:, None], int(nCh), axis=1)
+
+
+def crop_index(N_u, n_u):
+    """bmImCrope.m: the n_u block occupies N/2-n/2 .. N/2+n/2-1 of N_u."""
+    return tuple(slice(int(a) // 2 - int(b) // 2, int(a) // 2 + int(b) // 2) for a, b in zip(N_u, n_u))
+
+
+def _crop_col(x, N_u, n_u):
+    nc = x.shape[1]
+    blk = x.reshape(tuple(int(v) for v in N_u) + (nc,), order="F")
+    return blk[crop_index(N_u, n_u)].reshape(-1, nc, order="F")
+
+
+def bmKF(C, N_u, n_u, dK_u, nCh, kernelType=None, nWin=None, kernelParam=None):
+    """K * (1/prod(N_u)/prod(dK_u)) * C cropped to n_u (bmKF.m:6-36)."""
+    N_u = np.ravel(N_u).astype(np.float32)
+    n_u = np.ravel(n_u).astype(np.float32)
+    dK_u = np.ravel(dK_u).astype(np.float32)
+    K = _crop_col(bmK(N_u, dK_u, nCh, kernelType, nWin, kernelParam), N_u, n_u)
+    F = np.float32(1 / np.prod(N_u) / np.prod(dK_u))
+    if C is None:
+        return (K * F).astype(np.float32)
+    C = np.asarray(C, np.complex64).reshape(K.shape[0], -1, order="F")
+    return (K * F * C).astype(np.complex64)
+
+
+def bmKF_conj(C_conj, N_u, n_u, dK_u, nCh, kernelType=None, nWin=None, kernelParam=None):
+    """K * (1/prod(dK_u)) * conj(C) cropped to n_u (bmKF_conj.m:6-39); the
+    caller passes conj(C), as in the reference."""
+    N_u = np.ravel(N_u).astype(np.float32)
+    n_u = np.ravel(n_u).astype(np.float32)
+    dK_u = np.ravel(dK_u).astype(np.float32)
+    K = _crop_col(bmK(N_u, dK_u, nCh, kernelType, nWin, kernelParam), N_u, n_u)
+    F = np.float32(1 / np.prod(dK_u))
+    if C_conj is None:
+        return (K * F).astype(np.float32)
+    C_conj = np.asarray(C_conj, np.complex64).reshape(K.shape[0], -1, order="F")
+    return (K * F * C_conj).astype(np.complex64)
+
+
+def _split(a, shape2):
+    a = np.asarray(a, np.complex64).reshape(shape2, order="F")
+    return np.ascontiguousarray(a.real.T), np.ascontiguousarray(a.imag.T)  # column-major
+
+
+class NufftPlan:
+    """Device-resident Shanna / Nakatsha operator pair (mlg_plan_t).
+
+    Gu, Gut: DeviceMatrix (or bmSparseMat, uploaded); KFC / KFC_conj:
+    [prod(n_u), nCh] complex.  Device tensors are complex64 CUDA tensors:
+    images [prod(n_u)], k-space [nPt, nCh] (point layout)."""
+
+    def __init__(self, N_u, n_u, nCh, Gu, Gut, KFC, KFC_conj, dK_u=None):
+        self.N_u = _ints(N_u)
+        self.n_u = _ints(n_u if n_u is not None else N_u)
+        self.imDim = self.N_u.size
+        self.nCh = int(nCh)
+        self._keep = []
+        if isinstance(Gu, bmSparseMat):
+            Gu = Gu.to_device()
+        if isinstance(Gut, bmSparseMat):
+            Gut = Gut.to_device()
+        self._keep = [Gu, Gut]
+        self.nPt = Gu.l_size if Gu is not None else Gut.r_size
+        nu = int(np.prod(self.n_u))
+        kr, ki = _split(KFC, (nu, self.nCh)) if KFC is not None else (None, None)
+        cr, ci = _split(KFC_conj, (nu, self.nCh)) if KFC_conj is not None else (None, None)
+        h = ctypes.c_void_p()
+        N.call("mlg_plan_create", self.imDim, N.iptr(self.N_u), N.iptr(self.n_u), self.nCh,
+               Gu.handle if Gu is not None else None, Gut.handle if Gut is not None else None,
+               N.fptr(kr), N.fptr(ki), N.fptr(cr), N.fptr(ci), ctypes.byref(h))
+        self._h = h
+        if dK_u is not None:
+            N.call("mlg_plan_set_dk", self._h, N.dptr(np.ascontiguousarray(np.ravel(dK_u), np.float64)))
+
+    @property
+    def handle(self):
+        return self._h
+
+    def device_bytes(self) -> int:
+        b = ctypes.c_longlong()
+        N.call("mlg_plan_device_bytes", self._h, ctypes.byref(b))
+        return b.value
+
+    def shanna(self, x, out=None, per_coil=False):
+        import torch
+
+        if out is None:
+            out = torch.empty((self.nPt, self.nCh), dtype=torch.complex64, device=x.device)
+        N.call("mlg_shanna_dev", self._h, N.tptr(x), int(per_coil), N.tptr(out), N.stream_ptr())
+        return out
+
+    def nakatsha(self, y, HY=None, scale=1.0, out=None):
+        import torch
+
+        if out is None:
+            out = torch.empty(int(np.prod(self.n_u)), dtype=torch.complex64, device=y.device)
+        N.call("mlg_nakatsha_dev", self._h, N.tptr(y), N.tfptr(HY), float(scale), N.tptr(out), N.stream_ptr())
+        return out
+
+    def close(self):
+        if getattr(self, "_h", None):
+            N.lib().mlg_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def bmShanna(x, G: bmSparseMat, KFC, n_u=None):
+    """y = Gu * FFT(ZF(x .* KFC)) with host arrays (bmShanna.m /
+    bmShanna_MATLAB.m).  x [prod(n_u)] or [prod(n_u), nCh] -> y [nPt, nCh]."""
+    N_u = _ints(G.N_u)
+    n_u = _ints(n_u if n_u is not None else G.N_u)
+    KFC = np.asarray(KFC)
+    nu = int(np.prod(n_u))
+    nCh = KFC.reshape(nu, -1, order="F").shape[1]
+    x = np.asarray(x, np.complex64).reshape(nu, -1, order="F")
+    kr, ki = _split(KFC, (nu, nCh))
+    xr, xi = _split(x, x.shape)
+    r_size, r_jump, r_nJump, m_val, l_size, l_jump, l_nJump = G.jump_arrays()
+    yR = np.zeros((nCh, l_size), np.float32)
+    yI = np.zeros((nCh, l_size), np.float32)
+    N.call("mlg_shanna", N_u.size, N.iptr(N_u), N.iptr(n_u), nCh, N.fptr(xr), N.fptr(xi), x.shape[1], N.fptr(kr),
+           N.fptr(ki), r_size, N.iptr(r_jump), N.iptr(r_nJump), N.fptr(m_val), l_size, N.iptr(l_jump), l_nJump,
+           N.fptr(yR), N.fptr(yI))
+    return (yR + 1j * yI).T.astype(np.complex64)
+
+
+def bmNakatsha(y, Gut: bmSparseMat, KFC_conj, C_flag=True, n_u=None):
+    """x = sum_c KFC_conj .* Crop(IFFT(Gut * y)) with host arrays
+    (bmNakatsha.m).  As in the reference's GPU branch, C_flag must be true."""
+    if not C_flag:
+        raise ValueError(" 'C_flag' must be 'true' for the CUFFT version of bmNakatsha. ")
+    N_u = _ints(Gut.N_u)
+    n_u = _ints(n_u if n_u is not None else Gut.N_u)
+    y = np.asarray(y, np.complex64)
+    if y.ndim == 1:
+        y = y[:, None]
+    nPt, nCh = y.shape
+    nu = int(np.prod(n_u))
+    cr, ci = _split(KFC_conj, (nu, nCh))
+    yr, yi = _split(y, y.shape)
+    r_size, r_jump, r_nJump, m_val, l_size, l_jump, l_nJump = Gut.jump_arrays()
+    xR = np.zeros(nu, np.float32)
+    xI = np.zeros(nu, np.float32)
+    N.call("mlg_nakatsha", N_u.size, N.iptr(N_u), N.iptr(n_u), nCh, N.fptr(yr), N.fptr(yi), N.fptr(cr), N.fptr(ci),
+           r_size, N.iptr(r_jump), N.iptr(r_nJump), N.fptr(m_val), l_size, N.iptr(l_jump), l_nJump, N.fptr(xR),
+           N.fptr(xI))
+    return (xR + 1j * xI).astype(np.complex64)[:, None]
+
+
+def bmIDF(x, N_u, dK_u):
+    """fftshift(ifft(ifftshift(x))) * prod(N_u)*prod(dK_u) over the first
+    len(N_u) dimensions of x (block [N_u..., nCol], MATLAB order)."""
+    N_u = _ints(N_u)
+    x = np.asarray(x, np.complex64)
+    nu = int(np.prod(N_u))
+    shape = x.shape
+    xc = x.reshape(nu, -1, order="F")
+    nCol = xc.shape[1]
+    xr = np.ascontiguousarray(xc.real.T)
+    xi = np.ascontiguousarray(xc.imag.T)
+    yR = np.zeros((nCol, nu), np.float32)
+    yI = np.zeros((nCol, nu), np.float32)
+    N.call("mlg_idf", N_u.size, N.iptr(N_u), N.fptr(np.ascontiguousarray(np.ravel(dK_u), np.float32)), nCol,
+           N.fptr(xr), N.fptr(xi), N.fptr(yR), N.fptr(yI))
+    return (yR + 1j * yI).T.reshape(shape, order="F").astype(np.complex64)
+
+
+def bmCoilSense_pinv(C, x0):
+    """src/coilSense/map/bmCoilSense_pinv.m:10."""
+    C = np.asarray(C, np.complex64)
+    return (np.sum(np.conj(C) * x0, axis=1) / np.sum(np.abs(C) ** 2, axis=1)).astype(np.complex64)
+
+
+def bmMathilda(y, t, v, C, N_u, n_u, dK_u, kernelType=None, nWin=None, kernelParam=None, leight_flag=True):
+    """Gridded reconstruction (bmMathilda.m:14-125, CUFFT branch): adjoint
+    gridding -> bmIDF -> deapodisation -> crop -> coil pinv.
+    y [nPt, nCh] -> x [prod(n_u)] (or [prod(n_u), nCh] without C)."""
+    kernelType, nWin, kp = kernel_defaults(kernelType, nWin, kernelParam)
+    y = np.asarray(y, np.complex64)
+    if y.ndim == 1:
+        y = y[:, None]
+    if y.shape[0] < y.shape[1]:
+        y = y.T  # bmMathilda.m:35-37 expects more points than coils
+    N_u = _ints(N_u)
+    n_u = _ints(n_u)
+    dK_u = np.ravel(dK_u).astype(np.float32).astype(np.float64)
+    nCh = y.shape[1]
+    grid = bmGridder_n2u_leight if leight_flag else bmGridder_n2u
+    xg = grid(y.T, t, v, N_u, dK_u, kernelType, nWin, kp)  # [nCh, prod(N_u)]
+    x = xg.T.reshape(tuple(N_u) + (nCh,), order="F")
+    x = bmIDF(x, N_u, dK_u)
+    K = bmK(N_u, dK_u, nCh, kernelType, nWin, kp).reshape(tuple(N_u) + (nCh,), order="F")
+    x = (x * K).astype(np.complex64)[crop_index(N_u, n_u)].reshape(-1, nCh, order="F")
+    if C is not None:
+        return bmCoilSense_pinv(np.asarray(C).reshape(x.shape[0], -1, order="F"), x)
+    return x

@@ -1,0 +1,201 @@
+"""Sparse gridding matrices: the reference's ``bmSparseMat`` data class,
+device-resident matrices, ``bmTraj2SparseMat`` on the GPU and
+``bmSparseMat_vec``.
+
+Reference: src/sparseMat/m/bmSparseMat.m (format, lines 15-47 and
+cpp_prepare 100-188), src/gridding123/m/bmTraj2SparseMat.m (builder),
+src/sparseMat/m/bmSparseMat_vec.m (product dispatch).
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _native as N
+
+
+def kernel_defaults(kernelType=None, nWin=None, kernelParam=None):
+    """src/varargin/bmVarargin_kernelType_nWin_kernelParam.m:15-40."""
+    if not kernelType:
+        kernelType = "gauss"
+    if kernelType not in ("gauss", "kaiser"):
+        raise ValueError(f"unknown kernel type {kernelType!r}")
+    if nWin is None:
+        nWin = 3
+    if kernelParam is None:
+        kernelParam = [0.61, 10] if kernelType == "gauss" else [1.95, 10, 10]
+    kp = np.asarray(np.ravel(kernelParam), np.float32).astype(np.float64)
+    if kernelType == "gauss" and kp.size == 3:
+        raise ValueError("Wrong list of gridding kernel parameters. ")
+    if kernelType == "kaiser" and kp.size == 2:
+        raise ValueError("Wrong list of gridding kernel parameters. ")
+    return kernelType, int(np.float32(nWin)), kp
+
+
+def kernel_code(kernelType: str) -> int:
+    return N.MLG_KERNEL_GAUSS if kernelType == "gauss" else N.MLG_KERNEL_KAISER
+
+
+@dataclass
+class bmSparseMat:
+    """A cpp_prepared 'one_block' jump-coded CSR (bmSparseMat.m:15-47):
+    ``r_jump`` holds column deltas (first entry absolute, 0-based),
+    ``r_nJump`` entries per stored row, ``l_jump`` row deltas of the stored
+    rows when rows are squeezed (empty otherwise)."""
+
+    r_size: int
+    r_jump: np.ndarray
+    r_nJump: np.ndarray
+    m_val: np.ndarray
+    l_size: int
+    l_jump: np.ndarray
+    l_nJump: int
+    N_u: np.ndarray | None = None
+    d_u: np.ndarray | None = None
+    kernel_type: str = "void"
+    nWin: int = 0
+    kernelParam: np.ndarray | None = None
+    block_type: str = "one_block"
+    type: str = "cpp_prepared"
+    extra: dict = field(default_factory=dict)
+
+    @property
+    def l_squeeze_flag(self) -> bool:
+        return self.l_jump is not None and self.l_jump.size > 0
+
+    def jump_arrays(self):
+        c = lambda a, t: np.ascontiguousarray(np.ravel(a), t)
+        lj = c(self.l_jump, np.int32) if self.l_squeeze_flag else None
+        return (int(self.r_size), c(self.r_jump, np.int32), c(self.r_nJump, np.int32), c(self.m_val, np.float32),
+                int(self.l_size), lj, int(self.l_nJump))
+
+    def to_device(self) -> "DeviceMatrix":
+        return DeviceMatrix.from_bm(self)
+
+
+class DeviceMatrix:
+    """A bmSparseMat resident in device memory (mlg_matrix_t)."""
+
+    def __init__(self, handle, meta: dict, squeezed: bool):
+        self._h = handle
+        self.meta = meta
+        self.squeezed = squeezed
+        nnz, r, l = ctypes.c_longlong(), ctypes.c_int(), ctypes.c_int()
+        N.call("mlg_matrix_info", self._h, ctypes.byref(nnz), ctypes.byref(r), ctypes.byref(l))
+        self.nnz, self.r_size, self.l_size = nnz.value, r.value, l.value
+
+    @property
+    def handle(self):
+        return self._h
+
+    def row_stats(self):
+        """(non-empty rows, rows longer than 256 entries)."""
+        a, b = ctypes.c_int(), ctypes.c_int()
+        N.call("mlg_matrix_row_stats", self._h, ctypes.byref(a), ctypes.byref(b))
+        return a.value, b.value
+
+    @classmethod
+    def from_bm(cls, G: bmSparseMat) -> "DeviceMatrix":
+        r_size, r_jump, r_nJump, m_val, l_size, l_jump, l_nJump = G.jump_arrays()
+        h = ctypes.c_void_p()
+        N.call("mlg_matrix_create", r_size, N.iptr(r_jump), N.iptr(r_nJump), N.fptr(m_val), l_size,
+               N.iptr(l_jump), l_nJump, ctypes.byref(h))
+        meta = dict(N_u=G.N_u, d_u=G.d_u, kernel_type=G.kernel_type, nWin=G.nWin, kernelParam=G.kernelParam)
+        return cls(h, meta, G.l_squeeze_flag)
+
+    def download(self) -> bmSparseMat:
+        r_jump = np.zeros(self.nnz, np.int32)
+        r_nJump = np.zeros(self.l_size, np.int32)
+        m_val = np.zeros(self.nnz, np.float32)
+        l_jump = np.zeros(self.l_size, np.int32) if self.squeezed else None
+        n = ctypes.c_int()
+        N.call("mlg_matrix_download", self._h, N.iptr(r_jump), N.iptr(r_nJump), N.fptr(m_val),
+               N.iptr(l_jump) if l_jump is not None else None, ctypes.byref(n))
+        if self.squeezed:
+            r_nJump, l_jump = r_nJump[:n.value].copy(), l_jump[:n.value].copy()
+        return bmSparseMat(r_size=self.r_size, r_jump=r_jump, r_nJump=r_nJump, m_val=m_val, l_size=self.l_size,
+                           l_jump=l_jump if l_jump is not None else np.zeros(0, np.int32),
+                           l_nJump=n.value if self.squeezed else self.l_size,
+                           type="l_squeezed_cpp_prepared" if self.squeezed else "cpp_prepared", **self.meta)
+
+    def spmm(self, v, out=None):
+        """w = M v for complex64 CUDA tensors in point layout [rows, nVec]."""
+        import torch
+
+        nVec = v.shape[1] if v.dim() == 2 else 1
+        assert v.dtype == torch.complex64 and v.shape[0] == self.r_size
+        if out is None:
+            out = torch.empty((self.l_size, nVec), dtype=torch.complex64, device=v.device)
+        N.call("mlg_matrix_spmm_dev", self._h, N.tptr(v.contiguous()), nVec, N.tptr(out), N.stream_ptr())
+        return out
+
+    def close(self):
+        if self._h:
+            N.lib().mlg_matrix_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def bmTraj2SparseMat(t, v, N_u, dK_u, kernelType=None, nWin=None, kernelParam=None):
+    """GPU form of src/gridding123/m/bmTraj2SparseMat.m (two outputs): returns
+    device-resident (Gu, Gut).  t [imDim, nPt] physical units, v volume
+    elements (they cancel in the row-normalised Gu/Gut)."""
+    kernelType, nWin, kp = kernel_defaults(kernelType, nWin, kernelParam)
+    t = np.asarray(t, np.float64)
+    if t.ndim == 1:
+        t = t[None, :]
+    imDim, nPt = t.shape
+    tt = np.ascontiguousarray(t.T)  # column-major [imDim, nPt]
+    Nu = np.ascontiguousarray(np.ravel(N_u), np.int32)
+    dK = np.ascontiguousarray(np.ravel(dK_u), np.float64)
+    kp3 = np.zeros(3)
+    kp3[:kp.size] = kp
+    hu, ht = ctypes.c_void_p(), ctypes.c_void_p()
+    N.call("mlg_traj2sparsemat", imDim, nPt, N.dptr(tt), None, N.iptr(Nu), N.dptr(dK), kernel_code(kernelType),
+           nWin, N.dptr(kp3), ctypes.byref(hu), ctypes.byref(ht))
+    meta = dict(N_u=Nu.copy(), d_u=dK.astype(np.float32), kernel_type=kernelType, nWin=nWin,
+                kernelParam=kp.astype(np.float32))
+    return DeviceMatrix(hu, meta, False), DeviceMatrix(ht, meta, True)
+
+
+def bmSparseMat_vec(G: bmSparseMat, v, layout: str = "column"):
+    """bmSparseMat_vec (src/sparseMat/m/bmSparseMat_vec.m:11-243) for a
+    cpp_prepared one-block matrix: complex or real v.
+
+    layout 'column': v [r_size, nVec] -> w [l_size, nVec] (the cC / rC MEX);
+    layout 'row': v [nVec, r_size] -> w [nVec, l_size] (the cR MEX)."""
+    r_size, r_jump, r_nJump, m_val, l_size, l_jump, l_nJump = G.jump_arrays()
+    v = np.asarray(v)
+    if v.ndim == 1:
+        v = v[:, None] if layout == "column" else v[None, :]
+    if layout == "column":
+        nVec = v.shape[1]
+        if np.iscomplexobj(v):
+            vR = np.ascontiguousarray(v.real.T, np.float32)
+            vI = np.ascontiguousarray(v.imag.T, np.float32)
+            wR = np.zeros((nVec, l_size), np.float32)
+            wI = np.zeros((nVec, l_size), np.float32)
+            N.call("mlg_sparsemat_vec_cC", r_size, N.iptr(r_jump), N.iptr(r_nJump), N.fptr(m_val), l_size,
+                   N.iptr(l_jump), l_nJump, N.fptr(vR), N.fptr(vI), nVec, N.fptr(wR), N.fptr(wI))
+            return (wR + 1j * wI).T.astype(np.complex64)
+        vR = np.ascontiguousarray(v.T, np.float32)
+        w = np.zeros((nVec, l_size), np.float32)
+        N.call("mlg_sparsemat_vec_rC", r_size, N.iptr(r_jump), N.iptr(r_nJump), N.fptr(m_val), l_size,
+               N.iptr(l_jump), l_nJump, N.fptr(vR), nVec, N.fptr(w))
+        return w.T.copy()
+    nVec = v.shape[0]
+    # column-major [nVec, r_size] == C-order [r_size][nVec]
+    vR = np.ascontiguousarray(np.real(v).T, np.float32)
+    vI = np.ascontiguousarray(np.imag(v).T, np.float32)
+    wR = np.zeros((l_size, nVec), np.float32)
+    wI = np.zeros((l_size, nVec), np.float32)
+    N.call("mlg_sparsemat_vec_cR", r_size, N.iptr(r_jump), N.iptr(r_nJump), N.fptr(m_val), l_size,
+           N.iptr(l_jump), l_nJump, N.fptr(vR), N.fptr(vI), nVec, N.fptr(wR), N.fptr(wI))
+    return (wR + 1j * wI).T.astype(np.complex64)

@@ -1,0 +1,70 @@
+"""Seeded synthetic workloads with the shapes of the benchmark
+configurations (no public dataset is involved; the reference's example data
+is not available).
+
+koosh3d: 3-D koosh-ball radial (spiral-phyllotaxis spoke directions),
+  128^3 image, 256^3 grid (oversampling 2), 4096 spokes x 256 samples,
+  16 coils with smooth random complex sensitivities, k-space simulated from a
+  random ellipsoid phantom by the forward operator, CG-SENSE 30 iterations,
+  Gaussian window nWin = 3, (sigma, K_max) = (0.61, 10).
+radial2d: 2-D golden-angle radial, 256^2 image, 512^2 grid, 256 spokes x 512
+  samples, Kaiser-Bessel width 3, 1 coil, i.i.d. Gaussian complex64 k-space.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import traj as T
+
+
+@dataclass
+class Workload:
+    name: str
+    imDim: int
+    n_u: np.ndarray
+    N_u: np.ndarray
+    dK_u: np.ndarray
+    nCh: int
+    nCGD: int
+    kernelType: str
+    nWin: int
+    kernelParam: list
+    t: np.ndarray = None
+    ve: np.ndarray = None
+    C: np.ndarray = None
+    x_true: np.ndarray = None
+    y: np.ndarray = None  # host k-space [nPt, nCh] when not simulated on the device
+    info: dict = field(default_factory=dict)
+
+    @property
+    def nPt(self) -> int:
+        return int(self.t.shape[1])
+
+
+def koosh3d(n=128, oversampling=2, nSpoke=4096, nRead=256, nCh=16, nCGD=30, seed=2) -> Workload:
+    N = n * oversampling
+    w = Workload("koosh3d", 3, np.array([n] * 3), np.array([N] * 3), np.ones(3), nCh, nCGD, "gauss", 3, [0.61, 10])
+    # the reference generator with N = nRead points per line covering +-N/2 grid units
+    w.t = T.bmTraj_fullRadial3_phyllotaxis_lineAssym2(nRead, nSpoke, 1, N / nRead)
+    w.ve = T.bmVolumeElement_full_radial3(w.t)
+    w.C = T.coil_maps(w.n_u, nCh, seed)
+    w.x_true = T.ellipsoid_phantom(w.n_u, 10, seed + 100)
+    w.info = dict(image=f"{n}^3", grid=f"{N}^3", spokes=nSpoke, samples_per_spoke=nRead, coils=nCh,
+                  kernel="gauss nWin=3 sigma=0.61", iterations=nCGD, seed=seed)
+    return w
+
+
+def radial2d(n=256, oversampling=2, nSpoke=256, nRead=512, nCh=1, nCGD=20, seed=1) -> Workload:
+    N = n * oversampling
+    w = Workload("radial2d", 2, np.array([n] * 2), np.array([N] * 2), np.ones(2), nCh, nCGD, "kaiser", 3,
+                 [1.95, 10, 10])
+    w.t = T.golden_angle_radial2(nRead, nSpoke, N / nRead)
+    w.ve = T.bmVolumeElement_voronoi_full_radial2(T.bmTraj_fullRadial2_lineAssym2(nRead, nSpoke, N / nRead), nRead)
+    rng = np.random.default_rng(seed)
+    w.C = np.ones((int(np.prod(w.n_u)), nCh), np.complex64)
+    w.y = (rng.standard_normal((w.t.shape[1], nCh)) + 1j * rng.standard_normal((w.t.shape[1], nCh))).astype(np.complex64)
+    w.info = dict(image=f"{n}^2", grid=f"{N}^2", spokes=nSpoke, samples_per_spoke=nRead, coils=nCh,
+                  kernel="kaiser nWin=3 tau=1.95 alpha=10", iterations=nCGD, seed=seed)
+    return w
