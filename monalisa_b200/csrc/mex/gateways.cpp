@@ -46,7 +46,7 @@ void leight(int imDim, int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[
   if (imDim == 1 && nrhs == 12) {
     iDn = 4, iCh = 5, iN = 7, iW = 9;
   } else {
-    need(nrhs == 7 + 2 * imDim, "wrong number of arguments");
+    need(nrhs == 8 + 2 * imDim, "wrong number of arguments");
     iDn = 2 + imDim, iCh = 3 + imDim, iN = 5 + imDim, iW = 5 + 2 * imDim;
   }
   const int nCh = scalar_i(prhs[iCh]), nPt = scalar_i(prhs[iCh + 1]);

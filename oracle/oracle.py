@@ -353,8 +353,9 @@ def traj2sparsemat(t, v, N_u, dK_u, kernelType=None, nWin=None, kernelParam=None
         A.sum_duplicates()
         A.eliminate_zeros()
         A.sort_indices()
-        s = np.add.reduceat(A.data, A.indptr[:-1]) if A.nnz else np.zeros(nPt)
-        s = np.where(np.diff(A.indptr) > 0, s, 0.0)
+        # row sums in ascending column order (MATLAB's sum(A, 2) over CSC)
+        row_of = np.repeat(np.arange(nPt), np.diff(A.indptr))
+        s = np.bincount(row_of, weights=A.data, minlength=nPt)
         inv = np.zeros_like(s)
         inv[s != 0] = 1.0 / s[s != 0]
         A = sp.csr_matrix((A.data * np.repeat(inv, np.diff(A.indptr)), A.indices, A.indptr), shape=A.shape)
