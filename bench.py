@@ -103,20 +103,27 @@ def _dist():
     return ws, rank, local
 
 
+STAGES = ["fwd_x", "fwd_y", "fwd_z", "gu", "gut", "inv_z", "inv_y", "inv_x"]
+
+
 def algorithmic_bytes(w, Gu, Gut, nCh):
-    """Bytes each stage must move at least (the per-unit figures of the
-    design notes), for one operator application."""
+    """Bytes each stage must move at least, for one operator application
+    (forward passes read the non-zero part only and write what the next pass
+    needs; the inverse passes keep only the cropped lines)."""
     nnz = Gu.nnz
     nPt = Gu.l_size
-    Nu = int(np.prod(w.N_u))
-    nu = int(np.prod(w.n_u))
+    N0, N1, N2 = (int(v) for v in w.N_u)
+    n0, n1, n2 = (int(v) for v in w.n_u)
+    Nu, nu = N0 * N1 * N2, n0 * n1 * n2
+    A = N0 * n1 * n2 * nCh * 8
+    B = N0 * N1 * n2 * nCh * 8
+    G = Nu * nCh * 8
     touched, _ = Gut.row_stats()
     return {
-        "pre": nu * 8 + nu * nCh * 8 + Nu * nCh * 8,
+        "fwd_x": nu * 8 + nu * nCh * 8 + A, "fwd_y": A + B, "fwd_z": B + G,
         "gu": nnz * 8 + 4 * (nPt + 1) + touched * nCh * 8 + nPt * nCh * 8,
-        "gut": nnz * 8 + 4 * (Nu + 1) + nPt * nCh * 8 + 4 * nPt + Nu * nCh * 8,
-        "post": nu * nCh * 8 + nu * nCh * 8 + nu * 8,
-        "fft": 2 * Nu * nCh * 8,
+        "gut": nnz * 8 + 4 * (Nu + 1) + nPt * nCh * 8 + 4 * nPt + G,
+        "inv_z": G + B, "inv_y": B + A, "inv_x": A + nu * nCh * 8 + nu * 8,
     }
 
 
@@ -221,19 +228,16 @@ def run_gpu(args):
 
     # per-stage live timing of the operator kernels (CUDA events on the
     # plan's stream) -> roofline of the dominant kernel of this library
-    st = np.zeros(6)
+    st = np.zeros(len(STAGES))
     N.call("mlg_plan_profile", rec.plan.handle, 5, N.dptr(st))
-    stage_names = ["pre", "fft_fwd", "gu", "gut", "fft_inv", "post"]
     B = algorithmic_bytes(w, Gu, Gut, w.nCh)
     peak, peak_kind = _peaks()
     stages = {}
-    for i, nm in enumerate(stage_names):
-        b = B["fft"] if nm.startswith("fft") else B[nm]
-        gbs = b / (st[i] * 1e-3) / 1e9
-        stages[nm] = {"ms": round(float(st[i]), 4), "algorithmic_bytes": int(b), "GBps": round(gbs, 1),
-                      "frac": round(gbs / peak, 4), "library": nm.startswith("fft")}
-    ours = [k for k in stage_names if not k.startswith("fft")]
-    dom = max(ours, key=lambda k: stages[k]["ms"])
+    for i, nm in enumerate(STAGES):
+        gbs = B[nm] / (st[i] * 1e-3) / 1e9 if st[i] > 0 else 0.0
+        stages[nm] = {"ms": round(float(st[i]), 4), "algorithmic_bytes": int(B[nm]), "GBps": round(gbs, 1),
+                      "frac": round(gbs / peak, 4)}
+    dom = max(STAGES, key=lambda k: stages[k]["ms"])
     traffic_file = os.path.join(ROOT, "profiles", "traffic.json")
     traffic = None
     if os.path.exists(traffic_file):

@@ -178,8 +178,8 @@ int mlg_plan_set_dk(mlg_plan_t p, const double* dK_u);
 int mlg_plan_device_bytes(mlg_plan_t p, long long* bytes);
 
 /* bmShanna (src/fourier123/map_function/nonCartesian/bmShanna_MATLAB.m:6-56)
- * on device buffers: x [prod(n_u)] (or [nCh][prod(n_u)] if x_per_coil) ->
- * y [nPt][nCh]. */
+ * on device buffers: x [prod(n_u)] (or [prod(n_u)][nCh], coil fastest, if
+ * x_per_coil) -> y [nPt][nCh]. */
 int mlg_shanna_dev(mlg_plan_t p, const void* x, int x_per_coil, void* y,
                    void* stream);
 /* bmNakatsha with C_flag = true (bmNakatsha_MATLAB.m:6-58): y [nPt][nCh] ->
@@ -218,9 +218,10 @@ int mlg_idf(int imDim, const int* N_u, const float* dK_u, int nCol,
 
 /* Times the stages of one Shanna and one Nakatsha on the plan's stream with
  * CUDA events, averaged over `iters` repetitions after one warm-up:
- * ms[0] pre-FFT kernel, ms[1] forward cuFFT, ms[2] Gu product,
- * ms[3] Gut product, ms[4] inverse cuFFT, ms[5] post-FFT kernel.
- * Measurement helper; no reference counterpart. */
+ * ms[0..2] forward x, y, z FFT passes (x pass fused with x .* KFC),
+ * ms[3] Gu product, ms[4] Gut product, ms[5..7] inverse z, y, x FFT passes
+ * (x pass fused with .* KFC_conj and the coil sum).  Passes a 2-D / 1-D
+ * plan does not run read 0.  Measurement helper; no reference counterpart. */
 int mlg_plan_profile(mlg_plan_t p, int iters, double* ms);
 
 /* ---- reconstructions ---------------------------------------------------- */

@@ -1,0 +1,56 @@
+// Pruned, fused line-FFT passes over coil-fastest volumes (mlg_fft.cu).
+//
+// A volume is float2 [z][y][x][c] (coils fastest).  One pass transforms every
+// line along one axis; the line lives on the full axis [0, N) but the input
+// buffer only holds [in_lo, in_lo + in_len) of it (the rest is zero) and
+// the output buffer only keeps [out_lo, out_lo + out_len).  Zero-filling and
+// cropping therefore cost nothing, and the centred-DFT modulation, the coil
+// maps (x .* KFC on the way in, .* KFC_conj + coil sum on the way out) are
+// fused into the first / last pass.
+#pragma once
+
+#include "mlg_internal.cuh"
+
+namespace mlg {
+
+enum class PassMode : int {
+  kPlain = 0,        // zero-filled load, cropped store
+  kShannaIn = 1,     // load x .* KFC .* (-1)^(x+y+z) from the image (axis x)
+  kNakatshaOut = 2,  // store sum_c s .* KFC_conj (coil sum) into the image (axis x)
+};
+
+struct FftAxisPlan {
+  int N = 0, N1 = 0, N2 = 0;  // N = N1 * N2, both <= 32
+  bool fast = false;          // templated power-of-two path
+  float2* tw = nullptr;       // exp(-2 pi i j / N), j < N (device)
+};
+
+struct PassDesc {
+  int ax = 0;                     // FFT axis
+  int dir = -1;                   // -1 forward (e^-i), +1 inverse (unnormalised)
+  int C = 1;                      // coils
+  int dims[3] = {1, 1, 1};        // line grid: extents of the non-FFT axes (dims[ax] unused)
+  const float2* in = nullptr;
+  float2* out = nullptr;
+  long long in_stride[3] = {0, 0, 0};   // in float2 units, coil stride 1
+  long long out_stride[3] = {0, 0, 0};
+  int in_lo = 0, in_len = 0, out_lo = 0, out_len = 0;
+  // fusion (kShannaIn / kNakatshaOut); image is [n_z][n_y][n_x], KFC [pix][c]
+  const float2* img = nullptr;
+  int img_per_coil = 0;
+  const float2* kfc = nullptr;
+  float2* img_out = nullptr;
+  int coord_off[3] = {0, 0, 0};   // full-grid coordinate of line-grid index 0 (sign)
+  float sfac = 1.0f;              // kNakatshaOut scale (sign applied per element)
+  double* partial = nullptr;      // kNakatshaOut: FP64 |x|^2 per CTA
+};
+
+int fft_axis_init(int N, FftAxisPlan& a);
+void fft_axis_free(FftAxisPlan& a);
+// Launches one pass; *n_partial receives the CTA count when partial sums are
+// written (kNakatshaOut).
+int fft_pass(const FftAxisPlan& a, PassMode mode, const PassDesc& d, int* n_partial, cudaStream_t s);
+// CTA count of a pass (for partial-sum buffer sizing).
+int fft_pass_blocks(const FftAxisPlan& a, const PassDesc& d);
+
+}  // namespace mlg

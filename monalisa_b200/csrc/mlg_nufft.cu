@@ -1,18 +1,27 @@
-// Fused NUFFT operators around cuFFT.
+// Fused NUFFT operators.
 //
 // bmShanna (src/fourier123/map_function/nonCartesian/bmShanna_MATLAB.m:28-54):
 //   x .* KFC -> zero-fill n_u -> N_u -> fftshift(fft(ifftshift)) -> Gu
 // bmNakatsha (bmNakatsha_MATLAB.m:32-56):
 //   Gut -> fftshift(ifft(ifftshift)) -> crop -> .* KFC_conj -> coil sum
 //
+// Gridded data are coil-fastest [cell][coil]: a grid cell's coils share one
+// 128-byte line, which is what the Gu / Gut gathers read or write per matrix
+// entry.  The transforms are this library's pruned line-FFT passes
+// (mlg_fft.cu): the forward runs x, y, z passes where each pass only
+// transforms the lines that can be non-zero and zero-fills on load (the
+// zero-filled n_u block never exists in memory); the inverse runs z, y, x
+// passes that keep only the lines of the cropped n_u block.  x .* KFC and the
+// input modulation are fused into the first forward pass, .* KFC_conj, the
+// output modulation, the 1/prod(N) scaling and the coil sum into the last
+// inverse pass.
+//
 // For even N the centred transform is a modulated plain DFT:
 //   fftshift(F(ifftshift(v)))[k] = (-1)^k (-1)^(N/2) F((-1)^n v)[k]
-// (same for the inverse).  The input modulation is fused into the
-// pre-kernel (Shanna) or folded into the row signs of Gut (Nakatsha); the
-// output modulation is folded into the column signs of Gu (Shanna) or fused
-// into the post-kernel (Nakatsha).  So a Shanna is three kernels
-// (pre, cuFFT, SpMM) and a Nakatsha three (SpMM, cuFFT, post), with every
-// elementwise stage of the reference fused into one of them.
+// (same for the inverse).  The input modulation of the forward is fused into
+// the x pass and its output modulation folded into the column signs of Gu;
+// the inverse's input modulation is folded into the row signs of Gut and its
+// output modulation fused into the last pass.
 #include <algorithm>
 #include <vector>
 
@@ -22,128 +31,137 @@ namespace mlg {
 
 constexpr int kEwThreads = 256;
 
-struct Geo {
-  int imDim;
-  int N[3], n[3], off[3];  // off = N/2 - n/2 (zero-fill / crop origin)
-  long long Nu, nu;
-  int nCh;
-};
-
-static Geo geo_of(const mlg_plan_s* p) {
-  Geo g;
-  g.imDim = p->imDim;
-  for (int d = 0; d < 3; ++d) {
-    g.N[d] = p->N[d];
-    g.n[d] = p->n[d];
-    g.off[d] = p->N[d] / 2 - p->n[d] / 2;
-  }
-  g.Nu = p->Nu_tot;
-  g.nu = p->nu_tot;
-  g.nCh = p->nCh;
-  return g;
-}
-
-__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
-  return make_float2(__fsub_rn(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y)),
-                     __fadd_rn(__fmul_rn(a.x, b.y), __fmul_rn(a.y, b.x)));
-}
-
-// grid[c][cell] = (cell in image block ? x[m] * KFC[c][m] : 0) * (-1)^(x+y+z)
-__global__ void __launch_bounds__(kEwThreads) shanna_pre_kernel(Geo g, const float2* __restrict__ x, int x_per_coil,
-                                                                const float2* __restrict__ KFC,
-                                                                float2* __restrict__ grid) {
-  const long long total = g.Nu * g.nCh;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
-       i += (long long)gridDim.x * blockDim.x) {
-    const int c = (int)(i / g.Nu);
-    const long long cell = i - (long long)c * g.Nu;
-    const int cx = (int)(cell % g.N[0]);
-    const long long q = cell / g.N[0];
-    const int cy = (int)(q % g.N[1]);
-    const int cz = (int)(q / g.N[1]);
-    const int bx = cx - g.off[0], by = cy - g.off[1], bz = cz - g.off[2];
-    float2 v = make_float2(0.f, 0.f);
-    if (bx >= 0 && bx < g.n[0] && by >= 0 && by < g.n[1] && bz >= 0 && bz < g.n[2]) {
-      const long long m = bx + (long long)g.n[0] * (by + (long long)g.n[1] * bz);
-      const float2 xv = __ldg(x + (x_per_coil ? (long long)c * g.nu + m : m));
-      v = cmul(xv, __ldg(KFC + (long long)c * g.nu + m));
-      if ((cx + cy + cz) & 1) v = make_float2(-v.x, -v.y);
-    }
-    grid[i] = v;
-  }
-}
-
-// x[m] = scale * sum_c KFCc[c][m] * s(n) * grid[c][n(m)],
-// s(n) = (-1)^(x+y+z) * shift_const / prod(N); optional FP64 |x|^2 partials.
-__global__ void __launch_bounds__(kEwThreads) nakatsha_post_kernel(Geo g, const float2* __restrict__ grid,
-                                                                   const float2* __restrict__ KFCc, float sfac,
-                                                                   float2* __restrict__ x, double* partial) {
-  __shared__ double sh[kEwThreads / 32];
-  double sq = 0.0;
-  for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < g.nu;
-       m += (long long)gridDim.x * blockDim.x) {
-    const int bx = (int)(m % g.n[0]);
-    const long long q = m / g.n[0];
-    const int by = (int)(q % g.n[1]);
-    const int bz = (int)(q / g.n[1]);
-    const int cx = bx + g.off[0], cy = by + g.off[1], cz = bz + g.off[2];
-    const long long cell = cx + (long long)g.N[0] * (cy + (long long)g.N[1] * cz);
-    const float s = ((cx + cy + cz) & 1) ? -sfac : sfac;
-    float2 acc = make_float2(0.f, 0.f);
-    for (int c = 0; c < g.nCh; ++c) {
-      float2 v = __ldg(grid + (long long)c * g.Nu + cell);
-      v = make_float2(__fmul_rn(v.x, s), __fmul_rn(v.y, s));
-      const float2 t = cmul(v, __ldg(KFCc + (long long)c * g.nu + m));
-      acc = make_float2(__fadd_rn(acc.x, t.x), __fadd_rn(acc.y, t.y));
-    }
-    x[m] = acc;
-    sq += (double)acc.x * acc.x + (double)acc.y * acc.y;
-  }
-  if (partial) {
-    for (int o = 16; o > 0; o >>= 1) sq += __shfl_down_sync(0xffffffffu, sq, o);
-    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = sq;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double t = 0.0;
-      for (int i = 0; i < kEwThreads / 32; ++i) t += sh[i];
-      partial[blockIdx.x] = t;
-    }
-  }
-}
-
 static int ew_grid(long long n) {
   return (int)std::max<long long>(1, std::min<long long>((n + kEwThreads - 1) / kEwThreads, 148LL * 16));
 }
 
-int post_partial_count(const mlg_plan_s* p) { return ew_grid(p->nu_tot); }
-
-int shanna_pre(mlg_plan_s* p, const float2* x, bool x_per_coil, cudaStream_t s) {
-  const Geo g = geo_of(p);
-  shanna_pre_kernel<<<ew_grid(g.Nu * g.nCh), kEwThreads, 0, s>>>(g, x, x_per_coil ? 1 : 0, p->KFC, p->grid);
-  MLG_LAUNCHED();
-  return MLG_OK;
+// element strides (float2 units) of a coil-fastest box with extents e[3]
+static void box_strides(const int e[3], int C, long long st[3]) {
+  st[0] = C;
+  st[1] = (long long)C * e[0];
+  st[2] = (long long)C * e[0] * e[1];
 }
 
-int fft_exec(mlg_plan_s* p, bool forward, cudaStream_t s) {
-  MLG_CUFFT(cufftSetStream(p->fft, s));
-  MLG_CUFFT(cufftExecC2C(p->fft, (cufftComplex*)p->grid, (cufftComplex*)p->grid,
-                         forward ? CUFFT_FORWARD : CUFFT_INVERSE));
-  count_launch();
-  return MLG_OK;
+// Forward passes: x (image -> A), y (A -> B), z (B -> grid).  The last pass
+// of the transform writes the grid.
+static int forward_pass(mlg_plan_s* p, int ax, const float2* x, bool x_per_coil, cudaStream_t s) {
+  const int C = p->nCh, d = p->imDim;
+  const int* N = p->N;
+  const int* n = p->n;
+  const int eA[3] = {N[0], n[1], n[2]};
+  const int eB[3] = {N[0], N[1], n[2]};
+  const int eG[3] = {N[0], N[1], N[2]};
+  PassDesc pd;
+  pd.ax = ax;
+  pd.dir = -1;
+  pd.C = C;
+  if (ax == 0) {
+    pd.dims[1] = n[1];
+    pd.dims[2] = n[2];
+    pd.in_lo = p->off[0];
+    pd.in_len = n[0];
+    pd.img = x;
+    pd.img_per_coil = x_per_coil ? 1 : 0;
+    pd.kfc = p->KFC;
+    for (int k = 0; k < 3; ++k) pd.coord_off[k] = p->off[k];
+    pd.out = d == 1 ? p->grid : p->bufA;
+    box_strides(d == 1 ? eG : eA, C, pd.out_stride);
+    pd.out_lo = 0;
+    pd.out_len = N[0];
+    return fft_pass(p->ax[0], PassMode::kShannaIn, pd, nullptr, s);
+  }
+  if (ax == 1) {
+    pd.dims[0] = N[0];
+    pd.dims[2] = n[2];
+    pd.in = p->bufA;
+    box_strides(eA, C, pd.in_stride);
+    pd.in_lo = p->off[1];
+    pd.in_len = n[1];
+    pd.out = d == 2 ? p->grid : p->bufB;
+    box_strides(d == 2 ? eG : eB, C, pd.out_stride);
+    pd.out_lo = 0;
+    pd.out_len = N[1];
+    return fft_pass(p->ax[1], PassMode::kPlain, pd, nullptr, s);
+  }
+  pd.dims[0] = N[0];
+  pd.dims[1] = N[1];
+  pd.in = p->bufB;
+  box_strides(eB, C, pd.in_stride);
+  pd.in_lo = p->off[2];
+  pd.in_len = n[2];
+  pd.out = p->grid;
+  box_strides(eG, C, pd.out_stride);
+  pd.out_lo = 0;
+  pd.out_len = N[2];
+  return fft_pass(p->ax[2], PassMode::kPlain, pd, nullptr, s);
 }
 
-int shanna_run(mlg_plan_s* p, const float2* x, bool x_per_coil, float2* y, const float* sqn_w, double* partial,
-               int* n_partial, cudaStream_t s) {
-  MLG_TRY(shanna_pre(p, x, x_per_coil, s));
-  MLG_TRY(fft_exec(p, true, s));
-  return shanna_spmm(p, y, sqn_w, partial, n_partial, s);
+// Inverse passes: z (grid -> B), y (B -> A), x (A -> image, coil sum).  The
+// first pass of the transform reads the grid.
+static int inverse_pass(mlg_plan_s* p, int ax, float scale, float2* x, double* partial, int* n_partial,
+                        cudaStream_t s) {
+  const int C = p->nCh, d = p->imDim;
+  const int* N = p->N;
+  const int* n = p->n;
+  const int eA[3] = {N[0], n[1], n[2]};
+  const int eB[3] = {N[0], N[1], n[2]};
+  const int eG[3] = {N[0], N[1], N[2]};
+  PassDesc pd;
+  pd.ax = ax;
+  pd.dir = 1;
+  pd.C = C;
+  if (ax == 2) {
+    pd.dims[0] = N[0];
+    pd.dims[1] = N[1];
+    pd.in = p->grid;
+    box_strides(eG, C, pd.in_stride);
+    pd.in_lo = 0;
+    pd.in_len = N[2];
+    pd.out = p->bufB;
+    box_strides(eB, C, pd.out_stride);
+    pd.out_lo = p->off[2];
+    pd.out_len = n[2];
+    return fft_pass(p->ax[2], PassMode::kPlain, pd, nullptr, s);
+  }
+  if (ax == 1) {
+    pd.dims[0] = N[0];
+    pd.dims[2] = n[2];
+    pd.in = d == 2 ? p->grid : p->bufB;
+    box_strides(d == 2 ? eG : eB, C, pd.in_stride);
+    pd.in_lo = 0;
+    pd.in_len = N[1];
+    pd.out = p->bufA;
+    box_strides(eA, C, pd.out_stride);
+    pd.out_lo = p->off[1];
+    pd.out_len = n[1];
+    return fft_pass(p->ax[1], PassMode::kPlain, pd, nullptr, s);
+  }
+  pd.dims[1] = n[1];
+  pd.dims[2] = n[2];
+  pd.in = d == 1 ? p->grid : p->bufA;
+  box_strides(d == 1 ? eG : eA, C, pd.in_stride);
+  pd.in_lo = 0;
+  pd.in_len = N[0];
+  pd.out_lo = p->off[0];
+  pd.out_len = n[0];
+  pd.img_out = x;
+  pd.kfc = p->KFCc;
+  for (int k = 0; k < 3; ++k) pd.coord_off[k] = p->off[k];
+  pd.sfac = (float)((double)p->shift_const / (double)p->Nu_tot * (double)scale);
+  pd.partial = partial;
+  return fft_pass(p->ax[0], PassMode::kNakatshaOut, pd, n_partial, s);
 }
 
-int shanna_spmm(mlg_plan_s* p, float2* y, const float* sqn_w, double* partial, int* n_partial, cudaStream_t s) {
+int shanna_stage(mlg_plan_s* p, int stage, const float2* x, bool x_per_coil, float2* y, const float* sqn_w,
+                 double* partial, int* n_partial, cudaStream_t s) {
+  if (stage < 3) {
+    if (stage >= p->imDim) return MLG_OK;
+    return forward_pass(p, stage, x, x_per_coil, s);
+  }
   SpmmArgs a;
   a.m = &p->Gu_s;
   a.nCh = p->nCh;
-  a.in.layout = Layout::kCoilC64;
+  a.in.layout = Layout::kPointC64;
   a.in.a = p->grid;
   a.in.rows = p->Nu_tot;
   a.out.layout = Layout::kPointC64;
@@ -155,34 +173,38 @@ int shanna_spmm(mlg_plan_s* p, float2* y, const float* sqn_w, double* partial, i
   return spmm(a, s);
 }
 
-int nakatsha_run(mlg_plan_s* p, const float2* y, const float* HY, float scale, float2* x, double* partial,
-                 int* n_partial, cudaStream_t s) {
-  MLG_TRY(nakatsha_spmm(p, y, HY, s));
-  MLG_TRY(fft_exec(p, false, s));
-  return nakatsha_post(p, scale, x, partial, n_partial, s);
+int nakatsha_stage(mlg_plan_s* p, int stage, const float2* y, const float* HY, float scale, float2* x,
+                   double* partial, int* n_partial, cudaStream_t s) {
+  if (stage == 0) {
+    SpmmArgs a;
+    a.m = &p->Gut_s;
+    a.nCh = p->nCh;
+    a.in.layout = Layout::kPointC64;
+    a.in.a = const_cast<float2*>(y);
+    a.in.rows = p->nPt;
+    a.in_row_scale = HY;
+    a.out.layout = Layout::kPointC64;
+    a.out.a = p->grid;
+    a.out.rows = p->Nu_tot;
+    return spmm(a, s);
+  }
+  const int ax = 3 - stage;  // stages 1, 2, 3 = z, y, x passes
+  if (ax >= p->imDim) return MLG_OK;
+  return inverse_pass(p, ax, scale, x, partial, n_partial, s);
 }
 
-int nakatsha_post(mlg_plan_s* p, float scale, float2* x, double* partial, int* n_partial, cudaStream_t s) {
-  const Geo g = geo_of(p);
-  const float sfac = (float)((double)p->shift_const / (double)p->Nu_tot * (double)scale);
-  nakatsha_post_kernel<<<ew_grid(g.nu), kEwThreads, 0, s>>>(g, p->grid, p->KFCc, sfac, x, partial);
-  MLG_LAUNCHED();
-  if (n_partial) *n_partial = partial ? ew_grid(g.nu) : 0;
+int shanna_run(mlg_plan_s* p, const float2* x, bool x_per_coil, float2* y, const float* sqn_w, double* partial,
+               int* n_partial, cudaStream_t s) {
+  for (int st = 0; st < kShannaStages; ++st)
+    MLG_TRY(shanna_stage(p, st, x, x_per_coil, y, sqn_w, partial, n_partial, s));
   return MLG_OK;
 }
 
-int nakatsha_spmm(mlg_plan_s* p, const float2* y, const float* HY, cudaStream_t s) {
-  SpmmArgs a;
-  a.m = &p->Gut_s;
-  a.nCh = p->nCh;
-  a.in.layout = Layout::kPointC64;
-  a.in.a = const_cast<float2*>(y);
-  a.in.rows = p->nPt;
-  a.in_row_scale = HY;
-  a.out.layout = Layout::kCoilC64;
-  a.out.a = p->grid;
-  a.out.rows = p->Nu_tot;
-  return spmm(a, s);
+int nakatsha_run(mlg_plan_s* p, const float2* y, const float* HY, float scale, float2* x, double* partial,
+                 int* n_partial, cudaStream_t s) {
+  for (int st = 0; st < kNakatshaStages; ++st)
+    MLG_TRY(nakatsha_stage(p, st, y, HY, scale, x, partial, n_partial, s));
+  return MLG_OK;
 }
 
 // ---- layout conversion kernels ----------------------------------------------
@@ -251,12 +273,14 @@ static void plan_free(mlg_plan_s* p) {
   if (!p) return;
   cudaSetDevice(p->device);
   if (p->cg_graph) cudaGraphExecDestroy(p->cg_graph);
-  if (p->fft_ready) cufftDestroy(p->fft);
+  for (int d = 0; d < 3; ++d) fft_axis_free(p->ax[d]);
   csr_free_sign_copy(p->Gu_s);
   csr_free_sign_copy(p->Gut_s);
   cudaFree(p->KFC);
   cudaFree(p->KFCc);
   cudaFree(p->grid);
+  cudaFree(p->bufA);
+  cudaFree(p->bufB);
   cudaFree(p->partial);
   cudaFree(p->scalars);
   cudaFree(p->x_p);
@@ -270,9 +294,26 @@ static void plan_free(mlg_plan_s* p) {
   delete p;
 }
 
+// KFC / KFC_conj arrive as [prod(n_u), nCh] column layout (separate real and
+// imaginary parts, host memory) and are stored coil-fastest.
+static int upload_kfc(const float* re, const float* im, long long nu, int nCh, float2* dst, cudaStream_t s) {
+  const long long nk = nu * nCh;
+  if (!re) {
+    MLG_CUDA(cudaMemsetAsync(dst, 0, sizeof(float2) * (size_t)nk, s));
+    return MLG_OK;
+  }
+  DevBuf<float> tmp;
+  MLG_TRY(tmp.alloc(2 * (size_t)nk, s));
+  MLG_CUDA(cudaMemcpyAsync(tmp.p, re, sizeof(float) * nk, cudaMemcpyHostToDevice, s));
+  if (im) MLG_CUDA(cudaMemcpyAsync(tmp.p + nk, im, sizeof(float) * nk, cudaMemcpyHostToDevice, s));
+  MLG_TRY(pack_col_to_point(tmp.p, im ? tmp.p + nk : nullptr, nu, nCh, dst, s));
+  MLG_CUDA(cudaStreamSynchronize(s));
+  return MLG_OK;
+}
+
 static int plan_create_impl(int imDim, const int* N_u, const int* n_u, int nCh, const Csr* Gu, const Csr* Gut,
                             const float* KFC_re, const float* KFC_im, const float* KFCc_re, const float* KFCc_im,
-                            bool kfc_on_device, mlg_plan_s** out) {
+                            mlg_plan_s** out) {
   MLG_CHECK(out, "NULL output");
   *out = nullptr;
   MLG_CHECK(imDim >= 1 && imDim <= 3, "imDim must be 1, 2 or 3");
@@ -280,6 +321,10 @@ static int plan_create_impl(int imDim, const int* N_u, const int* n_u, int nCh, 
   MLG_CHECK(Gu || Gut, "at least one of Gu / Gut is needed");
   MLG_TRY(ensure_device());
   mlg_plan_s* p = new mlg_plan_s();
+  auto bail = [&](int status) {
+    plan_free(p);
+    return status;
+  };
   cudaGetDevice(&p->device);
   p->imDim = imDim;
   p->nCh = nCh;
@@ -289,13 +334,12 @@ static int plan_create_impl(int imDim, const int* N_u, const int* n_u, int nCh, 
     p->N[d] = d < imDim ? N_u[d] : 1;
     p->n[d] = d < imDim ? (n_u ? n_u[d] : N_u[d]) : 1;
     if (d < imDim) {
-      if (p->N[d] < 2 || (p->N[d] & 1) || p->n[d] < 2 || (p->n[d] & 1) || p->n[d] > p->N[d]) {
-        plan_free(p);
-        return fail(MLG_ERR_ARG, "N_u and n_u must be even, >= 2, with n_u <= N_u (dim %d: N=%d n=%d)", d,
-                    N_u[d], n_u ? n_u[d] : N_u[d]);
-      }
+      if (p->N[d] < 2 || (p->N[d] & 1) || p->n[d] < 2 || (p->n[d] & 1) || p->n[d] > p->N[d])
+        return bail(fail(MLG_ERR_ARG, "N_u and n_u must be even, >= 2, with n_u <= N_u (dim %d: N=%d n=%d)", d,
+                         N_u[d], n_u ? n_u[d] : N_u[d]));
       if ((p->N[d] / 2) & 1) sc = -sc;
     }
+    p->off[d] = p->N[d] / 2 - p->n[d] / 2;
     Nu *= p->N[d];
     nu *= p->n[d];
   }
@@ -304,26 +348,16 @@ static int plan_create_impl(int imDim, const int* N_u, const int* n_u, int nCh, 
   p->shift_const = sc;
   p->HX = 1.0;  // dK_u = 1 until mlg_plan_set_dk
   for (int d = 0; d < imDim; ++d) p->HX = (double)((float)p->HX * (1.0f / (float)p->N[d]));
-  if (Gu && (Gu->r_size != Nu)) {
-    plan_free(p);
-    return fail(MLG_ERR_ARG, "Gu has %d columns, prod(N_u) = %lld", Gu->r_size, Nu);
-  }
-  if (Gut && (Gut->l_size != Nu)) {
-    plan_free(p);
-    return fail(MLG_ERR_ARG, "Gut has %d rows, prod(N_u) = %lld", Gut->l_size, Nu);
-  }
-  if (Gu && Gut && Gu->l_size != Gut->r_size) {
-    plan_free(p);
-    return fail(MLG_ERR_ARG, "Gu rows (%d) and Gut columns (%d) differ", Gu->l_size, Gut->r_size);
-  }
+  if (Gu && Gu->r_size != Nu) return bail(fail(MLG_ERR_ARG, "Gu has %d columns, prod(N_u) = %lld", Gu->r_size, Nu));
+  if (Gut && Gut->l_size != Nu) return bail(fail(MLG_ERR_ARG, "Gut has %d rows, prod(N_u) = %lld", Gut->l_size, Nu));
+  if (Gu && Gut && Gu->l_size != Gut->r_size)
+    return bail(fail(MLG_ERR_ARG, "Gu rows (%d) and Gut columns (%d) differ", Gu->l_size, Gut->r_size));
   p->nPt = Gu ? Gu->l_size : Gut->r_size;
   p->Gu = Gu;
   p->Gut = Gut;
   int st = MLG_OK;
-  auto bail = [&](int status) {
-    plan_free(p);
-    return status;
-  };
+  for (int d = 0; d < imDim; ++d)
+    if ((st = fft_axis_init(p->N[d], p->ax[d])) != MLG_OK) return bail(st);
   if (cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreateWithFlags(&p->ev_in, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&p->ev_out, cudaEventDisableTiming) != cudaSuccess) {
@@ -334,48 +368,24 @@ static int plan_create_impl(int imDim, const int* N_u, const int* n_u, int nCh, 
   if (Gu && (st = csr_sign_copy(*Gu, false, imDim, p->N, sc, p->Gu_s, s)) != MLG_OK) return bail(st);
   if (Gut && (st = csr_sign_copy(*Gut, true, imDim, p->N, 1.0f, p->Gut_s, s)) != MLG_OK) return bail(st);
   const size_t kbytes = sizeof(float2) * (size_t)nu * nCh;
+  const size_t gbytes = sizeof(float2) * (size_t)Nu * nCh;
+  const size_t abytes = sizeof(float2) * (size_t)p->N[0] * p->n[1] * p->n[2] * nCh;
+  const size_t bbytes = sizeof(float2) * (size_t)p->N[0] * p->N[1] * p->n[2] * nCh;
   if (cudaMalloc(&p->KFC, kbytes) != cudaSuccess || cudaMalloc(&p->KFCc, kbytes) != cudaSuccess ||
-      cudaMalloc(&p->grid, sizeof(float2) * (size_t)Nu * nCh) != cudaSuccess) {
+      cudaMalloc(&p->grid, gbytes) != cudaSuccess || cudaMalloc(&p->bufA, abytes) != cudaSuccess ||
+      cudaMalloc(&p->bufB, bbytes) != cudaSuccess) {
     cudaGetLastError();
     return bail(fail(MLG_ERR_OOM, "plan: device allocation failed"));
   }
-  // KFC / KFC_conj: [prod(n_u), nCh] column layout = coil-major
-  const long long nk = nu * nCh;
-  if (kfc_on_device) {
-    if ((st = interleave(KFC_re, KFC_im, nk, p->KFC, s)) != MLG_OK) return bail(st);
-    if ((st = interleave(KFCc_re, KFCc_im, nk, p->KFCc, s)) != MLG_OK) return bail(st);
-  } else {
-    float* tmp = nullptr;
-    if (cudaMalloc(&tmp, sizeof(float) * 2 * (size_t)nk) != cudaSuccess) {
-      cudaGetLastError();
-      return bail(fail(MLG_ERR_OOM, "plan: staging allocation failed"));
-    }
-    const float* srcs[2][2] = {{KFC_re, KFC_im}, {KFCc_re, KFCc_im}};
-    float2* dsts[2] = {p->KFC, p->KFCc};
-    for (int k = 0; k < 2; ++k) {
-      if (!srcs[k][0]) {
-        cudaMemsetAsync(dsts[k], 0, sizeof(float2) * (size_t)nk, s);
-        continue;
-      }
-      cudaMemcpyAsync(tmp, srcs[k][0], sizeof(float) * nk, cudaMemcpyHostToDevice, s);
-      if (srcs[k][1]) cudaMemcpyAsync(tmp + nk, srcs[k][1], sizeof(float) * nk, cudaMemcpyHostToDevice, s);
-      if ((st = interleave(tmp, srcs[k][1] ? tmp + nk : nullptr, nk, dsts[k], s)) != MLG_OK) {
-        cudaFree(tmp);
-        return bail(st);
-      }
-    }
-    cudaStreamSynchronize(s);
-    cudaFree(tmp);
-  }
-  int n[3];
-  for (int d = 0; d < imDim; ++d) n[d] = p->N[imDim - 1 - d];  // cuFFT: slowest dimension first
-  if (cufftPlanMany(&p->fft, imDim, n, nullptr, 1, (int)Nu, nullptr, 1, (int)Nu, CUFFT_C2C, nCh) != CUFFT_SUCCESS)
-    return bail(fail(MLG_ERR_CUDA, "cufftPlanMany failed for N=(%d,%d,%d) batch %d", p->N[0], p->N[1], p->N[2], nCh));
-  p->fft_ready = true;
-  size_t fft_bytes = 0;
-  cufftGetSize(p->fft, &fft_bytes);
+  if ((st = upload_kfc(KFC_re, KFC_im, nu, nCh, p->KFC, s)) != MLG_OK) return bail(st);
+  if ((st = upload_kfc(KFCc_re, KFCc_im, nu, nCh, p->KFCc, s)) != MLG_OK) return bail(st);
   // partial-sum buffer: the largest CTA count any fused reduction uses
-  int cap = post_partial_count(p) + 8;
+  PassDesc last;
+  last.ax = 0;
+  last.C = nCh;
+  last.dims[1] = p->n[1];
+  last.dims[2] = p->n[2];
+  int cap = fft_pass_blocks(p->ax[0], last) + 8;
   if (Gu) {
     SpmmArgs a;
     a.m = &p->Gu_s;
@@ -383,6 +393,7 @@ static int plan_create_impl(int imDim, const int* N_u, const int* n_u, int nCh, 
     cap = std::max(cap, spmm_partial_count(a));
   }
   cap = std::max(cap, ew_grid((long long)p->nPt * nCh) + 8);
+  cap = std::max(cap, 256);  // the solver's two-stage max over ve uses 128 floats
   p->partial_cap = cap;
   if (cudaMalloc(&p->partial, sizeof(double) * (size_t)cap) != cudaSuccess ||
       cudaMalloc(&p->scalars, sizeof(double) * 64) != cudaSuccess) {
@@ -390,13 +401,13 @@ static int plan_create_impl(int imDim, const int* N_u, const int* n_u, int nCh, 
     return bail(fail(MLG_ERR_OOM, "plan: partial buffer allocation failed"));
   }
   if (cudaStreamSynchronize(s) != cudaSuccess) return bail(fail(MLG_ERR_CUDA, "plan creation failed"));
-  p->bytes = 2 * kbytes + sizeof(float2) * (size_t)Nu * nCh + fft_bytes +
+  p->bytes = 2 * kbytes + gbytes + abytes + bbytes +
              sizeof(float) * (size_t)((Gu ? Gu->nnz : 0) + (Gut ? Gut->nnz : 0)) + sizeof(double) * (cap + 64);
   *out = p;
   return MLG_OK;
 }
 
-// Orders `work` on the plan's stream after the caller's stream and back.
+// Orders the plan's stream after the caller's stream and back.
 struct StreamJoin {
   mlg_plan_s* p;
   cudaStream_t user;
@@ -421,7 +432,7 @@ int mlg_plan_create(int imDim, const int* N_u, const int* n_u, int nCh, mlg_matr
                     mlg_plan_t* out) {
   MLG_CHECK(Gu || Gut, "at least one of Gu / Gut is needed");
   return plan_create_impl(imDim, N_u, n_u, nCh, Gu ? &Gu->csr : nullptr, Gut ? &Gut->csr : nullptr, KFC_re, KFC_im,
-                          KFCc_re, KFCc_im, false, out);
+                          KFCc_re, KFCc_im, out);
 }
 
 int mlg_plan_destroy(mlg_plan_t p) {
@@ -461,38 +472,38 @@ int mlg_shanna(int imDim, const int* N_u, const int* n_u, int nCh, const float* 
   mlg_matrix_t G = nullptr;
   MLG_TRY(mlg_matrix_create(r_size, r_jump, r_nJump, m_val, l_size, l_jump, l_nJump, &G));
   mlg_plan_s* p = nullptr;
-  int st = plan_create_impl(imDim, N_u, n_u, nCh, &G->csr, nullptr, KFC_R, KFC_I, nullptr, nullptr, false, &p);
+  int st = plan_create_impl(imDim, N_u, n_u, nCh, &G->csr, nullptr, KFC_R, KFC_I, nullptr, nullptr, &p);
   if (st != MLG_OK) {
     mlg_matrix_destroy(G);
     return st;
   }
   cudaStream_t s = p->stream;
   const long long nx = p->nu_tot * x_nCol, ny = (long long)p->nPt * nCh;
-  float *dx = nullptr, *dy = nullptr;
-  float2 *x2 = nullptr, *y2 = nullptr;
-  if (cudaMalloc(&dx, sizeof(float) * 2 * nx) != cudaSuccess || cudaMalloc(&x2, sizeof(float2) * nx) != cudaSuccess ||
-      cudaMalloc(&y2, sizeof(float2) * ny) != cudaSuccess || cudaMalloc(&dy, sizeof(float) * 2 * ny) != cudaSuccess) {
-    cudaGetLastError();
-    st = fail(MLG_ERR_OOM, "shanna: device allocation failed");
-  }
+  DevBuf<float> dx, dy;
+  DevBuf<float2> x2, y2;
+  if (st == MLG_OK) st = dx.alloc(2 * nx, s);
+  if (st == MLG_OK) st = x2.alloc(nx, s);
+  if (st == MLG_OK) st = y2.alloc(ny, s);
+  if (st == MLG_OK) st = dy.alloc(2 * ny, s);
   if (st == MLG_OK) {
-    cudaMemcpyAsync(dx, xR, sizeof(float) * nx, cudaMemcpyHostToDevice, s);
-    if (xI) cudaMemcpyAsync(dx + nx, xI, sizeof(float) * nx, cudaMemcpyHostToDevice, s);
-    st = interleave(dx, xI ? dx + nx : nullptr, nx, x2, s);
+    cudaMemcpyAsync(dx.p, xR, sizeof(float) * nx, cudaMemcpyHostToDevice, s);
+    if (xI) cudaMemcpyAsync(dx.p + nx, xI, sizeof(float) * nx, cudaMemcpyHostToDevice, s);
+    // [prod(n_u), x_nCol] column layout -> [pixel][coil]
+    st = pack_col_to_point(dx.p, xI ? dx.p + nx : nullptr, p->nu_tot, x_nCol, x2.p, s);
   }
-  if (st == MLG_OK) st = shanna_run(p, x2, x_nCol > 1, y2, nullptr, nullptr, nullptr, s);
-  if (st == MLG_OK) st = unpack_point_to_col(y2, p->nPt, nCh, dy, dy + ny, s);
+  if (st == MLG_OK) st = shanna_run(p, x2.p, x_nCol > 1, y2.p, nullptr, nullptr, nullptr, s);
+  if (st == MLG_OK) st = unpack_point_to_col(y2.p, p->nPt, nCh, dy.p, dy.p + ny, s);
   if (st == MLG_OK) {
-    cudaMemcpyAsync(yR, dy, sizeof(float) * ny, cudaMemcpyDeviceToHost, s);
-    cudaMemcpyAsync(yI, dy + ny, sizeof(float) * ny, cudaMemcpyDeviceToHost, s);
-    if (cudaStreamSynchronize(s) != cudaSuccess) st = fail(MLG_ERR_CUDA, "shanna failed: %s",
-                                                           cudaGetErrorString(cudaGetLastError()));
+    cudaMemcpyAsync(yR, dy.p, sizeof(float) * ny, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(yI, dy.p + ny, sizeof(float) * ny, cudaMemcpyDeviceToHost, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess)
+      st = fail(MLG_ERR_CUDA, "shanna failed: %s", cudaGetErrorString(cudaGetLastError()));
   }
+  dx.reset();
+  dy.reset();
+  x2.reset();
+  y2.reset();
   cudaStreamSynchronize(s);
-  cudaFree(dx);
-  cudaFree(dy);
-  cudaFree(x2);
-  cudaFree(y2);
   plan_free(p);
   mlg_matrix_destroy(G);
   return st;
@@ -506,38 +517,37 @@ int mlg_nakatsha(int imDim, const int* N_u, const int* n_u, int nCh, const float
   mlg_matrix_t G = nullptr;
   MLG_TRY(mlg_matrix_create(r_size, r_jump, r_nJump, m_val, l_size, l_jump, l_nJump, &G));
   mlg_plan_s* p = nullptr;
-  int st = plan_create_impl(imDim, N_u, n_u, nCh, nullptr, &G->csr, nullptr, nullptr, KFCc_R, KFCc_I, false, &p);
+  int st = plan_create_impl(imDim, N_u, n_u, nCh, nullptr, &G->csr, nullptr, nullptr, KFCc_R, KFCc_I, &p);
   if (st != MLG_OK) {
     mlg_matrix_destroy(G);
     return st;
   }
   cudaStream_t s = p->stream;
   const long long ny = (long long)p->nPt * nCh, nx = p->nu_tot;
-  float *dy = nullptr, *dx = nullptr;
-  float2 *y2 = nullptr, *x2 = nullptr;
-  if (cudaMalloc(&dy, sizeof(float) * 2 * ny) != cudaSuccess || cudaMalloc(&y2, sizeof(float2) * ny) != cudaSuccess ||
-      cudaMalloc(&x2, sizeof(float2) * nx) != cudaSuccess || cudaMalloc(&dx, sizeof(float) * 2 * nx) != cudaSuccess) {
-    cudaGetLastError();
-    st = fail(MLG_ERR_OOM, "nakatsha: device allocation failed");
-  }
+  DevBuf<float> dy, dx;
+  DevBuf<float2> y2, x2;
+  if (st == MLG_OK) st = dy.alloc(2 * ny, s);
+  if (st == MLG_OK) st = y2.alloc(ny, s);
+  if (st == MLG_OK) st = x2.alloc(nx, s);
+  if (st == MLG_OK) st = dx.alloc(2 * nx, s);
   if (st == MLG_OK) {
-    cudaMemcpyAsync(dy, yR, sizeof(float) * ny, cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(dy + ny, yI, sizeof(float) * ny, cudaMemcpyHostToDevice, s);
-    st = pack_col_to_point(dy, dy + ny, p->nPt, nCh, y2, s);
+    cudaMemcpyAsync(dy.p, yR, sizeof(float) * ny, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(dy.p + ny, yI, sizeof(float) * ny, cudaMemcpyHostToDevice, s);
+    st = pack_col_to_point(dy.p, dy.p + ny, p->nPt, nCh, y2.p, s);
   }
-  if (st == MLG_OK) st = nakatsha_run(p, y2, nullptr, 1.0f, x2, nullptr, nullptr, s);
-  if (st == MLG_OK) st = deinterleave(x2, nx, dx, dx + nx, s);
+  if (st == MLG_OK) st = nakatsha_run(p, y2.p, nullptr, 1.0f, x2.p, nullptr, nullptr, s);
+  if (st == MLG_OK) st = deinterleave(x2.p, nx, dx.p, dx.p + nx, s);
   if (st == MLG_OK) {
-    cudaMemcpyAsync(xR, dx, sizeof(float) * nx, cudaMemcpyDeviceToHost, s);
-    cudaMemcpyAsync(xI, dx + nx, sizeof(float) * nx, cudaMemcpyDeviceToHost, s);
-    if (cudaStreamSynchronize(s) != cudaSuccess) st = fail(MLG_ERR_CUDA, "nakatsha failed: %s",
-                                                           cudaGetErrorString(cudaGetLastError()));
+    cudaMemcpyAsync(xR, dx.p, sizeof(float) * nx, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(xI, dx.p + nx, sizeof(float) * nx, cudaMemcpyDeviceToHost, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess)
+      st = fail(MLG_ERR_CUDA, "nakatsha failed: %s", cudaGetErrorString(cudaGetLastError()));
   }
+  dx.reset();
+  dy.reset();
+  x2.reset();
+  y2.reset();
   cudaStreamSynchronize(s);
-  cudaFree(dx);
-  cudaFree(dy);
-  cudaFree(x2);
-  cudaFree(y2);
   plan_free(p);
   mlg_matrix_destroy(G);
   return st;

@@ -2,31 +2,34 @@
 // (mlg_solver.cu) translation units.
 #pragma once
 
+#include "mlg_fft.cuh"
 #include "mlg_internal.cuh"
 
 struct mlg_plan_s {
   int device = 0;
   int imDim = 3;
-  int N[3] = {1, 1, 1};  // grid (N_u)
-  int n[3] = {1, 1, 1};  // image (n_u)
+  int N[3] = {1, 1, 1};    // grid (N_u)
+  int n[3] = {1, 1, 1};    // image (n_u)
+  int off[3] = {0, 0, 0};  // N/2 - n/2: where the image block sits in the grid
   int nCh = 1;
   long long Nu_tot = 1, nu_tot = 1;
-  int nPt = 0;           // rows of Gu
-  // fftshift as modulation: the forward/inverse centred DFT equals
-  // (-1)^k * c * DFT((-1)^n x) with c = prod_d (-1)^(N_d/2)
+  int nPt = 0;             // rows of Gu
+  // fftshift as modulation: the centred DFT equals (-1)^k * c * DFT((-1)^n x)
+  // with c = prod_d (-1)^(N_d/2)
   float shift_const = 1.0f;
   const mlg::Csr* Gu = nullptr;   // caller's matrices
   const mlg::Csr* Gut = nullptr;
   mlg::Csr Gu_s;                  // values x (-1)^(col cell) x shift_const
   mlg::Csr Gut_s;                 // values x (-1)^(row cell)
-  float2* KFC = nullptr;          // [nCh][nu]
-  float2* KFCc = nullptr;         // [nCh][nu]
-  float2* grid = nullptr;         // [nCh][Nu]
+  float2* KFC = nullptr;          // [nu][nCh]
+  float2* KFCc = nullptr;         // [nu][nCh]
+  float2* grid = nullptr;         // [Nu][nCh] (coil fastest)
+  float2* bufA = nullptr;         // [n_z][n_y][N_x][nCh]
+  float2* bufB = nullptr;         // [n_z][N_y][N_x][nCh]
+  mlg::FftAxisPlan ax[3];
   double* partial = nullptr;      // FP64 partial sums (CTA results)
   int partial_cap = 0;
   double* scalars = nullptr;      // solver scalars (device)
-  cufftHandle fft = 0;
-  bool fft_ready = false;
   cudaStream_t stream = nullptr;  // internal non-blocking stream
   cudaEvent_t ev_in = nullptr, ev_out = nullptr;
   size_t bytes = 0;
@@ -39,23 +42,22 @@ struct mlg_plan_s {
   // captured inner CG step (replayed nCGD-1 times per outer iteration)
   cudaGraphExec_t cg_graph = nullptr;
   const void* cg_graph_x = nullptr;  // solution buffer baked into the graph
-  const void* cg_graph_y = nullptr;
   long long cg_graph_kernels = 0;
 };
 
 namespace mlg {
 
+// stages of the two operators (stage timing helper uses them one by one)
+constexpr int kShannaStages = 4;    // x, y, z passes, Gu
+constexpr int kNakatshaStages = 4;  // Gut, z, y, x passes
+int shanna_stage(mlg_plan_s* p, int stage, const float2* x, bool x_per_coil, float2* y, const float* sqn_w,
+                 double* partial, int* n_partial, cudaStream_t s);
+int nakatsha_stage(mlg_plan_s* p, int stage, const float2* y, const float* HY, float scale, float2* x,
+                   double* partial, int* n_partial, cudaStream_t s);
 int shanna_run(mlg_plan_s* p, const float2* x, bool x_per_coil, float2* y, const float* sqn_w, double* partial,
                int* n_partial, cudaStream_t s);
 int nakatsha_run(mlg_plan_s* p, const float2* y, const float* HY, float scale, float2* x, double* partial,
                  int* n_partial, cudaStream_t s);
-// stages of the two operators
-int shanna_pre(mlg_plan_s* p, const float2* x, bool x_per_coil, cudaStream_t s);
-int fft_exec(mlg_plan_s* p, bool forward, cudaStream_t s);
-int shanna_spmm(mlg_plan_s* p, float2* y, const float* sqn_w, double* partial, int* n_partial, cudaStream_t s);
-int nakatsha_spmm(mlg_plan_s* p, const float2* y, const float* HY, cudaStream_t s);
-int nakatsha_post(mlg_plan_s* p, float scale, float2* x, double* partial, int* n_partial, cudaStream_t s);
-int post_partial_count(const mlg_plan_s* p);
 int sensa_run(mlg_plan_s* p, const float2* y, const float* ve, float ve_max, int nIter, int nCGD, float2* x,
               double* residual, bool use_graph, cudaStream_t s);
 

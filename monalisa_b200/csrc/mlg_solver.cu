@@ -62,17 +62,19 @@ __global__ void hy_kernel(const float* __restrict__ ve, int n, float ve_max, flo
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) HY[i] = fminf(ve[i], ve_max);
 }
 
+// max over v[0..n): each CTA reduces a grid-stride slice into out[blockIdx.x];
+// run once with many CTAs, then once with one CTA over those partials
 __global__ void max_kernel(const float* __restrict__ v, int n, float* out) {
   __shared__ float sh[kT];
   float m = -FLT_MAX;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) m = fmaxf(m, v[i]);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) m = fmaxf(m, v[i]);
   sh[threadIdx.x] = m;
   __syncthreads();
   for (int w = blockDim.x / 2; w > 0; w >>= 1) {
     if ((int)threadIdx.x < w) sh[threadIdx.x] = fmaxf(sh[threadIdx.x], sh[threadIdx.x + w]);
     __syncthreads();
   }
-  if (threadIdx.x == 0) out[0] = sh[0];
+  if (threadIdx.x == 0) out[blockIdx.x] = sh[0];
 }
 
 // res = y - Mx (k-space), optional partials of sum HY |res|^2
@@ -222,7 +224,10 @@ int sensa_run(mlg_plan_s* p, const float2* y, const float* ve, float ve_max, int
   float vmax = ve_max;
   if (!(vmax > 0.f)) {
     float* dmax = (float*)(p->scalars + S_COUNT);
-    max_kernel<<<1, kT, 0, s>>>(ve, p->nPt, dmax);
+    float* dpart = (float*)p->partial;  // >= 128 doubles of room
+    max_kernel<<<128, kT, 0, s>>>(ve, p->nPt, dpart);
+    MLG_LAUNCHED();
+    max_kernel<<<1, kT, 0, s>>>(dpart, 128, dmax);
     MLG_LAUNCHED();
     MLG_CUDA(cudaMemcpyAsync(&vmax, dmax, sizeof(float), cudaMemcpyDeviceToHost, s));
     MLG_CUDA(cudaStreamSynchronize(s));
@@ -231,7 +236,11 @@ int sensa_run(mlg_plan_s* p, const float2* y, const float* ve, float ve_max, int
   MLG_LAUNCHED();
 
   const int full = std::max(0, nCGD - 1);  // inner steps that run to p_next
-  if (use_graph && full > 0 && (!p->cg_graph || p->cg_graph_x != x)) {
+  // Captured once per solution buffer, after the first init phase has run
+  // every kernel of the step at least once (first launches set kernel
+  // attributes, which must not happen during capture).
+  auto ensure_graph = [&]() -> int {
+    if (!use_graph || full == 0 || (p->cg_graph && p->cg_graph_x == x)) return MLG_OK;
     if (p->cg_graph) cudaGraphExecDestroy(p->cg_graph);
     p->cg_graph = nullptr;
     cudaGraph_t graph;
@@ -247,7 +256,8 @@ int sensa_run(mlg_plan_s* p, const float2* y, const float* ve, float ve_max, int
     cudaGraphDestroy(graph);
     if (ie != cudaSuccess) return fail(MLG_ERR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(ie));
     p->cg_graph_x = x;
-  }
+    return MLG_OK;
+  };
 
   DevBuf<double> hist;
   MLG_TRY(hist.alloc(std::max(1, nIter), s));
@@ -261,6 +271,7 @@ int sensa_run(mlg_plan_s* p, const float2* y, const float* ve, float ve_max, int
     cg_init_kernel<<<1, kT, 0, s>>>(p->partial, np, HX, eps, p->scalars);
     MLG_LAUNCHED();
     MLG_CUDA(cudaMemcpyAsync(p->x_p, p->x_dagM, sizeof(float2) * (size_t)p->nu_tot, cudaMemcpyDeviceToDevice, s));
+    if (full > 0) MLG_TRY(ensure_graph());
     for (int i = 0; i < full; ++i) {
       if (use_graph) {
         MLG_CUDA(cudaGraphLaunch(p->cg_graph, s));
@@ -354,24 +365,6 @@ int mlg_sensa(mlg_plan_t p, const float* yR, const float* yI, const float* ve, f
 }  // extern "C"
 
 // ---- stage timing -------------------------------------------------------------
-namespace mlg {
-namespace {
-
-struct Timer {
-  cudaEvent_t a = nullptr, b = nullptr;
-  Timer() {
-    cudaEventCreate(&a);
-    cudaEventCreate(&b);
-  }
-  ~Timer() {
-    cudaEventDestroy(a);
-    cudaEventDestroy(b);
-  }
-};
-
-}  // namespace
-}  // namespace mlg
-
 extern "C" int mlg_plan_profile(mlg_plan_t p, int iters, double* ms) {
   using namespace mlg;
   MLG_CHECK(p && ms && iters >= 1, "invalid argument");
@@ -382,37 +375,30 @@ extern "C" int mlg_plan_profile(mlg_plan_t p, int iters, double* ms) {
   const long long nk = (long long)p->nPt * p->nCh;
   MLG_CUDA(cudaMemsetAsync(p->x_p, 0, sizeof(float2) * (size_t)p->nu_tot, s));
   MLG_CUDA(cudaMemsetAsync(p->k_res, 0, sizeof(float2) * (size_t)nk, s));
-  Timer t[6];
-  double acc[6] = {0, 0, 0, 0, 0, 0};
-  for (int it = 0; it <= iters; ++it) {
-    // Shanna stages
-    cudaEventRecord(t[0].a, s);
-    MLG_TRY(shanna_pre(p, p->x_p, false, s));
-    cudaEventRecord(t[0].b, s);
-    cudaEventRecord(t[1].a, s);
-    MLG_TRY(fft_exec(p, true, s));
-    cudaEventRecord(t[1].b, s);
-    cudaEventRecord(t[2].a, s);
-    MLG_TRY(shanna_spmm(p, p->k_Mp, nullptr, nullptr, nullptr, s));
-    cudaEventRecord(t[2].b, s);
-    // Nakatsha stages
-    cudaEventRecord(t[3].a, s);
-    MLG_TRY(nakatsha_spmm(p, p->k_res, nullptr, s));
-    cudaEventRecord(t[3].b, s);
-    cudaEventRecord(t[4].a, s);
-    MLG_TRY(fft_exec(p, false, s));
-    cudaEventRecord(t[4].b, s);
-    cudaEventRecord(t[5].a, s);
-    MLG_TRY(nakatsha_post(p, 1.0f, p->x_dagM, nullptr, nullptr, s));
-    cudaEventRecord(t[5].b, s);
-    MLG_CUDA(cudaStreamSynchronize(s));
-    if (it == 0) continue;  // warm-up
-    for (int k = 0; k < 6; ++k) {
+  constexpr int S = kShannaStages + kNakatshaStages;
+  cudaEvent_t ev[S + 1];
+  for (int k = 0; k <= S; ++k) MLG_CUDA(cudaEventCreate(&ev[k]));
+  double acc[S] = {0};
+  int st = MLG_OK;
+  for (int it = 0; it <= iters && st == MLG_OK; ++it) {
+    cudaEventRecord(ev[0], s);
+    for (int k = 0; k < kShannaStages && st == MLG_OK; ++k) {
+      st = shanna_stage(p, k, p->x_p, false, p->k_Mp, nullptr, nullptr, nullptr, s);
+      cudaEventRecord(ev[k + 1], s);
+    }
+    for (int k = 0; k < kNakatshaStages && st == MLG_OK; ++k) {
+      st = nakatsha_stage(p, k, p->k_res, nullptr, 1.0f, p->x_dagM, nullptr, nullptr, s);
+      cudaEventRecord(ev[kShannaStages + k + 1], s);
+    }
+    if (cudaStreamSynchronize(s) != cudaSuccess) st = fail(MLG_ERR_CUDA, "profile run failed");
+    if (it == 0 || st != MLG_OK) continue;  // first run is the warm-up
+    for (int k = 0; k < S; ++k) {
       float v = 0.f;
-      cudaEventElapsedTime(&v, t[k].a, t[k].b);
+      cudaEventElapsedTime(&v, ev[k], ev[k + 1]);
       acc[k] += v;
     }
   }
-  for (int k = 0; k < 6; ++k) ms[k] = acc[k] / iters;
-  return MLG_OK;
+  for (int k = 0; k <= S; ++k) cudaEventDestroy(ev[k]);
+  for (int k = 0; k < S; ++k) ms[k] = acc[k] / iters;
+  return st;
 }
