@@ -103,13 +103,18 @@ def _dist():
     return ws, rank, local
 
 
+# profile order of mlg_plan_profile: forward x/y/z passes, Gu, the Gut product
+# (all rows, non-empty rows, or only the long rows, by adjoint strategy),
+# inverse z pass (reading the grid, the occupancy-masked grid, or gathering
+# the Gut rows itself), inverse y, inverse x (fused coil sum)
 STAGES = ["fwd_x", "fwd_y", "fwd_z", "gu", "gut", "inv_z", "inv_y", "inv_x"]
 
 
-def algorithmic_bytes(w, Gu, Gut, nCh):
+def algorithmic_bytes(w, Gu, Gut, nCh, adjoint):
     """Bytes each stage must move at least, for one operator application
     (forward passes read the non-zero part only and write what the next pass
-    needs; the inverse passes keep only the cropped lines)."""
+    needs; the inverse passes keep only the cropped lines).  The Gut / inverse
+    z split depends on the adjoint strategy the plan runs."""
     nnz = Gu.nnz
     nPt = Gu.l_size
     N0, N1, N2 = (int(v) for v in w.N_u)
@@ -118,12 +123,19 @@ def algorithmic_bytes(w, Gu, Gut, nCh):
     A = N0 * n1 * n2 * nCh * 8
     B = N0 * N1 * n2 * nCh * 8
     G = Nu * nCh * 8
-    touched, _ = Gut.row_stats()
+    touched, n_long = Gut.row_stats()
+    T = touched * nCh * 8  # the non-empty grid cells
+    ysrc = nnz * 8 + nPt * nCh * 8 + 4 * nPt  # entries, k-space rows, their weights once
+    if adjoint == "masked":
+        gut, inv_z = ysrc + 12 * touched + T, T + Nu // 8 + B
+    elif adjoint == "fused":
+        gut, inv_z = n_long * nCh * 8, ysrc + 4 * (Nu + 1) + B
+    else:
+        gut, inv_z = ysrc + 4 * (Nu + 1) + G, G + B
     return {
         "fwd_x": nu * 8 + nu * nCh * 8 + A, "fwd_y": A + B, "fwd_z": B + G,
-        "gu": nnz * 8 + 4 * (nPt + 1) + touched * nCh * 8 + nPt * nCh * 8,
-        "gut": nnz * 8 + 4 * (Nu + 1) + nPt * nCh * 8 + 4 * nPt + G,
-        "inv_z": G + B, "inv_y": B + A, "inv_x": A + nu * nCh * 8 + nu * 8,
+        "gu": nnz * 8 + 4 * (nPt + 1) + T + nPt * nCh * 8,
+        "gut": gut, "inv_z": inv_z, "inv_y": B + A, "inv_x": A + nu * nCh * 8 + nu * 8,
     }
 
 
@@ -142,7 +154,7 @@ def run_gpu(args):
     t0 = time.time()
     w = koosh3d()
     Gu, Gut = mb.bmTraj2SparseMat(w.t, w.ve, w.N_u, w.dK_u, w.kernelType, w.nWin, w.kernelParam)
-    rec = mb.SensaRecon(Gu, Gut, w.C, w.n_u)
+    rec = mb.SensaRecon(Gu, Gut, w.C, w.n_u, autotune=True)
     dev = torch.device("cuda", local)
     x_true = torch.from_numpy(w.x_true).to(dev)
     y = rec.plan.shanna(x_true)
@@ -230,7 +242,7 @@ def run_gpu(args):
     # plan's stream) -> roofline of the dominant kernel of this library
     st = np.zeros(len(STAGES))
     N.call("mlg_plan_profile", rec.plan.handle, 5, N.dptr(st))
-    B = algorithmic_bytes(w, Gu, Gut, w.nCh)
+    B = algorithmic_bytes(w, Gu, Gut, w.nCh, rec.plan.adjoint_mode)
     peak, peak_kind = _peaks()
     stages = {}
     for i, nm in enumerate(STAGES):
@@ -261,6 +273,7 @@ def run_gpu(args):
                    "l2": "working set (2.1 GB grid) larger than L2 each step", **w.info},
         "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
         "recon_rel_err_vs_phantom": round(err, 5), "setup_s": round(setup_s, 2),
+        "autotune": {"adjoint": rec.plan.adjoint_mode, "ms": {k: round(v, 4) for k, v in rec.tuning.items()}},
     }
     if rank == 0:
         print(json.dumps(out), flush=True)

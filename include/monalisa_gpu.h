@@ -216,6 +216,24 @@ int mlg_nakatsha(int imDim, const int* N_u, const int* n_u, int nCh,
 int mlg_idf(int imDim, const int* N_u, const float* dK_u, int nCol,
             const float* xR, const float* xI, float* yR, float* yI);
 
+/* How the adjoint (Nakatsha) feeds its first inverse FFT pass with the Gut
+ * product: MLG_ADJ_FULL_GRID writes every grid cell and streams the grid;
+ * MLG_ADJ_FUSED gathers the Gut rows inside the pass (2-D/3-D);
+ * MLG_ADJ_MASKED writes only the non-empty Gut rows and reads a cell only if
+ * its occupancy bit is set (even nCh).  All give the same values up to
+ * floating-point summation order of the long rows.  Tuning API; no reference
+ * counterpart. */
+#define MLG_ADJ_FULL_GRID 0
+#define MLG_ADJ_FUSED 1
+#define MLG_ADJ_MASKED 2
+int mlg_plan_set_adjoint(mlg_plan_t p, int mode);
+int mlg_plan_get_adjoint(mlg_plan_t p, int* mode);
+/* Autotuner: times every valid adjoint strategy on the plan's own matrices
+ * (`reps` runs each after a warm-up, CUDA events on the plan's stream) and
+ * keeps the fastest.  ms (may be NULL) receives 3 times in milliseconds,
+ * negative for strategies the plan cannot run. */
+int mlg_plan_autotune(mlg_plan_t p, int reps, double* ms);
+
 /* Times the stages of one Shanna and one Nakatsha on the plan's stream with
  * CUDA events, averaged over `iters` repetitions after one warm-up:
  * ms[0..2] forward x, y, z FFT passes (x pass fused with x .* KFC),

@@ -82,7 +82,113 @@ void csr_free(Csr& c) {
   cudaFree(c.col);
   cudaFree(c.val);
   cudaFree(c.long_rows);
+  cudaFree(c.seg_lo);
+  cudaFree(c.seg_hi);
+  cudaFree(c.long_seg0);
+  cudaFree(c.nz_rows);
+  cudaFree(c.nz_mask);
   c = Csr();
+}
+
+// bit r set <=> row r non-empty; one thread per 32-row word
+__global__ void nz_mask_kernel(const uint32_t* __restrict__ row_ptr, int l_size, uint32_t* __restrict__ mask,
+                               int* __restrict__ word_count) {
+  const int nw = (l_size + 31) / 32;
+  for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < nw; w += gridDim.x * blockDim.x) {
+    uint32_t m = 0;
+    for (int b = 0; b < 32; ++b) {
+      const long long r = (long long)w * 32 + b;
+      if (r < l_size && row_ptr[r + 1] > row_ptr[r]) m |= 1u << b;
+    }
+    mask[w] = m;
+    word_count[w] = __popc(m);
+  }
+}
+
+__global__ void nz_rows_kernel(const uint32_t* __restrict__ mask, const int* __restrict__ word_off, int nw,
+                               int* __restrict__ rows) {
+  for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < nw; w += gridDim.x * blockDim.x) {
+    uint32_t m = mask[w];
+    int o = word_off[w];
+    while (m) {
+      const int b = __ffs(m) - 1;
+      rows[o++] = w * 32 + b;
+      m &= m - 1;
+    }
+  }
+}
+
+int csr_build_nonempty(Csr& c, cudaStream_t s) {
+  if (c.nz_mask) return MLG_OK;
+  const int nw = (c.l_size + 31) / 32;
+  int *cnt = nullptr, *off = nullptr;
+  MLG_CUDA(cudaMalloc(&c.nz_mask, sizeof(uint32_t) * (size_t)std::max(1, nw)));
+  MLG_CUDA(cudaMalloc(&cnt, sizeof(int) * (size_t)(nw + 1)));
+  MLG_CUDA(cudaMalloc(&off, sizeof(int) * (size_t)(nw + 1)));
+  const int g = std::max(1, std::min(4096, (nw + 255) / 256));
+  nz_mask_kernel<<<g, 256, 0, s>>>(c.row_ptr, c.l_size, c.nz_mask, cnt);
+  count_launch();
+  // exclusive scan of the word counts on the host (nw is small: l_size/32)
+  std::vector<int> h(nw + 1, 0);
+  MLG_CUDA(cudaMemcpyAsync(h.data(), cnt, sizeof(int) * nw, cudaMemcpyDeviceToHost, s));
+  MLG_CUDA(cudaStreamSynchronize(s));
+  int run = 0;
+  for (int w = 0; w < nw; ++w) {
+    const int v = h[w];
+    h[w] = run;
+    run += v;
+  }
+  h[nw] = run;
+  c.n_nonempty = run;
+  MLG_CUDA(cudaMemcpyAsync(off, h.data(), sizeof(int) * (nw + 1), cudaMemcpyHostToDevice, s));
+  MLG_CUDA(cudaMalloc(&c.nz_rows, sizeof(int) * (size_t)std::max(1, run)));
+  nz_rows_kernel<<<g, 256, 0, s>>>(c.nz_mask, off, nw, c.nz_rows);
+  count_launch();
+  MLG_CUDA(cudaStreamSynchronize(s));
+  cudaFree(cnt);
+  cudaFree(off);
+  return MLG_OK;
+}
+
+__global__ void long_bounds_kernel(const uint32_t* __restrict__ row_ptr, const int* __restrict__ rows, int n,
+                                   uint32_t* __restrict__ out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    out[2 * i] = row_ptr[rows[i]];
+    out[2 * i + 1] = row_ptr[rows[i] + 1];
+  }
+}
+
+int csr_build_segments(Csr& c, cudaStream_t s) {
+  c.n_seg = 0;
+  if (c.n_long == 0) return MLG_OK;
+  uint32_t* d_b = nullptr;
+  MLG_CUDA(cudaMalloc(&d_b, sizeof(uint32_t) * 2 * (size_t)c.n_long));
+  long_bounds_kernel<<<(c.n_long + 255) / 256, 256, 0, s>>>(c.row_ptr, c.long_rows, c.n_long, d_b);
+  count_launch();
+  std::vector<uint32_t> b(2 * (size_t)c.n_long);
+  cudaError_t e = cudaMemcpyAsync(b.data(), d_b, sizeof(uint32_t) * b.size(), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  cudaFree(d_b);
+  if (e != cudaSuccess) return fail(MLG_ERR_CUDA, "segment bounds: %s", cudaGetErrorString(e));
+  std::vector<uint32_t> lo, hi;
+  std::vector<int> seg0(c.n_long + 1);
+  for (int j = 0; j < c.n_long; ++j) {
+    seg0[j] = (int)lo.size();
+    for (uint32_t a = b[2 * j]; a < b[2 * j + 1]; a += kSegLen) {
+      lo.push_back(a);
+      hi.push_back(std::min<uint32_t>(a + kSegLen, b[2 * j + 1]));
+    }
+  }
+  seg0[c.n_long] = (int)lo.size();
+  c.n_seg = (int)lo.size();
+  MLG_CUDA(cudaMalloc(&c.seg_lo, sizeof(uint32_t) * lo.size()));
+  MLG_CUDA(cudaMalloc(&c.seg_hi, sizeof(uint32_t) * hi.size()));
+  MLG_CUDA(cudaMalloc(&c.long_seg0, sizeof(int) * seg0.size()));
+  MLG_CUDA(cudaMemcpyAsync(c.seg_lo, lo.data(), sizeof(uint32_t) * lo.size(), cudaMemcpyHostToDevice, s));
+  MLG_CUDA(cudaMemcpyAsync(c.seg_hi, hi.data(), sizeof(uint32_t) * hi.size(), cudaMemcpyHostToDevice, s));
+  MLG_CUDA(cudaMemcpyAsync(c.long_seg0, seg0.data(), sizeof(int) * seg0.size(), cudaMemcpyHostToDevice, s));
+  MLG_CUDA(cudaStreamSynchronize(s));
+  return MLG_OK;
 }
 
 // Decodes the jump format on the host (one pass, 64-bit running indices,
@@ -152,6 +258,13 @@ int csr_from_jump(int r_size, const int* r_jump, const int* r_nJump, const float
     MLG_CUDA(cudaMemcpyAsync(m.long_rows, longs.data(), sizeof(int) * longs.size(), cudaMemcpyHostToDevice, s));
   }
   MLG_CUDA(cudaStreamSynchronize(s));  // host vectors go out of scope
+  {
+    const int st = csr_build_segments(m, s);
+    if (st != MLG_OK) {
+      csr_free(m);
+      return st;
+    }
+  }
   out = m;
   return MLG_OK;
 }

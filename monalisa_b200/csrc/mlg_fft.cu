@@ -22,6 +22,7 @@ namespace mlg {
 
 constexpr int kFftThreads = 256;
 constexpr size_t kFftSmemCap = 100 * 1024;
+constexpr int kGatherBatch = 8;  // cells gathered concurrently per thread (kGutIn)
 
 __device__ __forceinline__ float2 cmulf(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -170,6 +171,11 @@ __device__ __forceinline__ float2 load_elem(const PassDesc& d, const Lines& ln, 
     if ((n + d.coord_off[1] + ui + d.coord_off[2] + ln.vi) & 1) v = make_float2(-v.x, -v.y);
     return v;
   } else {
+    if (d.in_mask) {
+      const long long cell = (long long)ui * d.cell_stride[ln.u] + (long long)ln.vi * d.cell_stride[ln.v] +
+                             (long long)n * d.cell_stride[d.ax];
+      if (!((__ldg(d.in_mask + (cell >> 5)) >> (cell & 31)) & 1u)) return make_float2(0.f, 0.f);
+    }
     const long long off = (long long)(n - d.in_lo) * d.in_stride[d.ax] + (long long)ui * d.in_stride[ln.u] +
                           (long long)ln.vi * d.in_stride[ln.v] + c;
     return __ldg(d.in + off);
@@ -260,6 +266,80 @@ __device__ __forceinline__ void smem_fft(float2* s, int cols, int rN1, int rN2, 
   __syncthreads();
 }
 
+// kGutIn load: each thread owns V adjacent coils (V = 2: 16-byte loads) of
+// one line and walks the line's cells with a stride; four cells are
+// gathered at a time so four dependency chains (row pointer -> entry ->
+// k-space row) are in flight per thread.  Per cell the entries are summed in
+// stored order with round-to-nearest multiply/add, as the SpMM kernels do.
+template <int V>
+__device__ __forceinline__ void gut_load(const PassDesc& d, const Lines& ln, float2* s, int N, int cols) {
+  using VT = typename std::conditional<V == 2, float4, float2>::type;
+  const int C = d.C;
+  const int cv = cols / V;
+  const int vc = threadIdx.x % cv, rstep = blockDim.x / cv;
+  const int col0 = vc * V, l = col0 / C, c = col0 - l * C;
+  const int ui = ln.u0 + l;
+  const bool line_ok = ui < d.dims[ln.u];
+  const long long cell_base = (long long)ui * d.cell_stride[ln.u] + (long long)ln.vi * d.cell_stride[ln.v];
+  const long long cst = d.cell_stride[d.ax];
+  VT* sv = reinterpret_cast<VT*>(s);
+  constexpr int B = kGatherBatch;
+  for (int n0 = threadIdx.x / cv; n0 < N; n0 += B * rstep) {
+    uint32_t b[B], len[B];
+    float acc[B][2 * V];
+#pragma unroll
+    for (int j = 0; j < B; ++j) {
+      const int n = n0 + j * rstep;
+      b[j] = len[j] = 0;
+#pragma unroll
+      for (int q = 0; q < 2 * V; ++q) acc[j][q] = 0.f;
+      if (line_ok && n < N) {
+        const long long cell = cell_base + (long long)n * cst;
+        b[j] = __ldg(d.g_rowptr + cell);
+        len[j] = __ldg(d.g_rowptr + cell + 1) - b[j];
+        if (len[j] > (uint32_t)kLongRow) {  // precomputed by the long-row kernel
+          const float* gl = reinterpret_cast<const float*>(d.g_long + cell * C + c);
+#pragma unroll
+          for (int q = 0; q < 2 * V; ++q) acc[j][q] = gl[q];
+          len[j] = 0;
+        }
+      }
+    }
+    uint32_t maxlen = 0;
+#pragma unroll
+    for (int j = 0; j < B; ++j) maxlen = max(maxlen, len[j]);
+    for (uint32_t t = 0; t < maxlen; ++t) {
+#pragma unroll
+      for (int j = 0; j < B; ++j) {
+        if (t < len[j]) {
+          const uint32_t k = b[j] + t;
+          const int jc = __ldg(d.g_col + k);
+          const float m = __ldg(d.g_val + k);
+          const float h = d.g_hy ? __ldg(d.g_hy + jc) : 1.0f;
+          const VT yv = *reinterpret_cast<const VT*>(d.g_y + (long long)jc * C + c);
+          const float* yf = reinterpret_cast<const float*>(&yv);
+#pragma unroll
+          for (int q = 0; q < 2 * V; ++q) {
+            const float hv = d.g_hy ? __fmul_rn(h, yf[q]) : yf[q];
+            acc[j][q] = __fadd_rn(acc[j][q], __fmul_rn(m, hv));
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < B; ++j) {
+      const int n = n0 + j * rstep;
+      if (n < N) {
+        VT o;
+        float* of = reinterpret_cast<float*>(&o);
+#pragma unroll
+        for (int q = 0; q < 2 * V; ++q) of[q] = acc[j][q];
+        sv[n * cv + vc] = o;
+      }
+    }
+  }
+}
+
 template <int N1, int N2, int DIR, PassMode MODE>
 __global__ void __launch_bounds__(kFftThreads) fft_pass_kernel(PassDesc d, int L, int rN1, int rN2,
                                                                const float2* __restrict__ tw) {
@@ -271,7 +351,40 @@ __global__ void __launch_bounds__(kFftThreads) fft_pass_kernel(PassDesc d, int L
   const Lines ln = lines_of(d, L);
   // load (zero-filled outside the stored input range)
   const int cv = cols >> 1;  // coil pairs when C is even: 16-byte accesses
-  if ((C & 1) == 0 && (int)blockDim.x % cv == 0) {
+  if constexpr (MODE == PassMode::kGutIn) {
+    if ((C & 1) == 0 && (int)blockDim.x % cv == 0) {
+      gut_load<2>(d, ln, s, N, cols);
+    } else if ((int)blockDim.x % cols == 0) {
+      gut_load<1>(d, ln, s, N, cols);
+    } else {
+      for (int it = threadIdx.x; it < N * cols; it += blockDim.x) {
+        const int n = it / cols, col = it - (it / cols) * cols;
+        const int l = col / C, c = col - (col / C) * C;
+        const int ui = ln.u0 + l;
+        float2 a = make_float2(0.f, 0.f);
+        if (ui < d.dims[ln.u]) {
+          const long long cell = (long long)ui * d.cell_stride[ln.u] + (long long)ln.vi * d.cell_stride[ln.v] +
+                                 (long long)n * d.cell_stride[d.ax];
+          const uint32_t b = __ldg(d.g_rowptr + cell), e = __ldg(d.g_rowptr + cell + 1);
+          if (e - b > (uint32_t)kLongRow) {
+            a = d.g_long[cell * C + c];
+          } else {
+            for (uint32_t k = b; k < e; ++k) {
+              const int jc = __ldg(d.g_col + k);
+              const float m = __ldg(d.g_val + k);
+              float2 v = __ldg(d.g_y + (long long)jc * C + c);
+              if (d.g_hy) {
+                const float h = __ldg(d.g_hy + jc);
+                v = make_float2(__fmul_rn(h, v.x), __fmul_rn(h, v.y));
+              }
+              a = make_float2(__fadd_rn(a.x, __fmul_rn(m, v.x)), __fadd_rn(a.y, __fmul_rn(m, v.y)));
+            }
+          }
+        }
+        s[n * cols + col] = a;
+      }
+    }
+  } else if ((C & 1) == 0 && (int)blockDim.x % cv == 0) {
     // fixed coil pair per thread, rows strided: no divisions in the loop and
     // several independent 16-byte loads in flight per thread
     const int vc = threadIdx.x % cv, rstep = blockDim.x / cv;
@@ -308,11 +421,18 @@ __global__ void __launch_bounds__(kFftThreads) fft_pass_kernel(PassDesc d, int L
     } else {
       const float2* base = d.in + (long long)ui * d.in_stride[ln.u] + (long long)ln.vi * d.in_stride[ln.v] + c;
       const long long st = d.in_stride[d.ax];
+      const uint32_t* mask = d.in_mask;
+      const long long cell0 = (long long)ui * d.cell_stride[ln.u] + (long long)ln.vi * d.cell_stride[ln.v];
+      const long long cst = d.cell_stride[d.ax];
 #pragma unroll 4
       for (int n = threadIdx.x / cv; n < N; n += rstep) {
         float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (line_ok && n >= d.in_lo && n < d.in_lo + d.in_len)
-          v = __ldg(reinterpret_cast<const float4*>(base + (long long)(n - d.in_lo) * st));
+        bool ld = line_ok && n >= d.in_lo && n < d.in_lo + d.in_len;
+        if (ld && mask) {
+          const long long cell = cell0 + (long long)n * cst;
+          ld = (__ldg(mask + (cell >> 5)) >> (cell & 31)) & 1u;
+        }
+        if (ld) v = __ldg(reinterpret_cast<const float4*>(base + (long long)(n - d.in_lo) * st));
         s4[n * cv + vc] = v;
       }
     }
@@ -436,16 +556,23 @@ void fft_axis_free(FftAxisPlan& a) {
   a = FftAxisPlan();
 }
 
-static int lines_per_cta(const FftAxisPlan& a, int C) {
-  int L = std::max(1, (32 + C - 1) / C);
+// Lines per CTA: 32 columns (256-byte row segments) for streaming passes; the
+// gathering pass uses 16 columns so that twice as many CTAs (and gathers)
+// are resident per SM.
+static int lines_per_cta(const FftAxisPlan& a, int C, PassMode mode) {
+  const int target = mode == PassMode::kGutIn ? 16 : 32;
+  int L = std::max(1, (target + C - 1) / C);
   while (L > 1 && (size_t)a.N * L * C * sizeof(float2) > kFftSmemCap) --L;
   return L;
 }
 
-int fft_pass_blocks(const FftAxisPlan& a, const PassDesc& d) {
-  const int L = lines_per_cta(a, d.C);
+static int blocks_for(const PassDesc& d, int L) {
   const int u = d.ax == 0 ? 1 : 0, v = d.ax == 2 ? 1 : 2;
   return ((d.dims[u] + L - 1) / L) * d.dims[v];
+}
+
+int fft_pass_blocks(const FftAxisPlan& a, const PassDesc& d) {
+  return blocks_for(d, lines_per_cta(a, d.C, PassMode::kNakatshaOut));
 }
 
 template <int N1, int N2, int DIR, PassMode MODE>
@@ -457,7 +584,7 @@ static int launch_pass(const FftAxisPlan& a, const PassDesc& d, int L, cudaStrea
                                   (int)(200 * 1024)));
     attr = true;
   }
-  fft_pass_kernel<N1, N2, DIR, MODE><<<fft_pass_blocks(a, d), kFftThreads, smem, s>>>(d, L, a.N1, a.N2, a.tw);
+  fft_pass_kernel<N1, N2, DIR, MODE><<<blocks_for(d, L), kFftThreads, smem, s>>>(d, L, a.N1, a.N2, a.tw);
   MLG_LAUNCHED();
   return MLG_OK;
 }
@@ -482,10 +609,10 @@ static int dispatch_size(const FftAxisPlan& a, const PassDesc& d, int L, cudaStr
 int fft_pass(const FftAxisPlan& a, PassMode mode, const PassDesc& d, int* n_partial, cudaStream_t s) {
   MLG_CHECK(a.N >= 1 && a.tw, "FFT axis not initialised");
   MLG_CHECK(d.C >= 1, "C must be >= 1");
-  const int L = lines_per_cta(a, d.C);
+  const int L = lines_per_cta(a, d.C, mode);
   MLG_CHECK((size_t)a.N * L * d.C * sizeof(float2) <= 200 * 1024,
             "FFT line of %d points x %d coils exceeds shared memory", a.N, d.C);
-  if (n_partial) *n_partial = mode == PassMode::kNakatshaOut && d.partial ? fft_pass_blocks(a, d) : 0;
+  if (n_partial) *n_partial = mode == PassMode::kNakatshaOut && d.partial ? blocks_for(d, L) : 0;
   switch (mode) {
     case PassMode::kShannaIn:
       MLG_CHECK(d.ax == 0 && d.dir < 0, "kShannaIn is a forward x pass");
@@ -493,6 +620,9 @@ int fft_pass(const FftAxisPlan& a, PassMode mode, const PassDesc& d, int* n_part
     case PassMode::kNakatshaOut:
       MLG_CHECK(d.ax == 0 && d.dir > 0, "kNakatshaOut is an inverse x pass");
       return dispatch_size<1, PassMode::kNakatshaOut>(a, d, L, s);
+    case PassMode::kGutIn:
+      MLG_CHECK(d.dir > 0 && d.g_rowptr && d.g_y, "kGutIn is an inverse pass over Gut");
+      return dispatch_size<1, PassMode::kGutIn>(a, d, L, s);
     default:
       return d.dir < 0 ? dispatch_size<-1, PassMode::kPlain>(a, d, L, s)
                        : dispatch_size<1, PassMode::kPlain>(a, d, L, s);

@@ -17,6 +17,7 @@ enum class PassMode : int {
   kPlain = 0,        // zero-filled load, cropped store
   kShannaIn = 1,     // load x .* KFC .* (-1)^(x+y+z) from the image (axis x)
   kNakatshaOut = 2,  // store sum_c s .* KFC_conj (coil sum) into the image (axis x)
+  kGutIn = 3,        // load grid cells as Gut rows gathered from k-space (first inverse pass)
 };
 
 struct FftAxisPlan {
@@ -43,6 +44,20 @@ struct PassDesc {
   int coord_off[3] = {0, 0, 0};   // full-grid coordinate of line-grid index 0 (sign)
   float sfac = 1.0f;              // kNakatshaOut scale (sign applied per element)
   double* partial = nullptr;      // kNakatshaOut: FP64 |x|^2 per CTA
+  // kGutIn: cell (u, v, n) of the full grid is row u*cs[u] + v*cs[v] + n*cs[ax]
+  // of Gut (rows already carry the (-1)^cell modulation); rows longer than
+  // kLongRow were computed beforehand into g_long ([cell][c], the grid buffer)
+  const uint32_t* g_rowptr = nullptr;
+  const int* g_col = nullptr;
+  const float* g_val = nullptr;
+  const float* g_hy = nullptr;    // row weights of y (NULL = 1)
+  const float2* g_y = nullptr;    // k-space [nPt][C]
+  const float2* g_long = nullptr;
+  long long cell_stride[3] = {0, 0, 0};
+  // kPlain: when set, input cell (u, v, n) (index via cell_stride) is read
+  // only if its bit is set and is zero otherwise (cells a sparse product left
+  // unwritten)
+  const uint32_t* in_mask = nullptr;
 };
 
 int fft_axis_init(int N, FftAxisPlan& a);

@@ -522,6 +522,7 @@ int n2u_build_csr(const float* d_w, const int* d_nJump, int nNb, int nPt, int Nu
   MLG_CUDA(cudaStreamSynchronize(s));
   m.long_rows = list;
   m.n_long = hn;
+  MLG_TRY(csr_build_segments(m, s));
   return MLG_OK;
 }
 

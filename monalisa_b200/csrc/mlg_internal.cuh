@@ -113,9 +113,27 @@ struct Csr {
   int* long_rows = nullptr;     // rows with > kLongRow entries
   int n_long = 0;
   int n_nonempty = 0;
+  // long rows cut into segments of at most kSegLen entries: segment i covers
+  // entries [seg_lo[i], seg_hi[i]); long row j owns segments
+  // [long_seg0[j], long_seg0[j+1])
+  uint32_t* seg_lo = nullptr;
+  uint32_t* seg_hi = nullptr;
+  int* long_seg0 = nullptr;
+  int n_seg = 0;
+  // non-empty rows in ascending order and a bitmask over all rows (bit r of
+  // word r/32 set when row r has entries); built on demand by
+  // csr_build_nonempty
+  int* nz_rows = nullptr;
+  uint32_t* nz_mask = nullptr;
 };
+constexpr int kSegLen = 512;
 
 void csr_free(Csr& c);
+// Builds the segment tables of the long rows (call once the long-row list is
+// on the device).
+int csr_build_segments(Csr& c, cudaStream_t s);
+// Builds nz_rows / nz_mask (idempotent).
+int csr_build_nonempty(Csr& c, cudaStream_t s);
 
 }  // namespace mlg
 
@@ -170,7 +188,19 @@ struct SpmmArgs {
   // NULL = 1): one double per CTA written to partial[], count in *n_partial.
   const float* sqn_row_weight = nullptr;
   double* partial = nullptr;
+  // Only the rows longer than kLongRow (the CTA-split kernel); the others are
+  // left untouched (a fused consumer gathers them itself).
+  bool long_only = false;
+  // Per-segment partial sums of the long rows: >= spmm_scratch_floats()
+  // floats.  NULL: spmm allocates them (not allowed during stream capture).
+  float* seg_scratch = nullptr;
+  // Only the non-empty rows (m->nz_rows, which must exist) are computed and
+  // written; the others are left untouched.
+  bool nonempty_only = false;
 };
+
+// Scratch floats spmm needs for the long-row segments of `m` at nCh coils.
+size_t spmm_scratch_floats(const Csr& m, int nCh);
 
 int spmm(const SpmmArgs& a, cudaStream_t s);
 // Number of FP64 partial sums spmm writes for this matrix / mapping.

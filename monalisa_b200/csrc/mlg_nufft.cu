@@ -96,10 +96,38 @@ static int forward_pass(mlg_plan_s* p, int ax, const float2* x, bool x_per_coil,
   return fft_pass(p->ax[2], PassMode::kPlain, pd, nullptr, s);
 }
 
-// Inverse passes: z (grid -> B), y (B -> A), x (A -> image, coil sum).  The
-// first pass of the transform reads the grid.
-static int inverse_pass(mlg_plan_s* p, int ax, float scale, float2* x, double* partial, int* n_partial,
-                        cudaStream_t s) {
+// Inverse passes: z (grid -> B), y (B -> A), x (A -> image, coil sum).  In 2-D
+// and 3-D the first pass does not read a grid at all: it gathers the Gut rows
+// of its cells from k-space itself (kGutIn), so the adjoint never writes or
+// reads the full grid; only rows longer than kLongRow were computed into the
+// grid buffer beforehand.  In 1-D the first pass is also the last one and
+// reads the grid written by the Gut product.
+enum : int { kAdjFullGrid = 0, kAdjFused = 1, kAdjMasked = 2 };
+
+static bool fused_gut(const mlg_plan_s* p) { return p->adjoint_mode == kAdjFused; }
+
+// adjoint variants a plan can run
+bool adjoint_mode_valid(const mlg_plan_s* p, int mode) {
+  if (mode == kAdjFullGrid) return true;
+  if (mode == kAdjFused) return p->imDim >= 2;
+  if (mode == kAdjMasked) return (p->nCh % 2) == 0 && p->Gut_s.nz_mask != nullptr;
+  return false;
+}
+
+static void set_gut_input(mlg_plan_s* p, PassDesc& pd, const float2* y, const float* HY) {
+  pd.g_rowptr = p->Gut_s.row_ptr;
+  pd.g_col = p->Gut_s.col;
+  pd.g_val = p->Gut_s.val;
+  pd.g_hy = HY;
+  pd.g_y = y;
+  pd.g_long = p->grid;
+  pd.cell_stride[0] = 1;
+  pd.cell_stride[1] = p->N[0];
+  pd.cell_stride[2] = (long long)p->N[0] * p->N[1];
+}
+
+static int inverse_pass(mlg_plan_s* p, int ax, const float2* y, const float* HY, float scale, float2* x,
+                        double* partial, int* n_partial, cudaStream_t s) {
   const int C = p->nCh, d = p->imDim;
   const int* N = p->N;
   const int* n = p->n;
@@ -110,6 +138,15 @@ static int inverse_pass(mlg_plan_s* p, int ax, float scale, float2* x, double* p
   pd.ax = ax;
   pd.dir = 1;
   pd.C = C;
+  const bool gut_in = fused_gut(p) && ax == d - 1;
+  if (gut_in) set_gut_input(p, pd, y, HY);
+  if (p->adjoint_mode == kAdjMasked && ax == d - 1) {
+    pd.in_mask = p->Gut_s.nz_mask;
+    pd.cell_stride[0] = 1;
+    pd.cell_stride[1] = p->N[0];
+    pd.cell_stride[2] = (long long)p->N[0] * p->N[1];
+  }
+  const PassMode plain = gut_in ? PassMode::kGutIn : PassMode::kPlain;
   if (ax == 2) {
     pd.dims[0] = N[0];
     pd.dims[1] = N[1];
@@ -121,7 +158,7 @@ static int inverse_pass(mlg_plan_s* p, int ax, float scale, float2* x, double* p
     box_strides(eB, C, pd.out_stride);
     pd.out_lo = p->off[2];
     pd.out_len = n[2];
-    return fft_pass(p->ax[2], PassMode::kPlain, pd, nullptr, s);
+    return fft_pass(p->ax[2], plain, pd, nullptr, s);
   }
   if (ax == 1) {
     pd.dims[0] = N[0];
@@ -134,7 +171,7 @@ static int inverse_pass(mlg_plan_s* p, int ax, float scale, float2* x, double* p
     box_strides(eA, C, pd.out_stride);
     pd.out_lo = p->off[1];
     pd.out_len = n[1];
-    return fft_pass(p->ax[1], PassMode::kPlain, pd, nullptr, s);
+    return fft_pass(p->ax[1], plain, pd, nullptr, s);
   }
   pd.dims[1] = n[1];
   pd.dims[2] = n[2];
@@ -169,13 +206,20 @@ int shanna_stage(mlg_plan_s* p, int stage, const float2* x, bool x_per_coil, flo
   a.out.rows = p->nPt;
   a.sqn_row_weight = sqn_w;
   a.partial = partial;
+  a.seg_scratch = p->seg_scratch;
   if (n_partial) *n_partial = partial ? spmm_partial_count(a) : 0;
   return spmm(a, s);
 }
 
+// stage 0: the Gut product into the grid buffer -- all rows (kAdjFullGrid),
+// the non-empty rows (kAdjMasked) or only the long rows (kAdjFused, whose
+// first pass gathers the rest itself); stages 1..imDim: inverse passes over
+// the last, ..., first dimension
 int nakatsha_stage(mlg_plan_s* p, int stage, const float2* y, const float* HY, float scale, float2* x,
                    double* partial, int* n_partial, cudaStream_t s) {
   if (stage == 0) {
+    if (fused_gut(p) && p->Gut_s.n_long == 0) return MLG_OK;
+    // the masked variant leaves empty rows stale: the pass never reads them
     SpmmArgs a;
     a.m = &p->Gut_s;
     a.nCh = p->nCh;
@@ -186,11 +230,14 @@ int nakatsha_stage(mlg_plan_s* p, int stage, const float2* y, const float* HY, f
     a.out.layout = Layout::kPointC64;
     a.out.a = p->grid;
     a.out.rows = p->Nu_tot;
+    a.long_only = fused_gut(p);
+    a.nonempty_only = p->adjoint_mode == kAdjMasked;
+    a.seg_scratch = p->seg_scratch;
     return spmm(a, s);
   }
-  const int ax = 3 - stage;  // stages 1, 2, 3 = z, y, x passes
-  if (ax >= p->imDim) return MLG_OK;
-  return inverse_pass(p, ax, scale, x, partial, n_partial, s);
+  const int ax = p->imDim - stage;
+  if (ax < 0) return MLG_OK;
+  return inverse_pass(p, ax, y, HY, scale, x, partial, n_partial, s);
 }
 
 int shanna_run(mlg_plan_s* p, const float2* x, bool x_per_coil, float2* y, const float* sqn_w, double* partial,
@@ -282,6 +329,7 @@ static void plan_free(mlg_plan_s* p) {
   cudaFree(p->bufA);
   cudaFree(p->bufB);
   cudaFree(p->partial);
+  cudaFree(p->seg_scratch);
   cudaFree(p->scalars);
   cudaFree(p->x_p);
   cudaFree(p->x_dagM);
@@ -366,7 +414,11 @@ static int plan_create_impl(int imDim, const int* N_u, const int* n_u, int nCh, 
   }
   cudaStream_t s = p->stream;
   if (Gu && (st = csr_sign_copy(*Gu, false, imDim, p->N, sc, p->Gu_s, s)) != MLG_OK) return bail(st);
+  // occupancy tables live with the caller's matrix (built once, shared by the
+  // sign-folded copy)
+  if (Gut && (nCh % 2) == 0 && (st = csr_build_nonempty(const_cast<Csr&>(*Gut), s)) != MLG_OK) return bail(st);
   if (Gut && (st = csr_sign_copy(*Gut, true, imDim, p->N, 1.0f, p->Gut_s, s)) != MLG_OK) return bail(st);
+  p->adjoint_mode = adjoint_mode_valid(p, kAdjMasked) ? kAdjMasked : (imDim >= 2 ? kAdjFused : kAdjFullGrid);
   const size_t kbytes = sizeof(float2) * (size_t)nu * nCh;
   const size_t gbytes = sizeof(float2) * (size_t)Nu * nCh;
   const size_t abytes = sizeof(float2) * (size_t)p->N[0] * p->n[1] * p->n[2] * nCh;
@@ -395,7 +447,10 @@ static int plan_create_impl(int imDim, const int* N_u, const int* n_u, int nCh, 
   cap = std::max(cap, ew_grid((long long)p->nPt * nCh) + 8);
   cap = std::max(cap, 256);  // the solver's two-stage max over ve uses 128 floats
   p->partial_cap = cap;
+  const size_t seg_floats = std::max<size_t>(
+      1, std::max(Gu ? spmm_scratch_floats(*Gu, nCh) : 0, Gut ? spmm_scratch_floats(*Gut, nCh) : 0));
   if (cudaMalloc(&p->partial, sizeof(double) * (size_t)cap) != cudaSuccess ||
+      cudaMalloc(&p->seg_scratch, sizeof(float) * seg_floats) != cudaSuccess ||
       cudaMalloc(&p->scalars, sizeof(double) * 64) != cudaSuccess) {
     cudaGetLastError();
     return bail(fail(MLG_ERR_OOM, "plan: partial buffer allocation failed"));

@@ -29,6 +29,13 @@ struct mlg_plan_s {
   mlg::FftAxisPlan ax[3];
   double* partial = nullptr;      // FP64 partial sums (CTA results)
   int partial_cap = 0;
+  float* seg_scratch = nullptr;   // long-row segment partials of Gu / Gut
+  // How the adjoint feeds its first inverse pass:
+  //  0 kAdjFullGrid: Gut writes every grid cell, the pass streams the grid;
+  //  1 kAdjFused:    the pass gathers Gut rows from k-space itself (2-D/3-D);
+  //  2 kAdjMasked:   Gut writes only its non-empty rows, the pass reads a
+  //                  cell only when its occupancy bit is set (even nCh).
+  int adjoint_mode = 0;
   double* scalars = nullptr;      // solver scalars (device)
   cudaStream_t stream = nullptr;  // internal non-blocking stream
   cudaEvent_t ev_in = nullptr, ev_out = nullptr;
@@ -54,6 +61,7 @@ int shanna_stage(mlg_plan_s* p, int stage, const float2* x, bool x_per_coil, flo
                  double* partial, int* n_partial, cudaStream_t s);
 int nakatsha_stage(mlg_plan_s* p, int stage, const float2* y, const float* HY, float scale, float2* x,
                    double* partial, int* n_partial, cudaStream_t s);
+bool adjoint_mode_valid(const mlg_plan_s* p, int mode);
 int shanna_run(mlg_plan_s* p, const float2* x, bool x_per_coil, float2* y, const float* sqn_w, double* partial,
                int* n_partial, cudaStream_t s);
 int nakatsha_run(mlg_plan_s* p, const float2* y, const float* HY, float scale, float2* x, double* partial,

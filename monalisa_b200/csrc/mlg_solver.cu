@@ -402,3 +402,65 @@ extern "C" int mlg_plan_profile(mlg_plan_t p, int iters, double* ms) {
   for (int k = 0; k < S; ++k) ms[k] = acc[k] / iters;
   return st;
 }
+
+// ---- adjoint strategy and autotuner ------------------------------------------
+extern "C" int mlg_plan_set_adjoint(mlg_plan_t p, int mode) {
+  using namespace mlg;
+  MLG_CHECK(p, "NULL plan");
+  MLG_CHECK(adjoint_mode_valid(p, mode), "adjoint strategy %d not available for this plan", mode);
+  if (p->adjoint_mode != mode) {
+    p->adjoint_mode = mode;
+    if (p->cg_graph) cudaGraphExecDestroy(p->cg_graph);  // captured with the old strategy
+    p->cg_graph = nullptr;
+    p->cg_graph_x = nullptr;
+  }
+  return MLG_OK;
+}
+
+extern "C" int mlg_plan_get_adjoint(mlg_plan_t p, int* mode) {
+  MLG_CHECK(p && mode, "NULL argument");
+  *mode = p->adjoint_mode;
+  return MLG_OK;
+}
+
+extern "C" int mlg_plan_autotune(mlg_plan_t p, int reps, double* ms) {
+  using namespace mlg;
+  MLG_CHECK(p && reps >= 1, "invalid argument");
+  MLG_CHECK(p->Gut, "autotuning needs a plan with Gut");
+  MLG_CUDA(cudaSetDevice(p->device));
+  MLG_TRY(ensure_solver_buffers(p));
+  cudaStream_t s = p->stream;
+  MLG_CUDA(cudaMemsetAsync(p->k_res, 0, sizeof(float2) * (size_t)p->nPt * p->nCh, s));
+  cudaEvent_t a, b;
+  MLG_CUDA(cudaEventCreate(&a));
+  MLG_CUDA(cudaEventCreate(&b));
+  const int orig = p->adjoint_mode;
+  int best = orig;
+  double best_ms = 1e30;
+  int st = MLG_OK;
+  for (int mode = 0; mode < 3 && st == MLG_OK; ++mode) {
+    double t = -1.0;
+    if (adjoint_mode_valid(p, mode)) {
+      p->adjoint_mode = mode;
+      st = nakatsha_run(p, p->k_res, nullptr, 1.0f, p->x_dagM, nullptr, nullptr, s);  // warm-up
+      cudaEventRecord(a, s);
+      for (int r = 0; r < reps && st == MLG_OK; ++r)
+        st = nakatsha_run(p, p->k_res, nullptr, 1.0f, p->x_dagM, nullptr, nullptr, s);
+      cudaEventRecord(b, s);
+      if (cudaEventSynchronize(b) != cudaSuccess) st = fail(MLG_ERR_CUDA, "autotune run failed");
+      float v = 0.f;
+      cudaEventElapsedTime(&v, a, b);
+      t = v / reps;
+      if (st == MLG_OK && t < best_ms) {
+        best_ms = t;
+        best = mode;
+      }
+    }
+    if (ms) ms[mode] = t;
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  p->adjoint_mode = orig;
+  if (st != MLG_OK) return st;
+  return mlg_plan_set_adjoint(p, best);
+}

@@ -160,15 +160,17 @@ __global__ void __launch_bounds__(256) spmm_short_kernel(SpmmParams p) {
   }
 }
 
-template <Layout IN, Layout OUT>
-__global__ void __launch_bounds__(256) spmm_long_kernel(SpmmParams p) {
+// Long rows: one CTA per segment of at most kSegLen entries.  Thread groups
+// of `cper` coils split the segment's entries (stride = number of groups);
+// the group partials are summed in group order and written, per coil, to
+// seg_scratch[segment][coil] = (re, im, weight sum).
+template <Layout IN>
+__global__ void __launch_bounds__(256) spmm_seg_kernel(SpmmParams p, const uint32_t* __restrict__ seg_lo,
+                                                       const uint32_t* __restrict__ seg_hi, float3* scratch) {
   __shared__ float3 part[256];
-  __shared__ double sh[32];
-  const long long r = __ldg(p.long_rows + blockIdx.x);
-  const uint32_t b = __ldg(p.row_ptr + r), e = __ldg(p.row_ptr + r + 1);
+  const uint32_t b = __ldg(seg_lo + blockIdx.x), e = __ldg(seg_hi + blockIdx.x);
   const int cper = min(p.nCh, (int)blockDim.x);   // coils per pass
   const int groups = (int)blockDim.x / cper;      // entry groups per coil
-  double sq = 0.0;
   for (int c0 = 0; c0 < p.nCh; c0 += cper) {
     const int cl = threadIdx.x % cper, g = threadIdx.x / cper;
     const int c = c0 + cl;
@@ -185,8 +187,29 @@ __global__ void __launch_bounds__(256) spmm_long_kernel(SpmmParams p) {
         sy = __fadd_rn(sy, q.y);
         sw = __fadd_rn(sw, q.z);
       }
-      sq += finish<OUT>(p, r, c0 + threadIdx.x, sx, sy, sw);
+      scratch[(long long)blockIdx.x * p.nCh + c0 + threadIdx.x] = make_float3(sx, sy, sw);
     }
+  }
+}
+
+// One CTA per long row: sums its segments in segment order, then finishes
+// (normalise / scale / store / FP64 partial) like the short-row kernel.
+template <Layout OUT>
+__global__ void __launch_bounds__(256) spmm_seg_combine_kernel(SpmmParams p, const int* __restrict__ seg0,
+                                                               const float3* __restrict__ scratch) {
+  __shared__ double sh[32];
+  const long long r = __ldg(p.long_rows + blockIdx.x);
+  const int s0 = __ldg(seg0 + blockIdx.x), s1 = __ldg(seg0 + blockIdx.x + 1);
+  double sq = 0.0;
+  for (int c = threadIdx.x; c < p.nCh; c += blockDim.x) {
+    float sx = 0.f, sy = 0.f, sw = 0.f;
+    for (int k = s0; k < s1; ++k) {
+      const float3 q = scratch[(long long)k * p.nCh + c];
+      sx = __fadd_rn(sx, q.x);
+      sy = __fadd_rn(sy, q.y);
+      sw = __fadd_rn(sw, q.z);
+    }
+    sq += finish<OUT>(p, r, c, sx, sy, sw);
   }
   if (p.partial) {
     const double t = block_sum(sq, sh);
@@ -194,21 +217,83 @@ __global__ void __launch_bounds__(256) spmm_long_kernel(SpmmParams p) {
   }
 }
 
-static int rows_per_block(const SpmmArgs& a) { return std::max(1, 1024 / std::max(1, a.nCh)); }
+// Point layout in and out, even nCh: a thread owns a (row, coil pair) output
+// and moves 16 bytes per load/store; the row's column/value stream is read
+// once per pair instead of once per coil.  `rows` (optional) lists the rows
+// to compute (the non-empty ones); other rows are left untouched.  Entries
+// are summed in stored order with round-to-nearest multiply/add.
+__global__ void __launch_bounds__(256) spmm_pair_kernel(SpmmParams p, const int* __restrict__ rows, int n_rows) {
+  __shared__ double sh[32];
+  const int P = p.nCh >> 1;
+  const long long i0 = (long long)blockIdx.x * p.rows_per_block;
+  const int nr = (int)min((long long)p.rows_per_block, (long long)n_rows - i0);
+  const float4* in = reinterpret_cast<const float4*>(p.in.a);
+  float4* out = reinterpret_cast<float4*>(p.out.a);
+  const bool scale = p.in_row_scale != nullptr;
+  double sq = 0.0;
+  for (int it = threadIdx.x; it < nr * P; it += blockDim.x) {
+    const int lr = it / P, pi = it - (it / P) * P;
+    const long long r = rows ? (long long)__ldg(rows + i0 + lr) : i0 + lr;
+    const uint32_t b = __ldg(p.row_ptr + r), e = __ldg(p.row_ptr + r + 1);
+    if (e - b > (uint32_t)kLongRow) continue;  // segment kernels own it
+    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll 4
+    for (uint32_t k = b; k < e; ++k) {
+      const int j = __ldg(p.col + k);
+      const float m = __ldg(p.val + k);
+      float4 v = __ldg(in + (long long)j * P + pi);
+      if (scale) {
+        const float h = __ldg(p.in_row_scale + j);
+        v = make_float4(__fmul_rn(h, v.x), __fmul_rn(h, v.y), __fmul_rn(h, v.z), __fmul_rn(h, v.w));
+      }
+      acc.x = __fadd_rn(acc.x, __fmul_rn(m, v.x));
+      acc.y = __fadd_rn(acc.y, __fmul_rn(m, v.y));
+      acc.z = __fadd_rn(acc.z, __fmul_rn(m, v.z));
+      acc.w = __fadd_rn(acc.w, __fmul_rn(m, v.w));
+    }
+    if (p.out_scale != 1.0f)
+      acc = make_float4(__fmul_rn(acc.x, p.out_scale), __fmul_rn(acc.y, p.out_scale), __fmul_rn(acc.z, p.out_scale),
+                        __fmul_rn(acc.w, p.out_scale));
+    out[r * P + pi] = acc;
+    if (p.partial) {
+      const double w = p.sqn_w ? (double)__ldg(p.sqn_w + r) : 1.0;
+      sq += w * ((double)acc.x * acc.x + (double)acc.y * acc.y + (double)acc.z * acc.z + (double)acc.w * acc.w);
+    }
+  }
+  if (p.partial) {
+    const double t = block_sum(sq, sh);
+    if (threadIdx.x == 0) p.partial[blockIdx.x] = t;
+  }
+}
+
+static bool use_pair_kernel(const SpmmArgs& a) {
+  return a.in.layout == Layout::kPointC64 && a.out.layout == Layout::kPointC64 && (a.nCh % 2) == 0 && !a.normalize;
+}
+
+static int rows_per_block(const SpmmArgs& a) {
+  if (use_pair_kernel(a)) return std::max(1, 1024 / (a.nCh / 2));
+  return std::max(1, 1024 / std::max(1, a.nCh));
+}
+
+static long long spmm_rows(const SpmmArgs& a) { return a.nonempty_only ? a.m->n_nonempty : a.m->l_size; }
 
 int spmm_partial_count(const SpmmArgs& a) {
   const int rpb = rows_per_block(a);
-  return (int)((a.m->l_size + (long long)rpb - 1) / rpb) + a.m->n_long;
+  return (int)((spmm_rows(a) + rpb - 1) / rpb) + a.m->n_long;
 }
 
+size_t spmm_scratch_floats(const Csr& m, int nCh) { return 3 * (size_t)m.n_seg * (size_t)nCh; }
+
 template <Layout IN, Layout OUT, bool ROW_FAST>
-static int launch(const SpmmParams& p, int grid_short, cudaStream_t s) {
+static int launch(const SpmmParams& p, const Csr& m, float3* scratch, int grid_short, cudaStream_t s) {
   if (grid_short > 0) {
     spmm_short_kernel<IN, OUT, ROW_FAST><<<grid_short, 256, 0, s>>>(p);
     MLG_LAUNCHED();
   }
   if (p.n_long > 0) {
-    spmm_long_kernel<IN, OUT><<<p.n_long, 256, 0, s>>>(p);
+    spmm_seg_kernel<IN><<<m.n_seg, 256, 0, s>>>(p, m.seg_lo, m.seg_hi, scratch);
+    MLG_LAUNCHED();
+    spmm_seg_combine_kernel<OUT><<<p.n_long, 256, 0, s>>>(p, m.long_seg0, scratch);
     MLG_LAUNCHED();
   }
   return MLG_OK;
@@ -233,16 +318,38 @@ int spmm(const SpmmArgs& a, cudaStream_t s) {
   p.normalize = a.normalize ? 1 : 0;
   p.sqn_w = a.sqn_row_weight;
   p.partial = a.partial;
-  const int grid_short = (int)((m.l_size + (long long)p.rows_per_block - 1) / p.rows_per_block);
-  p.partial_long_offset = grid_short;
+  MLG_CHECK(!a.nonempty_only || (m.nz_rows && use_pair_kernel(a)),
+            "non-empty-row products need the row list and the coil-pair kernel");
+  const long long nrows = spmm_rows(a);
+  const int grid_all = (int)((nrows + p.rows_per_block - 1) / p.rows_per_block);
+  const int grid_short = a.long_only ? 0 : grid_all;
+  p.partial_long_offset = grid_all;
+  MLG_CHECK(m.n_long == 0 || m.n_seg > 0, "long rows without segment tables");
+  DevBuf<float> own;
+  float* scratch = a.seg_scratch;
+  if (m.n_long > 0 && !scratch) {
+    MLG_TRY(own.alloc(spmm_scratch_floats(m, a.nCh), s));
+    scratch = own.p;
+  }
+  float3* sc3 = reinterpret_cast<float3*>(scratch);
   using L = Layout;
+  if (use_pair_kernel(a)) {
+    if (grid_short > 0) {
+      spmm_pair_kernel<<<grid_short, 256, 0, s>>>(p, a.nonempty_only ? m.nz_rows : nullptr, (int)nrows);
+      MLG_LAUNCHED();
+    }
+    return launch<L::kPointC64, L::kPointC64, false>(p, m, sc3, 0, s);
+  }
   const L i = a.in.layout, o = a.out.layout;
-  if (i == L::kCoilC64 && o == L::kPointC64) return launch<L::kCoilC64, L::kPointC64, false>(p, grid_short, s);
-  if (i == L::kPointC64 && o == L::kCoilC64) return launch<L::kPointC64, L::kCoilC64, true>(p, grid_short, s);
-  if (i == L::kPointC64 && o == L::kPointC64) return launch<L::kPointC64, L::kPointC64, false>(p, grid_short, s);
-  if (i == L::kCoilSplit && o == L::kCoilSplit) return launch<L::kCoilSplit, L::kCoilSplit, true>(p, grid_short, s);
-  if (i == L::kPointSplit && o == L::kPointSplit) return launch<L::kPointSplit, L::kPointSplit, false>(p, grid_short, s);
-  if (i == L::kCoilReal && o == L::kCoilReal) return launch<L::kCoilReal, L::kCoilReal, true>(p, grid_short, s);
+  if (i == L::kCoilC64 && o == L::kPointC64) return launch<L::kCoilC64, L::kPointC64, false>(p, m, sc3, grid_short, s);
+  if (i == L::kPointC64 && o == L::kCoilC64) return launch<L::kPointC64, L::kCoilC64, true>(p, m, sc3, grid_short, s);
+  if (i == L::kPointC64 && o == L::kPointC64)
+    return launch<L::kPointC64, L::kPointC64, false>(p, m, sc3, grid_short, s);
+  if (i == L::kCoilSplit && o == L::kCoilSplit)
+    return launch<L::kCoilSplit, L::kCoilSplit, true>(p, m, sc3, grid_short, s);
+  if (i == L::kPointSplit && o == L::kPointSplit)
+    return launch<L::kPointSplit, L::kPointSplit, false>(p, m, sc3, grid_short, s);
+  if (i == L::kCoilReal && o == L::kCoilReal) return launch<L::kCoilReal, L::kCoilReal, true>(p, m, sc3, grid_short, s);
   return fail(MLG_ERR_UNSUPPORTED, "spmm: layout pair (%d,%d) not instantiated", (int)i, (int)o);
 }
 

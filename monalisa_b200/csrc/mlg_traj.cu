@@ -219,6 +219,7 @@ static int finish_csr(Csr& m, int* counts, cudaStream_t s) {
   m.long_rows = list;
   m.n_long = h[0];
   m.n_nonempty = h[1];
+  MLG_TRY(csr_build_segments(m, s));
   return MLG_OK;
 }
 

@@ -117,6 +117,25 @@ class NufftPlan:
     def handle(self):
         return self._h
 
+    ADJOINT_MODES = ("full_grid", "fused", "masked")
+
+    @property
+    def adjoint_mode(self) -> str:
+        m = ctypes.c_int()
+        N.call("mlg_plan_get_adjoint", self._h, ctypes.byref(m))
+        return self.ADJOINT_MODES[m.value]
+
+    @adjoint_mode.setter
+    def adjoint_mode(self, name: str):
+        N.call("mlg_plan_set_adjoint", self._h, self.ADJOINT_MODES.index(name))
+
+    def autotune(self, reps: int = 3) -> dict:
+        """Times the valid adjoint strategies and keeps the fastest; returns
+        {strategy: ms} (strategies the plan cannot run are omitted)."""
+        ms = np.zeros(3)
+        N.call("mlg_plan_autotune", self._h, int(reps), N.dptr(ms))
+        return {n: float(t) for n, t in zip(self.ADJOINT_MODES, ms) if t >= 0}
+
     def device_bytes(self) -> int:
         b = ctypes.c_longlong()
         N.call("mlg_plan_device_bytes", self._h, ctypes.byref(b))

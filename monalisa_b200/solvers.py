@@ -27,7 +27,7 @@ class SensaRecon:
     """CG-SENSE with everything resident on the device: Gu/Gut, KFC,
     KFC_conj, cuFFT plans and work vectors (one per trajectory/coil set)."""
 
-    def __init__(self, Gu, Gut, C, n_u, dK_u=None):
+    def __init__(self, Gu, Gut, C, n_u, dK_u=None, autotune=False):
         if isinstance(Gu, bmSparseMat):
             Gu = Gu.to_device()
         if isinstance(Gut, bmSparseMat):
@@ -44,6 +44,7 @@ class SensaRecon:
         self.plan = NufftPlan(self.N_u, self.n_u, self.nCh, Gu, Gut, KFC, KFC_conj, self.dK_u)
         self.nPt = self.plan.nPt
         self._mats = (Gu, Gut)
+        self.tuning = self.plan.autotune() if autotune else None
 
     def run_dev(self, y, ve, x, nIter=1, nCGD=20, ve_max=None, residual=None):
         """y [nPt, nCh], ve [nPt] float32, x [prod(n_u)] (in/out) CUDA tensors."""

@@ -238,6 +238,41 @@ def test_operators_3d_and_per_coil():
     assert rel(xn, oracle.bmNakatsha(yy, G["Gut"], KFCc, True, n_u)) <= 1e-5
 
 
+@pytest.mark.parametrize("nCh", [4, 3])
+def test_adjoint_strategies_agree(nCh):
+    """Every adjoint strategy of a plan gives the oracle's Nakatsha; the
+    autotuner picks one of them."""
+    import monalisa_b200 as mb
+    import torch
+
+    rng = np.random.default_rng(21)
+    N_u, n_u = np.array([32, 32, 32]), np.array([16, 16, 16])
+    t = _radial3(300, 32, 32, 2)  # dense centre: long rows exist
+    Gu, Gut = mb.bmTraj2SparseMat(t, np.ones(t.shape[1]), N_u, [1, 1, 1])
+    C = (rng.standard_normal((n_u.prod(), nCh)) + 1j * rng.standard_normal((n_u.prod(), nCh))).astype(np.complex64)
+    KFC = oracle.bmKF(C, N_u, n_u, [1, 1, 1], nCh, "gauss", 3, [0.61, 10])
+    KFCc = oracle.bmKF_conj(np.conj(C), N_u, n_u, [1, 1, 1], nCh, "gauss", 3, [0.61, 10])
+    plan = mb.NufftPlan(N_u, n_u, nCh, Gu, Gut, KFC, KFCc)
+    y = (rng.standard_normal((t.shape[1], nCh)) + 1j * rng.standard_normal((t.shape[1], nCh))).astype(np.complex64)
+    gut_o = Gut.download()
+    G = oracle.SparseMat(r_size=gut_o.r_size, l_size=gut_o.l_size, r_nJump=gut_o.r_nJump, m_val=gut_o.m_val,
+                         r_jump=gut_o.r_jump, l_jump=gut_o.l_jump, l_nJump=gut_o.l_nJump, N_u=N_u)
+    ref = oracle.bmNakatsha(y, G, KFCc, True, n_u).ravel()
+    yd = torch.from_numpy(y).cuda()
+    outs = {}
+    for mode in mb.NufftPlan.ADJOINT_MODES:
+        try:
+            plan.adjoint_mode = mode
+        except mb.MonalisaError:
+            assert mode == "masked" and nCh % 2  # masked needs an even coil count
+            continue
+        outs[mode] = plan.nakatsha(yd).cpu().numpy()
+        assert rel(outs[mode], ref) <= 1e-5, mode
+    times = plan.autotune(2)
+    assert set(times) == set(outs) and plan.adjoint_mode in outs
+    assert min(times.values()) > 0
+
+
 def test_idf_gateway(mex):
     rng = np.random.default_rng(4)
     x = (rng.standard_normal((16, 12, 2)) + 1j * rng.standard_normal((16, 12, 2))).astype(np.complex64)
