@@ -76,6 +76,33 @@ int mlg_gridder_n2u_leight(int imDim, const float* aReal, const float* aImag,
                            int Nz, int nWin, float kernelParam_1,
                            float kernelParam_2, float* bReal, float* bImag);
 
+/* The gridder of mlg_gridder_n2u_leight for callers that cannot allocate
+ * device memory while they run (a program that reserved the GPU's memory for
+ * its own pool at start-up, an embedding that forbids allocation after
+ * initialisation, a real-time loop that cannot afford an allocation's
+ * synchronisation).  No counterpart in the reference: it is an addition of
+ * this library.
+ *  - Inputs and outputs are device pointers owned by the caller, in the same
+ *    layouts as mlg_gridder_n2u_leight: aReal/aImag [nCh, nPt], tx/ty/tz/Dn
+ *    [nPt], bReal/bImag [nCh, Nx*Ny*Nz].  Work is ordered on `stream`
+ *    (NULL = default stream); the call returns once the gridding kernels are
+ *    queued, so the outputs are ready when the stream reaches that point.
+ *  - Nothing is allocated: all scratch comes from one fixed 32 MiB array in
+ *    device memory that every GPU loading the library holds until exit.  A
+ *    problem whose counters or bins do not fit is rejected with MLG_ERR_ARG
+ *    and a message giving the bytes it would need.
+ *  - The first call on a device looks up the array's device address; make it
+ *    before any stream capture.
+ *  - All calls share the array: calls that overlap on the GPU (other threads,
+ *    other streams) race.  Each call clears the counters it relies on. */
+int mlg_gridder_n2u_leight_noalloc(int imDim, const float* aReal,
+                                   const float* aImag, const float* tx,
+                                   const float* ty, const float* tz,
+                                   const float* Dn, int nCh, int nPt, int Nx,
+                                   int Ny, int Nz, int nWin,
+                                   float kernelParam_1, float kernelParam_2,
+                                   float* bReal, float* bImag, void* stream);
+
 /* Replaces bmGridder_n2u_mex
  * (src/gridding123/mex/bmGridder_n2u/bmGridder_n2u_mex.cpp:23 gateway, :72
  * kernel), as called by src/gridding123/m/bmGridder_n2u.m:203.

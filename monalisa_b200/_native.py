@@ -32,6 +32,8 @@ SIGNATURES = {
     "mlg_gridder_n2u_leight": [c_int, P_f, P_f, P_f, P_f, P_f, P_f, c_int, c_int, c_int, c_int, c_int, c_int,
                                c_float, c_float, P_f, P_f],
     "mlg_gridder_n2u": [P_f, P_f, P_f, P_i, c_int, c_int, c_int, c_int, P_f, P_f],
+    "mlg_gridder_n2u_leight_noalloc": [c_int, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_int, c_int, c_int, c_int, c_int,
+                                       c_int, c_float, c_float, c_vp, c_vp, c_vp],
     "mlg_sparsemat_vec_cC": [c_int, P_i, P_i, P_f, c_int, P_i, c_int, P_f, P_f, c_int, P_f, P_f],
     "mlg_sparsemat_vec_cR": [c_int, P_i, P_i, P_f, c_int, P_i, c_int, P_f, P_f, c_int, P_f, P_f],
     "mlg_sparsemat_vec_rC": [c_int, P_i, P_i, P_f, c_int, P_i, c_int, P_f, c_int, P_f],
