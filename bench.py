@@ -96,13 +96,6 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
-def _dist():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return ws, rank, local
-
-
 # profile order of mlg_plan_profile: forward x/y/z passes, Gu, the Gut product
 # (all rows, non-empty rows, or only the long rows, by adjoint strategy),
 # inverse z pass (reading the grid, the occupancy-masked grid, or gathering
@@ -141,12 +134,12 @@ def algorithmic_bytes(w, Gu, Gut, nCh, adjoint):
 
 def run_gpu(args):
     import torch
-    import torch.distributed as dist
 
-    ws, rank, local = _dist()
+    from monalisa_b200 import replicas
+
+    ws, rank, local = replicas.world()
     torch.cuda.set_device(local)
-    if ws > 1:
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    replicas.init("nccl", timeout_s=600)
     import monalisa_b200 as mb
     from monalisa_b200 import _native as N
     from monalisa_b200.workloads import koosh3d
@@ -181,8 +174,7 @@ def run_gpu(args):
     clocks.start()
     l0 = N.launch_count()
     stream = torch.cuda.current_stream()
-    if ws > 1:
-        dist.barrier()
+    replicas.barrier()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
@@ -190,16 +182,12 @@ def run_gpu(args):
         step()
     e1.record(stream)
     torch.cuda.synchronize()
-    if ws > 1:
-        dist.barrier()
+    replicas.barrier()
     launches = N.launch_count() - l0
     ms = e0.elapsed_time(e1)
     clk = clocks.stop()
-    if ws > 1:
-        tt = torch.tensor([ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
-    value = ws * args.steps / (ms / 1e3)
+    ms = replicas.max_over_ranks(ms, device=dev)
+    value = replicas.throughput(ws, args.steps, ms / 1e3)
 
     # end to end through the C ABI with host buffers (pinned), copies inside
     ypin = torch.empty((w.nPt, w.nCh), dtype=torch.complex64, pin_memory=True)
@@ -223,17 +211,12 @@ def run_gpu(args):
                N.fptr(xI), N.dptr(res))
 
     e2e_step()
-    if ws > 1:
-        dist.barrier()
+    replicas.barrier()
     ta = time.perf_counter()
     for _ in range(args.steps):
         e2e_step()
-    e2e_s = time.perf_counter() - ta
-    if ws > 1:
-        tt = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_s = float(tt.item())
-    e2e = {"value": ws * args.steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(yR_p.nbytes + yI_p.nbytes +
+    e2e_s = replicas.max_over_ranks(time.perf_counter() - ta, device=dev)
+    e2e = {"value": replicas.throughput(ws, args.steps, e2e_s), "unit": UNIT, "h2d_bytes_per_step": int(yR_p.nbytes + yI_p.nbytes +
                                                                                      ve_h.nbytes + xR.nbytes +
                                                                                      xI.nbytes),
            "d2h_bytes_per_step": int(xR.nbytes + xI.nbytes + res.nbytes)}
@@ -278,8 +261,7 @@ def run_gpu(args):
     if rank == 0:
         print(json.dumps(out), flush=True)
     rec.plan.close()
-    if ws > 1:
-        dist.destroy_process_group()
+    replicas.shutdown()
 
 
 def _oracle():
@@ -326,7 +308,9 @@ def cpu_baseline(w, gu, gut, y):
 
 
 def run_reference(args):
-    ws, rank, local = _dist()
+    from monalisa_b200 import replicas
+
+    ws, rank, local = replicas.world()
     if rank != 0:
         return
     from monalisa_b200.workloads import koosh3d
