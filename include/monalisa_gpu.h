@@ -187,8 +187,8 @@ int mlg_deapodization(int imDim, const int* N_u, const double* dK_u,
 
 /* ---- fused operators (NUFFT plan) --------------------------------------- */
 
-/* A plan holds cuFFT plans, the sign-folded copies of Gu/Gut used by the
- * fused operators, KFC and KFC_conj ([nCh, prod(n_u)] coil-major, host
+/* A plan holds the FFT pass tables, the sign-folded copies of Gu/Gut used by
+ * the fused operators, KFC and KFC_conj ([prod(n_u), nCh] column layout, host
  * arrays as produced by src/fourier123/prep_function/bmKF.m and
  * bmKF_conj.m) and work buffers.  N_u and n_u must be even; n_u <= N_u.
  * Gu / Gut stay owned by the caller and must outlive the plan. */
@@ -196,7 +196,17 @@ int mlg_plan_create(int imDim, const int* N_u, const int* n_u, int nCh,
                     mlg_matrix_t Gu, mlg_matrix_t Gut, const float* KFC_re,
                     const float* KFC_im, const float* KFCc_re,
                     const float* KFCc_im, mlg_plan_t* out);
+/* MLG_ERR_STATE while plans created by mlg_plan_create_sharing borrow from p. */
 int mlg_plan_destroy(mlg_plan_t p);
+/* A plan over other matrices on base's grid (another frame bin or another
+ * trajectory with the same N_u, n_u, coils and KFC): it borrows base's KFC,
+ * KFC_conj, grid buffers, FFT tables, dK_u and stream, so its operators run
+ * in the order of base's stream and it costs only the matrices'
+ * sign-folded copies.  The frame bins of bmTevaMorphosia_chain.m:56-57 all
+ * use one KFC.  No reference counterpart (the reference recomputes its FFT
+ * buffers per call). */
+int mlg_plan_create_sharing(mlg_plan_t base, mlg_matrix_t Gu, mlg_matrix_t Gut,
+                            mlg_plan_t* out);
 /* k-space grid step dK_u [imDim] (default 1): sets the image-space volume
  * element HX = prod((1/dK_u)/N_u) used by the solvers
  * (src/fourier123/solver_function/imDim/nonCartesian/bmSensa.m:26-27). */
@@ -286,6 +296,45 @@ int mlg_sensa_dev(mlg_plan_t p, const void* y, const float* ve, float ve_max,
 int mlg_sensa(mlg_plan_t p, const float* yR, const float* yI, const float* ve,
               float ve_max, int nIter, int nCGD, float* xR, float* xI,
               double* residual);
+
+/* Frame bins of a temporal reconstruction: one plan per frame (same device,
+ * N_u, n_u, nCh; each with Gu and Gut; typically plans 1.. created with
+ * mlg_plan_create_sharing from plan 0).  HX comes from plan 0's dK_u.  The
+ * chain holds the solver's work arrays over all frames; the plans stay the
+ * caller's, must outlive the chain and must not be used while a chain call
+ * runs. */
+typedef struct mlg_chain_s* mlg_chain_t;
+int mlg_chain_create(int nFr, const mlg_plan_t* plans, mlg_chain_t* out);
+int mlg_chain_destroy(mlg_chain_t c);
+/* nFr, the total k-space rows sum(nPt_f) and the pixels per frame. */
+int mlg_chain_info(mlg_chain_t c, int* nFr, long long* rows, long long* pixels);
+
+#define MLG_REGUL_NORMAL 0 /* delta, rho from linspace(first, last, nIter) */
+#define MLG_REGUL_ADAPT 1  /* delta = factor * regul / dafi, rho = factor * delta */
+/* Temporal-TV ADMM,
+ * src/fourier123/solver_function/imDim_morphosia/nonCartesian/
+ * bmTevaMorphosia_chain.m:6-195, with Tu = Tut = [] (no deformation):
+ *   min sum_f 0.5 |y_f - M_f x_f|^2_HY + delta sum_f |x_f - x_{f-1}|_1
+ * with circular frame differences.  nIter ADMM iterations, each a CG run of
+ * at most nCGD x-updates.  Device buffers: y [sum nPt_f][nCh] (frames in
+ * order), ve [sum nPt_f], x, z, u [nFr][prod(n_u)] (x in: initial guess,
+ * out: result; z, u in/out, set to F x and 0 first when init_zu).  delta and
+ * rho are {first, last} of their per-iteration lists (equal values for a
+ * constant).  history (host, may be NULL) receives per iteration
+ * {0.5 dafi + 0.5 delta regul, dafi, regul} (:172-178).  Norms and step sizes
+ * are FP64. */
+int mlg_tevamorphosia_dev(mlg_chain_t c, const void* y, const float* ve,
+                          float ve_max, const float* delta, const float* rho,
+                          int regul_mode, int nIter, int nCGD, void* x,
+                          void* z, void* u, int init_zu, double* history,
+                          void* stream);
+/* Same with host buffers in MATLAB layouts: y{f} [nPt_f, nCh] column-major,
+ * frames concatenated (yR, yI), ve{f} concatenated, x [prod(n_u), nFr]
+ * (xR, xI in/out).  z and u start as F x and 0 (the reference's defaults). */
+int mlg_tevamorphosia(mlg_chain_t c, const float* yR, const float* yI,
+                      const float* ve, float ve_max, const float* delta,
+                      const float* rho, int regul_mode, int nIter, int nCGD,
+                      float* xR, float* xI, double* history);
 
 #if defined(__GNUC__)
 #pragma GCC visibility pop

@@ -63,6 +63,13 @@ SIGNATURES = {
     "mlg_idf": [c_int, P_i, P_f, c_int, P_f, P_f, P_f, P_f],
     "mlg_sensa_dev": [c_vp, c_vp, P_f, c_float, c_int, c_int, c_vp, P_d, c_vp],
     "mlg_sensa": [c_vp, P_f, P_f, P_f, c_float, c_int, c_int, P_f, P_f, P_d],
+    "mlg_plan_create_sharing": [c_vp, c_vp, c_vp, ctypes.POINTER(c_vp)],
+    "mlg_chain_create": [c_int, ctypes.POINTER(c_vp), ctypes.POINTER(c_vp)],
+    "mlg_chain_destroy": [c_vp],
+    "mlg_chain_info": [c_vp, P_i, P_ll, P_ll],
+    "mlg_tevamorphosia_dev": [c_vp, c_vp, P_f, c_float, P_f, P_f, c_int, c_int, c_int, c_vp, c_vp, c_vp, c_int, P_d,
+                              c_vp],
+    "mlg_tevamorphosia": [c_vp, P_f, P_f, P_f, c_float, P_f, P_f, c_int, c_int, c_int, P_f, P_f, P_d],
 }
 _RESTYPE = {"mlg_status_string": ctypes.c_char_p, "mlg_last_error": ctypes.c_char_p,
             "mlg_kernel_launch_count": c_ll}

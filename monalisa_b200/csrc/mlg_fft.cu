@@ -7,7 +7,7 @@
 //      n1*N2 + n2), each output k1 multiplied by W_N^(n2*k1);
 //   C. for every k1 < N1 and column: an N2-point FFT over n2 (elements
 //      k1*N2 + n2) -> X[k1 + N1*k2] stored at position k1*N2 + k2.
-// Sub-FFTs of power-of-two size run as unrolled radix-2 butterflies in
+// Sub-FFTs of size 2^a 3^b run as unrolled radix-2/radix-3 butterflies in
 // registers (templated fast path); other sizes <= 32 use a direct DFT
 // (runtime path).  Twiddles come from a per-axis table exp(-2 pi i j/N)
 // computed on the host in double precision.
@@ -20,7 +20,8 @@
 
 namespace mlg {
 
-constexpr int kFftThreads = 256;
+constexpr int kFftThreads = 256;     // target threads per CTA
+constexpr int kFftMaxThreads = 512;  // launch bound (columns that need lcm(cols, 32) > 256)
 constexpr size_t kFftSmemCap = 100 * 1024;
 constexpr int kGatherBatch = 8;  // cells gathered concurrently per thread (kGutIn)
 
@@ -108,10 +109,58 @@ __device__ __forceinline__ void rstages(float2 (&r)[R]) {
   }
 }
 
-// DIR < 0: X[k] = sum_j r[j] exp(-2 pi i jk/R) (forward); DIR > 0: inverse
+constexpr bool cx_pow2(int v) { return v > 0 && (v & (v - 1)) == 0; }
+
+template <int R, int DIR>
+__device__ __forceinline__ void reg_fft(float2 (&r)[R]);
+
+// R = 3M (M = 2^a 3^b): decimation in time by 3.  The three M-point
+// transforms of r[3m], r[3m+1], r[3m+2] are combined by radix-3 butterflies
+// with compile-time twiddles W_R^k, W_R^2k:
+//   X[k] = a + b + c,  X[k+M], X[k+2M] = a - (b+c)/2 -+ DIR i (sqrt3/2)(b-c)
+// where b, c carry their twiddles (DIR = -1 forward, +1 inverse).
+template <int R, int DIR>
+__device__ __forceinline__ void reg_fft_radix3(float2 (&r)[R]) {
+  constexpr int M = R / 3;
+  float2 a[M], b[M], c[M];
+  sfor<M>([&](auto mc) {
+    constexpr int m = decltype(mc)::value;
+    a[m] = r[3 * m];
+    b[m] = r[3 * m + 1];
+    c[m] = r[3 * m + 2];
+  });
+  reg_fft<M, DIR>(a);
+  reg_fft<M, DIR>(b);
+  reg_fft<M, DIR>(c);
+  constexpr float h = (float)(0.86602540378443864676 * (double)DIR);  // DIR * sqrt(3)/2
+  sfor<M>([&](auto kc) {
+    constexpr int k = decltype(kc)::value;
+    constexpr double a1 = cx_reduce((double)DIR * 2.0 * kPiD * (double)k / (double)R);
+    constexpr double a2 = cx_reduce((double)DIR * 2.0 * kPiD * (double)(2 * k) / (double)R);
+    constexpr float w1r = (float)cx_cos_red(a1), w1i = (float)cx_sin_red(a1);
+    constexpr float w2r = (float)cx_cos_red(a2), w2i = (float)cx_sin_red(a2);
+    float2 bv = b[k], cv = c[k];
+    if constexpr (k != 0) {
+      bv = make_float2(w1r * b[k].x - w1i * b[k].y, w1r * b[k].y + w1i * b[k].x);
+      cv = make_float2(w2r * c[k].x - w2i * c[k].y, w2r * c[k].y + w2i * c[k].x);
+    }
+    const float2 s = make_float2(bv.x + cv.x, bv.y + cv.y);
+    const float2 d = make_float2(bv.x - cv.x, bv.y - cv.y);
+    const float2 m = make_float2(a[k].x - 0.5f * s.x, a[k].y - 0.5f * s.y);
+    r[k] = make_float2(a[k].x + s.x, a[k].y + s.y);
+    r[k + M] = make_float2(m.x - h * d.y, m.y + h * d.x);      // m + h i d
+    r[k + 2 * M] = make_float2(m.x + h * d.y, m.y - h * d.x);  // m - h i d
+  });
+}
+
+// DIR < 0: X[k] = sum_j r[j] exp(-2 pi i jk/R) (forward); DIR > 0: inverse.
+// R = 2^a 3^b.
 template <int R, int DIR>
 __device__ __forceinline__ void reg_fft(float2 (&r)[R]) {
-  if constexpr (R > 1) {
+  if constexpr (R > 1 && !cx_pow2(R)) {
+    static_assert(R % 3 == 0, "register FFT length must be 2^a 3^b");
+    reg_fft_radix3<R, DIR>(r);
+  } else if constexpr (R > 1) {
     sfor<R>([&](auto ic) {  // bit-reversal permutation
       constexpr int i = decltype(ic)::value;
       constexpr int j = bitrev(i, R);
@@ -341,7 +390,7 @@ __device__ __forceinline__ void gut_load(const PassDesc& d, const Lines& ln, flo
 }
 
 template <int N1, int N2, int DIR, PassMode MODE>
-__global__ void __launch_bounds__(kFftThreads) fft_pass_kernel(PassDesc d, int L, int rN1, int rN2,
+__global__ void __launch_bounds__(kFftMaxThreads) fft_pass_kernel(PassDesc d, int L, int rN1, int rN2,
                                                                const float2* __restrict__ tw) {
   extern __shared__ float2 s[];
   const int n1s = N1 > 0 ? N1 : rN1, n2s = N2 > 0 ? N2 : rN2;
@@ -447,7 +496,7 @@ __global__ void __launch_bounds__(kFftThreads) fft_pass_kernel(PassDesc d, int L
   smem_fft<N1, N2, DIR>(s, cols, n1s, n2s, tw);
   // X[k] sits at position (k % n1s) * n2s + k / n1s
   if constexpr (MODE == PassMode::kNakatshaOut) {
-    __shared__ double red[kFftThreads / 32];
+    __shared__ double red[kFftMaxThreads / 32];
     // group of gc lanes per output pixel, lanes over coils, fixed-order tree
     int gc = 1;
     while (gc < C && gc < 32) gc <<= 1;
@@ -492,7 +541,7 @@ __global__ void __launch_bounds__(kFftThreads) fft_pass_kernel(PassDesc d, int L
       __syncthreads();
       if (threadIdx.x == 0) {
         double t = 0.0;
-        for (int i = 0; i < kFftThreads / 32; ++i) t += red[i];
+        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += red[i];
         d.partial[blockIdx.x] = t;
       }
     }
@@ -540,7 +589,11 @@ int fft_axis_init(int N, FftAxisPlan& a) {
   a.N = N;
   a.N1 = best1;
   a.N2 = N / best1;
-  a.fast = pow2(a.N1) && pow2(a.N2) && a.N1 >= 4 && a.N2 <= 32 && (a.N2 == a.N1 || a.N2 == 2 * a.N1);
+  // unrolled register transforms exist for these factor pairs (lengths 2^k
+  // and 3 * 2^k from 16 to 1024); other lengths use the runtime DFT
+  static const int kFast[] = {404, 408, 808, 816, 1616, 1632, 3232, 608, 812, 1216, 1624, 2432};
+  a.fast = false;
+  for (int f : kFast) a.fast = a.fast || f == a.N1 * 100 + a.N2;
   std::vector<float2> t(N);
   for (int j = 0; j < N; ++j) {
     const double ang = -2.0 * M_PI * (double)j / (double)N;
@@ -575,6 +628,24 @@ int fft_pass_blocks(const FftAxisPlan& a, const PassDesc& d) {
   return blocks_for(d, lines_per_cta(a, d.C, PassMode::kNakatshaOut));
 }
 
+// Threads per CTA: a multiple of the CTA's columns (and of the warp) so that
+// every thread keeps one column (or coil pair) through the load, the
+// transform and the store; the multiple nearest kFftThreads.  Columns whose
+// lcm with 32 exceeds kFftMaxThreads take kFftThreads and the per-element
+// paths.
+static int threads_for(int cols) {
+  int g = cols, b = 32;
+  while (b) {
+    const int t = g % b;
+    g = b;
+    b = t;
+  }
+  const int l = cols / g * 32;  // lcm(cols, 32)
+  if (l > kFftMaxThreads) return kFftThreads;
+  const int k = std::max(1, (kFftThreads + l / 2) / l);
+  return std::min(kFftMaxThreads / l * l, k * l);
+}
+
 template <int N1, int N2, int DIR, PassMode MODE>
 static int launch_pass(const FftAxisPlan& a, const PassDesc& d, int L, cudaStream_t s) {
   const size_t smem = (size_t)a.N * L * d.C * sizeof(float2);
@@ -584,7 +655,7 @@ static int launch_pass(const FftAxisPlan& a, const PassDesc& d, int L, cudaStrea
                                   (int)(200 * 1024)));
     attr = true;
   }
-  fft_pass_kernel<N1, N2, DIR, MODE><<<blocks_for(d, L), kFftThreads, smem, s>>>(d, L, a.N1, a.N2, a.tw);
+  fft_pass_kernel<N1, N2, DIR, MODE><<<blocks_for(d, L), threads_for(L * d.C), smem, s>>>(d, L, a.N1, a.N2, a.tw);
   MLG_LAUNCHED();
   return MLG_OK;
 }
@@ -600,6 +671,11 @@ static int dispatch_size(const FftAxisPlan& a, const PassDesc& d, int L, cudaStr
       case 1616: return launch_pass<16, 16, DIR, MODE>(a, d, L, s);
       case 1632: return launch_pass<16, 32, DIR, MODE>(a, d, L, s);
       case 3232: return launch_pass<32, 32, DIR, MODE>(a, d, L, s);
+      case 608: return launch_pass<6, 8, DIR, MODE>(a, d, L, s);
+      case 812: return launch_pass<8, 12, DIR, MODE>(a, d, L, s);
+      case 1216: return launch_pass<12, 16, DIR, MODE>(a, d, L, s);
+      case 1624: return launch_pass<16, 24, DIR, MODE>(a, d, L, s);
+      case 2432: return launch_pass<24, 32, DIR, MODE>(a, d, L, s);
       default: break;
     }
   }

@@ -319,15 +319,22 @@ int deinterleave(const float2* in, long long n, float* re, float* im, cudaStream
 static void plan_free(mlg_plan_s* p) {
   if (!p) return;
   cudaSetDevice(p->device);
+  if (p->borrowed && p->stream) cudaStreamSynchronize(p->stream);  // the owner's stream stays alive
+  if (p->owner) --p->owner->n_borrowers;
   if (p->cg_graph) cudaGraphExecDestroy(p->cg_graph);
-  for (int d = 0; d < 3; ++d) fft_axis_free(p->ax[d]);
   csr_free_sign_copy(p->Gu_s);
   csr_free_sign_copy(p->Gut_s);
-  cudaFree(p->KFC);
-  cudaFree(p->KFCc);
-  cudaFree(p->grid);
-  cudaFree(p->bufA);
-  cudaFree(p->bufB);
+  if (!p->borrowed) {
+    for (int d = 0; d < 3; ++d) fft_axis_free(p->ax[d]);
+    cudaFree(p->KFC);
+    cudaFree(p->KFCc);
+    cudaFree(p->grid);
+    cudaFree(p->bufA);
+    cudaFree(p->bufB);
+    if (p->ev_in) cudaEventDestroy(p->ev_in);
+    if (p->ev_out) cudaEventDestroy(p->ev_out);
+    if (p->stream) cudaStreamDestroy(p->stream);
+  }
   cudaFree(p->partial);
   cudaFree(p->seg_scratch);
   cudaFree(p->scalars);
@@ -336,11 +343,10 @@ static void plan_free(mlg_plan_s* p) {
   cudaFree(p->k_res);
   cudaFree(p->k_Mp);
   cudaFree(p->HY);
-  if (p->ev_in) cudaEventDestroy(p->ev_in);
-  if (p->ev_out) cudaEventDestroy(p->ev_out);
-  if (p->stream) cudaStreamDestroy(p->stream);
   delete p;
 }
+
+void plan_destroy(mlg_plan_s* p) { plan_free(p); }
 
 // KFC / KFC_conj arrive as [prod(n_u), nCh] column layout (separate real and
 // imaginary parts, host memory) and are stored coil-fastest.
@@ -361,7 +367,7 @@ static int upload_kfc(const float* re, const float* im, long long nu, int nCh, f
 
 static int plan_create_impl(int imDim, const int* N_u, const int* n_u, int nCh, const Csr* Gu, const Csr* Gut,
                             const float* KFC_re, const float* KFC_im, const float* KFCc_re, const float* KFCc_im,
-                            mlg_plan_s** out) {
+                            mlg_plan_s** out, const mlg_plan_s* share = nullptr) {
   MLG_CHECK(out, "NULL output");
   *out = nullptr;
   MLG_CHECK(imDim >= 1 && imDim <= 3, "imDim must be 1, 2 or 3");
@@ -369,11 +375,15 @@ static int plan_create_impl(int imDim, const int* N_u, const int* n_u, int nCh, 
   MLG_CHECK(Gu || Gut, "at least one of Gu / Gut is needed");
   MLG_TRY(ensure_device());
   mlg_plan_s* p = new mlg_plan_s();
+  p->borrowed = share != nullptr;
   auto bail = [&](int status) {
     plan_free(p);
     return status;
   };
   cudaGetDevice(&p->device);
+  if (share && share->device != p->device)
+    return bail(fail(MLG_ERR_ARG, "the shared plan lives on device %d, the current device is %d", share->device,
+                     p->device));
   p->imDim = imDim;
   p->nCh = nCh;
   long long Nu = 1, nu = 1;
@@ -404,13 +414,21 @@ static int plan_create_impl(int imDim, const int* N_u, const int* n_u, int nCh, 
   p->Gu = Gu;
   p->Gut = Gut;
   int st = MLG_OK;
-  for (int d = 0; d < imDim; ++d)
-    if ((st = fft_axis_init(p->N[d], p->ax[d])) != MLG_OK) return bail(st);
-  if (cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaEventCreateWithFlags(&p->ev_in, cudaEventDisableTiming) != cudaSuccess ||
-      cudaEventCreateWithFlags(&p->ev_out, cudaEventDisableTiming) != cudaSuccess) {
-    cudaGetLastError();
-    return bail(fail(MLG_ERR_CUDA, "stream/event creation failed"));
+  if (share) {
+    for (int d = 0; d < 3; ++d) p->ax[d] = share->ax[d];
+    p->stream = share->stream;
+    p->ev_in = share->ev_in;
+    p->ev_out = share->ev_out;
+    p->HX = share->HX;
+  } else {
+    for (int d = 0; d < imDim; ++d)
+      if ((st = fft_axis_init(p->N[d], p->ax[d])) != MLG_OK) return bail(st);
+    if (cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&p->ev_in, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&p->ev_out, cudaEventDisableTiming) != cudaSuccess) {
+      cudaGetLastError();
+      return bail(fail(MLG_ERR_CUDA, "stream/event creation failed"));
+    }
   }
   cudaStream_t s = p->stream;
   if (Gu && (st = csr_sign_copy(*Gu, false, imDim, p->N, sc, p->Gu_s, s)) != MLG_OK) return bail(st);
@@ -423,14 +441,22 @@ static int plan_create_impl(int imDim, const int* N_u, const int* n_u, int nCh, 
   const size_t gbytes = sizeof(float2) * (size_t)Nu * nCh;
   const size_t abytes = sizeof(float2) * (size_t)p->N[0] * p->n[1] * p->n[2] * nCh;
   const size_t bbytes = sizeof(float2) * (size_t)p->N[0] * p->N[1] * p->n[2] * nCh;
-  if (cudaMalloc(&p->KFC, kbytes) != cudaSuccess || cudaMalloc(&p->KFCc, kbytes) != cudaSuccess ||
-      cudaMalloc(&p->grid, gbytes) != cudaSuccess || cudaMalloc(&p->bufA, abytes) != cudaSuccess ||
-      cudaMalloc(&p->bufB, bbytes) != cudaSuccess) {
-    cudaGetLastError();
-    return bail(fail(MLG_ERR_OOM, "plan: device allocation failed"));
+  if (share) {
+    p->KFC = share->KFC;
+    p->KFCc = share->KFCc;
+    p->grid = share->grid;
+    p->bufA = share->bufA;
+    p->bufB = share->bufB;
+  } else {
+    if (cudaMalloc(&p->KFC, kbytes) != cudaSuccess || cudaMalloc(&p->KFCc, kbytes) != cudaSuccess ||
+        cudaMalloc(&p->grid, gbytes) != cudaSuccess || cudaMalloc(&p->bufA, abytes) != cudaSuccess ||
+        cudaMalloc(&p->bufB, bbytes) != cudaSuccess) {
+      cudaGetLastError();
+      return bail(fail(MLG_ERR_OOM, "plan: device allocation failed"));
+    }
+    if ((st = upload_kfc(KFC_re, KFC_im, nu, nCh, p->KFC, s)) != MLG_OK) return bail(st);
+    if ((st = upload_kfc(KFCc_re, KFCc_im, nu, nCh, p->KFCc, s)) != MLG_OK) return bail(st);
   }
-  if ((st = upload_kfc(KFC_re, KFC_im, nu, nCh, p->KFC, s)) != MLG_OK) return bail(st);
-  if ((st = upload_kfc(KFCc_re, KFCc_im, nu, nCh, p->KFCc, s)) != MLG_OK) return bail(st);
   // partial-sum buffer: the largest CTA count any fused reduction uses
   PassDesc last;
   last.ax = 0;
@@ -456,9 +482,20 @@ static int plan_create_impl(int imDim, const int* N_u, const int* n_u, int nCh, 
     return bail(fail(MLG_ERR_OOM, "plan: partial buffer allocation failed"));
   }
   if (cudaStreamSynchronize(s) != cudaSuccess) return bail(fail(MLG_ERR_CUDA, "plan creation failed"));
-  p->bytes = 2 * kbytes + gbytes + abytes + bbytes +
-             sizeof(float) * (size_t)((Gu ? Gu->nnz : 0) + (Gut ? Gut->nnz : 0)) + sizeof(double) * (cap + 64);
+  p->bytes = (share ? 0 : 2 * kbytes + gbytes + abytes + bbytes) +
+             sizeof(float) * (size_t)((Gu ? Gu->nnz : 0) + (Gut ? Gut->nnz : 0)) + sizeof(double) * (cap + 64) +
+             sizeof(float) * seg_floats;
   *out = p;
+  return MLG_OK;
+}
+
+int plan_create_sharing(const mlg_plan_s* base, const Csr* Gu, const Csr* Gut, mlg_plan_s** out) {
+  MLG_CHECK(base && out, "NULL argument");
+  MLG_CHECK(!base->borrowed, "share the plan that owns the buffers, not a plan that borrows them");
+  MLG_TRY(plan_create_impl(base->imDim, base->N, base->n, base->nCh, Gu, Gut, nullptr, nullptr, nullptr, nullptr, out,
+                           base));
+  (*out)->owner = const_cast<mlg_plan_s*>(base);
+  ++(*out)->owner->n_borrowers;
   return MLG_OK;
 }
 
@@ -491,8 +528,17 @@ int mlg_plan_create(int imDim, const int* N_u, const int* n_u, int nCh, mlg_matr
 }
 
 int mlg_plan_destroy(mlg_plan_t p) {
+  if (p && p->n_borrowers > 0)
+    return fail(MLG_ERR_STATE, "%d plan(s) still borrow this plan's buffers: destroy them first", p->n_borrowers);
   plan_free(p);
   return MLG_OK;
+}
+
+int mlg_plan_create_sharing(mlg_plan_t base, mlg_matrix_t Gu, mlg_matrix_t Gut, mlg_plan_t* out) {
+  MLG_CHECK(base && out, "NULL argument");
+  MLG_CHECK(Gu || Gut, "at least one of Gu / Gut is needed");
+  MLG_CUDA(cudaSetDevice(base->device));
+  return plan_create_sharing(base, Gu ? &Gu->csr : nullptr, Gut ? &Gut->csr : nullptr, out);
 }
 
 int mlg_plan_device_bytes(mlg_plan_t p, long long* bytes) {

@@ -50,6 +50,12 @@ struct mlg_plan_s {
   cudaGraphExec_t cg_graph = nullptr;
   const void* cg_graph_x = nullptr;  // solution buffer baked into the graph
   long long cg_graph_kernels = 0;
+  // A plan created from another one (same grid, image, coils and KFC, other
+  // matrices) borrows that plan's KFC, KFCc, grid, bufA, bufB, FFT tables,
+  // stream and events; both then run in the order of that one stream.
+  bool borrowed = false;
+  mlg_plan_s* owner = nullptr;  // the plan whose buffers are borrowed
+  int n_borrowers = 0;          // plans borrowing this one's buffers
 };
 
 namespace mlg {
@@ -68,6 +74,9 @@ int nakatsha_run(mlg_plan_s* p, const float2* y, const float* HY, float scale, f
                  int* n_partial, cudaStream_t s);
 int sensa_run(mlg_plan_s* p, const float2* y, const float* ve, float ve_max, int nIter, int nCGD, float2* x,
               double* residual, bool use_graph, cudaStream_t s);
+// a plan over other matrices that borrows base's buffers (see `borrowed`)
+int plan_create_sharing(const mlg_plan_s* base, const Csr* Gu, const Csr* Gut, mlg_plan_s** out);
+void plan_destroy(mlg_plan_s* p);
 
 // layout conversions (mlg_nufft.cu)
 int pack_col_to_point(const float* re, const float* im, long long rows, int nCh, float2* out, cudaStream_t s);

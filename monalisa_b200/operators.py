@@ -113,6 +113,25 @@ class NufftPlan:
         if dK_u is not None:
             N.call("mlg_plan_set_dk", self._h, N.dptr(np.ascontiguousarray(np.ravel(dK_u), np.float64)))
 
+    @classmethod
+    def sharing(cls, base: "NufftPlan", Gu, Gut):
+        """A plan over other matrices on base's grid that borrows base's KFC,
+        grid buffers, FFT tables and stream (mlg_plan_create_sharing)."""
+        if isinstance(Gu, bmSparseMat):
+            Gu = Gu.to_device()
+        if isinstance(Gut, bmSparseMat):
+            Gut = Gut.to_device()
+        self = cls.__new__(cls)
+        self.N_u, self.n_u, self.imDim, self.nCh = base.N_u, base.n_u, base.imDim, base.nCh
+        self._keep = [Gu, Gut]
+        self._base = base  # outlives this plan
+        self.nPt = Gu.l_size if Gu is not None else Gut.r_size
+        h = ctypes.c_void_p()
+        N.call("mlg_plan_create_sharing", base.handle, Gu.handle if Gu is not None else None,
+               Gut.handle if Gut is not None else None, ctypes.byref(h))
+        self._h = h
+        return self
+
     @property
     def handle(self):
         return self._h

@@ -168,20 +168,20 @@ def coil_maps(n_u, nCh, seed):
     """Smooth random complex sensitivities [prod(n_u), nCh] (complex64)."""
     rng = np.random.default_rng(seed)
     n_u = [int(v) for v in np.ravel(n_u)]
+    d = len(n_u)
     axes = [np.linspace(-0.5, 0.5, n) for n in n_u]
-    P = [lambda x: np.ones_like(x), lambda x: x, lambda x: 0.5 * (3 * x ** 2 - 1)]
-    grids = np.meshgrid(*axes, indexing="ij")
-    basis = []
-    idx = np.stack(np.meshgrid(*([np.arange(3)] * len(n_u)), indexing="ij"), -1).reshape(-1, len(n_u))
-    for combo in idx:
-        b = np.ones(grids[0].shape)
-        for d, k in enumerate(combo):
-            b = b * P[k](grids[d])
-        basis.append(b.ravel(order="F"))
-    B = np.stack(basis, 1)  # [prod(n_u), 3^d]
-    out = np.zeros((B.shape[0], nCh), np.complex64)
+    # Legendre polynomials of degree 0..2 along each axis: the tensor basis
+    # P_k0(x) P_k1(y) P_k2(z) is evaluated separably
+    P1 = [np.stack([np.ones_like(a), a, 0.5 * (3 * a ** 2 - 1)], 1) for a in axes]  # [n_d, 3]
+    sub = "xyz"[:d]
+    expr = "".join("ijk"[:d]) + "," + ",".join(f"{sub[k]}{'ijk'[k]}" for k in range(d)) + "->" + sub
+    out = np.zeros((int(np.prod(n_u)), nCh), np.complex64)
+
+    def field_of(coef):  # coefficients in the order of the basis index (k0, k1, k2), last fastest
+        return np.einsum(expr, coef.reshape((3,) * d), *P1, optimize=True).ravel(order="F")
+
     for c in range(nCh):
-        m = B @ rng.standard_normal(B.shape[1]) + 1j * (B @ rng.standard_normal(B.shape[1]))
+        m = field_of(rng.standard_normal(3 ** d)) + 1j * field_of(rng.standard_normal(3 ** d))
         mag = np.abs(m)
         mag = mag * (1 / (mag.max() - mag.min()))
         out[:, c] = (mag * np.exp(1j * np.angle(m))).astype(np.complex64)

@@ -68,3 +68,66 @@ def radial2d(n=256, oversampling=2, nSpoke=256, nRead=512, nCh=1, nCGD=20, seed=
     w.info = dict(image=f"{n}^2", grid=f"{N}^2", spokes=nSpoke, samples_per_spoke=nRead, coils=nCh,
                   kernel="kaiser nWin=3 tau=1.95 alpha=10", iterations=nCGD, seed=seed)
     return w
+
+
+@dataclass
+class BinnedWorkload:
+    """Frame bins of one temporal reconstruction: per-bin trajectories t[f],
+    volume elements ve[f] and phantoms x_true[f]; one coil set C."""
+    name: str
+    n_u: np.ndarray
+    N_u: np.ndarray
+    dK_u: np.ndarray
+    nCh: int
+    kernelType: str
+    nWin: int
+    kernelParam: list
+    delta: float
+    rho: float
+    nIter: int
+    nCGD: int
+    t: list = field(default_factory=list)
+    ve: list = field(default_factory=list)
+    x_true: list = field(default_factory=list)
+    C: np.ndarray = None
+    info: dict = field(default_factory=dict)
+
+    @property
+    def nFr(self) -> int:
+        return len(self.t)
+
+    @property
+    def nPt(self) -> list:
+        return [int(t.shape[1]) for t in self.t]
+
+
+def koosh3d_bins(n=96, oversampling=2, nFr=20, spokes=(200, 1500), nRead=256, nCh=12, nIter=30, nCGD=5,
+                 seed=3) -> BinnedWorkload:
+    """3-D koosh-ball frame bins: bin f takes rng.integers(200, 1501) spokes,
+    the next run of one spiral-phyllotaxis sequence (continuing its counter,
+    directions spread over the whole sequence's angular range), 256 samples
+    per spoke; 96^3 image, 192^3 grid, 12 coils; temporal-TV ADMM with
+    delta = 0.01, rho = 10 delta, 30 iterations of 5 CG steps.  The phantom's
+    ellipsoids drift and pulse from bin to bin."""
+    N = n * oversampling
+    rng = np.random.default_rng(seed)
+    counts = rng.integers(spokes[0], spokes[1] + 1, nFr)
+    total = int(counts.sum())
+    w = BinnedWorkload("koosh3d_bins", np.array([n] * 3), np.array([N] * 3), np.ones(3), nCh, "gauss", 3, [0.61, 10],
+                       0.01, 0.1, nIter, nCGD)
+    w.C = T.coil_maps(w.n_u, nCh, seed)
+    base = T.ellipsoid_phantom(w.n_u, 10, seed + 100)
+    counter = 1
+    for f, ns in enumerate(counts):
+        t = T.bmTraj_fullRadial3_phyllotaxis_lineAssym2(nRead, int(ns), 1, N / nRead, counter_start=counter,
+                                                        q_segments=total)
+        counter += int(ns)
+        w.t.append(t)
+        w.ve.append(T.bmVolumeElement_full_radial3(t))
+        phase = 2 * np.pi * f / nFr
+        w.x_true.append((base * (1 + 0.2 * np.sin(phase))
+                         + 0.3 * T.ellipsoid_phantom(w.n_u, 1, seed + 200 + f)).astype(np.complex64))
+    w.info = dict(image=f"{n}^3", grid=f"{N}^3", bins=nFr, spokes_per_bin=[int(c) for c in counts],
+                  samples_per_spoke=nRead, coils=nCh, kernel="gauss nWin=3 sigma=0.61", admm_iterations=nIter,
+                  cg_steps=nCGD, delta=0.01, rho=0.1, seed=seed)
+    return w

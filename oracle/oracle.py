@@ -716,10 +716,13 @@ def prox_one_norm(w, s):
 
 
 def bmTevaMorphosia_chain(x, y, ve, C, Gu, Gut, n_u, delta, rho, nCGD, ve_max, nIter, spmv=None,
-                          workers=None, history=None):
-    """bmTevaMorphosia_chain.m:6-291, 'normal' mode, Tu = Tut = [] (identity
-    deformation), z and u initialised as in :75-81.  x, y, ve, Gu, Gut are
-    lists over frames."""
+                          workers=None, history=None, regul_mode="normal"):
+    """bmTevaMorphosia_chain.m:6-291, Tu = Tut = [] (identity deformation),
+    z and u initialised as in :75-81.  x, y, ve, Gu, Gut are lists over
+    frames.  regul_mode 'normal' takes delta / rho from their lists (:104-106);
+    'adapt' sets delta = delta_list(c) * regul / dafi and rho = rho_list(c) *
+    delta from the latest monitoring (:107-109, private_adapt_delta_rho
+    :240-248), the first one taken on the initial x (:86)."""
     myEps = 10 * np.finfo(np.float32).eps
     nFr = len(y)
     nCh = y[0].shape[1]
@@ -748,8 +751,21 @@ def bmTevaMorphosia_chain(x, y, ve, C, Gu, Gut, n_u, delta, rho, nCGD, ve_max, n
         np.linspace(abs(delta[0]), abs(delta[1]), nIter).astype(np.float32)
     rl = np.full(nIter, np.float32(abs(rho)), np.float32) if np.isscalar(rho) else \
         np.linspace(abs(rho[0]), abs(rho[1]), nIter).astype(np.float32)
+
+    def dafi_regul(x):  # private_dafi_regul (:211-224)
+        dafi = sum(_dot(yy - m, yy - m, HY[i]) for i, (yy, m) in enumerate(zip(y, Mop(x))))
+        regul = 0.0
+        for i in range(nFr):
+            tr = x[(i - 1) % nFr] - x[i]
+            regul += HZ * float(np.sum(np.abs(tr.real), dtype=np.float64) + np.sum(np.abs(tr.imag), dtype=np.float64))
+        return dafi, regul
+
+    dafi, regul = dafi_regul(x) if regul_mode == "adapt" else (None, None)
     for c in range(nIter):
         dlt, r = float(dl[c]), float(rl[c])
+        if regul_mode == "adapt":
+            dlt = float(np.float32(dlt * regul / dafi))
+            r = float(np.float32(r * dlt))
         res_y = [y[i] - m for i, m in enumerate(Mop(x))]
         Fx = Fop(x)
         res_z = [(z[i] - u[i]) - Fx[i] for i in range(nFr)]
@@ -780,13 +796,10 @@ def bmTevaMorphosia_chain(x, y, ve, C, Gu, Gut, n_u, delta, rho, nCGD, ve_max, n
         Fxu = [(u[i] + Fx[i]).astype(np.complex64) for i in range(nFr)]
         z = [prox_one_norm(v, dlt / r) for v in Fxu]
         u = [(Fxu[i] - z[i]).astype(np.complex64) for i in range(nFr)]
-        if history is not None:
-            dafi = sum(_dot(yy - m, yy - m, HY[i]) for i, (yy, m) in enumerate(zip(y, Mop(x))))
-            regul = 0.0
-            for i in range(nFr):
-                tr = x[(i - 1) % nFr] - x[i]
-                regul += HZ * float(np.sum(np.abs(tr.real), dtype=np.float64) + np.sum(np.abs(tr.imag), dtype=np.float64))
-            history.append((0.5 * dafi + 0.5 * dlt * regul, dafi, regul))
+        if history is not None or regul_mode == "adapt":
+            dafi, regul = dafi_regul(x)
+            if history is not None:
+                history.append((0.5 * dafi + 0.5 * dlt * regul, dafi, regul))
     return [xi.ravel() for xi in x]
 
 
