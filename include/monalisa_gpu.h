@@ -336,6 +336,27 @@ int mlg_tevamorphosia(mlg_chain_t c, const float* yR, const float* yI,
                       const float* rho, int regul_mode, int nIter, int nCGD,
                       float* xR, float* xI, double* history);
 
+/* Spatial-TV ADMM of one image,
+ * src/fourier123/solver_function/imDim/nonCartesian/bmSteva.m:6-138, on a
+ * chain of one frame:
+ *   min 0.5 |y - M x|^2_HY + delta |G x|_1
+ * with G the backward gradient along each image axis scaled by 1/dX_u
+ * (src/optim/bmBackGradient_n.m).  Device buffers: y [nPt][nCh], ve [nPt],
+ * x [prod(n_u)] in/out, z, u [imDim][prod(n_u)] in/out (set to G x and 0
+ * first when init_zu).  ve_max <= 0 means max(ve) (bmSteva.m:25-27).
+ * delta, rho as for mlg_tevamorphosia_dev.  history (host, may be NULL)
+ * receives per iteration {R = |y - Mx|^2_HY, TV = HZ |G x|_1}
+ * (bmSteva.m:117-125). */
+int mlg_steva_dev(mlg_chain_t c, const void* y, const float* ve, float ve_max,
+                  const float* delta, const float* rho, int nIter, int nCGD,
+                  void* x, void* z, void* u, int init_zu, double* history,
+                  void* stream);
+/* Same with host buffers: yR/yI [nPt, nCh] column-major, ve [nPt], xR/xI
+ * [prod(n_u)] in/out; z and u start as G x and 0. */
+int mlg_steva(mlg_chain_t c, const float* yR, const float* yI, const float* ve,
+              float ve_max, const float* delta, const float* rho, int nIter,
+              int nCGD, float* xR, float* xI, double* history);
+
 #if defined(__GNUC__)
 #pragma GCC visibility pop
 #endif

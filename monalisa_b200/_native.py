@@ -70,6 +70,8 @@ SIGNATURES = {
     "mlg_tevamorphosia_dev": [c_vp, c_vp, P_f, c_float, P_f, P_f, c_int, c_int, c_int, c_vp, c_vp, c_vp, c_int, P_d,
                               c_vp],
     "mlg_tevamorphosia": [c_vp, P_f, P_f, P_f, c_float, P_f, P_f, c_int, c_int, c_int, P_f, P_f, P_d],
+    "mlg_steva_dev": [c_vp, c_vp, P_f, c_float, P_f, P_f, c_int, c_int, c_vp, c_vp, c_vp, c_int, P_d, c_vp],
+    "mlg_steva": [c_vp, P_f, P_f, P_f, c_float, P_f, P_f, c_int, c_int, P_f, P_f, P_d],
 }
 _RESTYPE = {"mlg_status_string": ctypes.c_char_p, "mlg_last_error": ctypes.c_char_p,
             "mlg_kernel_launch_count": c_ll}

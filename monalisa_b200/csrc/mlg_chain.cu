@@ -1,6 +1,13 @@
-// Temporal-TV ADMM over frame bins on the device: the semantics of
-// src/fourier123/solver_function/imDim_morphosia/nonCartesian/
-// bmTevaMorphosia_chain.m:6-195 with Tu = Tut = [] (identity deformation).
+// TV-regularised ADMM reconstructions on the device:
+//  * temporal TV over frame bins, the semantics of
+//    src/fourier123/solver_function/imDim_morphosia/nonCartesian/
+//    bmTevaMorphosia_chain.m:6-195 with Tu = Tut = [] (identity deformation);
+//  * spatial TV of one image, the semantics of
+//    src/fourier123/solver_function/imDim/nonCartesian/bmSteva.m:6-138
+//    (a chain of one frame whose sparsifier is the backward gradient,
+//    src/optim/bmBackGradient_n.m / bmBackGradient_nT.m).
+// Both share the CG/ADMM skeleton below; bmTevaMorphosia_chain.m line
+// numbers are cited as ":n", bmSteva.m ones by name.
 //
 // Frame f has its own trajectory (plan f: Gu{f}, Gut{f}, k-space rows
 // y{f}, weights ve{f}); all frames share the grid, image size, coils and KFC.
@@ -25,18 +32,31 @@
 
 #include "mlg_plan.cuh"
 
+// image geometry of the spatial sparsifier: extents, element strides and
+// pixel sizes dX_u along each axis (column-major image)
+struct ImGeom {
+  int dim = 1;
+  int n[3] = {1, 1, 1};
+  long long st[3] = {1, 1, 1};
+  float dX[3] = {1.f, 1.f, 1.f};
+};
+
 struct mlg_chain_s {
   int device = 0;
   int nFr = 0;
   int nCh = 1;
   long long nu = 0;                 // pixels per frame
+  ImGeom geom;
+  long long nd_cap = 0;             // rows of the dual arrays: max(nFr, imDim)
+  bool spatial = false;             // the run in progress: bmSteva (true) or the temporal chain
   std::vector<mlg_plan_s*> fr;      // caller's plans, one per frame
   std::vector<long long> row_off;   // first k-space row of each frame
   long long rows = 0;               // sum of nPt over frames
   double HX = 1.0;
   // work arrays
-  float2 *p = nullptr, *dA = nullptr, *res_z = nullptr, *Fp = nullptr;  // [nFr][nu]
-  float2 *z = nullptr, *u = nullptr;                                      // host-API z, u
+  float2 *p = nullptr, *dA = nullptr;                                     // [nFr][nu]
+  float2 *res_z = nullptr, *Fp = nullptr;                                 // [nd_cap][nu]
+  float2 *z = nullptr, *u = nullptr;                                      // host-API z, u [nd_cap][nu]
   float2 *res_y = nullptr, *Mp = nullptr;                                 // [rows][nCh]
   float* HY = nullptr;                                                    // [rows]
   double* partial = nullptr;
@@ -48,7 +68,7 @@ struct mlg_chain_s {
   cudaEvent_t ev_in = nullptr, ev_out = nullptr;
   cudaGraphExec_t graph = nullptr;
   const void* graph_key[4] = {nullptr, nullptr, nullptr, nullptr};
-  std::vector<int> graph_modes;     // the frames' adjoint strategies it was captured with
+  std::vector<int> graph_modes;     // sparsifier and the frames' adjoint strategies it was captured with
   long long graph_kernels = 0;
 };
 
@@ -298,10 +318,12 @@ __global__ void tv_regul_kernel(const float2* __restrict__ x, int nFr, long long
   if (threadIdx.x == 0) partial[blockIdx.x] = s;
 }
 
-// dafi, regul; objective = 0.5 dafi + 0.5 delta regul into hist[3c..3c+2]
-// (:174-179), or only the slots when hist is NULL (the initial monitoring)
+// dafi, regul; with hstride 3: objective = 0.5 dafi + 0.5 delta regul,
+// dafi, regul into hist[3c..3c+2] (:174-179); with hstride 2 (bmSteva.m:
+// 117-125): R, TV into hist[2c..2c+1].  Only the slots when hist is NULL
+// (the initial monitoring).
 __global__ void tv_monitor_kernel(const double* __restrict__ partial, int n_res, int n_reg, double HZ, double* sc,
-                                  double* hist) {
+                                  double* hist, int hstride) {
   const double dafi = sum_range(partial, 0, n_res);
   const double reg = HZ * sum_range(partial, n_res, n_res + n_reg);
   if (threadIdx.x == 0) {
@@ -309,12 +331,124 @@ __global__ void tv_monitor_kernel(const double* __restrict__ partial, int n_res,
     sc[T_REGUL] = reg;
     if (hist) {
       const int c = (int)sc[T_ITER];
-      hist[3 * c] = 0.5 * dafi + 0.5 * sc[T_DELTA] * reg;
-      hist[3 * c + 1] = dafi;
-      hist[3 * c + 2] = reg;
+      double* h = hist + (size_t)hstride * c;
+      if (hstride == 3) *h++ = 0.5 * dafi + 0.5 * sc[T_DELTA] * reg;
+      h[0] = dafi;
+      h[1] = reg;
       sc[T_ITER] = c + 1;
     }
   }
+}
+
+// ---- spatial sparsifier (bmSteva) ---------------------------------------------
+// Backward differences along each image axis d (bmBackGradient_n.m:28-46):
+//   (G_d v)[i] = (v[i] - v[i - e_d]) / dX_d, 0 on the first slice along d;
+// the transposed form the solver uses (bmBackGradient_nT.m:23-44):
+//   (T_d h)[i] = (h[i] (0 on the first slice) - h[i + e_d, circular]) / dX_d.
+__device__ __forceinline__ int axis_pos(long long i, const ImGeom& g, int d) {
+  return (int)((i / g.st[d]) % g.n[d]);
+}
+
+__device__ __forceinline__ float2 bgrad(const float2* __restrict__ v, long long i, const ImGeom& g, int d) {
+  if (axis_pos(i, g, d) == 0) return make_float2(0.f, 0.f);
+  const float2 t = csub(v[i], v[i - g.st[d]]);
+  return make_float2(__fdiv_rn(t.x, g.dX[d]), __fdiv_rn(t.y, g.dX[d]));
+}
+
+// z_d = G_d x, u = 0   (bmSteva.m:40-45)
+__global__ void st_init_zu_kernel(const float2* __restrict__ x, long long nu, ImGeom g, float2* __restrict__ z,
+                                  float2* __restrict__ u) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nu; i += (long long)gridDim.x * blockDim.x)
+    for (int d = 0; d < g.dim; ++d) {
+      z[d * nu + i] = bgrad(x, i, g, d);
+      u[d * nu + i] = make_float2(0.f, 0.f);
+    }
+}
+
+// res_z = (z - u) - G x   (bmSteva.m:58)
+__global__ void st_res_z_kernel(const float2* __restrict__ x, const float2* __restrict__ z,
+                                const float2* __restrict__ u, long long nu, ImGeom g, float2* __restrict__ res_z) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nu; i += (long long)gridDim.x * blockDim.x)
+    for (int d = 0; d < g.dim; ++d) res_z[d * nu + i] = csub(csub(z[d * nu + i], u[d * nu + i]), bgrad(x, i, g, d));
+}
+
+// dA = dA + (rho (1/HX)) sum_d T_d(HZ res_z_d), dA holding (1/HX) M*(HY res_y)
+// (bmSteva.m:60-63); partials of |dA|^2
+__global__ void st_dA_kernel(float2* __restrict__ dA, const float2* __restrict__ res_z, long long nu, ImGeom g,
+                             float HZ, float invHX, const double* __restrict__ sc, double* __restrict__ partial) {
+  const float s = __fmul_rn((float)sc[T_RHO], invHX);
+  double acc = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nu; i += (long long)gridDim.x * blockDim.x) {
+    float2 t = make_float2(0.f, 0.f);
+    for (int d = 0; d < g.dim; ++d) {
+      const int pos = axis_pos(i, g, d);
+      const long long nxt = pos == g.n[d] - 1 ? i - (long long)(g.n[d] - 1) * g.st[d] : i + g.st[d];
+      const float2 hi = res_z[d * nu + i], hn = res_z[d * nu + nxt];
+      const float2 a = pos == 0 ? make_float2(0.f, 0.f) : make_float2(__fmul_rn(HZ, hi.x), __fmul_rn(HZ, hi.y));
+      const float2 b = make_float2(__fmul_rn(HZ, hn.x), __fmul_rn(HZ, hn.y));
+      const float2 q = csub(a, b);
+      t = cadd(t, make_float2(__fdiv_rn(q.x, g.dX[d]), __fdiv_rn(q.y, g.dX[d])));
+    }
+    const float2 v = cadd(dA[i], make_float2(__fmul_rn(s, t.x), __fmul_rn(s, t.y)));
+    dA[i] = v;
+    acc += nrm2(v);
+  }
+  const double r = block_sum(acc);
+  if (threadIdx.x == 0) partial[blockIdx.x] = r;
+}
+
+// Fp_d = G_d p with partials of |Fp|^2   (bmSteva.m:83)
+__global__ void st_Fp_kernel(const float2* __restrict__ p, long long nu, ImGeom g, float2* __restrict__ Fp,
+                             double* __restrict__ partial) {
+  double acc = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nu; i += (long long)gridDim.x * blockDim.x)
+    for (int d = 0; d < g.dim; ++d) {
+      const float2 v = bgrad(p, i, g, d);
+      Fp[d * nu + i] = v;
+      acc += nrm2(v);
+    }
+  const double r = block_sum(acc);
+  if (threadIdx.x == 0) partial[blockIdx.x] = r;
+}
+
+// bGx_plus_u = G x + u; z = prox(., delta/rho); u = bGx_plus_u - z   (bmSteva.m:112-114)
+__global__ void st_zu_kernel(const float2* __restrict__ x, long long nu, ImGeom g, float2* __restrict__ z,
+                             float2* __restrict__ u, const double* __restrict__ sc) {
+  const float s = fabsf(__fdiv_rn((float)sc[T_DELTA], (float)sc[T_RHO]));
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nu; i += (long long)gridDim.x * blockDim.x)
+    for (int d = 0; d < g.dim; ++d) {
+      const float2 w = cadd(bgrad(x, i, g, d), u[d * nu + i]);
+      const float2 zz = make_float2(soft(w.x, s), soft(w.y, s));
+      z[d * nu + i] = zz;
+      u[d * nu + i] = csub(w, zz);
+    }
+}
+
+// partials of sum_d |Re G_d x| + |Im G_d x|   (bmSteva.m:121-122)
+__global__ void st_regul_kernel(const float2* __restrict__ x, long long nu, ImGeom g, double* __restrict__ partial) {
+  double acc = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nu; i += (long long)gridDim.x * blockDim.x)
+    for (int d = 0; d < g.dim; ++d) {
+      const float2 t = bgrad(x, i, g, d);
+      acc += (double)fabsf(t.x) + (double)fabsf(t.y);
+    }
+  const double r = block_sum(acc);
+  if (threadIdx.x == 0) partial[blockIdx.x] = r;
+}
+
+// max over v[0..n) per CTA (grid-stride), then over the CTA results
+__global__ void vmax_kernel(const float* __restrict__ v, long long n, float* out) {
+  __shared__ float sh[kT];
+  float m = -FLT_MAX;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    m = fmaxf(m, v[i]);
+  sh[threadIdx.x] = m;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) sh[threadIdx.x] = fmaxf(sh[threadIdx.x], sh[threadIdx.x + w]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[blockIdx.x] = sh[0];
 }
 
 // ---- host side ---------------------------------------------------------------
@@ -363,8 +497,12 @@ static int chain_dagA(mlg_chain_s* c, bool first, cudaStream_t s) {
   const double eps = 10.0 * (double)FLT_EPSILON;
   MLG_TRY(chain_adjoint(c, c->res_y, c->dA, s));
   const int g = grid1(ni);
-  tv_dA_kernel<<<g, kT, 0, s>>>(c->dA, c->res_z, c->nFr, c->nu, (float)c->HX, (float)(1.0 / c->HX), c->sc,
-                                c->partial);
+  if (c->spatial)
+    st_dA_kernel<<<g, kT, 0, s>>>(c->dA, c->res_z, c->nu, c->geom, (float)c->HX, (float)(1.0 / c->HX), c->sc,
+                                  c->partial);
+  else
+    tv_dA_kernel<<<g, kT, 0, s>>>(c->dA, c->res_z, c->nFr, c->nu, (float)c->HX, (float)(1.0 / c->HX), c->sc,
+                                  c->partial);
   MLG_LAUNCHED();
   if (first)
     tv_sq_init_kernel<<<1, kT, 0, s>>>(c->partial, g, c->HX, eps, c->sc);
@@ -380,7 +518,10 @@ static int chain_cg_half(mlg_chain_s* c, float2* x, cudaStream_t s) {
   int n_mp = 0;
   MLG_TRY(chain_forward(c, c->p, c->Mp, c->HY, &n_mp, s));
   const int g = grid1(ni);
-  tv_Fp_kernel<<<g, kT, 0, s>>>(c->p, c->nFr, c->nu, c->Fp, c->partial + n_mp);
+  if (c->spatial)
+    st_Fp_kernel<<<g, kT, 0, s>>>(c->p, c->nu, c->geom, c->Fp, c->partial + n_mp);
+  else
+    tv_Fp_kernel<<<g, kT, 0, s>>>(c->p, c->nFr, c->nu, c->Fp, c->partial + n_mp);
   MLG_LAUNCHED();
   tv_alpha_kernel<<<1, kT, 0, s>>>(c->partial, n_mp, g, c->HX, c->sc);
   MLG_LAUNCHED();
@@ -391,11 +532,11 @@ static int chain_cg_half(mlg_chain_s* c, float2* x, cudaStream_t s) {
 
 // one full CG step j < nCGD (:128-161)
 static int chain_cg_step(mlg_chain_s* c, float2* x, cudaStream_t s) {
-  const long long ni = c->nu * c->nFr, nk = c->rows * c->nCh;
+  const long long ni = c->nu * c->nFr, nk = c->rows * c->nCh, nd = c->nu * (c->spatial ? c->geom.dim : c->nFr);
   MLG_TRY(chain_cg_half(c, x, s));
   tv_axpy_kernel<true><<<grid1(nk), kT, 0, s>>>(c->res_y, c->Mp, nk, c->sc);
   MLG_LAUNCHED();
-  tv_axpy_kernel<true><<<grid1(ni), kT, 0, s>>>(c->res_z, c->Fp, ni, c->sc);
+  tv_axpy_kernel<true><<<grid1(nd), kT, 0, s>>>(c->res_z, c->Fp, nd, c->sc);
   MLG_LAUNCHED();
   MLG_TRY(chain_dagA(c, false, s));
   tv_update_p_kernel<<<grid1(ni), kT, 0, s>>>(c->p, c->dA, ni, c->sc);
@@ -410,20 +551,39 @@ static int chain_monitor(mlg_chain_s* c, const float2* y, const float2* x, doubl
   const int gk = grid1(nk), gi = grid1(ni);
   tv_residual_kernel<<<gk, kT, 0, s>>>(y, c->Mp, nk, c->nCh, c->HY, c->res_y, c->partial);
   MLG_LAUNCHED();
-  tv_regul_kernel<<<gi, kT, 0, s>>>(x, c->nFr, c->nu, c->partial + gk);
+  if (c->spatial)
+    st_regul_kernel<<<gi, kT, 0, s>>>(x, c->nu, c->geom, c->partial + gk);
+  else
+    tv_regul_kernel<<<gi, kT, 0, s>>>(x, c->nFr, c->nu, c->partial + gk);
   MLG_LAUNCHED();
-  tv_monitor_kernel<<<1, kT, 0, s>>>(c->partial, gk, gi, c->HX, c->sc, hist);
+  tv_monitor_kernel<<<1, kT, 0, s>>>(c->partial, gk, gi, c->HX, c->sc, hist, c->spatial ? 2 : 3);
   MLG_LAUNCHED();
   return MLG_OK;
 }
 
-static int chain_run(mlg_chain_s* c, const float2* y, const float* ve, float ve_max, const float* delta,
-                     const float* rho, int adapt, int nIter, int nCGD, float2* x, float2* z, float2* u, bool init_zu,
-                     double* history, cudaStream_t s) {
+// spatial: bmSteva (one frame, dual arrays [imDim][nu]); else the temporal
+// chain (dual arrays [nFr][nu]).  ve_max <= 0 means max(ve).
+static int chain_run(mlg_chain_s* c, bool spatial, const float2* y, const float* ve, float ve_max,
+                     const float* delta, const float* rho, int adapt, int nIter, int nCGD, float2* x, float2* z,
+                     float2* u, bool init_zu, double* history, cudaStream_t s) {
   MLG_CHECK(nIter >= 0 && nCGD >= 0, "nIter / nCGD must be >= 0");
-  MLG_CHECK(ve_max > 0.f, "ve_max must be > 0");
   MLG_CHECK(delta && rho, "NULL delta / rho");
+  MLG_CHECK(!spatial || (c->nFr == 1 && !adapt), "the spatial solver runs on a chain of one frame, 'normal' mode");
+  c->spatial = spatial;
+  c->HX = c->fr[0]->HX;  // dK_u may have been set after the chain was made
+  for (int d = 0; d < c->geom.dim; ++d) c->geom.dX[d] = c->fr[0]->dX[d];
   const long long ni = c->nu * c->nFr;
+  const int hstride = spatial ? 2 : 3;
+  if (!(ve_max > 0.f)) {  // bmSteva.m:25-27
+    float* part = reinterpret_cast<float*>(c->partial);  // >= 64 doubles of room
+    float* dmax = part + 64;
+    vmax_kernel<<<32, kT, 0, s>>>(ve, c->rows, part);
+    MLG_LAUNCHED();
+    vmax_kernel<<<1, kT, 0, s>>>(part, 32, dmax);
+    MLG_LAUNCHED();
+    MLG_CUDA(cudaMemcpyAsync(&ve_max, dmax, sizeof(float), cudaMemcpyDeviceToHost, s));
+    MLG_CUDA(cudaStreamSynchronize(s));
+  }
   // delta / rho lists: linspace(first, last, nIter) (private_init_regul_param, :226-238)
   if (nIter > c->lists_cap) {
     cudaFree(c->lists);
@@ -444,19 +604,22 @@ static int chain_run(mlg_chain_s* c, const float2* y, const float* ve, float ve_
   tv_hy_kernel<<<grid1(c->rows), kT, 0, s>>>(ve, c->rows, ve_max, c->HY);
   MLG_LAUNCHED();
   if (init_zu) {
-    tv_init_zu_kernel<<<grid1(ni), kT, 0, s>>>(x, c->nFr, c->nu, z, u);
+    if (spatial)
+      st_init_zu_kernel<<<grid1(ni), kT, 0, s>>>(x, c->nu, c->geom, z, u);
+    else
+      tv_init_zu_kernel<<<grid1(ni), kT, 0, s>>>(x, c->nFr, c->nu, z, u);
     MLG_LAUNCHED();
   }
   MLG_CUDA(cudaMemsetAsync(c->sc, 0, sizeof(double) * T_COUNT, s));
   DevBuf<double> hist;
-  MLG_TRY(hist.alloc(3 * (size_t)std::max(1, nIter), s));
+  MLG_TRY(hist.alloc(hstride * (size_t)std::max(1, nIter), s));
   // initial monitoring: res_y = y - M x, dafi, regul (:86)
   MLG_TRY(chain_monitor(c, y, x, nullptr, s));
 
   const int full = std::max(0, nCGD - 1);
   auto ensure_graph = [&]() -> int {
     const void* key[4] = {x, z, u, y};
-    std::vector<int> modes;
+    std::vector<int> modes{spatial ? 1 : 0};
     for (const mlg_plan_s* p : c->fr) modes.push_back(p->adjoint_mode);
     if (full == 0 || (c->graph && std::equal(key, key + 4, c->graph_key) && modes == c->graph_modes)) return MLG_OK;
     if (c->graph) cudaGraphExecDestroy(c->graph);
@@ -482,7 +645,10 @@ static int chain_run(mlg_chain_s* c, const float2* y, const float* ve, float ve_
     tv_params_kernel<<<1, 1, 0, s>>>(c->lists, c->lists_cap, adapt, c->sc);
     MLG_LAUNCHED();
     // L_Aube (:116-123): res_y is the kept monitoring residual
-    tv_res_z_kernel<<<grid1(ni), kT, 0, s>>>(x, z, u, c->nFr, c->nu, c->res_z);
+    if (spatial)
+      st_res_z_kernel<<<grid1(ni), kT, 0, s>>>(x, z, u, c->nu, c->geom, c->res_z);
+    else
+      tv_res_z_kernel<<<grid1(ni), kT, 0, s>>>(x, z, u, c->nFr, c->nu, c->res_z);
     MLG_LAUNCHED();
     MLG_TRY(chain_dagA(c, true, s));
     MLG_CUDA(cudaMemcpyAsync(c->p, c->dA, sizeof(float2) * (size_t)ni, cudaMemcpyDeviceToDevice, s));
@@ -492,12 +658,15 @@ static int chain_run(mlg_chain_s* c, const float2* y, const float* ve, float ve_
       count_launch(c->graph_kernels);
     }
     if (nCGD > 0) MLG_TRY(chain_cg_half(c, x, s));  // the last step stops after x += a p (:148-150)
-    tv_zu_kernel<<<grid1(ni), kT, 0, s>>>(x, c->nFr, c->nu, z, u, c->sc);
+    if (spatial)
+      st_zu_kernel<<<grid1(ni), kT, 0, s>>>(x, c->nu, c->geom, z, u, c->sc);
+    else
+      tv_zu_kernel<<<grid1(ni), kT, 0, s>>>(x, c->nFr, c->nu, z, u, c->sc);
     MLG_LAUNCHED();
     MLG_TRY(chain_monitor(c, y, x, hist.p, s));
   }
   if (history && nIter > 0) {
-    MLG_CUDA(cudaMemcpyAsync(history, hist.p, sizeof(double) * 3 * nIter, cudaMemcpyDeviceToHost, s));
+    MLG_CUDA(cudaMemcpyAsync(history, hist.p, sizeof(double) * hstride * nIter, cudaMemcpyDeviceToHost, s));
     MLG_CUDA(cudaStreamSynchronize(s));
   }
   return MLG_OK;
@@ -531,6 +700,13 @@ int mlg_chain_create(int nFr, const mlg_plan_t* plans, mlg_chain_t* out) {
   c->nCh = p0->nCh;
   c->nu = p0->nu_tot;
   c->HX = p0->HX;
+  c->geom.dim = p0->imDim;
+  for (int d = 0; d < p0->imDim; ++d) {
+    c->geom.n[d] = p0->n[d];
+    c->geom.st[d] = d == 0 ? 1 : c->geom.st[d - 1] * p0->n[d - 1];
+    c->geom.dX[d] = p0->dX[d];
+  }
+  c->nd_cap = std::max(nFr, p0->imDim);
   int cap = 0;
   for (int f = 0; f < nFr; ++f) {
     c->fr.push_back(plans[f]);
@@ -542,11 +718,12 @@ int mlg_chain_create(int nFr, const mlg_plan_t* plans, mlg_chain_t* out) {
   cap = std::max(cap, grid1(nk) + grid1(ni)) + grid1(ni) + 64;
   c->partial_cap = cap;
   const size_t bi = sizeof(float2) * (size_t)ni, bk = sizeof(float2) * (size_t)std::max(1LL, nk);
+  const size_t bd = sizeof(float2) * (size_t)(c->nu * c->nd_cap);
   bool ok = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) == cudaSuccess &&
             cudaEventCreateWithFlags(&c->ev_in, cudaEventDisableTiming) == cudaSuccess &&
             cudaEventCreateWithFlags(&c->ev_out, cudaEventDisableTiming) == cudaSuccess;
   ok = ok && cudaMalloc(&c->p, bi) == cudaSuccess && cudaMalloc(&c->dA, bi) == cudaSuccess &&
-       cudaMalloc(&c->res_z, bi) == cudaSuccess && cudaMalloc(&c->Fp, bi) == cudaSuccess &&
+       cudaMalloc(&c->res_z, bd) == cudaSuccess && cudaMalloc(&c->Fp, bd) == cudaSuccess &&
        cudaMalloc(&c->res_y, bk) == cudaSuccess && cudaMalloc(&c->Mp, bk) == cudaSuccess &&
        cudaMalloc(&c->HY, sizeof(float) * (size_t)std::max(1LL, c->rows)) == cudaSuccess &&
        cudaMalloc(&c->partial, sizeof(double) * (size_t)cap) == cudaSuccess &&
@@ -573,35 +750,37 @@ int mlg_chain_info(mlg_chain_t c, int* nFr, long long* rows, long long* pixels) 
   return MLG_OK;
 }
 
-int mlg_tevamorphosia_dev(mlg_chain_t c, const void* y, const float* ve, float ve_max, const float* delta,
-                          const float* rho, int regul_mode, int nIter, int nCGD, void* x, void* z, void* u,
-                          int init_zu, double* history, void* stream) {
+}  // extern "C"
+
+namespace mlg {
+
+static int run_dev(mlg_chain_t c, bool spatial, const void* y, const float* ve, float ve_max, const float* delta,
+                   const float* rho, int adapt, int nIter, int nCGD, void* x, void* z, void* u, int init_zu,
+                   double* history, void* stream) {
   MLG_CHECK(c && y && ve && x && z && u, "NULL argument");
-  MLG_CHECK(regul_mode == MLG_REGUL_NORMAL || regul_mode == MLG_REGUL_ADAPT, "unknown regul_mode %d", regul_mode);
   MLG_CUDA(cudaSetDevice(c->device));
   cudaStream_t user = (cudaStream_t)stream;
   MLG_CUDA(cudaEventRecord(c->ev_in, user));
   MLG_CUDA(cudaStreamWaitEvent(c->stream, c->ev_in, 0));
   // the frames' plans may run on their own streams elsewhere: order them
   for (mlg_plan_s* p : c->fr) MLG_CUDA(cudaStreamWaitEvent(c->stream, p->ev_out, 0));
-  const int st = chain_run(c, (const float2*)y, ve, ve_max, delta, rho, regul_mode == MLG_REGUL_ADAPT, nIter, nCGD,
-                           (float2*)x, (float2*)z, (float2*)u, init_zu != 0, history, c->stream);
+  const int st = chain_run(c, spatial, (const float2*)y, ve, ve_max, delta, rho, adapt, nIter, nCGD, (float2*)x,
+                           (float2*)z, (float2*)u, init_zu != 0, history, c->stream);
   cudaEventRecord(c->ev_out, c->stream);
   cudaStreamWaitEvent(user, c->ev_out, 0);
   return st;
 }
 
-int mlg_tevamorphosia(mlg_chain_t c, const float* yR, const float* yI, const float* ve, float ve_max,
-                      const float* delta, const float* rho, int regul_mode, int nIter, int nCGD, float* xR, float* xI,
-                      double* history) {
+static int run_host(mlg_chain_t c, bool spatial, const float* yR, const float* yI, const float* ve, float ve_max,
+                    const float* delta, const float* rho, int adapt, int nIter, int nCGD, float* xR, float* xI,
+                    double* history) {
   MLG_CHECK(c && yR && yI && ve && xR && xI, "NULL argument");
-  MLG_CHECK(regul_mode == MLG_REGUL_NORMAL || regul_mode == MLG_REGUL_ADAPT, "unknown regul_mode %d", regul_mode);
   MLG_CUDA(cudaSetDevice(c->device));
   cudaStream_t s = c->stream;
   const long long nk = c->rows * c->nCh, ni = c->nu * c->nFr;
   if (!c->z) {
-    if (cudaMalloc(&c->z, sizeof(float2) * (size_t)ni) != cudaSuccess ||
-        cudaMalloc(&c->u, sizeof(float2) * (size_t)ni) != cudaSuccess) {
+    const size_t bd = sizeof(float2) * (size_t)(c->nu * c->nd_cap);
+    if (cudaMalloc(&c->z, bd) != cudaSuccess || cudaMalloc(&c->u, bd) != cudaSuccess) {
       cudaGetLastError();
       return fail(MLG_ERR_OOM, "chain: z/u allocation failed");
     }
@@ -625,14 +804,44 @@ int mlg_tevamorphosia(mlg_chain_t c, const float* yR, const float* yI, const flo
   }
   MLG_TRY(mlg::interleave(dx.p, dx.p + ni, ni, x2.p, s));
   for (mlg_plan_s* p : c->fr) MLG_CUDA(cudaStreamWaitEvent(s, p->ev_out, 0));
-  MLG_TRY(chain_run(c, y2.p, dve.p, ve_max, delta, rho, regul_mode == MLG_REGUL_ADAPT, nIter, nCGD, x2.p, c->z, c->u,
-                    true, history, s));
+  MLG_TRY(chain_run(c, spatial, y2.p, dve.p, ve_max, delta, rho, adapt, nIter, nCGD, x2.p, c->z, c->u, true, history,
+                    s));
   MLG_TRY(mlg::deinterleave(x2.p, ni, dx.p, dx.p + ni, s));
   MLG_CUDA(cudaMemcpyAsync(xR, dx.p, sizeof(float) * ni, cudaMemcpyDeviceToHost, s));
   MLG_CUDA(cudaMemcpyAsync(xI, dx.p + ni, sizeof(float) * ni, cudaMemcpyDeviceToHost, s));
   if (cudaStreamSynchronize(s) != cudaSuccess)
-    return fail(MLG_ERR_CUDA, "tevamorphosia failed: %s", cudaGetErrorString(cudaGetLastError()));
+    return fail(MLG_ERR_CUDA, "ADMM solver failed: %s", cudaGetErrorString(cudaGetLastError()));
   return MLG_OK;
+}
+
+}  // namespace mlg
+
+extern "C" {
+
+int mlg_tevamorphosia_dev(mlg_chain_t c, const void* y, const float* ve, float ve_max, const float* delta,
+                          const float* rho, int regul_mode, int nIter, int nCGD, void* x, void* z, void* u,
+                          int init_zu, double* history, void* stream) {
+  MLG_CHECK(regul_mode == MLG_REGUL_NORMAL || regul_mode == MLG_REGUL_ADAPT, "unknown regul_mode %d", regul_mode);
+  return run_dev(c, false, y, ve, ve_max, delta, rho, regul_mode == MLG_REGUL_ADAPT, nIter, nCGD, x, z, u, init_zu,
+                 history, stream);
+}
+
+int mlg_tevamorphosia(mlg_chain_t c, const float* yR, const float* yI, const float* ve, float ve_max,
+                      const float* delta, const float* rho, int regul_mode, int nIter, int nCGD, float* xR, float* xI,
+                      double* history) {
+  MLG_CHECK(regul_mode == MLG_REGUL_NORMAL || regul_mode == MLG_REGUL_ADAPT, "unknown regul_mode %d", regul_mode);
+  return run_host(c, false, yR, yI, ve, ve_max, delta, rho, regul_mode == MLG_REGUL_ADAPT, nIter, nCGD, xR, xI,
+                  history);
+}
+
+int mlg_steva_dev(mlg_chain_t c, const void* y, const float* ve, float ve_max, const float* delta, const float* rho,
+                  int nIter, int nCGD, void* x, void* z, void* u, int init_zu, double* history, void* stream) {
+  return run_dev(c, true, y, ve, ve_max, delta, rho, 0, nIter, nCGD, x, z, u, init_zu, history, stream);
+}
+
+int mlg_steva(mlg_chain_t c, const float* yR, const float* yI, const float* ve, float ve_max, const float* delta,
+              const float* rho, int nIter, int nCGD, float* xR, float* xI, double* history) {
+  return run_host(c, true, yR, yI, ve, ve_max, delta, rho, 0, nIter, nCGD, xR, xI, history);
 }
 
 }  // extern "C"

@@ -405,7 +405,10 @@ static int plan_create_impl(int imDim, const int* N_u, const int* n_u, int nCh, 
   p->nu_tot = nu;
   p->shift_const = sc;
   p->HX = 1.0;  // dK_u = 1 until mlg_plan_set_dk
-  for (int d = 0; d < imDim; ++d) p->HX = (double)((float)p->HX * (1.0f / (float)p->N[d]));
+  for (int d = 0; d < imDim; ++d) {
+    p->dX[d] = 1.0f / (float)p->N[d];
+    p->HX = (double)((float)p->HX * p->dX[d]);
+  }
   if (Gu && Gu->r_size != Nu) return bail(fail(MLG_ERR_ARG, "Gu has %d columns, prod(N_u) = %lld", Gu->r_size, Nu));
   if (Gut && Gut->l_size != Nu) return bail(fail(MLG_ERR_ARG, "Gut has %d rows, prod(N_u) = %lld", Gut->l_size, Nu));
   if (Gu && Gut && Gu->l_size != Gut->r_size)
@@ -420,6 +423,7 @@ static int plan_create_impl(int imDim, const int* N_u, const int* n_u, int nCh, 
     p->ev_in = share->ev_in;
     p->ev_out = share->ev_out;
     p->HX = share->HX;
+    for (int d = 0; d < 3; ++d) p->dX[d] = share->dX[d];
   } else {
     for (int d = 0; d < imDim; ++d)
       if ((st = fft_axis_init(p->N[d], p->ax[d])) != MLG_OK) return bail(st);

@@ -44,8 +44,9 @@ struct mlg_plan_s {
   float2 *x_p = nullptr, *x_dagM = nullptr, *k_res = nullptr, *k_Mp = nullptr;
   float* HY = nullptr;
   int solver_nPt = 0;
-  // HX = prod(dX_u), dX_u = (1/dK_u)/N_u (bmSensa.m:26-27)
+  // HX = prod(dX_u), dX_u = (1/dK_u)/N_u (bmSensa.m:26-27), single precision
   double HX = 1.0;
+  float dX[3] = {1.f, 1.f, 1.f};
   // captured inner CG step (replayed nCGD-1 times per outer iteration)
   cudaGraphExec_t cg_graph = nullptr;
   const void* cg_graph_x = nullptr;  // solution buffer baked into the graph

@@ -311,13 +311,15 @@ extern "C" {
 int mlg_plan_set_dk(mlg_plan_t p, const double* dK_u) {
   MLG_CHECK(p && dK_u, "NULL argument");
   double hx = 1.0;
+  float dx[3] = {1.f, 1.f, 1.f};
   for (int d = 0; d < p->imDim; ++d) {
     MLG_CHECK(dK_u[d] > 0, "dK_u must be > 0");
     // single-precision arithmetic of bmSensa.m:26-27
-    const float dx = (1.0f / (float)dK_u[d]) / (float)p->N[d];
-    hx = (double)((float)hx * dx);
+    dx[d] = (1.0f / (float)dK_u[d]) / (float)p->N[d];
+    hx = (double)((float)hx * dx[d]);
   }
   p->HX = hx;
+  for (int d = 0; d < 3; ++d) p->dX[d] = dx[d];
   return MLG_OK;
 }
 

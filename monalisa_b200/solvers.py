@@ -189,3 +189,31 @@ def bmTevaMorphosia_chain(x, z, u, y, ve, C, Gu, Gut, n_u, Tu, Tut, delta, rho, 
     out = r.run_host(y, ve, x, delta, rho, nIter, int(nCGD), ve_max, regul_mode, hist)
     r.close()
     return [o.reshape(n_u, order="F") for o in out]
+
+
+def bmSteva(x, z, u, y, ve, C, Gu, Gut, n_u, delta, rho, nCGD, ve_max=None, convCond=None, witnessInfo=None):
+    """Spatial-TV ADMM (bmSteva.m): a chain of one frame whose sparsifier is
+    the backward gradient.  x initial image [prod(n_u)], y [nPt, nCh], ve
+    [nPt]; z, u must be empty (they start as G x and 0, :40-45); delta, rho
+    scalars or (first, last) pairs.  Returns the image as an n_u block
+    (MATLAB order).  ``witnessInfo`` may be a list that receives (R, TV) per
+    iteration (:117-125)."""
+    if (z is not None and len(z)) or (u is not None and len(u)):
+        raise NotImplementedError("z / u start values are taken from x (pass empty z and u)")
+    r = TevaMorphosiaChain([Gu], [Gut], C, n_u)
+    nIter = _niter(convCond)
+    nu = int(np.prod(r.n_u))
+    y = np.asarray(y, np.complex64)
+    yR = np.ascontiguousarray(y.real.T, np.float32)
+    yI = np.ascontiguousarray(y.imag.T, np.float32)
+    xx = np.zeros(nu, np.complex64) if x is None else np.asarray(x, np.complex64).ravel(order="F")
+    xR = np.ascontiguousarray(xx.real, np.float32)
+    xI = np.ascontiguousarray(xx.imag, np.float32)
+    hist = np.zeros(2 * max(1, nIter), np.float64)
+    N.call("mlg_steva", r.handle, N.fptr(yR), N.fptr(yI), N.fptr(np.ascontiguousarray(np.ravel(ve), np.float32)),
+           float(ve_max or 0.0), N.fptr(r._pair(delta)), N.fptr(r._pair(rho)), int(nIter), int(nCGD), N.fptr(xR),
+           N.fptr(xI), N.dptr(hist))
+    r.close()
+    if isinstance(witnessInfo, list):
+        witnessInfo.extend(tuple(hist[2 * c:2 * c + 2]) for c in range(nIter))
+    return (xR + 1j * xI).astype(np.complex64).reshape(tuple(int(v) for v in np.ravel(n_u)), order="F")

@@ -715,6 +715,112 @@ def prox_one_norm(w, s):
     return st(w)
 
 
+def back_gradient(x, n_u, dX_u):
+    """bmBackGradient.m:6-17 / bmBackGradient_n.m:6-51: per axis n,
+    (x - circshift(x, e_n)) / dX_u(n) with the first slice along n zeroed.
+    x [prod(n_u)] -> [prod(n_u), imDim] (single)."""
+    n_u = [int(v) for v in np.ravel(n_u)]
+    dX_u = np.ravel(dX_u).astype(np.float32)
+    xb = np.asarray(x, np.complex64).reshape(n_u, order="F")
+    out = np.zeros((xb.size, len(n_u)), np.complex64)
+    for n in range(len(n_u)):
+        g = ((xb - np.roll(xb, 1, axis=n)) / dX_u[n]).astype(np.complex64)
+        idx = [slice(None)] * len(n_u)
+        idx[n] = 0
+        g[tuple(idx)] = 0
+        out[:, n] = g.ravel(order="F")
+    return out
+
+
+def back_gradient_T(g, n_u, dX_u):
+    """bmBackGradientT.m:6-17 / bmBackGradient_nT.m:6-47: sum over axes of
+    (g_n with its first slice zeroed - circshift(g_n, -e_n)) / dX_u(n); the
+    shifted term uses g_n before zeroing.  [prod(n_u), imDim] -> [prod(n_u)]."""
+    n_u = [int(v) for v in np.ravel(n_u)]
+    dX_u = np.ravel(dX_u).astype(np.float32)
+    g = np.asarray(g, np.complex64)
+    x = np.zeros(int(np.prod(n_u)), np.complex64)
+    for n in range(len(n_u)):
+        xb = g[:, n].reshape(n_u, order="F")
+        gz = xb.copy()
+        idx = [slice(None)] * len(n_u)
+        idx[n] = 0
+        gz[tuple(idx)] = 0
+        t = ((gz - np.roll(xb, -1, axis=n)) / dX_u[n]).astype(np.complex64)
+        x = (x + t.ravel(order="F")).astype(np.complex64)
+    return x
+
+
+def bmSteva(x, y, ve, C, Gu, Gut, n_u, delta, rho, nCGD, ve_max=None, nIter=1, spmv=None, workers=None,
+            history=None):
+    """bmSteva.m:6-138, spatial-TV ADMM with z, u initialised as in :40-45.
+    delta, rho: scalars or (first, last) of their per-iteration linspace
+    (private_init_delta_rho, :140-157).  history receives (R, TV) per
+    iteration (:117-125)."""
+    myEps = 10 * np.finfo(np.float32).eps
+    y = np.asarray(y, np.complex64)
+    nCh = y.shape[1]
+    N_u = np.ravel(Gu.N_u).astype(int)
+    n_u = np.ravel(n_u).astype(int)
+    imDim = N_u.size
+    dK_u = single(np.ravel(Gu.d_u)).astype(np.float64)
+    dX_u = ((np.float32(1) / dK_u.astype(np.float32)) / N_u.astype(np.float32)).astype(np.float32)
+    ve = np.asarray(ve, np.float32)
+    ve = np.broadcast_to(ve.reshape(-1, 1) if ve.ndim == 1 else ve, y.shape)
+    if ve_max is None:
+        ve_max = float(np.max(ve))
+    lin = lambda v: (np.full(nIter, np.float32(abs(v)), np.float32) if np.isscalar(v) else
+                     np.linspace(abs(v[0]), abs(v[1]), nIter).astype(np.float32))
+    dl, rl = lin(delta), lin(rho)
+    HX = np.float32(np.prod(dX_u))
+    HZ = HX
+    HY = np.minimum(ve, np.float32(ve_max)).astype(np.float32)
+    KFC = bmKF(C, N_u, n_u, dK_u, nCh, Gu.kernel_type, Gu.nWin, Gu.kernelParam)
+    KFC_conj = bmKF_conj(np.conj(C), N_u, n_u, dK_u, nCh, Gu.kernel_type, Gu.nWin, Gu.kernelParam)
+    x = np.asarray(x, np.complex64).ravel()
+    M = lambda v: bmShanna(v, Gu, KFC, n_u, spmv, workers)[:, :]
+    G = lambda v: back_gradient(v, n_u, dX_u)
+    GT = lambda g: back_gradient_T(g, n_u, dX_u)
+    dagM = lambda r: (np.float32(1 / HX) * bmNakatsha((HY * r).astype(np.complex64), Gut, KFC_conj, True, n_u,
+                                                       spmv, workers).ravel()).astype(np.complex64)
+    z = G(x)
+    u = np.zeros((x.size, imDim), np.complex64)
+    for c in range(nIter):
+        r = np.float32(rl[c])
+        s = np.float32(r * np.float32(1 / HX))
+        res_y = (y - M(x)).astype(np.complex64)
+        res_z = ((z - u) - G(x)).astype(np.complex64)
+        dA = (dagM(res_y) + s * GT((HZ * res_z).astype(np.complex64))).astype(np.complex64)
+        p = dA
+        sq_next = float(HX) * _dot(dA, dA)
+        for i in range(1, nCGD + 1):
+            res_y_c, res_z_c, sq_c, p_c = res_y, res_z, sq_next, p
+            if sq_c < myEps:
+                break
+            Mp = M(p_c)
+            Fp = G(p_c)
+            a = sq_c / (_dot(Mp, Mp, HY) + float(np.float32(r * HZ)) * _dot(Fp, Fp))
+            x = (x + np.float32(a) * p_c).astype(np.complex64)
+            if i == nCGD:
+                break
+            res_y = (res_y_c - np.float32(a) * Mp).astype(np.complex64)
+            res_z = (res_z_c - np.float32(a) * Fp).astype(np.complex64)
+            dA = (dagM(res_y) + s * GT((HZ * res_z).astype(np.complex64))).astype(np.complex64)
+            sq_next = float(HX) * _dot(dA, dA)
+            b = sq_next / sq_c
+            p = (dA + np.float32(b) * p_c).astype(np.complex64)
+        bGu = (G(x) + u).astype(np.complex64)
+        z = prox_one_norm(bGu, float(np.float32(dl[c] / r)))
+        u = (bGu - z).astype(np.complex64)
+        if history is not None:
+            tr = y - M(x)
+            R = _dot(tr, tr, HY)
+            g = G(x)
+            TV = float(HZ) * float(np.sum(np.abs(g.real), dtype=np.float64) + np.sum(np.abs(g.imag), dtype=np.float64))
+            history.append((R, TV))
+    return x
+
+
 def bmTevaMorphosia_chain(x, y, ve, C, Gu, Gut, n_u, delta, rho, nCGD, ve_max, nIter, spmv=None,
                           workers=None, history=None, regul_mode="normal"):
     """bmTevaMorphosia_chain.m:6-291, Tu = Tut = [] (identity deformation),

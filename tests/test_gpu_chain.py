@@ -170,3 +170,44 @@ def test_sharing_plans_match_own_plans(case):
     shared.close()
     base.close()
     own.close()
+
+
+@pytest.mark.parametrize("dims", [2, 3])
+def test_steva_matches_oracle(dims):
+    """Spatial-TV ADMM (bmSteva) vs the oracle: 2-D golden-angle radial and
+    3-D random samples, dK_u != 1 so the gradient's 1/dX_u scaling counts."""
+    import monalisa_b200 as mb
+    from monalisa_b200 import traj
+
+    rng = np.random.default_rng(40 + dims)
+    if dims == 2:
+        N_u, n_u, dK = np.array([48, 40]), np.array([24, 20]), np.array([0.5, 0.5])
+        t = traj.golden_angle_radial2(48, 40, 0.5)
+        ve = traj.bmVolumeElement_voronoi_full_radial2(t, 48).astype(np.float32)
+    else:
+        N_u, n_u, dK = np.array([24, 16, 20]), np.array([12, 8, 10]), np.array([1.0, 2.0, 1.0])
+        t = rng.uniform(-0.5, 0.5, (3, 6000)) * (N_u * dK)[:, None]
+        ve = rng.uniform(0.5, 1.5, 6000).astype(np.float32)
+    nCh = 4
+    C = traj.coil_maps(n_u, nCh, 5)
+    G = oracle.traj2sparsemat(t, ve, N_u, dK, "gauss", 3, KP)
+    KFC = oracle.bmKF(C, N_u, n_u, dK, nCh, "gauss", 3, KP)
+    xt = traj.ellipsoid_phantom(n_u, 3, 7)
+    y = oracle.bmShanna(xt, G["Gu"], KFC, n_u)
+    y = (y + 1e-2 * np.abs(y).mean() * (rng.standard_normal(y.shape) + 1j * rng.standard_normal(y.shape))
+         ).astype(np.complex64)
+    delta, rho, nIter, nCGD = (1e-4, 1e-3), 1e-2, 3, 4
+    ho = []
+    ref = oracle.bmSteva(np.zeros(int(np.prod(n_u)), np.complex64), y, ve, C, G["Gu"], G["Gut"], n_u, delta, rho,
+                         nCGD, None, nIter, history=ho)
+    conv = lambda M: mb.bmSparseMat(r_size=M.r_size, r_jump=M.r_jump, r_nJump=M.r_nJump, m_val=M.m_val,
+                                    l_size=M.l_size, l_jump=M.l_jump, l_nJump=M.l_nJump, N_u=N_u,
+                                    d_u=dK.astype(np.float32), kernel_type="gauss", nWin=3,
+                                    kernelParam=np.array(KP, np.float32))
+    h = []
+    out = mb.bmSteva(None, None, None, y, ve, C, conv(G["Gu"]), conv(G["Gut"]), n_u, delta, rho, nCGD, None, nIter, h)
+    assert rel(out.ravel(order="F"), ref) <= 1e-4
+    assert len(h) == nIter
+    for c in range(nIter):
+        for k in range(2):
+            assert abs(h[c][k] - ho[c][k]) <= 1e-4 * abs(ho[c][k]), (c, k)
