@@ -132,6 +132,86 @@ def algorithmic_bytes(w, Gu, Gut, nCh, adjoint):
     }
 
 
+class PlainGpuSensa:
+    """The comparison arm the metric names ("vs plain GPU"): CG-SENSE with
+    the reference's operators moved to the GPU as stock library calls and
+    nothing fused -- x .* KFC, zero-fill, fftshift(fftn(ifftshift)) by
+    torch.fft (cuFFT), Gu / Gut as cuSPARSE CSR products of the real
+    matrices with [cells, 2 nCh] float views, crop, .* KFC_conj, coil sum,
+    and bmSensa.m's CG loop with single-precision dot products and a host
+    check of the stopping test each step.  Not part of the library."""
+
+    def __init__(self, w, Gu, Gut, KFC, KFCc, dev):
+        import warnings
+
+        import torch
+
+        warnings.filterwarnings("ignore", message=".*[Ss]parse.*")
+        self.t = torch
+        self.dev = dev
+        self.n = [int(v) for v in w.n_u]
+        self.N = [int(v) for v in w.N_u]
+        self.nCh = int(w.nCh)
+
+        def csr(D):
+            indptr, indices, data = D.download().to_csr()
+            return torch.sparse_csr_tensor(torch.from_numpy(indptr.astype(np.int32)).to(dev),
+                                           torch.from_numpy(indices).to(dev), torch.from_numpy(data).to(dev),
+                                           size=(D.l_size, D.r_size))
+
+        self.Gu, self.Gut = csr(Gu), csr(Gut)
+        nu = int(np.prod(self.n))
+        self.KFC = torch.from_numpy(np.ascontiguousarray(np.asarray(KFC, np.complex64).reshape(nu, -1, order="F").T)).to(dev)
+        self.KFCc = torch.from_numpy(np.ascontiguousarray(np.asarray(KFCc, np.complex64).reshape(nu, -1, order="F").T)).to(dev)
+        self.dims = tuple(range(1, 1 + len(self.n)))
+        self.box = tuple(slice(N // 2 - n // 2, N // 2 - n // 2 + n) for N, n in zip(self.N[::-1], self.n[::-1]))
+
+    def M(self, x):
+        t, C = self.t, self.nCh
+        v = (self.KFC * x[None, :]).reshape(C, *self.n[::-1])
+        g = t.zeros((C, *self.N[::-1]), dtype=t.complex64, device=self.dev)
+        g[(slice(None),) + self.box] = v
+        g = t.fft.fftshift(t.fft.fftn(t.fft.ifftshift(g, dim=self.dims), dim=self.dims), dim=self.dims)
+        g = t.view_as_real(g.reshape(C, -1).T.contiguous()).reshape(-1, 2 * C)
+        return t.view_as_complex(t.sparse.mm(self.Gu, g).reshape(-1, C, 2).contiguous())
+
+    def MH(self, y, HY, scale):
+        t, C = self.t, self.nCh
+        yr = t.view_as_real((HY[:, None] * y).contiguous()).reshape(-1, 2 * C)
+        g = t.view_as_complex(t.sparse.mm(self.Gut, yr).reshape(-1, C, 2).contiguous())
+        g = g.T.reshape(C, *self.N[::-1])
+        g = t.fft.fftshift(t.fft.ifftn(t.fft.ifftshift(g, dim=self.dims), dim=self.dims), dim=self.dims)
+        v = g[(slice(None),) + self.box].reshape(C, -1)
+        return scale * (self.KFCc * v).sum(0)
+
+    def sensa(self, y, ve, HX, nCGD):
+        t = self.t
+        eps = 10 * float(np.finfo(np.float32).eps)
+        HY = t.minimum(ve, ve.max())
+        x = t.zeros(int(np.prod(self.n)), dtype=t.complex64, device=self.dev)
+        invHX = float(np.float32(1) / np.float32(HX))
+        res = y - self.M(x)
+        dagM = self.MH(res, HY, invHX)
+        sq = HX * float(t.vdot(dagM, dagM).real)
+        p = dagM
+        for i in range(1, nCGD + 1):
+            if sq < eps:
+                break
+            Mp = self.M(p)
+            a = sq / float(t.vdot(Mp.reshape(-1), (HY[:, None] * Mp).reshape(-1)).real)
+            x = x + a * p
+            if i == nCGD:
+                break
+            res = res - a * Mp
+            dagM = self.MH(res, HY, invHX)
+            sqn = HX * float(t.vdot(dagM, dagM).real)
+            p = dagM + (sqn / sq) * p
+            sq = sqn
+        r = y - self.M(x)  # monitoring (bmSensa.m:82-83)
+        float(t.vdot(r.reshape(-1), (HY[:, None] * r).reshape(-1)).real)
+        return x
+
+
 def run_gpu(args):
     import torch
 
@@ -246,6 +326,30 @@ def run_gpu(args):
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(w, _to_oracle(w, Gu), _to_oracle(w, Gut), y.cpu().numpy())
 
+    # the same reconstruction by the plain GPU arm (stock cuFFT / cuSPARSE
+    # calls, nothing fused), one warm-up run and one timed run, and the
+    # relative difference of the two reconstructions
+    plain = None
+    if not args.no_plain:
+        HX = np.float32(1)
+        for d in range(3):
+            HX = np.float32(HX * np.float32(np.float32(1) / np.float32(w.dK_u[d]) / np.float32(w.N_u[d])))
+        pg = PlainGpuSensa(w, Gu, Gut, rec.KFC, rec.KFC_conj, dev)
+        pg.sensa(y, ve, float(HX), w.nCGD)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        xp = pg.sensa(y, ve, float(HX), w.nCGD)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms_plain = e0.elapsed_time(e1)
+        step()
+        torch.cuda.synchronize()
+        plain = {"recons_per_s": round(1000.0 / ms_plain, 4), "ms_per_recon": round(ms_plain, 2),
+                 "speedup": round(ms_plain / (ms / args.steps), 2),
+                 "rel_diff": float((x - xp).norm() / xp.norm()),
+                 "arm": "torch.fft (cuFFT) + torch.sparse CSR (cuSPARSE), FP32 CG scalars, same inputs"}
+        del pg, xp
+
     out = {
         "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True,
@@ -257,6 +361,7 @@ def run_gpu(args):
         "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
         "recon_rel_err_vs_phantom": round(err, 5), "setup_s": round(setup_s, 2),
         "autotune": {"adjoint": rec.plan.adjoint_mode, "ms": {k: round(v, 4) for k, v in rec.tuning.items()}},
+        "vs_plain_gpu": plain,
     }
     if rank == 0:
         print(json.dumps(out), flush=True)
@@ -344,6 +449,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain-GPU comparison arm")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -63,6 +63,10 @@ def build(verbose: bool = False, jobs: int | None = None) -> str:
     headers = glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(INCLUDE, "*.h"))
     cu = sorted(glob.glob(os.path.join(CSRC, "*.cu")))
     cpp = sorted(glob.glob(os.path.join(CSRC, "*.cpp")))
+    so = os.path.join(LIB, "libmonalisa_gpu.so")
+    # a library newer than every source needs no objects (they need not be
+    # present: only the library travels with the sources)
+    lib_current = not _newer(so, cu + cpp + headers)
     objs, cmds = [], []
     for src in cu:
         o = os.path.join(OBJ, os.path.basename(src) + ".o")
@@ -75,10 +79,11 @@ def build(verbose: bool = False, jobs: int | None = None) -> str:
         if _newer(o, [src] + headers):
             cmds.append([CXX, "-O3", "-std=c++17", "-fPIC", "-fvisibility=hidden", "-I", INCLUDE,
                          "-I", os.path.join(CUDA_HOME, "include"), "-c", src, "-o", o])
+    if lib_current:
+        cmds = []
     with ThreadPoolExecutor(jobs or min(8, os.cpu_count() or 4)) as ex:
         list(ex.map(_run, cmds))
-    so = os.path.join(LIB, "libmonalisa_gpu.so")
-    if _newer(so, objs):
+    if not lib_current and _newer(so, objs):
         _run([NVCC, *ARCH, "-shared", "-o", so, *objs, "-L", os.path.join(CUDA_HOME, "lib64"),
               "-lcufft", "-lcudart", "-Xlinker", "-rpath," + os.path.join(CUDA_HOME, "lib64")])
     shim_src = os.path.join(CSRC, "mexshim", "mexshim.cpp")

@@ -1,582 +1,12 @@
-// Pruned, fused line-FFT passes (see mlg_fft.cuh).
-//
-// One CTA transforms `cols` = L lines x C coils of length N = N1 * N2 held
-// in shared memory as s[n][col] (col fastest), with the four-step
-// decomposition:
-//   A. for every n2 < N2 and column: an N1-point FFT over n1 (elements
-//      n1*N2 + n2), each output k1 multiplied by W_N^(n2*k1);
-//   C. for every k1 < N1 and column: an N2-point FFT over n2 (elements
-//      k1*N2 + n2) -> X[k1 + N1*k2] stored at position k1*N2 + k2.
-// Sub-FFTs of size 2^a 3^b run as unrolled radix-2/radix-3 butterflies in
-// registers (templated fast path); other sizes <= 32 use a direct DFT
-// (runtime path).  Twiddles come from a per-axis table exp(-2 pi i j/N)
-// computed on the host in double precision.
+// Pruned, fused line-FFT passes (see mlg_fft.cuh): host side -- axis tables
+// and the per-pass dispatch into the instantiations of mlg_fft_pass_*.cu.
 #include <algorithm>
 #include <cmath>
-#include <utility>
 #include <vector>
 
-#include "mlg_fft.cuh"
+#include "mlg_fft_kernels.cuh"
 
 namespace mlg {
-
-constexpr int kFftThreads = 256;     // target threads per CTA
-constexpr int kFftMaxThreads = 512;  // launch bound (columns that need lcm(cols, 32) > 256)
-constexpr size_t kFftSmemCap = 100 * 1024;
-constexpr int kGatherBatch = 8;  // cells gathered concurrently per thread (kGutIn)
-
-__device__ __forceinline__ float2 cmulf(float2 a, float2 b) {
-  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
-}
-
-template <int DIR>
-__device__ __forceinline__ float2 twid(const float2* __restrict__ tw, int j) {
-  const float2 w = __ldg(tw + j);
-  return DIR < 0 ? w : make_float2(w.x, -w.y);
-}
-
-// ---- in-register radix-2 FFT with compile-time twiddles ----------------------
-// The sub-FFT twiddles W_R^j depend only on template parameters: they are
-// evaluated at compile time (constexpr series for sin/cos in double, rounded
-// to float) and become instruction immediates -- no twiddle loads.
-constexpr double kPiD = 3.14159265358979323846264338327950288;
-
-constexpr double cx_sin_red(double x) {  // |x| <= pi
-  double term = x, sum = x;
-  for (int k = 1; k < 16; ++k) {
-    term *= -x * x / ((2.0 * k) * (2.0 * k + 1.0));
-    sum += term;
-  }
-  return sum;
-}
-constexpr double cx_cos_red(double x) {  // |x| <= pi
-  double term = 1.0, sum = 1.0;
-  for (int k = 1; k < 16; ++k) {
-    term *= -x * x / ((2.0 * k - 1.0) * (2.0 * k));
-    sum += term;
-  }
-  return sum;
-}
-constexpr double cx_reduce(double x) {  // to [-pi, pi]
-  while (x > kPiD) x -= 2 * kPiD;
-  while (x < -kPiD) x += 2 * kPiD;
-  return x;
-}
-
-template <class F, int... Is>
-__device__ __forceinline__ void sfor_impl(F&& f, std::integer_sequence<int, Is...>) {
-  (f(std::integral_constant<int, Is>{}), ...);
-}
-template <int N, class F>
-__device__ __forceinline__ void sfor(F&& f) {
-  sfor_impl(f, std::make_integer_sequence<int, N>{});
-}
-
-constexpr int bitrev(int i, int R) {
-  int j = 0;
-  for (int b = 1; b < R; b <<= 1, i >>= 1) j = (j << 1) | (i & 1);
-  return j;
-}
-
-template <int R, int DIR, int LEN>
-__device__ __forceinline__ void rstage(float2 (&r)[R]) {
-  sfor<R / LEN>([&](auto ic) {
-    constexpr int I = decltype(ic)::value * LEN;
-    sfor<LEN / 2>([&](auto jc) {
-      constexpr int J = decltype(jc)::value;
-      constexpr double ang = cx_reduce((double)DIR * 2.0 * kPiD * (double)J / (double)LEN);
-      constexpr float wr = (float)cx_cos_red(ang), wi = (float)cx_sin_red(ang);
-      const float2 u = r[I + J], v = r[I + J + LEN / 2];
-      float2 t;
-      if constexpr (J == 0) {
-        t = v;
-      } else if constexpr (4 * J == LEN) {  // +-i: a swap and a sign
-        t = DIR < 0 ? make_float2(v.y, -v.x) : make_float2(-v.y, v.x);
-      } else {
-        t = make_float2(wr * v.x - wi * v.y, wr * v.y + wi * v.x);
-      }
-      r[I + J] = make_float2(u.x + t.x, u.y + t.y);
-      r[I + J + LEN / 2] = make_float2(u.x - t.x, u.y - t.y);
-    });
-  });
-}
-
-template <int R, int DIR, int LEN = 2>
-__device__ __forceinline__ void rstages(float2 (&r)[R]) {
-  if constexpr (LEN <= R) {
-    rstage<R, DIR, LEN>(r);
-    rstages<R, DIR, LEN * 2>(r);
-  }
-}
-
-constexpr bool cx_pow2(int v) { return v > 0 && (v & (v - 1)) == 0; }
-
-template <int R, int DIR>
-__device__ __forceinline__ void reg_fft(float2 (&r)[R]);
-
-// R = 3M (M = 2^a 3^b): decimation in time by 3.  The three M-point
-// transforms of r[3m], r[3m+1], r[3m+2] are combined by radix-3 butterflies
-// with compile-time twiddles W_R^k, W_R^2k:
-//   X[k] = a + b + c,  X[k+M], X[k+2M] = a - (b+c)/2 -+ DIR i (sqrt3/2)(b-c)
-// where b, c carry their twiddles (DIR = -1 forward, +1 inverse).
-template <int R, int DIR>
-__device__ __forceinline__ void reg_fft_radix3(float2 (&r)[R]) {
-  constexpr int M = R / 3;
-  float2 a[M], b[M], c[M];
-  sfor<M>([&](auto mc) {
-    constexpr int m = decltype(mc)::value;
-    a[m] = r[3 * m];
-    b[m] = r[3 * m + 1];
-    c[m] = r[3 * m + 2];
-  });
-  reg_fft<M, DIR>(a);
-  reg_fft<M, DIR>(b);
-  reg_fft<M, DIR>(c);
-  constexpr float h = (float)(0.86602540378443864676 * (double)DIR);  // DIR * sqrt(3)/2
-  sfor<M>([&](auto kc) {
-    constexpr int k = decltype(kc)::value;
-    constexpr double a1 = cx_reduce((double)DIR * 2.0 * kPiD * (double)k / (double)R);
-    constexpr double a2 = cx_reduce((double)DIR * 2.0 * kPiD * (double)(2 * k) / (double)R);
-    constexpr float w1r = (float)cx_cos_red(a1), w1i = (float)cx_sin_red(a1);
-    constexpr float w2r = (float)cx_cos_red(a2), w2i = (float)cx_sin_red(a2);
-    float2 bv = b[k], cv = c[k];
-    if constexpr (k != 0) {
-      bv = make_float2(w1r * b[k].x - w1i * b[k].y, w1r * b[k].y + w1i * b[k].x);
-      cv = make_float2(w2r * c[k].x - w2i * c[k].y, w2r * c[k].y + w2i * c[k].x);
-    }
-    const float2 s = make_float2(bv.x + cv.x, bv.y + cv.y);
-    const float2 d = make_float2(bv.x - cv.x, bv.y - cv.y);
-    const float2 m = make_float2(a[k].x - 0.5f * s.x, a[k].y - 0.5f * s.y);
-    r[k] = make_float2(a[k].x + s.x, a[k].y + s.y);
-    r[k + M] = make_float2(m.x - h * d.y, m.y + h * d.x);      // m + h i d
-    r[k + 2 * M] = make_float2(m.x + h * d.y, m.y - h * d.x);  // m - h i d
-  });
-}
-
-// DIR < 0: X[k] = sum_j r[j] exp(-2 pi i jk/R) (forward); DIR > 0: inverse.
-// R = 2^a 3^b.
-template <int R, int DIR>
-__device__ __forceinline__ void reg_fft(float2 (&r)[R]) {
-  if constexpr (R > 1 && !cx_pow2(R)) {
-    static_assert(R % 3 == 0, "register FFT length must be 2^a 3^b");
-    reg_fft_radix3<R, DIR>(r);
-  } else if constexpr (R > 1) {
-    sfor<R>([&](auto ic) {  // bit-reversal permutation
-      constexpr int i = decltype(ic)::value;
-      constexpr int j = bitrev(i, R);
-      if constexpr (j > i) {
-        const float2 t = r[i];
-        r[i] = r[j];
-        r[j] = t;
-      }
-    });
-    rstages<R, DIR>(r);
-  }
-}
-
-// Direct DFT of runtime size R <= 32 (slow path).
-template <int DIR>
-__device__ __forceinline__ void dft_any(float2* r, int R, const float2* __restrict__ tw, int tstride) {
-  float2 o[32];
-  for (int k = 0; k < R; ++k) {
-    float2 acc = make_float2(0.f, 0.f);
-    for (int j = 0; j < R; ++j) {
-      const float2 w = twid<DIR>(tw, ((j * k) % R) * tstride);
-      const float2 t = cmulf(w, r[j]);
-      acc.x += t.x;
-      acc.y += t.y;
-    }
-    o[k] = acc;
-  }
-  for (int k = 0; k < R; ++k) r[k] = o[k];
-}
-
-struct Lines {
-  int u, v;       // non-FFT axes, u groups adjacent lines
-  int u0, vi;     // first u index of this CTA, v index
-  int L;          // lines per CTA
-};
-
-__device__ __forceinline__ Lines lines_of(const PassDesc& d, int L) {
-  Lines ln;
-  ln.u = d.ax == 0 ? 1 : 0;
-  ln.v = d.ax == 2 ? 1 : 2;
-  const int gu = (d.dims[ln.u] + L - 1) / L;
-  ln.u0 = (int)(blockIdx.x % gu) * L;
-  ln.vi = (int)(blockIdx.x / gu);
-  ln.L = L;
-  return ln;
-}
-
-template <PassMode MODE>
-__device__ __forceinline__ float2 load_elem(const PassDesc& d, const Lines& ln, int n, int l, int c) {
-  const int ui = ln.u0 + l;
-  if (ui >= d.dims[ln.u] || n < d.in_lo || n >= d.in_lo + d.in_len) return make_float2(0.f, 0.f);
-  if constexpr (MODE == PassMode::kShannaIn) {
-    // axis x: pixel (n - in_lo, ui, vi) of the n_x * n_y * n_z image
-    const long long m = (n - d.in_lo) + (long long)d.in_len * (ui + (long long)d.dims[1] * ln.vi);
-    const float2 xv = __ldg(d.img + (d.img_per_coil ? m * d.C + c : m));
-    float2 v = cmulf(xv, __ldg(d.kfc + m * d.C + c));
-    if ((n + d.coord_off[1] + ui + d.coord_off[2] + ln.vi) & 1) v = make_float2(-v.x, -v.y);
-    return v;
-  } else {
-    if (d.in_mask) {
-      const long long cell = (long long)ui * d.cell_stride[ln.u] + (long long)ln.vi * d.cell_stride[ln.v] +
-                             (long long)n * d.cell_stride[d.ax];
-      if (!((__ldg(d.in_mask + (cell >> 5)) >> (cell & 31)) & 1u)) return make_float2(0.f, 0.f);
-    }
-    const long long off = (long long)(n - d.in_lo) * d.in_stride[d.ax] + (long long)ui * d.in_stride[ln.u] +
-                          (long long)ln.vi * d.in_stride[ln.v] + c;
-    return __ldg(d.in + off);
-  }
-}
-
-template <int DIR>
-__device__ __forceinline__ void step_twiddle(float2* r, int R, int n2, const float2* tw) {
-  for (int k1 = 1; k1 < R; ++k1) {
-    if (n2 == 0) break;
-    r[k1] = cmulf(r[k1], twid<DIR>(tw, n2 * k1));
-  }
-}
-
-// The in-shared-memory transform; N1/N2 > 0 select the unrolled path.
-template <int N1, int N2, int DIR>
-__device__ __forceinline__ void smem_fft(float2* s, int cols, int rN1, int rN2, const float2* __restrict__ tw) {
-  const int n1s = N1 > 0 ? N1 : rN1, n2s = N2 > 0 ? N2 : rN2;
-  const int N = n1s * n2s;
-  if constexpr (N1 > 0) {
-    if ((int)blockDim.x % cols == 0) {
-      // fixed column per thread, rows strided by the number of row groups
-      const int col = threadIdx.x % cols, g = threadIdx.x / cols, G = blockDim.x / cols;
-      for (int n2 = g; n2 < N2; n2 += G) {
-        float2 r[N1];
-#pragma unroll
-        for (int n1 = 0; n1 < N1; ++n1) r[n1] = s[(n1 * N2 + n2) * cols + col];
-        reg_fft<N1, DIR>(r);
-        if (n2) {
-#pragma unroll
-          for (int k1 = 1; k1 < N1; ++k1) r[k1] = cmulf(r[k1], twid<DIR>(tw, n2 * k1));
-        }
-#pragma unroll
-        for (int k1 = 0; k1 < N1; ++k1) s[(k1 * N2 + n2) * cols + col] = r[k1];
-      }
-      __syncthreads();
-      for (int k1 = g; k1 < N1; k1 += G) {
-        float2 r[N2];
-#pragma unroll
-        for (int n2 = 0; n2 < N2; ++n2) r[n2] = s[(k1 * N2 + n2) * cols + col];
-        reg_fft<N2, DIR>(r);
-#pragma unroll
-        for (int k2 = 0; k2 < N2; ++k2) s[(k1 * N2 + k2) * cols + col] = r[k2];
-      }
-      __syncthreads();
-      return;
-    }
-  }
-  // step A
-  for (int it = threadIdx.x; it < n2s * cols; it += blockDim.x) {
-    const int n2 = it / cols, col = it - (it / cols) * cols;
-    if constexpr (N1 > 0) {
-      float2 r[N1];
-#pragma unroll
-      for (int n1 = 0; n1 < N1; ++n1) r[n1] = s[(n1 * N2 + n2) * cols + col];
-      reg_fft<N1, DIR>(r);
-#pragma unroll
-      for (int k1 = 1; k1 < N1; ++k1)
-        if (n2) r[k1] = cmulf(r[k1], twid<DIR>(tw, n2 * k1));
-#pragma unroll
-      for (int k1 = 0; k1 < N1; ++k1) s[(k1 * N2 + n2) * cols + col] = r[k1];
-    } else {
-      float2 r[32];
-      for (int n1 = 0; n1 < n1s; ++n1) r[n1] = s[(n1 * n2s + n2) * cols + col];
-      dft_any<DIR>(r, n1s, tw, N / n1s);
-      step_twiddle<DIR>(r, n1s, n2, tw);
-      for (int k1 = 0; k1 < n1s; ++k1) s[(k1 * n2s + n2) * cols + col] = r[k1];
-    }
-  }
-  __syncthreads();
-  // step C
-  for (int it = threadIdx.x; it < n1s * cols; it += blockDim.x) {
-    const int k1 = it / cols, col = it - (it / cols) * cols;
-    if constexpr (N2 > 0) {
-      float2 r[N2];
-#pragma unroll
-      for (int n2 = 0; n2 < N2; ++n2) r[n2] = s[(k1 * N2 + n2) * cols + col];
-      reg_fft<N2, DIR>(r);
-#pragma unroll
-      for (int k2 = 0; k2 < N2; ++k2) s[(k1 * N2 + k2) * cols + col] = r[k2];
-    } else {
-      float2 r[32];
-      for (int n2 = 0; n2 < n2s; ++n2) r[n2] = s[(k1 * n2s + n2) * cols + col];
-      dft_any<DIR>(r, n2s, tw, N / n2s);
-      for (int k2 = 0; k2 < n2s; ++k2) s[(k1 * n2s + k2) * cols + col] = r[k2];
-    }
-  }
-  __syncthreads();
-}
-
-// kGutIn load: each thread owns V adjacent coils (V = 2: 16-byte loads) of
-// one line and walks the line's cells with a stride; four cells are
-// gathered at a time so four dependency chains (row pointer -> entry ->
-// k-space row) are in flight per thread.  Per cell the entries are summed in
-// stored order with round-to-nearest multiply/add, as the SpMM kernels do.
-template <int V>
-__device__ __forceinline__ void gut_load(const PassDesc& d, const Lines& ln, float2* s, int N, int cols) {
-  using VT = typename std::conditional<V == 2, float4, float2>::type;
-  const int C = d.C;
-  const int cv = cols / V;
-  const int vc = threadIdx.x % cv, rstep = blockDim.x / cv;
-  const int col0 = vc * V, l = col0 / C, c = col0 - l * C;
-  const int ui = ln.u0 + l;
-  const bool line_ok = ui < d.dims[ln.u];
-  const long long cell_base = (long long)ui * d.cell_stride[ln.u] + (long long)ln.vi * d.cell_stride[ln.v];
-  const long long cst = d.cell_stride[d.ax];
-  VT* sv = reinterpret_cast<VT*>(s);
-  constexpr int B = kGatherBatch;
-  for (int n0 = threadIdx.x / cv; n0 < N; n0 += B * rstep) {
-    uint32_t b[B], len[B];
-    float acc[B][2 * V];
-#pragma unroll
-    for (int j = 0; j < B; ++j) {
-      const int n = n0 + j * rstep;
-      b[j] = len[j] = 0;
-#pragma unroll
-      for (int q = 0; q < 2 * V; ++q) acc[j][q] = 0.f;
-      if (line_ok && n < N) {
-        const long long cell = cell_base + (long long)n * cst;
-        b[j] = __ldg(d.g_rowptr + cell);
-        len[j] = __ldg(d.g_rowptr + cell + 1) - b[j];
-        if (len[j] > (uint32_t)kLongRow) {  // precomputed by the long-row kernel
-          const float* gl = reinterpret_cast<const float*>(d.g_long + cell * C + c);
-#pragma unroll
-          for (int q = 0; q < 2 * V; ++q) acc[j][q] = gl[q];
-          len[j] = 0;
-        }
-      }
-    }
-    uint32_t maxlen = 0;
-#pragma unroll
-    for (int j = 0; j < B; ++j) maxlen = max(maxlen, len[j]);
-    for (uint32_t t = 0; t < maxlen; ++t) {
-#pragma unroll
-      for (int j = 0; j < B; ++j) {
-        if (t < len[j]) {
-          const uint32_t k = b[j] + t;
-          const int jc = __ldg(d.g_col + k);
-          const float m = __ldg(d.g_val + k);
-          const float h = d.g_hy ? __ldg(d.g_hy + jc) : 1.0f;
-          const VT yv = *reinterpret_cast<const VT*>(d.g_y + (long long)jc * C + c);
-          const float* yf = reinterpret_cast<const float*>(&yv);
-#pragma unroll
-          for (int q = 0; q < 2 * V; ++q) {
-            const float hv = d.g_hy ? __fmul_rn(h, yf[q]) : yf[q];
-            acc[j][q] = __fadd_rn(acc[j][q], __fmul_rn(m, hv));
-          }
-        }
-      }
-    }
-#pragma unroll
-    for (int j = 0; j < B; ++j) {
-      const int n = n0 + j * rstep;
-      if (n < N) {
-        VT o;
-        float* of = reinterpret_cast<float*>(&o);
-#pragma unroll
-        for (int q = 0; q < 2 * V; ++q) of[q] = acc[j][q];
-        sv[n * cv + vc] = o;
-      }
-    }
-  }
-}
-
-template <int N1, int N2, int DIR, PassMode MODE>
-__global__ void __launch_bounds__(kFftMaxThreads) fft_pass_kernel(PassDesc d, int L, int rN1, int rN2,
-                                                               const float2* __restrict__ tw) {
-  extern __shared__ float2 s[];
-  const int n1s = N1 > 0 ? N1 : rN1, n2s = N2 > 0 ? N2 : rN2;
-  const int N = n1s * n2s;
-  const int C = d.C;
-  const int cols = L * C;
-  const Lines ln = lines_of(d, L);
-  // load (zero-filled outside the stored input range)
-  const int cv = cols >> 1;  // coil pairs when C is even: 16-byte accesses
-  if constexpr (MODE == PassMode::kGutIn) {
-    if ((C & 1) == 0 && (int)blockDim.x % cv == 0) {
-      gut_load<2>(d, ln, s, N, cols);
-    } else if ((int)blockDim.x % cols == 0) {
-      gut_load<1>(d, ln, s, N, cols);
-    } else {
-      for (int it = threadIdx.x; it < N * cols; it += blockDim.x) {
-        const int n = it / cols, col = it - (it / cols) * cols;
-        const int l = col / C, c = col - (col / C) * C;
-        const int ui = ln.u0 + l;
-        float2 a = make_float2(0.f, 0.f);
-        if (ui < d.dims[ln.u]) {
-          const long long cell = (long long)ui * d.cell_stride[ln.u] + (long long)ln.vi * d.cell_stride[ln.v] +
-                                 (long long)n * d.cell_stride[d.ax];
-          const uint32_t b = __ldg(d.g_rowptr + cell), e = __ldg(d.g_rowptr + cell + 1);
-          if (e - b > (uint32_t)kLongRow) {
-            a = d.g_long[cell * C + c];
-          } else {
-            for (uint32_t k = b; k < e; ++k) {
-              const int jc = __ldg(d.g_col + k);
-              const float m = __ldg(d.g_val + k);
-              float2 v = __ldg(d.g_y + (long long)jc * C + c);
-              if (d.g_hy) {
-                const float h = __ldg(d.g_hy + jc);
-                v = make_float2(__fmul_rn(h, v.x), __fmul_rn(h, v.y));
-              }
-              a = make_float2(__fadd_rn(a.x, __fmul_rn(m, v.x)), __fadd_rn(a.y, __fmul_rn(m, v.y)));
-            }
-          }
-        }
-        s[n * cols + col] = a;
-      }
-    }
-  } else if ((C & 1) == 0 && (int)blockDim.x % cv == 0) {
-    // fixed coil pair per thread, rows strided: no divisions in the loop and
-    // several independent 16-byte loads in flight per thread
-    const int vc = threadIdx.x % cv, rstep = blockDim.x / cv;
-    const int col = vc * 2, l = col / C, c = col - l * C;
-    const int ui = ln.u0 + l;
-    const bool line_ok = ui < d.dims[ln.u];
-    float4* s4 = reinterpret_cast<float4*>(s);
-    if constexpr (MODE == PassMode::kShannaIn) {
-      const long long mrow = (long long)d.in_len * (ui + (long long)d.dims[1] * ln.vi);
-      const int par = (d.coord_off[1] + ui + d.coord_off[2] + ln.vi) & 1;
-#pragma unroll 4
-      for (int n = threadIdx.x / cv; n < N; n += rstep) {
-        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (line_ok && n >= d.in_lo && n < d.in_lo + d.in_len) {
-          const long long m = mrow + (n - d.in_lo);
-          const float4 k = __ldg(reinterpret_cast<const float4*>(d.kfc + m * C + c));
-          float2 a, b;
-          if (d.img_per_coil) {
-            const float4 xv = __ldg(reinterpret_cast<const float4*>(d.img + m * C + c));
-            a = make_float2(xv.x, xv.y);
-            b = make_float2(xv.z, xv.w);
-          } else {
-            a = b = __ldg(d.img + m);
-          }
-          float2 r0 = cmulf(a, make_float2(k.x, k.y)), r1 = cmulf(b, make_float2(k.z, k.w));
-          if ((n + par) & 1) {
-            r0 = make_float2(-r0.x, -r0.y);
-            r1 = make_float2(-r1.x, -r1.y);
-          }
-          v = make_float4(r0.x, r0.y, r1.x, r1.y);
-        }
-        s4[n * cv + vc] = v;
-      }
-    } else {
-      const float2* base = d.in + (long long)ui * d.in_stride[ln.u] + (long long)ln.vi * d.in_stride[ln.v] + c;
-      const long long st = d.in_stride[d.ax];
-      const uint32_t* mask = d.in_mask;
-      const long long cell0 = (long long)ui * d.cell_stride[ln.u] + (long long)ln.vi * d.cell_stride[ln.v];
-      const long long cst = d.cell_stride[d.ax];
-#pragma unroll 4
-      for (int n = threadIdx.x / cv; n < N; n += rstep) {
-        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-        bool ld = line_ok && n >= d.in_lo && n < d.in_lo + d.in_len;
-        if (ld && mask) {
-          const long long cell = cell0 + (long long)n * cst;
-          ld = (__ldg(mask + (cell >> 5)) >> (cell & 31)) & 1u;
-        }
-        if (ld) v = __ldg(reinterpret_cast<const float4*>(base + (long long)(n - d.in_lo) * st));
-        s4[n * cv + vc] = v;
-      }
-    }
-  } else {
-    for (int it = threadIdx.x; it < N * cols; it += blockDim.x) {
-      const int n = it / cols, col = it - (it / cols) * cols;
-      const int l = col / C, c = col - (col / C) * C;
-      s[n * cols + col] = load_elem<MODE>(d, ln, n, l, c);
-    }
-  }
-  __syncthreads();
-  smem_fft<N1, N2, DIR>(s, cols, n1s, n2s, tw);
-  // X[k] sits at position (k % n1s) * n2s + k / n1s
-  if constexpr (MODE == PassMode::kNakatshaOut) {
-    __shared__ double red[kFftMaxThreads / 32];
-    // group of gc lanes per output pixel, lanes over coils, fixed-order tree
-    int gc = 1;
-    while (gc < C && gc < 32) gc <<= 1;
-    const int groups = blockDim.x / gc;
-    const int lane = threadIdx.x % gc, grp = threadIdx.x / gc;
-    double sq = 0.0;
-    const int nout = L * d.out_len;
-    // loop bound uniform across the warp so every lane reaches the shuffles
-    const int rounds = (nout + groups - 1) / groups;
-    for (int rd = 0; rd < rounds; ++rd) {
-      const int o = rd * groups + grp;
-      const bool live = o < nout;
-      const int l = live ? o / d.out_len : 0;
-      const int k = d.out_lo + (live ? o - l * d.out_len : 0);
-      const int ui = ln.u0 + l;
-      const bool ok = live && ui < d.dims[1];
-      const long long m = (k - d.out_lo) + (long long)d.out_len * (ui + (long long)d.dims[1] * ln.vi);
-      const int pos = (k % n1s) * n2s + k / n1s;
-      const float sg = ((k + d.coord_off[1] + ui + d.coord_off[2] + ln.vi) & 1) ? -d.sfac : d.sfac;
-      float2 acc = make_float2(0.f, 0.f);
-      if (ok) {
-        for (int c = lane; c < C; c += gc) {
-          float2 v = s[pos * cols + l * C + c];
-          v = make_float2(v.x * sg, v.y * sg);
-          const float2 t = cmulf(v, __ldg(d.kfc + m * C + c));
-          acc.x += t.x;
-          acc.y += t.y;
-        }
-      }
-      for (int w = gc / 2; w > 0; w >>= 1) {
-        acc.x += __shfl_xor_sync(0xffffffffu, acc.x, w, gc);
-        acc.y += __shfl_xor_sync(0xffffffffu, acc.y, w, gc);
-      }
-      if (ok && lane == 0) {
-        d.img_out[m] = acc;
-        sq += (double)acc.x * acc.x + (double)acc.y * acc.y;
-      }
-    }
-    if (d.partial) {
-      for (int o = 16; o > 0; o >>= 1) sq += __shfl_down_sync(0xffffffffu, sq, o);
-      if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = sq;
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        double t = 0.0;
-        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += red[i];
-        d.partial[blockIdx.x] = t;
-      }
-    }
-  } else if ((C & 1) == 0 && (int)blockDim.x % cv == 0) {
-    const int vc = threadIdx.x % cv, rstep = blockDim.x / cv;
-    const int col = vc * 2, l = col / C, c = col - l * C;
-    const int ui = ln.u0 + l;
-    if (ui < d.dims[ln.u]) {
-      const float4* s4 = reinterpret_cast<const float4*>(s);
-      float2* base = d.out + (long long)ui * d.out_stride[ln.u] + (long long)ln.vi * d.out_stride[ln.v] + c;
-      const long long st = d.out_stride[d.ax];
-#pragma unroll 4
-      for (int kk = threadIdx.x / cv; kk < d.out_len; kk += rstep) {
-        const int k = d.out_lo + kk;
-        const int pos = (k % n1s) * n2s + k / n1s;
-        *reinterpret_cast<float4*>(base + (long long)kk * st) = s4[pos * cv + vc];
-      }
-    }
-  } else {
-    for (int it = threadIdx.x; it < d.out_len * cols; it += blockDim.x) {
-      const int kk = it / cols, col = it - (it / cols) * cols;
-      const int l = col / C, c = col - (col / C) * C;
-      const int ui = ln.u0 + l;
-      if (ui >= d.dims[ln.u]) continue;
-      const int k = d.out_lo + kk;
-      const int pos = (k % n1s) * n2s + k / n1s;
-      const long long off = (long long)kk * d.out_stride[d.ax] + (long long)ui * d.out_stride[ln.u] +
-                            (long long)ln.vi * d.out_stride[ln.v] + c;
-      d.out[off] = s[pos * cols + col];
-    }
-  }
-}
-
-// ---- host side ---------------------------------------------------------------
-static bool pow2(int v) { return v > 0 && (v & (v - 1)) == 0; }
 
 int fft_axis_init(int N, FftAxisPlan& a) {
   a = FftAxisPlan();
@@ -609,77 +39,8 @@ void fft_axis_free(FftAxisPlan& a) {
   a = FftAxisPlan();
 }
 
-// Lines per CTA: 32 columns (256-byte row segments) for streaming passes; the
-// gathering pass uses 16 columns so that twice as many CTAs (and gathers)
-// are resident per SM.
-static int lines_per_cta(const FftAxisPlan& a, int C, PassMode mode) {
-  const int target = mode == PassMode::kGutIn ? 16 : 32;
-  int L = std::max(1, (target + C - 1) / C);
-  while (L > 1 && (size_t)a.N * L * C * sizeof(float2) > kFftSmemCap) --L;
-  return L;
-}
-
-static int blocks_for(const PassDesc& d, int L) {
-  const int u = d.ax == 0 ? 1 : 0, v = d.ax == 2 ? 1 : 2;
-  return ((d.dims[u] + L - 1) / L) * d.dims[v];
-}
-
 int fft_pass_blocks(const FftAxisPlan& a, const PassDesc& d) {
   return blocks_for(d, lines_per_cta(a, d.C, PassMode::kNakatshaOut));
-}
-
-// Threads per CTA: a multiple of the CTA's columns (and of the warp) so that
-// every thread keeps one column (or coil pair) through the load, the
-// transform and the store; the multiple nearest kFftThreads.  Columns whose
-// lcm with 32 exceeds kFftMaxThreads take kFftThreads and the per-element
-// paths.
-static int threads_for(int cols) {
-  int g = cols, b = 32;
-  while (b) {
-    const int t = g % b;
-    g = b;
-    b = t;
-  }
-  const int l = cols / g * 32;  // lcm(cols, 32)
-  if (l > kFftMaxThreads) return kFftThreads;
-  const int k = std::max(1, (kFftThreads + l / 2) / l);
-  return std::min(kFftMaxThreads / l * l, k * l);
-}
-
-template <int N1, int N2, int DIR, PassMode MODE>
-static int launch_pass(const FftAxisPlan& a, const PassDesc& d, int L, cudaStream_t s) {
-  const size_t smem = (size_t)a.N * L * d.C * sizeof(float2);
-  static bool attr = false;  // per instantiation
-  if (!attr) {
-    MLG_CUDA(cudaFuncSetAttribute(fft_pass_kernel<N1, N2, DIR, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)(200 * 1024)));
-    attr = true;
-  }
-  fft_pass_kernel<N1, N2, DIR, MODE><<<blocks_for(d, L), threads_for(L * d.C), smem, s>>>(d, L, a.N1, a.N2, a.tw);
-  MLG_LAUNCHED();
-  return MLG_OK;
-}
-
-template <int DIR, PassMode MODE>
-static int dispatch_size(const FftAxisPlan& a, const PassDesc& d, int L, cudaStream_t s) {
-  if (a.fast) {
-    switch (a.N1 * 100 + a.N2) {
-      case 404: return launch_pass<4, 4, DIR, MODE>(a, d, L, s);
-      case 408: return launch_pass<4, 8, DIR, MODE>(a, d, L, s);
-      case 808: return launch_pass<8, 8, DIR, MODE>(a, d, L, s);
-      case 816: return launch_pass<8, 16, DIR, MODE>(a, d, L, s);
-      case 1616: return launch_pass<16, 16, DIR, MODE>(a, d, L, s);
-      case 1632: return launch_pass<16, 32, DIR, MODE>(a, d, L, s);
-      case 3232: return launch_pass<32, 32, DIR, MODE>(a, d, L, s);
-      case 608: return launch_pass<6, 8, DIR, MODE>(a, d, L, s);
-      case 812: return launch_pass<8, 12, DIR, MODE>(a, d, L, s);
-      case 1216: return launch_pass<12, 16, DIR, MODE>(a, d, L, s);
-      case 1624: return launch_pass<16, 24, DIR, MODE>(a, d, L, s);
-      case 2432: return launch_pass<24, 32, DIR, MODE>(a, d, L, s);
-      default: break;
-    }
-  }
-  return launch_pass<0, 0, DIR, MODE>(a, d, L, s);
 }
 
 int fft_pass(const FftAxisPlan& a, PassMode mode, const PassDesc& d, int* n_partial, cudaStream_t s) {
@@ -692,16 +53,15 @@ int fft_pass(const FftAxisPlan& a, PassMode mode, const PassDesc& d, int* n_part
   switch (mode) {
     case PassMode::kShannaIn:
       MLG_CHECK(d.ax == 0 && d.dir < 0, "kShannaIn is a forward x pass");
-      return dispatch_size<-1, PassMode::kShannaIn>(a, d, L, s);
+      return fft_dispatch_shanna_in(a, d, L, s);
     case PassMode::kNakatshaOut:
       MLG_CHECK(d.ax == 0 && d.dir > 0, "kNakatshaOut is an inverse x pass");
-      return dispatch_size<1, PassMode::kNakatshaOut>(a, d, L, s);
+      return fft_dispatch_nakatsha_out(a, d, L, s);
     case PassMode::kGutIn:
       MLG_CHECK(d.dir > 0 && d.g_rowptr && d.g_y, "kGutIn is an inverse pass over Gut");
-      return dispatch_size<1, PassMode::kGutIn>(a, d, L, s);
+      return fft_dispatch_gut_in(a, d, L, s);
     default:
-      return d.dir < 0 ? dispatch_size<-1, PassMode::kPlain>(a, d, L, s)
-                       : dispatch_size<1, PassMode::kPlain>(a, d, L, s);
+      return d.dir < 0 ? fft_dispatch_plain_fwd(a, d, L, s) : fft_dispatch_plain_inv(a, d, L, s);
   }
 }
 

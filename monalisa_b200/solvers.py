@@ -28,7 +28,8 @@ def _niter(convCond) -> int:
 
 class SensaRecon:
     """CG-SENSE with everything resident on the device: Gu/Gut, KFC,
-    KFC_conj, cuFFT plans and work vectors (one per trajectory/coil set)."""
+    KFC_conj, FFT pass tables and work vectors (one per trajectory/coil
+    set)."""
 
     def __init__(self, Gu, Gut, C, n_u, dK_u=None, autotune=False):
         if isinstance(Gu, bmSparseMat):
@@ -45,6 +46,7 @@ class SensaRecon:
         KFC = bmKF(C, self.N_u, self.n_u, self.dK_u, self.nCh, kt, nw, kp)
         KFC_conj = bmKF_conj(np.conj(C), self.N_u, self.n_u, self.dK_u, self.nCh, kt, nw, kp)
         self.plan = NufftPlan(self.N_u, self.n_u, self.nCh, Gu, Gut, KFC, KFC_conj, self.dK_u)
+        self.KFC, self.KFC_conj = KFC, KFC_conj  # host copies, [prod(n_u), nCh]
         self.nPt = self.plan.nPt
         self._mats = (Gu, Gut)
         self.tuning = self.plan.autotune() if autotune else None

@@ -74,6 +74,30 @@ class bmSparseMat:
     def to_device(self) -> "DeviceMatrix":
         return DeviceMatrix.from_bm(self)
 
+    def to_csr(self):
+        """Standard CSR arrays (indptr int64 [l_size + 1], indices int32
+        [nnz], data float32 [nnz]) of this [l_size, r_size] matrix: columns
+        are the running sum of r_jump, stored rows the running sum of l_jump
+        (or every row when rows are not squeezed), r_nJump entries each
+        (bmSparseMat.m:100-188, bmSparseMat_r_nJump2index_mex.cpp:12-80)."""
+        r_size, r_jump, r_nJump, m_val, l_size, l_jump, l_nJump = self.jump_arrays()
+        cols = np.cumsum(r_jump.astype(np.int64))
+        if cols.size and (cols.min() < 0 or cols.max() >= r_size):
+            raise ValueError("column index outside the matrix")
+        counts = np.zeros(l_size, np.int64)
+        if l_jump is not None:
+            rows = np.cumsum(l_jump.astype(np.int64))
+            if rows.size and (rows.min() < 0 or rows.max() >= l_size):
+                raise ValueError("row index outside the matrix")
+            counts[rows] = r_nJump[:rows.size]
+        else:
+            counts[:] = r_nJump[:l_size]
+        indptr = np.zeros(l_size + 1, np.int64)
+        np.cumsum(counts, out=indptr[1:])
+        if indptr[-1] != cols.size:
+            raise ValueError("r_nJump does not add up to the number of entries")
+        return indptr, cols.astype(np.int32), m_val.copy()
+
 
 class DeviceMatrix:
     """A bmSparseMat resident in device memory (mlg_matrix_t)."""

@@ -110,3 +110,23 @@ def test_volume_element_1d_matches_restatement():
     mid = (x[1:] + x[:-1]) / 2
     edges = np.concatenate([[x[0] - (mid[0] - x[0])], mid, [x[-1] + (x[-1] - mid[-1])]])
     assert np.allclose(v, np.diff(edges))
+
+
+def test_to_csr_decodes_the_jump_format():
+    """bmSparseMat.to_csr (product) against the oracle's decoder, for a
+    row-complete Gu and an l-squeezed Gut."""
+    import oracle
+    from monalisa_b200 import bmSparseMat
+
+    rng = np.random.default_rng(17)
+    t = rng.uniform(-6, 6, (2, 300))
+    G = oracle.traj2sparsemat(t, np.ones(300), [12, 12], [1, 1], "gauss", 3, [0.61, 10])
+    for name in ("Gu", "Gut"):
+        M = G[name]
+        ref = M.to_scipy()
+        ref.sum_duplicates()
+        b = bmSparseMat(r_size=M.r_size, r_jump=M.r_jump, r_nJump=M.r_nJump, m_val=M.m_val, l_size=M.l_size,
+                        l_jump=M.l_jump, l_nJump=M.l_nJump)
+        indptr, indices, data = b.to_csr()
+        assert np.array_equal(indptr, ref.indptr) and np.array_equal(indices, ref.indices)
+        assert np.array_equal(data, ref.data)
