@@ -139,6 +139,33 @@ int mlg_sparsemat_vec_rC(int r_size, const int* r_jump, const int* r_nJump,
                          const float* m_val, int l_size, const int* l_jump,
                          int l_nJump, const float* v, int nVec, float* w);
 
+/* Replaces bmSparseMat_rR_oBlock_mex
+ * (…/bmSparseMat_rR_oBlock/bmSparseMat_rR_oBlock_mex.cpp:13 gateway): real
+ * row layout v [nVec, r_size] -> w [nVec, l_size]. */
+int mlg_sparsemat_vec_rR(int r_size, const int* r_jump, const int* r_nJump,
+                         const float* m_val, int l_size, const int* l_jump,
+                         int l_nJump, const float* v, int nVec, float* w);
+
+/* Every product of src/sparseMat/m/bmSparseMat_vec.m:120-240 in one entry
+ * point: layout MLG_LAYOUT_CC (complex, column layout v [r_size, nVec], split
+ * real/imaginary), _CR (complex row layout [nVec, r_size]), _RC (real
+ * column), _RR (real row).  nBlock = 0: the one-block jump format; nBlock >
+ * 0: the multi-block format of bmSparseMat.m:100-188 (running sums restart
+ * at every block; block_length, l_block_start [nBlock] int32,
+ * m_block_start [nBlock] int64), as the *_nBlock_omp_mex kernels read it
+ * (…/bmSparseMat_cR_nBlock_omp_mex.cpp:19-95, bmSparseMat_rR_nBlock_omp_mex.cpp:20-85).
+ * vI / wI are ignored for the real layouts. */
+#define MLG_LAYOUT_CC 0
+#define MLG_LAYOUT_CR 1
+#define MLG_LAYOUT_RC 2
+#define MLG_LAYOUT_RR 3
+int mlg_sparsemat_vec(int layout, int r_size, const int* r_jump,
+                      const int* r_nJump, const float* m_val, int l_size,
+                      const int* l_jump, int l_nJump, int nBlock,
+                      const int* block_length, const int* l_block_start,
+                      const long long* m_block_start, const float* vR,
+                      const float* vI, int nVec, float* wR, float* wI);
+
 /* Replaces bmSparseMat_r_nJump2index_mex
  * (…/bmSparseMat_r_nJump2index/bmSparseMat_r_nJump2index_mex.cpp:12,70):
  * out[out_length] = 0-based row index of every stored entry. */
@@ -151,6 +178,13 @@ int mlg_sparsemat_r_nJump2index(int l_size, const int* r_nJump,
 int mlg_matrix_create(int r_size, const int* r_jump, const int* r_nJump,
                       const float* m_val, int l_size, const int* l_jump,
                       int l_nJump, mlg_matrix_t* out);
+/* Same for a matrix prepared with argMode 'multi_block' (block arrays as for
+ * mlg_sparsemat_vec; nBlock = 0 is mlg_matrix_create). */
+int mlg_matrix_create_blocks(int r_size, const int* r_jump, const int* r_nJump,
+                             const float* m_val, int l_size, const int* l_jump,
+                             int l_nJump, int nBlock, const int* block_length,
+                             const int* l_block_start,
+                             const long long* m_block_start, mlg_matrix_t* out);
 int mlg_matrix_destroy(mlg_matrix_t m);
 int mlg_matrix_info(mlg_matrix_t m, long long* nnz, int* r_size, int* l_size);
 /* Rows holding at least one entry, and rows handled by the split long-row

@@ -15,6 +15,7 @@ LIB_PATH = os.path.join(_LIB_DIR, "libmonalisa_gpu.so")
 MLG_OK = 0
 MLG_KERNEL_GAUSS = 0
 MLG_KERNEL_KAISER = 1
+MLG_LAYOUT_CC, MLG_LAYOUT_CR, MLG_LAYOUT_RC, MLG_LAYOUT_RR = 0, 1, 2, 3
 
 c_int, c_float, c_double, c_ll, c_vp = ctypes.c_int, ctypes.c_float, ctypes.c_double, ctypes.c_longlong, ctypes.c_void_p
 P_f = ctypes.POINTER(ctypes.c_float)
@@ -38,6 +39,11 @@ SIGNATURES = {
     "mlg_sparsemat_vec_cR": [c_int, P_i, P_i, P_f, c_int, P_i, c_int, P_f, P_f, c_int, P_f, P_f],
     "mlg_sparsemat_vec_rC": [c_int, P_i, P_i, P_f, c_int, P_i, c_int, P_f, c_int, P_f],
     "mlg_sparsemat_r_nJump2index": [c_int, P_i, c_ll, P_i],
+    "mlg_sparsemat_vec_rR": [c_int, P_i, P_i, P_f, c_int, P_i, c_int, P_f, c_int, P_f],
+    "mlg_sparsemat_vec": [c_int, c_int, P_i, P_i, P_f, c_int, P_i, c_int, c_int, P_i, P_i, P_ll, P_f, P_f, c_int, P_f,
+                          P_f],
+    "mlg_matrix_create_blocks": [c_int, P_i, P_i, P_f, c_int, P_i, c_int, c_int, P_i, P_i, P_ll,
+                                 ctypes.POINTER(c_vp)],
     "mlg_matrix_create": [c_int, P_i, P_i, P_f, c_int, P_i, c_int, ctypes.POINTER(c_vp)],
     "mlg_matrix_destroy": [c_vp],
     "mlg_matrix_info": [c_vp, P_ll, P_i, P_i],
@@ -132,6 +138,13 @@ def dptr(a):
         return None
     assert a.dtype.name == "float64" and a.flags.c_contiguous, (a.dtype, a.flags)
     return a.ctypes.data_as(P_d)
+
+
+def llptr(a):
+    if a is None or a.size == 0:
+        return None
+    assert a.dtype.name == "int64" and a.flags.c_contiguous, (a.dtype, a.flags)
+    return a.ctypes.data_as(P_ll)
 
 
 def tptr(t):

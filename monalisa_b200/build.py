@@ -37,6 +37,8 @@ GATEWAYS = [
     "bmGridder_n2u_mex",
     "bmSparseMat_cC_oBlock_omp_mex", "bmSparseMat_cC_oBlock_mex", "bmSparseMat_cR_oBlock_mex",
     "bmSparseMat_rC_oBlock_mex", "bmSparseMat_rC_oBlock_omp_mex", "bmSparseMat_r_nJump2index_mex",
+    "bmSparseMat_rR_oBlock_mex", "bmSparseMat_cR_nBlock_omp_mex", "bmSparseMat_rR_nBlock_omp_mex",
+    "bmSparseMat_cC_oBlock_2_omp_mex",
     "bmShanna1_CUFFT_omp_mex", "bmShanna2_CUFFT_omp_mex", "bmShanna3_CUFFT_omp_mex",
     "bmNakatsha1_CUFFT_omp_mex", "bmNakatsha2_CUFFT_omp_mex", "bmNakatsha3_CUFFT_omp_mex",
     "bmIDF1_CUFFT_mex", "bmIDF2_CUFFT_mex", "bmIDF3_CUFFT_mex",

@@ -152,6 +152,110 @@ void vec_rC(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
         "bmSparseMat_rC_oBlock");
 }
 
+// rR_oBlock: real row layout v [n_vec, r_size] (prhs[8]), n_vec (prhs[9]) ->
+// w [n_vec, l_size] (bmSparseMat_rR_oBlock_mex.cpp:40-62)
+void vec_rR(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
+  (void)nlhs;
+  need(nrhs == 10, "wrong number of arguments");
+  Jump j = jump_args(prhs);
+  const int nVec = scalar_i(prhs[9]);
+  need(nVec >= 1 && mxGetNumberOfElements(prhs[8]) >= (size_t)j.r_size * nVec, "v must be [n_vec, r_size]");
+  plhs[0] = single_matrix(nVec, j.l_size);
+  check(mlg_sparsemat_vec_rR(j.r_size, j.r_jump, j.r_nJump, j.m_val, j.l_size, j.l_jump, j.l_nJump,
+                             data<float>(prhs[8]), nVec, (float*)mxGetData(plhs[0])),
+        "bmSparseMat_rR_oBlock");
+}
+
+// block arrays of the *_nBlock_omp gateways: nBlock, block_length,
+// l_block_start (int32), m_block_start (int64) in prhs[8..11]
+// (bmSparseMat_cR_nBlock_omp_mex.cpp:63-66)
+struct Blocks {
+  int n;
+  const int* length;
+  const int* l_start;
+  const long long* m_start;
+};
+
+Blocks block_args(const mxArray* prhs[]) {
+  Blocks b;
+  b.n = scalar_i(prhs[8]);
+  need(b.n >= 1, "nBlock must be >= 1");
+  need(mxGetNumberOfElements(prhs[9]) >= (size_t)b.n && mxGetNumberOfElements(prhs[10]) >= (size_t)b.n &&
+           mxGetNumberOfElements(prhs[11]) >= (size_t)b.n,
+       "block arrays shorter than nBlock");
+  need(mxIsInt32(prhs[9]) && mxIsInt32(prhs[10]) && mxIsInt64(prhs[11]),
+       "block_length / l_block_start must be int32 and m_block_start int64");
+  b.length = data<int>(prhs[9]);
+  b.l_start = data<int>(prhs[10]);
+  b.m_start = data<long long>(prhs[11]);
+  return b;
+}
+
+// cR_nBlock_omp: the gateway reads one complex v [n_vec, r_size] (prhs[12],
+// separate imaginary storage) and n_vec (prhs[13])
+// (bmSparseMat_cR_nBlock_omp_mex.cpp:69-71).  bmSparseMat_vec.m:167-172 calls
+// it with real(v), imag(v), n_vec instead (15 arguments), which the reference
+// gateway misreads; both forms are accepted here.
+void vec_cR_nBlock(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
+  (void)nlhs;
+  need(nrhs == 14 || nrhs == 15, "wrong number of arguments");
+  Jump j = jump_args(prhs);
+  Blocks b = block_args(prhs);
+  const int nVec = scalar_i(prhs[nrhs - 1]);
+  need(nVec >= 1 && mxGetNumberOfElements(prhs[12]) >= (size_t)j.r_size * nVec, "v must be [n_vec, r_size]");
+  const float* vr = data<float>(prhs[12]);
+  const float* vi = nrhs == 15 ? data<float>(prhs[13]) : (const float*)mxGetImagData(prhs[12]);
+  if (nrhs == 15) need(mxGetNumberOfElements(prhs[13]) >= (size_t)j.r_size * nVec, "imag(v) must be [n_vec, r_size]");
+  std::vector<float> zeros;
+  if (!vi) {
+    zeros.assign((size_t)j.r_size * nVec, 0.f);
+    vi = zeros.data();
+  }
+  plhs[0] = single_matrix(nVec, j.l_size, mxCOMPLEX);
+  check(mlg_sparsemat_vec(MLG_LAYOUT_CR, j.r_size, j.r_jump, j.r_nJump, j.m_val, j.l_size, j.l_jump, j.l_nJump, b.n,
+                          b.length, b.l_start, b.m_start, vr, vi, nVec, (float*)mxGetData(plhs[0]),
+                          (float*)mxGetImagData(plhs[0])),
+        "bmSparseMat_cR_nBlock_omp");
+}
+
+// rR_nBlock_omp: real v [n_vec, r_size] (prhs[12]), n_vec (prhs[13])
+// (bmSparseMat_rR_nBlock_omp_mex.cpp:52-82)
+void vec_rR_nBlock(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
+  (void)nlhs;
+  need(nrhs == 14, "wrong number of arguments");
+  Jump j = jump_args(prhs);
+  Blocks b = block_args(prhs);
+  const int nVec = scalar_i(prhs[13]);
+  need(nVec >= 1 && mxGetNumberOfElements(prhs[12]) >= (size_t)j.r_size * nVec, "v must be [n_vec, r_size]");
+  plhs[0] = single_matrix(nVec, j.l_size);
+  check(mlg_sparsemat_vec(MLG_LAYOUT_RR, j.r_size, j.r_jump, j.r_nJump, j.m_val, j.l_size, j.l_jump, j.l_nJump, b.n,
+                          b.length, b.l_start, b.m_start, data<float>(prhs[12]), nullptr, nVec,
+                          (float*)mxGetData(plhs[0]), nullptr),
+        "bmSparseMat_rR_nBlock_omp");
+}
+
+// cC_oBlock_2_omp: complex column-layout v [r_size, n_vec] with separate
+// imaginary storage (prhs[8]), n_vec (prhs[9]) -> complex w [l_size, n_vec]
+// (bmSparseMat_cC_oBlock_2_omp_mex.cpp:44-68)
+void vec_cC2(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
+  (void)nlhs;
+  need(nrhs == 10, "wrong number of arguments");
+  Jump j = jump_args(prhs);
+  const int nVec = scalar_i(prhs[9]);
+  need(nVec >= 1 && mxGetNumberOfElements(prhs[8]) >= (size_t)j.r_size * nVec, "v must be [r_size, n_vec]");
+  const float* vi = (const float*)mxGetImagData(prhs[8]);
+  std::vector<float> zeros;
+  if (!vi) {
+    zeros.assign((size_t)j.r_size * nVec, 0.f);
+    vi = zeros.data();
+  }
+  plhs[0] = single_matrix(j.l_size, nVec, mxCOMPLEX);
+  check(mlg_sparsemat_vec_cC(j.r_size, j.r_jump, j.r_nJump, j.m_val, j.l_size, j.l_jump, j.l_nJump,
+                             data<float>(prhs[8]), vi, nVec, (float*)mxGetData(plhs[0]),
+                             (float*)mxGetImagData(plhs[0])),
+        "bmSparseMat_cC_oBlock_2_omp");
+}
+
 void nJump2index(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
   need(nrhs == 3, "wrong number of arguments");
   const int l_size = scalar_i(prhs[0]);
@@ -263,6 +367,14 @@ extern "C" void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* 
   vec_cR(nlhs, plhs, nrhs, prhs);
 #elif defined(MLG_GATEWAY_bmSparseMat_rC_oBlock_mex) || defined(MLG_GATEWAY_bmSparseMat_rC_oBlock_omp_mex)
   vec_rC(nlhs, plhs, nrhs, prhs);
+#elif defined(MLG_GATEWAY_bmSparseMat_rR_oBlock_mex)
+  vec_rR(nlhs, plhs, nrhs, prhs);
+#elif defined(MLG_GATEWAY_bmSparseMat_cR_nBlock_omp_mex)
+  vec_cR_nBlock(nlhs, plhs, nrhs, prhs);
+#elif defined(MLG_GATEWAY_bmSparseMat_rR_nBlock_omp_mex)
+  vec_rR_nBlock(nlhs, plhs, nrhs, prhs);
+#elif defined(MLG_GATEWAY_bmSparseMat_cC_oBlock_2_omp_mex)
+  vec_cC2(nlhs, plhs, nrhs, prhs);
 #elif defined(MLG_GATEWAY_bmSparseMat_r_nJump2index_mex)
   nJump2index(nlhs, plhs, nrhs, prhs);
 #elif defined(MLG_GATEWAY_bmShanna1_CUFFT_omp_mex)

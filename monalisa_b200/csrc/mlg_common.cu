@@ -195,7 +195,8 @@ int csr_build_segments(Csr& c, cudaStream_t s) {
 // every index range-checked), then uploads.  bmSparseMat.m:135-166 defines
 // the format: r_jump/l_jump hold deltas whose first entry is absolute.
 int csr_from_jump(int r_size, const int* r_jump, const int* r_nJump, const float* m_val, int l_size,
-                  const int* l_jump, int l_nJump, Csr& out, cudaStream_t s) {
+                  const int* l_jump, int l_nJump, Csr& out, cudaStream_t s, int nBlock, const int* block_length,
+                  const int* l_block_start, const long long* m_block_start) {
   MLG_CHECK(r_size > 0 && l_size > 0, "matrix sizes must be positive (r_size=%d l_size=%d)", r_size, l_size);
   MLG_CHECK(l_nJump >= 0 && r_nJump != nullptr, "r_nJump missing");
   MLG_CHECK(l_jump != nullptr || l_nJump == l_size,
@@ -208,11 +209,35 @@ int csr_from_jump(int r_size, const int* r_jump, const int* r_nJump, const float
   MLG_CHECK(nnz < (1LL << 32) - 1, "nnz=%lld exceeds the 32-bit row pointer", nnz);
   MLG_CHECK(nnz == 0 || (r_jump && m_val), "r_jump / m_val missing");
 
+  // block starts: stored rows and entries where the running sums restart
+  // (one block: row 0 and entry 0); the blocks must tile the stored rows and
+  // m_block_start must count the entries before each block
+  std::vector<char> row_start((size_t)l_nJump + 1, 0), ent_start((size_t)nnz + 1, 0);
+  row_start[0] = ent_start[0] = 1;
+  if (nBlock > 0) {
+    MLG_CHECK(block_length && l_block_start && m_block_start, "block arrays missing (nBlock=%d)", nBlock);
+    long long next_row = 0, entries = 0;
+    int ri = 0;
+    for (int b = 0; b < nBlock; ++b) {
+      MLG_CHECK(l_block_start[b] == next_row && block_length[b] >= 1 &&
+                    (long long)l_block_start[b] + block_length[b] <= l_nJump,
+                "block %d: l_block_start=%d / block_length=%d do not tile the stored rows", b, l_block_start[b],
+                block_length[b]);
+      for (; ri < l_block_start[b]; ++ri) entries += r_nJump[ri];
+      MLG_CHECK(m_block_start[b] == entries, "block %d: m_block_start=%lld, expected %lld", b, m_block_start[b],
+                entries);
+      row_start[(size_t)l_block_start[b]] = 1;
+      ent_start[(size_t)entries] = 1;
+      next_row = (long long)l_block_start[b] + block_length[b];
+    }
+    MLG_CHECK(next_row == l_nJump, "blocks cover %lld of %d stored rows", next_row, l_nJump);
+  }
+
   std::vector<uint32_t> row_ptr((size_t)l_size + 1, 0);
   long long row = -1;
   for (int i = 0; i < l_nJump; ++i) {
-    // the first l_jump is the absolute 0-based row, later ones are deltas
-    long long r = l_jump ? (i == 0 ? (long long)l_jump[0] : row + l_jump[i]) : i;
+    // l_jump holds row deltas, absolute 0-based at a block's first row
+    long long r = l_jump ? (row_start[i] ? (long long)l_jump[i] : row + l_jump[i]) : i;
     MLG_CHECK(r > row && r < l_size, "row index %lld out of order or range at stored row %d", r, i);
     row = r;
     row_ptr[(size_t)r + 1] = (uint32_t)r_nJump[i];
@@ -222,7 +247,7 @@ int csr_from_jump(int r_size, const int* r_jump, const int* r_nJump, const float
   std::vector<int> col((size_t)nnz);
   long long c = 0;
   for (long long e = 0; e < nnz; ++e) {
-    c += r_jump[e];
+    c = ent_start[(size_t)e] ? (long long)r_jump[e] : c + r_jump[e];
     MLG_CHECK(c >= 0 && c < r_size, "column index %lld out of range [0,%d) at entry %lld", c, r_size, e);
     col[(size_t)e] = (int)c;
   }

@@ -144,9 +144,15 @@ struct mlg_matrix_s {
 
 namespace mlg {
 
-// Builds a Csr from host jump-format arrays (validated).
+// Builds a Csr from host jump-format arrays (validated).  With nBlock > 0
+// the matrix is in the multi-block form of bmSparseMat.m:100-188: the running
+// column sum restarts at each block's first entry m_block_start[b] and the
+// running row sum at each block's first stored row l_block_start[b]
+// (block_length[b] rows each); nBlock = 0 is the one-block form.
 int csr_from_jump(int r_size, const int* r_jump, const int* r_nJump, const float* m_val, int l_size,
-                  const int* l_jump, int l_nJump, Csr& out, cudaStream_t s);
+                  const int* l_jump, int l_nJump, Csr& out, cudaStream_t s, int nBlock = 0,
+                  const int* block_length = nullptr, const int* l_block_start = nullptr,
+                  const long long* m_block_start = nullptr);
 // Finishes a Csr whose row_ptr/col/val are already on the device: lists the
 // long rows and counts the non-empty ones.
 int csr_index_long_rows(Csr& c, cudaStream_t s);
@@ -165,6 +171,7 @@ enum class Layout : int {
   kCoilSplit = 2,  // float re[nCh][rows], im[...] (MATLAB column layout)
   kPointSplit = 3, // float re[rows][nCh], im[...] (MATLAB point layout)
   kCoilReal = 4,   // float [nCh][rows]           (real, column layout)
+  kPointReal = 5,  // float [rows][nCh]           (real, row layout)
 };
 
 struct Operand {

@@ -53,6 +53,8 @@ __device__ __forceinline__ float2 ld(const Operand& o, long long row, int c, int
   } else if constexpr (L == Layout::kPointSplit) {
     const long long i = row * nCh + c;
     return make_float2(__ldg(reinterpret_cast<const float*>(o.a) + i), __ldg(reinterpret_cast<const float*>(o.b) + i));
+  } else if constexpr (L == Layout::kPointReal) {
+    return make_float2(__ldg(reinterpret_cast<const float*>(o.a) + row * nCh + c), 0.f);
   } else {
     return make_float2(__ldg(reinterpret_cast<const float*>(o.a) + (long long)c * o.rows + row), 0.f);
   }
@@ -72,6 +74,8 @@ __device__ __forceinline__ void st(const Operand& o, long long row, int c, int n
     const long long i = row * nCh + c;
     reinterpret_cast<float*>(o.a)[i] = v.x;
     reinterpret_cast<float*>(o.b)[i] = v.y;
+  } else if constexpr (L == Layout::kPointReal) {
+    reinterpret_cast<float*>(o.a)[row * nCh + c] = v.x;
   } else {
     reinterpret_cast<float*>(o.a)[(long long)c * o.rows + row] = v.x;
   }
@@ -350,6 +354,8 @@ int spmm(const SpmmArgs& a, cudaStream_t s) {
   if (i == L::kPointSplit && o == L::kPointSplit)
     return launch<L::kPointSplit, L::kPointSplit, false>(p, m, sc3, grid_short, s);
   if (i == L::kCoilReal && o == L::kCoilReal) return launch<L::kCoilReal, L::kCoilReal, true>(p, m, sc3, grid_short, s);
+  if (i == L::kPointReal && o == L::kPointReal)
+    return launch<L::kPointReal, L::kPointReal, false>(p, m, sc3, grid_short, s);
   return fail(MLG_ERR_UNSUPPORTED, "spmm: layout pair (%d,%d) not instantiated", (int)i, (int)o);
 }
 
@@ -412,13 +418,15 @@ struct HostCall {
 
 int vec_call(int r_size, const int* r_jump, const int* r_nJump, const float* m_val, int l_size,
              const int* l_jump, int l_nJump, const float* vR, const float* vI, int nVec, float* wR,
-             float* wI, Layout layout) {
+             float* wI, Layout layout, int nBlock = 0, const int* block_length = nullptr,
+             const int* l_block_start = nullptr, const long long* m_block_start = nullptr) {
   MLG_TRY(ensure_device());
   MLG_CHECK(nVec >= 1, "n_vec must be >= 1");
-  MLG_CHECK(vR && wR && (layout == Layout::kCoilReal || (vI && wI)), "NULL vector buffer");
+  const bool cplx = layout != Layout::kCoilReal && layout != Layout::kPointReal;
+  MLG_CHECK(vR && wR && (!cplx || (vI && wI)), "NULL vector buffer");
   HostCall hc;
-  MLG_TRY(csr_from_jump(r_size, r_jump, r_nJump, m_val, l_size, l_jump, l_nJump, hc.m, hc.s));
-  const bool cplx = layout != Layout::kCoilReal;
+  MLG_TRY(csr_from_jump(r_size, r_jump, r_nJump, m_val, l_size, l_jump, l_nJump, hc.m, hc.s, nBlock, block_length,
+                        l_block_start, m_block_start));
   const size_t nin = (size_t)r_size * nVec, nout = (size_t)l_size * nVec;
   DevBuf<float> din, dout;
   MLG_TRY(din.alloc(nin * (cplx ? 2 : 1), hc.s));
@@ -484,20 +492,52 @@ int mlg_sparsemat_r_nJump2index(int l_size, const int* r_nJump, long long out_le
   return MLG_OK;
 }
 
-int mlg_matrix_create(int r_size, const int* r_jump, const int* r_nJump, const float* m_val, int l_size,
-                      const int* l_jump, int l_nJump, mlg_matrix_t* out) {
+int mlg_matrix_create_blocks(int r_size, const int* r_jump, const int* r_nJump, const float* m_val, int l_size,
+                             const int* l_jump, int l_nJump, int nBlock, const int* block_length,
+                             const int* l_block_start, const long long* m_block_start, mlg_matrix_t* out) {
   MLG_CHECK(out, "NULL output handle");
   *out = nullptr;
+  MLG_CHECK(nBlock >= 0, "nBlock must be >= 0");
   MLG_TRY(ensure_device());
   mlg_matrix_s* h = new mlg_matrix_s();
   cudaGetDevice(&h->device);
-  int st = csr_from_jump(r_size, r_jump, r_nJump, m_val, l_size, l_jump, l_nJump, h->csr, nullptr);
+  int st = csr_from_jump(r_size, r_jump, r_nJump, m_val, l_size, l_jump, l_nJump, h->csr, nullptr, nBlock,
+                         block_length, l_block_start, m_block_start);
   if (st != MLG_OK) {
     delete h;
     return st;
   }
   *out = h;
   return MLG_OK;
+}
+
+int mlg_matrix_create(int r_size, const int* r_jump, const int* r_nJump, const float* m_val, int l_size,
+                      const int* l_jump, int l_nJump, mlg_matrix_t* out) {
+  return mlg_matrix_create_blocks(r_size, r_jump, r_nJump, m_val, l_size, l_jump, l_nJump, 0, nullptr, nullptr,
+                                  nullptr, out);
+}
+
+int mlg_sparsemat_vec(int layout, int r_size, const int* r_jump, const int* r_nJump, const float* m_val, int l_size,
+                      const int* l_jump, int l_nJump, int nBlock, const int* block_length, const int* l_block_start,
+                      const long long* m_block_start, const float* vR, const float* vI, int nVec, float* wR,
+                      float* wI) {
+  Layout L;
+  switch (layout) {
+    case MLG_LAYOUT_CC: L = Layout::kCoilSplit; break;
+    case MLG_LAYOUT_CR: L = Layout::kPointSplit; break;
+    case MLG_LAYOUT_RC: L = Layout::kCoilReal; break;
+    case MLG_LAYOUT_RR: L = Layout::kPointReal; break;
+    default: return fail(MLG_ERR_ARG, "unknown layout %d", layout);
+  }
+  MLG_CHECK(nBlock >= 0, "nBlock must be >= 0");
+  return vec_call(r_size, r_jump, r_nJump, m_val, l_size, l_jump, l_nJump, vR, vI, nVec, wR, wI, L, nBlock,
+                  block_length, l_block_start, m_block_start);
+}
+
+int mlg_sparsemat_vec_rR(int r_size, const int* r_jump, const int* r_nJump, const float* m_val, int l_size,
+                         const int* l_jump, int l_nJump, const float* v, int nVec, float* w) {
+  return vec_call(r_size, r_jump, r_nJump, m_val, l_size, l_jump, l_nJump, v, nullptr, nVec, w, nullptr,
+                  Layout::kPointReal);
 }
 
 int mlg_matrix_destroy(mlg_matrix_t m) {

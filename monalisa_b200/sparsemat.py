@@ -124,8 +124,15 @@ class DeviceMatrix:
     def from_bm(cls, G: bmSparseMat) -> "DeviceMatrix":
         r_size, r_jump, r_nJump, m_val, l_size, l_jump, l_nJump = G.jump_arrays()
         h = ctypes.c_void_p()
-        N.call("mlg_matrix_create", r_size, N.iptr(r_jump), N.iptr(r_nJump), N.fptr(m_val), l_size,
-               N.iptr(l_jump), l_nJump, ctypes.byref(h))
+        nb = int(G.extra.get("nBlock", 0) or 0)
+        if nb > 1:  # multi-block preparation
+            N.call("mlg_matrix_create_blocks", r_size, N.iptr(r_jump), N.iptr(r_nJump), N.fptr(m_val), l_size,
+                   N.iptr(l_jump), l_nJump, nb, N.iptr(np.ascontiguousarray(G.extra["block_length"], np.int32)),
+                   N.iptr(np.ascontiguousarray(G.extra["l_block_start"], np.int32)),
+                   N.llptr(np.ascontiguousarray(G.extra["m_block_start"], np.int64)), ctypes.byref(h))
+        else:
+            N.call("mlg_matrix_create", r_size, N.iptr(r_jump), N.iptr(r_nJump), N.fptr(m_val), l_size,
+                   N.iptr(l_jump), l_nJump, ctypes.byref(h))
         meta = dict(N_u=G.N_u, d_u=G.d_u, kernel_type=G.kernel_type, nWin=G.nWin, kernelParam=G.kernelParam)
         return cls(h, meta, G.l_squeeze_flag)
 
@@ -191,35 +198,40 @@ def bmTraj2SparseMat(t, v, N_u, dK_u, kernelType=None, nWin=None, kernelParam=No
 
 def bmSparseMat_vec(G: bmSparseMat, v, layout: str = "column"):
     """bmSparseMat_vec (src/sparseMat/m/bmSparseMat_vec.m:11-243) for a
-    cpp_prepared one-block matrix: complex or real v.
+    cpp_prepared matrix, one block or multi-block (G.extra['nBlock'],
+    'block_length', 'l_block_start', 'm_block_start'): complex or real v.
 
     layout 'column': v [r_size, nVec] -> w [l_size, nVec] (the cC / rC MEX);
-    layout 'row': v [nVec, r_size] -> w [nVec, l_size] (the cR MEX)."""
+    layout 'row': v [nVec, r_size] -> w [nVec, l_size] (the cR / rR MEX)."""
     r_size, r_jump, r_nJump, m_val, l_size, l_jump, l_nJump = G.jump_arrays()
+    nb = int(G.extra.get("nBlock", 0) or 0)
+    if nb > 1:
+        bl = np.ascontiguousarray(G.extra["block_length"], np.int32)
+        ls = np.ascontiguousarray(G.extra["l_block_start"], np.int32)
+        ms = np.ascontiguousarray(G.extra["m_block_start"], np.int64)
+    else:
+        nb, bl, ls, ms = 0, None, None, None
     v = np.asarray(v)
     if v.ndim == 1:
         v = v[:, None] if layout == "column" else v[None, :]
+    cplx = np.iscomplexobj(v)
     if layout == "column":
         nVec = v.shape[1]
-        if np.iscomplexobj(v):
-            vR = np.ascontiguousarray(v.real.T, np.float32)
-            vI = np.ascontiguousarray(v.imag.T, np.float32)
-            wR = np.zeros((nVec, l_size), np.float32)
-            wI = np.zeros((nVec, l_size), np.float32)
-            N.call("mlg_sparsemat_vec_cC", r_size, N.iptr(r_jump), N.iptr(r_nJump), N.fptr(m_val), l_size,
-                   N.iptr(l_jump), l_nJump, N.fptr(vR), N.fptr(vI), nVec, N.fptr(wR), N.fptr(wI))
-            return (wR + 1j * wI).T.astype(np.complex64)
-        vR = np.ascontiguousarray(v.T, np.float32)
-        w = np.zeros((nVec, l_size), np.float32)
-        N.call("mlg_sparsemat_vec_rC", r_size, N.iptr(r_jump), N.iptr(r_nJump), N.fptr(m_val), l_size,
-               N.iptr(l_jump), l_nJump, N.fptr(vR), nVec, N.fptr(w))
-        return w.T.copy()
-    nVec = v.shape[0]
-    # column-major [nVec, r_size] == C-order [r_size][nVec]
-    vR = np.ascontiguousarray(np.real(v).T, np.float32)
-    vI = np.ascontiguousarray(np.imag(v).T, np.float32)
-    wR = np.zeros((l_size, nVec), np.float32)
-    wI = np.zeros((l_size, nVec), np.float32)
-    N.call("mlg_sparsemat_vec_cR", r_size, N.iptr(r_jump), N.iptr(r_nJump), N.fptr(m_val), l_size,
-           N.iptr(l_jump), l_nJump, N.fptr(vR), N.fptr(vI), nVec, N.fptr(wR), N.fptr(wI))
-    return (wR + 1j * wI).T.astype(np.complex64)
+        code = N.MLG_LAYOUT_CC if cplx else N.MLG_LAYOUT_RC
+        vR = np.ascontiguousarray(np.real(v).T, np.float32)  # [nVec][r_size]: column layout
+        vI = np.ascontiguousarray(np.imag(v).T, np.float32) if cplx else None
+        wR = np.zeros((nVec, l_size), np.float32)
+        wI = np.zeros((nVec, l_size), np.float32) if cplx else None
+    else:
+        nVec = v.shape[0]
+        code = N.MLG_LAYOUT_CR if cplx else N.MLG_LAYOUT_RR
+        # column-major [nVec, r_size] == C-order [r_size][nVec]
+        vR = np.ascontiguousarray(np.real(v).T, np.float32)
+        vI = np.ascontiguousarray(np.imag(v).T, np.float32) if cplx else None
+        wR = np.zeros((l_size, nVec), np.float32)
+        wI = np.zeros((l_size, nVec), np.float32) if cplx else None
+    N.call("mlg_sparsemat_vec", code, r_size, N.iptr(r_jump), N.iptr(r_nJump), N.fptr(m_val), l_size,
+           N.iptr(l_jump), l_nJump, nb, N.iptr(bl), N.iptr(ls), N.llptr(ms), N.fptr(vR), N.fptr(vI), nVec,
+           N.fptr(wR), N.fptr(wI))
+    w = (wR + 1j * wI) if cplx else wR
+    return w.T.astype(np.complex64 if cplx else np.float32)

@@ -234,10 +234,20 @@ class SparseMat:
     extra: dict = field(default_factory=dict)
 
     def to_scipy(self) -> sp.csr_matrix:
-        """Decodes the jump format into a scipy CSR [l_size, r_size]."""
-        cols = np.cumsum(self.r_jump.astype(np.int64))
+        """Decodes the jump format into a scipy CSR [l_size, r_size]; running
+        sums restart at every block's first entry / first stored row."""
+        def seg_cumsum(jump, starts):
+            out = np.empty(jump.size, np.int64)
+            bounds = list(np.ravel(starts).astype(np.int64)) + [jump.size]
+            for s, e in zip(bounds[:-1], bounds[1:]):
+                out[s:e] = np.cumsum(jump[s:e].astype(np.int64))
+            return out
+
+        m_starts = self.extra.get("m_block_start", [0])
+        l_starts = self.extra.get("l_block_start", [0])
+        cols = seg_cumsum(self.r_jump, m_starts)
         if self.l_jump is not None and self.l_jump.size:
-            rows_nz = np.cumsum(self.l_jump.astype(np.int64))
+            rows_nz = seg_cumsum(self.l_jump, l_starts)
         else:
             rows_nz = np.arange(self.l_size)
         rows = np.repeat(rows_nz, self.r_nJump.astype(np.int64))
@@ -269,19 +279,62 @@ def l_squeeze(G: SparseMat) -> SparseMat:
     return G
 
 
-def cpp_prepare(G: SparseMat) -> SparseMat:
-    """bmSparseMat.m:100-188 with argMode 'one_block': r_jump = deltas of
-    r_ind with the first entry absolute 0-based; likewise l_jump."""
-    if int(G.r_nJump.sum()) <= 0:
+def block_partition(r_nJump, nJumpPerBlock_factor=None, blockLengthMax_factor=None, one=False):
+    """bmSparseMat_blockPartition.m:6-181: greedy blocks of consecutive stored
+    rows; a block grows while its entry count stays below
+    fix(f1 * max(r_nJump)) + 1 and its length below fix(f2 * max(r_nJump)).
+    Returns (l_block_start, block_length) as int32 arrays."""
+    r_nJump = np.ravel(r_nJump).astype(np.int64)
+    if r_nJump.sum() <= 0:
         raise ValueError("The sparse matrix got a zero block. Preparation aborted.")
+    if one:
+        return np.zeros(1, np.int32), np.array([r_nJump.size], np.int32)
+    l_nJump = r_nJump.size
+    mx = int(r_nJump.max())
+    per_block = int(np.fix(nJumpPerBlock_factor * mx)) + 1
+    len_max = int(np.fix(blockLengthMax_factor * mx))
+    starts, lengths = [], []
+    start = 0
+    while start < l_nJump:
+        length, nxt = 1, start + 1
+        if nxt < l_nJump:
+            acc = int(r_nJump[start])
+            while nxt < l_nJump:
+                acc += int(r_nJump[nxt])
+                if acc < per_block and length < len_max:
+                    length += 1
+                    nxt += 1
+                else:
+                    break
+        starts.append(start)
+        lengths.append(length)
+        start += length
+    return np.array(starts, np.int32), np.array(lengths, np.int32)
+
+
+def cpp_prepare(G: SparseMat, argMode="one_block", nJumpPerBlock_factor=None, blockLengthMax_factor=None) -> SparseMat:
+    """bmSparseMat.m:100-188: r_jump = deltas of r_ind and l_jump = deltas of
+    l_ind, except that the first entry and the first stored row of every
+    block are absolute 0-based (:135-168); m_block_start = entries before
+    each block (int64)."""
+    if argMode == "one_block":
+        l_block_start, block_length = block_partition(G.r_nJump, one=True)
+    elif argMode == "multi_block":
+        l_block_start, block_length = block_partition(G.r_nJump, nJumpPerBlock_factor, blockLengthMax_factor)
+    else:
+        raise ValueError("Wrong list of arguments. ")
     r_ind = G.r_ind.astype(np.int64)
     r_jump = np.diff(np.concatenate([[0], r_ind]))
-    r_jump[0] = r_ind[0] - 1
+    csum = np.concatenate([[0], np.cumsum(G.r_nJump.astype(np.int64))])
+    m_block_start = csum[l_block_start.astype(np.int64)].astype(np.int64)
+    for m in m_block_start:
+        r_jump[m] = r_ind[m] - 1
     G.r_jump = r_jump.astype(np.int32)
     if G.type == "l_squeezed_matlab_ind":
         l_ind = G.l_ind.astype(np.int64)
         l_jump = np.diff(np.concatenate([[0], l_ind]))
-        l_jump[0] = l_ind[0] - 1
+        for s in l_block_start:
+            l_jump[s] = l_ind[s] - 1
         G.l_jump = l_jump.astype(np.int32)
         G.l_nJump = int(G.l_jump.size)
         G.type = "l_squeezed_cpp_prepared"
@@ -291,8 +344,9 @@ def cpp_prepare(G: SparseMat) -> SparseMat:
         G.type = "cpp_prepared"
     G.r_ind = None
     G.l_ind = None
-    G.block_type = "one_block"
-    G.extra["nBlock"] = 1
+    G.block_type = argMode
+    G.extra.update(nBlock=int(l_block_start.size), l_block_start=l_block_start, block_length=block_length,
+                   m_block_start=m_block_start)
     return G
 
 

@@ -363,3 +363,53 @@ def test_gateway_rejects_bad_matrix(mex):
     with pytest.raises(MexError, match="column index"):
         mex["bmSparseMat_cC_oBlock_omp_mex"](*args, np.ascontiguousarray(v.real), np.ascontiguousarray(v.imag),
                                              np.int32(v.shape[1]), nlhs=2)
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="compiled reference kernels absent")
+@pytest.mark.parametrize("squeeze", [False, True])
+def test_block_and_real_row_gateways_bitexact(mex, squeeze):
+    """bmSparseMat_{cR,rR}_nBlock_omp_mex, rR_oBlock_mex and
+    cC_oBlock_2_omp_mex against the reference's own compiled kernels on the
+    same multi-block / one-block matrices, bit for bit (short rows); the
+    cR_nBlock gateway also takes the 15-argument form of
+    bmSparseMat_vec.m:167-172 (real and imaginary parts apart)."""
+    from test_oracle_pinning import _block_args, _jump, _random_bm
+
+    rng = np.random.default_rng(50 + squeeze)
+    Gm, _ = _random_bm(rng, 400, 500, 0.02, squeeze, "multi_block")
+    G1, _ = _random_bm(np.random.default_rng(50 + squeeze), 400, 500, 0.02, squeeze, "one_block")
+    nVec = 4
+    v = (rng.standard_normal((nVec, 500)) + 1j * rng.standard_normal((nVec, 500))).astype(np.complex64)
+    vr = rng.standard_normal((nVec, 500)).astype(np.float32)
+    cases = [
+        ("bmSparseMat_cR_nBlock_omp_mex", (*_jump(Gm), *_block_args(Gm), v, np.int32(nVec))),
+        ("bmSparseMat_rR_nBlock_omp_mex", (*_jump(Gm), *_block_args(Gm), vr, np.int32(nVec))),
+        ("bmSparseMat_rR_oBlock_mex", (*_jump(G1), vr, np.int32(nVec))),
+        ("bmSparseMat_cC_oBlock_2_omp_mex", (*_jump(G1), np.asfortranarray(v.T), np.int32(nVec))),
+    ]
+    for name, args in cases:
+        ref = oracle.ref_mex(name)(*args)
+        got = mex[name](*args)
+        assert got.shape == ref.shape and np.array_equal(got, ref), name
+    split = mex["bmSparseMat_cR_nBlock_omp_mex"](*_jump(Gm), *_block_args(Gm), np.ascontiguousarray(v.real),
+                                                 np.ascontiguousarray(v.imag), np.int32(nVec))
+    assert np.array_equal(split, oracle.ref_mex("bmSparseMat_cR_nBlock_omp_mex")(*cases[0][1]))
+
+
+def test_multi_block_matrix_on_device():
+    """A multi-block bmSparseMat uploads (mlg_matrix_create_blocks) to the
+    same device matrix as its one-block form."""
+    import monalisa_b200 as mb
+    import torch
+    from test_oracle_pinning import _random_bm
+
+    Gm, a = _random_bm(np.random.default_rng(61), 300, 350, 0.03, True, "multi_block")
+    conv = lambda G: mb.bmSparseMat(r_size=G.r_size, r_jump=G.r_jump, r_nJump=G.r_nJump, m_val=G.m_val,
+                                    l_size=G.l_size, l_jump=G.l_jump, l_nJump=G.l_nJump, extra=dict(G.extra))
+    D = conv(Gm).to_device()
+    v = torch.randn((350, 2), dtype=torch.complex64, device="cuda")
+    got = D.spmm(v).cpu().numpy()
+    ref = a.astype(np.float64) @ v.cpu().numpy().astype(np.complex128)
+    assert np.allclose(got, ref, rtol=1e-5, atol=1e-5)
+    w = mb.bmSparseMat_vec(conv(Gm), v.cpu().numpy().T, layout="row")
+    assert np.allclose(w.T, ref, rtol=1e-5, atol=1e-5)

@@ -150,3 +150,57 @@ def test_deapodisation_is_inverse_kernel_transform():
     K = oracle.bmK([32, 32], [1, 1], 1, "gauss", 3, [0.61, 10])[:, 0].reshape(32, 32, order="F")
     assert K.min() >= 1.0 - 1e-6 and K.max() <= 10.0 + 1e-6
     assert abs(K[16, 16] - 1.0) < 1e-6  # kernel transform is maximal at the centre
+
+
+def _random_bm(rng, l_size, r_size, density, squeeze, mode, f=(1.5, 6)):
+    """A random sparse matrix with some empty rows, prepared as the reference
+    does (matlabSparse2bmSparseMat, optional l_squeeze, cpp_prepare)."""
+    import scipy.sparse as sp
+
+    a = sp.random(l_size, r_size, density=density, random_state=np.random.RandomState(rng.integers(1 << 30)),
+                  dtype=np.float32, format="csr")
+    a = sp.csr_matrix(a.multiply(rng.random((l_size, 1)) > 0.2))  # empty rows
+    a.eliminate_zeros()
+    G = oracle.matlab_sparse_to_bm(a, [r_size], [1], "gauss", 3, [0.61, 10])
+    if squeeze:
+        G = oracle.l_squeeze(G)
+    return oracle.cpp_prepare(G, mode, *f), a
+
+
+def _block_args(G):
+    e = G.extra
+    return (np.int32(e["nBlock"]), e["block_length"][None], e["l_block_start"][None],
+            e["m_block_start"].astype(np.int64)[None])
+
+
+def _jump(G):
+    lj = G.l_jump
+    return (np.int32(G.r_size), G.r_jump[None], G.r_nJump[None], G.m_val[None], np.int32(G.l_size),
+            lj[None] if lj.size else None, np.int32(G.l_nJump), np.int32(1 if lj.size else 0))
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="compiled reference kernels absent")
+@pytest.mark.parametrize("squeeze", [False, True])
+def test_multi_block_restatement_matches_reference(squeeze):
+    """The multi-block cpp_prepare restatement (bmSparseMat.m:100-188 with
+    bmSparseMat_blockPartition.m) fed to the reference's own nBlock kernels
+    gives, bit for bit, its one-block kernels' products; and the products
+    are the matrix's (float64 check)."""
+    rng = np.random.default_rng(31 + squeeze)
+    Gm, a = _random_bm(rng, 300, 400, 0.03, squeeze, "multi_block")
+    G1, _ = _random_bm(np.random.default_rng(31 + squeeze), 300, 400, 0.03, squeeze, "one_block")
+    assert Gm.extra["nBlock"] > 5 and np.array_equal(Gm.m_val, G1.m_val)
+    nVec = 3
+    v = (rng.standard_normal((nVec, 400)) + 1j * rng.standard_normal((nVec, 400))).astype(np.complex64)
+    wm = oracle.ref_mex("bmSparseMat_cR_nBlock_omp_mex")(*_jump(Gm), *_block_args(Gm), v, np.int32(nVec))
+    w1 = oracle.ref_mex("bmSparseMat_cR_oBlock_mex")(*_jump(G1), v, np.int32(nVec))
+    assert np.array_equal(wm, w1)
+    ref = (a.astype(np.float64) @ v.T.astype(np.complex128)).T
+    assert np.allclose(wm, ref, rtol=1e-5, atol=1e-5)
+    vr = rng.standard_normal((nVec, 400)).astype(np.float32)
+    rm = oracle.ref_mex("bmSparseMat_rR_nBlock_omp_mex")(*_jump(Gm), *_block_args(Gm), vr, np.int32(nVec))
+    r1 = oracle.ref_mex("bmSparseMat_rR_oBlock_mex")(*_jump(G1), vr, np.int32(nVec))
+    assert np.array_equal(rm, r1)
+    S = Gm.to_scipy()
+    S.sum_duplicates()
+    assert (S != a).nnz == 0
