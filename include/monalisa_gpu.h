@@ -210,6 +210,15 @@ int mlg_traj2sparsemat(int imDim, int nPt, const double* t, const double* ve,
                        const int* N_u, const double* dK_u, int kernelType,
                        int nWin, const double* kernelParam, mlg_matrix_t* Gu,
                        mlg_matrix_t* Gut);
+/* The three-output form [Gn, Gu, Gut] = bmTraj2SparseMat(...) (nargout 3,
+ * bmTraj2SparseMat.m:245-297).  Gn [prod(N_u), nPt]: weight * Dn with Dn =
+ * ve / prod(dK_u), rows (grid cells) normalised to sum 1, empty rows
+ * squeezed, entries of a row in ascending sample order.  Any output pointer
+ * may be NULL; ve is needed for Gn. */
+int mlg_traj2sparsemat3(int imDim, int nPt, const double* t, const double* ve,
+                        const int* N_u, const double* dK_u, int kernelType,
+                        int nWin, const double* kernelParam, mlg_matrix_t* Gn,
+                        mlg_matrix_t* Gu, mlg_matrix_t* Gut);
 
 /* ---- deapodisation ------------------------------------------------------ */
 
@@ -314,6 +323,31 @@ int mlg_plan_autotune(mlg_plan_t p, int reps, double* ms);
 int mlg_plan_profile(mlg_plan_t p, int iters, double* ms);
 
 /* ---- reconstructions ---------------------------------------------------- */
+
+/* bmMathilda-style leight gridding on device buffers (stream-ordered): the
+ * arguments of mlg_gridder_n2u_leight with aReal/aImag [nPt][nCh],
+ * tx/ty/tz/Dn [nPt], bReal/bImag [prod(N)][nCh] device pointers; scratch
+ * from the library's stream-ordered pool.  No reference counterpart (the
+ * reference's gridder takes MATLAB arrays). */
+int mlg_gridder_n2u_leight_dev(int imDim, const float* aReal, const float* aImag,
+                               const float* tx, const float* ty, const float* tz,
+                               const float* Dn, int nCh, int nPt, int Nx, int Ny,
+                               int Nz, int nWin, float kernelParam_1,
+                               float kernelParam_2, float* bReal, float* bImag,
+                               void* stream);
+
+/* The tail of the gridded reconstructions bmMathilda.m:76-121 and
+ * bmNasha.m:48-88 on device buffers:
+ *   x = coil_pinv(crop_{n_u}(K .* bmIDF(grid)))
+ * grid [prod(N_u)][nCh] point layout: interleaved complex (grid_split = 0,
+ * grid_a) or split (grid_split = 1, grid_a = real, grid_b = imaginary
+ * parts); K [prod(N_u)] float (mlg_deapodization); C [prod(n_u)][nCh]
+ * complex or NULL.  x [prod(n_u)] complex with C, else [nCh][prod(n_u)]
+ * (every coil's image, the column layout of [prod(n_u), nCh]).  N_u even. */
+int mlg_gridded_tail_dev(int imDim, const int* N_u, const int* n_u,
+                         const float* dK_u, int nCh, int grid_split,
+                         const void* grid_a, const void* grid_b, const float* K,
+                         const void* C, void* x, void* stream);
 
 /* CG-SENSE, src/fourier123/solver_function/imDim/nonCartesian/bmSensa.m:6-96:
  * nIter outer iterations (the convergence condition's iteration cap), each

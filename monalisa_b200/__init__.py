@@ -9,12 +9,12 @@ mirrors the reference's MATLAB interface on top of it.
 from ._native import MonalisaError, launch_count  # noqa: F401
 from .gridding import bmGridder_n2u, bmGridder_n2u_leight  # noqa: F401
 from .operators import (NufftPlan, bmCoilSense_pinv, bmIDF, bmK, bmKF, bmKF_conj, bmMathilda,  # noqa: F401
-                        bmNakatsha, bmShanna)
+                        bmNakatsha, bmNasha, bmShanna)
 from .solvers import SensaRecon, TevaMorphosiaChain, bmSensa, bmSteva, bmTevaMorphosia_chain  # noqa: F401
 from .sparsemat import DeviceMatrix, bmSparseMat, bmSparseMat_vec, bmTraj2SparseMat  # noqa: F401
 
 __all__ = [
     "MonalisaError", "bmGridder_n2u", "bmGridder_n2u_leight", "NufftPlan", "bmIDF", "bmK", "bmKF", "bmKF_conj",
-    "bmMathilda", "bmNakatsha", "bmShanna", "bmCoilSense_pinv", "SensaRecon", "bmSensa", "bmSteva", "TevaMorphosiaChain",
+    "bmMathilda", "bmNasha", "bmNakatsha", "bmShanna", "bmCoilSense_pinv", "SensaRecon", "bmSensa", "bmSteva", "TevaMorphosiaChain",
     "bmTevaMorphosia_chain", "DeviceMatrix", "bmSparseMat", "bmSparseMat_vec", "bmTraj2SparseMat", "launch_count",
 ]

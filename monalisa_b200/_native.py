@@ -76,6 +76,11 @@ SIGNATURES = {
     "mlg_tevamorphosia_dev": [c_vp, c_vp, P_f, c_float, P_f, P_f, c_int, c_int, c_int, c_vp, c_vp, c_vp, c_int, P_d,
                               c_vp],
     "mlg_tevamorphosia": [c_vp, P_f, P_f, P_f, c_float, P_f, P_f, c_int, c_int, c_int, P_f, P_f, P_d],
+    "mlg_traj2sparsemat3": [c_int, c_int, P_d, P_d, P_i, P_d, c_int, c_int, P_d, ctypes.POINTER(c_vp),
+                            ctypes.POINTER(c_vp), ctypes.POINTER(c_vp)],
+    "mlg_gridder_n2u_leight_dev": [c_int, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_int, c_int, c_int, c_int, c_int,
+                                   c_int, c_float, c_float, c_vp, c_vp, c_vp],
+    "mlg_gridded_tail_dev": [c_int, P_i, P_i, P_f, c_int, c_int, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp],
     "mlg_steva_dev": [c_vp, c_vp, P_f, c_float, P_f, P_f, c_int, c_int, c_vp, c_vp, c_vp, c_int, P_d, c_vp],
     "mlg_steva": [c_vp, P_f, P_f, P_f, c_float, P_f, P_f, c_int, c_int, P_f, P_f, P_d],
 }

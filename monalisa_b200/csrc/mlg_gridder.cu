@@ -610,6 +610,42 @@ int mlg_gridder_n2u_leight(int imDim, const float* aReal, const float* aImag, co
   return leight_host(imDim, aReal, aImag, tx, ty, tz, Dn, nCh, nPt, N, nWin, kernelParam_1, bReal, bImag);
 }
 
+int mlg_gridder_n2u_leight_dev(int imDim, const float* aReal, const float* aImag, const float* tx, const float* ty,
+                               const float* tz, const float* Dn, int nCh, int nPt, int Nx, int Ny, int Nz, int nWin,
+                               float kernelParam_1, float kernelParam_2, float* bReal, float* bImag, void* stream) {
+  (void)kernelParam_2;  // unused by the reference kernel too
+  MLG_TRY(ensure_device());
+  MLG_CHECK(nPt >= 0, "nPt must be >= 0");
+  MLG_CHECK(bReal && bImag, "NULL output");
+  MLG_CHECK(nPt == 0 || (aReal && aImag && tx && Dn && (imDim < 2 || ty) && (imDim < 3 || tz)),
+            "NULL input for nPt=%d", nPt);
+  const int N[3] = {Nx, Ny, Nz};
+  LeightGeom g;
+  MLG_TRY(leight_geometry(imDim, nCh, N, nWin, kernelParam_1, g));
+  cudaStream_t s = (cudaStream_t)stream;
+  LeightInputs in;
+  in.layout = Layout::kPointSplit;
+  in.re = aReal;
+  in.im = aImag;
+  in.tx = tx;
+  in.ty = imDim > 1 ? ty : nullptr;
+  in.tz = imDim > 2 ? tz : nullptr;
+  in.Dn = Dn;
+  LeightOutput out;
+  out.layout = Layout::kPointSplit;
+  out.re = bReal;
+  out.im = bImag;
+  DevBuf<char> counters;
+  MLG_TRY(counters.alloc(LeightWorkspace::counters_bytes(g), s));
+  LeightWorkspace ws;
+  ws.counters = counters.p;
+  ws.counters_cap = counters.n;
+  ws.grow_bins = grow_bins_pool;
+  const int st = leight_run(g, in, nPt, out, ws, s);
+  if (ws.bins) dev_free(ws.bins, s);  // stream-ordered: freed after the run
+  return st;
+}
+
 int mlg_gridder_n2u(const float* aReal, const float* aImag, const float* w, const int* nJump, int nCh, int nNb,
                     int nPt, int Nu_tot, float* bReal, float* bImag) {
   MLG_TRY(ensure_device());

@@ -60,9 +60,10 @@ static double bessel_i0_host(double x) {
 }
 
 // Entries of one sample: returns the count (0 for deleted samples), writes
-// sorted unique cells and normalised FP32 values.
+// sorted unique cells and normalised FP32 values (and, when traw is given,
+// the raw FP64 weights the Gn output needs).
 __global__ void traj_rows_kernel(TrajGeom g, const double* __restrict__ t, int nPt, int* __restrict__ cnt,
-                                 int* __restrict__ tcol, float* __restrict__ tval) {
+                                 int* __restrict__ tcol, float* __restrict__ tval, double* __restrict__ traw) {
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < nPt; p += gridDim.x * blockDim.x) {
     double tg[3], tf[3], tr[3];
     bool del = false;
@@ -143,6 +144,7 @@ __global__ void traj_rows_kernel(TrajGeom g, const double* __restrict__ t, int n
     for (int q = 0; q < m; ++q) {
       tcol[(long long)p * g.nNb + q] = cols[q];
       tval[(long long)p * g.nNb + q] = (float)(ws[q] * inv);
+      if (traw) traw[(long long)p * g.nNb + q] = ws[q];
     }
     cnt[p] = m;
   }
@@ -157,6 +159,65 @@ __global__ void traj_compact_kernel(int nNb, int nPt, const int* __restrict__ cn
       col[o + q] = tcol[(long long)p * nNb + q];
       val[o + q] = tval[(long long)p * nNb + q];
       erow[o + q] = p;
+    }
+  }
+}
+
+__global__ void traj_compact_raw_kernel(int nNb, int nPt, const int* __restrict__ cnt, const int* __restrict__ off,
+                                        const double* __restrict__ traw, double* __restrict__ raw) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < nPt; p += gridDim.x * blockDim.x)
+    for (int q = 0; q < cnt[p]; ++q) raw[off[p] + q] = traw[(long long)p * nNb + q];
+}
+
+// Dn = ve / prod(dK_u), the divisions in dimension order (bmTraj2SparseMat.m:81-106)
+__global__ void traj_dn_kernel(const double* __restrict__ ve, int nPt, double dk0, double dk1, double dk2, int imDim,
+                               double* __restrict__ Dn) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < nPt; p += gridDim.x * blockDim.x) {
+    double v = ve[p] / dk0;
+    if (imDim > 1) v /= dk1;
+    if (imDim > 2) v /= dk2;
+    Dn[p] = v;
+  }
+}
+
+// Gn (bmTraj2SparseMat.m:245-256): per grid cell, over its entries in
+// ascending sample order (the transposed order), w * Dn with zeros dropped;
+// count and FP64 row sum ...
+__global__ void gn_count_kernel(const int* __restrict__ toff, long long Nu, const int* __restrict__ perm,
+                                const int* __restrict__ erow, const double* __restrict__ raw,
+                                const double* __restrict__ Dn, int* __restrict__ cnt, double* __restrict__ sum) {
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < Nu; c += (long long)gridDim.x * blockDim.x) {
+    int n = 0;
+    double s = 0.0;
+    for (int i = toff[c]; i < toff[c + 1]; ++i) {
+      const int k = perm[i];
+      const double v = raw[k] * Dn[erow[k]];
+      if (v != 0.0) {
+        ++n;
+        s += v;
+      }
+    }
+    cnt[c] = n;
+    sum[c] = s;
+  }
+}
+
+// ... then the row normalised to sum 1 (value * (1/sum), as myDiag * A)
+__global__ void gn_fill_kernel(const int* __restrict__ toff, long long Nu, const int* __restrict__ perm,
+                               const int* __restrict__ erow, const double* __restrict__ raw,
+                               const double* __restrict__ Dn, const double* __restrict__ sum,
+                               const uint32_t* __restrict__ row_ptr, int* __restrict__ col, float* __restrict__ val) {
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < Nu; c += (long long)gridDim.x * blockDim.x) {
+    const double inv = sum[c] != 0.0 ? 1.0 / sum[c] : 0.0;
+    uint32_t o = row_ptr[c];
+    for (int i = toff[c]; i < toff[c + 1]; ++i) {
+      const int k = perm[i];
+      const double v = raw[k] * Dn[erow[k]];
+      if (v != 0.0) {
+        col[o] = erow[k];
+        val[o] = (float)(v * inv);
+        ++o;
+      }
     }
   }
 }
@@ -224,7 +285,9 @@ static int finish_csr(Csr& m, int* counts, cudaStream_t s) {
 }
 
 int traj2sparsemat(int imDim, int nPt, const double* t_host, const int* N_u, const double* dK_u, int kernelType,
-                   int nWin, const double* kp, Csr* Gu, Csr* Gut, cudaStream_t s) {
+                   int nWin, const double* kp, Csr* Gu, Csr* Gut, cudaStream_t s, const double* ve_host = nullptr,
+                   Csr* Gn = nullptr) {
+  MLG_CHECK(!Gn || ve_host, "Gn needs the volume elements ve");
   TrajGeom g;
   g.imDim = imDim;
   g.nWin = nWin;
@@ -268,7 +331,9 @@ int traj2sparsemat(int imDim, int nPt, const double* t_host, const int* N_u, con
   MLG_TRY(tval.alloc((size_t)cap + 1, s));
   MLG_CUDA(cudaMemcpyAsync(dt.p, t_host, sizeof(double) * imDim * nPt, cudaMemcpyHostToDevice, s));
   MLG_CUDA(cudaMemsetAsync(cnt.p + nPt, 0, sizeof(int), s));
-  traj_rows_kernel<<<g1d(nPt), 128, 0, s>>>(g, dt.p, nPt, cnt.p, tcol.p, tval.p);
+  DevBuf<double> traw;
+  if (Gn) MLG_TRY(traw.alloc((size_t)cap + 1, s));
+  traj_rows_kernel<<<g1d(nPt), 128, 0, s>>>(g, dt.p, nPt, cnt.p, tcol.p, tval.p, Gn ? traw.p : nullptr);
   MLG_LAUNCHED();
   DevBuf<int> off;
   MLG_TRY(off.alloc((size_t)nPt + 1, s));
@@ -292,17 +357,17 @@ int traj2sparsemat(int imDim, int nPt, const double* t_host, const int* N_u, con
   MLG_TRY(erow.alloc((size_t)nnz + 1, s));
   traj_compact_kernel<<<g1d(nPt), 256, 0, s>>>(g.nNb, nPt, cnt.p, off.p, tcol.p, tval.p, u.col, u.val, erow.p);
   MLG_LAUNCHED();
+  DevBuf<double> raw;
+  if (Gn) {
+    MLG_TRY(raw.alloc((size_t)nnz + 1, s));
+    traj_compact_raw_kernel<<<g1d(nPt), 256, 0, s>>>(g.nNb, nPt, cnt.p, off.p, traw.p, raw.p);
+    MLG_LAUNCHED();
+  }
   // Gu row pointer: counts -> scan (reuse cnt with a trailing zero)
   MLG_TRY(finish_csr(u, cnt.p, s));
 
-  if (Gut) {
-    Csr v;
-    v.r_size = nPt;
-    v.l_size = (int)Nu;
-    v.nnz = nnz;
-    MLG_CUDA(cudaMalloc(&v.row_ptr, sizeof(uint32_t) * ((size_t)Nu + 1)));
-    MLG_CUDA(cudaMalloc(&v.col, sizeof(int) * (size_t)std::max(1, nnz)));
-    MLG_CUDA(cudaMalloc(&v.val, sizeof(float) * (size_t)std::max(1, nnz)));
+  if (Gut || Gn) {
+    // entries grouped by cell, samples ascending within a cell (stable sort)
     DevBuf<int> keys_out, perm_in, perm_out, ccnt;
     MLG_TRY(keys_out.alloc((size_t)nnz + 1, s));
     MLG_TRY(perm_in.alloc((size_t)nnz + 1, s));
@@ -317,13 +382,65 @@ int traj2sparsemat(int imDim, int nPt, const double* t_host, const int* N_u, con
     DevBuf<char> stmp;
     MLG_TRY(stmp.alloc(sb, s));
     MLG_CUDA(cub::DeviceRadixSort::SortPairs(stmp.p, sb, u.col, keys_out.p, perm_in.p, perm_out.p, nnz, 0, end_bit, s));
-    transpose_fill_kernel<<<g1d(nnz), 256, 0, s>>>(perm_out.p, erow.p, u.val, nnz, v.col, v.val);
-    MLG_LAUNCHED();
     MLG_CUDA(cudaMemsetAsync(ccnt.p, 0, sizeof(int) * ((size_t)Nu + 1), s));
     cell_count_kernel<<<g1d(nnz), 256, 0, s>>>(u.col, nnz, ccnt.p);
     MLG_LAUNCHED();
-    MLG_TRY(finish_csr(v, ccnt.p, s));
-    *Gut = v;
+    if (Gut) {
+      Csr v;
+      v.r_size = nPt;
+      v.l_size = (int)Nu;
+      v.nnz = nnz;
+      MLG_CUDA(cudaMalloc(&v.row_ptr, sizeof(uint32_t) * ((size_t)Nu + 1)));
+      MLG_CUDA(cudaMalloc(&v.col, sizeof(int) * (size_t)std::max(1, nnz)));
+      MLG_CUDA(cudaMalloc(&v.val, sizeof(float) * (size_t)std::max(1, nnz)));
+      transpose_fill_kernel<<<g1d(nnz), 256, 0, s>>>(perm_out.p, erow.p, u.val, nnz, v.col, v.val);
+      MLG_LAUNCHED();
+      MLG_TRY(finish_csr(v, ccnt.p, s));  // leaves the cell offsets in ccnt
+      *Gut = v;
+    } else {
+      size_t tb2 = 0;
+      cub::DeviceScan::ExclusiveSum(nullptr, tb2, ccnt.p, ccnt.p, Nu + 1);
+      DevBuf<char> tmp2;
+      MLG_TRY(tmp2.alloc(tb2, s));
+      MLG_CUDA(cub::DeviceScan::ExclusiveSum(tmp2.p, tb2, ccnt.p, ccnt.p, Nu + 1, s));
+    }
+    if (Gn) {
+      DevBuf<double> dve, Dn, gsum;
+      DevBuf<int> gcnt;
+      MLG_TRY(dve.alloc((size_t)nPt, s));
+      MLG_TRY(Dn.alloc((size_t)nPt, s));
+      MLG_TRY(gsum.alloc((size_t)Nu, s));
+      MLG_TRY(gcnt.alloc((size_t)Nu + 1, s));
+      MLG_CUDA(cudaMemcpyAsync(dve.p, ve_host, sizeof(double) * nPt, cudaMemcpyHostToDevice, s));
+      traj_dn_kernel<<<g1d(nPt), 256, 0, s>>>(dve.p, nPt, g.dK[0], g.dK[1], g.dK[2], imDim, Dn.p);
+      MLG_LAUNCHED();
+      MLG_CUDA(cudaMemsetAsync(gcnt.p + Nu, 0, sizeof(int), s));
+      gn_count_kernel<<<g1d(Nu), 256, 0, s>>>(ccnt.p, Nu, perm_out.p, erow.p, raw.p, Dn.p, gcnt.p, gsum.p);
+      MLG_LAUNCHED();
+      Csr w;
+      w.r_size = nPt;
+      w.l_size = (int)Nu;
+      MLG_CUDA(cudaMalloc(&w.row_ptr, sizeof(uint32_t) * ((size_t)Nu + 1)));
+      const int st = finish_csr(w, gcnt.p, s);
+      uint32_t nnz_n = 0;
+      if (st == MLG_OK) {
+        MLG_CUDA(cudaMemcpyAsync(&nnz_n, w.row_ptr + Nu, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        MLG_CUDA(cudaStreamSynchronize(s));
+      }
+      w.nnz = nnz_n;
+      if (st != MLG_OK || cudaMalloc(&w.col, sizeof(int) * (size_t)std::max<uint32_t>(1, nnz_n)) != cudaSuccess ||
+          cudaMalloc(&w.val, sizeof(float) * (size_t)std::max<uint32_t>(1, nnz_n)) != cudaSuccess) {
+        cudaGetLastError();
+        csr_free(w);
+        if (Gu) *Gu = u;  // the caller frees what it asked for
+        else csr_free(u);
+        return st != MLG_OK ? st : fail(MLG_ERR_OOM, "Gn: device allocation failed");
+      }
+      gn_fill_kernel<<<g1d(Nu), 256, 0, s>>>(ccnt.p, Nu, perm_out.p, erow.p, raw.p, Dn.p, gsum.p, w.row_ptr, w.col,
+                                             w.val);
+      MLG_LAUNCHED();
+      *Gn = w;
+    }
   }
   if (Gu) {
     *Gu = u;
@@ -336,37 +453,45 @@ int traj2sparsemat(int imDim, int nPt, const double* t_host, const int* N_u, con
 
 }  // namespace mlg
 
-extern "C" int mlg_traj2sparsemat(int imDim, int nPt, const double* t, const double* ve, const int* N_u,
-                                  const double* dK_u, int kernelType, int nWin, const double* kernelParam,
-                                  mlg_matrix_t* Gu, mlg_matrix_t* Gut) {
-  (void)ve;  // Gu / Gut are row-normalised: the volume elements cancel (bmTraj2SparseMat.m:271-281)
+extern "C" int mlg_traj2sparsemat3(int imDim, int nPt, const double* t, const double* ve, const int* N_u,
+                                   const double* dK_u, int kernelType, int nWin, const double* kernelParam,
+                                   mlg_matrix_t* Gn, mlg_matrix_t* Gu, mlg_matrix_t* Gut) {
   MLG_CHECK(imDim >= 1 && imDim <= 3 && nPt >= 1 && t && N_u && dK_u && kernelParam, "invalid argument");
   MLG_CHECK(kernelType == MLG_KERNEL_GAUSS || kernelType == MLG_KERNEL_KAISER, "unknown kernel type");
   MLG_CHECK(nWin >= 1, "nWin must be >= 1");
-  MLG_CHECK(Gu || Gut, "no output requested");
+  MLG_CHECK(Gn || Gu || Gut, "no output requested");
+  MLG_CHECK(!Gn || ve, "Gn needs the volume elements ve");
   for (int d = 0; d < imDim; ++d) MLG_CHECK(N_u[d] >= 1 && dK_u[d] > 0, "invalid N_u / dK_u");
   MLG_TRY(mlg::ensure_device());
+  if (Gn) *Gn = nullptr;
   if (Gu) *Gu = nullptr;
   if (Gut) *Gut = nullptr;
-  mlg::Csr u, v;
+  mlg::Csr u, v, w;
   int st = mlg::traj2sparsemat(imDim, nPt, t, N_u, dK_u, kernelType, nWin, kernelParam, Gu ? &u : nullptr,
-                               Gut ? &v : nullptr, nullptr);
+                               Gut ? &v : nullptr, nullptr, ve, Gn ? &w : nullptr);
   if (st != MLG_OK) {
     mlg::csr_free(u);
     mlg::csr_free(v);
+    mlg::csr_free(w);
     return st;
   }
   int dev = 0;
   cudaGetDevice(&dev);
-  if (Gu) {
-    *Gu = new mlg_matrix_s();
-    (*Gu)->csr = u;
-    (*Gu)->device = dev;
-  }
-  if (Gut) {
-    *Gut = new mlg_matrix_s();
-    (*Gut)->csr = v;
-    (*Gut)->device = dev;
-  }
+  mlg_matrix_t* outs[3] = {Gn, Gu, Gut};
+  mlg::Csr* csrs[3] = {&w, &u, &v};
+  for (int i = 0; i < 3; ++i)
+    if (outs[i]) {
+      *outs[i] = new mlg_matrix_s();
+      (*outs[i])->csr = *csrs[i];
+      (*outs[i])->device = dev;
+    }
   return MLG_OK;
+}
+
+extern "C" int mlg_traj2sparsemat(int imDim, int nPt, const double* t, const double* ve, const int* N_u,
+                                  const double* dK_u, int kernelType, int nWin, const double* kernelParam,
+                                  mlg_matrix_t* Gu, mlg_matrix_t* Gut) {
+  // Gu / Gut are row-normalised: the volume elements cancel (bmTraj2SparseMat.m:271-281)
+  MLG_CHECK(Gu || Gut, "no output requested");
+  return mlg_traj2sparsemat3(imDim, nPt, t, ve, N_u, dK_u, kernelType, nWin, kernelParam, nullptr, Gu, Gut);
 }

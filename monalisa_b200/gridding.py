@@ -19,6 +19,54 @@ def _point(a, dtype):
     return a[None, :] if a.ndim == 1 else a
 
 
+def _leight_prepare(data_n, t, Dn, N_u, dK_u):
+    """Argument preparation of bmGridder_n2u_leight.m:40-87 (single
+    precision): grid units, Dn / prod(dK_u), samples outside the grid box
+    deleted.  Returns aR, aI [nPt][nCh], the per-axis t, Dn, nCh, nPt and the
+    three grid extents."""
+    t = _point(t, np.float32).copy()
+    data_n = _point(data_n, np.complex64)
+    Dn = np.asarray(Dn, np.float32).ravel().copy()
+    imDim = t.shape[0]
+    N_u = np.ravel(N_u).astype(np.float64)
+    dK_u = np.ravel(dK_u).astype(np.float64)
+    for i in range(imDim):
+        t[i] = t[i] / np.float32(dK_u[i])
+        Dn = Dn / np.float32(dK_u[i])
+    t = t + np.array([np.fix(N_u[i] / 2 + 1) for i in range(imDim)], np.float32)[:, None]
+    mask = np.zeros(t.shape[1], bool)
+    for i in range(imDim):
+        mask |= (t[i] < 1) | (t[i] > N_u[i])
+    t, Dn, a = t[:, ~mask], Dn[~mask], data_n[:, ~mask]
+    nCh, nPt = a.shape
+    aR = np.ascontiguousarray(a.real.T, np.float32)
+    aI = np.ascontiguousarray(a.imag.T, np.float32)
+    tx = [np.ascontiguousarray(t[i]) for i in range(imDim)] + [None] * (3 - imDim)
+    Ns = [int(N_u[i]) if i < imDim else 1 for i in range(3)]
+    return aR, aI, tx, np.ascontiguousarray(Dn), nCh, nPt, Ns
+
+
+def bmGridder_n2u_leight_dev(data_n, t, Dn, N_u, dK_u, kernelType=None, nWin=None, kernelParam=None):
+    """The leight gridder with its output left on the device: returns CUDA
+    float32 tensors (bR, bI), each [prod(N_u)][nCh] (point layout)."""
+    import torch
+
+    kernelType, nWin, kp = kernel_defaults(kernelType, nWin, kernelParam)
+    aR, aI, tx, Dn, nCh, nPt, Ns = _leight_prepare(data_n, t, Dn, N_u, dK_u)
+    imDim = np.ravel(N_u).size
+    dev = torch.device("cuda", torch.cuda.current_device())
+    up = lambda a: torch.from_numpy(a).to(dev) if a is not None else None
+    dA, dI, dD = up(aR), up(aI), up(Dn)
+    dT = [up(v) for v in tx]
+    nu = int(np.prod(Ns))
+    bR = torch.empty((nu, nCh), dtype=torch.float32, device=dev)
+    bI = torch.empty((nu, nCh), dtype=torch.float32, device=dev)
+    N.call("mlg_gridder_n2u_leight_dev", imDim, N.tptr(dA), N.tptr(dI), N.tptr(dT[0]), N.tptr(dT[1]),
+           N.tptr(dT[2]), N.tptr(dD), nCh, nPt, Ns[0], Ns[1], Ns[2], nWin, float(kp[0]), float(kp[1]), N.tptr(bR),
+           N.tptr(bI), N.stream_ptr())
+    return bR, bI
+
+
 def bmGridder_n2u_leight(data_n, t, Dn, N_u, dK_u, kernelType=None, nWin=None, kernelParam=None):
     """data_n [nCh, nPt] (point layout), t [imDim, nPt], Dn [nPt] ->
     data_u [nCh, prod(N_u)] complex64 (column order of N_u)."""

@@ -259,6 +259,10 @@ def bmMathilda(y, t, v, C, N_u, n_u, dK_u, kernelType=None, nWin=None, kernelPar
     """Gridded reconstruction (bmMathilda.m:14-125, CUFFT branch): adjoint
     gridding -> bmIDF -> deapodisation -> crop -> coil pinv.
     y [nPt, nCh] -> x [prod(n_u)] (or [prod(n_u), nCh] without C)."""
+    import torch
+
+    from .gridding import bmGridder_n2u_leight_dev
+
     kernelType, nWin, kp = kernel_defaults(kernelType, nWin, kernelParam)
     y = np.asarray(y, np.complex64)
     if y.ndim == 1:
@@ -266,15 +270,69 @@ def bmMathilda(y, t, v, C, N_u, n_u, dK_u, kernelType=None, nWin=None, kernelPar
     if y.shape[0] < y.shape[1]:
         y = y.T  # bmMathilda.m:35-37 expects more points than coils
     N_u = _ints(N_u)
-    n_u = _ints(n_u)
     dK_u = np.ravel(dK_u).astype(np.float32).astype(np.float64)
     nCh = y.shape[1]
-    grid = bmGridder_n2u_leight if leight_flag else bmGridder_n2u
-    xg = grid(y.T, t, v, N_u, dK_u, kernelType, nWin, kp)  # [nCh, prod(N_u)]
-    x = xg.T.reshape(tuple(N_u) + (nCh,), order="F")
-    x = bmIDF(x, N_u, dK_u)
-    K = bmK(N_u, dK_u, nCh, kernelType, nWin, kp).reshape(tuple(N_u) + (nCh,), order="F")
-    x = (x * K).astype(np.complex64)[crop_index(N_u, n_u)].reshape(-1, nCh, order="F")
+    dev = torch.device("cuda", torch.cuda.current_device())
+    if leight_flag:
+        bR, bI = bmGridder_n2u_leight_dev(y.T, t, v, N_u, dK_u, kernelType, nWin, kp)
+    else:  # precomputed-weight gridder (host arguments), result moved to the device
+        xg = bmGridder_n2u(y.T, t, v, N_u, dK_u, kernelType, nWin, kp)  # [nCh, prod(N_u)]
+        bR = torch.from_numpy(np.ascontiguousarray(xg.real.T, np.float32)).to(dev)
+        bI = torch.from_numpy(np.ascontiguousarray(xg.imag.T, np.float32)).to(dev)
+    return _gridded_tail(bR, bI, N_u, n_u, dK_u, nCh, C, kernelType, nWin, kp)
+
+
+def _gridded_tail(ga, gb, N_u, n_u, dK_u, nCh, C, kernelType, nWin, kp, K=None):
+    """coil_pinv(crop(K .* bmIDF(grid))) on the device (mlg_gridded_tail_dev);
+    ga, gb: split [prod(N_u)][nCh] float32 CUDA tensors, or ga an interleaved
+    complex64 one and gb None.  Returns host x [prod(n_u)] with C, else
+    [prod(n_u), nCh]."""
+    import torch
+
+    N_u = _ints(N_u)
+    n_u = _ints(n_u if n_u is not None else N_u)
+    dev = ga.device
+    if K is None:
+        Kv = bmK(N_u, dK_u, 1, kernelType, nWin, kp)[:, 0]
+    else:  # [prod(N_u)] or [prod(N_u), nCh] (identical columns)
+        Kv = np.asarray(K, np.float32).reshape(int(np.prod(N_u)), -1, order="F")[:, 0]
+    Kd = torch.from_numpy(np.ascontiguousarray(Kv, np.float32)).to(dev)
+    nu = int(np.prod(n_u))
+    Cd = None
     if C is not None:
-        return bmCoilSense_pinv(np.asarray(C).reshape(x.shape[0], -1, order="F"), x)
-    return x
+        Cd = torch.from_numpy(np.ascontiguousarray(np.asarray(C, np.complex64).reshape(nu, -1, order="F"))).to(dev)
+        if Cd.shape[1] != nCh:
+            raise ValueError("C must be [prod(n_u), nCh]")
+    x = torch.empty((nu if C is not None else nCh * nu,), dtype=torch.complex64, device=dev)
+    N.call("mlg_gridded_tail_dev", N_u.size, N.iptr(N_u), N.iptr(n_u),
+           N.fptr(np.ascontiguousarray(np.ravel(dK_u), np.float32)), nCh, 1 if gb is not None else 0, N.tptr(ga),
+           N.tptr(gb), N.tptr(Kd), N.tptr(Cd), N.tptr(x), N.stream_ptr())
+    out = x.cpu().numpy()
+    return out if C is not None else out.reshape(nCh, nu).T.copy()
+
+
+def bmNasha(y, G, n_u=None, C=None, K=None):
+    """Gridded reconstruction with the Gn matrix (src/fourier123/
+    map_function/nonCartesian/bmNasha.m:6-91): x = Gn y, bmIDF, .* K, crop,
+    coil pinv (C given) -- all on the device.  y [nPt, nCh]; G the Gn
+    bmSparseMat or DeviceMatrix ([prod(N_u), nPt], from bmTraj2SparseMat
+    with nargout 1 or 3); K optional ([prod(N_u)] or [prod(N_u), nCh]),
+    computed from G's kernel when absent (:25-28)."""
+    import torch
+
+    Gd = G.to_device() if isinstance(G, bmSparseMat) else G
+    meta = Gd.meta
+    N_u = _ints(meta["N_u"])
+    dK_u = np.ravel(meta["d_u"]).astype(np.float32).astype(np.float64)
+    y = np.asarray(y, np.complex64)
+    if y.ndim == 1:
+        y = y[:, None]
+    nPt, nCh = y.shape
+    if nPt != Gd.r_size:  # bmNasha.m:117-120
+        raise ValueError("The data matrix 'y' is not in the correct size. ")
+    if np.any(N_u % 2):  # bmNasha.m:137-140
+        raise ValueError("N_u must have all components even for the Fourier transform. ")
+    dev = torch.device("cuda", torch.cuda.current_device())
+    g = Gd.spmm(torch.from_numpy(np.ascontiguousarray(y)).to(dev))  # [prod(N_u)][nCh]
+    return _gridded_tail(g, None, N_u, n_u, dK_u, nCh, C, meta["kernel_type"], int(meta["nWin"]),
+                         np.ravel(meta["kernelParam"]).astype(np.float64), K)

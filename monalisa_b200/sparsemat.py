@@ -174,10 +174,11 @@ class DeviceMatrix:
             pass
 
 
-def bmTraj2SparseMat(t, v, N_u, dK_u, kernelType=None, nWin=None, kernelParam=None):
-    """GPU form of src/gridding123/m/bmTraj2SparseMat.m (two outputs): returns
-    device-resident (Gu, Gut).  t [imDim, nPt] physical units, v volume
-    elements (they cancel in the row-normalised Gu/Gut)."""
+def bmTraj2SparseMat(t, v, N_u, dK_u, kernelType=None, nWin=None, kernelParam=None, nargout=2):
+    """GPU form of src/gridding123/m/bmTraj2SparseMat.m: returns
+    device-resident (Gu, Gut) (nargout 2), Gn (nargout 1) or (Gn, Gu, Gut)
+    (nargout 3).  t [imDim, nPt] physical units, v volume elements (they
+    cancel in the row-normalised Gu/Gut; Gn carries them, :245-256)."""
     kernelType, nWin, kp = kernel_defaults(kernelType, nWin, kernelParam)
     t = np.asarray(t, np.float64)
     if t.ndim == 1:
@@ -188,12 +189,21 @@ def bmTraj2SparseMat(t, v, N_u, dK_u, kernelType=None, nWin=None, kernelParam=No
     dK = np.ascontiguousarray(np.ravel(dK_u), np.float64)
     kp3 = np.zeros(3)
     kp3[:kp.size] = kp
-    hu, ht = ctypes.c_void_p(), ctypes.c_void_p()
-    N.call("mlg_traj2sparsemat", imDim, nPt, N.dptr(tt), None, N.iptr(Nu), N.dptr(dK), kernel_code(kernelType),
-           nWin, N.dptr(kp3), ctypes.byref(hu), ctypes.byref(ht))
+    if nargout not in (1, 2, 3):
+        raise ValueError("nargout must be 1, 2 or 3")
+    want_n, want_u = nargout in (1, 3), nargout in (2, 3)
+    ve = np.ascontiguousarray(np.ravel(v), np.float64) if want_n else None
+    hn, hu, ht = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()
+    N.call("mlg_traj2sparsemat3", imDim, nPt, N.dptr(tt), N.dptr(ve), N.iptr(Nu), N.dptr(dK),
+           kernel_code(kernelType), nWin, N.dptr(kp3), ctypes.byref(hn) if want_n else None,
+           ctypes.byref(hu) if want_u else None, ctypes.byref(ht) if want_u else None)
     meta = dict(N_u=Nu.copy(), d_u=dK.astype(np.float32), kernel_type=kernelType, nWin=nWin,
                 kernelParam=kp.astype(np.float32))
-    return DeviceMatrix(hu, meta, False), DeviceMatrix(ht, meta, True)
+    Gn = DeviceMatrix(hn, meta, True) if want_n else None
+    if nargout == 1:
+        return Gn
+    Gu, Gut = DeviceMatrix(hu, meta, False), DeviceMatrix(ht, meta, True)
+    return (Gn, Gu, Gut) if nargout == 3 else (Gu, Gut)
 
 
 def bmSparseMat_vec(G: bmSparseMat, v, layout: str = "column"):

@@ -693,6 +693,30 @@ def bmMathilda(y, t, v, C, N_u, n_u, dK_u, kernelType=None, nWin=None, kernelPar
     return x
 
 
+def bmNasha(y, Gn: SparseMat, n_u, C=None, K=None, spmv=None):
+    """bmNasha.m:6-91 (MATLAB FFT branch): x = Gn y (the complex column
+    product, :45), reshape to N_u, bmIDF, .* K (:77), crop (:80-82), coil
+    pinv (:85-88).  y [nPt, nCh] -> x [prod(n_u)] (C given) or
+    [prod(n_u), nCh]."""
+    y = np.asarray(y, np.complex64)
+    if y.ndim == 1:
+        y = y[:, None]
+    nCh = y.shape[1]
+    N_u = np.ravel(Gn.N_u).astype(int)
+    n_u = N_u if n_u is None else np.ravel(n_u).astype(int)
+    dK_u = single(np.ravel(Gn.d_u))
+    if K is None:
+        K = bmK(N_u, dK_u, nCh, Gn.kernel_type, Gn.nWin, Gn.kernelParam)
+    x = _spmv(spmv)(Gn, y)  # [prod(N_u), nCh]
+    x = x.reshape(tuple(N_u) + (nCh,), order="F")
+    x = bmIDF(x, N_u, dK_u)
+    x = (x * np.asarray(K, np.float32).reshape(tuple(N_u) + (-1,), order="F")).astype(np.complex64)
+    x = x[crop_index(N_u, n_u)].reshape(-1, nCh, order="F")
+    if C is not None:
+        return coil_pinv(np.asarray(C).reshape(x.shape[0], -1, order="F"), x)
+    return x
+
+
 # --------------------------------------------------------------------------
 # solvers (FP32 data, FP64 scalars)
 # --------------------------------------------------------------------------

@@ -186,6 +186,50 @@ def test_traj2sparsemat_gpu_matches_restatement():
             assert np.allclose(dev.m_val, r.m_val, rtol=2e-7, atol=0)
 
 
+def test_gn_builder_matches_restatement():
+    """The Gn output of the GPU builder (nargout 3) against the restatement
+    of bmTraj2SparseMat.m:245-264: same pattern, values within one float
+    rounding (FP64 weights and cell sums on both sides)."""
+    import monalisa_b200 as mb
+
+    rng = np.random.default_rng(18)
+    for imDim, N, kt, kp, nWin, dK in ((2, [24, 20], "kaiser", [1.95, 10, 10], 3, [1.0, 0.5]),
+                                       (3, [12, 10, 14], "gauss", [0.61, 10], 3, [1.0, 1.0, 2.0])):
+        nPt = 900
+        t = rng.uniform(-0.6, 0.6, (imDim, nPt)) * (np.array(N) * np.array(dK))[:, None]
+        ve = rng.uniform(0.5, 1.5, nPt)
+        ref = oracle.traj2sparsemat(t, ve, N, dK, kt, nWin, kp, want=("Gn",))["Gn"]
+        Gn, Gu, Gut = mb.bmTraj2SparseMat(t, ve, N, dK, kt, nWin, kp, nargout=3)
+        dev = Gn.download()
+        assert np.array_equal(dev.r_nJump, ref.r_nJump)
+        assert np.array_equal(dev.r_jump, ref.r_jump)
+        assert np.array_equal(dev.l_jump, ref.l_jump)
+        assert np.allclose(dev.m_val, ref.m_val, rtol=2.5e-7, atol=0)
+        assert mb.bmTraj2SparseMat(t, ve, N, dK, kt, nWin, kp, nargout=1).nnz == Gn.nnz
+
+
+@pytest.mark.parametrize("with_C", [True, False])
+def test_nasha_matches_oracle(with_C):
+    """bmNasha (Gn product, IDF, K, crop, coil pinv on the device) against
+    the restatement of bmNasha.m, relative L2 <= 1e-5."""
+    import monalisa_b200 as mb
+    from monalisa_b200 import traj
+
+    rng = np.random.default_rng(19)
+    N_u, n_u, nCh, kp = np.array([40, 32]), np.array([20, 16]), 3, [1.95, 10, 10]
+    t = traj.golden_angle_radial2(40, 36, 1.0)
+    ve = traj.bmVolumeElement_voronoi_full_radial2(t, 40)
+    G = oracle.traj2sparsemat(t, ve, N_u, [1, 1], "kaiser", 3, kp, want=("Gn",))["Gn"]
+    y = (rng.standard_normal((t.shape[1], nCh)) + 1j * rng.standard_normal((t.shape[1], nCh))).astype(np.complex64)
+    C = traj.coil_maps(n_u, nCh, 4) if with_C else None
+    Gb = mb.bmSparseMat(r_size=G.r_size, r_jump=G.r_jump, r_nJump=G.r_nJump, m_val=G.m_val, l_size=G.l_size,
+                        l_jump=G.l_jump, l_nJump=G.l_nJump, N_u=N_u, d_u=np.array([1, 1], np.float32),
+                        kernel_type="kaiser", nWin=3, kernelParam=np.array(kp, np.float32))
+    x = mb.bmNasha(y, Gb, n_u, C)
+    xo = oracle.bmNasha(y, G, n_u, C)
+    assert x.shape == xo.shape and rel(x, xo) <= 1e-5
+
+
 @pytest.fixture(scope="module")
 def op2d():
     g = _g("operators2d")
@@ -336,6 +380,14 @@ def test_mathilda_matches_oracle():
     C = traj.coil_maps(n_u, nCh, 3)
     x = mb.bmMathilda(y, t, ve, C, N_u, n_u, [1, 1])
     xo = oracle.bmMathilda(y, t, ve, C, N_u, n_u, [1, 1])
+    assert rel(x, xo) <= 1e-5
+    # every coil's image (no C), and the precomputed-weight (Kaiser) gridder
+    x = mb.bmMathilda(y, t, ve, None, N_u, n_u, [1, 1])
+    xo = oracle.bmMathilda(y, t, ve, None, N_u, n_u, [1, 1])
+    assert x.shape == xo.shape == (256, nCh) and rel(x, xo) <= 1e-5
+    kp = [1.95, 10, 10]
+    x = mb.bmMathilda(y, t, ve, C, N_u, n_u, [1, 1], "kaiser", 3, kp, leight_flag=False)
+    xo = oracle.bmMathilda(y, t, ve, C, N_u, n_u, [1, 1], "kaiser", 3, kp, leight=False)
     assert rel(x, xo) <= 1e-5
 
 
