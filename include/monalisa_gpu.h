@@ -314,6 +314,20 @@ int mlg_plan_get_adjoint(mlg_plan_t p, int* mode);
  * negative for strategies the plan cannot run. */
 int mlg_plan_autotune(mlg_plan_t p, int reps, double* ms);
 
+/* Precision of the plan's CG-SENSE solver (mlg_sensa_dev / mlg_sensa).
+ * MLG_PRECISION_FP32: FP32 data and matrix values, FP64 scalars (the
+ * reference's single-precision arithmetic).  MLG_PRECISION_MIXED: FP16 matrix
+ * values (copies of Gu/Gut made once), BF16 storage of the k-space work
+ * vectors (residual, M p), FP32 sums and FFTs, FP64 scalars; the caller's y
+ * and x stay complex64.  Mixed precision turns the fused-gather adjoint
+ * strategy off (it reads FP32 k-space).  The operator entry points
+ * (mlg_shanna_dev, mlg_nakatsha_dev) of a mixed plan read the FP16 values
+ * but keep their complex64 k-space buffers.  No reference counterpart. */
+#define MLG_PRECISION_FP32 0
+#define MLG_PRECISION_MIXED 1
+int mlg_plan_set_precision(mlg_plan_t p, int precision);
+int mlg_plan_get_precision(mlg_plan_t p, int* precision);
+
 /* Times the stages of one Shanna and one Nakatsha on the plan's stream with
  * CUDA events, averaged over `iters` repetitions after one warm-up:
  * ms[0..2] forward x, y, z FFT passes (x pass fused with x .* KFC),

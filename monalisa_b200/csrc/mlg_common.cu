@@ -87,6 +87,7 @@ void csr_free(Csr& c) {
   cudaFree(c.long_seg0);
   cudaFree(c.nz_rows);
   cudaFree(c.nz_mask);
+  cudaFree(c.val_h);
   c = Csr();
 }
 

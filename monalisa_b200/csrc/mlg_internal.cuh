@@ -1,6 +1,8 @@
 // Internal declarations shared by the libmonalisa_gpu translation units.
 #pragma once
 
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <cufft.h>
 
@@ -125,6 +127,8 @@ struct Csr {
   // csr_build_nonempty
   int* nz_rows = nullptr;
   uint32_t* nz_mask = nullptr;
+  // FP16 copy of val for the mixed-precision solver (built on demand)
+  __half* val_h = nullptr;
 };
 constexpr int kSegLen = 512;
 
@@ -162,6 +166,8 @@ int csr_sign_copy(const Csr& src, bool by_row, int imDim, const int* N, float gl
                   cudaStream_t s);
 // Frees a copy made by csr_sign_copy (only its values are owned).
 void csr_free_sign_copy(Csr& c);
+// Adds the FP16 copy of the values (val_h) if absent.
+int csr_make_half(Csr& c, cudaStream_t s);
 
 // ---- SpMM kernels (mlg_sparsemat.cu) ---------------------------------------
 // Element layouts of the dense operands.
@@ -172,6 +178,7 @@ enum class Layout : int {
   kPointSplit = 3, // float re[rows][nCh], im[...] (MATLAB point layout)
   kCoilReal = 4,   // float [nCh][rows]           (real, column layout)
   kPointReal = 5,  // float [rows][nCh]           (real, row layout)
+  kPointBF16 = 6,  // __nv_bfloat162 [rows][nCh]  (complex, BF16 storage, coil fastest)
 };
 
 struct Operand {
@@ -204,6 +211,9 @@ struct SpmmArgs {
   // Only the non-empty rows (m->nz_rows, which must exist) are computed and
   // written; the others are left untouched.
   bool nonempty_only = false;
+  // Read the matrix values from m->val_h (FP16) instead of m->val; the sums
+  // stay FP32.
+  bool half_values = false;
 };
 
 // Scratch floats spmm needs for the long-row segments of `m` at nCh coils.

@@ -109,7 +109,8 @@ static bool fused_gut(const mlg_plan_s* p) { return p->adjoint_mode == kAdjFused
 // adjoint variants a plan can run
 bool adjoint_mode_valid(const mlg_plan_s* p, int mode) {
   if (mode == kAdjFullGrid) return true;
-  if (mode == kAdjFused) return p->imDim >= 2;
+  // the fused gather reads FP32 k-space inside the FFT pass: not in mixed precision
+  if (mode == kAdjFused) return p->imDim >= 2 && p->precision == 0;
   if (mode == kAdjMasked) return (p->nCh % 2) == 0 && p->Gut_s.nz_mask != nullptr;
   return false;
 }
@@ -201,7 +202,8 @@ int shanna_stage(mlg_plan_s* p, int stage, const float2* x, bool x_per_coil, flo
   a.in.layout = Layout::kPointC64;
   a.in.a = p->grid;
   a.in.rows = p->Nu_tot;
-  a.out.layout = Layout::kPointC64;
+  a.out.layout = p->mixed_run ? Layout::kPointBF16 : Layout::kPointC64;  // k-space storage
+  a.half_values = p->precision == MLG_PRECISION_MIXED;
   a.out.a = y;
   a.out.rows = p->nPt;
   a.sqn_row_weight = sqn_w;
@@ -223,7 +225,8 @@ int nakatsha_stage(mlg_plan_s* p, int stage, const float2* y, const float* HY, f
     SpmmArgs a;
     a.m = &p->Gut_s;
     a.nCh = p->nCh;
-    a.in.layout = Layout::kPointC64;
+    a.in.layout = p->mixed_run ? Layout::kPointBF16 : Layout::kPointC64;  // k-space storage
+    a.half_values = p->precision == MLG_PRECISION_MIXED;
     a.in.a = const_cast<float2*>(y);
     a.in.rows = p->nPt;
     a.in_row_scale = HY;

@@ -55,6 +55,12 @@ struct mlg_plan_s {
   // matrices) borrows that plan's KFC, KFCc, grid, bufA, bufB, FFT tables,
   // stream and events; both then run in the order of that one stream.
   bool borrowed = false;
+  // MLG_PRECISION_FP32 or MLG_PRECISION_MIXED (the CG-SENSE solver then keeps
+  // its k-space vectors in BF16 and reads FP16 matrix values); mixed_run is
+  // set while such a solve runs and selects those forms in the stages
+  int precision = 0;
+  bool mixed_run = false;
+  int cg_graph_prec = -1;  // precision the captured CG step was built for
   mlg_plan_s* owner = nullptr;  // the plan whose buffers are borrowed
   int n_borrowers = 0;          // plans borrowing this one's buffers
 };

@@ -77,15 +77,33 @@ __global__ void max_kernel(const float* __restrict__ v, int n, float* out) {
   if (threadIdx.x == 0) out[blockIdx.x] = sh[0];
 }
 
-// res = y - Mx (k-space), optional partials of sum HY |res|^2
-__global__ void residual_kernel(const float2* __restrict__ y, const float2* __restrict__ Mx, long long n, int nCh,
-                                const float* __restrict__ HY, float2* __restrict__ res, double* partial) {
+// k-space work vectors: FP32 complex, or BF16 pairs in mixed precision
+template <bool BF>
+__device__ __forceinline__ float2 kld(const void* v, long long i) {
+  if constexpr (BF)
+    return __bfloat1622float2(reinterpret_cast<const __nv_bfloat162*>(v)[i]);
+  else
+    return reinterpret_cast<const float2*>(v)[i];
+}
+template <bool BF>
+__device__ __forceinline__ void kst(void* v, long long i, float2 x) {
+  if constexpr (BF)
+    reinterpret_cast<__nv_bfloat162*>(v)[i] = __float22bfloat162_rn(x);
+  else
+    reinterpret_cast<float2*>(v)[i] = x;
+}
+
+// res = y - Mx (k-space), optional partials of sum HY |res|^2; y is the
+// caller's FP32 data, Mx and res the work vectors
+template <bool BF>
+__global__ void residual_kernel(const float2* __restrict__ y, const void* __restrict__ Mx, long long n, int nCh,
+                                const float* __restrict__ HY, void* __restrict__ res, double* partial) {
   __shared__ double sh[kT / 32];
   double sq = 0.0;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-    const float2 a = y[i], b = Mx[i];
+    const float2 a = y[i], b = kld<BF>(Mx, i);
     const float2 r = make_float2(__fsub_rn(a.x, b.x), __fsub_rn(a.y, b.y));
-    if (res) res[i] = r;
+    if (res) kst<BF>(res, i, r);
     sq += (double)HY[i / nCh] * ((double)r.x * r.x + (double)r.y * r.y);
   }
   if (partial) {
@@ -150,17 +168,26 @@ __global__ void cg_update_x_kernel(float2* __restrict__ x, const float2* __restr
 }
 
 // res -= a Mp   (bmSensa.m:71)
-__global__ void cg_update_res_kernel(float2* __restrict__ res, const float2* __restrict__ Mp, long long n,
+template <bool BF>
+__global__ void cg_update_res_kernel(void* __restrict__ res, const void* __restrict__ Mp, long long n,
                                      const double* __restrict__ sc) {
   if (sc[S_DONE] != 0.0) return;
   const float a = (float)sc[S_A];
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-    const float2 m = Mp[i];
-    float2 r = res[i];
+    const float2 m = kld<BF>(Mp, i);
+    float2 r = kld<BF>(res, i);
     r.x = __fsub_rn(r.x, __fmul_rn(a, m.x));
     r.y = __fsub_rn(r.y, __fmul_rn(a, m.y));
-    res[i] = r;
+    kst<BF>(res, i, r);
   }
+}
+
+static void launch_residual(bool bf, int g, const float2* y, const void* Mx, long long n, int nCh, const float* HY,
+                            void* res, double* partial, cudaStream_t s) {
+  if (bf)
+    residual_kernel<true><<<g, kT, 0, s>>>(y, Mx, n, nCh, HY, res, partial);
+  else
+    residual_kernel<false><<<g, kT, 0, s>>>(y, Mx, n, nCh, HY, res, partial);
 }
 
 // p = dagM + b p   (bmSensa.m:77)
@@ -202,7 +229,10 @@ static int cg_step(mlg_plan_s* p, float2* x, double HX, double eps, cudaStream_t
   MLG_LAUNCHED();
   cg_update_x_kernel<<<grid1(p->nu_tot), kT, 0, s>>>(x, p->x_p, p->nu_tot, p->scalars);
   MLG_LAUNCHED();
-  cg_update_res_kernel<<<grid1(nk), kT, 0, s>>>(p->k_res, p->k_Mp, nk, p->scalars);
+  if (p->mixed_run)
+    cg_update_res_kernel<true><<<grid1(nk), kT, 0, s>>>(p->k_res, p->k_Mp, nk, p->scalars);
+  else
+    cg_update_res_kernel<false><<<grid1(nk), kT, 0, s>>>(p->k_res, p->k_Mp, nk, p->scalars);
   MLG_LAUNCHED();
   MLG_TRY(nakatsha_run(p, p->k_res, p->HY, (float)(1.0 / HX), p->x_dagM, p->partial, &np, s));
   cg_beta_kernel<<<1, kT, 0, s>>>(p->partial, np, HX, eps, p->scalars);
@@ -212,10 +242,21 @@ static int cg_step(mlg_plan_s* p, float2* x, double HX, double eps, cudaStream_t
   return MLG_OK;
 }
 
+static int sensa_body(mlg_plan_s* p, const float2* y, const float* ve, float ve_max, int nIter, int nCGD, float2* x,
+                      double* residual, bool use_graph, cudaStream_t s);
+
 int sensa_run(mlg_plan_s* p, const float2* y, const float* ve, float ve_max, int nIter, int nCGD, float2* x,
               double* residual, bool use_graph, cudaStream_t s) {
   MLG_CHECK(p->Gu && p->Gut, "CG-SENSE needs a plan with both Gu and Gut");
   MLG_CHECK(nIter >= 0 && nCGD >= 0, "nIter / nCGD must be >= 0");
+  p->mixed_run = p->precision == MLG_PRECISION_MIXED;
+  const int st = sensa_body(p, y, ve, ve_max, nIter, nCGD, x, residual, use_graph, s);
+  p->mixed_run = false;
+  return st;
+}
+
+static int sensa_body(mlg_plan_s* p, const float2* y, const float* ve, float ve_max, int nIter, int nCGD, float2* x,
+                      double* residual, bool use_graph, cudaStream_t s) {
   MLG_TRY(ensure_solver_buffers(p));
   const long long nk = (long long)p->nPt * p->nCh;
   const double HX = p->HX;
@@ -240,7 +281,8 @@ int sensa_run(mlg_plan_s* p, const float2* y, const float* ve, float ve_max, int
   // every kernel of the step at least once (first launches set kernel
   // attributes, which must not happen during capture).
   auto ensure_graph = [&]() -> int {
-    if (!use_graph || full == 0 || (p->cg_graph && p->cg_graph_x == x)) return MLG_OK;
+    if (!use_graph || full == 0 || (p->cg_graph && p->cg_graph_x == x && p->cg_graph_prec == (int)p->mixed_run))
+      return MLG_OK;
     if (p->cg_graph) cudaGraphExecDestroy(p->cg_graph);
     p->cg_graph = nullptr;
     cudaGraph_t graph;
@@ -256,6 +298,7 @@ int sensa_run(mlg_plan_s* p, const float2* y, const float* ve, float ve_max, int
     cudaGraphDestroy(graph);
     if (ie != cudaSuccess) return fail(MLG_ERR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(ie));
     p->cg_graph_x = x;
+    p->cg_graph_prec = (int)p->mixed_run;
     return MLG_OK;
   };
 
@@ -265,7 +308,7 @@ int sensa_run(mlg_plan_s* p, const float2* y, const float* ve, float ve_max, int
     // res = y - M x; dagM = (1/HX) M*(HY res); sqn = HX |dagM|^2; p = dagM
     int np = 0;
     MLG_TRY(shanna_run(p, x, false, p->k_Mp, nullptr, nullptr, nullptr, s));
-    residual_kernel<<<grid1(nk), kT, 0, s>>>(y, p->k_Mp, nk, p->nCh, p->HY, p->k_res, nullptr);
+    launch_residual(p->mixed_run, grid1(nk), y, p->k_Mp, nk, p->nCh, p->HY, p->k_res, nullptr, s);
     MLG_LAUNCHED();
     MLG_TRY(nakatsha_run(p, p->k_res, p->HY, (float)(1.0 / HX), p->x_dagM, p->partial, &np, s));
     cg_init_kernel<<<1, kT, 0, s>>>(p->partial, np, HX, eps, p->scalars);
@@ -290,7 +333,7 @@ int sensa_run(mlg_plan_s* p, const float2* y, const float* ve, float ve_max, int
     // monitoring: R = |y - Mx|^2_HY   (bmSensa.m:82-83)
     MLG_TRY(shanna_run(p, x, false, p->k_Mp, nullptr, nullptr, nullptr, s));
     const int g = grid1(nk);
-    residual_kernel<<<g, kT, 0, s>>>(y, p->k_Mp, nk, p->nCh, p->HY, nullptr, p->partial);
+    launch_residual(p->mixed_run, g, y, p->k_Mp, nk, p->nCh, p->HY, nullptr, p->partial, s);
     MLG_LAUNCHED();
     sum_to_slot_kernel<<<1, kT, 0, s>>>(p->partial, g, hist.p, it);
     MLG_LAUNCHED();
@@ -440,6 +483,7 @@ extern "C" int mlg_plan_autotune(mlg_plan_t p, int reps, double* ms) {
   int best = orig;
   double best_ms = 1e30;
   int st = MLG_OK;
+  p->mixed_run = p->precision == MLG_PRECISION_MIXED;  // time the form the solver runs
   for (int mode = 0; mode < 3 && st == MLG_OK; ++mode) {
     double t = -1.0;
     if (adjoint_mode_valid(p, mode)) {
@@ -462,7 +506,35 @@ extern "C" int mlg_plan_autotune(mlg_plan_t p, int reps, double* ms) {
   }
   cudaEventDestroy(a);
   cudaEventDestroy(b);
+  p->mixed_run = false;
   p->adjoint_mode = orig;
   if (st != MLG_OK) return st;
   return mlg_plan_set_adjoint(p, best);
+}
+
+extern "C" int mlg_plan_set_precision(mlg_plan_t p, int precision) {
+  using namespace mlg;
+  MLG_CHECK(p, "NULL plan");
+  MLG_CHECK(precision == MLG_PRECISION_FP32 || precision == MLG_PRECISION_MIXED, "unknown precision %d",
+            precision);
+  MLG_CUDA(cudaSetDevice(p->device));
+  if (precision == MLG_PRECISION_MIXED) {
+    MLG_CHECK(p->Gu && p->Gut, "mixed precision needs a plan with both Gu and Gut");
+    MLG_TRY(csr_make_half(p->Gu_s, p->stream));
+    MLG_TRY(csr_make_half(p->Gut_s, p->stream));
+    MLG_CUDA(cudaStreamSynchronize(p->stream));
+  }
+  p->precision = precision;
+  if (!adjoint_mode_valid(p, p->adjoint_mode))  // the fused gather reads FP32 k-space
+    p->adjoint_mode = adjoint_mode_valid(p, 2) ? 2 : 0;
+  if (p->cg_graph) cudaGraphExecDestroy(p->cg_graph);
+  p->cg_graph = nullptr;
+  p->cg_graph_x = nullptr;
+  return MLG_OK;
+}
+
+extern "C" int mlg_plan_get_precision(mlg_plan_t p, int* precision) {
+  MLG_CHECK(p && precision, "NULL argument");
+  *precision = p->precision;
+  return MLG_OK;
 }

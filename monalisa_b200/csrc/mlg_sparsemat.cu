@@ -26,6 +26,7 @@ struct SpmmParams {
   const uint32_t* row_ptr;
   const int* col;
   const float* val;
+  const __half* val_h;  // FP16 values in place of val when set
   int l_size;
   int nCh;
   int rows_per_block;
@@ -55,6 +56,8 @@ __device__ __forceinline__ float2 ld(const Operand& o, long long row, int c, int
     return make_float2(__ldg(reinterpret_cast<const float*>(o.a) + i), __ldg(reinterpret_cast<const float*>(o.b) + i));
   } else if constexpr (L == Layout::kPointReal) {
     return make_float2(__ldg(reinterpret_cast<const float*>(o.a) + row * nCh + c), 0.f);
+  } else if constexpr (L == Layout::kPointBF16) {
+    return __bfloat1622float2(reinterpret_cast<const __nv_bfloat162*>(o.a)[row * nCh + c]);
   } else {
     return make_float2(__ldg(reinterpret_cast<const float*>(o.a) + (long long)c * o.rows + row), 0.f);
   }
@@ -76,9 +79,15 @@ __device__ __forceinline__ void st(const Operand& o, long long row, int c, int n
     reinterpret_cast<float*>(o.b)[i] = v.y;
   } else if constexpr (L == Layout::kPointReal) {
     reinterpret_cast<float*>(o.a)[row * nCh + c] = v.x;
+  } else if constexpr (L == Layout::kPointBF16) {
+    reinterpret_cast<__nv_bfloat162*>(o.a)[row * nCh + c] = __float22bfloat162_rn(v);
   } else {
     reinterpret_cast<float*>(o.a)[(long long)c * o.rows + row] = v.x;
   }
+}
+
+__device__ __forceinline__ float val_at(const SpmmParams& p, uint32_t k) {
+  return p.val_h ? __half2float(p.val_h[k]) : __ldg(p.val + k);
 }
 
 // Accumulates entries [b, e) with stride `step` of one row for coil c.
@@ -89,7 +98,7 @@ __device__ __forceinline__ void accumulate(const SpmmParams& p, uint32_t b, uint
 #pragma unroll 4
   for (uint32_t k = b; k < e; k += step) {
     const int j = __ldg(p.col + k);
-    const float m = __ldg(p.val + k);
+    const float m = val_at(p, k);
     float2 v = ld<IN>(p.in, j, c, p.nCh);
     if (scale) {
       const float h = __ldg(p.in_row_scale + j);
@@ -226,13 +235,39 @@ __global__ void __launch_bounds__(256) spmm_seg_combine_kernel(SpmmParams p, con
 // once per pair instead of once per coil.  `rows` (optional) lists the rows
 // to compute (the non-empty ones); other rows are left untouched.  Entries
 // are summed in stored order with round-to-nearest multiply/add.
+// A coil pair: two complex values, FP32 (float4) or BF16 (4 x bf16 = uint2).
+template <bool BF>
+__device__ __forceinline__ float4 ld_pair(const void* base, long long i) {
+  if constexpr (BF) {
+    const uint2 r = __ldg(reinterpret_cast<const uint2*>(base) + i);
+    const float2 a = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&r.x));
+    const float2 b = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&r.y));
+    return make_float4(a.x, a.y, b.x, b.y);
+  } else {
+    return __ldg(reinterpret_cast<const float4*>(base) + i);
+  }
+}
+
+template <bool BF>
+__device__ __forceinline__ void st_pair(void* base, long long i, float4 v) {
+  if constexpr (BF) {
+    const __nv_bfloat162 a = __float22bfloat162_rn(make_float2(v.x, v.y));
+    const __nv_bfloat162 b = __float22bfloat162_rn(make_float2(v.z, v.w));
+    uint2 r;
+    r.x = *reinterpret_cast<const unsigned int*>(&a);
+    r.y = *reinterpret_cast<const unsigned int*>(&b);
+    reinterpret_cast<uint2*>(base)[i] = r;
+  } else {
+    reinterpret_cast<float4*>(base)[i] = v;
+  }
+}
+
+template <bool IN_BF, bool OUT_BF>
 __global__ void __launch_bounds__(256) spmm_pair_kernel(SpmmParams p, const int* __restrict__ rows, int n_rows) {
   __shared__ double sh[32];
   const int P = p.nCh >> 1;
   const long long i0 = (long long)blockIdx.x * p.rows_per_block;
   const int nr = (int)min((long long)p.rows_per_block, (long long)n_rows - i0);
-  const float4* in = reinterpret_cast<const float4*>(p.in.a);
-  float4* out = reinterpret_cast<float4*>(p.out.a);
   const bool scale = p.in_row_scale != nullptr;
   double sq = 0.0;
   for (int it = threadIdx.x; it < nr * P; it += blockDim.x) {
@@ -244,8 +279,8 @@ __global__ void __launch_bounds__(256) spmm_pair_kernel(SpmmParams p, const int*
 #pragma unroll 4
     for (uint32_t k = b; k < e; ++k) {
       const int j = __ldg(p.col + k);
-      const float m = __ldg(p.val + k);
-      float4 v = __ldg(in + (long long)j * P + pi);
+      const float m = val_at(p, k);
+      float4 v = ld_pair<IN_BF>(p.in.a, (long long)j * P + pi);
       if (scale) {
         const float h = __ldg(p.in_row_scale + j);
         v = make_float4(__fmul_rn(h, v.x), __fmul_rn(h, v.y), __fmul_rn(h, v.z), __fmul_rn(h, v.w));
@@ -258,7 +293,7 @@ __global__ void __launch_bounds__(256) spmm_pair_kernel(SpmmParams p, const int*
     if (p.out_scale != 1.0f)
       acc = make_float4(__fmul_rn(acc.x, p.out_scale), __fmul_rn(acc.y, p.out_scale), __fmul_rn(acc.z, p.out_scale),
                         __fmul_rn(acc.w, p.out_scale));
-    out[r * P + pi] = acc;
+    st_pair<OUT_BF>(p.out.a, r * P + pi, acc);
     if (p.partial) {
       const double w = p.sqn_w ? (double)__ldg(p.sqn_w + r) : 1.0;
       sq += w * ((double)acc.x * acc.x + (double)acc.y * acc.y + (double)acc.z * acc.z + (double)acc.w * acc.w);
@@ -270,8 +305,10 @@ __global__ void __launch_bounds__(256) spmm_pair_kernel(SpmmParams p, const int*
   }
 }
 
+static bool point_c(Layout l) { return l == Layout::kPointC64 || l == Layout::kPointBF16; }
+
 static bool use_pair_kernel(const SpmmArgs& a) {
-  return a.in.layout == Layout::kPointC64 && a.out.layout == Layout::kPointC64 && (a.nCh % 2) == 0 && !a.normalize;
+  return point_c(a.in.layout) && point_c(a.out.layout) && (a.nCh % 2) == 0 && !a.normalize;
 }
 
 static int rows_per_block(const SpmmArgs& a) {
@@ -310,6 +347,8 @@ int spmm(const SpmmArgs& a, cudaStream_t s) {
   p.row_ptr = m.row_ptr;
   p.col = m.col;
   p.val = m.val;
+  MLG_CHECK(!a.half_values || m.val_h || m.nnz == 0, "FP16 values requested but not built");
+  p.val_h = a.half_values ? m.val_h : nullptr;
   p.l_size = m.l_size;
   p.nCh = a.nCh;
   p.rows_per_block = rows_per_block(a);
@@ -337,18 +376,35 @@ int spmm(const SpmmArgs& a, cudaStream_t s) {
   }
   float3* sc3 = reinterpret_cast<float3*>(scratch);
   using L = Layout;
+  const L i = a.in.layout, o = a.out.layout;
   if (use_pair_kernel(a)) {
+    const bool ib = i == L::kPointBF16, ob = o == L::kPointBF16;
     if (grid_short > 0) {
-      spmm_pair_kernel<<<grid_short, 256, 0, s>>>(p, a.nonempty_only ? m.nz_rows : nullptr, (int)nrows);
+      const int* rl = a.nonempty_only ? m.nz_rows : nullptr;
+      if (ib && !ob)
+        spmm_pair_kernel<true, false><<<grid_short, 256, 0, s>>>(p, rl, (int)nrows);
+      else if (!ib && ob)
+        spmm_pair_kernel<false, true><<<grid_short, 256, 0, s>>>(p, rl, (int)nrows);
+      else if (ib && ob)
+        spmm_pair_kernel<true, true><<<grid_short, 256, 0, s>>>(p, rl, (int)nrows);
+      else
+        spmm_pair_kernel<false, false><<<grid_short, 256, 0, s>>>(p, rl, (int)nrows);
       MLG_LAUNCHED();
     }
+    // long rows (segment kernels) with the same element types
+    if (ib && !ob) return launch<L::kPointBF16, L::kPointC64, false>(p, m, sc3, 0, s);
+    if (!ib && ob) return launch<L::kPointC64, L::kPointBF16, false>(p, m, sc3, 0, s);
+    if (ib && ob) return launch<L::kPointBF16, L::kPointBF16, false>(p, m, sc3, 0, s);
     return launch<L::kPointC64, L::kPointC64, false>(p, m, sc3, 0, s);
   }
-  const L i = a.in.layout, o = a.out.layout;
   if (i == L::kCoilC64 && o == L::kPointC64) return launch<L::kCoilC64, L::kPointC64, false>(p, m, sc3, grid_short, s);
   if (i == L::kPointC64 && o == L::kCoilC64) return launch<L::kPointC64, L::kCoilC64, true>(p, m, sc3, grid_short, s);
   if (i == L::kPointC64 && o == L::kPointC64)
     return launch<L::kPointC64, L::kPointC64, false>(p, m, sc3, grid_short, s);
+  if (i == L::kPointC64 && o == L::kPointBF16)
+    return launch<L::kPointC64, L::kPointBF16, false>(p, m, sc3, grid_short, s);
+  if (i == L::kPointBF16 && o == L::kPointC64)
+    return launch<L::kPointBF16, L::kPointC64, false>(p, m, sc3, grid_short, s);
   if (i == L::kCoilSplit && o == L::kCoilSplit)
     return launch<L::kCoilSplit, L::kCoilSplit, true>(p, m, sc3, grid_short, s);
   if (i == L::kPointSplit && o == L::kPointSplit)
@@ -387,13 +443,29 @@ __global__ void sign_by_row_kernel(const uint32_t* __restrict__ row_ptr, const f
 
 void csr_free_sign_copy(Csr& c) {
   cudaFree(c.val);
+  cudaFree(c.val_h);
   c = Csr();
+}
+
+__global__ void to_half_kernel(const float* __restrict__ v, long long n, __half* __restrict__ h) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    h[i] = __float2half_rn(v[i]);
+}
+
+int csr_make_half(Csr& c, cudaStream_t s) {
+  if (c.val_h || c.nnz == 0) return MLG_OK;
+  MLG_CUDA(cudaMalloc(&c.val_h, sizeof(__half) * (size_t)c.nnz));
+  to_half_kernel<<<(int)std::max<long long>(1, std::min<long long>(148LL * 16, (c.nnz + 255) / 256)), 256, 0, s>>>(
+      c.val, c.nnz, c.val_h);
+  MLG_LAUNCHED();
+  return MLG_OK;
 }
 
 int csr_sign_copy(const Csr& src, bool by_row, int imDim, const int* N, float global_sign, Csr& dst,
                   cudaStream_t s) {
   dst = src;  // shares row_ptr / col / long_rows with src (not owned)
   dst.val = nullptr;
+  dst.val_h = nullptr;
   MLG_CUDA(cudaMalloc(&dst.val, sizeof(float) * (size_t)std::max<long long>(1, src.nnz)));
   const int Nx = N[0], Ny = imDim > 1 ? N[1] : 1;
   if (by_row) {

@@ -148,6 +148,20 @@ class NufftPlan:
     def adjoint_mode(self, name: str):
         N.call("mlg_plan_set_adjoint", self._h, self.ADJOINT_MODES.index(name))
 
+    PRECISIONS = ("fp32", "mixed")
+
+    @property
+    def precision(self) -> str:
+        m = ctypes.c_int()
+        N.call("mlg_plan_get_precision", self._h, ctypes.byref(m))
+        return self.PRECISIONS[m.value]
+
+    @precision.setter
+    def precision(self, name: str):
+        """'fp32' or 'mixed' (FP16 matrix values, BF16 k-space work vectors
+        in the CG-SENSE solver, FP32 sums, FP64 scalars)."""
+        N.call("mlg_plan_set_precision", self._h, self.PRECISIONS.index(name))
+
     def autotune(self, reps: int = 3) -> dict:
         """Times the valid adjoint strategies and keeps the fastest; returns
         {strategy: ms} (strategies the plan cannot run are omitted)."""

@@ -31,7 +31,7 @@ class SensaRecon:
     KFC_conj, FFT pass tables and work vectors (one per trajectory/coil
     set)."""
 
-    def __init__(self, Gu, Gut, C, n_u, dK_u=None, autotune=False):
+    def __init__(self, Gu, Gut, C, n_u, dK_u=None, autotune=False, precision="fp32"):
         if isinstance(Gu, bmSparseMat):
             Gu = Gu.to_device()
         if isinstance(Gut, bmSparseMat):
@@ -49,6 +49,8 @@ class SensaRecon:
         self.KFC, self.KFC_conj = KFC, KFC_conj  # host copies, [prod(n_u), nCh]
         self.nPt = self.plan.nPt
         self._mats = (Gu, Gut)
+        if precision != "fp32":
+            self.plan.precision = precision
         self.tuning = self.plan.autotune() if autotune else None
 
     def run_dev(self, y, ve, x, nIter=1, nCGD=20, ve_max=None, residual=None):

@@ -543,6 +543,10 @@ class SpMV:
         self._mex = ref_mex("bmSparseMat_cC_oBlock_omp_mex") if kind == "reference" else None
 
     def __call__(self, G: SparseMat, v: np.ndarray) -> np.ndarray:
+        if self.kind == "fp64":  # float64 product of the same float32 matrix
+            S = G.to_scipy().astype(np.float64)
+            v = np.asarray(v, np.complex128)
+            return np.asarray(S @ (v[:, None] if v.ndim == 1 else v), np.complex128)
         v = np.asarray(v, np.complex64)
         if v.ndim == 1:
             v = v[:, None]
@@ -568,43 +572,44 @@ def _spmv(kind=None):
     return _default_spmv
 
 
-def bmShanna(x, G: SparseMat, KFC, n_u=None, spmv=None, workers=None):
-    """bmShanna_MATLAB.m:6-56: y = Gu * FFT(ZF(x .* KFC)), y [nPt, nCh]."""
+def bmShanna(x, G: SparseMat, KFC, n_u=None, spmv=None, workers=None, dtype=np.complex64):
+    """bmShanna_MATLAB.m:6-56: y = Gu * FFT(ZF(x .* KFC)), y [nPt, nCh].
+    dtype complex128 (with spmv 'fp64') gives the FP64 restatement."""
     N_u = np.ravel(G.N_u).astype(int)
     n_u = N_u if n_u is None else np.ravel(n_u).astype(int)
-    x = np.asarray(x, np.complex64)
+    x = np.asarray(x, dtype)
     if x.ndim == 1:
         x = x[:, None]
     KFC = np.asarray(KFC)
     nCh = KFC.shape[1] if x.shape[1] == 1 else x.shape[1]
     if x.shape[1] < nCh:
         x = np.repeat(x, nCh, axis=1)
-    x = (x * KFC).astype(np.complex64)
+    x = (x * KFC).astype(dtype)
     if not np.array_equal(N_u, n_u):
         x = zerofill_col(x, N_u, n_u)
     blk = x.reshape(tuple(N_u) + (nCh,), order="F")
-    blk = _shift_fft(blk, range(len(N_u)), workers=workers).astype(np.complex64)
+    blk = _shift_fft(blk, range(len(N_u)), workers=workers).astype(dtype)
     x = blk.reshape(-1, nCh, order="F")
     return (spmv or _spmv())(G, x)
 
 
-def bmNakatsha(y, Gut: SparseMat, KFC_conj, C_flag=True, n_u=None, spmv=None, workers=None):
+def bmNakatsha(y, Gut: SparseMat, KFC_conj, C_flag=True, n_u=None, spmv=None, workers=None, dtype=np.complex64):
     """bmNakatsha_MATLAB.m:6-58: x = sum_c KFC_conj .* Crop(IFFT(Gut * y))."""
     N_u = np.ravel(Gut.N_u).astype(int)
     n_u = N_u if n_u is None else np.ravel(n_u).astype(int)
-    y = np.asarray(y, np.complex64)
+    y = np.asarray(y, dtype)
     if y.ndim == 1:
         y = y[:, None]
     nCh = y.shape[1]
     x = (spmv or _spmv())(Gut, y)
     blk = x.reshape(tuple(N_u) + (nCh,), order="F")
-    blk = _shift_fft(blk, range(len(N_u)), inverse=True, workers=workers).astype(np.complex64)
+    blk = _shift_fft(blk, range(len(N_u)), inverse=True, workers=workers).astype(dtype)
     x = blk.reshape(-1, nCh, order="F")
     if not np.array_equal(N_u, n_u):
         x = crop_col(x, N_u, n_u)
-    x = (x * KFC_conj).astype(np.complex64)
+    x = (x * KFC_conj).astype(dtype)
     if C_flag:
-        x = x.sum(axis=1, dtype=np.complex64)[:, None]
+        x = x.sum(axis=1, dtype=dtype)[:, None]
     return x
 
 
@@ -752,9 +757,11 @@ def bmSensa(x, y, ve, C, Gu, Gut, n_u, nCGD, ve_max=None, nIter=1, spmv=None, dt
         ve_max = float(np.max(ve))
     HY = np.minimum(ve, np.float32(ve_max)).astype(np.float32)
 
-    M = lambda v: bmShanna(v, Gu, KFC, n_u, spmv, workers).astype(dtype)
-    dagM = lambda r: ((1 / HX) * bmNakatsha((HY * r).astype(np.complex64), Gut, KFC_conj, True, n_u, spmv,
-                                            workers)).astype(dtype)
+    if dtype == np.complex128 and spmv is None:
+        spmv = SpMV("fp64")  # the FP64 restatement: products in double too
+    M = lambda v: bmShanna(v, Gu, KFC, n_u, spmv, workers, dtype).astype(dtype)
+    dagM = lambda r: ((1 / HX) * bmNakatsha((HY * r).astype(dtype), Gut, KFC_conj, True, n_u, spmv,
+                                            workers, dtype)).astype(dtype)
     for _ in range(nIter):
         res_next = y - M(x)
         dagM_res_next = dagM(res_next)
