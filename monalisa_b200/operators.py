@@ -51,15 +51,38 @@ def _crop_col(x, N_u, n_u):
     return blk[crop_index(N_u, n_u)].reshape(-1, nc, order="F")
 
 
+_K_CACHE = {}
+_K_LOCK = __import__("threading").Lock()
+
+
+def _cropped_K(N_u, n_u, dK_u, kernelType, nWin, kernelParam):
+    """One column of bmK cropped to n_u, [prod(n_u), 1] float32.  Every coil
+    column of bmK is the same (bmK.m:148-152), so one is computed; it is
+    cached per grid, image and kernel (read-only, shared)."""
+    kernelType, nWin, kp = kernel_defaults(kernelType, nWin, kernelParam)
+    key = (tuple(np.ravel(N_u).astype(int)), tuple(np.ravel(n_u).astype(int)),
+           tuple(np.ravel(dK_u).astype(np.float32)), kernelType, int(nWin), tuple(kp))
+    with _K_LOCK:
+        K = _K_CACHE.get(key)
+    if K is None:
+        K = _crop_col(bmK(N_u, dK_u, 1, kernelType, nWin, kp), N_u, n_u)
+        K.setflags(write=False)
+        with _K_LOCK:
+            if len(_K_CACHE) > 16:
+                _K_CACHE.clear()
+            _K_CACHE[key] = K
+    return K
+
+
 def bmKF(C, N_u, n_u, dK_u, nCh, kernelType=None, nWin=None, kernelParam=None):
     """K * (1/prod(N_u)/prod(dK_u)) * C cropped to n_u (bmKF.m:6-36)."""
     N_u = np.ravel(N_u).astype(np.float32)
     n_u = np.ravel(n_u).astype(np.float32)
     dK_u = np.ravel(dK_u).astype(np.float32)
-    K = _crop_col(bmK(N_u, dK_u, nCh, kernelType, nWin, kernelParam), N_u, n_u)
+    K = _cropped_K(N_u, n_u, dK_u, kernelType, nWin, kernelParam)
     F = np.float32(1 / np.prod(N_u) / np.prod(dK_u))
     if C is None:
-        return (K * F).astype(np.float32)
+        return np.repeat((K * F).astype(np.float32), int(nCh), axis=1)
     C = np.asarray(C, np.complex64).reshape(K.shape[0], -1, order="F")
     return (K * F * C).astype(np.complex64)
 
@@ -70,10 +93,10 @@ def bmKF_conj(C_conj, N_u, n_u, dK_u, nCh, kernelType=None, nWin=None, kernelPar
     N_u = np.ravel(N_u).astype(np.float32)
     n_u = np.ravel(n_u).astype(np.float32)
     dK_u = np.ravel(dK_u).astype(np.float32)
-    K = _crop_col(bmK(N_u, dK_u, nCh, kernelType, nWin, kernelParam), N_u, n_u)
+    K = _cropped_K(N_u, n_u, dK_u, kernelType, nWin, kernelParam)
     F = np.float32(1 / np.prod(dK_u))
     if C_conj is None:
-        return (K * F).astype(np.float32)
+        return np.repeat((K * F).astype(np.float32), int(nCh), axis=1)
     C_conj = np.asarray(C_conj, np.complex64).reshape(K.shape[0], -1, order="F")
     return (K * F * C_conj).astype(np.complex64)
 

@@ -131,3 +131,45 @@ def koosh3d_bins(n=96, oversampling=2, nFr=20, spokes=(200, 1500), nRead=256, nC
                   samples_per_spoke=nRead, coils=nCh, kernel="gauss nWin=3 sigma=0.61", admm_iterations=nIter,
                   cg_steps=nCGD, delta=0.01, rho=0.1, seed=seed)
     return w
+
+
+# request mix for serving: 60 % 2-D golden-angle radial (256^2 image, 512^2
+# grid, 128-512 spokes x 512 samples), 40 % 3-D koosh ball (96^3 or 128^3
+# image, 1000-4096 spokes x 256 samples), 8-16 coils, CG-SENSE with 20 CG
+# steps, Poisson arrivals.  A fixed set of protocol templates (trajectory,
+# volume elements, coil maps, phantom) stands for the scanner protocols the
+# requests come from; each template is one trajectory key.
+SERVING_TEMPLATES_2D = ((128, 8), (256, 12), (512, 16))               # spokes, coils
+SERVING_TEMPLATES_3D = ((96, 1024, 8), (128, 2048, 12), (128, 4096, 16))  # n, spokes, coils
+
+
+def serving_templates(seed=5, scale=1.0):
+    """The protocol templates of the serving mix; ``scale`` < 1 shrinks the
+    spoke counts (tests)."""
+    out = []
+    for k, (ns, nCh) in enumerate(SERVING_TEMPLATES_2D):
+        ns = max(8, int(ns * scale))
+        n, N = 256, 512
+        t = T.golden_angle_radial2(512, ns, N / 512)
+        ve = T.bmVolumeElement_voronoi_full_radial2(T.bmTraj_fullRadial2_lineAssym2(512, ns, N / 512), 512)
+        out.append(dict(key=("2d", k), imDim=2, t=t, ve=ve, N_u=np.array([N, N]), n_u=np.array([n, n]),
+                        C=T.coil_maps([n, n], nCh, seed + k), x_true=T.ellipsoid_phantom([n, n], 6, seed + 10 + k)))
+    for k, (n, ns, nCh) in enumerate(SERVING_TEMPLATES_3D):
+        ns = max(16, int(ns * scale))
+        N = 2 * n
+        t = T.bmTraj_fullRadial3_phyllotaxis_lineAssym2(256, ns, 1, N / 256)
+        out.append(dict(key=("3d", k), imDim=3, t=t, ve=T.bmVolumeElement_full_radial3(t), N_u=np.array([N] * 3),
+                        n_u=np.array([n] * 3), C=T.coil_maps([n] * 3, nCh, seed + 20 + k),
+                        x_true=T.ellipsoid_phantom([n] * 3, 8, seed + 30 + k)))
+    return out
+
+
+def serving_schedule(n_requests, rate, seed=5):
+    """Poisson arrival offsets (seconds) and template indices: 60 % drawn from
+    the 2-D templates, 40 % from the 3-D ones."""
+    rng = np.random.default_rng(seed)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, n_requests))
+    is3d = rng.random(n_requests) < 0.4
+    n2, n3 = len(SERVING_TEMPLATES_2D), len(SERVING_TEMPLATES_3D)
+    tmpl = np.where(is3d, n2 + rng.integers(0, n3, n_requests), rng.integers(0, n2, n_requests))
+    return arrivals, tmpl
