@@ -350,6 +350,19 @@ def run_gpu(args):
                  "arm": "torch.fft (cuFFT) + torch.sparse CSR (cuSPARSE), FP32 CG scalars, same inputs"}
         del pg, xp
 
+    # the other configurations of the benchmark, each timed with CUDA events
+    extra = {}
+    adjoint_c2 = rec.plan.adjoint_mode
+    if not args.no_extra:
+        x_fp32 = x.clone()
+        extra["c4_mixed_precision"] = {
+            p: _mixed(w, Gu, Gut, y, ve, x_fp32, ms / args.steps, plain, stream, p) for p in ("mixed", "fp16_values")}
+        rec.plan.close()
+        extra["c1_radial2d"] = _c1(stream)
+        extra["c3_frame_bins"] = _c3(stream)
+        if rank == 0:
+            extra["c5_serving"] = _c5()
+
     out = {
         "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True,
@@ -360,13 +373,144 @@ def run_gpu(args):
                    "l2": "working set (2.1 GB grid) larger than L2 each step", **w.info},
         "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
         "recon_rel_err_vs_phantom": round(err, 5), "setup_s": round(setup_s, 2),
-        "autotune": {"adjoint": rec.plan.adjoint_mode, "ms": {k: round(v, 4) for k, v in rec.tuning.items()}},
+        "autotune": {"adjoint": adjoint_c2, "ms": {k: round(v, 4) for k, v in rec.tuning.items()}},
         "vs_plain_gpu": plain,
+        **extra,
     }
     if rank == 0:
         print(json.dumps(out), flush=True)
     rec.plan.close()
     replicas.shutdown()
+
+
+def _event_ms(fn, reps, stream):
+    import torch
+
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(reps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def _mixed(w, Gu, Gut, y, ve, x_fp32, ms_fp32, plain, stream, precision="mixed"):
+    """c4: the c2 reconstruction in reduced precision: 'mixed' (FP16 matrix
+    values, BF16 k-space work vectors, FP32 sums, FP64 scalars) or
+    'fp16_values' (FP16 matrix values only)."""
+    import torch
+
+    import monalisa_b200 as mb
+
+    rec = mb.SensaRecon(Gu, Gut, w.C, w.n_u, precision=precision, autotune=True)
+    x = torch.zeros_like(x_fp32)
+
+    def step():
+        x.zero_()
+        rec.run_dev(y, ve, x, nIter=1, nCGD=w.nCGD)
+
+    for _ in range(2):
+        step()
+    ms = _event_ms(step, 3, stream)
+    out = {"workload": f"c2 inputs (3D koosh 128^3/256^3, 16 coils, 30 CG), precision {precision}",
+           "recons_per_s": round(1000.0 / ms, 4), "ms_per_recon": round(ms, 2),
+           "speedup_vs_fp32": round(ms_fp32 / ms, 3),
+           "speedup_vs_plain_gpu": round(plain["ms_per_recon"] / ms, 2) if plain else None,
+           "rel_diff_vs_fp32_recon": float((x - x_fp32).norm() / x_fp32.norm()),
+           "adjoint": rec.plan.adjoint_mode,
+           "precision": {"mixed": "fp16 matrix values, bf16 k-space vectors, fp32 sums/FFT, fp64 CG scalars",
+                         "fp16_values": "fp16 matrix values, fp32 k-space/sums/FFT, fp64 CG scalars"}[precision]}
+    rec.plan.close()
+    return out
+
+
+def _c1(stream):
+    """c1: 2-D golden-angle radial CG-SENSE, 256^2 / 512^2, 1 coil, KB, 20 CG."""
+    import torch
+
+    import monalisa_b200 as mb
+    from monalisa_b200.workloads import radial2d
+
+    w = radial2d()
+    Gu, Gut = mb.bmTraj2SparseMat(w.t, w.ve, w.N_u, w.dK_u, w.kernelType, w.nWin, w.kernelParam)
+    rec = mb.SensaRecon(Gu, Gut, w.C, w.n_u, autotune=True)
+    y = torch.from_numpy(w.y).cuda()
+    ve = torch.from_numpy(np.ascontiguousarray(w.ve, np.float32)).cuda()
+    x = torch.zeros(int(np.prod(w.n_u)), dtype=torch.complex64, device="cuda")
+
+    def step():
+        x.zero_()
+        rec.run_dev(y, ve, x, nIter=1, nCGD=w.nCGD)
+
+    for _ in range(3):
+        step()
+    ms = _event_ms(step, 10, stream)
+    adjoint = rec.plan.adjoint_mode
+    rec.plan.close()
+    return {"workload": "2D golden-angle radial 256^2 image, 512^2 grid, 256x512 samples, 1 coil, KB nWin 3, "
+                        "20 CG iterations from x = 0 (working set inside L2)",
+            "recons_per_s": round(1000.0 / ms, 3), "ms_per_recon": round(ms, 3), "adjoint": adjoint}
+
+
+def _c3(stream):
+    """c3: temporal-TV ADMM over 20 koosh frame bins (96^3 / 192^3, 12 coils,
+    30 ADMM x 5 CG)."""
+    import torch
+
+    import monalisa_b200 as mb
+    from monalisa_b200.workloads import koosh3d_bins
+
+    w = koosh3d_bins()
+    mats = [mb.bmTraj2SparseMat(t, v, w.N_u, w.dK_u, w.kernelType, w.nWin, w.kernelParam) for t, v in zip(w.t, w.ve)]
+    chain = mb.TevaMorphosiaChain([m[0] for m in mats], [m[1] for m in mats], w.C, w.n_u, autotune=True)
+    gen = torch.Generator(device="cuda").manual_seed(33)
+    ys = []
+    for f in range(w.nFr):
+        yy = chain.plans[f].shanna(torch.from_numpy(w.x_true[f]).cuda())
+        yy += torch.randn(yy.shape, dtype=torch.complex64, device="cuda", generator=gen) * (yy.abs().mean() * 1e-3)
+        ys.append(yy)
+    y = torch.cat(ys)
+    ve = torch.from_numpy(np.concatenate(w.ve).astype(np.float32)).cuda()
+    nu = int(np.prod(w.n_u))
+    x, z, u = [torch.zeros((w.nFr, nu), dtype=torch.complex64, device="cuda") for _ in range(3)]
+    chain.run_dev(y, ve, x, z, u, w.delta, w.rho, 1, w.nCGD, 10.0)  # warm-up (captures the CG step)
+    hist = []
+
+    def recon():
+        x.zero_()
+        hist.clear()
+        chain.run_dev(y, ve, x, z, u, w.delta, w.rho, w.nIter, w.nCGD, 10.0, history=hist)
+
+    ms = _event_ms(recon, 1, stream)
+    chain.close()
+    ops = w.nFr * (w.nIter * (w.nCGD + 1) + 1), w.nFr * w.nIter * w.nCGD
+    return {"workload": "20 koosh frame bins (200-1500 spokes x 256), 96^3 image, 192^3 grid, 12 coils, "
+                        "temporal-TV ADMM 30 x 5 CG",
+            "recons_per_s": round(1000.0 / ms, 4), "s_per_recon": round(ms / 1000.0, 3),
+            "ms_per_admm_iteration": round(ms / w.nIter, 2), "shanna_nakatsha_per_recon": list(ops),
+            "objective_first_last": [hist[0][0], hist[-1][0]], "samples": int(sum(w.nPt))}
+
+
+def _c5():
+    """c5: the serving mix (60 % 2-D, 40 % 3-D, 8-16 coils, 20 CG), Poisson
+    arrivals at 50 requests/s, continuous admission on one GPU."""
+    from monalisa_b200 import serving
+    from monalisa_b200.workloads import serving_schedule, serving_templates
+
+    templates = serving_templates()
+    for k, tp in enumerate(templates):
+        tp["y"] = serving.simulate_data(tp, seed=k)
+    server = serving.ReconServer(workers=4)
+    serving.run_poisson(server, templates, np.zeros(len(templates)), np.arange(len(templates)))
+    arrivals, tmpl = serving_schedule(150, 50.0)
+    reqs = serving.run_poisson(server, templates, arrivals, tmpl)
+    server.close()
+    return {"workload": "Poisson 50 req/s, 150 requests: 60% 2D 256^2/512^2 (128-512 spokes x 512), 40% 3D "
+                        "96^3-128^3 (1024-4096 spokes x 256), 8-16 coils, CG-SENSE 20",
+            "offered_rate": 50.0, **{k: (round(v, 2) if isinstance(v, float) else v)
+                                     for k, v in serving.latency_stats(reqs).items()}}
 
 
 def _oracle():
@@ -450,6 +594,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-GPU comparison arm")
+    ap.add_argument("--no-extra", action="store_true", help="skip the c1 / c3 / c4 / c5 configurations")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -325,6 +325,8 @@ int mlg_plan_autotune(mlg_plan_t p, int reps, double* ms);
  * but keep their complex64 k-space buffers.  No reference counterpart. */
 #define MLG_PRECISION_FP32 0
 #define MLG_PRECISION_MIXED 1
+/* FP16 matrix values only; the k-space work vectors stay FP32. */
+#define MLG_PRECISION_FP16_VALUES 2
 int mlg_plan_set_precision(mlg_plan_t p, int precision);
 int mlg_plan_get_precision(mlg_plan_t p, int* precision);
 

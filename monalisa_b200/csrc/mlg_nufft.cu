@@ -109,8 +109,9 @@ static bool fused_gut(const mlg_plan_s* p) { return p->adjoint_mode == kAdjFused
 // adjoint variants a plan can run
 bool adjoint_mode_valid(const mlg_plan_s* p, int mode) {
   if (mode == kAdjFullGrid) return true;
-  // the fused gather reads FP32 k-space inside the FFT pass: not in mixed precision
-  if (mode == kAdjFused) return p->imDim >= 2 && p->precision == 0;
+  // the fused gather reads FP32 k-space and FP32 values inside the FFT pass:
+  // FP32 plans only
+  if (mode == kAdjFused) return p->imDim >= 2 && p->precision == MLG_PRECISION_FP32;
   if (mode == kAdjMasked) return (p->nCh % 2) == 0 && p->Gut_s.nz_mask != nullptr;
   return false;
 }
@@ -203,7 +204,7 @@ int shanna_stage(mlg_plan_s* p, int stage, const float2* x, bool x_per_coil, flo
   a.in.a = p->grid;
   a.in.rows = p->Nu_tot;
   a.out.layout = p->mixed_run ? Layout::kPointBF16 : Layout::kPointC64;  // k-space storage
-  a.half_values = p->precision == MLG_PRECISION_MIXED;
+  a.half_values = p->precision != MLG_PRECISION_FP32;
   a.out.a = y;
   a.out.rows = p->nPt;
   a.sqn_row_weight = sqn_w;
@@ -226,7 +227,7 @@ int nakatsha_stage(mlg_plan_s* p, int stage, const float2* y, const float* HY, f
     a.m = &p->Gut_s;
     a.nCh = p->nCh;
     a.in.layout = p->mixed_run ? Layout::kPointBF16 : Layout::kPointC64;  // k-space storage
-    a.half_values = p->precision == MLG_PRECISION_MIXED;
+    a.half_values = p->precision != MLG_PRECISION_FP32;
     a.in.a = const_cast<float2*>(y);
     a.in.rows = p->nPt;
     a.in_row_scale = HY;

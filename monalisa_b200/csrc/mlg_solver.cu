@@ -515,10 +515,11 @@ extern "C" int mlg_plan_autotune(mlg_plan_t p, int reps, double* ms) {
 extern "C" int mlg_plan_set_precision(mlg_plan_t p, int precision) {
   using namespace mlg;
   MLG_CHECK(p, "NULL plan");
-  MLG_CHECK(precision == MLG_PRECISION_FP32 || precision == MLG_PRECISION_MIXED, "unknown precision %d",
-            precision);
+  MLG_CHECK(precision == MLG_PRECISION_FP32 || precision == MLG_PRECISION_MIXED ||
+                precision == MLG_PRECISION_FP16_VALUES,
+            "unknown precision %d", precision);
   MLG_CUDA(cudaSetDevice(p->device));
-  if (precision == MLG_PRECISION_MIXED) {
+  if (precision != MLG_PRECISION_FP32) {
     MLG_CHECK(p->Gu && p->Gut, "mixed precision needs a plan with both Gu and Gut");
     MLG_TRY(csr_make_half(p->Gu_s, p->stream));
     MLG_TRY(csr_make_half(p->Gut_s, p->stream));

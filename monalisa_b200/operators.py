@@ -171,7 +171,7 @@ class NufftPlan:
     def adjoint_mode(self, name: str):
         N.call("mlg_plan_set_adjoint", self._h, self.ADJOINT_MODES.index(name))
 
-    PRECISIONS = ("fp32", "mixed")
+    PRECISIONS = ("fp32", "mixed", "fp16_values")
 
     @property
     def precision(self) -> str:
@@ -181,8 +181,9 @@ class NufftPlan:
 
     @precision.setter
     def precision(self, name: str):
-        """'fp32' or 'mixed' (FP16 matrix values, BF16 k-space work vectors
-        in the CG-SENSE solver, FP32 sums, FP64 scalars)."""
+        """'fp32', 'mixed' (FP16 matrix values, BF16 k-space work vectors in
+        the CG-SENSE solver, FP32 sums, FP64 scalars) or 'fp16_values' (FP16
+        matrix values only)."""
         N.call("mlg_plan_set_precision", self._h, self.PRECISIONS.index(name))
 
     def autotune(self, reps: int = 3) -> dict:

@@ -55,10 +55,13 @@ def test_mixed_cg_sense_within_1e3_of_fp64(case):
     r32, x32 = _recon(case, "fp32")
     rm, xm = _recon(case, "mixed")
     assert rm.plan.precision == "mixed" and rm.plan.adjoint_mode != "fused"
-    e32, em = rel(x32, x64), rel(xm, x64)
+    rh, xh = _recon(case, "fp16_values")
+    assert rh.plan.precision == "fp16_values"
+    e32, em, eh = rel(x32, x64), rel(xm, x64), rel(xh, x64)
     assert e32 <= 1e-4, e32
     assert em <= 1e-3, em
-    assert em > e32  # the mixed path really runs in lower precision
+    assert eh <= 1e-3, eh
+    assert em > e32 and eh > e32  # the reduced-precision paths really run in lower precision
 
 
 def test_mixed_forward_model_vs_nudft(case):
