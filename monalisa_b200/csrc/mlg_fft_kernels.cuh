@@ -583,6 +583,109 @@ __global__ void __launch_bounds__(MAXT) fft_pass_kernel(PassDesc d, int L, int r
   }
 }
 
+// ---- pipelined plain passes ------------------------------------------------------
+// A persistent CTA walks the line bundles b = blockIdx.x, + gridDim.x, ...
+// with two shared buffers: while it transforms and stores bundle b from one,
+// the next bundle's lines arrive in the other through 16-byte asynchronous
+// copies (cp.async); cells outside the stored input range or unset in the
+// occupancy mask are written as zeros directly.  Loads thus overlap the
+// transform and the stores inside every CTA instead of only across CTAs.
+// Coil pairs per thread (even C), fixed column per thread (blockDim a
+// multiple of the columns), templated transform sizes only.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int PENDING>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(PENDING) : "memory");
+}
+
+template <int N1, int N2, int DIR, int MAXT>
+__global__ void __launch_bounds__(MAXT, MAXT > 256 ? 1 : (N1 * N2 <= 256 ? 3 : 2))
+    fft_pass_pipe_kernel(PassDesc d, int L, int nbundles,
+                                                             const float2* __restrict__ tw) {
+  extern __shared__ float4 s4all[];
+  constexpr int N = N1 * N2;
+  const int C = d.C, cols = L * C, cv = cols >> 1;
+  float4* const buf0 = s4all;
+  float4* const buf1 = s4all + (size_t)N * cv;
+  const int vc = threadIdx.x % cv, rstep = blockDim.x / cv, r0 = threadIdx.x / cv;
+  const int col = vc * 2, l = col / C, c = col - l * C;
+  const int u = d.ax == 0 ? 1 : 0, v = d.ax == 2 ? 1 : 2;
+  const int gu = (d.dims[u] + L - 1) / L;
+  const long long ist = d.in_stride[d.ax], ost = d.out_stride[d.ax], cst = d.cell_stride[d.ax];
+  const uint32_t* mask = d.in_mask;
+
+  auto issue = [&](int b, float4* dst) {
+    const int ui = (b % gu) * L + l, vi = b / gu;
+    const bool line_ok = ui < d.dims[u];
+    const float2* base = d.in + (long long)ui * d.in_stride[u] + (long long)vi * d.in_stride[v] + c;
+    const long long cell0 = (long long)ui * d.cell_stride[u] + (long long)vi * d.cell_stride[v];
+    // rows in batches of 8: the batch's mask words are loaded together before
+    // any copy depends on them
+    constexpr int kB = 8;
+    for (int n0 = r0; n0 < N; n0 += kB * rstep) {
+      bool ld[kB];
+#pragma unroll
+      for (int j = 0; j < kB; ++j) {
+        const int n = n0 + j * rstep;
+        ld[j] = line_ok && n < N && n >= d.in_lo && n < d.in_lo + d.in_len;
+      }
+      if (mask) {
+        uint32_t w[kB];
+#pragma unroll
+        for (int j = 0; j < kB; ++j) {
+          const long long cell = cell0 + (long long)(n0 + j * rstep) * cst;
+          w[j] = ld[j] ? __ldg(mask + (cell >> 5)) >> (cell & 31) : 0u;
+        }
+#pragma unroll
+        for (int j = 0; j < kB; ++j) ld[j] = ld[j] && (w[j] & 1u);
+      }
+#pragma unroll
+      for (int j = 0; j < kB; ++j) {
+        const int n = n0 + j * rstep;
+        if (n < N) {
+          float4* dp = dst + n * cv + vc;
+          if (ld[j])
+            cp_async16(dp, base + (long long)(n - d.in_lo) * ist);
+          else
+            *dp = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+      }
+    }
+    cp_async_commit();
+  };
+
+  int b = blockIdx.x;
+  if (b >= nbundles) return;
+  issue(b, buf0);
+  for (int it = 0; b < nbundles; ++it, b += gridDim.x) {
+    float4* cur = (it & 1) ? buf1 : buf0;
+    const int nb = b + gridDim.x;
+    if (nb < nbundles) {
+      issue(nb, (it & 1) ? buf0 : buf1);
+      cp_async_wait<1>();  // all but the copies just issued have landed
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    smem_fft<N1, N2, DIR>(reinterpret_cast<float2*>(cur), cols, N1, N2, tw);  // ends with a barrier
+    const int ui = (b % gu) * L + l, vi = b / gu;
+    if (ui < d.dims[u]) {
+      float2* obase = d.out + (long long)ui * d.out_stride[u] + (long long)vi * d.out_stride[v] + c;
+#pragma unroll 4
+      for (int kk = r0; kk < d.out_len; kk += rstep) {
+        const int k = d.out_lo + kk;
+        const int pos = (k % N1) * N2 + k / N1;
+        *reinterpret_cast<float4*>(obase + (long long)kk * ost) = cur[pos * cv + vc];
+      }
+    }
+    __syncthreads();  // cur is refilled by the copies issued in the next iteration
+  }
+}
+
 // ---- launch helpers ------------------------------------------------------------
 // Lines per CTA: 32 columns (256-byte row segments) for streaming passes; the
 // gathering pass uses 16 columns so that twice as many CTAs (and gathers)
@@ -631,8 +734,51 @@ static int launch_bounded(const FftAxisPlan& a, const PassDesc& d, int L, int th
   return MLG_OK;
 }
 
+// Pipelined plain pass: ~16 columns per bundle (the two buffers take the
+// shared memory of one 32-column buffer), a persistent grid of (resident
+// CTAs per SM) x SMs.
+template <int N1, int N2, int DIR, int MAXT>
+static int launch_pipe(const FftAxisPlan& a, const PassDesc& d, int Lp, int threads, cudaStream_t s) {
+  const size_t smem = 2 * (size_t)a.N * Lp * d.C * sizeof(float2);
+  // per instantiation and host thread (serving workers launch concurrently);
+  // recomputed when the coil count changes the CTA's shared memory or threads
+  thread_local int per_sm = 0, sms = 0, per_sm_threads = 0;
+  thread_local size_t per_sm_smem = 0;
+  if (per_sm == 0 || per_sm_smem != smem || per_sm_threads != threads) {
+    MLG_CUDA(cudaFuncSetAttribute(fft_pass_pipe_kernel<N1, N2, DIR, MAXT>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(200 * 1024)));
+    int dev = 0;
+    MLG_CUDA(cudaGetDevice(&dev));
+    MLG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    MLG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fft_pass_pipe_kernel<N1, N2, DIR, MAXT>,
+                                                           threads, smem));
+    per_sm = std::max(1, per_sm);
+    per_sm_smem = smem;
+    per_sm_threads = threads;
+  }
+  const int nb = blocks_for(d, Lp);
+  const int grid = std::max(1, std::min(nb, per_sm * sms));
+  fft_pass_pipe_kernel<N1, N2, DIR, MAXT><<<grid, threads, smem, s>>>(d, Lp, nb, a.tw);
+  MLG_LAUNCHED();
+  return MLG_OK;
+}
+
+static inline int pipe_lines(const FftAxisPlan& a, int C) {
+  int L = std::max(1, (16 + C - 1) / C);
+  while (L > 1 && 2 * (size_t)a.N * L * C * sizeof(float2) > kFftSmemCap) --L;
+  return L;
+}
+
 template <int N1, int N2, int DIR, PassMode MODE>
 static int launch_pass(const FftAxisPlan& a, const PassDesc& d, int L, cudaStream_t s) {
+  if constexpr (MODE == PassMode::kPlain && N1 > 0) {
+    const int Lp = pipe_lines(a, d.C);
+    const int cols = Lp * d.C, tp = threads_for(cols);
+    if ((d.C & 1) == 0 && tp % cols == 0 && 2 * (size_t)a.N * cols * sizeof(float2) <= kFftSmemCap) {
+      if (tp <= kFftThreads) return launch_pipe<N1, N2, DIR, kFftThreads>(a, d, Lp, tp, s);
+      return launch_pipe<N1, N2, DIR, kFftMaxThreads>(a, d, Lp, tp, s);
+    }
+  }
   const int threads = threads_for(L * d.C);
   if (threads <= kFftThreads) return launch_bounded<N1, N2, DIR, MODE, kFftThreads>(a, d, L, threads, s);
   return launch_bounded<N1, N2, DIR, MODE, kFftMaxThreads>(a, d, L, threads, s);
