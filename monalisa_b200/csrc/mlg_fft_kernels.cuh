@@ -28,6 +28,25 @@ namespace mlg {
 constexpr int kFftThreads = 256;     // target threads per CTA
 constexpr int kFftMaxThreads = 512;  // launch bound (columns that need lcm(cols, 32) > 256)
 constexpr size_t kFftSmemCap = 100 * 1024;
+
+// Threads per CTA: a multiple of the CTA's columns (and of the warp) so that
+// every thread keeps one column (or coil pair) through the load, the
+// transform and the store; the multiple nearest kFftThreads.  Columns whose
+// lcm with 32 exceeds kFftMaxThreads take kFftThreads and the per-element
+// paths.
+constexpr int cta_threads(int cols) {
+  int g = cols, b = 32;
+  while (b) {
+    const int t = g % b;
+    g = b;
+    b = t;
+  }
+  const int l = cols / g * 32;  // lcm(cols, 32)
+  if (l > kFftMaxThreads) return kFftThreads;
+  const int k = (kFftThreads + l / 2) / l > 1 ? (kFftThreads + l / 2) / l : 1;
+  return kFftMaxThreads / l * l < k * l ? kFftMaxThreads / l * l : k * l;
+}
+static_assert(cta_threads(16) == 256 && cta_threads(32) == 256 && cta_threads(24) == 288, "CTA sizes");
 constexpr int kGatherBatch = 8;  // cells gathered concurrently per thread (kGutIn)
 
 __device__ __forceinline__ float2 cmulf(float2 a, float2 b) {
@@ -602,42 +621,104 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(PENDING) : "memory");
 }
 
-template <int N1, int N2, int DIR, int MAXT>
-__global__ void __launch_bounds__(MAXT, MAXT > 256 ? 1 : (N1 * N2 <= 256 ? 3 : 2))
-    fft_pass_pipe_kernel(PassDesc d, int L, int nbundles,
-                                                             const float2* __restrict__ tw) {
+// The transform of smem_fft for a compile-time column count COLS and CTA
+// size NT (a multiple of COLS): every shared-memory offset is an immediate.
+template <int N1, int N2, int DIR, int COLS, int NT>
+__device__ __forceinline__ void smem_fft_fixed(float2* s, const float2* __restrict__ tw) {
+  static_assert(NT % COLS == 0, "CTA size must be a multiple of the columns");
+  constexpr int G = NT / COLS;  // row groups
+  const int col = threadIdx.x % COLS, g = threadIdx.x / COLS;
+  float2* const sc = s + col;
+#pragma unroll
+  for (int n2b = 0; n2b < N2; n2b += G) {
+    const int n2 = n2b + g;
+    if (N2 % G == 0 || n2 < N2) {
+      float2* const p = sc + n2 * COLS;
+      float2 r[N1];
+#pragma unroll
+      for (int n1 = 0; n1 < N1; ++n1) r[n1] = p[n1 * N2 * COLS];
+      reg_fft<N1, DIR>(r);
+      if (n2) {
+#pragma unroll
+        for (int k1 = 1; k1 < N1; ++k1) r[k1] = cmulf(r[k1], twid<DIR>(tw, n2 * k1));
+      }
+#pragma unroll
+      for (int k1 = 0; k1 < N1; ++k1) p[k1 * N2 * COLS] = r[k1];
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k1b = 0; k1b < N1; k1b += G) {
+    const int k1 = k1b + g;
+    if (N1 % G == 0 || k1 < N1) {
+      float2* const p = sc + k1 * N2 * COLS;
+      float2 r[N2];
+#pragma unroll
+      for (int n2 = 0; n2 < N2; ++n2) r[n2] = p[n2 * COLS];
+      reg_fft<N2, DIR>(r);
+#pragma unroll
+      for (int k2 = 0; k2 < N2; ++k2) p[k2 * COLS] = r[k2];
+    }
+  }
+  __syncthreads();
+}
+
+// Resident CTAs per SM the pipelined pass asks the register allocator for:
+// what its shared memory allows (two N x cols buffers), at most 3.
+constexpr int pipe_min_blocks(int N, int cols, int maxt) {
+  if (cols == 0) return maxt > 256 ? 1 : (N <= 256 ? 3 : 2);
+  const int by_smem = (227 * 1024) / (2 * N * cols * 8 + 1024);
+  return by_smem < 1 ? 1 : (by_smem > 3 ? 3 : by_smem);
+}
+
+// COLS > 0: the CTA covers exactly COLS columns with cta_threads(COLS)
+// threads, both compile-time; COLS == 0: L * C columns, blockDim threads.
+template <int N1, int N2, int DIR, int MAXT, int COLS>
+__global__ void __launch_bounds__(COLS > 0 ? cta_threads(COLS) : MAXT,
+                                  pipe_min_blocks(N1 * N2, COLS, COLS > 0 ? cta_threads(COLS) : MAXT))
+    fft_pass_pipe_kernel(PassDesc d, int L, int nbundles, const float2* __restrict__ tw) {
   extern __shared__ float4 s4all[];
   constexpr int N = N1 * N2;
-  const int C = d.C, cols = L * C, cv = cols >> 1;
+  constexpr int NT = COLS > 0 ? cta_threads(COLS) : 0;
+  constexpr int kRstep = COLS > 0 ? NT / (COLS / 2) : 0;
+  constexpr bool kExact = COLS > 0 && N % kRstep == 0;  // every thread has the same rows
+  const int C = d.C;
+  const int cols = COLS > 0 ? COLS : L * C, cv = cols >> 1;
+  const int nthr = COLS > 0 ? NT : (int)blockDim.x;
   float4* const buf0 = s4all;
   float4* const buf1 = s4all + (size_t)N * cv;
-  const int vc = threadIdx.x % cv, rstep = blockDim.x / cv, r0 = threadIdx.x / cv;
+  const int vc = threadIdx.x % cv, rstep = nthr / cv, r0 = threadIdx.x / cv;
   const int col = vc * 2, l = col / C, c = col - l * C;
   const int u = d.ax == 0 ? 1 : 0, v = d.ax == 2 ? 1 : 2;
   const int gu = (d.dims[u] + L - 1) / L;
   const long long ist = d.in_stride[d.ax], ost = d.out_stride[d.ax], cst = d.cell_stride[d.ax];
   const uint32_t* mask = d.in_mask;
+  const int in_lo = d.in_lo, in_hi = d.in_lo + d.in_len;
 
   auto issue = [&](int b, float4* dst) {
     const int ui = (b % gu) * L + l, vi = b / gu;
     const bool line_ok = ui < d.dims[u];
-    const float2* base = d.in + (long long)ui * d.in_stride[u] + (long long)vi * d.in_stride[v] + c;
-    const long long cell0 = (long long)ui * d.cell_stride[u] + (long long)vi * d.cell_stride[v];
+    const float2* src = d.in + (long long)ui * d.in_stride[u] + (long long)vi * d.in_stride[v] + c +
+                        (long long)(r0 - in_lo) * ist;
+    const long long cell0 = (long long)ui * d.cell_stride[u] + (long long)vi * d.cell_stride[v] + (long long)r0 * cst;
+    float4* const drow = dst + r0 * cv + vc;
     // rows in batches of 8: the batch's mask words are loaded together before
     // any copy depends on them
     constexpr int kB = 8;
-    for (int n0 = r0; n0 < N; n0 += kB * rstep) {
+#pragma unroll
+    for (int nb0 = 0; nb0 < N; nb0 += kB * rstep) {
       bool ld[kB];
 #pragma unroll
       for (int j = 0; j < kB; ++j) {
-        const int n = n0 + j * rstep;
-        ld[j] = line_ok && n < N && n >= d.in_lo && n < d.in_lo + d.in_len;
+        const int n = nb0 + j * rstep + r0;
+        const bool row = kExact ? nb0 + j * rstep < N : n < N;
+        ld[j] = line_ok && row && n >= in_lo && n < in_hi;
       }
       if (mask) {
         uint32_t w[kB];
 #pragma unroll
         for (int j = 0; j < kB; ++j) {
-          const long long cell = cell0 + (long long)(n0 + j * rstep) * cst;
+          const long long cell = cell0 + (long long)(nb0 + j * rstep) * cst;
           w[j] = ld[j] ? __ldg(mask + (cell >> 5)) >> (cell & 31) : 0u;
         }
 #pragma unroll
@@ -645,11 +726,12 @@ __global__ void __launch_bounds__(MAXT, MAXT > 256 ? 1 : (N1 * N2 <= 256 ? 3 : 2
       }
 #pragma unroll
       for (int j = 0; j < kB; ++j) {
-        const int n = n0 + j * rstep;
-        if (n < N) {
-          float4* dp = dst + n * cv + vc;
+        const int nrel = nb0 + j * rstep;
+        const bool row = kExact ? nrel < N : nrel + r0 < N;
+        if (row) {
+          float4* dp = drow + nrel * cv;
           if (ld[j])
-            cp_async16(dp, base + (long long)(n - d.in_lo) * ist);
+            cp_async16(dp, src + (long long)nrel * ist);
           else
             *dp = make_float4(0.f, 0.f, 0.f, 0.f);
         }
@@ -671,15 +753,19 @@ __global__ void __launch_bounds__(MAXT, MAXT > 256 ? 1 : (N1 * N2 <= 256 ? 3 : 2
       cp_async_wait<0>();
     }
     __syncthreads();
-    smem_fft<N1, N2, DIR>(reinterpret_cast<float2*>(cur), cols, N1, N2, tw);  // ends with a barrier
+    if constexpr (COLS > 0)
+      smem_fft_fixed<N1, N2, DIR, COLS, NT>(reinterpret_cast<float2*>(cur), tw);  // ends with a barrier
+    else
+      smem_fft<N1, N2, DIR>(reinterpret_cast<float2*>(cur), cols, N1, N2, tw);
     const int ui = (b % gu) * L + l, vi = b / gu;
     if (ui < d.dims[u]) {
       float2* obase = d.out + (long long)ui * d.out_stride[u] + (long long)vi * d.out_stride[v] + c;
+      const float4* const scol = cur + vc;
 #pragma unroll 4
       for (int kk = r0; kk < d.out_len; kk += rstep) {
         const int k = d.out_lo + kk;
         const int pos = (k % N1) * N2 + k / N1;
-        *reinterpret_cast<float4*>(obase + (long long)kk * ost) = cur[pos * cv + vc];
+        *reinterpret_cast<float4*>(obase + (long long)kk * ost) = scol[pos * cv];
       }
     }
     __syncthreads();  // cur is refilled by the copies issued in the next iteration
@@ -702,23 +788,7 @@ static inline int blocks_for(const PassDesc& d, int L) {
   return ((d.dims[u] + L - 1) / L) * d.dims[v];
 }
 
-// Threads per CTA: a multiple of the CTA's columns (and of the warp) so that
-// every thread keeps one column (or coil pair) through the load, the
-// transform and the store; the multiple nearest kFftThreads.  Columns whose
-// lcm with 32 exceeds kFftMaxThreads take kFftThreads and the per-element
-// paths.
-static inline int threads_for(int cols) {
-  int g = cols, b = 32;
-  while (b) {
-    const int t = g % b;
-    g = b;
-    b = t;
-  }
-  const int l = cols / g * 32;  // lcm(cols, 32)
-  if (l > kFftMaxThreads) return kFftThreads;
-  const int k = std::max(1, (kFftThreads + l / 2) / l);
-  return std::min(kFftMaxThreads / l * l, k * l);
-}
+static inline int threads_for(int cols) { return cta_threads(cols); }
 
 template <int N1, int N2, int DIR, PassMode MODE, int MAXT>
 static int launch_bounded(const FftAxisPlan& a, const PassDesc& d, int L, int threads, cudaStream_t s) {
@@ -737,7 +807,7 @@ static int launch_bounded(const FftAxisPlan& a, const PassDesc& d, int L, int th
 // Pipelined plain pass: ~16 columns per bundle (the two buffers take the
 // shared memory of one 32-column buffer), a persistent grid of (resident
 // CTAs per SM) x SMs.
-template <int N1, int N2, int DIR, int MAXT>
+template <int N1, int N2, int DIR, int MAXT, int COLS>
 static int launch_pipe(const FftAxisPlan& a, const PassDesc& d, int Lp, int threads, cudaStream_t s) {
   const size_t smem = 2 * (size_t)a.N * Lp * d.C * sizeof(float2);
   // per instantiation and host thread (serving workers launch concurrently);
@@ -745,12 +815,12 @@ static int launch_pipe(const FftAxisPlan& a, const PassDesc& d, int Lp, int thre
   thread_local int per_sm = 0, sms = 0, per_sm_threads = 0;
   thread_local size_t per_sm_smem = 0;
   if (per_sm == 0 || per_sm_smem != smem || per_sm_threads != threads) {
-    MLG_CUDA(cudaFuncSetAttribute(fft_pass_pipe_kernel<N1, N2, DIR, MAXT>,
+    MLG_CUDA(cudaFuncSetAttribute(fft_pass_pipe_kernel<N1, N2, DIR, MAXT, COLS>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(200 * 1024)));
     int dev = 0;
     MLG_CUDA(cudaGetDevice(&dev));
     MLG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    MLG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fft_pass_pipe_kernel<N1, N2, DIR, MAXT>,
+    MLG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fft_pass_pipe_kernel<N1, N2, DIR, MAXT, COLS>,
                                                            threads, smem));
     per_sm = std::max(1, per_sm);
     per_sm_smem = smem;
@@ -758,7 +828,7 @@ static int launch_pipe(const FftAxisPlan& a, const PassDesc& d, int Lp, int thre
   }
   const int nb = blocks_for(d, Lp);
   const int grid = std::max(1, std::min(nb, per_sm * sms));
-  fft_pass_pipe_kernel<N1, N2, DIR, MAXT><<<grid, threads, smem, s>>>(d, Lp, nb, a.tw);
+  fft_pass_pipe_kernel<N1, N2, DIR, MAXT, COLS><<<grid, threads, smem, s>>>(d, Lp, nb, a.tw);
   MLG_LAUNCHED();
   return MLG_OK;
 }
@@ -775,8 +845,15 @@ static int launch_pass(const FftAxisPlan& a, const PassDesc& d, int L, cudaStrea
     const int Lp = pipe_lines(a, d.C);
     const int cols = Lp * d.C, tp = threads_for(cols);
     if ((d.C & 1) == 0 && tp % cols == 0 && 2 * (size_t)a.N * cols * sizeof(float2) <= kFftSmemCap) {
-      if (tp <= kFftThreads) return launch_pipe<N1, N2, DIR, kFftThreads>(a, d, Lp, tp, s);
-      return launch_pipe<N1, N2, DIR, kFftMaxThreads>(a, d, Lp, tp, s);
+      // the column counts of 2, 4, 8, 12, 16, 24 and 32 coils: compile-time
+      switch (cols) {
+        case 16: return launch_pipe<N1, N2, DIR, kFftThreads, 16>(a, d, Lp, tp, s);
+        case 24: return launch_pipe<N1, N2, DIR, kFftMaxThreads, 24>(a, d, Lp, tp, s);
+        case 32: return launch_pipe<N1, N2, DIR, kFftThreads, 32>(a, d, Lp, tp, s);
+        default: break;
+      }
+      if (tp <= kFftThreads) return launch_pipe<N1, N2, DIR, kFftThreads, 0>(a, d, Lp, tp, s);
+      return launch_pipe<N1, N2, DIR, kFftMaxThreads, 0>(a, d, Lp, tp, s);
     }
   }
   const int threads = threads_for(L * d.C);
