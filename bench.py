@@ -227,7 +227,9 @@ def run_gpu(args):
     t0 = time.time()
     w = koosh3d()
     Gu, Gut = mb.bmTraj2SparseMat(w.t, w.ve, w.N_u, w.dK_u, w.kernelType, w.nWin, w.kernelParam)
-    rec = mb.SensaRecon(Gu, Gut, w.C, w.n_u, autotune=True)
+    rec = mb.SensaRecon(Gu, Gut, w.C, w.n_u, autotune=args.adjoint == "auto")
+    if args.adjoint != "auto":  # fixed strategy (profiling: launch timing under a profiler misleads the tuner)
+        rec.plan.adjoint_mode = args.adjoint
     dev = torch.device("cuda", local)
     x_true = torch.from_numpy(w.x_true).to(dev)
     y = rec.plan.shanna(x_true)
@@ -373,7 +375,7 @@ def run_gpu(args):
                    "l2": "working set (2.1 GB grid) larger than L2 each step", **w.info},
         "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
         "recon_rel_err_vs_phantom": round(err, 5), "setup_s": round(setup_s, 2),
-        "autotune": {"adjoint": adjoint_c2, "ms": {k: round(v, 4) for k, v in rec.tuning.items()}},
+        "autotune": {"adjoint": adjoint_c2, "ms": {k: round(v, 4) for k, v in (rec.tuning or {}).items()}},
         "vs_plain_gpu": plain,
         **extra,
     }
@@ -595,6 +597,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-GPU comparison arm")
     ap.add_argument("--no-extra", action="store_true", help="skip the c1 / c3 / c4 / c5 configurations")
+    ap.add_argument("--adjoint", default="auto", choices=["auto", "masked", "fused", "full_grid"],
+                    help="adjoint strategy of the headline plan (auto: autotuned)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

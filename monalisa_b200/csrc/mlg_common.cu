@@ -87,6 +87,7 @@ void csr_free(Csr& c) {
   cudaFree(c.long_seg0);
   cudaFree(c.nz_rows);
   cudaFree(c.nz_mask);
+  cudaFree(c.nz_rowptr);
   cudaFree(c.val_h);
   c = Csr();
 }
@@ -119,6 +120,14 @@ __global__ void nz_rows_kernel(const uint32_t* __restrict__ mask, const int* __r
   }
 }
 
+// rp[i] = row_ptr[rows[i]] (i < n), rp[n] = row_ptr[l_size]: the entries of
+// the non-empty rows are contiguous and in row order
+__global__ void nz_rowptr_kernel(const uint32_t* __restrict__ row_ptr, const int* __restrict__ rows, int n, int l_size,
+                                 uint32_t* __restrict__ rp) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i <= n; i += gridDim.x * blockDim.x)
+    rp[i] = i < n ? row_ptr[rows[i]] : row_ptr[l_size];
+}
+
 int csr_build_nonempty(Csr& c, cudaStream_t s) {
   if (c.nz_mask) return MLG_OK;
   const int nw = (c.l_size + 31) / 32;
@@ -144,6 +153,10 @@ int csr_build_nonempty(Csr& c, cudaStream_t s) {
   MLG_CUDA(cudaMemcpyAsync(off, h.data(), sizeof(int) * (nw + 1), cudaMemcpyHostToDevice, s));
   MLG_CUDA(cudaMalloc(&c.nz_rows, sizeof(int) * (size_t)std::max(1, run)));
   nz_rows_kernel<<<g, 256, 0, s>>>(c.nz_mask, off, nw, c.nz_rows);
+  count_launch();
+  MLG_CUDA(cudaMalloc(&c.nz_rowptr, sizeof(uint32_t) * (size_t)(run + 1)));
+  nz_rowptr_kernel<<<std::max(1, std::min(4096, (run + 256) / 256)), 256, 0, s>>>(c.row_ptr, c.nz_rows, run,
+                                                                                  c.l_size, c.nz_rowptr);
   count_launch();
   MLG_CUDA(cudaStreamSynchronize(s));
   cudaFree(cnt);

@@ -663,6 +663,61 @@ __device__ __forceinline__ void smem_fft_fixed(float2* s, const float2* __restri
   __syncthreads();
 }
 
+// Issues (without committing) the asynchronous copies of line bundle b into
+// dst ([N][cv] float4, coil pairs): thread (r0, vc) copies rows r0, r0 +
+// rstep, ... of its coil pair; rows outside the stored input range, cells
+// unset in the occupancy mask and lines past the grid edge are written as
+// zeros.  EXACT: rstep divides N (every thread has the same row count).
+template <int N, bool EXACT>
+__device__ __forceinline__ void pipe_issue_lines(const PassDesc& d, int L, int gu, int l, int c, int vc, int r0,
+                                                 int cv, int rstep, int b, float4* dst) {
+  const int u = d.ax == 0 ? 1 : 0, v = d.ax == 2 ? 1 : 2;
+  const long long ist = d.in_stride[d.ax], cst = d.cell_stride[d.ax];
+  const uint32_t* mask = d.in_mask;
+  const int in_lo = d.in_lo, in_hi = d.in_lo + d.in_len;
+  const int ui = (b % gu) * L + l, vi = b / gu;
+  const bool line_ok = ui < d.dims[u];
+  const float2* src = d.in + (long long)ui * d.in_stride[u] + (long long)vi * d.in_stride[v] + c +
+                      (long long)(r0 - in_lo) * ist;
+  const long long cell0 = (long long)ui * d.cell_stride[u] + (long long)vi * d.cell_stride[v] + (long long)r0 * cst;
+  float4* const drow = dst + r0 * cv + vc;
+  // rows in batches of 8: the batch's mask words are loaded together before
+  // any copy depends on them
+  constexpr int kB = 8;
+#pragma unroll
+  for (int nb0 = 0; nb0 < N; nb0 += kB * rstep) {
+    bool ld[kB];
+#pragma unroll
+    for (int j = 0; j < kB; ++j) {
+      const int n = nb0 + j * rstep + r0;
+      const bool row = EXACT ? nb0 + j * rstep < N : n < N;
+      ld[j] = line_ok && row && n >= in_lo && n < in_hi;
+    }
+    if (mask) {
+      uint32_t w[kB];
+#pragma unroll
+      for (int j = 0; j < kB; ++j) {
+        const long long cell = cell0 + (long long)(nb0 + j * rstep) * cst;
+        w[j] = ld[j] ? __ldg(mask + (cell >> 5)) >> (cell & 31) : 0u;
+      }
+#pragma unroll
+      for (int j = 0; j < kB; ++j) ld[j] = ld[j] && (w[j] & 1u);
+    }
+#pragma unroll
+    for (int j = 0; j < kB; ++j) {
+      const int nrel = nb0 + j * rstep;
+      const bool row = EXACT ? nrel < N : nrel + r0 < N;
+      if (row) {
+        float4* dp = drow + nrel * cv;
+        if (ld[j])
+          cp_async16(dp, src + (long long)nrel * ist);
+        else
+          *dp = make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+    }
+  }
+}
+
 // Resident CTAs per SM the pipelined pass asks the register allocator for:
 // what its shared memory allows (two N x cols buffers), at most 3.
 constexpr int pipe_min_blocks(int N, int cols, int maxt) {
@@ -691,52 +746,10 @@ __global__ void __launch_bounds__(COLS > 0 ? cta_threads(COLS) : MAXT,
   const int col = vc * 2, l = col / C, c = col - l * C;
   const int u = d.ax == 0 ? 1 : 0, v = d.ax == 2 ? 1 : 2;
   const int gu = (d.dims[u] + L - 1) / L;
-  const long long ist = d.in_stride[d.ax], ost = d.out_stride[d.ax], cst = d.cell_stride[d.ax];
-  const uint32_t* mask = d.in_mask;
-  const int in_lo = d.in_lo, in_hi = d.in_lo + d.in_len;
+  const long long ost = d.out_stride[d.ax];
 
   auto issue = [&](int b, float4* dst) {
-    const int ui = (b % gu) * L + l, vi = b / gu;
-    const bool line_ok = ui < d.dims[u];
-    const float2* src = d.in + (long long)ui * d.in_stride[u] + (long long)vi * d.in_stride[v] + c +
-                        (long long)(r0 - in_lo) * ist;
-    const long long cell0 = (long long)ui * d.cell_stride[u] + (long long)vi * d.cell_stride[v] + (long long)r0 * cst;
-    float4* const drow = dst + r0 * cv + vc;
-    // rows in batches of 8: the batch's mask words are loaded together before
-    // any copy depends on them
-    constexpr int kB = 8;
-#pragma unroll
-    for (int nb0 = 0; nb0 < N; nb0 += kB * rstep) {
-      bool ld[kB];
-#pragma unroll
-      for (int j = 0; j < kB; ++j) {
-        const int n = nb0 + j * rstep + r0;
-        const bool row = kExact ? nb0 + j * rstep < N : n < N;
-        ld[j] = line_ok && row && n >= in_lo && n < in_hi;
-      }
-      if (mask) {
-        uint32_t w[kB];
-#pragma unroll
-        for (int j = 0; j < kB; ++j) {
-          const long long cell = cell0 + (long long)(nb0 + j * rstep) * cst;
-          w[j] = ld[j] ? __ldg(mask + (cell >> 5)) >> (cell & 31) : 0u;
-        }
-#pragma unroll
-        for (int j = 0; j < kB; ++j) ld[j] = ld[j] && (w[j] & 1u);
-      }
-#pragma unroll
-      for (int j = 0; j < kB; ++j) {
-        const int nrel = nb0 + j * rstep;
-        const bool row = kExact ? nrel < N : nrel + r0 < N;
-        if (row) {
-          float4* dp = drow + nrel * cv;
-          if (ld[j])
-            cp_async16(dp, src + (long long)nrel * ist);
-          else
-            *dp = make_float4(0.f, 0.f, 0.f, 0.f);
-        }
-      }
-    }
+    pipe_issue_lines<N, kExact>(d, L, gu, l, c, vc, r0, cv, rstep, b, dst);
     cp_async_commit();
   };
 
@@ -769,6 +782,107 @@ __global__ void __launch_bounds__(COLS > 0 ? cta_threads(COLS) : MAXT,
       }
     }
     __syncthreads();  // cur is refilled by the copies issued in the next iteration
+  }
+}
+
+// Pipelined inverse x pass fused with .* KFC_conj and the coil sum
+// (kNakatshaOut) for coil counts C = 2 CP with CP | 8 (2, 4, 8, 16 coils):
+// 16 columns (L = 16 / C lines) per bundle.  The bundle's KFC_conj rows
+// (contiguous: L lines x out_len pixels x C coils) arrive in the same copy
+// group as its lines.  After the transform a group of CP lanes per output
+// pixel multiplies its coil pairs and sums them by a shuffle tree; the
+// group's first lane stores the pixel and adds |x|^2 (FP64) to the thread's
+// sum, reduced per CTA into partial[blockIdx.x].  CTA 0 zeroes the slots
+// [gridDim.x, n_slots) so that the caller reduces n_slots values.
+template <int N1, int N2, int CP>
+__global__ void __launch_bounds__(256, 2)
+    fft_nak_pipe_kernel(PassDesc d, int L, int nbundles, int n_slots, const float2* __restrict__ tw) {
+  constexpr int COLS = 16, NT = 256, N = N1 * N2, CV = COLS / 2, RSTEP = NT / CV;
+  static_assert(cta_threads(COLS) == NT && CV % CP == 0, "bundle shape");
+  constexpr int G = NT / CP;  // pixel groups per round
+  extern __shared__ float4 s4all[];
+  __shared__ double red[NT / 32];
+  const int C = 2 * CP;
+  const int out_len = d.out_len;
+  float4* const lb0 = s4all;
+  float4* const lb1 = s4all + N * CV;
+  float4* const kb0 = s4all + 2 * N * CV;
+  float4* const kb1 = kb0 + out_len * CV;
+  const int vc = threadIdx.x % CV, r0 = threadIdx.x / CV;
+  const int col = vc * 2, l = col / C, c = col - l * C;
+  const int gu = (d.dims[1] + L - 1) / L;  // x pass: lines over (y, z)
+  const int q = threadIdx.x % CP, grp = threadIdx.x / CP;
+
+  auto issue = [&](int b, float4* ldst, float4* kdst) {
+    pipe_issue_lines<N, N % RSTEP == 0>(d, L, gu, l, c, vc, r0, CV, RSTEP, b, ldst);
+    const int u0 = (b % gu) * L, vi = b / gu;
+    const int nl = min(L, d.dims[1] - u0);  // lines inside the grid
+    const float4* ksrc =
+        reinterpret_cast<const float4*>(d.kfc + (long long)out_len * (u0 + (long long)d.dims[1] * vi) * C);
+    const int n4 = nl * out_len * CP;
+    for (int i = threadIdx.x; i < n4; i += NT) cp_async16(kdst + i, ksrc + i);
+    cp_async_commit();
+  };
+
+  double sq = 0.0;
+  int b = blockIdx.x;
+  if (b < nbundles) issue(b, lb0, kb0);
+  for (int it = 0; b < nbundles; ++it, b += gridDim.x) {
+    float4* const cur = (it & 1) ? lb1 : lb0;
+    const float4* const kcur = (it & 1) ? kb1 : kb0;
+    const int nb = b + gridDim.x;
+    if (nb < nbundles) {
+      issue(nb, (it & 1) ? lb0 : lb1, (it & 1) ? kb0 : kb1);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    smem_fft_fixed<N1, N2, 1, COLS, NT>(reinterpret_cast<float2*>(cur), tw);  // ends with a barrier
+    const int u0 = (b % gu) * L, vi = b / gu;
+    const int total = L * out_len;
+    const int rounds = (total + G - 1) / G;  // uniform: every lane reaches the shuffles
+    for (int rd = 0; rd < rounds; ++rd) {
+      const int o = rd * G + grp;
+      const bool live = o < total;
+      const int ll = live ? o / out_len : 0;
+      const int kk = live ? o - ll * out_len : 0;
+      const int ui = u0 + ll;
+      const bool ok = live && ui < d.dims[1];
+      const int k = d.out_lo + kk;
+      float2 acc = make_float2(0.f, 0.f);
+      if (ok) {
+        const int pos = (k % N1) * N2 + k / N1;
+        const float sg = ((k + d.coord_off[1] + ui + d.coord_off[2] + vi) & 1) ? -d.sfac : d.sfac;
+        const float4 sv = cur[pos * CV + ll * CP + q];
+        const float4 kv = kcur[(ll * out_len + kk) * CP + q];
+        const float2 t0 = cmulf(make_float2(sv.x * sg, sv.y * sg), make_float2(kv.x, kv.y));
+        const float2 t1 = cmulf(make_float2(sv.z * sg, sv.w * sg), make_float2(kv.z, kv.w));
+        acc = make_float2(t0.x + t1.x, t0.y + t1.y);
+      }
+#pragma unroll
+      for (int w = CP / 2; w > 0; w >>= 1) {
+        acc.x += __shfl_xor_sync(0xffffffffu, acc.x, w, CP);
+        acc.y += __shfl_xor_sync(0xffffffffu, acc.y, w, CP);
+      }
+      if (ok && q == 0) {
+        d.img_out[kk + (long long)out_len * (ui + (long long)d.dims[1] * vi)] = acc;
+        sq += (double)acc.x * acc.x + (double)acc.y * acc.y;
+      }
+    }
+    __syncthreads();  // both buffers are refilled by the next iteration's copies
+  }
+  if (d.partial) {
+    for (int o = 16; o > 0; o >>= 1) sq += __shfl_down_sync(0xffffffffu, sq, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = sq;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int i = 0; i < NT / 32; ++i) t += red[i];
+      d.partial[blockIdx.x] = t;
+    }
+    if (blockIdx.x == 0)
+      for (int i = (int)gridDim.x + threadIdx.x; i < n_slots; i += NT) d.partial[i] = 0.0;
   }
 }
 
@@ -839,8 +953,46 @@ static inline int pipe_lines(const FftAxisPlan& a, int C) {
   return L;
 }
 
+// Pipelined kNakatshaOut pass; n_slots = the CTA count of the unpipelined
+// pass (the partial-sum slots the caller reduces), an upper bound of the grid.
+template <int N1, int N2, int CP>
+static int launch_nak_pipe(const FftAxisPlan& a, const PassDesc& d, int n_slots, cudaStream_t s) {
+  const int Lp = 16 / (2 * CP);
+  const size_t smem = 2 * ((size_t)a.N + d.out_len) * 16 * sizeof(float2);
+  thread_local int per_sm = 0, sms = 0;
+  thread_local size_t per_sm_smem = 0;
+  if (per_sm == 0 || per_sm_smem != smem) {
+    MLG_CUDA(cudaFuncSetAttribute(fft_nak_pipe_kernel<N1, N2, CP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)(200 * 1024)));
+    int dev = 0;
+    MLG_CUDA(cudaGetDevice(&dev));
+    MLG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    MLG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fft_nak_pipe_kernel<N1, N2, CP>, 256, smem));
+    per_sm = std::max(1, per_sm);
+    per_sm_smem = smem;
+  }
+  const int nb = blocks_for(d, Lp);
+  const int grid = std::max(1, std::min(std::min(nb, per_sm * sms), n_slots));
+  fft_nak_pipe_kernel<N1, N2, CP><<<grid, 256, smem, s>>>(d, Lp, nb, n_slots, a.tw);
+  MLG_LAUNCHED();
+  return MLG_OK;
+}
+
 template <int N1, int N2, int DIR, PassMode MODE>
 static int launch_pass(const FftAxisPlan& a, const PassDesc& d, int L, cudaStream_t s) {
+  if constexpr (MODE == PassMode::kNakatshaOut && N1 > 0) {
+    // 2, 4, 8 or 16 coils, two bundles of lines and KFC rows within ~100 KB
+    if (2 * ((size_t)a.N + d.out_len) * 16 * sizeof(float2) <= 104 * 1024) {
+      const int n_slots = blocks_for(d, L);
+      switch (d.C) {
+        case 16: return launch_nak_pipe<N1, N2, 8>(a, d, n_slots, s);
+        case 8: return launch_nak_pipe<N1, N2, 4>(a, d, n_slots, s);
+        case 4: return launch_nak_pipe<N1, N2, 2>(a, d, n_slots, s);
+        case 2: return launch_nak_pipe<N1, N2, 1>(a, d, n_slots, s);
+        default: break;
+      }
+    }
+  }
   if constexpr (MODE == PassMode::kPlain && N1 > 0) {
     const int Lp = pipe_lines(a, d.C);
     const int cols = Lp * d.C, tp = threads_for(cols);

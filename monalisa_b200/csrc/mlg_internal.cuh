@@ -127,6 +127,9 @@ struct Csr {
   // csr_build_nonempty
   int* nz_rows = nullptr;
   uint32_t* nz_mask = nullptr;
+  // entry bounds of the non-empty rows: row nz_rows[i] holds entries
+  // [nz_rowptr[i], nz_rowptr[i + 1]) ([n_nonempty + 1])
+  uint32_t* nz_rowptr = nullptr;
   // FP16 copy of val for the mixed-precision solver (built on demand)
   __half* val_h = nullptr;
 };

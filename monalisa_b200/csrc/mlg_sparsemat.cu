@@ -233,7 +233,8 @@ __global__ void __launch_bounds__(256) spmm_seg_combine_kernel(SpmmParams p, con
 // Point layout in and out, even nCh: a thread owns a (row, coil pair) output
 // and moves 16 bytes per load/store; the row's column/value stream is read
 // once per pair instead of once per coil.  `rows` (optional) lists the rows
-// to compute (the non-empty ones); other rows are left untouched.  Entries
+// to compute (the non-empty ones) and `rptr` their entry bounds (rows[i]
+// holds entries [rptr[i], rptr[i + 1])); other rows are left untouched.  Entries
 // are summed in stored order with round-to-nearest multiply/add.
 // A coil pair: two complex values, FP32 (float4) or BF16 (4 x bf16 = uint2).
 template <bool BF>
@@ -263,7 +264,8 @@ __device__ __forceinline__ void st_pair(void* base, long long i, float4 v) {
 }
 
 template <bool IN_BF, bool OUT_BF>
-__global__ void __launch_bounds__(256) spmm_pair_kernel(SpmmParams p, const int* __restrict__ rows, int n_rows) {
+__global__ void __launch_bounds__(256, 6) spmm_pair_kernel(SpmmParams p, const int* __restrict__ rows,
+                                                        const uint32_t* __restrict__ rptr, int n_rows) {
   __shared__ double sh[32];
   const int P = p.nCh >> 1;
   const long long i0 = (long long)blockIdx.x * p.rows_per_block;
@@ -272,8 +274,17 @@ __global__ void __launch_bounds__(256) spmm_pair_kernel(SpmmParams p, const int*
   double sq = 0.0;
   for (int it = threadIdx.x; it < nr * P; it += blockDim.x) {
     const int lr = it / P, pi = it - (it / P) * P;
-    const long long r = rows ? (long long)__ldg(rows + i0 + lr) : i0 + lr;
-    const uint32_t b = __ldg(p.row_ptr + r), e = __ldg(p.row_ptr + r + 1);
+    long long r;
+    uint32_t b, e;
+    if (rows) {  // listed rows: bounds from rptr, independent of the row index load
+      r = __ldg(rows + i0 + lr);
+      b = __ldg(rptr + i0 + lr);
+      e = __ldg(rptr + i0 + lr + 1);
+    } else {
+      r = i0 + lr;
+      b = __ldg(p.row_ptr + r);
+      e = __ldg(p.row_ptr + r + 1);
+    }
     if (e - b > (uint32_t)kLongRow) continue;  // segment kernels own it
     float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll 4
@@ -303,6 +314,11 @@ __global__ void __launch_bounds__(256) spmm_pair_kernel(SpmmParams p, const int*
     const double t = block_sum(sq, sh);
     if (threadIdx.x == 0) p.partial[blockIdx.x] = t;
   }
+}
+
+template <bool IN_BF, bool OUT_BF>
+static void launch_pair(const SpmmParams& p, const Csr& m, const int* rows, int nrows, int grid, cudaStream_t s) {
+  spmm_pair_kernel<IN_BF, OUT_BF><<<grid, 256, 0, s>>>(p, rows, rows ? m.nz_rowptr : nullptr, nrows);
 }
 
 static bool point_c(Layout l) { return l == Layout::kPointC64 || l == Layout::kPointBF16; }
@@ -381,14 +397,15 @@ int spmm(const SpmmArgs& a, cudaStream_t s) {
     const bool ib = i == L::kPointBF16, ob = o == L::kPointBF16;
     if (grid_short > 0) {
       const int* rl = a.nonempty_only ? m.nz_rows : nullptr;
+      MLG_CHECK(!rl || m.nz_rowptr, "non-empty-row products need the row bounds");
       if (ib && !ob)
-        spmm_pair_kernel<true, false><<<grid_short, 256, 0, s>>>(p, rl, (int)nrows);
+        launch_pair<true, false>(p, m, rl, (int)nrows, grid_short, s);
       else if (!ib && ob)
-        spmm_pair_kernel<false, true><<<grid_short, 256, 0, s>>>(p, rl, (int)nrows);
+        launch_pair<false, true>(p, m, rl, (int)nrows, grid_short, s);
       else if (ib && ob)
-        spmm_pair_kernel<true, true><<<grid_short, 256, 0, s>>>(p, rl, (int)nrows);
+        launch_pair<true, true>(p, m, rl, (int)nrows, grid_short, s);
       else
-        spmm_pair_kernel<false, false><<<grid_short, 256, 0, s>>>(p, rl, (int)nrows);
+        launch_pair<false, false>(p, m, rl, (int)nrows, grid_short, s);
       MLG_LAUNCHED();
     }
     // long rows (segment kernels) with the same element types

@@ -261,16 +261,19 @@ def test_shanna_nakatsha_gateways(mex, op2d):
     assert rel(xR + 1j * xI, g["nakatsha"]) <= 1e-5
 
 
+@pytest.mark.parametrize("nCh", [3, 8, 16])
 @pytest.mark.parametrize("N_u,n_u", [([16, 20, 12], [8, 10, 6]), ([48, 96, 16], [24, 48, 8]),
                                      ([192, 16, 24], [96, 8, 12])])
-def test_operators_3d_and_per_coil(N_u, n_u):
+def test_operators_3d_and_per_coil(N_u, n_u, nCh):
     """3-D Shanna with per-coil x and Nakatsha, package API, vs oracle.
     Line lengths: 16, 32 (radix-2 passes), 20, 12, 24 (runtime DFT passes),
-    48, 96, 192 (radix-3 x radix-2 passes)."""
+    48, 96, 192 (radix-3 x radix-2 passes).  Coil counts: odd (per-element
+    passes), 8 and 16 (pipelined passes of 16 columns: 2 and 1 lines per
+    bundle)."""
     import monalisa_b200 as mb
 
     rng = np.random.default_rng(3)
-    N_u, n_u, nCh = np.array(N_u), np.array(n_u), 3
+    N_u, n_u = np.array(N_u), np.array(n_u)
     t = rng.uniform(-0.5, 0.5, (3, 3000)) * N_u[:, None]
     G = oracle.traj2sparsemat(t, np.ones(3000), N_u, [1, 1, 1], "gauss", 3, [0.61, 10])
     C = (rng.standard_normal((n_u.prod(), nCh)) + 1j * rng.standard_normal((n_u.prod(), nCh))).astype(np.complex64)
