@@ -58,6 +58,11 @@ struct PassDesc {
   // only if its bit is set and is zero otherwise (cells a sparse product left
   // unwritten)
   const uint32_t* in_mask = nullptr;
+  // the same bits regrouped per line (optional, with in_mask): bit n of word
+  // n / 32 of line ui + dims[u] * vi, lmask_words words per line (a multiple
+  // of 4); the pipelined pass fetches them ahead of the line copies
+  const uint32_t* in_lmask = nullptr;
+  int lmask_words = 0;
 };
 
 int fft_axis_init(int N, FftAxisPlan& a);

@@ -668,9 +668,12 @@ __device__ __forceinline__ void smem_fft_fixed(float2* s, const float2* __restri
 // rstep, ... of its coil pair; rows outside the stored input range, cells
 // unset in the occupancy mask and lines past the grid edge are written as
 // zeros.  EXACT: rstep divides N (every thread has the same row count).
+// lbits (optional): the bundle's line masks in shared memory (lw words per
+// line), read in place of the occupancy mask in global memory.
 template <int N, bool EXACT>
 __device__ __forceinline__ void pipe_issue_lines(const PassDesc& d, int L, int gu, int l, int c, int vc, int r0,
-                                                 int cv, int rstep, int b, float4* dst) {
+                                                 int cv, int rstep, int b, float4* dst, const uint32_t* lbits,
+                                                 int lw) {
   const int u = d.ax == 0 ? 1 : 0, v = d.ax == 2 ? 1 : 2;
   const long long ist = d.in_stride[d.ax], cst = d.cell_stride[d.ax];
   const uint32_t* mask = d.in_mask;
@@ -693,7 +696,14 @@ __device__ __forceinline__ void pipe_issue_lines(const PassDesc& d, int L, int g
       const bool row = EXACT ? nb0 + j * rstep < N : n < N;
       ld[j] = line_ok && row && n >= in_lo && n < in_hi;
     }
-    if (mask) {
+    if (lbits) {
+      const uint32_t* lb = lbits + l * lw;
+#pragma unroll
+      for (int j = 0; j < kB; ++j) {
+        const int n = nb0 + j * rstep + r0;
+        ld[j] = ld[j] && ((lb[n >> 5] >> (n & 31)) & 1u);
+      }
+    } else if (mask) {
       uint32_t w[kB];
 #pragma unroll
       for (int j = 0; j < kB; ++j) {
@@ -747,20 +757,43 @@ __global__ void __launch_bounds__(COLS > 0 ? cta_threads(COLS) : MAXT,
   const int u = d.ax == 0 ? 1 : 0, v = d.ax == 2 ? 1 : 2;
   const int gu = (d.dims[u] + L - 1) / L;
   const long long ost = d.out_stride[d.ax];
-
-  auto issue = [&](int b, float4* dst) {
-    pipe_issue_lines<N, kExact>(d, L, gu, l, c, vc, r0, cv, rstep, b, dst);
-    cp_async_commit();
+  // line masks (optional): a ring of 4 slots of L x LW words after the two
+  // buffers; the masks of the bundle three iterations ahead are copied with
+  // the next bundle's lines, so they have landed (and a barrier has passed)
+  // before the iteration that issues that bundle's copies reads them
+  const int LW = d.lmask_words;
+  uint32_t* const ring = d.in_lmask ? reinterpret_cast<uint32_t*>(s4all + 2 * (size_t)N * cv) : nullptr;
+  auto slot = [&](int k) { return ring + (k & 3) * L * LW; };
+  auto fetch_masks = [&](int bk, uint32_t* dst) {
+    const int per_line = LW >> 2;
+    for (int t = threadIdx.x; t < L * per_line; t += nthr) {
+      const int ll = t / per_line, w4 = t - ll * per_line;
+      const int ui = (bk % gu) * L + ll, vi = bk / gu;
+      if (ui < d.dims[u])
+        cp_async16(dst + ll * LW + 4 * w4, d.in_lmask + ((long long)ui + (long long)d.dims[u] * vi) * LW + 4 * w4);
+    }
   };
 
   int b = blockIdx.x;
   if (b >= nbundles) return;
-  issue(b, buf0);
-  for (int it = 0; b < nbundles; ++it, b += gridDim.x) {
+  const int G = gridDim.x;
+  if (ring) {  // masks of the first three bundles
+    for (int k = 0; k < 3; ++k)
+      if (b + k * G < nbundles) fetch_masks(b + k * G, slot(k));
+    cp_async_commit();
+    cp_async_wait<0>();
+    __syncthreads();
+  }
+  pipe_issue_lines<N, kExact>(d, L, gu, l, c, vc, r0, cv, rstep, b, buf0, ring ? slot(0) : nullptr, LW);
+  cp_async_commit();
+  for (int it = 0; b < nbundles; ++it, b += G) {
     float4* cur = (it & 1) ? buf1 : buf0;
-    const int nb = b + gridDim.x;
+    const int nb = b + G;
     if (nb < nbundles) {
-      issue(nb, (it & 1) ? buf0 : buf1);
+      pipe_issue_lines<N, kExact>(d, L, gu, l, c, vc, r0, cv, rstep, nb, (it & 1) ? buf0 : buf1,
+                                  ring ? slot(it + 1) : nullptr, LW);
+      if (ring && b + 3 * G < nbundles) fetch_masks(b + 3 * G, slot(it + 3));
+      cp_async_commit();
       cp_async_wait<1>();  // all but the copies just issued have landed
     } else {
       cp_async_wait<0>();
@@ -814,7 +847,7 @@ __global__ void __launch_bounds__(256, 2)
   const int q = threadIdx.x % CP, grp = threadIdx.x / CP;
 
   auto issue = [&](int b, float4* ldst, float4* kdst) {
-    pipe_issue_lines<N, N % RSTEP == 0>(d, L, gu, l, c, vc, r0, CV, RSTEP, b, ldst);
+    pipe_issue_lines<N, N % RSTEP == 0>(d, L, gu, l, c, vc, r0, CV, RSTEP, b, ldst, nullptr, 0);
     const int u0 = (b % gu) * L, vi = b / gu;
     const int nl = min(L, d.dims[1] - u0);  // lines inside the grid
     const float4* ksrc =
@@ -923,7 +956,8 @@ static int launch_bounded(const FftAxisPlan& a, const PassDesc& d, int L, int th
 // CTAs per SM) x SMs.
 template <int N1, int N2, int DIR, int MAXT, int COLS>
 static int launch_pipe(const FftAxisPlan& a, const PassDesc& d, int Lp, int threads, cudaStream_t s) {
-  const size_t smem = 2 * (size_t)a.N * Lp * d.C * sizeof(float2);
+  const size_t smem = 2 * (size_t)a.N * Lp * d.C * sizeof(float2) +
+                      (d.in_lmask ? 4 * (size_t)Lp * d.lmask_words * sizeof(uint32_t) : 0);
   // per instantiation and host thread (serving workers launch concurrently);
   // recomputed when the coil count changes the CTA's shared memory or threads
   thread_local int per_sm = 0, sms = 0, per_sm_threads = 0;

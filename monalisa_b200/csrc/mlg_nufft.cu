@@ -144,6 +144,8 @@ static int inverse_pass(mlg_plan_s* p, int ax, const float2* y, const float* HY,
   if (gut_in) set_gut_input(p, pd, y, HY);
   if (p->adjoint_mode == kAdjMasked && ax == d - 1) {
     pd.in_mask = p->Gut_s.nz_mask;
+    pd.in_lmask = p->line_mask;
+    pd.lmask_words = p->line_mask_words;
     pd.cell_stride[0] = 1;
     pd.cell_stride[1] = p->N[0];
     pd.cell_stride[2] = (long long)p->N[0] * p->N[1];
@@ -319,6 +321,44 @@ int deinterleave(const float2* in, long long n, float* re, float* im, cudaStream
   return MLG_OK;
 }
 
+// Line masks of the masked first inverse pass: word w of line (ui, vi) holds
+// the occupancy bits of cells ui*cu + vi*cv + n*cax, n = 32w .. 32w+31.
+__global__ void line_mask_kernel(const uint32_t* __restrict__ nz, int du, int dv, long long cu, long long cv,
+                                 long long cax, int Nax, int LW, uint32_t* __restrict__ lm) {
+  const long long total = (long long)du * dv * LW;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long line = i / LW;
+    const int w = (int)(i - line * LW);
+    const long long base = (line % du) * cu + (line / du) * cv;
+    uint32_t m = 0;
+    for (int j = 0; j < 32 && w * 32 + j < Nax; ++j) {
+      const long long cell = base + (long long)(w * 32 + j) * cax;
+      m |= ((nz[cell >> 5] >> (cell & 31)) & 1u) << j;
+    }
+    lm[i] = m;
+  }
+}
+
+// Geometry as inverse_pass sets it for axis imDim - 1 (2-D and 3-D; in 1-D
+// that pass is the fused x pass, which reads the occupancy mask itself).
+static int build_line_mask(mlg_plan_s* p, cudaStream_t s) {
+  if (!p->Gut_s.nz_mask || p->imDim < 2) return MLG_OK;
+  const int ax = p->imDim - 1;
+  const int du = p->N[0];
+  const int dv = ax == 2 ? p->N[1] : p->n[2];
+  const long long cs[3] = {1, p->N[0], (long long)p->N[0] * p->N[1]};
+  const int v = ax == 2 ? 1 : 2;
+  const int LW = ((p->N[ax] + 31) / 32 + 3) / 4 * 4;
+  const long long total = (long long)du * dv * LW;
+  MLG_CUDA(cudaMalloc(&p->line_mask, sizeof(uint32_t) * (size_t)total));
+  p->line_mask_words = LW;
+  line_mask_kernel<<<ew_grid(total), kEwThreads, 0, s>>>(p->Gut_s.nz_mask, du, dv, cs[0], cs[v], cs[ax], p->N[ax], LW,
+                                                         p->line_mask);
+  MLG_LAUNCHED();
+  return MLG_OK;
+}
+
 // ---- plan lifecycle ---------------------------------------------------------
 static void plan_free(mlg_plan_s* p) {
   if (!p) return;
@@ -341,6 +381,7 @@ static void plan_free(mlg_plan_s* p) {
   }
   cudaFree(p->partial);
   cudaFree(p->seg_scratch);
+  cudaFree(p->line_mask);
   cudaFree(p->scalars);
   cudaFree(p->x_p);
   cudaFree(p->x_dagM);
@@ -444,6 +485,7 @@ static int plan_create_impl(int imDim, const int* N_u, const int* n_u, int nCh, 
   // sign-folded copy)
   if (Gut && (nCh % 2) == 0 && (st = csr_build_nonempty(const_cast<Csr&>(*Gut), s)) != MLG_OK) return bail(st);
   if (Gut && (st = csr_sign_copy(*Gut, true, imDim, p->N, 1.0f, p->Gut_s, s)) != MLG_OK) return bail(st);
+  if ((st = build_line_mask(p, s)) != MLG_OK) return bail(st);
   p->adjoint_mode = adjoint_mode_valid(p, kAdjMasked) ? kAdjMasked : (imDim >= 2 ? kAdjFused : kAdjFullGrid);
   const size_t kbytes = sizeof(float2) * (size_t)nu * nCh;
   const size_t gbytes = sizeof(float2) * (size_t)Nu * nCh;

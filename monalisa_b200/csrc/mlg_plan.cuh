@@ -36,6 +36,11 @@ struct mlg_plan_s {
   //  2 kAdjMasked:   Gut writes only its non-empty rows, the pass reads a
   //                  cell only when its occupancy bit is set (even nCh).
   int adjoint_mode = 0;
+  // Gut's occupancy bits regrouped per line of the first inverse pass (axis
+  // imDim - 1): line_mask_words words per line (built with the occupancy
+  // tables, for kAdjMasked)
+  uint32_t* line_mask = nullptr;
+  int line_mask_words = 0;
   double* scalars = nullptr;      // solver scalars (device)
   cudaStream_t stream = nullptr;  // internal non-blocking stream
   cudaEvent_t ev_in = nullptr, ev_out = nullptr;
