@@ -400,7 +400,7 @@ def _event_ms(fn, reps, stream):
 
 def _mixed(w, Gu, Gut, y, ve, x_fp32, ms_fp32, plain, stream, precision="mixed"):
     """c4: the c2 reconstruction in reduced precision: 'mixed' (FP16 matrix
-    values, BF16 k-space work vectors, FP32 sums, FP64 scalars) or
+    values, M p stored in scaled FP16, FP32 residual and sums, FP64 scalars) or
     'fp16_values' (FP16 matrix values only)."""
     import torch
 
@@ -422,7 +422,8 @@ def _mixed(w, Gu, Gut, y, ve, x_fp32, ms_fp32, plain, stream, precision="mixed")
            "speedup_vs_plain_gpu": round(plain["ms_per_recon"] / ms, 2) if plain else None,
            "rel_diff_vs_fp32_recon": float((x - x_fp32).norm() / x_fp32.norm()),
            "adjoint": rec.plan.adjoint_mode,
-           "precision": {"mixed": "fp16 matrix values, bf16 k-space vectors, fp32 sums/FFT, fp64 CG scalars",
+           "precision": {"mixed": "fp16 matrix values, M p in fp16 x 2^k per CG step, fp32 residual/sums/FFT, "
+                                  "fp64 CG scalars",
                          "fp16_values": "fp16 matrix values, fp32 k-space/sums/FFT, fp64 CG scalars"}[precision]}
     rec.plan.close()
     return out

@@ -317,9 +317,11 @@ int mlg_plan_autotune(mlg_plan_t p, int reps, double* ms);
 /* Precision of the plan's CG-SENSE solver (mlg_sensa_dev / mlg_sensa).
  * MLG_PRECISION_FP32: FP32 data and matrix values, FP64 scalars (the
  * reference's single-precision arithmetic).  MLG_PRECISION_MIXED: FP16 matrix
- * values (copies of Gu/Gut made once), BF16 storage of the k-space work
- * vectors (residual, M p), FP32 sums and FFTs, FP64 scalars; the caller's y
- * and x stay complex64.  Mixed precision turns the fused-gather adjoint
+ * values (copies of Gu/Gut made once), 16-bit storage of the forward product
+ * M p inside the CG steps (FP16 times a power of two chosen per step from the
+ * previous step's largest value; the first step keeps FP32), an FP32
+ * residual, FP32 sums and FFTs, FP64 scalars; the caller's y and x stay
+ * complex64.  Mixed precision turns the fused-gather adjoint
  * strategy off (it reads FP32 k-space).  The operator entry points
  * (mlg_shanna_dev, mlg_nakatsha_dev) of a mixed plan read the FP16 values
  * but keep their complex64 k-space buffers.  No reference counterpart. */

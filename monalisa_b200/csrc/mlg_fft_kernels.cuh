@@ -615,6 +615,10 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
   const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
 }
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int PENDING>
 __device__ __forceinline__ void cp_async_wait() {
@@ -818,6 +822,84 @@ __global__ void __launch_bounds__(COLS > 0 ? cta_threads(COLS) : MAXT,
   }
 }
 
+// Pipelined forward x pass fused with x .* KFC, the zero-fill and the
+// (-1)^(x+y+z) modulation (kShannaIn, one image shared by the coils).  The
+// descriptor's `in` / `in_stride` describe KFC ([pixel][C], lines of in_len
+// pixels): its rows arrive through pipe_issue_lines (zero outside [in_lo,
+// in_lo + in_len)) and the bundle's image rows (L x in_len pixels,
+// contiguous) through 8-byte copies in the same group.  The product is formed
+// in shared memory before the transform.
+template <int N1, int N2, int COLS>
+__global__ void __launch_bounds__(cta_threads(COLS), pipe_min_blocks(N1 * N2, COLS, cta_threads(COLS)))
+    fft_shanna_pipe_kernel(PassDesc d, int L, int nbundles, const float2* __restrict__ tw) {
+  constexpr int N = N1 * N2, NT = cta_threads(COLS), CV = COLS / 2, RSTEP = NT / CV;
+  extern __shared__ float4 s4all[];
+  const int C = d.C, in_lo = d.in_lo, in_len = d.in_len, in_hi = d.in_lo + d.in_len;
+  float4* const lb0 = s4all;
+  float4* const lb1 = s4all + N * CV;
+  float2* const xb0 = reinterpret_cast<float2*>(s4all + 2 * N * CV);
+  float2* const xb1 = xb0 + L * in_len;
+  const int vc = threadIdx.x % CV, r0 = threadIdx.x / CV;
+  const int col = vc * 2, l = col / C, c = col - l * C;
+  const int gu = (d.dims[1] + L - 1) / L;  // x pass: lines over (y, z)
+
+  auto issue = [&](int b, float4* ldst, float2* xdst) {
+    pipe_issue_lines<N, N % RSTEP == 0>(d, L, gu, l, c, vc, r0, CV, RSTEP, b, ldst, nullptr, 0);
+    const int u0 = (b % gu) * L, vi = b / gu;
+    const int nl = min(L, d.dims[1] - u0);
+    const float2* xsrc = d.img + (long long)in_len * (u0 + (long long)d.dims[1] * vi);
+    for (int i = threadIdx.x; i < nl * in_len; i += NT) cp_async8(xdst + i, xsrc + i);
+    cp_async_commit();
+  };
+
+  int b = blockIdx.x;
+  if (b >= nbundles) return;
+  issue(b, lb0, xb0);
+  for (int it = 0; b < nbundles; ++it, b += gridDim.x) {
+    float4* const cur = (it & 1) ? lb1 : lb0;
+    const float2* const xcur = (it & 1) ? xb1 : xb0;
+    const int nb = b + gridDim.x;
+    if (nb < nbundles) {
+      issue(nb, (it & 1) ? lb0 : lb1, (it & 1) ? xb0 : xb1);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    const int ui = (b % gu) * L + l, vi = b / gu;
+    if (ui < d.dims[1]) {  // other lines hold zeros (and no image rows)
+      const int par = (d.coord_off[1] + ui + d.coord_off[2] + vi) & 1;
+      const float2* const xl = xcur + l * in_len - in_lo;
+      for (int n = r0; n < N; n += RSTEP) {
+        if (n >= in_lo && n < in_hi) {
+          const float4 k = cur[n * CV + vc];
+          const float2 a = xl[n];
+          float2 p0 = cmulf(a, make_float2(k.x, k.y)), p1 = cmulf(a, make_float2(k.z, k.w));
+          if ((n + par) & 1) {
+            p0 = make_float2(-p0.x, -p0.y);
+            p1 = make_float2(-p1.x, -p1.y);
+          }
+          cur[n * CV + vc] = make_float4(p0.x, p0.y, p1.x, p1.y);
+        }
+      }
+    }
+    __syncthreads();
+    smem_fft_fixed<N1, N2, -1, COLS, NT>(reinterpret_cast<float2*>(cur), tw);  // ends with a barrier
+    if (ui < d.dims[1]) {
+      float2* obase = d.out + (long long)ui * d.out_stride[1] + (long long)vi * d.out_stride[2] + c;
+      const float4* const scol = cur + vc;
+      const long long ost = d.out_stride[0];
+#pragma unroll 4
+      for (int kk = r0; kk < d.out_len; kk += RSTEP) {
+        const int k = d.out_lo + kk;
+        const int pos = (k % N1) * N2 + k / N1;
+        *reinterpret_cast<float4*>(obase + (long long)kk * ost) = scol[pos * CV];
+      }
+    }
+    __syncthreads();  // both buffers are refilled by the next iteration's copies
+  }
+}
+
 // Pipelined inverse x pass fused with .* KFC_conj and the coil sum
 // (kNakatshaOut) for coil counts C = 2 CP with CP | 8 (2, 4, 8, 16 coils):
 // 16 columns (L = 16 / C lines) per bundle.  The bundle's KFC_conj rows
@@ -1012,8 +1094,51 @@ static int launch_nak_pipe(const FftAxisPlan& a, const PassDesc& d, int n_slots,
   return MLG_OK;
 }
 
+// Pipelined kShannaIn pass over COLS columns (Lp lines).
+template <int N1, int N2, int COLS>
+static int launch_shanna_pipe(const FftAxisPlan& a, const PassDesc& d, int Lp, cudaStream_t s) {
+  PassDesc k = d;  // KFC as the copied input: rows of C values, lines of in_len rows
+  k.in = d.kfc;
+  k.in_stride[0] = d.C;
+  k.in_stride[1] = (long long)d.in_len * d.C;
+  k.in_stride[2] = (long long)d.in_len * d.dims[1] * d.C;
+  k.in_mask = nullptr;
+  k.in_lmask = nullptr;
+  const size_t smem = 2 * (size_t)a.N * COLS * sizeof(float2) + 2 * (size_t)Lp * d.in_len * sizeof(float2);
+  thread_local int per_sm = 0, sms = 0;
+  thread_local size_t per_sm_smem = 0;
+  if (per_sm == 0 || per_sm_smem != smem) {
+    MLG_CUDA(cudaFuncSetAttribute(fft_shanna_pipe_kernel<N1, N2, COLS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)(200 * 1024)));
+    int dev = 0;
+    MLG_CUDA(cudaGetDevice(&dev));
+    MLG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    MLG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fft_shanna_pipe_kernel<N1, N2, COLS>,
+                                                           cta_threads(COLS), smem));
+    per_sm = std::max(1, per_sm);
+    per_sm_smem = smem;
+  }
+  const int nb = blocks_for(d, Lp);
+  const int grid = std::max(1, std::min(nb, per_sm * sms));
+  fft_shanna_pipe_kernel<N1, N2, COLS><<<grid, cta_threads(COLS), smem, s>>>(k, Lp, nb, a.tw);
+  MLG_LAUNCHED();
+  return MLG_OK;
+}
+
 template <int N1, int N2, int DIR, PassMode MODE>
 static int launch_pass(const FftAxisPlan& a, const PassDesc& d, int L, cudaStream_t s) {
+  if constexpr (MODE == PassMode::kShannaIn && N1 > 0) {
+    // one image shared by the coils, even C, 16 / 24 / 32 columns per bundle
+    const int Lp = pipe_lines(a, d.C), cols = Lp * d.C;
+    if (!d.img_per_coil && (d.C & 1) == 0 && 2 * (size_t)a.N * cols * sizeof(float2) <= kFftSmemCap) {
+      switch (cols) {
+        case 16: return launch_shanna_pipe<N1, N2, 16>(a, d, Lp, s);
+        case 24: return launch_shanna_pipe<N1, N2, 24>(a, d, Lp, s);
+        case 32: return launch_shanna_pipe<N1, N2, 32>(a, d, Lp, s);
+        default: break;
+      }
+    }
+  }
   if constexpr (MODE == PassMode::kNakatshaOut && N1 > 0) {
     // 2, 4, 8 or 16 coils, two bundles of lines and KFC rows within ~100 KB
     if (2 * ((size_t)a.N + d.out_len) * 16 * sizeof(float2) <= 104 * 1024) {

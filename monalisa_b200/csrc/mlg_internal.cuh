@@ -181,7 +181,10 @@ enum class Layout : int {
   kPointSplit = 3, // float re[rows][nCh], im[...] (MATLAB point layout)
   kCoilReal = 4,   // float [nCh][rows]           (real, column layout)
   kPointReal = 5,  // float [rows][nCh]           (real, row layout)
-  kPointBF16 = 6,  // __nv_bfloat162 [rows][nCh]  (complex, BF16 storage, coil fastest)
+  // complex [rows][nCh] in FP16, scaled: __half2(v * scale[0]) saturated at
+  // +-65504, read back as __half2 * scale[1] (scale[0] a power of two); while
+  // scale[0] == 0 the buffer holds plain float2 [rows][nCh] instead
+  kPointF16 = 6,
 };
 
 struct Operand {
@@ -189,6 +192,7 @@ struct Operand {
   void* a = nullptr;        // float2* or float* (re)
   void* b = nullptr;        // im (split layouts)
   long long rows = 0;       // leading dimension for coil-major layouts
+  const float* scale = nullptr;  // kPointF16: device {store factor, load factor}
 };
 
 struct SpmmArgs {
@@ -217,6 +221,9 @@ struct SpmmArgs {
   // Read the matrix values from m->val_h (FP16) instead of m->val; the sums
   // stay FP32.
   bool half_values = false;
+  // Optional: raised (atomicMax on the bits) to the largest |re| or |im| of
+  // the values written, before any FP16 rounding (device, non-negative float)
+  unsigned* absmax = nullptr;
 };
 
 // Scratch floats spmm needs for the long-row segments of `m` at nCh coils.

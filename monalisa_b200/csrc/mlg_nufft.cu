@@ -205,7 +205,13 @@ int shanna_stage(mlg_plan_s* p, int stage, const float2* x, bool x_per_coil, flo
   a.in.layout = Layout::kPointC64;
   a.in.a = p->grid;
   a.in.rows = p->Nu_tot;
-  a.out.layout = p->mixed_run ? Layout::kPointBF16 : Layout::kPointC64;  // k-space storage
+  if (p->mp_half) {  // M p of the mixed CG steps: scaled FP16, largest value recorded
+    a.out.layout = Layout::kPointF16;
+    a.out.scale = p->kscale;
+    a.absmax = p->kabsmax;
+  } else {
+    a.out.layout = Layout::kPointC64;
+  }
   a.half_values = p->precision != MLG_PRECISION_FP32;
   a.out.a = y;
   a.out.rows = p->nPt;
@@ -228,7 +234,7 @@ int nakatsha_stage(mlg_plan_s* p, int stage, const float2* y, const float* HY, f
     SpmmArgs a;
     a.m = &p->Gut_s;
     a.nCh = p->nCh;
-    a.in.layout = p->mixed_run ? Layout::kPointBF16 : Layout::kPointC64;  // k-space storage
+    a.in.layout = Layout::kPointC64;  // the solver's residual stays FP32 in every precision
     a.half_values = p->precision != MLG_PRECISION_FP32;
     a.in.a = const_cast<float2*>(y);
     a.in.rows = p->nPt;
@@ -382,6 +388,7 @@ static void plan_free(mlg_plan_s* p) {
   cudaFree(p->partial);
   cudaFree(p->seg_scratch);
   cudaFree(p->line_mask);
+  cudaFree(p->kscale);
   cudaFree(p->scalars);
   cudaFree(p->x_p);
   cudaFree(p->x_dagM);

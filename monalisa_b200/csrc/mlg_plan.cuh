@@ -60,11 +60,16 @@ struct mlg_plan_s {
   // matrices) borrows that plan's KFC, KFCc, grid, bufA, bufB, FFT tables,
   // stream and events; both then run in the order of that one stream.
   bool borrowed = false;
-  // MLG_PRECISION_FP32 or MLG_PRECISION_MIXED (the CG-SENSE solver then keeps
-  // its k-space vectors in BF16 and reads FP16 matrix values); mixed_run is
-  // set while such a solve runs and selects those forms in the stages
+  // MLG_PRECISION_FP32, _MIXED (the CG-SENSE solver then stores M p in
+  // scaled FP16 and reads FP16 matrix values) or _FP16_VALUES; mixed_run is
+  // set while a mixed solve runs, mp_half while its CG steps run (the forward
+  // product then writes Layout::kPointF16 with scale kscale[0..1] and raises
+  // *kabsmax, kscale + 2)
   int precision = 0;
   bool mixed_run = false;
+  bool mp_half = false;
+  float* kscale = nullptr;
+  unsigned* kabsmax = nullptr;
   int cg_graph_prec = -1;  // precision the captured CG step was built for
   mlg_plan_s* owner = nullptr;  // the plan whose buffers are borrowed
   int n_borrowers = 0;          // plans borrowing this one's buffers

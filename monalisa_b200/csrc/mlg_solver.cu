@@ -77,33 +77,45 @@ __global__ void max_kernel(const float* __restrict__ v, int n, float* out) {
   if (threadIdx.x == 0) out[blockIdx.x] = sh[0];
 }
 
-// k-space work vectors: FP32 complex, or BF16 pairs in mixed precision
-template <bool BF>
-__device__ __forceinline__ float2 kld(const void* v, long long i) {
-  if constexpr (BF)
-    return __bfloat1622float2(reinterpret_cast<const __nv_bfloat162*>(v)[i]);
-  else
-    return reinterpret_cast<const float2*>(v)[i];
+// k-space work vectors: the residual is FP32 complex; M p (recomputed from p
+// every step, so its rounding does not accumulate) is FP32 or, in mixed
+// precision, scaled FP16 (Layout::kPointF16: __half2 * scale[1], or float2
+// while scale[0] == 0)
+template <bool H>
+__device__ __forceinline__ float2 kld(const void* v, long long i, float s, float inv) {
+  if (H && s != 0.f) {
+    const float2 h = __half22float2(reinterpret_cast<const __half2*>(v)[i]);
+    return make_float2(h.x * inv, h.y * inv);
+  }
+  return reinterpret_cast<const float2*>(v)[i];
 }
-template <bool BF>
-__device__ __forceinline__ void kst(void* v, long long i, float2 x) {
-  if constexpr (BF)
-    reinterpret_cast<__nv_bfloat162*>(v)[i] = __float22bfloat162_rn(x);
-  else
-    reinterpret_cast<float2*>(v)[i] = x;
+
+// Scale of the next FP16 M p: the power of two that maps this step's largest
+// |component| just below 2^12 (16x headroom before saturation at 65504, the
+// smallest normal half 2^-26 of that maximum); absmax is reset.
+__global__ void f16_scale_kernel(unsigned* absmax, float* scale) {
+  const float m = __uint_as_float(*absmax);
+  float s = 1.f;
+  if (m > 0.f && isfinite(m)) {
+    int e = 0;
+    frexpf(m, &e);  // m < 2^e
+    s = ldexpf(1.f, max(-120, min(120, 12 - e)));
+  }
+  scale[0] = s;
+  scale[1] = 1.f / s;  // exact: a power of two
+  *absmax = 0u;
 }
 
 // res = y - Mx (k-space), optional partials of sum HY |res|^2; y is the
-// caller's FP32 data, Mx and res the work vectors
-template <bool BF>
-__global__ void residual_kernel(const float2* __restrict__ y, const void* __restrict__ Mx, long long n, int nCh,
-                                const float* __restrict__ HY, void* __restrict__ res, double* partial) {
+// caller's FP32 data, Mx and res (FP32) the work vectors
+__global__ void residual_kernel(const float2* __restrict__ y, const float2* __restrict__ Mx, long long n, int nCh,
+                                const float* __restrict__ HY, float2* __restrict__ res, double* partial) {
   __shared__ double sh[kT / 32];
   double sq = 0.0;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-    const float2 a = y[i], b = kld<BF>(Mx, i);
+    const float2 a = y[i], b = Mx[i];
     const float2 r = make_float2(__fsub_rn(a.x, b.x), __fsub_rn(a.y, b.y));
-    if (res) kst<BF>(res, i, r);
+    if (res) res[i] = r;
     sq += (double)HY[i / nCh] * ((double)r.x * r.x + (double)r.y * r.y);
   }
   if (partial) {
@@ -167,27 +179,25 @@ __global__ void cg_update_x_kernel(float2* __restrict__ x, const float2* __restr
   }
 }
 
-// res -= a Mp   (bmSensa.m:71)
-template <bool BF>
-__global__ void cg_update_res_kernel(void* __restrict__ res, const void* __restrict__ Mp, long long n,
-                                     const double* __restrict__ sc) {
+// res -= a Mp   (bmSensa.m:71); H: Mp in scaled FP16 (kscale = {s, 1/s})
+template <bool H>
+__global__ void cg_update_res_kernel(float2* __restrict__ res, const void* __restrict__ Mp, long long n,
+                                     const double* __restrict__ sc, const float* __restrict__ kscale) {
   if (sc[S_DONE] != 0.0) return;
   const float a = (float)sc[S_A];
+  const float s = H ? kscale[0] : 0.f, inv = H ? kscale[1] : 1.f;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-    const float2 m = kld<BF>(Mp, i);
-    float2 r = kld<BF>(res, i);
+    const float2 m = kld<H>(Mp, i, s, inv);
+    float2 r = res[i];
     r.x = __fsub_rn(r.x, __fmul_rn(a, m.x));
     r.y = __fsub_rn(r.y, __fmul_rn(a, m.y));
-    kst<BF>(res, i, r);
+    res[i] = r;
   }
 }
 
-static void launch_residual(bool bf, int g, const float2* y, const void* Mx, long long n, int nCh, const float* HY,
-                            void* res, double* partial, cudaStream_t s) {
-  if (bf)
-    residual_kernel<true><<<g, kT, 0, s>>>(y, Mx, n, nCh, HY, res, partial);
-  else
-    residual_kernel<false><<<g, kT, 0, s>>>(y, Mx, n, nCh, HY, res, partial);
+static void launch_residual(int g, const float2* y, const float2* Mx, long long n, int nCh, const float* HY,
+                            float2* res, double* partial, cudaStream_t s) {
+  residual_kernel<<<g, kT, 0, s>>>(y, Mx, n, nCh, HY, res, partial);
 }
 
 // p = dagM + b p   (bmSensa.m:77)
@@ -209,12 +219,16 @@ static int ensure_solver_buffers(mlg_plan_s* p) {
   cudaFree(p->k_Mp);
   cudaFree(p->HY);
   const size_t ni = sizeof(float2) * (size_t)p->nu_tot, nk = sizeof(float2) * (size_t)p->nPt * p->nCh;
+  cudaFree(p->kscale);
+  p->kscale = nullptr;
   if (cudaMalloc(&p->x_p, ni) != cudaSuccess || cudaMalloc(&p->x_dagM, ni) != cudaSuccess ||
       cudaMalloc(&p->k_res, nk) != cudaSuccess || cudaMalloc(&p->k_Mp, nk) != cudaSuccess ||
-      cudaMalloc(&p->HY, sizeof(float) * (size_t)std::max(1, p->nPt)) != cudaSuccess) {
+      cudaMalloc(&p->HY, sizeof(float) * (size_t)std::max(1, p->nPt)) != cudaSuccess ||
+      cudaMalloc(&p->kscale, 4 * sizeof(float)) != cudaSuccess) {
     cudaGetLastError();
     return fail(MLG_ERR_OOM, "solver work buffers: device allocation failed");
   }
+  p->kabsmax = reinterpret_cast<unsigned*>(p->kscale + 2);
   p->solver_nPt = p->nPt;
   p->bytes += 2 * ni + 2 * nk + sizeof(float) * (size_t)p->nPt;
   return MLG_OK;
@@ -229,16 +243,20 @@ static int cg_step(mlg_plan_s* p, float2* x, double HX, double eps, cudaStream_t
   MLG_LAUNCHED();
   cg_update_x_kernel<<<grid1(p->nu_tot), kT, 0, s>>>(x, p->x_p, p->nu_tot, p->scalars);
   MLG_LAUNCHED();
-  if (p->mixed_run)
-    cg_update_res_kernel<true><<<grid1(nk), kT, 0, s>>>(p->k_res, p->k_Mp, nk, p->scalars);
+  if (p->mp_half)
+    cg_update_res_kernel<true><<<grid1(nk), kT, 0, s>>>(p->k_res, p->k_Mp, nk, p->scalars, p->kscale);
   else
-    cg_update_res_kernel<false><<<grid1(nk), kT, 0, s>>>(p->k_res, p->k_Mp, nk, p->scalars);
+    cg_update_res_kernel<false><<<grid1(nk), kT, 0, s>>>(p->k_res, p->k_Mp, nk, p->scalars, nullptr);
   MLG_LAUNCHED();
   MLG_TRY(nakatsha_run(p, p->k_res, p->HY, (float)(1.0 / HX), p->x_dagM, p->partial, &np, s));
   cg_beta_kernel<<<1, kT, 0, s>>>(p->partial, np, HX, eps, p->scalars);
   MLG_LAUNCHED();
   cg_update_p_kernel<<<grid1(p->nu_tot), kT, 0, s>>>(p->x_p, p->x_dagM, p->nu_tot, p->scalars);
   MLG_LAUNCHED();
+  if (p->mp_half) {  // the next step's FP16 scale, from this step's M p
+    f16_scale_kernel<<<1, 1, 0, s>>>(p->kabsmax, p->kscale);
+    MLG_LAUNCHED();
+  }
   return MLG_OK;
 }
 
@@ -252,6 +270,7 @@ int sensa_run(mlg_plan_s* p, const float2* y, const float* ve, float ve_max, int
   p->mixed_run = p->precision == MLG_PRECISION_MIXED;
   const int st = sensa_body(p, y, ve, ve_max, nIter, nCGD, x, residual, use_graph, s);
   p->mixed_run = false;
+  p->mp_half = false;
   return st;
 }
 
@@ -307,13 +326,18 @@ static int sensa_body(mlg_plan_s* p, const float2* y, const float* ve, float ve_
   for (int it = 0; it < nIter; ++it) {
     // res = y - M x; dagM = (1/HX) M*(HY res); sqn = HX |dagM|^2; p = dagM
     int np = 0;
+    p->mp_half = false;  // M x of the residual and of the monitoring stay FP32
     MLG_TRY(shanna_run(p, x, false, p->k_Mp, nullptr, nullptr, nullptr, s));
-    launch_residual(p->mixed_run, grid1(nk), y, p->k_Mp, nk, p->nCh, p->HY, p->k_res, nullptr, s);
+    launch_residual(grid1(nk), y, p->k_Mp, nk, p->nCh, p->HY, p->k_res, nullptr, s);
     MLG_LAUNCHED();
     MLG_TRY(nakatsha_run(p, p->k_res, p->HY, (float)(1.0 / HX), p->x_dagM, p->partial, &np, s));
     cg_init_kernel<<<1, kT, 0, s>>>(p->partial, np, HX, eps, p->scalars);
     MLG_LAUNCHED();
     MLG_CUDA(cudaMemcpyAsync(p->x_p, p->x_dagM, sizeof(float2) * (size_t)p->nu_tot, cudaMemcpyDeviceToDevice, s));
+    if (p->mixed_run) {  // the first CG step keeps M p in FP32 and measures it
+      MLG_CUDA(cudaMemsetAsync(p->kscale, 0, 4 * sizeof(float), s));
+      p->mp_half = true;
+    }
     if (full > 0) MLG_TRY(ensure_graph());
     for (int i = 0; i < full; ++i) {
       if (use_graph) {
@@ -331,9 +355,10 @@ static int sensa_body(mlg_plan_s* p, const float2* y, const float* ve, float ve_
       MLG_LAUNCHED();
     }
     // monitoring: R = |y - Mx|^2_HY   (bmSensa.m:82-83)
+    p->mp_half = false;
     MLG_TRY(shanna_run(p, x, false, p->k_Mp, nullptr, nullptr, nullptr, s));
     const int g = grid1(nk);
-    launch_residual(p->mixed_run, g, y, p->k_Mp, nk, p->nCh, p->HY, nullptr, p->partial, s);
+    launch_residual(g, y, p->k_Mp, nk, p->nCh, p->HY, nullptr, p->partial, s);
     MLG_LAUNCHED();
     sum_to_slot_kernel<<<1, kT, 0, s>>>(p->partial, g, hist.p, it);
     MLG_LAUNCHED();
@@ -483,7 +508,6 @@ extern "C" int mlg_plan_autotune(mlg_plan_t p, int reps, double* ms) {
   int best = orig;
   double best_ms = 1e30;
   int st = MLG_OK;
-  p->mixed_run = p->precision == MLG_PRECISION_MIXED;  // time the form the solver runs
   for (int mode = 0; mode < 3 && st == MLG_OK; ++mode) {
     double t = -1.0;
     if (adjoint_mode_valid(p, mode)) {
@@ -506,7 +530,6 @@ extern "C" int mlg_plan_autotune(mlg_plan_t p, int reps, double* ms) {
   }
   cudaEventDestroy(a);
   cudaEventDestroy(b);
-  p->mixed_run = false;
   p->adjoint_mode = orig;
   if (st != MLG_OK) return st;
   return mlg_plan_set_adjoint(p, best);

@@ -40,7 +40,25 @@ struct SpmmParams {
   const float* sqn_w;
   double* partial;
   int partial_long_offset;
+  unsigned* absmax;
 };
+
+// Scaled FP16 complex values (Layout::kPointF16): saturating conversion so
+// that a scale chosen from an earlier maximum never produces infinities.
+__device__ __forceinline__ __half2 to_f16_sat(float2 v, float s) {
+  constexpr float kMax = 65504.f;
+  return __floats2half2_rn(fminf(fmaxf(v.x * s, -kMax), kMax), fminf(fmaxf(v.y * s, -kMax), kMax));
+}
+
+__device__ __forceinline__ float abs_max4(float4 v) {
+  return fmaxf(fmaxf(fabsf(v.x), fabsf(v.y)), fmaxf(fabsf(v.z), fabsf(v.w)));
+}
+
+// One atomic per warp: the warp's largest value (all lanes must call).
+__device__ __forceinline__ void warp_absmax(unsigned* absmax, float v) {
+  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(absmax, __float_as_uint(v));
+}
 
 template <Layout L>
 __device__ __forceinline__ float2 ld(const Operand& o, long long row, int c, int nCh) {
@@ -56,8 +74,11 @@ __device__ __forceinline__ float2 ld(const Operand& o, long long row, int c, int
     return make_float2(__ldg(reinterpret_cast<const float*>(o.a) + i), __ldg(reinterpret_cast<const float*>(o.b) + i));
   } else if constexpr (L == Layout::kPointReal) {
     return make_float2(__ldg(reinterpret_cast<const float*>(o.a) + row * nCh + c), 0.f);
-  } else if constexpr (L == Layout::kPointBF16) {
-    return __bfloat1622float2(reinterpret_cast<const __nv_bfloat162*>(o.a)[row * nCh + c]);
+  } else if constexpr (L == Layout::kPointF16) {
+    if (__ldg(o.scale) == 0.f) return __ldg(reinterpret_cast<const float2*>(o.a) + row * nCh + c);
+    const float2 v = __half22float2(reinterpret_cast<const __half2*>(o.a)[row * nCh + c]);
+    const float inv = __ldg(o.scale + 1);
+    return make_float2(v.x * inv, v.y * inv);
   } else {
     return make_float2(__ldg(reinterpret_cast<const float*>(o.a) + (long long)c * o.rows + row), 0.f);
   }
@@ -79,8 +100,12 @@ __device__ __forceinline__ void st(const Operand& o, long long row, int c, int n
     reinterpret_cast<float*>(o.b)[i] = v.y;
   } else if constexpr (L == Layout::kPointReal) {
     reinterpret_cast<float*>(o.a)[row * nCh + c] = v.x;
-  } else if constexpr (L == Layout::kPointBF16) {
-    reinterpret_cast<__nv_bfloat162*>(o.a)[row * nCh + c] = __float22bfloat162_rn(v);
+  } else if constexpr (L == Layout::kPointF16) {
+    const float s = __ldg(o.scale);
+    if (s == 0.f)
+      reinterpret_cast<float2*>(o.a)[row * nCh + c] = v;
+    else
+      reinterpret_cast<__half2*>(o.a)[row * nCh + c] = to_f16_sat(v, s);
   } else {
     reinterpret_cast<float*>(o.a)[(long long)c * o.rows + row] = v.x;
   }
@@ -124,6 +149,7 @@ __device__ __forceinline__ double finish(const SpmmParams& p, long long r, int c
     ay = __fmul_rn(ay, p.out_scale);
   }
   st<OUT>(p.out, r, c, p.nCh, make_float2(ax, ay));
+  if (p.absmax) atomicMax(p.absmax, __float_as_uint(fmaxf(fabsf(ax), fabsf(ay))));
   if (p.partial) {
     const double w = p.sqn_w ? (double)__ldg(p.sqn_w + r) : 1.0;
     return w * ((double)ax * ax + (double)ay * ay);
@@ -236,24 +262,12 @@ __global__ void __launch_bounds__(256) spmm_seg_combine_kernel(SpmmParams p, con
 // to compute (the non-empty ones) and `rptr` their entry bounds (rows[i]
 // holds entries [rptr[i], rptr[i + 1])); other rows are left untouched.  Entries
 // are summed in stored order with round-to-nearest multiply/add.
-// A coil pair: two complex values, FP32 (float4) or BF16 (4 x bf16 = uint2).
-template <bool BF>
-__device__ __forceinline__ float4 ld_pair(const void* base, long long i) {
-  if constexpr (BF) {
-    const uint2 r = __ldg(reinterpret_cast<const uint2*>(base) + i);
-    const float2 a = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&r.x));
-    const float2 b = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&r.y));
-    return make_float4(a.x, a.y, b.x, b.y);
-  } else {
-    return __ldg(reinterpret_cast<const float4*>(base) + i);
-  }
-}
-
-template <bool BF>
-__device__ __forceinline__ void st_pair(void* base, long long i, float4 v) {
-  if constexpr (BF) {
-    const __nv_bfloat162 a = __float22bfloat162_rn(make_float2(v.x, v.y));
-    const __nv_bfloat162 b = __float22bfloat162_rn(make_float2(v.z, v.w));
+// A coil pair: two complex values; the input is FP32 (float4), the output
+// FP32 or, with OUT_H, scaled FP16 (Layout::kPointF16: 2 x __half2 = uint2).
+template <bool OUT_H>
+__device__ __forceinline__ void st_pair(void* base, long long i, float4 v, float s) {
+  if (OUT_H && s != 0.f) {
+    const __half2 a = to_f16_sat(make_float2(v.x, v.y), s), b = to_f16_sat(make_float2(v.z, v.w), s);
     uint2 r;
     r.x = *reinterpret_cast<const unsigned int*>(&a);
     r.y = *reinterpret_cast<const unsigned int*>(&b);
@@ -263,7 +277,7 @@ __device__ __forceinline__ void st_pair(void* base, long long i, float4 v) {
   }
 }
 
-template <bool IN_BF, bool OUT_BF>
+template <bool OUT_H>
 __global__ void __launch_bounds__(256, 6) spmm_pair_kernel(SpmmParams p, const int* __restrict__ rows,
                                                         const uint32_t* __restrict__ rptr, int n_rows) {
   __shared__ double sh[32];
@@ -271,6 +285,8 @@ __global__ void __launch_bounds__(256, 6) spmm_pair_kernel(SpmmParams p, const i
   const long long i0 = (long long)blockIdx.x * p.rows_per_block;
   const int nr = (int)min((long long)p.rows_per_block, (long long)n_rows - i0);
   const bool scale = p.in_row_scale != nullptr;
+  const float so = OUT_H ? __ldg(p.out.scale) : 0.f;
+  float amax = 0.f;
   double sq = 0.0;
   for (int it = threadIdx.x; it < nr * P; it += blockDim.x) {
     const int lr = it / P, pi = it - (it / P) * P;
@@ -291,7 +307,7 @@ __global__ void __launch_bounds__(256, 6) spmm_pair_kernel(SpmmParams p, const i
     for (uint32_t k = b; k < e; ++k) {
       const int j = __ldg(p.col + k);
       const float m = val_at(p, k);
-      float4 v = ld_pair<IN_BF>(p.in.a, (long long)j * P + pi);
+      float4 v = __ldg(reinterpret_cast<const float4*>(p.in.a) + (long long)j * P + pi);
       if (scale) {
         const float h = __ldg(p.in_row_scale + j);
         v = make_float4(__fmul_rn(h, v.x), __fmul_rn(h, v.y), __fmul_rn(h, v.z), __fmul_rn(h, v.w));
@@ -304,27 +320,33 @@ __global__ void __launch_bounds__(256, 6) spmm_pair_kernel(SpmmParams p, const i
     if (p.out_scale != 1.0f)
       acc = make_float4(__fmul_rn(acc.x, p.out_scale), __fmul_rn(acc.y, p.out_scale), __fmul_rn(acc.z, p.out_scale),
                         __fmul_rn(acc.w, p.out_scale));
-    st_pair<OUT_BF>(p.out.a, r * P + pi, acc);
+    st_pair<OUT_H>(p.out.a, r * P + pi, acc, so);
+    amax = fmaxf(amax, abs_max4(acc));
     if (p.partial) {
       const double w = p.sqn_w ? (double)__ldg(p.sqn_w + r) : 1.0;
       sq += w * ((double)acc.x * acc.x + (double)acc.y * acc.y + (double)acc.z * acc.z + (double)acc.w * acc.w);
     }
   }
+  if (p.absmax) warp_absmax(p.absmax, amax);
   if (p.partial) {
     const double t = block_sum(sq, sh);
     if (threadIdx.x == 0) p.partial[blockIdx.x] = t;
   }
 }
 
-template <bool IN_BF, bool OUT_BF>
-static void launch_pair(const SpmmParams& p, const Csr& m, const int* rows, int nrows, int grid, cudaStream_t s) {
-  spmm_pair_kernel<IN_BF, OUT_BF><<<grid, 256, 0, s>>>(p, rows, rows ? m.nz_rowptr : nullptr, nrows);
+static void launch_pair(bool out_h, const SpmmParams& p, const Csr& m, const int* rows, int nrows, int grid,
+                        cudaStream_t s) {
+  const uint32_t* rp = rows ? m.nz_rowptr : nullptr;
+  if (out_h)
+    spmm_pair_kernel<true><<<grid, 256, 0, s>>>(p, rows, rp, nrows);
+  else
+    spmm_pair_kernel<false><<<grid, 256, 0, s>>>(p, rows, rp, nrows);
 }
 
-static bool point_c(Layout l) { return l == Layout::kPointC64 || l == Layout::kPointBF16; }
-
 static bool use_pair_kernel(const SpmmArgs& a) {
-  return point_c(a.in.layout) && point_c(a.out.layout) && (a.nCh % 2) == 0 && !a.normalize;
+  return a.in.layout == Layout::kPointC64 &&
+         (a.out.layout == Layout::kPointC64 || a.out.layout == Layout::kPointF16) && (a.nCh % 2) == 0 &&
+         !a.normalize;
 }
 
 static int rows_per_block(const SpmmArgs& a) {
@@ -377,6 +399,7 @@ int spmm(const SpmmArgs& a, cudaStream_t s) {
   p.normalize = a.normalize ? 1 : 0;
   p.sqn_w = a.sqn_row_weight;
   p.partial = a.partial;
+  p.absmax = a.absmax;
   MLG_CHECK(!a.nonempty_only || (m.nz_rows && use_pair_kernel(a)),
             "non-empty-row products need the row list and the coil-pair kernel");
   const long long nrows = spmm_rows(a);
@@ -393,35 +416,26 @@ int spmm(const SpmmArgs& a, cudaStream_t s) {
   float3* sc3 = reinterpret_cast<float3*>(scratch);
   using L = Layout;
   const L i = a.in.layout, o = a.out.layout;
+  MLG_CHECK(i != L::kPointF16, "scaled FP16 is an output layout only");
+  MLG_CHECK(o != L::kPointF16 || a.out.scale, "scaled FP16 output needs its scale");
   if (use_pair_kernel(a)) {
-    const bool ib = i == L::kPointBF16, ob = o == L::kPointBF16;
+    const bool oh = o == L::kPointF16;
     if (grid_short > 0) {
       const int* rl = a.nonempty_only ? m.nz_rows : nullptr;
       MLG_CHECK(!rl || m.nz_rowptr, "non-empty-row products need the row bounds");
-      if (ib && !ob)
-        launch_pair<true, false>(p, m, rl, (int)nrows, grid_short, s);
-      else if (!ib && ob)
-        launch_pair<false, true>(p, m, rl, (int)nrows, grid_short, s);
-      else if (ib && ob)
-        launch_pair<true, true>(p, m, rl, (int)nrows, grid_short, s);
-      else
-        launch_pair<false, false>(p, m, rl, (int)nrows, grid_short, s);
+      launch_pair(oh, p, m, rl, (int)nrows, grid_short, s);
       MLG_LAUNCHED();
     }
     // long rows (segment kernels) with the same element types
-    if (ib && !ob) return launch<L::kPointBF16, L::kPointC64, false>(p, m, sc3, 0, s);
-    if (!ib && ob) return launch<L::kPointC64, L::kPointBF16, false>(p, m, sc3, 0, s);
-    if (ib && ob) return launch<L::kPointBF16, L::kPointBF16, false>(p, m, sc3, 0, s);
+    if (oh) return launch<L::kPointC64, L::kPointF16, false>(p, m, sc3, 0, s);
     return launch<L::kPointC64, L::kPointC64, false>(p, m, sc3, 0, s);
   }
   if (i == L::kCoilC64 && o == L::kPointC64) return launch<L::kCoilC64, L::kPointC64, false>(p, m, sc3, grid_short, s);
   if (i == L::kPointC64 && o == L::kCoilC64) return launch<L::kPointC64, L::kCoilC64, true>(p, m, sc3, grid_short, s);
   if (i == L::kPointC64 && o == L::kPointC64)
     return launch<L::kPointC64, L::kPointC64, false>(p, m, sc3, grid_short, s);
-  if (i == L::kPointC64 && o == L::kPointBF16)
-    return launch<L::kPointC64, L::kPointBF16, false>(p, m, sc3, grid_short, s);
-  if (i == L::kPointBF16 && o == L::kPointC64)
-    return launch<L::kPointBF16, L::kPointC64, false>(p, m, sc3, grid_short, s);
+  if (i == L::kPointC64 && o == L::kPointF16)
+    return launch<L::kPointC64, L::kPointF16, false>(p, m, sc3, grid_short, s);
   if (i == L::kCoilSplit && o == L::kCoilSplit)
     return launch<L::kCoilSplit, L::kCoilSplit, true>(p, m, sc3, grid_short, s);
   if (i == L::kPointSplit && o == L::kPointSplit)

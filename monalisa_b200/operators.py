@@ -181,9 +181,9 @@ class NufftPlan:
 
     @precision.setter
     def precision(self, name: str):
-        """'fp32', 'mixed' (FP16 matrix values, BF16 k-space work vectors in
-        the CG-SENSE solver, FP32 sums, FP64 scalars) or 'fp16_values' (FP16
-        matrix values only)."""
+        """'fp32', 'mixed' (FP16 matrix values, the CG-SENSE solver's forward
+        product M p stored in scaled FP16, FP32 residual and sums, FP64 scalars) or
+        'fp16_values' (FP16 matrix values only)."""
         N.call("mlg_plan_set_precision", self._h, self.PRECISIONS.index(name))
 
     def autotune(self, reps: int = 3) -> dict:

@@ -284,6 +284,8 @@ def test_operators_3d_and_per_coil(N_u, n_u, nCh):
                                     l_size=M.l_size, l_jump=M.l_jump, l_nJump=M.l_nJump, N_u=N_u)
     y = mb.bmShanna(x, conv(G["Gu"]), KFC, n_u)
     assert rel(y, oracle.bmShanna(x, G["Gu"], KFC, n_u)) <= 1e-5
+    x1 = np.ascontiguousarray(x[:, 0])  # one image shared by the coils (the solvers' form)
+    assert rel(mb.bmShanna(x1, conv(G["Gu"]), KFC, n_u), oracle.bmShanna(x1, G["Gu"], KFC, n_u)) <= 1e-5
     yy = (rng.standard_normal(y.shape) + 1j * rng.standard_normal(y.shape)).astype(np.complex64)
     xn = mb.bmNakatsha(yy, conv(G["Gut"]), KFCc, True, n_u)
     assert rel(xn, oracle.bmNakatsha(yy, G["Gut"], KFCc, True, n_u)) <= 1e-5
