@@ -1,0 +1,58 @@
+"""Operator timing on a 3-D koosh-ball case of chosen size: builds Gu/Gut and
+a NUFFT plan, runs `reps` forward (Shanna) and adjoint (Nakatsha) operator
+applications, and prints the per-stage CUDA-event times of the plan's
+stage profiler (forward x/y/z line-FFT passes, Gu, Gut, inverse z/y/x).
+
+A small case keeps profiler captures short, e.g.
+
+    python -m monalisa_b200.opbench --n 64 --spokes 1024 --samples 128 --coils 16
+
+(64^3 image, 128^3 grid: the grid, 268 MB, and the pass buffers still exceed
+the 126 MB L2).  The headline workload is --n 128 --spokes 4096 --samples 256.
+"""
+import argparse
+
+import numpy as np
+
+STAGES = ["fwd_x", "fwd_y", "fwd_z", "gu", "gut", "inv_z", "inv_y", "inv_x"]
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
+    ap.add_argument("--n", type=int, default=64, help="image edge (grid edge 2n)")
+    ap.add_argument("--spokes", type=int, default=1024)
+    ap.add_argument("--samples", type=int, default=128, help="samples per spoke")
+    ap.add_argument("--coils", type=int, default=16)
+    ap.add_argument("--reps", type=int, default=3, help="forward + adjoint applications")
+    ap.add_argument("--adjoint", default="masked", choices=["masked", "fused", "full_grid"])
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "mixed", "fp16_values"])
+    args = ap.parse_args(argv)
+
+    import torch
+
+    import monalisa_b200 as mb
+    from monalisa_b200 import _native as N
+    from monalisa_b200 import traj
+
+    n, Ng = args.n, 2 * args.n
+    t = traj.bmTraj_fullRadial3_phyllotaxis_lineAssym2(args.samples, args.spokes, 1, Ng / args.samples)
+    ve = traj.bmVolumeElement_full_radial3(t)
+    Gu, Gut = mb.bmTraj2SparseMat(t, ve, [Ng] * 3, [1, 1, 1])
+    rec = mb.SensaRecon(Gu, Gut, traj.coil_maps([n] * 3, args.coils, 1), [n] * 3, precision=args.precision)
+    rec.plan.adjoint_mode = args.adjoint
+    x = torch.from_numpy(traj.ellipsoid_phantom([n] * 3, 5, 2)).cuda()
+    for _ in range(args.reps):
+        y = rec.plan.shanna(x)
+        rec.plan.nakatsha(y)
+    torch.cuda.synchronize()
+    ms = np.zeros(len(STAGES))
+    N.call("mlg_plan_profile", rec.plan.handle, max(1, args.reps), N.dptr(ms))
+    print(f"{n}^3 image, {Ng}^3 grid, {args.spokes}x{args.samples} samples, {args.coils} coils, "
+          f"adjoint {rec.plan.adjoint_mode}, precision {args.precision}, Gu nnz {Gu.nnz}")
+    for name, v in zip(STAGES, ms):
+        print(f"  {name:6s} {v:8.4f} ms")
+    rec.plan.close()
+
+
+if __name__ == "__main__":
+    main()
