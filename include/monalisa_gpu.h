@@ -220,6 +220,20 @@ int mlg_traj2sparsemat3(int imDim, int nPt, const double* t, const double* ve,
                         int nWin, const double* kernelParam, mlg_matrix_t* Gn,
                         mlg_matrix_t* Gu, mlg_matrix_t* Gut);
 
+/* GPU form of src/gridding123/m/bmImDeformField2SparseMat.m:14-146 (weights
+ * of bmImDeformField2sparseMat_ind_weight.m): the image-deformation matrices
+ * of a displacement field v [imDim, prod(N_u)] (column-major, pixel units;
+ * pixel p moves to its 1-based position + v(:, p)).  Each pixel's row holds
+ * the bump weights exp(-1/(1-d^2)) (d < 1) of the 2^imDim cells
+ * floor(t) + {0, 1}, periodic wrap, normalised to sum 1; a pixel moved
+ * outside [1, N_u] keeps an empty row unless torus_flag.  Gu [prod(N_u),
+ * prod(N_u)] (the Tu of bmTevaMorphosia_chain), Gut = Gu^T (Tut), Gn:
+ * weight * Dn per cell, rows normalised (needs Dn [prod(N_u)]).  Any output
+ * pointer may be NULL. */
+int mlg_deform2sparsemat(int imDim, const int* N_u, const double* v,
+                         const double* Dn, int torus_flag, mlg_matrix_t* Gn,
+                         mlg_matrix_t* Gu, mlg_matrix_t* Gut);
+
 /* ---- deapodisation ------------------------------------------------------ */
 
 /* src/fourier123/prep_function/bmK.m:6-156 for one coil: K [prod(N_u)]
@@ -394,6 +408,14 @@ int mlg_chain_create(int nFr, const mlg_plan_t* plans, mlg_chain_t* out);
 int mlg_chain_destroy(mlg_chain_t c);
 /* nFr, the total k-space rows sum(nPt_f) and the pixels per frame. */
 int mlg_chain_info(mlg_chain_t c, int* nFr, long long* rows, long long* pixels);
+/* Deformation fields of the temporal sparsifier (the Tu, Tut arguments of
+ * bmTevaMorphosia_chain.m, applied as bmImDeform / bmImDeformT with K = []):
+ * Tu[f], Tut[f] for f < nFr, each [pixels x pixels] (e.g. from
+ * mlg_deform2sparsemat) or NULL (identity for that frame); NULL arrays: no
+ * deformation.  F x_f = Tu_f x_f - x_{f-1}, F* z_f = (1/HX)(Tut_f (HZ z_f)
+ * - HZ z_{f+1}).  The matrices stay the caller's and must outlive the
+ * chain's runs. */
+int mlg_chain_set_deform(mlg_chain_t c, const mlg_matrix_t* Tu, const mlg_matrix_t* Tut);
 
 #define MLG_REGUL_NORMAL 0 /* delta, rho from linspace(first, last, nIter) */
 #define MLG_REGUL_ADAPT 1  /* delta = factor * regul / dafi, rho = factor * delta */

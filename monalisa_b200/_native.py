@@ -85,6 +85,9 @@ SIGNATURES = {
     "mlg_gridded_tail_dev": [c_int, P_i, P_i, P_f, c_int, c_int, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp],
     "mlg_steva_dev": [c_vp, c_vp, P_f, c_float, P_f, P_f, c_int, c_int, c_vp, c_vp, c_vp, c_int, P_d, c_vp],
     "mlg_steva": [c_vp, P_f, P_f, P_f, c_float, P_f, P_f, c_int, c_int, P_f, P_f, P_d],
+    "mlg_deform2sparsemat": [c_int, P_i, P_d, P_d, c_int, ctypes.POINTER(c_vp), ctypes.POINTER(c_vp),
+                             ctypes.POINTER(c_vp)],
+    "mlg_chain_set_deform": [c_vp, ctypes.POINTER(c_vp), ctypes.POINTER(c_vp)],
 }
 _RESTYPE = {"mlg_status_string": ctypes.c_char_p, "mlg_last_error": ctypes.c_char_p,
             "mlg_kernel_launch_count": c_ll}

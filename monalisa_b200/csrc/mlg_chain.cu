@@ -70,6 +70,13 @@ struct mlg_chain_s {
   const void* graph_key[4] = {nullptr, nullptr, nullptr, nullptr};
   std::vector<int> graph_modes;     // sparsifier and the frames' adjoint strategies it was captured with
   long long graph_kernels = 0;
+  // deformation fields of the temporal sparsifier (caller's matrices, one
+  // per frame, NULL = identity): F x_f = Tu_f x_f - x_{f-1}, F* z_f =
+  // (1/HX)(Tut_f (HZ z_f) - HZ z_{f+1})
+  std::vector<const mlg::Csr*> Tu, Tut;
+  bool deform = false;
+  float2 *Dx = nullptr, *Sz = nullptr;  // [nFr][nu]: deformed frames; HZ res_z
+  float* dscratch = nullptr;            // long-row segment scratch of those products
 };
 
 namespace mlg {
@@ -132,15 +139,26 @@ __global__ void tv_hy_kernel(const float* __restrict__ ve, long long n, float ve
     HY[i] = fminf(ve[i], ve_max);
 }
 
+// In the temporal-TV kernels xd is the deformed current frame (Tu_f x_f,
+// private_F :262-269 via bmImDeform), x itself without deformation fields.
+
 // z = F x, u = 0   (:75-81)
-__global__ void tv_init_zu_kernel(const float2* __restrict__ x, int nFr, long long nu, float2* __restrict__ z,
-                                  float2* __restrict__ u) {
+__global__ void tv_init_zu_kernel(const float2* __restrict__ x, const float2* __restrict__ xd, int nFr, long long nu,
+                                  float2* __restrict__ z, float2* __restrict__ u) {
   const long long n = nu * nFr;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     const long long f = i / nu, k = i - f * nu;
     const long long prev = ((f + nFr - 1) % nFr) * nu + k;
-    z[i] = csub(x[i], x[prev]);
+    z[i] = csub(xd[i], x[prev]);
     u[i] = make_float2(0.f, 0.f);
+  }
+}
+
+// Sz = HZ res_z (the input of Tut_f in private_dagF :282-289)
+__global__ void tv_scale_kernel(const float2* __restrict__ v, long long n, float HZ, float2* __restrict__ out) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const float2 a = v[i];
+    out[i] = make_float2(__fmul_rn(HZ, a.x), __fmul_rn(HZ, a.y));
   }
 }
 
@@ -160,29 +178,38 @@ __global__ void tv_params_kernel(const double* __restrict__ lists, int cap, int 
 }
 
 // res_z = (z - u) - F x   (:118)
-__global__ void tv_res_z_kernel(const float2* __restrict__ x, const float2* __restrict__ z,
-                                const float2* __restrict__ u, int nFr, long long nu, float2* __restrict__ res_z) {
+__global__ void tv_res_z_kernel(const float2* __restrict__ x, const float2* __restrict__ xd,
+                                const float2* __restrict__ z, const float2* __restrict__ u, int nFr, long long nu,
+                                float2* __restrict__ res_z) {
   const long long n = nu * nFr;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     const long long f = i / nu, k = i - f * nu;
     const long long prev = ((f + nFr - 1) % nFr) * nu + k;
-    res_z[i] = csub(csub(z[i], u[i]), csub(x[i], x[prev]));
+    res_z[i] = csub(csub(z[i], u[i]), csub(xd[i], x[prev]));
   }
 }
 
 // dA = dA + rho * (1/HX) (HZ res_z_f - HZ res_z_{f+1}), with dA holding
-// (1/HX) M*(HY res_y) from the operators (:119-121); partials of |dA|^2
-__global__ void tv_dA_kernel(float2* __restrict__ dA, const float2* __restrict__ res_z, int nFr, long long nu,
-                             float HZ, float invHX, const double* __restrict__ sc, double* __restrict__ partial) {
+// (1/HX) M*(HY res_y) from the operators (:119-121); partials of |dA|^2.
+// ts (optional): Tut_f (HZ res_z_f), taken in place of HZ res_z_f.
+__global__ void tv_dA_kernel(float2* __restrict__ dA, const float2* __restrict__ res_z,
+                             const float2* __restrict__ ts, int nFr, long long nu, float HZ, float invHX,
+                             const double* __restrict__ sc, double* __restrict__ partial) {
   const float rho = (float)sc[T_RHO];
   const long long n = nu * nFr;
   double acc = 0.0;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     const long long f = i / nu, k = i - f * nu;
     const long long next = ((f + 1) % nFr) * nu + k;
-    const float2 a = res_z[i], b = res_z[next];
-    float2 t = make_float2(__fsub_rn(__fmul_rn(HZ, a.x), __fmul_rn(HZ, b.x)),
-                           __fsub_rn(__fmul_rn(HZ, a.y), __fmul_rn(HZ, b.y)));
+    const float2 b = res_z[next];
+    float2 a;
+    if (ts) {
+      a = ts[i];
+    } else {
+      const float2 r = res_z[i];
+      a = make_float2(__fmul_rn(HZ, r.x), __fmul_rn(HZ, r.y));
+    }
+    float2 t = make_float2(__fsub_rn(a.x, __fmul_rn(HZ, b.x)), __fsub_rn(a.y, __fmul_rn(HZ, b.y)));
     t = make_float2(__fmul_rn(rho, __fmul_rn(invHX, t.x)), __fmul_rn(rho, __fmul_rn(invHX, t.y)));
     const float2 v = cadd(dA[i], t);
     dA[i] = v;
@@ -201,15 +228,15 @@ __global__ void tv_sq_init_kernel(const double* __restrict__ partial, int n, dou
   }
 }
 
-// Fp = F p with partials of |Fp|^2
-__global__ void tv_Fp_kernel(const float2* __restrict__ p, int nFr, long long nu, float2* __restrict__ Fp,
-                             double* __restrict__ partial) {
+// Fp = F p with partials of |Fp|^2 (pd: the deformed current frame of p)
+__global__ void tv_Fp_kernel(const float2* __restrict__ p, const float2* __restrict__ pd, int nFr, long long nu,
+                             float2* __restrict__ Fp, double* __restrict__ partial) {
   const long long n = nu * nFr;
   double acc = 0.0;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     const long long f = i / nu, k = i - f * nu;
     const long long prev = ((f + nFr - 1) % nFr) * nu + k;
-    const float2 v = csub(p[i], p[prev]);
+    const float2 v = csub(pd[i], p[prev]);
     Fp[i] = v;
     acc += nrm2(v);
   }
@@ -277,14 +304,14 @@ __device__ __forceinline__ float soft(float w, float s) {
 }
 
 // Fxu = u + F x; z = prox(Fxu, delta/rho); u = Fxu - z   (:167-169)
-__global__ void tv_zu_kernel(const float2* __restrict__ x, int nFr, long long nu, float2* __restrict__ z,
-                             float2* __restrict__ u, const double* __restrict__ sc) {
+__global__ void tv_zu_kernel(const float2* __restrict__ x, const float2* __restrict__ xd, int nFr, long long nu,
+                             float2* __restrict__ z, float2* __restrict__ u, const double* __restrict__ sc) {
   const float s = fabsf(__fdiv_rn((float)sc[T_DELTA], (float)sc[T_RHO]));
   const long long n = nu * nFr;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     const long long f = i / nu, k = i - f * nu;
     const long long prev = ((f + nFr - 1) % nFr) * nu + k;
-    const float2 w = cadd(u[i], csub(x[i], x[prev]));
+    const float2 w = cadd(u[i], csub(xd[i], x[prev]));
     const float2 zz = make_float2(soft(w.x, s), soft(w.y, s));
     z[i] = zz;
     u[i] = csub(w, zz);
@@ -304,14 +331,15 @@ __global__ void tv_residual_kernel(const float2* __restrict__ y, const float2* _
   if (threadIdx.x == 0) partial[blockIdx.x] = s;
 }
 
-// partials of sum |Re(x_{f-1} - x_f)| + |Im(x_{f-1} - x_f)|   (:219-222)
-__global__ void tv_regul_kernel(const float2* __restrict__ x, int nFr, long long nu, double* __restrict__ partial) {
+// partials of sum |Re(x_{f-1} - Tu_f x_f)| + |Im(...)|   (:219-222)
+__global__ void tv_regul_kernel(const float2* __restrict__ x, const float2* __restrict__ xd, int nFr, long long nu,
+                                double* __restrict__ partial) {
   const long long n = nu * nFr;
   double acc = 0.0;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     const long long f = i / nu, k = i - f * nu;
     const long long prev = ((f + nFr - 1) % nFr) * nu + k;
-    const float2 t = csub(x[prev], x[i]);
+    const float2 t = csub(x[prev], xd[i]);
     acc += (double)fabsf(t.x) + (double)fabsf(t.y);
   }
   const double s = block_sum(acc);
@@ -458,7 +486,8 @@ static void chain_free(mlg_chain_s* c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   if (c->graph) cudaGraphExecDestroy(c->graph);
   for (void* q : {(void*)c->p, (void*)c->dA, (void*)c->res_z, (void*)c->Fp, (void*)c->z, (void*)c->u,
-                  (void*)c->res_y, (void*)c->Mp, (void*)c->HY, (void*)c->partial, (void*)c->sc, (void*)c->lists})
+                  (void*)c->res_y, (void*)c->Mp, (void*)c->HY, (void*)c->partial, (void*)c->sc, (void*)c->lists,
+                  (void*)c->Dx, (void*)c->Sz, (void*)c->dscratch})
     cudaFree(q);
   if (c->ev_in) cudaEventDestroy(c->ev_in);
   if (c->ev_out) cudaEventDestroy(c->ev_out);
@@ -491,18 +520,59 @@ static int chain_adjoint(mlg_chain_s* c, const float2* res, float2* out, cudaStr
   return MLG_OK;
 }
 
+// dst_f = T_f src_f for every frame (bmImDeform / bmImDeformT with K = []:
+// the FP32 sparse product in stored order); dst_f = src_f where T_f is NULL
+static int chain_apply(mlg_chain_s* c, const std::vector<const Csr*>& T, const float2* src, float2* dst,
+                       cudaStream_t s) {
+  for (int f = 0; f < c->nFr; ++f) {
+    const float2* a = src + (size_t)f * c->nu;
+    float2* b = dst + (size_t)f * c->nu;
+    if (!T[f]) {
+      MLG_CUDA(cudaMemcpyAsync(b, a, sizeof(float2) * (size_t)c->nu, cudaMemcpyDeviceToDevice, s));
+      continue;
+    }
+    SpmmArgs g;
+    g.m = T[f];
+    g.nCh = 1;
+    g.in.layout = Layout::kPointC64;
+    g.in.a = const_cast<float2*>(a);
+    g.in.rows = c->nu;
+    g.out.layout = Layout::kPointC64;
+    g.out.a = b;
+    g.out.rows = c->nu;
+    g.seg_scratch = c->dscratch;
+    MLG_TRY(spmm(g, s));
+  }
+  return MLG_OK;
+}
+
+// the current frames of F applied to v: Tu_f v_f with deformation fields, v itself otherwise
+static const float2* chain_deformed(mlg_chain_s* c, const float2* v, cudaStream_t s, int* st) {
+  if (!c->deform || c->spatial) return v;
+  *st = chain_apply(c, c->Tu, v, c->Dx, s);
+  return c->Dx;
+}
+
 // dA = dagM res_y + rho dagF res_z and sqn_dagA_res (:119-123 / :156-159)
 static int chain_dagA(mlg_chain_s* c, bool first, cudaStream_t s) {
   const long long ni = c->nu * c->nFr;
   const double eps = 10.0 * (double)FLT_EPSILON;
   MLG_TRY(chain_adjoint(c, c->res_y, c->dA, s));
   const int g = grid1(ni);
-  if (c->spatial)
+  if (c->spatial) {
     st_dA_kernel<<<g, kT, 0, s>>>(c->dA, c->res_z, c->nu, c->geom, (float)c->HX, (float)(1.0 / c->HX), c->sc,
                                   c->partial);
-  else
-    tv_dA_kernel<<<g, kT, 0, s>>>(c->dA, c->res_z, c->nFr, c->nu, (float)c->HX, (float)(1.0 / c->HX), c->sc,
+  } else {
+    const float2* ts = nullptr;
+    if (c->deform) {  // Tut_f (HZ res_z_f)
+      tv_scale_kernel<<<grid1(ni), kT, 0, s>>>(c->res_z, ni, (float)c->HX, c->Sz);
+      MLG_LAUNCHED();
+      MLG_TRY(chain_apply(c, c->Tut, c->Sz, c->Dx, s));
+      ts = c->Dx;
+    }
+    tv_dA_kernel<<<g, kT, 0, s>>>(c->dA, c->res_z, ts, c->nFr, c->nu, (float)c->HX, (float)(1.0 / c->HX), c->sc,
                                   c->partial);
+  }
   MLG_LAUNCHED();
   if (first)
     tv_sq_init_kernel<<<1, kT, 0, s>>>(c->partial, g, c->HX, eps, c->sc);
@@ -518,10 +588,14 @@ static int chain_cg_half(mlg_chain_s* c, float2* x, cudaStream_t s) {
   int n_mp = 0;
   MLG_TRY(chain_forward(c, c->p, c->Mp, c->HY, &n_mp, s));
   const int g = grid1(ni);
-  if (c->spatial)
+  if (c->spatial) {
     st_Fp_kernel<<<g, kT, 0, s>>>(c->p, c->nu, c->geom, c->Fp, c->partial + n_mp);
-  else
-    tv_Fp_kernel<<<g, kT, 0, s>>>(c->p, c->nFr, c->nu, c->Fp, c->partial + n_mp);
+  } else {
+    int st = MLG_OK;
+    const float2* pd = chain_deformed(c, c->p, s, &st);
+    MLG_TRY(st);
+    tv_Fp_kernel<<<g, kT, 0, s>>>(c->p, pd, c->nFr, c->nu, c->Fp, c->partial + n_mp);
+  }
   MLG_LAUNCHED();
   tv_alpha_kernel<<<1, kT, 0, s>>>(c->partial, n_mp, g, c->HX, c->sc);
   MLG_LAUNCHED();
@@ -551,10 +625,14 @@ static int chain_monitor(mlg_chain_s* c, const float2* y, const float2* x, doubl
   const int gk = grid1(nk), gi = grid1(ni);
   tv_residual_kernel<<<gk, kT, 0, s>>>(y, c->Mp, nk, c->nCh, c->HY, c->res_y, c->partial);
   MLG_LAUNCHED();
-  if (c->spatial)
+  if (c->spatial) {
     st_regul_kernel<<<gi, kT, 0, s>>>(x, c->nu, c->geom, c->partial + gk);
-  else
-    tv_regul_kernel<<<gi, kT, 0, s>>>(x, c->nFr, c->nu, c->partial + gk);
+  } else {
+    int st = MLG_OK;
+    const float2* xd = chain_deformed(c, x, s, &st);
+    MLG_TRY(st);
+    tv_regul_kernel<<<gi, kT, 0, s>>>(x, xd, c->nFr, c->nu, c->partial + gk);
+  }
   MLG_LAUNCHED();
   tv_monitor_kernel<<<1, kT, 0, s>>>(c->partial, gk, gi, c->HX, c->sc, hist, c->spatial ? 2 : 3);
   MLG_LAUNCHED();
@@ -604,10 +682,14 @@ static int chain_run(mlg_chain_s* c, bool spatial, const float2* y, const float*
   tv_hy_kernel<<<grid1(c->rows), kT, 0, s>>>(ve, c->rows, ve_max, c->HY);
   MLG_LAUNCHED();
   if (init_zu) {
-    if (spatial)
+    if (spatial) {
       st_init_zu_kernel<<<grid1(ni), kT, 0, s>>>(x, c->nu, c->geom, z, u);
-    else
-      tv_init_zu_kernel<<<grid1(ni), kT, 0, s>>>(x, c->nFr, c->nu, z, u);
+    } else {
+      int st = MLG_OK;
+      const float2* xd = chain_deformed(c, x, s, &st);
+      MLG_TRY(st);
+      tv_init_zu_kernel<<<grid1(ni), kT, 0, s>>>(x, xd, c->nFr, c->nu, z, u);
+    }
     MLG_LAUNCHED();
   }
   MLG_CUDA(cudaMemsetAsync(c->sc, 0, sizeof(double) * T_COUNT, s));
@@ -645,10 +727,14 @@ static int chain_run(mlg_chain_s* c, bool spatial, const float2* y, const float*
     tv_params_kernel<<<1, 1, 0, s>>>(c->lists, c->lists_cap, adapt, c->sc);
     MLG_LAUNCHED();
     // L_Aube (:116-123): res_y is the kept monitoring residual
-    if (spatial)
+    if (spatial) {
       st_res_z_kernel<<<grid1(ni), kT, 0, s>>>(x, z, u, c->nu, c->geom, c->res_z);
-    else
-      tv_res_z_kernel<<<grid1(ni), kT, 0, s>>>(x, z, u, c->nFr, c->nu, c->res_z);
+    } else {
+      int st = MLG_OK;
+      const float2* xd = chain_deformed(c, x, s, &st);
+      MLG_TRY(st);
+      tv_res_z_kernel<<<grid1(ni), kT, 0, s>>>(x, xd, z, u, c->nFr, c->nu, c->res_z);
+    }
     MLG_LAUNCHED();
     MLG_TRY(chain_dagA(c, true, s));
     MLG_CUDA(cudaMemcpyAsync(c->p, c->dA, sizeof(float2) * (size_t)ni, cudaMemcpyDeviceToDevice, s));
@@ -658,10 +744,14 @@ static int chain_run(mlg_chain_s* c, bool spatial, const float2* y, const float*
       count_launch(c->graph_kernels);
     }
     if (nCGD > 0) MLG_TRY(chain_cg_half(c, x, s));  // the last step stops after x += a p (:148-150)
-    if (spatial)
+    if (spatial) {
       st_zu_kernel<<<grid1(ni), kT, 0, s>>>(x, c->nu, c->geom, z, u, c->sc);
-    else
-      tv_zu_kernel<<<grid1(ni), kT, 0, s>>>(x, c->nFr, c->nu, z, u, c->sc);
+    } else {
+      int st = MLG_OK;
+      const float2* xd = chain_deformed(c, x, s, &st);
+      MLG_TRY(st);
+      tv_zu_kernel<<<grid1(ni), kT, 0, s>>>(x, xd, c->nFr, c->nu, z, u, c->sc);
+    }
     MLG_LAUNCHED();
     MLG_TRY(chain_monitor(c, y, x, hist.p, s));
   }
@@ -733,7 +823,49 @@ int mlg_chain_create(int nFr, const mlg_plan_t* plans, mlg_chain_t* out) {
     chain_free(c);
     return fail(MLG_ERR_OOM, "chain: device allocation failed");
   }
+  c->Tu.assign(nFr, nullptr);
+  c->Tut.assign(nFr, nullptr);
   *out = c;
+  return MLG_OK;
+}
+
+int mlg_chain_set_deform(mlg_chain_t c, const mlg_matrix_t* Tu, const mlg_matrix_t* Tut) {
+  MLG_CHECK(c, "NULL chain");
+  MLG_CUDA(cudaSetDevice(c->device));
+  std::vector<const Csr*> tu(c->nFr, nullptr), tut(c->nFr, nullptr);
+  size_t scratch = 0;
+  for (int f = 0; f < c->nFr; ++f)
+    for (int k = 0; k < 2; ++k) {
+      const mlg_matrix_t m = k == 0 ? (Tu ? Tu[f] : nullptr) : (Tut ? Tut[f] : nullptr);
+      if (!m) continue;
+      MLG_CHECK(m->device == c->device, "deformation matrix of frame %d is on another device", f);
+      MLG_CHECK(m->csr.l_size == c->nu && m->csr.r_size == c->nu,
+                "deformation matrix of frame %d must be [%lld x %lld] (image pixels), got [%d x %d]", f, c->nu,
+                c->nu, m->csr.l_size, m->csr.r_size);
+      (k == 0 ? tu : tut)[f] = &m->csr;
+      scratch = std::max(scratch, spmm_scratch_floats(m->csr, 1));
+    }
+  MLG_CUDA(cudaStreamSynchronize(c->stream));
+  const bool any = std::any_of(tu.begin(), tu.end(), [](const Csr* m) { return m != nullptr; }) ||
+                   std::any_of(tut.begin(), tut.end(), [](const Csr* m) { return m != nullptr; });
+  const size_t bi = sizeof(float2) * (size_t)(c->nu * c->nFr);
+  if (any && !c->Dx) {
+    if (cudaMalloc(&c->Dx, bi) != cudaSuccess || cudaMalloc(&c->Sz, bi) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(MLG_ERR_OOM, "chain: deformation buffers");
+    }
+  }
+  cudaFree(c->dscratch);
+  c->dscratch = nullptr;
+  if (scratch > 0 && cudaMalloc(&c->dscratch, sizeof(float) * scratch) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(MLG_ERR_OOM, "chain: deformation scratch");
+  }
+  c->Tu = tu;
+  c->Tut = tut;
+  c->deform = any;
+  if (c->graph) cudaGraphExecDestroy(c->graph);  // captured with the previous fields
+  c->graph = nullptr;
   return MLG_OK;
 }
 

@@ -35,6 +35,13 @@ struct TrajGeom {
   double kp[3];
   double I0a;        // I0(alpha) for Kaiser-Bessel
   double Du;
+  // deformation-field matrices (bmImDeformField2sparseMat_ind_weight.m):
+  // the input is a displacement per pixel, the position pixel (1-based) +
+  // displacement, the window the 2^imDim cells floor(t) + {0, 1}, the weight
+  // the bump exp(-1/(1-d^2)) for d < 1; torus keeps displaced pixels that
+  // leave the image (wrapped) instead of emptying their rows
+  int deform = 0;
+  int torus = 0;
 };
 
 __device__ double bessel_i0_dev(double x) {
@@ -67,10 +74,19 @@ __global__ void traj_rows_kernel(TrajGeom g, const double* __restrict__ t, int n
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < nPt; p += gridDim.x * blockDim.x) {
     double tg[3], tf[3], tr[3];
     bool del = false;
+    int q = p;  // pixel coordinates (deformation fields), x fastest
     for (int d = 0; d < 3; ++d) {
       if (d < g.imDim) {
-        tg[d] = t[(long long)p * g.imDim + d] / g.dK[d] + g.shift[d];
-        del = del || !(tg[d] >= 1.0) || !(tg[d] <= (double)g.N[d]);  // bmTraj2SparseMat.m:117-126
+        if (g.deform) {
+          // bmImDeformField2sparseMat_ind_weight.m:36-60: t = ndgrid(1:N) + v,
+          // deleted when outside [1, N] unless torus
+          tg[d] = (double)(q % g.N[d] + 1) + t[(long long)p * g.imDim + d];
+          q /= g.N[d];
+          del = del || (!g.torus && (!(tg[d] >= 1.0) || !(tg[d] <= (double)g.N[d])));
+        } else {
+          tg[d] = t[(long long)p * g.imDim + d] / g.dK[d] + g.shift[d];
+          del = del || !(tg[d] >= 1.0) || !(tg[d] <= (double)g.N[d]);  // bmTraj2SparseMat.m:117-126
+        }
         tf[d] = floor(tg[d] + g.floor_shift);
         tr[d] = tg[d] - tf[d];
       } else {
@@ -101,7 +117,12 @@ __global__ void traj_rows_kernel(TrajGeom g, const double* __restrict__ t, int n
       }
       const double dist = sqrt(d2);
       double w;
-      if (g.kernel == MLG_KERNEL_GAUSS) {
+      if (g.deform) {
+        // bump function (ind_weight.m:97-99): exp(-1/(1-d^2)), infinities
+        // to 0, zero unless |d| < 1
+        w = exp(-1.0 / (1.0 - dist * dist));
+        if (isinf(w) || !(fabs(dist) < 1.0)) w = 0.0;
+      } else if (g.kernel == MLG_KERNEL_GAUSS) {
         const double z = dist / g.kp[0];
         w = exp(-0.5 * (z * z)) / (sqrt(2 * M_PI) * g.kp[0]);
       } else {
@@ -284,6 +305,40 @@ static int finish_csr(Csr& m, int* counts, cudaStream_t s) {
   return MLG_OK;
 }
 
+static int build_sparsemats(const TrajGeom& g, int nPt, const double* t_host, Csr* Gu, Csr* Gut, cudaStream_t s,
+                            const double* ve_host, Csr* Gn);
+
+// src/gridding123/m/bmImDeformField2SparseMat.m:14-146 with the weights of
+// bmImDeformField2sparseMat_ind_weight.m: one row per pixel (deleted pixels
+// keep empty rows), Gu/Gut row-normalised, Gn = rows of cells with values
+// w * Dn normalised per cell (Dn given per pixel; dK = 1 so Dn passes
+// through the volume-element scaling unchanged).
+int deform2sparsemat(int imDim, const int* N_u, const double* v_host, const double* dn_host, bool torus, Csr* Gu,
+                     Csr* Gut, Csr* Gn, cudaStream_t s) {
+  TrajGeom g;
+  g.imDim = imDim;
+  g.deform = 1;
+  g.torus = torus ? 1 : 0;
+  long long Nu = 1;
+  for (int d = 0; d < 3; ++d) {
+    g.N[d] = d < imDim ? N_u[d] : 1;
+    g.dK[d] = 1.0;
+    g.shift[d] = 0.0;
+    if (d < imDim) Nu *= g.N[d];
+  }
+  MLG_CHECK(Nu < (1LL << 31), "image too large");
+  g.floor_shift = 0.0;
+  g.nWin = 2;
+  g.nRange = 2;
+  g.lo = 0;
+  g.nNb = 1 << imDim;
+  g.kernel = -1;
+  for (int i = 0; i < 3; ++i) g.kp[i] = 0.0;
+  g.I0a = 1.0;
+  g.Du = 1.0;
+  return build_sparsemats(g, (int)Nu, v_host, Gu, Gut, s, dn_host, Gn);
+}
+
 int traj2sparsemat(int imDim, int nPt, const double* t_host, const int* N_u, const double* dK_u, int kernelType,
                    int nWin, const double* kp, Csr* Gu, Csr* Gut, cudaStream_t s, const double* ve_host = nullptr,
                    Csr* Gn = nullptr) {
@@ -319,7 +374,17 @@ int traj2sparsemat(int imDim, int nPt, const double* t_host, const int* N_u, con
   MLG_CHECK(g.nNb <= kMaxNb, "window of %d cells exceeds %d", g.nNb, kMaxNb);
   for (int i = 0; i < 3; ++i) g.kp[i] = (double)(float)kp[i];  // double(single(kernelParam))
   g.I0a = kernelType == MLG_KERNEL_KAISER ? bessel_i0_host(g.kp[1]) : 1.0;
+  return build_sparsemats(g, nPt, t_host, Gu, Gut, s, ve_host, Gn);
+}
 
+// Rows of every sample (or pixel), then the CSR outputs: Gu, its transpose
+// Gut, and Gn (rows = cells, values w * Dn with Dn = ve / prod(dK),
+// normalised per cell).
+static int build_sparsemats(const TrajGeom& g, int nPt, const double* t_host, Csr* Gu, Csr* Gut, cudaStream_t s,
+                            const double* ve_host, Csr* Gn) {
+  const int imDim = g.imDim;
+  long long Nu = 1;
+  for (int d = 0; d < imDim; ++d) Nu *= g.N[d];
   const long long cap = (long long)nPt * g.nNb;
   MLG_CHECK(cap < (1LL << 31), "nPt * nNb too large");
   DevBuf<double> dt;
@@ -494,4 +559,36 @@ extern "C" int mlg_traj2sparsemat(int imDim, int nPt, const double* t, const dou
   // Gu / Gut are row-normalised: the volume elements cancel (bmTraj2SparseMat.m:271-281)
   MLG_CHECK(Gu || Gut, "no output requested");
   return mlg_traj2sparsemat3(imDim, nPt, t, ve, N_u, dK_u, kernelType, nWin, kernelParam, nullptr, Gu, Gut);
+}
+
+extern "C" int mlg_deform2sparsemat(int imDim, const int* N_u, const double* v, const double* Dn, int torus_flag,
+                                    mlg_matrix_t* Gn, mlg_matrix_t* Gu, mlg_matrix_t* Gut) {
+  MLG_CHECK(imDim >= 1 && imDim <= 3 && N_u && v, "invalid argument");
+  MLG_CHECK(Gn || Gu || Gut, "no output requested");
+  MLG_CHECK(!Gn || Dn, "Gn needs Dn");
+  for (int d = 0; d < imDim; ++d) MLG_CHECK(N_u[d] >= 1, "invalid N_u");
+  MLG_TRY(mlg::ensure_device());
+  if (Gn) *Gn = nullptr;
+  if (Gu) *Gu = nullptr;
+  if (Gut) *Gut = nullptr;
+  mlg::Csr u, t, w;
+  const int st = mlg::deform2sparsemat(imDim, N_u, v, Dn, torus_flag != 0, Gu ? &u : nullptr, Gut ? &t : nullptr,
+                                       Gn ? &w : nullptr, nullptr);
+  if (st != MLG_OK) {
+    mlg::csr_free(u);
+    mlg::csr_free(t);
+    mlg::csr_free(w);
+    return st;
+  }
+  int dev = 0;
+  cudaGetDevice(&dev);
+  mlg_matrix_t* outs[3] = {Gn, Gu, Gut};
+  mlg::Csr* csrs[3] = {&w, &u, &t};
+  for (int i = 0; i < 3; ++i)
+    if (outs[i]) {
+      *outs[i] = new mlg_matrix_s();
+      (*outs[i])->csr = *csrs[i];
+      (*outs[i])->device = dev;
+    }
+  return MLG_OK;
 }

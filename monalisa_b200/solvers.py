@@ -124,6 +124,26 @@ class TevaMorphosiaChain:
     def handle(self):
         return self._h
 
+    def set_deform(self, Tu=None, Tut=None):
+        """Deformation fields of the temporal sparsifier: lists over frames
+        of [prod(n_u), prod(n_u)] matrices (DeviceMatrix, bmSparseMat or
+        None = identity), e.g. from bmImDeformField2SparseMat.  F x_f =
+        Tu_f x_f - x_{f-1}; the adjoint applies Tut_f.  The matrices are kept
+        alive by the chain."""
+        def handles(T):
+            if T is None or len(T) == 0:
+                return None, []
+            if len(T) != self.nFr:
+                raise ValueError(f"need one deformation matrix (or None) per frame ({self.nFr})")
+            mats = [None if m is None else (m.to_device() if isinstance(m, bmSparseMat) else m) for m in T]
+            arr = (ctypes.c_void_p * self.nFr)(*[None if m is None else m.handle.value for m in mats])
+            return arr, mats
+
+        tu, mu = handles(Tu)
+        tut, mut = handles(Tut)
+        N.call("mlg_chain_set_deform", self._h, tu, tut)
+        self._deform = mu + mut  # the chain reads them on every run
+
     @staticmethod
     def _pair(v):
         v = np.abs(np.ravel(np.asarray(v, np.float32)))
@@ -178,15 +198,15 @@ def bmTevaMorphosia_chain(x, z, u, y, ve, C, Gu, Gut, n_u, Tu, Tut, delta, rho, 
                           convCond=None, witnessInfo=None):
     """Temporal-TV ADMM (bmTevaMorphosia_chain.m).  x, y, ve, Gu, Gut are
     lists over frames; z, u must be empty (None / []) -- they start as F x
-    and 0 as in the reference (:75-81).  Tu / Tut (deformation fields) must
-    be empty.  Returns the frame images as n_u blocks (MATLAB order).
-    ``witnessInfo`` may be a list that receives (objective, dafi, regul) per
-    iteration (:172-178)."""
-    if (Tu is not None and len(Tu)) or (Tut is not None and len(Tut)):
-        raise NotImplementedError("deformation fields (Tu / Tut) are not supported")
+    and 0 as in the reference (:75-81).  Tu / Tut: empty, or lists over
+    frames of deformation matrices (None entries = identity), as from
+    bmImDeformField2SparseMat.  Returns the frame images as n_u blocks
+    (MATLAB order).  ``witnessInfo`` may be a list that receives (objective,
+    dafi, regul) per iteration (:172-178)."""
     if (z is not None and len(z)) or (u is not None and len(u)):
         raise NotImplementedError("z / u start values are taken from x (pass empty z and u)")
     r = TevaMorphosiaChain(Gu, Gut, C, n_u)
+    r.set_deform(Tu, Tut)
     nIter = _niter(convCond)
     hist = witnessInfo if isinstance(witnessInfo, list) else None
     n_u = tuple(int(v) for v in np.ravel(n_u))

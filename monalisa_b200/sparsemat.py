@@ -206,6 +206,41 @@ def bmTraj2SparseMat(t, v, N_u, dK_u, kernelType=None, nWin=None, kernelParam=No
     return (Gn, Gu, Gut) if nargout == 3 else (Gu, Gut)
 
 
+def bmImDeformField2SparseMat(v, N_u, Dn=None, torus_flag=False, nargout=2):
+    """GPU form of src/gridding123/m/bmImDeformField2SparseMat.m for one
+    displacement field v [imDim, prod(N_u)] (pixel units): device-resident
+    (Tu, Tut) (nargout 2), Gn (nargout 1, needs Dn) or (Gn, Tu, Tut)
+    (nargout 3).  Each pixel's row holds bump weights on the 2^imDim cells
+    around its displaced position, normalised to sum 1; pixels displaced
+    outside the image keep empty rows unless torus_flag."""
+    v = np.asarray(v, np.float64)
+    if v.ndim == 1:
+        v = v[None, :]
+    N_u = np.ascontiguousarray(np.ravel(N_u), np.int32)
+    imDim = N_u.size
+    v = v.reshape(imDim, -1, order="F")
+    if v.shape[1] != int(np.prod(N_u)):
+        raise ValueError("the deformation field must have as many vectors as the number of pixels in the image")
+    if nargout not in (1, 2, 3):
+        raise ValueError("nargout must be 1, 2 or 3")
+    want_n, want_u = nargout in (1, 3), nargout in (2, 3)
+    if want_n and Dn is None:
+        raise ValueError("Gn needs Dn")
+    vv = np.ascontiguousarray(v.T)  # column-major [imDim, nPt]
+    dn = np.ascontiguousarray(np.ravel(Dn), np.float64) if want_n else None
+    hn, hu, ht = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()
+    N.call("mlg_deform2sparsemat", imDim, N.iptr(N_u), N.dptr(vv), N.dptr(dn), int(bool(torus_flag)),
+           ctypes.byref(hn) if want_n else None, ctypes.byref(hu) if want_u else None,
+           ctypes.byref(ht) if want_u else None)
+    meta = dict(N_u=N_u.copy(), d_u=np.ones(imDim, np.float32), kernel_type="bump", nWin=2,
+                kernelParam=np.zeros(0, np.float32))
+    Gn = DeviceMatrix(hn, meta, False) if want_n else None
+    if nargout == 1:
+        return Gn
+    Tu, Tut = DeviceMatrix(hu, meta, False), DeviceMatrix(ht, meta, False)
+    return (Gn, Tu, Tut) if nargout == 3 else (Tu, Tut)
+
+
 def bmSparseMat_vec(G: bmSparseMat, v, layout: str = "column"):
     """bmSparseMat_vec (src/sparseMat/m/bmSparseMat_vec.m:11-243) for a
     cpp_prepared matrix, one block or multi-block (G.extra['nBlock'],

@@ -420,6 +420,77 @@ def traj2sparsemat(t, v, N_u, dK_u, kernelType=None, nWin=None, kernelParam=None
     return out
 
 
+def deform2sparsemat(v, N_u, Dn=None, torus_flag=False, want=("Gu", "Gut")):
+    """bmImDeformField2SparseMat.m:14-146 with the weights of
+    bmImDeformField2sparseMat_ind_weight.m:6-150 for one displacement field
+    v [imDim, prod(N_u)] (pixel units).  Returns a dict with the requested
+    'Gn', 'Gu', 'Gut' (cpp_prepared bmSparseMat, not squeezed)."""
+    v = np.asarray(v, np.float64)
+    if v.ndim == 1:
+        v = v[None, :]
+    imDim, nPt = v.shape
+    N_u = np.ravel(N_u).astype(np.float64)
+    Nu_tot = int(np.prod(N_u))
+    if nPt != Nu_tot:
+        raise ValueError("the deformation field must have as many vectors as pixels")
+    # t = ndgrid(1:N) + v, x fastest (ind_weight.m:30-51)
+    grids = np.meshgrid(*[np.arange(1, int(n) + 1, dtype=np.float64) for n in N_u[:imDim]], indexing="ij")
+    t = np.stack([g.ravel(order="F") for g in grids]) + v
+    deleteMask = np.zeros(nPt, bool)
+    for i in range(imDim):  # :56-67
+        deleteMask |= (t[i] < 1) | (t[i] > N_u[i])
+    c = np.stack([g.ravel(order="F") for g in np.meshgrid(*[np.arange(2.0)] * imDim, indexing="ij")])  # [imDim, nNb]
+    nNb = c.shape[1]
+    t_floor = np.floor(t)
+    t_rest = t - t_floor
+    d2 = np.zeros((nNb, nPt))
+    for i in range(imDim):
+        d2 = d2 + (t_rest[i][None, :] - c[i][:, None]) ** 2
+    d = np.sqrt(d2)
+    with np.errstate(divide="ignore", over="ignore"):
+        w = np.exp(-1.0 / (1.0 - d ** 2))  # bump function (:97-99)
+    w[np.isinf(w)] = 0.0
+    w = w * (np.abs(d) < 1)
+    lin = np.zeros((nNb, nPt))
+    stride = 1.0
+    for i in range(imDim):  # periodic wrap (:105-118)
+        ni = np.mod(t_floor[i][None, :] + c[i][:, None] - 1, N_u[i]) + 1
+        lin = lin + (ni - 1) * stride
+        stride *= N_u[i]
+    keep = np.ones(nPt, bool) if torus_flag else ~deleteMask  # :122-130
+    rows = np.repeat(np.arange(nPt)[keep], nNb)
+    cols = lin[:, keep].T.ravel().astype(np.int64)
+    ww = w[:, keep].T.ravel()
+    out = {}
+    bump = ("bump", 2, [])
+    if "Gn" in want:
+        if Dn is None:
+            raise ValueError("Gn needs Dn")
+        dn = np.asarray(Dn, np.float64).ravel()[keep].repeat(nNb)
+        A = sp.coo_matrix((ww * dn, (rows, cols)), shape=(nPt, Nu_tot)).tocsr().T.tocsr()
+        A.sum_duplicates()
+        A.eliminate_zeros()
+        s = np.asarray(A.sum(axis=1)).ravel()
+        inv = np.zeros_like(s)
+        inv[s != 0] = 1.0 / s[s != 0]
+        out["Gn"] = cpp_prepare(matlab_sparse_to_bm(sp.diags(inv) @ A, N_u, [1, 1, 1], *bump))
+    if "Gu" in want or "Gut" in want:
+        A = sp.coo_matrix((ww, (rows, cols)), shape=(nPt, Nu_tot)).tocsr()
+        A.sum_duplicates()
+        A.eliminate_zeros()
+        A.sort_indices()
+        row_of = np.repeat(np.arange(nPt), np.diff(A.indptr))
+        s = np.bincount(row_of, weights=A.data, minlength=nPt)
+        inv = np.zeros_like(s)
+        inv[s != 0] = 1.0 / s[s != 0]
+        A = sp.csr_matrix((A.data * np.repeat(inv, np.diff(A.indptr)), A.indices, A.indptr), shape=A.shape)
+        if "Gu" in want:
+            out["Gu"] = cpp_prepare(matlab_sparse_to_bm(A, N_u, [1, 1, 1], *bump))
+        if "Gut" in want:
+            out["Gut"] = cpp_prepare(matlab_sparse_to_bm(A.T.tocsr(), N_u, [1, 1, 1], *bump))
+    return out
+
+
 def gridder_n2u_weights(t, Dn, N_u, dK_u, kernelType=None, nWin=None, kernelParam=None):
     """The argument preparation of bmGridder_n2u.m:22-211: returns the kept
     sample mask, weights w [nNb*nPt] (single) and jump-coded cells nJump."""
@@ -907,13 +978,16 @@ def bmSteva(x, y, ve, C, Gu, Gut, n_u, delta, rho, nCGD, ve_max=None, nIter=1, s
 
 
 def bmTevaMorphosia_chain(x, y, ve, C, Gu, Gut, n_u, delta, rho, nCGD, ve_max, nIter, spmv=None,
-                          workers=None, history=None, regul_mode="normal"):
-    """bmTevaMorphosia_chain.m:6-291, Tu = Tut = [] (identity deformation),
-    z and u initialised as in :75-81.  x, y, ve, Gu, Gut are lists over
-    frames.  regul_mode 'normal' takes delta / rho from their lists (:104-106);
-    'adapt' sets delta = delta_list(c) * regul / dafi and rho = rho_list(c) *
-    delta from the latest monitoring (:107-109, private_adapt_delta_rho
-    :240-248), the first one taken on the initial x (:86)."""
+                          workers=None, history=None, regul_mode="normal", Tu=None, Tut=None):
+    """bmTevaMorphosia_chain.m:6-291, z and u initialised as in :75-81.  x, y,
+    ve, Gu, Gut are lists over frames.  regul_mode 'normal' takes delta / rho
+    from their lists (:104-106); 'adapt' sets delta = delta_list(c) * regul /
+    dafi and rho = rho_list(c) * delta from the latest monitoring (:107-109,
+    private_adapt_delta_rho :240-248), the first one taken on the initial x
+    (:86).  Tu, Tut: per-frame deformation matrices (None, or None entries:
+    identity); F x_i = Tu_i x_i - x_{i-1} (private_F :262-269, bmImDeform.m
+    with K = []), F* z_i = (1/HX)(Tut_i (HZ z_i) - HZ z_{i+1}) (private_dagF
+    :282-289, bmImDeformT.m)."""
     myEps = 10 * np.finfo(np.float32).eps
     nFr = len(y)
     nCh = y[0].shape[1]
@@ -928,12 +1002,19 @@ def bmTevaMorphosia_chain(x, y, ve, C, Gu, Gut, n_u, delta, rho, nCGD, ve_max, n
     KFC = bmKF(C, N_u, n_u, dK_u, nCh, Gu[0].kernel_type, Gu[0].nWin, Gu[0].kernelParam)
     KFC_conj = bmKF_conj(np.conj(C), N_u, n_u, dK_u, nCh, Gu[0].kernel_type, Gu[0].nWin, Gu[0].kernelParam)
     x = [np.asarray(xi, np.complex64).ravel()[:, None] for xi in x]
+    Tu = Tu if Tu is not None else [None] * nFr
+    Tut = Tut if Tut is not None else [None] * nFr
+    sm = spmv or _spmv()
+
+    def deform(T, v):  # bmImDeform / bmImDeformT with K = []: T v in FP32, or v
+        return v if T is None else np.asarray(sm(T, v), np.complex64).reshape(v.shape)
+
     Mop = lambda v: [bmShanna(v[i], Gu[i], KFC, n_u, spmv, workers) for i in range(nFr)]
-    Fop = lambda v: [(v[i] - v[(i - 1) % nFr]).astype(np.complex64) for i in range(nFr)]
+    Fop = lambda v: [(deform(Tu[i], v[i]) - v[(i - 1) % nFr]).astype(np.complex64) for i in range(nFr)]
     dagM = lambda r: [((1 / HX) * bmNakatsha((HY[i] * r[i]).astype(np.complex64), Gut[i], KFC_conj, True, n_u,
                                              spmv, workers)).astype(np.complex64) for i in range(nFr)]
-    dagF = lambda z: [((1 / HX) * (np.float32(HZ) * z[i] - np.float32(HZ) * z[(i + 1) % nFr])).astype(np.complex64)
-                      for i in range(nFr)]
+    dagF = lambda z: [((1 / HX) * (deform(Tut[i], (np.float32(HZ) * z[i]).astype(np.complex64))
+                                   - np.float32(HZ) * z[(i + 1) % nFr])).astype(np.complex64) for i in range(nFr)]
     sqn = lambda v, h: sum(_dot(v[i], v[i], h[i] if isinstance(h, list) else None) * (1 if isinstance(h, list) else h)
                            for i in range(nFr))
     z = Fop(x)
@@ -947,7 +1028,7 @@ def bmTevaMorphosia_chain(x, y, ve, C, Gu, Gut, n_u, delta, rho, nCGD, ve_max, n
         dafi = sum(_dot(yy - m, yy - m, HY[i]) for i, (yy, m) in enumerate(zip(y, Mop(x))))
         regul = 0.0
         for i in range(nFr):
-            tr = x[(i - 1) % nFr] - x[i]
+            tr = x[(i - 1) % nFr] - deform(Tu[i], x[i])
             regul += HZ * float(np.sum(np.abs(tr.real), dtype=np.float64) + np.sum(np.abs(tr.imag), dtype=np.float64))
         return dafi, regul
 
