@@ -224,6 +224,11 @@ struct SpmmArgs {
   // Optional: raised (atomicMax on the bits) to the largest |re| or |im| of
   // the values written, before any FP16 rounding (device, non-negative float)
   unsigned* absmax = nullptr;
+  // Contracted arithmetic for the coil-pair rows (operators inside plans):
+  // the row scale folded into the matrix value (m * HY_j) and fused
+  // multiply-adds.  Off (the default): separate round-to-nearest multiply and
+  // add in stored order, bit-identical to the reference's CPU products.
+  bool contract = false;
 };
 
 // Scratch floats spmm needs for the long-row segments of `m` at nCh coils.

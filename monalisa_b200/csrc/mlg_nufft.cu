@@ -213,6 +213,7 @@ int shanna_stage(mlg_plan_s* p, int stage, const float2* x, bool x_per_coil, flo
     a.out.layout = Layout::kPointC64;
   }
   a.half_values = p->precision != MLG_PRECISION_FP32;
+  a.contract = true;  // operator-internal product: fused multiply-adds
   a.out.a = y;
   a.out.rows = p->nPt;
   a.sqn_row_weight = sqn_w;
@@ -236,6 +237,7 @@ int nakatsha_stage(mlg_plan_s* p, int stage, const float2* y, const float* HY, f
     a.nCh = p->nCh;
     a.in.layout = Layout::kPointC64;  // the solver's residual stays FP32 in every precision
     a.half_values = p->precision != MLG_PRECISION_FP32;
+    a.contract = true;  // HY folded into the matrix values, fused multiply-adds
     a.in.a = const_cast<float2*>(y);
     a.in.rows = p->nPt;
     a.in_row_scale = HY;
