@@ -1,6 +1,8 @@
 // Error plumbing, device selection, stream-ordered allocation, CSR upload
 // from the jump format, and the deterministic FP64 reduction used by the
 // solvers.
+#include <cub/device/device_radix_sort.cuh>
+
 #include <cstdarg>
 #include <cstring>
 #include <mutex>
@@ -87,7 +89,8 @@ void csr_free(Csr& c) {
   cudaFree(c.long_seg0);
   cudaFree(c.nz_rows);
   cudaFree(c.nz_mask);
-  cudaFree(c.nz_rowptr);
+  cudaFree(c.ord_rows);
+  cudaFree(c.ord_bounds);
   cudaFree(c.val_h);
   c = Csr();
 }
@@ -120,12 +123,80 @@ __global__ void nz_rows_kernel(const uint32_t* __restrict__ mask, const int* __r
   }
 }
 
-// rp[i] = row_ptr[rows[i]] (i < n), rp[n] = row_ptr[l_size]: the entries of
-// the non-empty rows are contiguous and in row order
-__global__ void nz_rowptr_kernel(const uint32_t* __restrict__ row_ptr, const int* __restrict__ rows, int n, int l_size,
-                                 uint32_t* __restrict__ rp) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i <= n; i += gridDim.x * blockDim.x)
-    rp[i] = i < n ? row_ptr[rows[i]] : row_ptr[l_size];
+// brick key of row i (rows[i], or i): its cell (the row itself, or the
+// column of its first entry when by_first_col; empty rows sort last)
+__global__ void order_keys_kernel(const uint32_t* __restrict__ row_ptr, const int* __restrict__ col,
+                                  const int* __restrict__ rows, int n, int by_first_col, int N0, int N1, int nbx,
+                                  int nby, uint32_t* __restrict__ keys, int* __restrict__ vals) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int r = rows ? rows[i] : i;
+    vals[i] = r;
+    long long cell = r;
+    if (by_first_col) {
+      const uint32_t b = row_ptr[r];
+      if (b == row_ptr[r + 1]) {
+        keys[i] = 0xffffffffu;
+        continue;
+      }
+      cell = col[b];
+    }
+    const long long x = cell % N0, t = cell / N0, y = t % N1, z = t / N1;
+    const long long brick = (x >> 3) + nbx * ((y >> 3) + (long long)nby * (z >> 3));
+    keys[i] = (uint32_t)(brick * 512 + (x & 7) + 8 * ((y & 7) + 8 * (z & 7)));
+  }
+}
+
+__global__ void order_bounds_kernel(const uint32_t* __restrict__ row_ptr, const int* __restrict__ rows, int n,
+                                    uint2* __restrict__ bounds) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int r = rows[i];
+    bounds[i] = make_uint2(row_ptr[r], row_ptr[r + 1]);
+  }
+}
+
+int csr_build_order(Csr& c, const int* N, bool nonempty, cudaStream_t s) {
+  if (c.ord_rows) return MLG_OK;
+  MLG_CHECK(!nonempty || c.nz_rows, "ordered non-empty rows need the row list");
+  const int n = nonempty ? c.n_nonempty : c.l_size;
+  const int nbx = (N[0] + 7) / 8, nby = (N[1] + 7) / 8, nbz = (N[2] + 7) / 8;
+  if ((double)nbx * nby * nbz * 512.0 >= 4294967295.0) return MLG_OK;  // keys would not fit: keep row order
+  DevBuf<uint32_t> keys, keys_out;
+  DevBuf<int> vals;
+  MLG_TRY(keys.alloc((size_t)std::max(1, n), s));
+  MLG_TRY(keys_out.alloc((size_t)std::max(1, n), s));
+  MLG_TRY(vals.alloc((size_t)std::max(1, n), s));
+  const int g = std::max(1, std::min(4096, (n + 255) / 256));
+  order_keys_kernel<<<g, 256, 0, s>>>(c.row_ptr, c.col, nonempty ? c.nz_rows : nullptr, n, nonempty ? 0 : 1, N[0],
+                                      N[1], nbx, nby, keys.p, vals.p);
+  count_launch();
+  int* ord = nullptr;
+  uint2* bounds = nullptr;
+  MLG_CUDA(cudaMalloc(&ord, sizeof(int) * (size_t)std::max(1, n)));
+  if (cudaMalloc(&bounds, sizeof(uint2) * (size_t)std::max(1, n)) != cudaSuccess) {
+    cudaGetLastError();
+    cudaFree(ord);
+    return fail(MLG_ERR_OOM, "row order: device allocation failed");
+  }
+  size_t tb = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, tb, keys.p, keys_out.p, vals.p, ord, n);
+  DevBuf<char> tmp;
+  int st = tmp.alloc(std::max<size_t>(tb, 1), s);
+  if (st == MLG_OK && cub::DeviceRadixSort::SortPairs(tmp.p, tb, keys.p, keys_out.p, vals.p, ord, n, 0, 32, s) !=
+                          cudaSuccess)
+    st = fail(MLG_ERR_CUDA, "row order: sort failed");
+  if (st != MLG_OK) {
+    cudaFree(ord);
+    cudaFree(bounds);
+    return st;
+  }
+  order_bounds_kernel<<<g, 256, 0, s>>>(c.row_ptr, ord, n, bounds);
+  count_launch();
+  MLG_CUDA(cudaStreamSynchronize(s));
+  c.ord_rows = ord;
+  c.ord_bounds = bounds;
+  c.n_ord = n;
+  c.ord_nonempty = nonempty;
+  return MLG_OK;
 }
 
 int csr_build_nonempty(Csr& c, cudaStream_t s) {
@@ -153,10 +224,6 @@ int csr_build_nonempty(Csr& c, cudaStream_t s) {
   MLG_CUDA(cudaMemcpyAsync(off, h.data(), sizeof(int) * (nw + 1), cudaMemcpyHostToDevice, s));
   MLG_CUDA(cudaMalloc(&c.nz_rows, sizeof(int) * (size_t)std::max(1, run)));
   nz_rows_kernel<<<g, 256, 0, s>>>(c.nz_mask, off, nw, c.nz_rows);
-  count_launch();
-  MLG_CUDA(cudaMalloc(&c.nz_rowptr, sizeof(uint32_t) * (size_t)(run + 1)));
-  nz_rowptr_kernel<<<std::max(1, std::min(4096, (run + 256) / 256)), 256, 0, s>>>(c.row_ptr, c.nz_rows, run,
-                                                                                  c.l_size, c.nz_rowptr);
   count_launch();
   MLG_CUDA(cudaStreamSynchronize(s));
   cudaFree(cnt);

@@ -127,9 +127,14 @@ struct Csr {
   // csr_build_nonempty
   int* nz_rows = nullptr;
   uint32_t* nz_mask = nullptr;
-  // entry bounds of the non-empty rows: row nz_rows[i] holds entries
-  // [nz_rowptr[i], nz_rowptr[i + 1]) ([n_nonempty + 1])
-  uint32_t* nz_rowptr = nullptr;
+  // a processing order of the rows for the coil-pair products: row
+  // ord_rows[i] holds entries [ord_bounds[i].x, ord_bounds[i].y); the rows
+  // are the non-empty ones (ord_nonempty) or all rows, sorted so that
+  // consecutive rows touch a compact block of grid cells (csr_build_order)
+  int* ord_rows = nullptr;
+  uint2* ord_bounds = nullptr;
+  int n_ord = 0;
+  bool ord_nonempty = false;
   // FP16 copy of val for the mixed-precision solver (built on demand)
   __half* val_h = nullptr;
 };
@@ -141,6 +146,11 @@ void csr_free(Csr& c);
 int csr_build_segments(Csr& c, cudaStream_t s);
 // Builds nz_rows / nz_mask (idempotent).
 int csr_build_nonempty(Csr& c, cudaStream_t s);
+// Builds ord_rows / ord_bounds (idempotent): the non-empty rows (nonempty;
+// rows are cells of the grid N) or all rows (rows keyed by the cell of their
+// first entry; empty rows last), in order of 8 x 8 x 8 bricks of cells, x
+// fastest within a brick; ties keep row order.  Needs nz_rows for nonempty.
+int csr_build_order(Csr& c, const int* N, bool nonempty, cudaStream_t s);
 
 }  // namespace mlg
 

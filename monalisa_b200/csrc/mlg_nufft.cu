@@ -112,7 +112,8 @@ bool adjoint_mode_valid(const mlg_plan_s* p, int mode) {
   // the fused gather reads FP32 k-space and FP32 values inside the FFT pass:
   // FP32 plans only
   if (mode == kAdjFused) return p->imDim >= 2 && p->precision == MLG_PRECISION_FP32;
-  if (mode == kAdjMasked) return (p->nCh % 2) == 0 && p->Gut_s.nz_mask != nullptr;
+  if (mode == kAdjMasked)
+    return (p->nCh % 2) == 0 && p->Gut_s.nz_mask != nullptr && p->Gut_s.ord_rows != nullptr && p->Gut_s.ord_nonempty;
   return false;
 }
 
@@ -489,10 +490,13 @@ static int plan_create_impl(int imDim, const int* N_u, const int* n_u, int nCh, 
     }
   }
   cudaStream_t s = p->stream;
-  if (Gu && (st = csr_sign_copy(*Gu, false, imDim, p->N, sc, p->Gu_s, s)) != MLG_OK) return bail(st);
-  // occupancy tables live with the caller's matrix (built once, shared by the
+  // occupancy tables and the list of Gut's non-empty cells (in blocks of
+  // nearby cells) live with the caller's matrix (built once, shared by the
   // sign-folded copy)
+  if (Gu && (st = csr_sign_copy(*Gu, false, imDim, p->N, sc, p->Gu_s, s)) != MLG_OK) return bail(st);
   if (Gut && (nCh % 2) == 0 && (st = csr_build_nonempty(const_cast<Csr&>(*Gut), s)) != MLG_OK) return bail(st);
+  if (Gut && (nCh % 2) == 0 && (st = csr_build_order(const_cast<Csr&>(*Gut), p->N, true, s)) != MLG_OK)
+    return bail(st);
   if (Gut && (st = csr_sign_copy(*Gut, true, imDim, p->N, 1.0f, p->Gut_s, s)) != MLG_OK) return bail(st);
   if ((st = build_line_mask(p, s)) != MLG_OK) return bail(st);
   p->adjoint_mode = adjoint_mode_valid(p, kAdjMasked) ? kAdjMasked : (imDim >= 2 ? kAdjFused : kAdjFullGrid);

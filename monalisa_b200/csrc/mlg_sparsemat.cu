@@ -259,8 +259,9 @@ __global__ void __launch_bounds__(256) spmm_seg_combine_kernel(SpmmParams p, con
 // Point layout in and out, even nCh: a thread owns a (row, coil pair) output
 // and moves 16 bytes per load/store; the row's column/value stream is read
 // once per pair instead of once per coil.  `rows` (optional) lists the rows
-// to compute (the non-empty ones) and `rptr` their entry bounds (rows[i]
-// holds entries [rptr[i], rptr[i + 1])); other rows are left untouched.  Entries
+// to compute, in that order (the matrix's ord_rows: non-empty rows, or all
+// rows, in blocks of nearby cells), and `bounds` their entry ranges; other
+// rows are left untouched.  Entries
 // are summed in stored order with round-to-nearest multiply/add, or, with
 // CONTRACT (operators inside plans), with the row scale folded into the
 // matrix value and fused multiply-adds: 9 instead of 16 arithmetic and load
@@ -282,52 +283,55 @@ __device__ __forceinline__ void st_pair(void* base, long long i, float4 v, float
 
 template <bool OUT_H, bool CONTRACT>
 __global__ void __launch_bounds__(256, 6) spmm_pair_kernel(SpmmParams p, const int* __restrict__ rows,
-                                                        const uint32_t* __restrict__ rptr, int n_rows) {
+                                                        const uint2* __restrict__ bounds, int n_rows) {
   __shared__ double sh[32];
   const int P = p.nCh >> 1;
   const long long i0 = (long long)blockIdx.x * p.rows_per_block;
   const int nr = (int)min((long long)p.rows_per_block, (long long)n_rows - i0);
+  const int total = nr * P;
   const bool scale = p.in_row_scale != nullptr;
   const float so = OUT_H ? __ldg(p.out.scale) : 0.f;
   float amax = 0.f;
   double sq = 0.0;
-  for (int it = threadIdx.x; it < nr * P; it += blockDim.x) {
-    const int lr = it / P, pi = it - (it / P) * P;
-    long long r;
-    uint32_t b, e;
-    if (rows) {  // listed rows: bounds from rptr, independent of the row index load
+  // item -> row, coil pair and entry range (empty for rows the segment kernels own)
+  auto fetch = [&](int it, long long& r, int& pi, uint32_t& b, uint32_t& n) {
+    const int lr = it / P;
+    pi = it - lr * P;
+    uint32_t e;
+    if (rows) {  // listed rows: bounds loaded beside the row index, not after it
       r = __ldg(rows + i0 + lr);
-      b = __ldg(rptr + i0 + lr);
-      e = __ldg(rptr + i0 + lr + 1);
+      const uint2 be = __ldg(bounds + i0 + lr);
+      b = be.x;
+      e = be.y;
     } else {
       r = i0 + lr;
       b = __ldg(p.row_ptr + r);
       e = __ldg(p.row_ptr + r + 1);
     }
-    if (e - b > (uint32_t)kLongRow) continue;  // segment kernels own it
-    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-#pragma unroll 4
-    for (uint32_t k = b; k < e; ++k) {
-      const int j = __ldg(p.col + k);
-      float m = val_at(p, k);
-      float4 v = __ldg(reinterpret_cast<const float4*>(p.in.a) + (long long)j * P + pi);
-      if constexpr (CONTRACT) {
-        if (scale) m = __fmul_rn(m, __ldg(p.in_row_scale + j));
-        acc.x = __fmaf_rn(m, v.x, acc.x);
-        acc.y = __fmaf_rn(m, v.y, acc.y);
-        acc.z = __fmaf_rn(m, v.z, acc.z);
-        acc.w = __fmaf_rn(m, v.w, acc.w);
-      } else {
-        if (scale) {
-          const float h = __ldg(p.in_row_scale + j);
-          v = make_float4(__fmul_rn(h, v.x), __fmul_rn(h, v.y), __fmul_rn(h, v.z), __fmul_rn(h, v.w));
-        }
-        acc.x = __fadd_rn(acc.x, __fmul_rn(m, v.x));
-        acc.y = __fadd_rn(acc.y, __fmul_rn(m, v.y));
-        acc.z = __fadd_rn(acc.z, __fmul_rn(m, v.z));
-        acc.w = __fadd_rn(acc.w, __fmul_rn(m, v.w));
+    n = e - b;
+  };
+  auto entry = [&](uint32_t k, int pi, float4& acc) {
+    const int j = __ldg(p.col + k);
+    float m = val_at(p, k);
+    float4 v = __ldg(reinterpret_cast<const float4*>(p.in.a) + (long long)j * P + pi);
+    if constexpr (CONTRACT) {
+      if (scale) m = __fmul_rn(m, __ldg(p.in_row_scale + j));
+      acc.x = __fmaf_rn(m, v.x, acc.x);
+      acc.y = __fmaf_rn(m, v.y, acc.y);
+      acc.z = __fmaf_rn(m, v.z, acc.z);
+      acc.w = __fmaf_rn(m, v.w, acc.w);
+    } else {
+      if (scale) {
+        const float h = __ldg(p.in_row_scale + j);
+        v = make_float4(__fmul_rn(h, v.x), __fmul_rn(h, v.y), __fmul_rn(h, v.z), __fmul_rn(h, v.w));
       }
+      acc.x = __fadd_rn(acc.x, __fmul_rn(m, v.x));
+      acc.y = __fadd_rn(acc.y, __fmul_rn(m, v.y));
+      acc.z = __fadd_rn(acc.z, __fmul_rn(m, v.z));
+      acc.w = __fadd_rn(acc.w, __fmul_rn(m, v.w));
     }
+  };
+  auto finish_item = [&](long long r, int pi, float4 acc) {
     if (p.out_scale != 1.0f)
       acc = make_float4(__fmul_rn(acc.x, p.out_scale), __fmul_rn(acc.y, p.out_scale), __fmul_rn(acc.z, p.out_scale),
                         __fmul_rn(acc.w, p.out_scale));
@@ -337,6 +341,17 @@ __global__ void __launch_bounds__(256, 6) spmm_pair_kernel(SpmmParams p, const i
       const double w = p.sqn_w ? (double)__ldg(p.sqn_w + r) : 1.0;
       sq += w * ((double)acc.x * acc.x + (double)acc.y * acc.y + (double)acc.z * acc.z + (double)acc.w * acc.w);
     }
+  };
+  for (int it = threadIdx.x; it < total; it += blockDim.x) {
+    long long r;
+    int pi;
+    uint32_t b, n;
+    fetch(it, r, pi, b, n);
+    if (n > (uint32_t)kLongRow) continue;  // segment kernels own it
+    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll 4
+    for (uint32_t k = b; k < b + n; ++k) entry(k, pi, acc);
+    finish_item(r, pi, acc);
   }
   if (p.absmax) warp_absmax(p.absmax, amax);
   if (p.partial) {
@@ -345,9 +360,8 @@ __global__ void __launch_bounds__(256, 6) spmm_pair_kernel(SpmmParams p, const i
   }
 }
 
-static void launch_pair(bool out_h, bool contract, const SpmmParams& p, const Csr& m, const int* rows, int nrows,
+static void launch_pair(bool out_h, bool contract, const SpmmParams& p, const int* rows, const uint2* rp, int nrows,
                         int grid, cudaStream_t s) {
-  const uint32_t* rp = rows ? m.nz_rowptr : nullptr;
   if (contract) {
     if (out_h)
       spmm_pair_kernel<true, true><<<grid, 256, 0, s>>>(p, rows, rp, nrows);
@@ -418,8 +432,8 @@ int spmm(const SpmmArgs& a, cudaStream_t s) {
   p.sqn_w = a.sqn_row_weight;
   p.partial = a.partial;
   p.absmax = a.absmax;
-  MLG_CHECK(!a.nonempty_only || (m.nz_rows && use_pair_kernel(a)),
-            "non-empty-row products need the row list and the coil-pair kernel");
+  MLG_CHECK(!a.nonempty_only || (m.ord_rows && m.ord_nonempty && use_pair_kernel(a)),
+            "non-empty-row products need the ordered row list and the coil-pair kernel");
   const long long nrows = spmm_rows(a);
   const int grid_all = (int)((nrows + p.rows_per_block - 1) / p.rows_per_block);
   const int grid_short = a.long_only ? 0 : grid_all;
@@ -439,9 +453,11 @@ int spmm(const SpmmArgs& a, cudaStream_t s) {
   if (use_pair_kernel(a)) {
     const bool oh = o == L::kPointF16;
     if (grid_short > 0) {
-      const int* rl = a.nonempty_only ? m.nz_rows : nullptr;
-      MLG_CHECK(!rl || m.nz_rowptr, "non-empty-row products need the row bounds");
-      launch_pair(oh, a.contract, p, m, rl, (int)nrows, grid_short, s);
+      // the matrix's processing order when it covers the requested rows
+      const bool ordered = m.ord_rows && m.ord_nonempty == a.nonempty_only;
+      MLG_CHECK(ordered || !a.nonempty_only, "non-empty-row products need the ordered row list");
+      launch_pair(oh, a.contract, p, ordered ? m.ord_rows : nullptr, ordered ? m.ord_bounds : nullptr, (int)nrows,
+                  grid_short, s);
       MLG_LAUNCHED();
     }
     // long rows (segment kernels) with the same element types
