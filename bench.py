@@ -361,6 +361,12 @@ def run_gpu(args):
             p: _mixed(w, Gu, Gut, y, ve, x_fp32, ms / args.steps, plain, stream, p) for p in ("mixed", "fp16_values")}
         rec.plan.close()
         extra["c1_radial2d"] = _c1(stream)
+        from monalisa_b200.workloads import radial2d
+
+        extra["gridding_leight"] = {
+            "c2": _gridder(w, stream, "3D koosh 4096x256 samples, 16 coils -> 256^3 grid, Gauss nWin 3"),
+            "c1": _gridder(radial2d(), stream, "2D radial 256x512 samples, 1 coil -> 512^2 grid, nWin 3 "
+                                               "(inside L2)")}
         extra["c3_frame_bins"] = _c3(stream)
         if rank == 0:
             extra["c5_serving"] = _c5()
@@ -455,6 +461,45 @@ def _c1(stream):
     return {"workload": "2D golden-angle radial 256^2 image, 512^2 grid, 256x512 samples, 1 coil, KB nWin 3, "
                         "20 CG iterations from x = 0 (working set inside L2)",
             "recons_per_s": round(1000.0 / ms, 3), "ms_per_recon": round(ms, 3), "adjoint": adjoint}
+
+
+def _gridder(w, stream, label, reps=5):
+    """The leight adjoint gridder (bmGridder_n2u_leight, §8 row a1) on a
+    workload's samples: device buffers in and out (mlg_gridder_n2u_leight_dev),
+    CUDA-event time per call, achieved GB/s of the algorithmic bytes
+    nPt (4 d + 4) + nPt nCh 8 + prod(N_u) nCh 8 + prod(N_u) 4 (positions and
+    Dn, split complex samples, split complex grid, weight sums)."""
+    import torch
+
+    from monalisa_b200 import _native as N
+    from monalisa_b200.gridding import _leight_prepare
+
+    rng = np.random.default_rng(7)
+    data = (rng.standard_normal((w.nCh, w.t.shape[1])) + 1j * rng.standard_normal((w.nCh, w.t.shape[1]))).astype(
+        np.complex64)
+    aR, aI, tx, Dn, nCh, nPt, Ns = _leight_prepare(data, w.t, w.ve, w.N_u, w.dK_u)
+    d = len(w.N_u)
+    up = lambda a: torch.from_numpy(a).cuda() if a is not None else None
+    dA, dI, dD = up(aR), up(aI), up(Dn)
+    dT = [up(v) for v in tx]
+    nu = int(np.prod(Ns))
+    bR = torch.empty((nu, nCh), dtype=torch.float32, device="cuda")
+    bI = torch.empty_like(bR)
+    kp = np.ravel(w.kernelParam).astype(np.float64)
+
+    def call():
+        N.call("mlg_gridder_n2u_leight_dev", d, N.tptr(dA), N.tptr(dI), N.tptr(dT[0]), N.tptr(dT[1]), N.tptr(dT[2]),
+               N.tptr(dD), nCh, nPt, Ns[0], Ns[1], Ns[2], int(w.nWin), float(kp[0]), float(kp[1]), N.tptr(bR),
+               N.tptr(bI), N.stream_ptr())
+
+    for _ in range(3):
+        call()
+    ms = _event_ms(call, reps, stream)
+    B = nPt * (4 * d + 4) + nPt * nCh * 8 + nu * nCh * 8 + nu * 4
+    peak, kind = _peaks()
+    gbs = B / (ms * 1e-3) / 1e9
+    return {"workload": label, "ms": round(ms, 4), "algorithmic_bytes": int(B), "GBps": round(gbs, 1),
+            "frac": round(gbs / peak, 4), "peak": peak, "peak_kind": kind}
 
 
 def _c3(stream):

@@ -63,8 +63,13 @@ int leight_geometry(int imDim, int nCh, const int* N, int nWin, float sigma, Lei
   // tile shape: start large, halve the largest extent until a tile's
   // accumulators fit the shared-memory budget
   const int G = 2 * nCh + 1;
+  g.gather = nCh == 8 || nCh == 12 || nCh == 16;
   int T[3];
-  if (imDim == 1) { T[0] = 4096; T[1] = 1; T[2] = 1; }
+  if (g.gather) {  // 512 cells: two per thread of a 256-thread CTA
+    if (imDim == 1) { T[0] = 512; T[1] = 1; T[2] = 1; }
+    else if (imDim == 2) { T[0] = 32; T[1] = 16; T[2] = 1; }
+    else { T[0] = 8; T[1] = 8; T[2] = 8; }
+  } else if (imDim == 1) { T[0] = 4096; T[1] = 1; T[2] = 1; }
   else if (imDim == 2) { T[0] = 64; T[1] = 32; T[2] = 1; }
   else { T[0] = 16; T[1] = 8; T[2] = 8; }
   for (int d = 0; d < 3; ++d) T[d] = std::min(T[d], g.N[d]);
@@ -150,26 +155,35 @@ __global__ void leight_fill_kernel(LeightGeom g, LeightInputs in, int nPt, const
 }
 
 // chunks per tile (>= 1 so that empty tiles are still written) and partial
-// slots (only tiles split over several chunks need them)
+// slots (only tiles split over several chunks need them; those tiles are
+// listed in split, in no particular order, for the combine kernel)
 __global__ void leight_chunk_count_kernel(long long ntiles, const int* __restrict__ count, int* __restrict__ nchunk,
-                                          int* __restrict__ nslot) {
+                                          int* __restrict__ nslot, int* __restrict__ split, int* __restrict__ nsplit) {
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < ntiles; t += (long long)gridDim.x * blockDim.x) {
     const int c = max(1, (count[t] + kChunkPairs - 1) / kChunkPairs);
     nchunk[t] = c;
     nslot[t] = c > 1 ? c : 0;
+    if (c > 1) split[atomicAdd(nsplit, 1)] = (int)t;
   }
 }
 
+// Chunk list: the chunks of split tiles first, at their slot index (the
+// longest-running CTAs start first), then the single-chunk tiles in no
+// particular order.  chunk = (tile, first pair, end pair, slot or -1).
 __global__ void leight_chunk_build_kernel(long long ntiles, const int* __restrict__ count,
                                           const int* __restrict__ offset, const int* __restrict__ nchunk,
-                                          const int* __restrict__ chunk_off, const int* __restrict__ slot_off,
+                                          const int* __restrict__ slot_off, int nslots, int* __restrict__ nsingle,
                                           int4* __restrict__ chunks) {
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < ntiles; t += (long long)gridDim.x * blockDim.x) {
     const int n = nchunk[t];
+    if (n == 1) {
+      chunks[nslots + atomicAdd(nsingle, 1)] = make_int4((int)t, offset[t], offset[t] + count[t], -1);
+      continue;
+    }
     for (int i = 0; i < n; ++i) {
       const int b = offset[t] + i * kChunkPairs;
       const int e = min(b + kChunkPairs, offset[t] + count[t]);
-      chunks[chunk_off[t] + i] = make_int4((int)t, b, e, n > 1 ? slot_off[t] + i : -1);
+      chunks[slot_off[t] + i] = make_int4((int)t, b, e, slot_off[t] + i);
     }
   }
 }
@@ -181,17 +195,28 @@ __device__ __forceinline__ void tile_origin(const LeightGeom& g, long long t, in
   o[2] = (int)(q / g.nt[1]) * g.T[2];
 }
 
-// Normalises and stores one cell's channels (acc = [norm, re0, im0, ...]).
-__device__ __forceinline__ void store_cell(const LeightGeom& g, const LeightOutput& out, long long cell,
-                                           const float* acc, int c) {
-  float s = acc[0];
-  if (s < 1e-5f) s = 1.0f;  // bmGridder_n2u_leight3_mex.cpp:341-344
-  const float re = __fdiv_rn(acc[1 + 2 * c], s), im = __fdiv_rn(acc[2 + 2 * c], s);
-  if (out.layout == Layout::kPointSplit) {
-    out.re[cell * g.nCh + c] = re;
-    out.im[cell * g.nCh + c] = im;
-  } else {  // kCoilC64
-    out.c64[(long long)c * g.Nu_tot + cell] = make_float2(re * out.scale, im * out.scale);
+// Normalises and stores a tile's accumulators (sm [tile_cells][G], acc =
+// [norm, re0, im0, ...]): one (cell, coil) per thread and step.
+__device__ __forceinline__ void store_tile(const LeightGeom& g, const LeightOutput& out, const float* sm,
+                                          const int org[3]) {
+  const int G = 2 * g.nCh + 1;
+  const int ncell_items = g.tile_cells * g.nCh;
+  for (int i = threadIdx.x; i < ncell_items; i += blockDim.x) {
+    const int c = i % g.nCh, lc = i / g.nCh;
+    const int lx = lc % g.T[0], ly = (lc / g.T[0]) % g.T[1], lz = lc / (g.T[0] * g.T[1]);
+    const int x = org[0] + lx, y = org[1] + ly, z = org[2] + lz;
+    if (x >= g.N[0] || y >= g.N[1] || z >= g.N[2]) continue;
+    const long long cell = x + (long long)g.N[0] * (y + (long long)g.N[1] * z);
+    const float* acc = sm + (size_t)lc * G;
+    float s = acc[0];
+    if (s < 1e-5f) s = 1.0f;  // bmGridder_n2u_leight3_mex.cpp:341-344
+    const float re = __fdiv_rn(acc[1 + 2 * c], s), im = __fdiv_rn(acc[2 + 2 * c], s);
+    if (out.layout == Layout::kPointSplit) {
+      out.re[cell * g.nCh + c] = re;
+      out.im[cell * g.nCh + c] = im;
+    } else {  // kCoilC64
+      out.c64[(long long)c * g.Nu_tot + cell] = make_float2(re * out.scale, im * out.scale);
+    }
   }
 }
 
@@ -263,23 +288,252 @@ __global__ void __launch_bounds__(kGridThreads) leight_accumulate_kernel(LeightG
     for (int i = threadIdx.x; i < g.tile_cells * G; i += blockDim.x) dst[i] = sm[i];
     return;
   }
-  const int ncell_items = g.tile_cells * g.nCh;
-  for (int i = threadIdx.x; i < ncell_items; i += blockDim.x) {
-    const int c = i % g.nCh, lc = i / g.nCh;
+  store_tile(g, out, sm, org);
+}
+
+// The same accumulation with a warp per sample, for many channels (G = 2 nCh
+// + 1 >= 17) and windows of at most 32 cells: lane k < W forms window cell
+// k's weight and tile-local cell once; every lane owns accumulator channels
+// lane, lane + 32, ... (norm, re0, im0, re1, ...) and loads its values of the
+// sample once; a loop over the window broadcasts (cell, weight) and each
+// lane adds its channel -- one shared-memory atomic per lane and cell, no
+// bank conflicts, instead of a coil loop per window cell.  Same values as
+// leight_accumulate_kernel; only the (already unordered) atomic order
+// differs.
+constexpr int kWarpMaxK = 3;  // channel chunks of 32: G <= 96
+
+__global__ void __launch_bounds__(kGridThreads) leight_accumulate_warp_kernel(LeightGeom g, LeightInputs in,
+                                                                              const int* __restrict__ pairs,
+                                                                              const int4* __restrict__ chunks,
+                                                                              float* __restrict__ partial,
+                                                                              LeightOutput out) {
+  extern __shared__ float sm[];
+  const int G = 2 * g.nCh + 1;
+  const int4 ch = chunks[blockIdx.x];
+  const long long tile = ch.x;
+  int org[3];
+  tile_origin(g, tile, org);
+  for (int i = threadIdx.x; i < g.tile_cells * G; i += blockDim.x) sm[i] = 0.f;
+  __syncthreads();
+
+  int W = g.nWin;
+  if (g.imDim > 1) W *= g.nWin;
+  if (g.imDim > 2) W *= g.nWin;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int nk = (G + 31) / 32;
+  for (int q = ch.y + warp; q < ch.z; q += nwarps) {
+    const int s = __ldg(pairs + q);
+    float r[3];
+    int lo[3];
+    sample_window(g, in, s, r, lo);
+    // lane k < W: weight and tile-local cell (-1: outside the tile or grid)
+    float wk = 0.f;
+    int cellk = -1;
+    if (lane < W) {
+      const int iw[3] = {lane % g.nWin, (lane / g.nWin) % g.nWin, lane / (g.nWin * g.nWin)};
+      int cl[3];
+      bool ok = true;
+      float d2 = 0.f;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        if (d < g.imDim) {
+          const int n = lo[d] + iw[d];
+          cl[d] = n - org[d];
+          ok = ok && n >= 0 && n < g.N[d] && cl[d] >= 0 && cl[d] < g.T[d];
+          const float u = (float)(iw[d] - g.half);
+          const float dd = r[d] - u;
+          d2 = d == 0 ? __fmul_rn(dd, dd) : __fadd_rn(d2, __fmul_rn(dd, dd));
+        } else {
+          cl[d] = 0;
+        }
+      }
+      if (ok) {
+        wk = __fmul_rn(__fmul_rn(g.g1, expf(__fmul_rn(g.g2, d2))), __ldg(in.Dn + s));
+        cellk = cl[0] + g.T[0] * (cl[1] + g.T[1] * cl[2]);
+      }
+    }
+    // this lane's channel values of the sample (channel 0 is the norm)
+    float a[kWarpMaxK];
+    const long long base = (long long)s * g.nCh;
+#pragma unroll
+    for (int j = 0; j < kWarpMaxK; ++j) {
+      const int chn = lane + 32 * j;
+      float v = 0.f;
+      if (j < nk && chn >= 1 && chn < G) {
+        const int c = (chn - 1) >> 1;
+        const bool imag = (chn - 1) & 1;
+        if (in.layout == Layout::kPointSplit) {
+          v = __ldg((imag ? in.im : in.re) + base + c);
+        } else {
+          const float2 z = __ldg(in.c64 + base + c);
+          v = imag ? z.y : z.x;
+        }
+      }
+      a[j] = v;
+    }
+    for (int k = 0; k < W; ++k) {
+      const int cell = __shfl_sync(0xffffffffu, cellk, k);
+      const float w = __shfl_sync(0xffffffffu, wk, k);
+      if (cell < 0) continue;  // uniform in the warp
+      float* acc = sm + cell * G;
+#pragma unroll
+      for (int j = 0; j < kWarpMaxK; ++j) {
+        const int chn = lane + 32 * j;
+        if (j < nk && chn < G) atomicAdd(acc + chn, chn == 0 ? w : __fmul_rn(w, a[j]));
+      }
+    }
+  }
+  __syncthreads();
+
+  if (ch.w >= 0) {  // partial tile of a split bin: raw accumulators to scratch
+    float* dst = partial + (long long)ch.w * g.tile_cells * G;
+    for (int i = threadIdx.x; i < g.tile_cells * G; i += blockDim.x) dst[i] = sm[i];
+    return;
+  }
+  store_tile(g, out, sm, org);
+}
+
+// Register-accumulating form for NCH = 8, 12, 16 coils (tiles of at most
+// 512 cells): thread t owns tile cells t and t + 256 with their 2 NCH + 1
+// accumulators in registers.  The chunk's samples pass through shared
+// memory in batches of kBatch (window corner and offsets, Dn, the NCH
+// complex values); every thread tests its cells against each sample's
+// window and accumulates the cells it covers -- no atomics, and per cell
+// the samples are summed in list order.  Weights as in
+// leight_accumulate_kernel.
+constexpr int kBatch = 128;
+
+template <int NCH>
+__global__ void __launch_bounds__(kGridThreads, 2) leight_gather_kernel(LeightGeom g, LeightInputs in,
+                                                                        const int* __restrict__ pairs,
+                                                                        const int4* __restrict__ chunks,
+                                                                        float* __restrict__ partial,
+                                                                        LeightOutput out) {
+  constexpr int G = 2 * NCH + 1, CPT = 2;
+  __shared__ int s_lo[3][kBatch];
+  __shared__ float s_r[3][kBatch];
+  __shared__ float s_dn[kBatch];
+  __shared__ int s_s[kBatch];
+  __shared__ __align__(16) float s_a[kBatch][2 * NCH];
+  const int4 ch = chunks[blockIdx.x];
+  int org[3];
+  tile_origin(g, ch.x, org);
+  int cx[CPT], cy[CPT], cz[CPT], lcs[CPT];
+  bool cin[CPT];
+#pragma unroll
+  for (int k = 0; k < CPT; ++k) {
+    const int lc = threadIdx.x + k * kGridThreads;
+    lcs[k] = lc;
     const int lx = lc % g.T[0], ly = (lc / g.T[0]) % g.T[1], lz = lc / (g.T[0] * g.T[1]);
-    const int x = org[0] + lx, y = org[1] + ly, z = org[2] + lz;
-    if (x >= g.N[0] || y >= g.N[1] || z >= g.N[2]) continue;
-    const long long cell = x + (long long)g.N[0] * (y + (long long)g.N[1] * z);
-    store_cell(g, out, cell, sm + lc * G, c);
+    cx[k] = org[0] + lx;
+    cy[k] = org[1] + ly;
+    cz[k] = org[2] + lz;
+    cin[k] = lc < g.tile_cells && cx[k] < g.N[0] && cy[k] < g.N[1] && cz[k] < g.N[2];
+  }
+  float acc[CPT][G];
+#pragma unroll
+  for (int k = 0; k < CPT; ++k)
+#pragma unroll
+    for (int q = 0; q < G; ++q) acc[k][q] = 0.f;
+
+  const unsigned nW = (unsigned)g.nWin;
+  for (int b0 = ch.y; b0 < ch.z; b0 += kBatch) {
+    const int nb = min(kBatch, ch.z - b0);
+    __syncthreads();  // the previous batch is consumed
+    if ((int)threadIdx.x < nb) {
+      const int s = __ldg(pairs + b0 + threadIdx.x);
+      float r[3];
+      int lo[3];
+      const bool hit = sample_window(g, in, s, r, lo);
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        s_lo[d][threadIdx.x] = hit ? lo[d] : -(1 << 29);  // a missed window covers no cell
+        s_r[d][threadIdx.x] = r[d];
+      }
+      s_dn[threadIdx.x] = __ldg(in.Dn + s);
+      s_s[threadIdx.x] = s;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < nb * NCH; i += kGridThreads) {
+      const int j = i / NCH, c = i - j * NCH;
+      const long long e = (long long)s_s[j] * NCH + c;
+      float2 v;
+      if (in.layout == Layout::kPointSplit)
+        v = make_float2(__ldg(in.re + e), __ldg(in.im + e));
+      else
+        v = __ldg(in.c64 + e);
+      s_a[j][2 * c] = v.x;
+      s_a[j][2 * c + 1] = v.y;
+    }
+    __syncthreads();
+    for (int j = 0; j < nb; ++j) {
+      const int l0 = s_lo[0][j], l1 = s_lo[1][j], l2 = s_lo[2][j];
+#pragma unroll
+      for (int k = 0; k < CPT; ++k) {
+        if (!cin[k]) continue;
+        const int i0 = cx[k] - l0, i1 = cy[k] - l1, i2 = cz[k] - l2;
+        if ((unsigned)i0 >= nW) continue;
+        if (g.imDim > 1 && (unsigned)i1 >= nW) continue;
+        if (g.imDim > 2 && (unsigned)i2 >= nW) continue;
+        const float dd0 = s_r[0][j] - (float)(i0 - g.half);
+        float d2 = __fmul_rn(dd0, dd0);
+        if (g.imDim > 1) {
+          const float dd1 = s_r[1][j] - (float)(i1 - g.half);
+          d2 = __fadd_rn(d2, __fmul_rn(dd1, dd1));
+        }
+        if (g.imDim > 2) {
+          const float dd2 = s_r[2][j] - (float)(i2 - g.half);
+          d2 = __fadd_rn(d2, __fmul_rn(dd2, dd2));
+        }
+        const float w = __fmul_rn(__fmul_rn(g.g1, expf(__fmul_rn(g.g2, d2))), s_dn[j]);
+        acc[k][0] = __fadd_rn(acc[k][0], w);
+        const float4* a4 = reinterpret_cast<const float4*>(s_a[j]);
+#pragma unroll
+        for (int q = 0; q < NCH / 2; ++q) {  // fused multiply-adds: the order of the sums differs anyway
+          const float4 a = a4[q];
+          acc[k][1 + 4 * q] = __fmaf_rn(w, a.x, acc[k][1 + 4 * q]);
+          acc[k][2 + 4 * q] = __fmaf_rn(w, a.y, acc[k][2 + 4 * q]);
+          acc[k][3 + 4 * q] = __fmaf_rn(w, a.z, acc[k][3 + 4 * q]);
+          acc[k][4 + 4 * q] = __fmaf_rn(w, a.w, acc[k][4 + 4 * q]);
+        }
+      }
+    }
+  }
+
+#pragma unroll
+  for (int k = 0; k < CPT; ++k) {
+    if (lcs[k] >= g.tile_cells) continue;
+    if (ch.w >= 0) {  // partial tile of a split bin: raw accumulators to scratch
+      float* dst = partial + ((long long)ch.w * g.tile_cells + lcs[k]) * G;
+#pragma unroll
+      for (int q = 0; q < G; ++q) dst[q] = acc[k][q];
+      continue;
+    }
+    if (!cin[k]) continue;
+    const long long cell = cx[k] + (long long)g.N[0] * (cy[k] + (long long)g.N[1] * cz[k]);
+    float s = acc[k][0];
+    if (s < 1e-5f) s = 1.0f;  // bmGridder_n2u_leight3_mex.cpp:341-344
+#pragma unroll
+    for (int c = 0; c < NCH; ++c) {
+      const float re = __fdiv_rn(acc[k][1 + 2 * c], s), im = __fdiv_rn(acc[k][2 + 2 * c], s);
+      if (out.layout == Layout::kPointSplit) {
+        out.re[cell * NCH + c] = re;
+        out.im[cell * NCH + c] = im;
+      } else {  // kCoilC64
+        out.c64[(long long)c * g.Nu_tot + cell] = make_float2(re * out.scale, im * out.scale);
+      }
+    }
   }
 }
 
-__global__ void __launch_bounds__(kGridThreads) leight_combine_kernel(LeightGeom g, const int* __restrict__ nchunk,
+// one CTA per split tile (split[blockIdx.x])
+__global__ void __launch_bounds__(kGridThreads) leight_combine_kernel(LeightGeom g, const int* __restrict__ split,
+                                                                      const int* __restrict__ nchunk,
                                                                       const int* __restrict__ slot_off,
                                                                       const float* __restrict__ partial,
                                                                       LeightOutput out) {
   extern __shared__ float sm[];
-  const long long tile = blockIdx.x;
+  const long long tile = split[blockIdx.x];
   const int n = nchunk[tile];
   if (n <= 1) return;
   const int G = 2 * g.nCh + 1;
@@ -293,14 +547,7 @@ __global__ void __launch_bounds__(kGridThreads) leight_combine_kernel(LeightGeom
   __syncthreads();
   int org[3];
   tile_origin(g, tile, org);
-  for (int i = threadIdx.x; i < g.tile_cells * g.nCh; i += blockDim.x) {
-    const int c = i % g.nCh, lc = i / g.nCh;
-    const int lx = lc % g.T[0], ly = (lc / g.T[0]) % g.T[1], lz = lc / (g.T[0] * g.T[1]);
-    const int x = org[0] + lx, y = org[1] + ly, z = org[2] + lz;
-    if (x >= g.N[0] || y >= g.N[1] || z >= g.N[2]) continue;
-    const long long cell = x + (long long)g.N[0] * (y + (long long)g.N[1] * z);
-    store_cell(g, out, cell, sm + lc * G, c);
-  }
+  store_tile(g, out, sm, org);
 }
 
 static int grid_for(long long n, int threads = 256) {
@@ -311,7 +558,7 @@ static int grid_for(long long n, int threads = 256) {
 size_t LeightWorkspace::counters_bytes(const LeightGeom& g) {
   size_t scan_tmp = 0;
   cub::DeviceScan::ExclusiveSum(nullptr, scan_tmp, (int*)nullptr, (int*)nullptr, (int)g.ntiles);
-  return align((size_t)g.ntiles * 4) * 7 + align(scan_tmp);
+  return align((size_t)g.ntiles * 4) * 8 + align(8) + align(scan_tmp);
 }
 
 size_t LeightWorkspace::bins_bytes(const LeightGeom& g, long long pairs, long long chunks, long long slots) {
@@ -340,33 +587,38 @@ int leight_run(const LeightGeom& g, const LeightInputs& in, int nPt, const Leigh
   int* chunk_off = (int*)take((size_t)nt * 4);
   int* nslot = (int*)take((size_t)nt * 4);
   int* slot_off = (int*)take((size_t)nt * 4);
+  int* split = (int*)take((size_t)nt * 4);
+  int* nsplit = (int*)take(8);  // [0]: split tiles, [1]: single-chunk tiles placed
   size_t scan_tmp = 0;
   cub::DeviceScan::ExclusiveSum(nullptr, scan_tmp, count, offset, nt);
   void* tmp = take(scan_tmp);
 
   MLG_CUDA(cudaMemsetAsync(count, 0, (size_t)nt * 4, s));
   MLG_CUDA(cudaMemsetAsync(cursor, 0, (size_t)nt * 4, s));
+  MLG_CUDA(cudaMemsetAsync(nsplit, 0, 4, s));
   if (nPt > 0) {
     leight_count_kernel<<<grid_for(nPt), 256, 0, s>>>(g, in, nPt, count);
     MLG_LAUNCHED();
   }
   MLG_CUDA(cub::DeviceScan::ExclusiveSum(tmp, scan_tmp, count, offset, nt, s));
-  leight_chunk_count_kernel<<<grid_for(nt), 256, 0, s>>>(g.ntiles, count, nchunk, nslot);
+  leight_chunk_count_kernel<<<grid_for(nt), 256, 0, s>>>(g.ntiles, count, nchunk, nslot, split, nsplit);
   MLG_LAUNCHED();
   MLG_CUDA(cub::DeviceScan::ExclusiveSum(tmp, scan_tmp, nchunk, chunk_off, nt, s));
   MLG_CUDA(cub::DeviceScan::ExclusiveSum(tmp, scan_tmp, nslot, slot_off, nt, s));
   // totals = last offset + last count
-  int h[6];
+  int h[7];
   MLG_CUDA(cudaMemcpyAsync(h + 0, offset + nt - 1, 4, cudaMemcpyDeviceToHost, s));
   MLG_CUDA(cudaMemcpyAsync(h + 1, count + nt - 1, 4, cudaMemcpyDeviceToHost, s));
   MLG_CUDA(cudaMemcpyAsync(h + 2, chunk_off + nt - 1, 4, cudaMemcpyDeviceToHost, s));
   MLG_CUDA(cudaMemcpyAsync(h + 3, nchunk + nt - 1, 4, cudaMemcpyDeviceToHost, s));
   MLG_CUDA(cudaMemcpyAsync(h + 4, slot_off + nt - 1, 4, cudaMemcpyDeviceToHost, s));
   MLG_CUDA(cudaMemcpyAsync(h + 5, nslot + nt - 1, 4, cudaMemcpyDeviceToHost, s));
+  MLG_CUDA(cudaMemcpyAsync(h + 6, nsplit, 4, cudaMemcpyDeviceToHost, s));
   MLG_CUDA(cudaStreamSynchronize(s));
   const long long npairs = (long long)h[0] + h[1];
   const long long nchunks = (long long)h[2] + h[3];
   const long long nslots = (long long)h[4] + h[5];
+  const int n_split = h[6];
   ws.last_pairs = npairs;
   ws.last_chunks = nchunks;
   ws.last_slots = nslots;
@@ -389,19 +641,38 @@ int leight_run(const LeightGeom& g, const LeightInputs& in, int nPt, const Leigh
     leight_fill_kernel<<<grid_for(nPt), 256, 0, s>>>(g, in, nPt, offset, cursor, pairs);
     MLG_LAUNCHED();
   }
-  leight_chunk_build_kernel<<<grid_for(nt), 256, 0, s>>>(g.ntiles, count, offset, nchunk, chunk_off, slot_off,
-                                                         chunks);
+  MLG_CUDA(cudaMemsetAsync(nsplit + 1, 0, 4, s));
+  leight_chunk_build_kernel<<<grid_for(nt), 256, 0, s>>>(g.ntiles, count, offset, nchunk, slot_off, (int)nslots,
+                                                         nsplit + 1, chunks);
   MLG_LAUNCHED();
+  // a warp per sample for many channels and windows of at most 32 cells
+  int W = g.nWin;
+  if (g.imDim > 1) W *= g.nWin;
+  if (g.imDim > 2) W *= g.nWin;
+  const int G = 2 * g.nCh + 1;
+  const bool warp_path = G >= 17 && G <= 32 * kWarpMaxK && W <= 32;
   if (g.smem_bytes > 48 * 1024) {
     MLG_CUDA(cudaFuncSetAttribute(leight_accumulate_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)kTileSmemBudget));
+    MLG_CUDA(cudaFuncSetAttribute(leight_accumulate_warp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)kTileSmemBudget));
     MLG_CUDA(cudaFuncSetAttribute(leight_combine_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)kTileSmemBudget));
   }
-  leight_accumulate_kernel<<<(int)nchunks, kGridThreads, g.smem_bytes, s>>>(g, in, pairs, chunks, partial, out);
+  if (g.gather && g.nCh == 16)
+    leight_gather_kernel<16><<<(int)nchunks, kGridThreads, 0, s>>>(g, in, pairs, chunks, partial, out);
+  else if (g.gather && g.nCh == 12)
+    leight_gather_kernel<12><<<(int)nchunks, kGridThreads, 0, s>>>(g, in, pairs, chunks, partial, out);
+  else if (g.gather && g.nCh == 8)
+    leight_gather_kernel<8><<<(int)nchunks, kGridThreads, 0, s>>>(g, in, pairs, chunks, partial, out);
+  else if (warp_path)
+    leight_accumulate_warp_kernel<<<(int)nchunks, kGridThreads, g.smem_bytes, s>>>(g, in, pairs, chunks, partial,
+                                                                                     out);
+  else
+    leight_accumulate_kernel<<<(int)nchunks, kGridThreads, g.smem_bytes, s>>>(g, in, pairs, chunks, partial, out);
   MLG_LAUNCHED();
-  if (nslots > 0) {
-    leight_combine_kernel<<<nt, kGridThreads, g.smem_bytes, s>>>(g, nchunk, slot_off, partial, out);
+  if (n_split > 0) {
+    leight_combine_kernel<<<n_split, kGridThreads, g.smem_bytes, s>>>(g, split, nchunk, slot_off, partial, out);
     MLG_LAUNCHED();
   }
   return MLG_OK;

@@ -16,6 +16,9 @@ struct LeightGeom {
   size_t smem_bytes = 0;
   float t_shift = 0.5f;
   float g1 = 0.f, g2 = 0.f;  // Gaussian constants
+  // register-accumulating tiles (8, 12 or 16 coils): at most 512 cells, two
+  // per thread; otherwise shared-memory accumulators sized by smem_bytes
+  bool gather = false;
 };
 
 struct LeightInputs {

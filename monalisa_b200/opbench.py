@@ -26,6 +26,8 @@ def main(argv=None):
     ap.add_argument("--reps", type=int, default=3, help="forward + adjoint applications")
     ap.add_argument("--adjoint", default="masked", choices=["masked", "fused", "full_grid"])
     ap.add_argument("--precision", default="fp32", choices=["fp32", "mixed", "fp16_values"])
+    ap.add_argument("--op", default="nufft", choices=["nufft", "gridder"],
+                    help="nufft: operator stages; gridder: the leight adjoint gridder on the samples")
     args = ap.parse_args(argv)
 
     import torch
@@ -37,6 +39,21 @@ def main(argv=None):
     n, Ng = args.n, 2 * args.n
     t = traj.bmTraj_fullRadial3_phyllotaxis_lineAssym2(args.samples, args.spokes, 1, Ng / args.samples)
     ve = traj.bmVolumeElement_full_radial3(t)
+    if args.op == "gridder":
+        rng = np.random.default_rng(7)
+        data = (rng.standard_normal((args.coils, t.shape[1])) +
+                1j * rng.standard_normal((args.coils, t.shape[1]))).astype(np.complex64)
+        for _ in range(max(1, args.reps)):
+            mb.gridding.bmGridder_n2u_leight_dev(data, t, ve, [Ng] * 3, [1, 1, 1], "gauss", 3, [0.61, 10])
+        torch.cuda.synchronize()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        ev[0].record()
+        mb.gridding.bmGridder_n2u_leight_dev(data, t, ve, [Ng] * 3, [1, 1, 1], "gauss", 3, [0.61, 10])
+        ev[1].record()
+        torch.cuda.synchronize()
+        print(f"leight gridder {t.shape[1]} samples, {args.coils} coils -> {Ng}^3: "
+              f"{ev[0].elapsed_time(ev[1]):.3f} ms (with host preparation and upload)")
+        return
     Gu, Gut = mb.bmTraj2SparseMat(t, ve, [Ng] * 3, [1, 1, 1])
     rec = mb.SensaRecon(Gu, Gut, traj.coil_maps([n] * 3, args.coils, 1), [n] * 3, precision=args.precision)
     rec.plan.adjoint_mode = args.adjoint

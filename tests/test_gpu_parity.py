@@ -110,10 +110,13 @@ def _radial3(nSpoke, nRead, N, seed):
 
 
 @pytest.mark.parametrize("imDim,N,nCh,nWin,nPt", [(3, 32, 4, 3, 60000), (2, 96, 3, 3, 120000), (3, 24, 1, 4, 8000),
-                                                  (2, 40, 16, 5, 20000), (1, 64, 2, 3, 5000)])
+                                                  (2, 40, 16, 5, 20000), (1, 64, 2, 3, 5000),
+                                                  (3, 32, 16, 3, 60000), (3, 24, 12, 3, 30000)])
 def test_leight_heavy_bins_match_port(imDim, N, nCh, nWin, nPt):
     """Dense central sampling: bins larger than one chunk exercise the
-    split-and-combine path; compared with the bit-exact C restatement."""
+    split-and-combine path; compared with the bit-exact C restatement.  8 or
+    more coils with windows of at most 32 cells take the warp-per-sample
+    accumulation, fewer coils the thread-per-cell one."""
     from monalisa_b200 import _native as NN
 
     rng = np.random.default_rng(11 + imDim)
