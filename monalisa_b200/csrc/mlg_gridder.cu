@@ -678,6 +678,519 @@ int leight_run(const LeightGeom& g, const LeightInputs& in, int nPt, const Leigh
   return MLG_OK;
 }
 
+// ---- cell-binned form ------------------------------------------------------
+// A sample whose window starts at cell lo (0-based, lo_d in [1 - nWin, N_d -
+// 1] for a window that meets the grid) is keyed by its corner cell e = lo +
+// nWin - 1 in the corner grid E_d = N_d + nWin - 1.  Grid cell x is covered
+// by the windows starting at x - nWin + 1 .. x, i.e. corner cells x .. x +
+// nWin - 1: along the fastest axis these are consecutive keys, so a cell
+// reads nWin^(imDim-1) contiguous runs of the sorted samples.  The sort is
+// stable: within a corner cell the samples keep their input order, and each
+// cell sums its runs in corner order -- deterministic from call to call.
+struct CornerGrid {
+  int E[3] = {1, 1, 1};
+  long long E_tot = 1;
+};
+
+static CornerGrid corner_grid(const LeightGeom& g) {
+  CornerGrid e;
+  e.E_tot = 1;
+  for (int d = 0; d < 3; ++d) {
+    e.E[d] = d < g.imDim ? g.N[d] + g.nWin - 1 : 1;
+    e.E_tot *= e.E[d];
+  }
+  return e;
+}
+
+__global__ void leight_key_kernel(LeightGeom g, CornerGrid e, LeightInputs in, int nPt, unsigned* __restrict__ keys,
+                                  int* __restrict__ idx, int* __restrict__ count) {
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nPt; s += gridDim.x * blockDim.x) {
+    float r[3];
+    int lo[3];
+    unsigned key = (unsigned)e.E_tot;  // missed windows sort after every corner cell
+    if (sample_window(g, in, s, r, lo)) {
+      const int k1 = g.imDim > 1 ? lo[1] + g.nWin - 1 : 0, k2 = g.imDim > 2 ? lo[2] + g.nWin - 1 : 0;
+      key = (unsigned)(lo[0] + g.nWin - 1 + (long long)e.E[0] * (k1 + (long long)e.E[1] * k2));
+      atomicAdd(count + key, 1);
+    }
+    keys[s] = key;
+    idx[s] = s;
+  }
+}
+
+// Sorted sample records: (t_x, t_y, t_z, Dn), the 1-based coordinates.
+__global__ void leight_record_kernel(LeightGeom g, LeightInputs in, const int* __restrict__ sidx,
+                                     const int* __restrict__ n_hits, float4* __restrict__ rec) {
+  const int n = *n_hits;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const int s = __ldg(sidx + k);
+    const float ty = g.imDim > 1 ? __ldg(in.ty + s) : 0.f, tz = g.imDim > 2 ? __ldg(in.tz + s) : 0.f;
+    rec[k] = make_float4(__ldg(in.tx + s), ty, tz, __ldg(in.Dn + s));
+  }
+}
+
+// CPT consecutive coils of sample s (split complex, [nPt][nCh]); the host
+// picks CPT so that the vector loads are aligned.
+template <int CPT>
+__device__ __forceinline__ void load_coils(const float* __restrict__ re, const float* __restrict__ im, long long o,
+                                           float* vr, float* vi) {
+  if constexpr (CPT % 4 == 0) {
+#pragma unroll
+    for (int j = 0; j < CPT / 4; ++j) {
+      const float4 a = __ldg(reinterpret_cast<const float4*>(re + o) + j);
+      const float4 b = __ldg(reinterpret_cast<const float4*>(im + o) + j);
+      vr[4 * j] = a.x, vr[4 * j + 1] = a.y, vr[4 * j + 2] = a.z, vr[4 * j + 3] = a.w;
+      vi[4 * j] = b.x, vi[4 * j + 1] = b.y, vi[4 * j + 2] = b.z, vi[4 * j + 3] = b.w;
+    }
+  } else if constexpr (CPT == 2) {
+    const float2 a = __ldg(reinterpret_cast<const float2*>(re + o));
+    const float2 b = __ldg(reinterpret_cast<const float2*>(im + o));
+    vr[0] = a.x, vr[1] = a.y, vi[0] = b.x, vi[1] = b.y;
+  } else {  // scalar: 1 or a whole odd (or 6-coil) cell
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) vr[c] = __ldg(re + o + c), vi[c] = __ldg(im + o + c);
+  }
+}
+
+template <int CPT>
+__device__ __forceinline__ void store_coils(float* re, float* im, long long o, const float* vr, const float* vi) {
+  if constexpr (CPT % 4 == 0) {
+#pragma unroll
+    for (int j = 0; j < CPT / 4; ++j) {
+      reinterpret_cast<float4*>(re + o)[j] = make_float4(vr[4 * j], vr[4 * j + 1], vr[4 * j + 2], vr[4 * j + 3]);
+      reinterpret_cast<float4*>(im + o)[j] = make_float4(vi[4 * j], vi[4 * j + 1], vi[4 * j + 2], vi[4 * j + 3]);
+    }
+  } else if constexpr (CPT == 2) {
+    *reinterpret_cast<float2*>(re + o) = make_float2(vr[0], vr[1]);
+    *reinterpret_cast<float2*>(im + o) = make_float2(vi[0], vi[1]);
+  } else {
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) re[o + c] = vr[c], im[o + c] = vi[c];
+  }
+}
+
+// Window weight of the grid cell with 1-based coordinates f for the sorted
+// sample record rc (bmGridder_n2u_leight3_mex.cpp: squared distances summed
+// x, y, z, then g1 exp(g2 d2) Dn).  The reference forms a distance as
+// (t - node) - u with node = trunc(t + shift) and u = f - node; t - node is
+// exact (Sterbenz), so that difference is the correctly rounded t - f --
+// one subtraction here, the same value except where t + shift itself
+// rounded across an integer (t within 2^-24 of a half-integer boundary).
+__device__ __forceinline__ float cell_weight(const LeightGeom& g, float4 rc, float fx, float fy, float fz) {
+  const float dx = rc.x - fx;
+  float d2 = __fmul_rn(dx, dx);
+  if (g.imDim > 1) {
+    const float dy = rc.y - fy;
+    d2 = __fadd_rn(d2, __fmul_rn(dy, dy));
+  }
+  if (g.imDim > 2) {
+    const float dz = rc.z - fz;
+    d2 = __fadd_rn(d2, __fmul_rn(dz, dz));
+  }
+  return __fmul_rn(__fmul_rn(g.g1, expf(__fmul_rn(g.g2, d2))), rc.w);
+}
+
+// Cells that gather more than this many (sample, window cell) incidences go
+// to the heavy list: one CTA each instead of one thread.
+constexpr int kHeavyIncidences = 64;
+
+struct HeavyList {
+  int* cells = nullptr;
+  int* count = nullptr;
+  long long cap = 0;
+};
+
+// A thread per (grid cell, CPT coils), cells in storage order.  Fused
+// multiply-adds into the coil sums, weight sum and normalisation as in the
+// reference (:341-344).  A cell with more than kHeavyIncidences entries is
+// appended to the heavy list by its first thread and left to
+// leight_heavy_kernel.
+// NW, DIM > 0: window width and dimension fixed at compile time, the
+// window rows' run bounds loaded together and kept in registers (in-order
+// issue would otherwise wait for each row's two loads in turn); 0: taken
+// from g.
+template <int CPT, int NW, int DIM>
+__global__ void __launch_bounds__(256) leight_cell_kernel(LeightGeom g, CornerGrid e, const int* __restrict__ off,
+                                                          const int* __restrict__ sidx,
+                                                          const float4* __restrict__ rec, LeightInputs in,
+                                                          LeightOutput out, HeavyList heavy, int cell_begin,
+                                                          int cell_end) {
+  // 32-bit index arithmetic: a launch covers fewer than 2^31 threads
+  const unsigned Q = (unsigned)(g.nCh / CPT);
+  const unsigned it = blockIdx.x * blockDim.x + threadIdx.x;
+  const unsigned lc = it / Q;
+  const int cell = cell_begin + (int)lc;
+  if (cell >= cell_end) return;
+  const int c0 = (int)(it - lc * Q) * CPT;
+  const unsigned q = (unsigned)cell / (unsigned)g.N[0];
+  const int x = cell - (int)q * g.N[0];
+  const int z = (int)(q / (unsigned)g.N[1]);
+  const int y = (int)q - z * g.N[1];
+  const int nW = NW ? NW : g.nWin, dim = DIM ? DIM : g.imDim;
+  const int W1 = dim > 1 ? nW : 1, R = W1 * (dim > 2 ? nW : 1);
+  constexpr int RS = NW ? (DIM == 3 ? NW * NW : (DIM == 2 ? NW : 1)) : 1;  // rows held in registers
+  auto row_key = [&](int r) {  // corner grid below 2^31 cells: 32-bit keys
+    const int iy = r % W1, iz = r / W1;
+    return x + e.E[0] * ((y + iy) + e.E[1] * (z + iz));
+  };
+  int rb[RS], rn[RS];
+  int total = 0;
+  if constexpr (NW != 0) {
+#pragma unroll
+    for (int r = 0; r < RS; ++r) {
+      const int rk = row_key(r);
+      rb[r] = __ldg(off + rk);
+      rn[r] = __ldg(off + rk + NW) - rb[r];
+      total += rn[r];
+    }
+  } else {
+    for (int r = 0; r < R; ++r) {
+      const int rk = row_key(r);
+      total += __ldg(off + rk + nW) - __ldg(off + rk);
+    }
+  }
+  if (total > kHeavyIncidences) {
+    if (c0 == 0) {
+      const int h = atomicAdd(heavy.count, 1);
+      if (h < heavy.cap) heavy.cells[h] = (int)cell;
+    }
+    return;
+  }
+  float ar[CPT], ai[CPT], ws = 0.f;
+#pragma unroll
+  for (int c = 0; c < CPT; ++c) ar[c] = ai[c] = 0.f;
+  const float fx = (float)(x + 1), fy = (float)(y + 1), fz = (float)(z + 1);
+  auto entry = [&](int k) {
+    const float4 rc = __ldg(rec + k);
+    const int s = __ldg(sidx + k);
+    float vr[CPT], vi[CPT];
+    load_coils<CPT>(in.re, in.im, (long long)s * g.nCh + c0, vr, vi);
+    const float w = cell_weight(g, rc, fx, fy, fz);
+    ws = __fadd_rn(ws, w);
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) {
+      ar[c] = __fmaf_rn(w, vr[c], ar[c]);
+      ai[c] = __fmaf_rn(w, vi[c], ai[c]);
+    }
+  };
+  if constexpr (NW != 0) {
+    // One loop over the cell's entries, rows in order: a warp's lanes
+    // diverge once (on their totals), not once per window row.
+    int r = -1, k = 0, end = 0;
+    for (int i = 0; i < total; ++i) {
+      if (k == end) {  // next non-empty row, selected without indexing the arrays
+        int nr = RS;
+#pragma unroll
+        for (int j = 0; j < RS; ++j) {
+          if (nr == RS && j > r && rn[j] > 0) {
+            nr = j;
+            k = rb[j];
+            end = rb[j] + rn[j];
+          }
+        }
+        r = nr;
+      }
+      entry(k++);
+    }
+  } else {
+    for (int r = 0; r < R && total > 0; ++r) {
+      const int rk = row_key(r);
+      const int b = __ldg(off + rk), en = __ldg(off + rk + nW);
+      for (int k = b; k < en; ++k) entry(k);
+    }
+  }
+  // weight sums below 1e-5 leave the sums unscaled (:341-344); otherwise one
+  // correctly rounded reciprocal and a multiply per value (within an ulp of
+  // the reference's division); cells without samples store zeros
+  if (ws >= 1e-5f) {
+    const float inv = __frcp_rn(ws);
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) {
+      ar[c] = __fmul_rn(ar[c], inv);
+      ai[c] = __fmul_rn(ai[c], inv);
+    }
+  }
+  store_coils<CPT>(out.re, out.im, (long long)cell * g.nCh + c0, ar, ai);
+}
+
+// Heavy cells: a persistent grid, one CTA per listed cell at a time.  The
+// 256 threads split each window row's run (thread t takes entries t, t +
+// 256, ...), accumulate kHeavyCoils coils per pass, and the CTA sums the
+// thread partials in a fixed tree (warp shuffles, then the eight warps in
+// order): deterministic.  VEC4: nCh % 4 == 0 and 16-byte aligned input.
+constexpr int kHeavyCoils = 16;
+
+template <bool VEC4>
+__global__ void __launch_bounds__(256) leight_heavy_kernel(LeightGeom g, CornerGrid e, const int* __restrict__ off,
+                                                           const int* __restrict__ sidx,
+                                                           const float4* __restrict__ rec, LeightInputs in,
+                                                           LeightOutput out, HeavyList heavy) {
+  __shared__ float red[8][2 * kHeavyCoils + 1];
+  __shared__ int s_b[256], s_pre[257];  // the cell's window rows (nWin^2 <= 256): run start, prefix of lengths
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nh = (int)min((long long)*heavy.count, heavy.cap);
+  const int nW = g.nWin, W1 = g.imDim > 1 ? nW : 1, R = W1 * (g.imDim > 2 ? nW : 1);
+  for (int h = blockIdx.x; h < nh; h += gridDim.x) {
+    const int cell = heavy.cells[h];
+    const unsigned q = (unsigned)cell / (unsigned)g.N[0];
+    const int x = cell - (int)q * g.N[0];
+    const int z = (int)(q / (unsigned)g.N[1]);
+    const int y = (int)q - z * g.N[1];
+    for (int r = threadIdx.x; r < R; r += blockDim.x) {
+      const int rk = x + e.E[0] * ((y + r % W1) + e.E[1] * (z + r / W1));
+      s_b[r] = __ldg(off + rk);
+      s_pre[r + 1] = __ldg(off + rk + nW) - s_b[r];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      s_pre[0] = 0;
+      for (int r = 0; r < R; ++r) s_pre[r + 1] += s_pre[r];
+    }
+    __syncthreads();
+    const int T = s_pre[R];
+    for (int c0 = 0; c0 < g.nCh; c0 += kHeavyCoils) {
+      const int nc = min(kHeavyCoils, g.nCh - c0);
+      float ar[kHeavyCoils], ai[kHeavyCoils], ws = 0.f;
+#pragma unroll
+      for (int c = 0; c < kHeavyCoils; ++c) ar[c] = ai[c] = 0.f;
+      {
+        const float fx = (float)(x + 1), fy = (float)(y + 1), fz = (float)(z + 1);
+        int r = 0;
+        for (int i = threadIdx.x; i < T; i += 256) {  // the rows' runs as one list
+          while (s_pre[r + 1] <= i) ++r;
+          {
+            const int k = s_b[r] + (i - s_pre[r]);
+            const float4 rc = __ldg(rec + k);
+            const long long o = (long long)__ldg(sidx + k) * g.nCh + c0;
+            const float w = cell_weight(g, rc, fx, fy, fz);
+            ws = __fadd_rn(ws, w);
+            if (VEC4) {
+#pragma unroll
+              for (int c4 = 0; c4 < kHeavyCoils / 4; ++c4) {
+                if (4 * c4 >= nc) break;
+                float vr[4], vi[4];
+                load_coils<4>(in.re, in.im, o + 4 * c4, vr, vi);
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                  ar[4 * c4 + c] = __fmaf_rn(w, vr[c], ar[4 * c4 + c]);
+                  ai[4 * c4 + c] = __fmaf_rn(w, vi[c], ai[4 * c4 + c]);
+                }
+              }
+            } else {
+#pragma unroll
+              for (int c = 0; c < kHeavyCoils; ++c) {
+                if (c >= nc) break;
+                ar[c] = __fmaf_rn(w, __ldg(in.re + o + c), ar[c]);
+                ai[c] = __fmaf_rn(w, __ldg(in.im + o + c), ai[c]);
+              }
+            }
+          }
+        }
+      }
+#pragma unroll
+      for (int sh = 16; sh > 0; sh >>= 1) {
+        ws += __shfl_down_sync(0xffffffffu, ws, sh);
+#pragma unroll
+        for (int c = 0; c < kHeavyCoils; ++c) {
+          ar[c] += __shfl_down_sync(0xffffffffu, ar[c], sh);
+          ai[c] += __shfl_down_sync(0xffffffffu, ai[c], sh);
+        }
+      }
+      if (lane == 0) {
+        red[warp][0] = ws;
+#pragma unroll
+        for (int c = 0; c < kHeavyCoils; ++c) {
+          red[warp][1 + 2 * c] = ar[c];
+          red[warp][2 + 2 * c] = ai[c];
+        }
+      }
+      __syncthreads();
+      if ((int)threadIdx.x < nc) {
+        const int c = threadIdx.x;
+        float sw = 0.f, sr = 0.f, si = 0.f;
+        for (int k = 0; k < 8; ++k) {
+          sw += red[k][0];
+          sr += red[k][1 + 2 * c];
+          si += red[k][2 + 2 * c];
+        }
+        const float inv = sw < 1e-5f ? 1.0f : __frcp_rn(sw);  // as in leight_cell_kernel
+        out.re[(long long)cell * g.nCh + c0 + c] = __fmul_rn(sr, inv);
+        out.im[(long long)cell * g.nCh + c0 + c] = __fmul_rn(si, inv);
+      }
+      __syncthreads();  // red is reused by the next pass or cell
+    }
+  }
+}
+
+namespace {
+
+struct CellLaunch {
+  const LeightGeom& g;
+  const CornerGrid& e;
+  const int* off;
+  const int* sidx;
+  const float4* rec;
+  const LeightInputs& in;
+  const LeightOutput& out;
+  const HeavyList& heavy;
+  cudaStream_t s;
+};
+
+// Compile-time rows for the common 3-wide windows in 2-D and 3-D; the grid
+// cells in ranges of fewer than 2^31 threads per launch.
+template <int CPT>
+void launch_cells(const CellLaunch& c) {
+  const long long Q = c.g.nCh / CPT;
+  const long long per = ((1LL << 31) - 256) / Q;  // cells per launch
+  for (long long c0 = 0; c0 < c.g.Nu_tot; c0 += per) {
+    const int b = (int)c0, en = (int)std::min(c.g.Nu_tot, c0 + per);
+    const unsigned blocks = (unsigned)(((long long)(en - b) * Q + 255) / 256);
+    if (c.g.nWin == 3 && c.g.imDim == 3)
+      leight_cell_kernel<CPT, 3, 3><<<blocks, 256, 0, c.s>>>(c.g, c.e, c.off, c.sidx, c.rec, c.in, c.out, c.heavy, b,
+                                                             en);
+    else if (c.g.nWin == 3 && c.g.imDim == 2)
+      leight_cell_kernel<CPT, 3, 2><<<blocks, 256, 0, c.s>>>(c.g, c.e, c.off, c.sidx, c.rec, c.in, c.out, c.heavy, b,
+                                                             en);
+    else
+      leight_cell_kernel<CPT, 0, 0><<<blocks, 256, 0, c.s>>>(c.g, c.e, c.off, c.sidx, c.rec, c.in, c.out, c.heavy, b,
+                                                             en);
+  }
+}
+
+struct CellsLayout {
+  size_t count, off, keys_in, keys_out, idx_in, idx_out, rec, heavy, heavy_n, scan_tmp, sort_tmp, total;
+  long long heavy_cap;
+};
+
+CellsLayout cells_layout(const LeightGeom& g, int nPt) {
+  using W = LeightWorkspace;
+  const CornerGrid e = corner_grid(g);
+  const int ne = (int)(e.E_tot + 1);
+  CellsLayout L;
+  size_t scan_tmp = 0, sort_tmp = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, scan_tmp, (int*)nullptr, (int*)nullptr, ne);
+  cub::DeviceRadixSort::SortPairs(nullptr, sort_tmp, (unsigned*)nullptr, (unsigned*)nullptr, (int*)nullptr,
+                                  (int*)nullptr, std::max(nPt, 1));
+  size_t p = 0;
+  auto take = [&](size_t bytes) {
+    const size_t at = p;
+    p += W::align(bytes);
+    return at;
+  };
+  L.count = take((size_t)ne * 4);
+  L.off = take((size_t)ne * 4);
+  L.keys_in = take((size_t)nPt * 4);
+  L.keys_out = take((size_t)nPt * 4);
+  L.idx_in = take((size_t)nPt * 4);
+  L.idx_out = take((size_t)nPt * 4);
+  L.rec = take((size_t)nPt * 16);
+  // a heavy cell holds more than kHeavyIncidences of the at most nPt x
+  // nWin^imDim incidences
+  long long wc = 1;
+  for (int d = 0; d < g.imDim; ++d) wc *= g.nWin;
+  L.heavy_cap = std::min<long long>(g.Nu_tot, (long long)nPt * wc / (kHeavyIncidences + 1) + 1);
+  L.heavy = take((size_t)L.heavy_cap * 4);
+  L.heavy_n = take(4);
+  L.scan_tmp = take(scan_tmp);
+  L.sort_tmp = take(sort_tmp);
+  L.total = p;
+  return L;
+}
+
+}  // namespace
+
+size_t leight_cells_bytes(const LeightGeom& g, int nPt) { return cells_layout(g, nPt).total; }
+
+int leight_run_cells(const LeightGeom& g, const LeightInputs& in, int nPt, const LeightOutput& out, void* ws,
+                     size_t ws_bytes, cudaStream_t s) {
+  MLG_CHECK(in.layout == Layout::kPointSplit && out.layout == Layout::kPointSplit,
+            "the cell-binned gridder takes split complex input and output");
+  const CornerGrid e = corner_grid(g);
+  MLG_CHECK(e.E_tot < (1LL << 31) - 1, "corner grid of %lld cells too large", e.E_tot);
+  const CellsLayout L = cells_layout(g, nPt);
+  MLG_CHECK(ws && ws_bytes >= L.total, "gridding workspace too small (%zu < %zu bytes)", ws_bytes, L.total);
+  char* base = static_cast<char*>(ws);
+  int* count = reinterpret_cast<int*>(base + L.count);
+  int* off = reinterpret_cast<int*>(base + L.off);
+  unsigned* keys_in = reinterpret_cast<unsigned*>(base + L.keys_in);
+  unsigned* keys_out = reinterpret_cast<unsigned*>(base + L.keys_out);
+  int* idx_in = reinterpret_cast<int*>(base + L.idx_in);
+  int* idx_out = reinterpret_cast<int*>(base + L.idx_out);
+  float4* rec = reinterpret_cast<float4*>(base + L.rec);
+  const int ne = (int)(e.E_tot + 1);
+
+  MLG_CUDA(cudaMemsetAsync(count, 0, (size_t)ne * 4, s));
+  if (nPt > 0) {
+    leight_key_kernel<<<grid_for(nPt), 256, 0, s>>>(g, e, in, nPt, keys_in, idx_in, count);
+    MLG_LAUNCHED();
+  }
+  size_t scan_tmp = L.sort_tmp - L.scan_tmp;
+  MLG_CUDA(cub::DeviceScan::ExclusiveSum(base + L.scan_tmp, scan_tmp, count, off, ne, s));
+  if (nPt > 0) {
+    size_t sort_tmp = L.total - L.sort_tmp;
+    const int end_bit = 32 - __builtin_clz((unsigned)e.E_tot);  // the miss key E_tot included
+    MLG_CUDA(cub::DeviceRadixSort::SortPairs(base + L.sort_tmp, sort_tmp, keys_in, keys_out, idx_in, idx_out, nPt, 0,
+                                             end_bit, s));
+    leight_record_kernel<<<grid_for(nPt), 256, 0, s>>>(g, in, idx_out, off + e.E_tot, rec);
+    MLG_LAUNCHED();
+  }
+  // Coils per thread: 8 or 4 (16-byte vectors) when they divide nCh and the
+  // buffers are aligned (16 coils: 8 measured fastest, ahead of 4 and 16); a
+  // whole cell per thread for 3, 5, 6 or 7 coils (scalar loads); else 2 or 1.
+  const uintptr_t align_bits = (uintptr_t)in.re | (uintptr_t)in.im | (uintptr_t)out.re | (uintptr_t)out.im;
+  const bool a16 = align_bits % 16 == 0, a8 = align_bits % 8 == 0;
+  int cpt = 1;
+  if (g.nCh % 8 == 0 && a16)
+    cpt = 8;
+  else if (g.nCh % 4 == 0 && a16)
+    cpt = 4;
+  else if (g.nCh == 3 || g.nCh == 5 || g.nCh == 6 || g.nCh == 7)
+    cpt = g.nCh;
+  else if (g.nCh % 2 == 0 && a8)
+    cpt = 2;
+  HeavyList heavy;
+  heavy.cells = reinterpret_cast<int*>(base + L.heavy);
+  heavy.count = reinterpret_cast<int*>(base + L.heavy_n);
+  heavy.cap = L.heavy_cap;
+  MLG_CUDA(cudaMemsetAsync(heavy.count, 0, 4, s));
+  const CellLaunch cl{g, e, off, idx_out, rec, in, out, heavy, s};
+  switch (cpt) {
+    case 7:
+      launch_cells<7>(cl);
+      break;
+    case 6:
+      launch_cells<6>(cl);
+      break;
+    case 5:
+      launch_cells<5>(cl);
+      break;
+    case 3:
+      launch_cells<3>(cl);
+      break;
+    case 8:
+      launch_cells<8>(cl);
+      break;
+    case 4:
+      launch_cells<4>(cl);
+      break;
+    case 2:
+      launch_cells<2>(cl);
+      break;
+    default:
+      launch_cells<1>(cl);
+  }
+  MLG_LAUNCHED();
+  if (nPt > 0) {
+    const int hb = (int)std::min<long long>(L.heavy_cap, 148LL * 4);
+    if ((g.nCh % 4) == 0 && ((uintptr_t)in.re | (uintptr_t)in.im) % 16 == 0)
+      leight_heavy_kernel<true><<<hb, 256, 0, s>>>(g, e, off, idx_out, rec, in, out, heavy);
+    else
+      leight_heavy_kernel<false><<<hb, 256, 0, s>>>(g, e, off, idx_out, rec, in, out, heavy);
+    MLG_LAUNCHED();
+  }
+  return MLG_OK;
+}
+
 // ---- precomputed-weight gridder (bmGridder_n2u_mex) -------------------------
 __global__ void widen_kernel(const int* __restrict__ a, long long* __restrict__ b, long long n) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
@@ -801,19 +1314,6 @@ int n2u_build_csr(const float* d_w, const int* d_nJump, int nNb, int nPt, int Nu
 
 using namespace mlg;
 
-namespace {
-
-int grow_bins_pool(LeightWorkspace& ws, size_t bytes, cudaStream_t s) {
-  if (ws.bins) dev_free(ws.bins, s);
-  ws.bins = nullptr;
-  ws.bins_cap = 0;
-  MLG_TRY(dev_alloc(&ws.bins, bytes, s));
-  ws.bins_cap = bytes;
-  return MLG_OK;
-}
-
-}  // namespace
-
 namespace mlg {
 
 int leight_host(int imDim, const float* aReal, const float* aImag, const float* tx, const float* ty, const float* tz,
@@ -851,19 +1351,14 @@ int leight_host(int imDim, const float* aReal, const float* aImag, const float* 
   out.layout = Layout::kPointSplit;
   out.re = dB.p;
   out.im = dB.p + nb;
-  DevBuf<char> counters;
-  MLG_TRY(counters.alloc(LeightWorkspace::counters_bytes(g), s));
-  LeightWorkspace ws;
-  ws.counters = counters.p;
-  ws.counters_cap = counters.n;
-  ws.grow_bins = grow_bins_pool;
-  int st = leight_run(g, in, nPt, out, ws, s);
+  DevBuf<char> ws;
+  MLG_TRY(ws.alloc(leight_cells_bytes(g, nPt), s));
+  int st = leight_run_cells(g, in, nPt, out, ws.p, ws.n, s);
   if (st == MLG_OK) {
     cudaError_t e1 = cudaMemcpyAsync(bReal, dB.p, nb * 4, cudaMemcpyDeviceToHost, s);
     cudaError_t e2 = cudaMemcpyAsync(bImag, dB.p + nb, nb * 4, cudaMemcpyDeviceToHost, s);
     if (e1 != cudaSuccess || e2 != cudaSuccess) st = fail(MLG_ERR_CUDA, "copy of the gridded data failed");
   }
-  if (ws.bins) dev_free(ws.bins, s);
   cudaError_t e = cudaStreamSynchronize(s);
   if (st == MLG_OK && e != cudaSuccess) st = fail(MLG_ERR_CUDA, "leight gridder: %s", cudaGetErrorString(e));
   return st;
@@ -906,15 +1401,9 @@ int mlg_gridder_n2u_leight_dev(int imDim, const float* aReal, const float* aImag
   out.layout = Layout::kPointSplit;
   out.re = bReal;
   out.im = bImag;
-  DevBuf<char> counters;
-  MLG_TRY(counters.alloc(LeightWorkspace::counters_bytes(g), s));
-  LeightWorkspace ws;
-  ws.counters = counters.p;
-  ws.counters_cap = counters.n;
-  ws.grow_bins = grow_bins_pool;
-  const int st = leight_run(g, in, nPt, out, ws, s);
-  if (ws.bins) dev_free(ws.bins, s);  // stream-ordered: freed after the run
-  return st;
+  DevBuf<char> ws;  // stream-ordered: freed after the run
+  MLG_TRY(ws.alloc(leight_cells_bytes(g, nPt), s));
+  return leight_run_cells(g, in, nPt, out, ws.p, ws.n, s);
 }
 
 int mlg_gridder_n2u(const float* aReal, const float* aImag, const float* w, const int* nJump, int nCh, int nNb,

@@ -64,6 +64,16 @@ int leight_geometry(int imDim, int nCh, const int* N, int nWin, float sigma, Lei
 int leight_run(const LeightGeom& g, const LeightInputs& in, int nPt, const LeightOutput& out, LeightWorkspace& ws,
                cudaStream_t s);
 
+// Cell-binned form (the entry points that may allocate): the samples are
+// sorted by the lower-corner cell of their window in a corner grid of
+// N + nWin - 1 cells per image axis, and every grid cell gathers the samples
+// of the corner cells whose windows cover it (no tiles, no atomics on the
+// grid, no host synchronisation).  Its workspace, leight_cells_bytes(g, nPt)
+// bytes, is known before the call.  Split complex input and output only.
+size_t leight_cells_bytes(const LeightGeom& g, int nPt);
+int leight_run_cells(const LeightGeom& g, const LeightInputs& in, int nPt, const LeightOutput& out, void* ws,
+                     size_t ws_bytes, cudaStream_t s);
+
 // Builds the "cell x sample" CSR of a precomputed-weight gridding call.
 int n2u_build_csr(const float* d_w, const int* d_nJump, int nNb, int nPt, int Nu_tot, Csr& m, cudaStream_t s);
 

@@ -109,23 +109,30 @@ def _radial3(nSpoke, nRead, N, seed):
     return traj.bmTraj_fullRadial3_phyllotaxis_lineAssym2(nRead, nSpoke, 1, N / nRead)
 
 
-@pytest.mark.parametrize("imDim,N,nCh,nWin,nPt", [(3, 32, 4, 3, 60000), (2, 96, 3, 3, 120000), (3, 24, 1, 4, 8000),
-                                                  (2, 40, 16, 5, 20000), (1, 64, 2, 3, 5000),
-                                                  (3, 32, 16, 3, 60000), (3, 24, 12, 3, 30000)])
-def test_leight_heavy_bins_match_port(imDim, N, nCh, nWin, nPt):
-    """Dense central sampling: bins larger than one chunk exercise the
-    split-and-combine path; compared with the bit-exact C restatement.  8 or
-    more coils with windows of at most 32 cells take the warp-per-sample
-    accumulation, fewer coils the thread-per-cell one."""
-    from monalisa_b200 import _native as NN
-
-    rng = np.random.default_rng(11 + imDim)
+def _dense_case(imDim, N, nCh, nPt, seed):
+    rng = np.random.default_rng(seed)
     # half the points crowd the centre, half spread out, some outside
     t = np.concatenate([rng.normal(N / 2 + 1, 1.5, (imDim, nPt // 2)),
                         rng.uniform(-1, N + 2, (imDim, nPt - nPt // 2))], 1).astype(np.float32)
     aR = rng.standard_normal((nCh, nPt)).astype(np.float32)
     aI = rng.standard_normal((nCh, nPt)).astype(np.float32)
     Dn = rng.uniform(0.1, 1, nPt).astype(np.float32)
+    return t, aR, aI, Dn
+
+
+@pytest.mark.parametrize("imDim,N,nCh,nWin,nPt", [(3, 32, 4, 3, 60000), (2, 96, 3, 3, 120000), (3, 24, 1, 4, 8000),
+                                                  (2, 40, 16, 5, 20000), (1, 64, 2, 3, 5000),
+                                                  (3, 32, 16, 3, 60000), (3, 24, 12, 3, 30000),
+                                                  (3, 32, 5, 3, 60000), (3, 24, 6, 3, 30000), (2, 64, 7, 3, 40000),
+                                                  (3, 20, 8, 2, 20000)])
+def test_leight_heavy_bins_match_port(imDim, N, nCh, nWin, nPt):
+    """Dense central sampling: cells covered by more than 64 samples take the
+    CTA-per-cell path, the rest a thread per (cell, coil group) with 1 to 8
+    coils per thread; 3-wide windows in 2-D and 3-D have their own compiled
+    forms.  Compared with the bit-exact C restatement."""
+    from monalisa_b200 import _native as NN
+
+    t, aR, aI, Dn = _dense_case(imDim, N, nCh, nPt, 11 + imDim)
     ref = oracle.port_gridder_leight(imDim, aR, aI, t[0], t[1] if imDim > 1 else None, t[2] if imDim > 2 else None,
                                      Dn, nCh, nPt, N, N, N, nWin, 0.61, 10.0)
     Ns = [N if d < imDim else 1 for d in range(3)]
@@ -137,6 +144,39 @@ def test_leight_heavy_bins_match_port(imDim, N, nCh, nWin, nPt):
             NN.fptr(tt[0]), NN.fptr(tt[1]), NN.fptr(tt[2]), NN.fptr(Dn), nCh, nPt, Ns[0], Ns[1], Ns[2], nWin,
             0.61, 10.0, NN.fptr(bR), NN.fptr(bI))
     assert rel(bR + 1j * bI, (ref[0] + 1j * ref[1]).T) <= 1e-5
+
+
+@pytest.mark.parametrize("shift", [0, 1])
+def test_leight_device_entry_deterministic_and_unaligned(shift):
+    """The device-buffer entry: repeated calls give bit-identical grids (the
+    samples are binned by a stable sort, each cell sums in a fixed order);
+    buffers one float off 16-byte alignment fall back to scalar coil access
+    with the same result."""
+    import torch
+
+    from monalisa_b200 import _native as NN
+
+    imDim, N, nCh, nWin, nPt = 3, 32, 16, 3, 60000
+    t, aR, aI, Dn = _dense_case(imDim, N, nCh, nPt, 21)
+    ref = oracle.port_gridder_leight(imDim, aR, aI, t[0], t[1], t[2], Dn, nCh, nPt, N, N, N, nWin, 0.61, 10.0)
+
+    def dev(a):  # a device copy starting `shift` floats into its allocation
+        buf = torch.zeros(a.size + shift, dtype=torch.float32, device="cuda")
+        buf[shift:] = torch.from_numpy(np.ascontiguousarray(a).ravel()).cuda()
+        return buf, buf[shift:]
+
+    keep = [dev(aR.T), dev(aI.T), dev(t[0]), dev(t[1]), dev(t[2]), dev(Dn)]
+    d = [v for _, v in keep]
+    nu = N ** 3
+    outs = []
+    for _ in range(2):
+        bR, bI = dev(np.zeros(nu * nCh, np.float32))[1], dev(np.zeros(nu * nCh, np.float32))[1]
+        NN.call("mlg_gridder_n2u_leight_dev", imDim, *[NN.tptr(x) for x in d], nCh, nPt, N, N, N, nWin, 0.61, 10.0,
+                NN.tptr(bR), NN.tptr(bI), NN.stream_ptr())
+        torch.cuda.synchronize()
+        outs.append((bR.cpu().numpy().reshape(nu, nCh), bI.cpu().numpy().reshape(nu, nCh)))
+    assert np.array_equal(outs[0][0], outs[1][0]) and np.array_equal(outs[0][1], outs[1][1])
+    assert rel(outs[0][0] + 1j * outs[0][1], (ref[0] + 1j * ref[1]).T) <= 1e-5
 
 
 def test_leight_empty_input():
