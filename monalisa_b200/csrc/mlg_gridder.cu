@@ -790,9 +790,13 @@ __device__ __forceinline__ float cell_weight(const LeightGeom& g, float4 rc, flo
   return __fmul_rn(__fmul_rn(g.g1, expf(__fmul_rn(g.g2, d2))), rc.w);
 }
 
-// Cells that gather more than this many (sample, window cell) incidences go
-// to the heavy list: one CTA each instead of one thread.
+// Cells that gather more than kHeavyIncidences (sample, window cell)
+// incidences leave the thread-per-cell kernel: up to kHugeIncidences (and at
+// most kMidRows window rows) to a warp each, beyond that to a CTA each.
 constexpr int kHeavyIncidences = 64;
+constexpr int kHugeIncidences = 2048;
+constexpr int kMidRows = 32;
+constexpr int kHeavyCoils = 16;  // coils per pass of the mid and huge kernels
 
 struct HeavyList {
   int* cells = nullptr;
@@ -803,8 +807,8 @@ struct HeavyList {
 // A thread per (grid cell, CPT coils), cells in storage order.  Fused
 // multiply-adds into the coil sums, weight sum and normalisation as in the
 // reference (:341-344).  A cell with more than kHeavyIncidences entries is
-// appended to the heavy list by its first thread and left to
-// leight_heavy_kernel.
+// appended by its first thread to the mid list (leight_mid_kernel) or the
+// huge list (leight_heavy_kernel).
 // NW, DIM > 0: window width and dimension fixed at compile time, the
 // window rows' run bounds loaded together and kept in registers (in-order
 // issue would otherwise wait for each row's two loads in turn); 0: taken
@@ -813,19 +817,15 @@ template <int CPT, int NW, int DIM>
 __global__ void __launch_bounds__(256) leight_cell_kernel(LeightGeom g, CornerGrid e, const int* __restrict__ off,
                                                           const int* __restrict__ sidx,
                                                           const float4* __restrict__ rec, LeightInputs in,
-                                                          LeightOutput out, HeavyList heavy, int cell_begin,
-                                                          int cell_end) {
-  // 32-bit index arithmetic: a launch covers fewer than 2^31 threads
-  const unsigned Q = (unsigned)(g.nCh / CPT);
-  const unsigned it = blockIdx.x * blockDim.x + threadIdx.x;
-  const unsigned lc = it / Q;
-  const int cell = cell_begin + (int)lc;
-  if (cell >= cell_end) return;
-  const int c0 = (int)(it - lc * Q) * CPT;
-  const unsigned q = (unsigned)cell / (unsigned)g.N[0];
-  const int x = cell - (int)q * g.N[0];
-  const int z = (int)(q / (unsigned)g.N[1]);
-  const int y = (int)q - z * g.N[1];
+                                                          LeightOutput out, HeavyList mid, HeavyList huge, int y0,
+                                                          int z0, int q0) {
+  // block (coil group, x run): a cell's coil groups in adjacent lanes; grid
+  // (x runs, y, z): no index division
+  const int x = blockIdx.x * blockDim.y + threadIdx.y;
+  if (x >= g.N[0]) return;
+  const int y = y0 + blockIdx.y, z = z0 + blockIdx.z;
+  const int c0 = (q0 + (int)threadIdx.x) * CPT;
+  const int cell = x + g.N[0] * (y + g.N[1] * z);
   const int nW = NW ? NW : g.nWin, dim = DIM ? DIM : g.imDim;
   const int W1 = dim > 1 ? nW : 1, R = W1 * (dim > 2 ? nW : 1);
   constexpr int RS = NW ? (DIM == 3 ? NW * NW : (DIM == 2 ? NW : 1)) : 1;  // rows held in registers
@@ -851,8 +851,9 @@ __global__ void __launch_bounds__(256) leight_cell_kernel(LeightGeom g, CornerGr
   }
   if (total > kHeavyIncidences) {
     if (c0 == 0) {
-      const int h = atomicAdd(heavy.count, 1);
-      if (h < heavy.cap) heavy.cells[h] = (int)cell;
+      const HeavyList& L = total > kHugeIncidences || R > kMidRows ? huge : mid;
+      const int h = atomicAdd(L.count, 1);
+      if (h < L.cap) L.cells[h] = cell;
     }
     return;
   }
@@ -913,13 +914,123 @@ __global__ void __launch_bounds__(256) leight_cell_kernel(LeightGeom g, CornerGr
   store_coils<CPT>(out.re, out.im, (long long)cell * g.nCh + c0, ar, ai);
 }
 
-// Heavy cells: a persistent grid, one CTA per listed cell at a time.  The
-// 256 threads split each window row's run (thread t takes entries t, t +
-// 256, ...), accumulate kHeavyCoils coils per pass, and the CTA sums the
-// thread partials in a fixed tree (warp shuffles, then the eight warps in
-// order): deterministic.  VEC4: nCh % 4 == 0 and 16-byte aligned input.
-constexpr int kHeavyCoils = 16;
+// Sums the coil chunk c0 .. c0 + nc of the cell's entries i = first, first +
+// step, ... < T; the window rows' run starts b[r] and entry prefixes pre[r]
+// (pre[0] = 0, pre[R] = T) are in shared memory.
+template <bool VEC4>
+__device__ __forceinline__ void heavy_partial(const LeightGeom& g, const int* b, const int* pre, int T, int first,
+                                              int step, const float4* __restrict__ rec, const int* __restrict__ sidx,
+                                              const LeightInputs& in, int c0, int nc, float fx, float fy, float fz,
+                                              float* ar, float* ai, float& ws) {
+  int r = 0;
+  for (int i = first; i < T; i += step) {  // the rows' runs as one list
+    while (pre[r + 1] <= i) ++r;
+    const int k = b[r] + (i - pre[r]);
+    const float4 rc = __ldg(rec + k);
+    const long long o = (long long)__ldg(sidx + k) * g.nCh + c0;
+    const float w = cell_weight(g, rc, fx, fy, fz);
+    ws = __fadd_rn(ws, w);
+    if (VEC4) {
+#pragma unroll
+      for (int c4 = 0; c4 < kHeavyCoils / 4; ++c4) {
+        if (4 * c4 >= nc) break;
+        float vr[4], vi[4];
+        load_coils<4>(in.re, in.im, o + 4 * c4, vr, vi);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          ar[4 * c4 + c] = __fmaf_rn(w, vr[c], ar[4 * c4 + c]);
+          ai[4 * c4 + c] = __fmaf_rn(w, vi[c], ai[4 * c4 + c]);
+        }
+      }
+    } else {
+#pragma unroll
+      for (int c = 0; c < kHeavyCoils; ++c) {
+        if (c >= nc) break;
+        ar[c] = __fmaf_rn(w, __ldg(in.re + o + c), ar[c]);
+        ai[c] = __fmaf_rn(w, __ldg(in.im + o + c), ai[c]);
+      }
+    }
+  }
+}
 
+// Warp sum of the coil partials in a fixed butterfly order: every lane ends
+// with the totals.
+__device__ __forceinline__ void warp_sum_coils(float* ar, float* ai, float& ws) {
+#pragma unroll
+  for (int sh = 16; sh > 0; sh >>= 1) {
+    ws += __shfl_xor_sync(0xffffffffu, ws, sh);
+#pragma unroll
+    for (int c = 0; c < kHeavyCoils; ++c) {
+      ar[c] += __shfl_xor_sync(0xffffffffu, ar[c], sh);
+      ai[c] += __shfl_xor_sync(0xffffffffu, ai[c], sh);
+    }
+  }
+}
+
+// Mid cells (kHeavyIncidences < T <= kHugeIncidences, at most kMidRows
+// window rows): a persistent grid of warps, one warp per listed cell at a
+// time; lane r loads window row r's run, a warp scan forms the prefixes, the
+// lanes split the entries and a butterfly sums them (deterministic).
+template <bool VEC4>
+__global__ void __launch_bounds__(256) leight_mid_kernel(LeightGeom g, CornerGrid e, const int* __restrict__ off,
+                                                         const int* __restrict__ sidx, const float4* __restrict__ rec,
+                                                         LeightInputs in, LeightOutput out, HeavyList mid) {
+  __shared__ int s_b[8][kMidRows], s_pre[8][kMidRows + 1];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nm = (int)min((long long)*mid.count, mid.cap);
+  const int nW = g.nWin, W1 = g.imDim > 1 ? nW : 1, R = W1 * (g.imDim > 2 ? nW : 1);
+  for (int h = blockIdx.x * 8 + warp; h < nm; h += gridDim.x * 8) {
+    const int cell = mid.cells[h];
+    const unsigned q = (unsigned)cell / (unsigned)g.N[0];
+    const int x = cell - (int)q * g.N[0];
+    const int z = (int)(q / (unsigned)g.N[1]);
+    const int y = (int)q - z * g.N[1];
+    int b = 0, len = 0;
+    if (lane < R) {
+      const int rk = x + e.E[0] * ((y + lane % W1) + e.E[1] * (z + lane / W1));
+      b = __ldg(off + rk);
+      len = __ldg(off + rk + nW) - b;
+    }
+    int incl = len;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    __syncwarp();  // the previous cell's rows are read
+    if (lane < R) {
+      s_b[warp][lane] = b;
+      s_pre[warp][lane + 1] = incl;
+    }
+    if (lane == 0) s_pre[warp][0] = 0;
+    const int T = __shfl_sync(0xffffffffu, incl, 31);
+    __syncwarp();
+    const float fx = (float)(x + 1), fy = (float)(y + 1), fz = (float)(z + 1);
+    for (int c0 = 0; c0 < g.nCh; c0 += kHeavyCoils) {
+      const int nc = min(kHeavyCoils, g.nCh - c0);
+      float ar[kHeavyCoils], ai[kHeavyCoils], ws = 0.f;
+#pragma unroll
+      for (int c = 0; c < kHeavyCoils; ++c) ar[c] = ai[c] = 0.f;
+      heavy_partial<VEC4>(g, s_b[warp], s_pre[warp], T, lane, 32, rec, sidx, in, c0, nc, fx, fy, fz, ar, ai, ws);
+      warp_sum_coils(ar, ai, ws);
+      const float inv = ws < 1e-5f ? 1.0f : __frcp_rn(ws);  // as in leight_cell_kernel
+#pragma unroll
+      for (int c = 0; c < kHeavyCoils; ++c) {
+        if (lane == c && c < nc) {
+          out.re[(long long)cell * g.nCh + c0 + c] = __fmul_rn(ar[c], inv);
+          out.im[(long long)cell * g.nCh + c0 + c] = __fmul_rn(ai[c], inv);
+        }
+      }
+    }
+  }
+}
+
+// Huge cells (more than kHugeIncidences entries, or more than kMidRows
+// window rows): a persistent grid, one CTA per listed cell at a time.  The
+// 256 threads split the cell's entries (thread t takes t, t + 256, ...),
+// accumulate kHeavyCoils coils per pass, and the CTA sums the thread
+// partials in a fixed tree (warp butterflies, then the eight warps in
+// order): deterministic.  VEC4: nCh % 4 == 0 and 16-byte aligned input.
 template <bool VEC4>
 __global__ void __launch_bounds__(256) leight_heavy_kernel(LeightGeom g, CornerGrid e, const int* __restrict__ off,
                                                            const int* __restrict__ sidx,
@@ -948,54 +1059,14 @@ __global__ void __launch_bounds__(256) leight_heavy_kernel(LeightGeom g, CornerG
     }
     __syncthreads();
     const int T = s_pre[R];
+    const float fx = (float)(x + 1), fy = (float)(y + 1), fz = (float)(z + 1);
     for (int c0 = 0; c0 < g.nCh; c0 += kHeavyCoils) {
       const int nc = min(kHeavyCoils, g.nCh - c0);
       float ar[kHeavyCoils], ai[kHeavyCoils], ws = 0.f;
 #pragma unroll
       for (int c = 0; c < kHeavyCoils; ++c) ar[c] = ai[c] = 0.f;
-      {
-        const float fx = (float)(x + 1), fy = (float)(y + 1), fz = (float)(z + 1);
-        int r = 0;
-        for (int i = threadIdx.x; i < T; i += 256) {  // the rows' runs as one list
-          while (s_pre[r + 1] <= i) ++r;
-          {
-            const int k = s_b[r] + (i - s_pre[r]);
-            const float4 rc = __ldg(rec + k);
-            const long long o = (long long)__ldg(sidx + k) * g.nCh + c0;
-            const float w = cell_weight(g, rc, fx, fy, fz);
-            ws = __fadd_rn(ws, w);
-            if (VEC4) {
-#pragma unroll
-              for (int c4 = 0; c4 < kHeavyCoils / 4; ++c4) {
-                if (4 * c4 >= nc) break;
-                float vr[4], vi[4];
-                load_coils<4>(in.re, in.im, o + 4 * c4, vr, vi);
-#pragma unroll
-                for (int c = 0; c < 4; ++c) {
-                  ar[4 * c4 + c] = __fmaf_rn(w, vr[c], ar[4 * c4 + c]);
-                  ai[4 * c4 + c] = __fmaf_rn(w, vi[c], ai[4 * c4 + c]);
-                }
-              }
-            } else {
-#pragma unroll
-              for (int c = 0; c < kHeavyCoils; ++c) {
-                if (c >= nc) break;
-                ar[c] = __fmaf_rn(w, __ldg(in.re + o + c), ar[c]);
-                ai[c] = __fmaf_rn(w, __ldg(in.im + o + c), ai[c]);
-              }
-            }
-          }
-        }
-      }
-#pragma unroll
-      for (int sh = 16; sh > 0; sh >>= 1) {
-        ws += __shfl_down_sync(0xffffffffu, ws, sh);
-#pragma unroll
-        for (int c = 0; c < kHeavyCoils; ++c) {
-          ar[c] += __shfl_down_sync(0xffffffffu, ar[c], sh);
-          ai[c] += __shfl_down_sync(0xffffffffu, ai[c], sh);
-        }
-      }
+      heavy_partial<VEC4>(g, s_b, s_pre, T, threadIdx.x, 256, rec, sidx, in, c0, nc, fx, fy, fz, ar, ai, ws);
+      warp_sum_coils(ar, ai, ws);
       if (lane == 0) {
         red[warp][0] = ws;
 #pragma unroll
@@ -1032,33 +1103,41 @@ struct CellLaunch {
   const float4* rec;
   const LeightInputs& in;
   const LeightOutput& out;
-  const HeavyList& heavy;
+  const HeavyList& mid;
+  const HeavyList& huge;
   cudaStream_t s;
 };
 
-// Compile-time rows for the common 3-wide windows in 2-D and 3-D; the grid
-// cells in ranges of fewer than 2^31 threads per launch.
+// Compile-time rows for the common 3-wide windows in 2-D and 3-D.  Blocks
+// of (coil group, x run of >= 32) threads, at most 256, so at most 8 groups
+// per launch; the grid spans x runs, y and z, in launches of at most 65535
+// along y and z.
 template <int CPT>
 void launch_cells(const CellLaunch& c) {
-  const long long Q = c.g.nCh / CPT;
-  const long long per = ((1LL << 31) - 256) / Q;  // cells per launch
-  for (long long c0 = 0; c0 < c.g.Nu_tot; c0 += per) {
-    const int b = (int)c0, en = (int)std::min(c.g.Nu_tot, c0 + per);
-    const unsigned blocks = (unsigned)(((long long)(en - b) * Q + 255) / 256);
-    if (c.g.nWin == 3 && c.g.imDim == 3)
-      leight_cell_kernel<CPT, 3, 3><<<blocks, 256, 0, c.s>>>(c.g, c.e, c.off, c.sidx, c.rec, c.in, c.out, c.heavy, b,
-                                                             en);
-    else if (c.g.nWin == 3 && c.g.imDim == 2)
-      leight_cell_kernel<CPT, 3, 2><<<blocks, 256, 0, c.s>>>(c.g, c.e, c.off, c.sidx, c.rec, c.in, c.out, c.heavy, b,
-                                                             en);
-    else
-      leight_cell_kernel<CPT, 0, 0><<<blocks, 256, 0, c.s>>>(c.g, c.e, c.off, c.sidx, c.rec, c.in, c.out, c.heavy, b,
-                                                             en);
+  const int Q = c.g.nCh / CPT, N0 = c.g.N[0], N1 = c.g.N[1], N2 = c.g.N[2];
+  for (int q0 = 0; q0 < Q; q0 += 8) {
+    const int nq = std::min(8, Q - q0);
+    int bx = std::max(32, 256 / nq / 32 * 32);
+    bx = std::min(bx, (N0 + 31) / 32 * 32);
+    const dim3 block(nq, bx);
+    for (int z0 = 0; z0 < N2; z0 += 65535)
+      for (int y0 = 0; y0 < N1; y0 += 65535) {
+        const dim3 grid((N0 + bx - 1) / bx, std::min(65535, N1 - y0), std::min(65535, N2 - z0));
+        if (c.g.nWin == 3 && c.g.imDim == 3)
+          leight_cell_kernel<CPT, 3, 3><<<grid, block, 0, c.s>>>(c.g, c.e, c.off, c.sidx, c.rec, c.in, c.out, c.mid,
+                                                                 c.huge, y0, z0, q0);
+        else if (c.g.nWin == 3 && c.g.imDim == 2)
+          leight_cell_kernel<CPT, 3, 2><<<grid, block, 0, c.s>>>(c.g, c.e, c.off, c.sidx, c.rec, c.in, c.out, c.mid,
+                                                                 c.huge, y0, z0, q0);
+        else
+          leight_cell_kernel<CPT, 0, 0><<<grid, block, 0, c.s>>>(c.g, c.e, c.off, c.sidx, c.rec, c.in, c.out, c.mid,
+                                                                 c.huge, y0, z0, q0);
+      }
   }
 }
 
 struct CellsLayout {
-  size_t count, off, keys_in, keys_out, idx_in, idx_out, rec, heavy, heavy_n, scan_tmp, sort_tmp, total;
+  size_t count, off, keys_in, keys_out, idx_in, idx_out, rec, mid, huge, lists_n, scan_tmp, sort_tmp, total;
   long long heavy_cap;
 };
 
@@ -1089,8 +1168,9 @@ CellsLayout cells_layout(const LeightGeom& g, int nPt) {
   long long wc = 1;
   for (int d = 0; d < g.imDim; ++d) wc *= g.nWin;
   L.heavy_cap = std::min<long long>(g.Nu_tot, (long long)nPt * wc / (kHeavyIncidences + 1) + 1);
-  L.heavy = take((size_t)L.heavy_cap * 4);
-  L.heavy_n = take(4);
+  L.mid = take((size_t)L.heavy_cap * 4);
+  L.huge = take((size_t)L.heavy_cap * 4);
+  L.lists_n = take(8);
   L.scan_tmp = take(scan_tmp);
   L.sort_tmp = take(sort_tmp);
   L.total = p;
@@ -1148,12 +1228,14 @@ int leight_run_cells(const LeightGeom& g, const LeightInputs& in, int nPt, const
     cpt = g.nCh;
   else if (g.nCh % 2 == 0 && a8)
     cpt = 2;
-  HeavyList heavy;
-  heavy.cells = reinterpret_cast<int*>(base + L.heavy);
-  heavy.count = reinterpret_cast<int*>(base + L.heavy_n);
-  heavy.cap = L.heavy_cap;
-  MLG_CUDA(cudaMemsetAsync(heavy.count, 0, 4, s));
-  const CellLaunch cl{g, e, off, idx_out, rec, in, out, heavy, s};
+  HeavyList mid, huge;
+  mid.cells = reinterpret_cast<int*>(base + L.mid);
+  huge.cells = reinterpret_cast<int*>(base + L.huge);
+  mid.count = reinterpret_cast<int*>(base + L.lists_n);
+  huge.count = mid.count + 1;
+  mid.cap = huge.cap = L.heavy_cap;
+  MLG_CUDA(cudaMemsetAsync(mid.count, 0, 8, s));
+  const CellLaunch cl{g, e, off, idx_out, rec, in, out, mid, huge, s};
   switch (cpt) {
     case 7:
       launch_cells<7>(cl);
@@ -1180,12 +1262,17 @@ int leight_run_cells(const LeightGeom& g, const LeightInputs& in, int nPt, const
       launch_cells<1>(cl);
   }
   MLG_LAUNCHED();
-  if (nPt > 0) {
+  if (nPt > 0) {  // persistent grids over the lists (lengths read on the device)
+    const bool vec4 = (g.nCh % 4) == 0 && ((uintptr_t)in.re | (uintptr_t)in.im) % 16 == 0;
+    const int mb = (int)std::min<long long>((L.heavy_cap + 7) / 8, 148LL * 8);
     const int hb = (int)std::min<long long>(L.heavy_cap, 148LL * 4);
-    if ((g.nCh % 4) == 0 && ((uintptr_t)in.re | (uintptr_t)in.im) % 16 == 0)
-      leight_heavy_kernel<true><<<hb, 256, 0, s>>>(g, e, off, idx_out, rec, in, out, heavy);
-    else
-      leight_heavy_kernel<false><<<hb, 256, 0, s>>>(g, e, off, idx_out, rec, in, out, heavy);
+    if (vec4) {
+      leight_mid_kernel<true><<<mb, 256, 0, s>>>(g, e, off, idx_out, rec, in, out, mid);
+      leight_heavy_kernel<true><<<hb, 256, 0, s>>>(g, e, off, idx_out, rec, in, out, huge);
+    } else {
+      leight_mid_kernel<false><<<mb, 256, 0, s>>>(g, e, off, idx_out, rec, in, out, mid);
+      leight_heavy_kernel<false><<<hb, 256, 0, s>>>(g, e, off, idx_out, rec, in, out, huge);
+    }
     MLG_LAUNCHED();
   }
   return MLG_OK;
