@@ -814,7 +814,7 @@ struct HeavyList {
 // issue would otherwise wait for each row's two loads in turn); 0: taken
 // from g.
 template <int CPT, int NW, int DIM>
-__global__ void __launch_bounds__(256) leight_cell_kernel(LeightGeom g, CornerGrid e, const int* __restrict__ off,
+__global__ void __launch_bounds__(256, 4) leight_cell_kernel(LeightGeom g, CornerGrid e, const int* __restrict__ off,
                                                           const int* __restrict__ sidx,
                                                           const float4* __restrict__ rec, LeightInputs in,
                                                           LeightOutput out, HeavyList mid, HeavyList huge, int y0,

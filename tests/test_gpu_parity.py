@@ -126,10 +126,10 @@ def _dense_case(imDim, N, nCh, nPt, seed):
                                                   (3, 32, 5, 3, 60000), (3, 24, 6, 3, 30000), (2, 64, 7, 3, 40000),
                                                   (3, 20, 8, 2, 20000)])
 def test_leight_heavy_bins_match_port(imDim, N, nCh, nWin, nPt):
-    """Dense central sampling: cells covered by more than 64 samples take the
-    CTA-per-cell path, the rest a thread per (cell, coil group) with 1 to 8
-    coils per thread; 3-wide windows in 2-D and 3-D have their own compiled
-    forms.  Compared with the bit-exact C restatement."""
+    """Dense central sampling: cells covered by more than 64 samples take a
+    warp or (beyond 2048) a CTA each, the rest a thread per (cell, coil
+    group) with 1 to 8 coils per thread; 3-wide windows in 2-D and 3-D have
+    their own compiled forms.  Compared with the bit-exact C restatement."""
     from monalisa_b200 import _native as NN
 
     t, aR, aI, Dn = _dense_case(imDim, N, nCh, nPt, 11 + imDim)
