@@ -281,22 +281,32 @@ __device__ __forceinline__ void st_pair(void* base, long long i, float4 v, float
   }
 }
 
-template <bool OUT_H, bool CONTRACT>
-__global__ void __launch_bounds__(256, 6) spmm_pair_kernel(SpmmParams p, const int* __restrict__ rows,
-                                                        const uint2* __restrict__ bounds, int n_rows) {
+// PPT coil pairs per thread: the row's bounds and each entry's column and
+// value are loaded once for PPT pairs.  Per coil the entries are summed in
+// the same order for every PPT, so the outputs do not depend on it.
+template <int PPT>
+constexpr int pair_min_blocks() {
+  return PPT == 1 ? 6 : (PPT == 2 ? 5 : 4);
+}
+
+template <bool OUT_H, bool CONTRACT, int PPT>
+__global__ void __launch_bounds__(256, pair_min_blocks<PPT>()) spmm_pair_kernel(SpmmParams p,
+                                                                               const int* __restrict__ rows,
+                                                                               const uint2* __restrict__ bounds,
+                                                                               int n_rows) {
   __shared__ double sh[32];
-  const int P = p.nCh >> 1;
+  const int P = p.nCh >> 1, G = P / PPT;  // pairs per row, thread groups per row
   const long long i0 = (long long)blockIdx.x * p.rows_per_block;
   const int nr = (int)min((long long)p.rows_per_block, (long long)n_rows - i0);
-  const int total = nr * P;
+  const int total = nr * G;
   const bool scale = p.in_row_scale != nullptr;
   const float so = OUT_H ? __ldg(p.out.scale) : 0.f;
   float amax = 0.f;
   double sq = 0.0;
-  // item -> row, coil pair and entry range (empty for rows the segment kernels own)
+  // item -> row, first coil pair and entry range (empty for rows the segment kernels own)
   auto fetch = [&](int it, long long& r, int& pi, uint32_t& b, uint32_t& n) {
-    const int lr = it / P;
-    pi = it - lr * P;
+    const int lr = it / G;
+    pi = (it - lr * G) * PPT;
     uint32_t e;
     if (rows) {  // listed rows: bounds loaded beside the row index, not after it
       r = __ldg(rows + i0 + lr);
@@ -310,37 +320,43 @@ __global__ void __launch_bounds__(256, 6) spmm_pair_kernel(SpmmParams p, const i
     }
     n = e - b;
   };
-  auto entry = [&](uint32_t k, int pi, float4& acc) {
+  auto entry = [&](uint32_t k, int pi, float4* acc) {
     const int j = __ldg(p.col + k);
     float m = val_at(p, k);
-    float4 v = __ldg(reinterpret_cast<const float4*>(p.in.a) + (long long)j * P + pi);
+    const float4* src = reinterpret_cast<const float4*>(p.in.a) + (long long)j * P + pi;
+    float4 v[PPT];
+#pragma unroll
+    for (int u = 0; u < PPT; ++u) v[u] = __ldg(src + u);
     if constexpr (CONTRACT) {
       if (scale) m = __fmul_rn(m, __ldg(p.in_row_scale + j));
-      acc.x = __fmaf_rn(m, v.x, acc.x);
-      acc.y = __fmaf_rn(m, v.y, acc.y);
-      acc.z = __fmaf_rn(m, v.z, acc.z);
-      acc.w = __fmaf_rn(m, v.w, acc.w);
-    } else {
-      if (scale) {
-        const float h = __ldg(p.in_row_scale + j);
-        v = make_float4(__fmul_rn(h, v.x), __fmul_rn(h, v.y), __fmul_rn(h, v.z), __fmul_rn(h, v.w));
+#pragma unroll
+      for (int u = 0; u < PPT; ++u) {
+        acc[u].x = __fmaf_rn(m, v[u].x, acc[u].x);
+        acc[u].y = __fmaf_rn(m, v[u].y, acc[u].y);
+        acc[u].z = __fmaf_rn(m, v[u].z, acc[u].z);
+        acc[u].w = __fmaf_rn(m, v[u].w, acc[u].w);
       }
-      acc.x = __fadd_rn(acc.x, __fmul_rn(m, v.x));
-      acc.y = __fadd_rn(acc.y, __fmul_rn(m, v.y));
-      acc.z = __fadd_rn(acc.z, __fmul_rn(m, v.z));
-      acc.w = __fadd_rn(acc.w, __fmul_rn(m, v.w));
+    } else {
+      const float h = scale ? __ldg(p.in_row_scale + j) : 1.f;
+#pragma unroll
+      for (int u = 0; u < PPT; ++u) {
+        float4 w = v[u];
+        if (scale) w = make_float4(__fmul_rn(h, w.x), __fmul_rn(h, w.y), __fmul_rn(h, w.z), __fmul_rn(h, w.w));
+        acc[u].x = __fadd_rn(acc[u].x, __fmul_rn(m, w.x));
+        acc[u].y = __fadd_rn(acc[u].y, __fmul_rn(m, w.y));
+        acc[u].z = __fadd_rn(acc[u].z, __fmul_rn(m, w.z));
+        acc[u].w = __fadd_rn(acc[u].w, __fmul_rn(m, w.w));
+      }
     }
   };
-  auto finish_item = [&](long long r, int pi, float4 acc) {
+  auto finish_pair = [&](long long r, int pi, float4 acc, double w) {
     if (p.out_scale != 1.0f)
       acc = make_float4(__fmul_rn(acc.x, p.out_scale), __fmul_rn(acc.y, p.out_scale), __fmul_rn(acc.z, p.out_scale),
                         __fmul_rn(acc.w, p.out_scale));
     st_pair<OUT_H>(p.out.a, r * P + pi, acc, so);
     amax = fmaxf(amax, abs_max4(acc));
-    if (p.partial) {
-      const double w = p.sqn_w ? (double)__ldg(p.sqn_w + r) : 1.0;
+    if (p.partial)
       sq += w * ((double)acc.x * acc.x + (double)acc.y * acc.y + (double)acc.z * acc.z + (double)acc.w * acc.w);
-    }
   };
   for (int it = threadIdx.x; it < total; it += blockDim.x) {
     long long r;
@@ -348,10 +364,14 @@ __global__ void __launch_bounds__(256, 6) spmm_pair_kernel(SpmmParams p, const i
     uint32_t b, n;
     fetch(it, r, pi, b, n);
     if (n > (uint32_t)kLongRow) continue;  // segment kernels own it
-    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-#pragma unroll 4
+    float4 acc[PPT];
+#pragma unroll
+    for (int u = 0; u < PPT; ++u) acc[u] = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll(PPT == 1 ? 4 : 2)
     for (uint32_t k = b; k < b + n; ++k) entry(k, pi, acc);
-    finish_item(r, pi, acc);
+    const double w = p.partial && p.sqn_w ? (double)__ldg(p.sqn_w + r) : 1.0;
+#pragma unroll
+    for (int u = 0; u < PPT; ++u) finish_pair(r, pi + u, acc[u], w);
   }
   if (p.absmax) warp_absmax(p.absmax, amax);
   if (p.partial) {
@@ -360,19 +380,30 @@ __global__ void __launch_bounds__(256, 6) spmm_pair_kernel(SpmmParams p, const i
   }
 }
 
-static void launch_pair(bool out_h, bool contract, const SpmmParams& p, const int* rows, const uint2* rp, int nrows,
-                        int grid, cudaStream_t s) {
+template <int PPT>
+static void launch_pair_ppt(bool out_h, bool contract, const SpmmParams& p, const int* rows, const uint2* rp,
+                            int nrows, int grid, cudaStream_t s) {
   if (contract) {
     if (out_h)
-      spmm_pair_kernel<true, true><<<grid, 256, 0, s>>>(p, rows, rp, nrows);
+      spmm_pair_kernel<true, true, PPT><<<grid, 256, 0, s>>>(p, rows, rp, nrows);
     else
-      spmm_pair_kernel<false, true><<<grid, 256, 0, s>>>(p, rows, rp, nrows);
+      spmm_pair_kernel<false, true, PPT><<<grid, 256, 0, s>>>(p, rows, rp, nrows);
   } else {
     if (out_h)
-      spmm_pair_kernel<true, false><<<grid, 256, 0, s>>>(p, rows, rp, nrows);
+      spmm_pair_kernel<true, false, PPT><<<grid, 256, 0, s>>>(p, rows, rp, nrows);
     else
-      spmm_pair_kernel<false, false><<<grid, 256, 0, s>>>(p, rows, rp, nrows);
+      spmm_pair_kernel<false, false, PPT><<<grid, 256, 0, s>>>(p, rows, rp, nrows);
   }
+}
+
+static void launch_pair(int ppt, bool out_h, bool contract, const SpmmParams& p, const int* rows, const uint2* rp,
+                        int nrows, int grid, cudaStream_t s) {
+  if (ppt == 4)
+    launch_pair_ppt<4>(out_h, contract, p, rows, rp, nrows, grid, s);
+  else if (ppt == 2)
+    launch_pair_ppt<2>(out_h, contract, p, rows, rp, nrows, grid, s);
+  else
+    launch_pair_ppt<1>(out_h, contract, p, rows, rp, nrows, grid, s);
 }
 
 static bool use_pair_kernel(const SpmmArgs& a) {
@@ -381,8 +412,13 @@ static bool use_pair_kernel(const SpmmArgs& a) {
          !a.normalize;
 }
 
+// Coil pairs per thread of the pair kernel: two when the pair count is even
+// (c2, 16 coils: Gu 0.43 -> 0.40 ms, Gut 0.760 -> 0.757 ms; four pairs
+// lose more to occupancy than they save: 0.69 / 0.90 ms).
+static int pair_ppt(const SpmmArgs& a) { return (a.nCh / 2) % 2 == 0 ? 2 : 1; }
+
 static int rows_per_block(const SpmmArgs& a) {
-  if (use_pair_kernel(a)) return std::max(1, 1024 / (a.nCh / 2));
+  if (use_pair_kernel(a)) return std::max(1, 1024 / (a.nCh / 2 / pair_ppt(a)));
   return std::max(1, 1024 / std::max(1, a.nCh));
 }
 
@@ -456,7 +492,7 @@ int spmm(const SpmmArgs& a, cudaStream_t s) {
       // the matrix's processing order when it covers the requested rows
       const bool ordered = m.ord_rows && m.ord_nonempty == a.nonempty_only;
       MLG_CHECK(ordered || !a.nonempty_only, "non-empty-row products need the ordered row list");
-      launch_pair(oh, a.contract, p, ordered ? m.ord_rows : nullptr, ordered ? m.ord_bounds : nullptr, (int)nrows,
+      launch_pair(pair_ppt(a), oh, a.contract, p, ordered ? m.ord_rows : nullptr, ordered ? m.ord_bounds : nullptr, (int)nrows,
                   grid_short, s);
       MLG_LAUNCHED();
     }
