@@ -412,10 +412,17 @@ static bool use_pair_kernel(const SpmmArgs& a) {
          !a.normalize;
 }
 
-// Coil pairs per thread of the pair kernel: two when the pair count is even
-// (c2, 16 coils: Gu 0.43 -> 0.40 ms, Gut 0.760 -> 0.757 ms; four pairs
-// lose more to occupancy than they save: 0.69 / 0.90 ms).
-static int pair_ppt(const SpmmArgs& a) { return (a.nCh / 2) % 2 == 0 ? 2 : 1; }
+// Coil pairs per thread of the pair kernel, as measured on a B200: two for
+// products over all rows with at least 8 (an even number of) coil pairs --
+// Gu of the 4096 x 256-sample, 16-coil koosh case 0.43 -> 0.40 ms, of a
+// 1500 x 256-sample one 0.178 -> 0.181 ms; one otherwise: with 12 or 8
+// coils two pairs were slower (Gu 0.37 -> 0.46 ms), and so were the
+// non-empty-row products Gut (0.37 -> 0.43 ms at 16 coils, 1500 spokes).
+// Four pairs lost more to occupancy than they saved (Gu 0.69 ms).
+static int pair_ppt(const SpmmArgs& a) {
+  const int P = a.nCh / 2;
+  return !a.nonempty_only && P >= 8 && P % 2 == 0 ? 2 : 1;
+}
 
 static int rows_per_block(const SpmmArgs& a) {
   if (use_pair_kernel(a)) return std::max(1, 1024 / (a.nCh / 2 / pair_ppt(a)));
