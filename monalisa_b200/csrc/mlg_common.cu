@@ -125,9 +125,13 @@ __global__ void nz_rows_kernel(const uint32_t* __restrict__ mask, const int* __r
 
 // brick key of row i (rows[i], or i): its cell (the row itself, or the
 // column of its first entry when by_first_col; empty rows sort last)
+// split: rows with more than kMidRow entries get the key's top bit (they
+// sort after the others, each group in brick order) and are counted in
+// n_mid.
 __global__ void order_keys_kernel(const uint32_t* __restrict__ row_ptr, const int* __restrict__ col,
                                   const int* __restrict__ rows, int n, int by_first_col, int N0, int N1, int nbx,
-                                  int nby, uint32_t* __restrict__ keys, int* __restrict__ vals) {
+                                  int nby, bool split, uint32_t* __restrict__ keys, int* __restrict__ vals,
+                                  int* __restrict__ n_mid) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const int r = rows ? rows[i] : i;
     vals[i] = r;
@@ -142,7 +146,12 @@ __global__ void order_keys_kernel(const uint32_t* __restrict__ row_ptr, const in
     }
     const long long x = cell % N0, t = cell / N0, y = t % N1, z = t / N1;
     const long long brick = (x >> 3) + nbx * ((y >> 3) + (long long)nby * (z >> 3));
-    keys[i] = (uint32_t)(brick * 512 + (x & 7) + 8 * ((y & 7) + 8 * (z & 7)));
+    uint32_t key = (uint32_t)(brick * 512 + (x & 7) + 8 * ((y & 7) + 8 * (z & 7)));
+    if (split && row_ptr[r + 1] - row_ptr[r] > (uint32_t)kMidRow) {
+      key |= 0x80000000u;
+      atomicAdd(n_mid, 1);
+    }
+    keys[i] = key;
   }
 }
 
@@ -159,16 +168,23 @@ int csr_build_order(Csr& c, const int* N, bool nonempty, cudaStream_t s) {
   MLG_CHECK(!nonempty || c.nz_rows, "ordered non-empty rows need the row list");
   const int n = nonempty ? c.n_nonempty : c.l_size;
   const int nbx = (N[0] + 7) / 8, nby = (N[1] + 7) / 8, nbz = (N[2] + 7) / 8;
-  if ((double)nbx * nby * nbz * 512.0 >= 4294967295.0) return MLG_OK;  // keys would not fit: keep row order
+  const double nkeys = (double)nbx * nby * nbz * 512.0;
+  if (nkeys >= 4294967295.0) return MLG_OK;  // keys would not fit: keep row order
+  // non-empty rows: short rows first when the keys leave the top bit free
+  const bool split = nonempty && nkeys < 2147483648.0;
   DevBuf<uint32_t> keys, keys_out;
-  DevBuf<int> vals;
+  DevBuf<int> vals, n_mid;
   MLG_TRY(keys.alloc((size_t)std::max(1, n), s));
   MLG_TRY(keys_out.alloc((size_t)std::max(1, n), s));
   MLG_TRY(vals.alloc((size_t)std::max(1, n), s));
+  MLG_TRY(n_mid.alloc(1, s));
+  MLG_CUDA(cudaMemsetAsync(n_mid.p, 0, sizeof(int), s));
   const int g = std::max(1, std::min(4096, (n + 255) / 256));
   order_keys_kernel<<<g, 256, 0, s>>>(c.row_ptr, c.col, nonempty ? c.nz_rows : nullptr, n, nonempty ? 0 : 1, N[0],
-                                      N[1], nbx, nby, keys.p, vals.p);
+                                      N[1], nbx, nby, split, keys.p, vals.p, n_mid.p);
   count_launch();
+  int h_mid = 0;
+  MLG_CUDA(cudaMemcpyAsync(&h_mid, n_mid.p, sizeof(int), cudaMemcpyDeviceToHost, s));
   int* ord = nullptr;
   uint2* bounds = nullptr;
   MLG_CUDA(cudaMalloc(&ord, sizeof(int) * (size_t)std::max(1, n)));
@@ -196,6 +212,7 @@ int csr_build_order(Csr& c, const int* N, bool nonempty, cudaStream_t s) {
   c.ord_bounds = bounds;
   c.n_ord = n;
   c.ord_nonempty = nonempty;
+  c.ord_short = split ? n - h_mid : -1;
   return MLG_OK;
 }
 

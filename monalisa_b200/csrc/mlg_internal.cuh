@@ -104,6 +104,11 @@ struct DevBuf {
 // jump format squeezes out are empty).  Long rows (more than kLongRow
 // entries) are listed separately so that one CTA can split them.
 constexpr int kLongRow = 256;
+// rows with more than kMidRow (and at most kLongRow) entries are gathered by
+// a warp each inside the operators (measured on Gut: 16, 32, 64, 128 entries
+// gave 0.797 / 0.769 / 0.757 / 0.749 ms on the 4096-spoke 16-coil koosh
+// case and 0.243 / 0.233 / 0.228 / 0.266 ms on a 1500-spoke 12-coil one)
+constexpr int kMidRow = 64;
 
 struct Csr {
   int r_size = 0;         // number of columns
@@ -135,6 +140,9 @@ struct Csr {
   uint2* ord_bounds = nullptr;
   int n_ord = 0;
   bool ord_nonempty = false;
+  // non-empty order only: the first ord_short rows have at most kMidRow
+  // entries, the rest more (each part in block order); -1: not split
+  int ord_short = -1;
   // FP16 copy of val for the mixed-precision solver (built on demand)
   __half* val_h = nullptr;
 };

@@ -281,6 +281,60 @@ __device__ __forceinline__ void st_pair(void* base, long long i, float4 v, float
   }
 }
 
+struct MidRows {
+  const int* rows = nullptr;
+  const uint2* bounds = nullptr;
+  int n = 0;
+  int blocks = 0;
+};
+
+// Rows with kMidRow < n <= kLongRow entries inside the operators (CONTRACT
+// semantics, FP32 point layout in and out, no partials): a warp per row at
+// a time, lane = (entry group eg, coil pair pi) for P <= 16 pairs, EG = 32 /
+// P groups; group eg takes entries eg, eg + EG, ... and the groups' sums are
+// added in group order (a fixed order: deterministic, but not the row's
+// stored order).
+__device__ __forceinline__ void mid_rows_block(const SpmmParams& p, const int* __restrict__ rows,
+                                               const uint2* __restrict__ bounds, int n_rows, int block,
+                                               int nblocks) {
+  const int P = p.nCh >> 1, EG = 32 / P;
+  const int lane = threadIdx.x & 31, eg = lane / P, pi = lane - eg * P;
+  const bool active = eg < EG;
+  const bool scale = p.in_row_scale != nullptr;
+  const float4* in = reinterpret_cast<const float4*>(p.in.a);
+  for (int i = block * 8 + (int)(threadIdx.x >> 5); i < n_rows; i += nblocks * 8) {
+    const uint2 be = __ldg(bounds + i);
+    if (be.y - be.x > (uint32_t)kLongRow) continue;  // segment kernels own it (uniform in the warp)
+    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (active) {
+      for (uint32_t k = be.x + eg; k < be.y; k += EG) {
+        const int j = __ldg(p.col + k);
+        float m = val_at(p, k);
+        if (scale) m = __fmul_rn(m, __ldg(p.in_row_scale + j));
+        const float4 v = __ldg(in + (long long)j * P + pi);
+        acc.x = __fmaf_rn(m, v.x, acc.x);
+        acc.y = __fmaf_rn(m, v.y, acc.y);
+        acc.z = __fmaf_rn(m, v.z, acc.z);
+        acc.w = __fmaf_rn(m, v.w, acc.w);
+      }
+    }
+    float4 s = acc;
+    for (int e = 1; e < EG; ++e) {  // lanes of group 0 add the other groups in order
+      const int src = pi + e * P;
+      s.x += __shfl_sync(0xffffffffu, acc.x, src);
+      s.y += __shfl_sync(0xffffffffu, acc.y, src);
+      s.z += __shfl_sync(0xffffffffu, acc.z, src);
+      s.w += __shfl_sync(0xffffffffu, acc.w, src);
+    }
+    if (eg == 0) {
+      if (p.out_scale != 1.0f)
+        s = make_float4(__fmul_rn(s.x, p.out_scale), __fmul_rn(s.y, p.out_scale), __fmul_rn(s.z, p.out_scale),
+                        __fmul_rn(s.w, p.out_scale));
+      reinterpret_cast<float4*>(p.out.a)[(long long)__ldg(rows + i) * P + pi] = s;
+    }
+  }
+}
+
 // PPT coil pairs per thread: the row's bounds and each entry's column and
 // value are loaded once for PPT pairs.  Per coil the entries are summed in
 // the same order for every PPT, so the outputs do not depend on it.
@@ -289,14 +343,22 @@ constexpr int pair_min_blocks() {
   return PPT == 1 ? 6 : (PPT == 2 ? 5 : 4);
 }
 
+// With mid_blocks > 0 (CONTRACT, FP32 output) the first mid_blocks blocks
+// gather the mid rows, a warp per row (mid_rows_block), and the others the
+// listed short rows: one launch, the long-running mid rows started first.
 template <bool OUT_H, bool CONTRACT, int PPT>
 __global__ void __launch_bounds__(256, pair_min_blocks<PPT>()) spmm_pair_kernel(SpmmParams p,
                                                                                const int* __restrict__ rows,
                                                                                const uint2* __restrict__ bounds,
-                                                                               int n_rows) {
+                                                                               int n_rows, MidRows mid) {
   __shared__ double sh[32];
+  if ((int)blockIdx.x < mid.blocks) {
+    if constexpr (CONTRACT && !OUT_H) mid_rows_block(p, mid.rows, mid.bounds, mid.n, blockIdx.x, mid.blocks);
+    return;
+  }
+  const int bid = (int)blockIdx.x - mid.blocks;
   const int P = p.nCh >> 1, G = P / PPT;  // pairs per row, thread groups per row
-  const long long i0 = (long long)blockIdx.x * p.rows_per_block;
+  const long long i0 = (long long)bid * p.rows_per_block;
   const int nr = (int)min((long long)p.rows_per_block, (long long)n_rows - i0);
   const int total = nr * G;
   const bool scale = p.in_row_scale != nullptr;
@@ -376,34 +438,33 @@ __global__ void __launch_bounds__(256, pair_min_blocks<PPT>()) spmm_pair_kernel(
   if (p.absmax) warp_absmax(p.absmax, amax);
   if (p.partial) {
     const double t = block_sum(sq, sh);
-    if (threadIdx.x == 0) p.partial[blockIdx.x] = t;
+    if (threadIdx.x == 0) p.partial[bid] = t;
   }
 }
 
 template <int PPT>
 static void launch_pair_ppt(bool out_h, bool contract, const SpmmParams& p, const int* rows, const uint2* rp,
-                            int nrows, int grid, cudaStream_t s) {
+                            int nrows, int grid, const MidRows& mid, cudaStream_t s) {
+  grid += mid.blocks;
   if (contract) {
     if (out_h)
-      spmm_pair_kernel<true, true, PPT><<<grid, 256, 0, s>>>(p, rows, rp, nrows);
+      spmm_pair_kernel<true, true, PPT><<<grid, 256, 0, s>>>(p, rows, rp, nrows, mid);
     else
-      spmm_pair_kernel<false, true, PPT><<<grid, 256, 0, s>>>(p, rows, rp, nrows);
+      spmm_pair_kernel<false, true, PPT><<<grid, 256, 0, s>>>(p, rows, rp, nrows, mid);
   } else {
     if (out_h)
-      spmm_pair_kernel<true, false, PPT><<<grid, 256, 0, s>>>(p, rows, rp, nrows);
+      spmm_pair_kernel<true, false, PPT><<<grid, 256, 0, s>>>(p, rows, rp, nrows, mid);
     else
-      spmm_pair_kernel<false, false, PPT><<<grid, 256, 0, s>>>(p, rows, rp, nrows);
+      spmm_pair_kernel<false, false, PPT><<<grid, 256, 0, s>>>(p, rows, rp, nrows, mid);
   }
 }
 
 static void launch_pair(int ppt, bool out_h, bool contract, const SpmmParams& p, const int* rows, const uint2* rp,
-                        int nrows, int grid, cudaStream_t s) {
-  if (ppt == 4)
-    launch_pair_ppt<4>(out_h, contract, p, rows, rp, nrows, grid, s);
-  else if (ppt == 2)
-    launch_pair_ppt<2>(out_h, contract, p, rows, rp, nrows, grid, s);
+                        int nrows, int grid, const MidRows& mid, cudaStream_t s) {
+  if (ppt == 2)
+    launch_pair_ppt<2>(out_h, contract, p, rows, rp, nrows, grid, mid, s);
   else
-    launch_pair_ppt<1>(out_h, contract, p, rows, rp, nrows, grid, s);
+    launch_pair_ppt<1>(out_h, contract, p, rows, rp, nrows, grid, mid, s);
 }
 
 static bool use_pair_kernel(const SpmmArgs& a) {
@@ -499,9 +560,24 @@ int spmm(const SpmmArgs& a, cudaStream_t s) {
       // the matrix's processing order when it covers the requested rows
       const bool ordered = m.ord_rows && m.ord_nonempty == a.nonempty_only;
       MLG_CHECK(ordered || !a.nonempty_only, "non-empty-row products need the ordered row list");
-      launch_pair(pair_ppt(a), oh, a.contract, p, ordered ? m.ord_rows : nullptr, ordered ? m.ord_bounds : nullptr, (int)nrows,
-                  grid_short, s);
-      MLG_LAUNCHED();
+      // operator products over a split order: the short rows by the pair
+      // kernel, the longer ones by a warp each
+      const bool split = ordered && a.contract && m.ord_short >= 0 && !oh && !a.partial && !a.absmax &&
+                         a.nCh / 2 <= 16;
+      const int n_pair = split ? m.ord_short : (int)nrows;
+      MidRows mid;
+      if (split && nrows > n_pair) {  // about two mid rows per warp
+        mid.rows = m.ord_rows + n_pair;
+        mid.bounds = m.ord_bounds + n_pair;
+        mid.n = (int)nrows - n_pair;
+        mid.blocks = (mid.n + 15) / 16;
+      }
+      const int grid_pair = split ? (n_pair + p.rows_per_block - 1) / p.rows_per_block : grid_short;
+      if (grid_pair + mid.blocks > 0) {
+        launch_pair(pair_ppt(a), oh, a.contract, p, ordered ? m.ord_rows : nullptr,
+                    ordered ? m.ord_bounds : nullptr, n_pair, grid_pair, mid, s);
+        MLG_LAUNCHED();
+      }
     }
     // long rows (segment kernels) with the same element types
     if (oh) return launch<L::kPointC64, L::kPointF16, false>(p, m, sc3, 0, s);
