@@ -241,6 +241,25 @@ int mlg_deform2sparsemat(int imDim, const int* N_u, const double* v,
 int mlg_deapodization(int imDim, const int* N_u, const double* dK_u,
                       int kernelType, int nWin, const double* kernelParam,
                       float* K);
+/* The same K computed on the device (K: device buffer of prod(N_u) floats),
+ * bit-identical to mlg_deapodization; stream-ordered, returns after the
+ * kernels finished.  (No reference counterpart: a device form of bmK.) */
+int mlg_deapodization_dev(int imDim, const int* N_u, const double* dK_u,
+                          int kernelType, int nWin,
+                          const double* kernelParam, float* K, void* stream);
+
+/* ---- volume elements ---------------------------------------------------- */
+
+/* Volume elements of a full radial trajectory on the device, FP64:
+ * imDim 3 as src/geom3/bmVolumeElement_full_radial3.m, imDim 2 as
+ * src/geom2/bmVolumeElement_voronoi_full_radial2.m.  t: device
+ * [imDim][nPt] (row-major), lines of N samples (line l = samples l*N ..
+ * l*N+N-1, through the centre at sample N/2); v: device [nPt].  Radial
+ * lengths are the 1-D Voronoi lengths along each line in the first line's
+ * order (bmVolumeElement1); the centre samples share one ball (3-D) or disc
+ * (2-D) element.  Stream-ordered. */
+int mlg_volume_element_radial_dev(int imDim, int nPt, int N, const double* t,
+                                  double* v, void* stream);
 
 /* ---- fused operators (NUFFT plan) --------------------------------------- */
 

@@ -59,6 +59,8 @@ SIGNATURES = {
     "mlg_traj2sparsemat": [c_int, c_int, P_d, P_d, P_i, P_d, c_int, c_int, P_d, ctypes.POINTER(c_vp),
                            ctypes.POINTER(c_vp)],
     "mlg_deapodization": [c_int, P_i, P_d, c_int, c_int, P_d, P_f],
+    "mlg_deapodization_dev": [c_int, P_i, P_d, c_int, c_int, P_d, c_vp, c_vp],
+    "mlg_volume_element_radial_dev": [c_int, c_int, c_int, c_vp, c_vp, c_vp],
     "mlg_plan_create": [c_int, P_i, P_i, c_int, c_vp, c_vp, P_f, P_f, P_f, P_f, ctypes.POINTER(c_vp)],
     "mlg_plan_destroy": [c_vp],
     "mlg_plan_set_dk": [c_vp, P_d],

@@ -47,24 +47,26 @@ double single(double v) { return (double)(float)v; }
 
 }  // namespace
 
-extern "C" int mlg_deapodization(int imDim, const int* N_u, const double* dK_u, int kernelType, int nWin,
-                                 const double* kernelParam, float* K) {
-  (void)dK_u;  // only scales the DFT, which cancels in the normalisation
-  MLG_CHECK(imDim >= 1 && imDim <= 3 && N_u && K && kernelParam, "invalid argument");
+namespace mlg {
+
+int deapod_tables(int imDim, const int* N_u, int kernelType, int nWin, const double* kernelParam, DeapodTables& T) {
+  MLG_CHECK(imDim >= 1 && imDim <= 3 && N_u && kernelParam, "invalid argument");
   MLG_CHECK(kernelType == MLG_KERNEL_GAUSS || kernelType == MLG_KERNEL_KAISER, "unknown kernel type");
   MLG_CHECK(nWin >= 1, "nWin must be >= 1");
-  int N[3] = {1, 1, 1};
+  T.imDim = imDim;
+  for (int d = 0; d < 3; ++d) T.N[d] = 1;
   for (int d = 0; d < imDim; ++d) {
     MLG_CHECK(N_u[d] >= 2 && (N_u[d] % 2) == 0, "N_u must have all components even");
-    N[d] = N_u[d];
+    T.N[d] = N_u[d];
   }
   // kernel parameters pass through single precision, as bmK.m:19 does
   double kp[3] = {single(kernelParam[0]), single(kernelParam[1]),
                   kernelType == MLG_KERNEL_KAISER ? single(kernelParam[2]) : 0.0};
-  const double K_max = kernelType == MLG_KERNEL_GAUSS ? kp[1] : kp[2];
+  T.K_max = kernelType == MLG_KERNEL_GAUSS ? kp[1] : kp[2];
   const int h = nWin / 2;  // fix(nWin/2)
   // support coordinates per dimension: x = -h, -h+1/2, ..., h (4h+1 values)
   const int S = 4 * h + 1;
+  T.S = S;
   std::vector<double> xs(S);
   for (int a = 0; a < S; ++a) xs[a] = -h + 0.5 * a;
   // which support coordinates survive the box mask; in 1D the reference's
@@ -73,14 +75,16 @@ extern "C" int mlg_deapodization(int imDim, const int* N_u, const double* dK_u, 
   if (imDim == 1)
     for (int a = 0; a < S; ++a) keep[a] = (xs[a] == (double)h);
   const int Sy = imDim > 1 ? S : 1, Sz = imDim > 2 ? S : 1;
+  T.Sy = Sy;
+  T.Sz = Sz;
   // weights w[az][ay][ax]
-  std::vector<double> w((size_t)S * Sy * Sz);
+  T.w.assign((size_t)S * Sy * Sz, 0.0);
   for (int az = 0; az < Sz; ++az)
     for (int ay = 0; ay < Sy; ++ay)
       for (int ax = 0; ax < S; ++ax) {
         const double x = xs[ax], y = imDim > 1 ? xs[ay] : 0.0, z = imDim > 2 ? xs[az] : 0.0;
         const bool in = keep[ax] && (imDim < 2 || keep[ay]) && (imDim < 3 || keep[az]);
-        w[((size_t)az * Sy + ay) * S + ax] = in ? kernel_weight(std::sqrt(x * x + y * y + z * z), kernelType, kp) : 0.0;
+        T.w[((size_t)az * Sy + ay) * S + ax] = in ? kernel_weight(std::sqrt(x * x + y * y + z * z), kernelType, kp) : 0.0;
       }
   // cos tables: c_d[j][a] = cos(2 pi (j - N/2) x_a / N); the support and the
   // weights are symmetric in each x_d, so the DFT is real
@@ -90,9 +94,24 @@ extern "C" int mlg_deapodization(int imDim, const int* N_u, const double* dK_u, 
       for (int a = 0; a < S; ++a) t[(size_t)j * S + a] = std::cos(2 * M_PI * (double)(j - n / 2) * xs[a] / n);
     return t;
   };
-  const std::vector<double> cx = table(N[0]);
-  const std::vector<double> cy = imDim > 1 ? table(N[1]) : std::vector<double>(S, 1.0);
-  const std::vector<double> cz = imDim > 2 ? table(N[2]) : std::vector<double>(S, 1.0);
+  T.cx = table(T.N[0]);
+  T.cy = imDim > 1 ? table(T.N[1]) : std::vector<double>(S, 1.0);
+  T.cz = imDim > 2 ? table(T.N[2]) : std::vector<double>(S, 1.0);
+  return MLG_OK;
+}
+
+}  // namespace mlg
+
+extern "C" int mlg_deapodization(int imDim, const int* N_u, const double* dK_u, int kernelType, int nWin,
+                                 const double* kernelParam, float* K) {
+  (void)dK_u;  // only scales the DFT, which cancels in the normalisation
+  MLG_CHECK(K, "invalid argument");
+  mlg::DeapodTables T;
+  MLG_TRY(mlg::deapod_tables(imDim, N_u, kernelType, nWin, kernelParam, T));
+  const int* N = T.N;
+  const int S = T.S, Sy = T.Sy, Sz = T.Sz;
+  const double K_max = T.K_max;
+  const std::vector<double>&w = T.w, &cx = T.cx, &cy = T.cy, &cz = T.cz;
   // pass x: A1[az][ay][jx]
   std::vector<double> A1((size_t)Sz * Sy * N[0], 0.0);
   for (int az = 0; az < Sz; ++az)

@@ -10,6 +10,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <string>
+#include <vector>
 
 #include "../../include/monalisa_gpu.h"
 
@@ -258,5 +259,18 @@ int spmm_partial_count(const SpmmArgs& a);
 
 // Deterministic final reduction of partial sums: out[0] = sum partial[0..n).
 int reduce_partials(const double* partial, int n, double* out, cudaStream_t s);
+
+// Tables of the deapodisation (bmK.m:6-156) shared by the host and device
+// computations (mlg_deapod.cpp): support weights w[az][ay][ax] (S, Sy, Sz
+// samples per axis) and cosine tables c_d[j][a] (all ones along absent
+// axes), grid N, clip K_max.
+struct DeapodTables {
+  int imDim = 1;
+  int N[3] = {1, 1, 1};
+  int S = 1, Sy = 1, Sz = 1;
+  double K_max = 0.0;
+  std::vector<double> w, cx, cy, cz;
+};
+int deapod_tables(int imDim, const int* N_u, int kernelType, int nWin, const double* kernelParam, DeapodTables& T);
 
 }  // namespace mlg

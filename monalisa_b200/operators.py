@@ -40,6 +40,22 @@ def bmK(N_u, dK_u, nCh, kernelType=None, nWin=None, kernelParam=None):
     return np.repeat(K[:, None], int(nCh), axis=1)
 
 
+def bmK_dev(N_u, dK_u, kernelType=None, nWin=None, kernelParam=None):
+    """One column of bmK computed on the device (mlg_deapodization_dev): a
+    CUDA float32 tensor [prod(N_u)], bit-identical to bmK's column."""
+    import torch
+
+    kernelType, nWin, kp = kernel_defaults(kernelType, nWin, kernelParam)
+    Nu = _ints(N_u)
+    dK = np.ascontiguousarray(np.ravel(dK_u), np.float64)
+    kp3 = np.zeros(3)
+    kp3[:kp.size] = kp
+    K = torch.empty(int(np.prod(Nu)), dtype=torch.float32, device="cuda")
+    N.call("mlg_deapodization_dev", Nu.size, N.iptr(Nu), N.dptr(dK), kernel_code(kernelType), nWin, N.dptr(kp3),
+           N.tptr(K), N.stream_ptr())
+    return K
+
+
 def crop_index(N_u, n_u):
     """bmImCrope.m: the n_u block occupies N/2-n/2 .. N/2+n/2-1 of N_u."""
     return tuple(slice(int(a) // 2 - int(b) // 2, int(a) // 2 + int(b) // 2) for a, b in zip(N_u, n_u))

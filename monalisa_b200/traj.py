@@ -155,6 +155,25 @@ def _ve_full_radial(t, imDim, N=None):
     return v
 
 
+def bmVolumeElement_radial_dev(t, N=None):
+    """Volume elements of a full radial trajectory computed on the device
+    (mlg_volume_element_radial_dev): 3-D as bmVolumeElement_full_radial3,
+    2-D as bmVolumeElement_voronoi_full_radial2.  t [imDim, nPt] (host or
+    CUDA); returns a CUDA float64 tensor [nPt]."""
+    import torch
+
+    from . import _native as NN
+
+    tt = torch.as_tensor(np.asarray(t, np.float64) if not torch.is_tensor(t) else t, dtype=torch.float64)
+    tt = tt.to("cuda").contiguous()
+    imDim, nPt = int(tt.shape[0]), int(tt.shape[1])
+    if N is None:
+        N = _points_per_line(tt.cpu().numpy())
+    v = torch.empty(nPt, dtype=torch.float64, device="cuda")
+    NN.call("mlg_volume_element_radial_dev", imDim, nPt, int(N), NN.tptr(tt), NN.tptr(v), NN.stream_ptr())
+    return v
+
+
 def _points_per_line(t):
     r = np.sqrt(np.sum(t ** 2, axis=0))
     # lines are symmetric around the centre: the first zero-radius sample is at N/2
