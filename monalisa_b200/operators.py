@@ -81,7 +81,13 @@ def _cropped_K(N_u, n_u, dK_u, kernelType, nWin, kernelParam):
     with _K_LOCK:
         K = _K_CACHE.get(key)
     if K is None:
-        K = _crop_col(bmK(N_u, dK_u, 1, kernelType, nWin, kp), N_u, n_u)
+        import torch
+
+        if torch.cuda.is_available():  # the device computation, bit-identical to the host one
+            col = bmK_dev(N_u, dK_u, kernelType, nWin, kp).cpu().numpy()[:, None]
+        else:
+            col = bmK(N_u, dK_u, 1, kernelType, nWin, kp)
+        K = _crop_col(col, N_u, n_u)
         K.setflags(write=False)
         with _K_LOCK:
             if len(_K_CACHE) > 16:
