@@ -429,7 +429,7 @@ __global__ void __launch_bounds__(256, pair_min_blocks<PPT>()) spmm_pair_kernel(
     float4 acc[PPT];
 #pragma unroll
     for (int u = 0; u < PPT; ++u) acc[u] = make_float4(0.f, 0.f, 0.f, 0.f);
-#pragma unroll(PPT == 1 ? 4 : 2)
+#pragma unroll 4
     for (uint32_t k = b; k < b + n; ++k) entry(k, pi, acc);
     const double w = p.partial && p.sqn_w ? (double)__ldg(p.sqn_w + r) : 1.0;
 #pragma unroll
