@@ -338,9 +338,13 @@ __device__ __forceinline__ void mid_rows_block(const SpmmParams& p, const int* _
 // PPT coil pairs per thread: the row's bounds and each entry's column and
 // value are loaded once for PPT pairs.  Per coil the entries are summed in
 // the same order for every PPT, so the outputs do not depend on it.
+// Resident blocks per SM: the gathers are latency-bound, so occupancy beats
+// spill-free code -- one pair per thread at 8 blocks (32 registers, a few
+// spilled bytes) took Gut on the 4096-spoke 16-coil koosh case from 0.757
+// (6 blocks) to 0.671 ms; 5 blocks gave 0.841 ms.
 template <int PPT>
 constexpr int pair_min_blocks() {
-  return PPT == 1 ? 6 : (PPT == 2 ? 5 : 4);
+  return PPT == 1 ? 8 : (PPT == 2 ? 5 : 4);
 }
 
 // With mid_blocks > 0 (CONTRACT, FP32 output) the first mid_blocks blocks
@@ -461,10 +465,8 @@ static void launch_pair_ppt(bool out_h, bool contract, const SpmmParams& p, cons
 
 static void launch_pair(int ppt, bool out_h, bool contract, const SpmmParams& p, const int* rows, const uint2* rp,
                         int nrows, int grid, const MidRows& mid, cudaStream_t s) {
-  if (ppt == 2)
-    launch_pair_ppt<2>(out_h, contract, p, rows, rp, nrows, grid, mid, s);
-  else
-    launch_pair_ppt<1>(out_h, contract, p, rows, rp, nrows, grid, mid, s);
+  (void)ppt;  // one pair per thread (pair_ppt)
+  launch_pair_ppt<1>(out_h, contract, p, rows, rp, nrows, grid, mid, s);
 }
 
 static bool use_pair_kernel(const SpmmArgs& a) {
@@ -473,17 +475,13 @@ static bool use_pair_kernel(const SpmmArgs& a) {
          !a.normalize;
 }
 
-// Coil pairs per thread of the pair kernel, as measured on a B200: two for
-// products over all rows with at least 8 (an even number of) coil pairs --
-// Gu of the 4096 x 256-sample, 16-coil koosh case 0.43 -> 0.40 ms, of a
-// 1500 x 256-sample one 0.178 -> 0.181 ms; one otherwise: with 12 or 8
-// coils two pairs were slower (Gu 0.37 -> 0.46 ms), and so were the
-// non-empty-row products Gut (0.37 -> 0.43 ms at 16 coils, 1500 spokes).
-// Four pairs lost more to occupancy than they saved (Gu 0.69 ms).
-static int pair_ppt(const SpmmArgs& a) {
-  const int P = a.nCh / 2;
-  return !a.nonempty_only && P >= 8 && P % 2 == 0 ? 2 : 1;
-}
+// Coil pairs per thread of the pair kernel, as measured on a B200: one.
+// With eight 256-thread blocks per SM (32 registers) one pair per thread
+// matched two on the 4096 x 256-sample 16-coil Gu (0.381 vs 0.379 ms) and
+// beat it on a 1500-spoke one (0.164 vs 0.174 ms); at lower occupancy two
+// pairs had helped only that 16-coil Gu and slowed 12- and 8-coil products
+// and the non-empty-row Gut.
+static int pair_ppt(const SpmmArgs&) { return 1; }
 
 static int rows_per_block(const SpmmArgs& a) {
   if (use_pair_kernel(a)) return std::max(1, 1024 / (a.nCh / 2 / pair_ppt(a)));
