@@ -566,9 +566,36 @@ size_t LeightWorkspace::bins_bytes(const LeightGeom& g, long long pairs, long lo
   return align((size_t)pairs * 4) + align((size_t)chunks * 16) + align((size_t)slots * g.tile_cells * G * 4);
 }
 
+long long leight_max_pairs(const LeightGeom& g, long long nPt) {
+  // a window of nWin cells meets at most ceil((nWin - 1) / T) + 1 tiles per axis
+  long long per = 1;
+  for (int d = 0; d < g.imDim; ++d) per *= (g.nWin - 1 + g.T[d] - 1) / g.T[d] + 1;
+  return nPt * per;
+}
+
+int leight_preload() {
+  cudaFuncAttributes a;
+  MLG_CUDA(cudaFuncGetAttributes(&a, leight_count_kernel));
+  MLG_CUDA(cudaFuncGetAttributes(&a, leight_fill_kernel));
+  MLG_CUDA(cudaFuncGetAttributes(&a, leight_chunk_count_kernel));
+  MLG_CUDA(cudaFuncGetAttributes(&a, leight_chunk_build_kernel));
+  MLG_CUDA(cudaFuncGetAttributes(&a, leight_accumulate_kernel));
+  MLG_CUDA(cudaFuncGetAttributes(&a, leight_accumulate_warp_kernel));
+  MLG_CUDA(cudaFuncGetAttributes(&a, leight_gather_kernel<16>));
+  MLG_CUDA(cudaFuncGetAttributes(&a, leight_gather_kernel<12>));
+  MLG_CUDA(cudaFuncGetAttributes(&a, leight_gather_kernel<8>));
+  MLG_CUDA(cudaFuncGetAttributes(&a, leight_combine_kernel));
+  return MLG_OK;
+}
+
 int leight_run(const LeightGeom& g, const LeightInputs& in, int nPt, const LeightOutput& out, LeightWorkspace& ws,
                cudaStream_t s) {
   MLG_CHECK(g.ntiles < (1LL << 31), "too many tiles");
+  // the per-tile counts, their scan and the bin offsets are 32-bit: refuse
+  // inputs whose (tile, sample) pairs could pass 2^31 before counting them
+  MLG_CHECK(leight_max_pairs(g, nPt) < (1LL << 31),
+            "%d samples may meet up to %lld (tile, sample) pairs; at most 2^31 - 1 are supported", nPt,
+            leight_max_pairs(g, nPt));
   const int nt = (int)g.ntiles;
   MLG_CHECK(ws.counters && ws.counters_cap >= LeightWorkspace::counters_bytes(g),
             "gridding counter workspace too small (%zu < %zu bytes)", ws.counters_cap,

@@ -61,6 +61,14 @@ struct LeightWorkspace {
 };
 
 int leight_geometry(int imDim, int nCh, const int* N, int nWin, float sigma, LeightGeom& g);
+// Upper bound of the (tile, sample) pairs nPt samples can produce.
+long long leight_max_pairs(const LeightGeom& g, long long nPt);
+// Loads every kernel the tile-binned form launches into the current device's
+// context (under CUDA's lazy module loading a kernel is otherwise loaded, and
+// its memory taken, at its first launch).
+int leight_preload();
+// Tile-binned form.  It waits on the host once per call: after the counting
+// kernels it synchronises `s` to read the bin totals, then queues the rest.
 int leight_run(const LeightGeom& g, const LeightInputs& in, int nPt, const LeightOutput& out, LeightWorkspace& ws,
                cudaStream_t s);
 

@@ -1,16 +1,17 @@
 // Adjoint gridding that allocates no memory.
 //
 // Some callers cannot allocate device memory at call time: a host program
-// that has reserved all of the GPU's memory for its own pool up front, an
-// embedding that forbids allocation after start-up, or a real-time loop
-// where a cudaMalloc (and the synchronisation it implies) is not acceptable.
+// that reserved all of the GPU's memory for its own pool at start-up (a
+// cudaMalloc would fail or take memory the pool counts on), or an embedding
+// whose rules forbid allocation after initialisation.
 // mlg_gridder_n2u_leight_noalloc gives them the on-the-fly Gaussian gridder
 // of mlg_gridder_n2u_leight with device-resident inputs and outputs that the
 // caller owns, and takes every scratch byte the tile-binned algorithm needs
 // (per-tile counters, scan space, the (tile, sample) bins, partial tiles of
 // split bins) from one file-scope device array of fixed size.  Nothing here
 // calls cudaMalloc, cudaFree, cudaMallocAsync or an allocating library
-// routine.
+// routine.  The tile-binned algorithm sizes its bins from counts it reads
+// back to the host, so each call waits once on its stream (see the header).
 #include <mutex>
 
 #include "mlg_gridder.cuh"
@@ -26,6 +27,9 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratch
 
 // In host code the array's name is only a host-side stand-in: the device
 // address is fetched once per device (with that device current) and cached.
+// The same set-up loads the gridding kernels, so that under CUDA's lazy
+// module loading the array and the kernels take their device memory at this
+// first call and never later.
 int scratch_base(void** out) {
   static std::mutex mu;
   static void* base[128] = {};
@@ -38,6 +42,7 @@ int scratch_base(void** out) {
     const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess || p == nullptr)
       return fail(MLG_ERR_CUDA, "cudaGetSymbolAddress of the gridding scratch failed: %s", cudaGetErrorString(e));
+    MLG_TRY(leight_preload());
     base[dev] = p;
   }
   *out = base[dev];

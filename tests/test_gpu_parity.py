@@ -5,7 +5,8 @@ drop-in boundary, called through the MEX-API shim) or the package API that
 wraps the C ABI.  Tolerances:
 * sparse products and the precomputed-weight gridder: bit-exact (the kernels
   keep the reference's per-row accumulation order, no FMA contraction);
-* on-the-fly gridder (shared-memory atomics, CUDA expf): relative L2 <= 1e-5;
+* on-the-fly gridder (cell-binned gather: each cell sums its samples in its
+  own fixed order, CUDA expf): relative L2 <= 1e-5;
 * FFT-based operators: relative L2 <= 1e-5 against the FP32 oracle;
 * CG-SENSE: relative L2 <= 1e-4 after 5 iterations (FP32 data, FP64 scalars
   on both sides).

@@ -1,11 +1,14 @@
 """The gridding entry point that allocates nothing
 (mlg_gridder_n2u_leight_noalloc), for callers that cannot allocate device
-memory while they run.  The caller owns every input and output buffer (here:
-torch CUDA tensors); the entry point takes its scratch from the library's
-fixed device array.  Its results must match the allocating entry point's
-(mlg_gridder_n2u_leight) within the gridder's tolerance (relative L2 1e-5;
-both accumulate with shared-memory atomics), on two calls in a row -- the
-second call reuses the scratch left by the first.
+memory while they run: a program that reserved the GPU's memory for its own
+pool, or an embedding that forbids allocation after start-up.  The caller
+owns every input and output buffer (here: torch CUDA tensors); the entry
+point takes its scratch from the library's fixed device array.  Its results
+must match the allocating entry point's (mlg_gridder_n2u_leight, the
+cell-binned gather) within the gridder's tolerance (relative L2 1e-5: the
+two forms sum each cell's samples in different orders), on two calls in a
+row -- the second call reuses the scratch left by the first -- and the
+second call must leave the device's free memory unchanged.
 
 Kept in a file of its own that pytest collects last."""
 import ctypes
@@ -49,10 +52,14 @@ def test_noalloc_gridder_matches_allocating_gridder_twice():
     for call in range(2):
         bR.fill_(float("nan"))  # every output cell must be written by the call
         bI.fill_(float("nan"))
+        torch.cuda.synchronize(dev)
+        free_before = torch.cuda.mem_get_info(dev)[0]
         N.call("mlg_gridder_n2u_leight_noalloc", imDim, *[ctypes.c_void_p(x.data_ptr()) for x in d_in], nCh, nPt,
                Nn, Nn, Nn, nWin, 0.61, 10.0, ctypes.c_void_p(bR.data_ptr()), ctypes.c_void_p(bI.data_ptr()),
                ctypes.c_void_p(stream.cuda_stream))
         torch.cuda.synchronize(dev)
+        if call == 1:  # the first call may load the library's kernels; the second takes no memory
+            assert torch.cuda.mem_get_info(dev)[0] == free_before, "the call changed the device's free memory"
         gotR, gotI = bR.cpu().numpy(), bI.cpu().numpy()
         assert np.isfinite(gotR).all() and np.isfinite(gotI).all(), f"call {call}: unwritten output cells"
         assert _rel(gotR + 1j * gotI, refR + 1j * refI) <= 1e-5, f"call {call}"
@@ -69,3 +76,18 @@ def test_noalloc_gridder_rejects_problems_beyond_its_scratch():
     with pytest.raises(N.MonalisaError, match="no-allocation scratch"):
         N.call("mlg_gridder_n2u_leight_noalloc", 3, None, None, None, None, None, None, 1, 0, 1536, 1024, 1024, 3,
                0.61, 10.0, ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(out.data_ptr()), None)
+
+
+def test_noalloc_gridder_rejects_too_many_tile_pairs():
+    import torch
+
+    from monalisa_b200 import _native as N
+
+    buf = torch.zeros(4, dtype=torch.float32, device="cuda")
+    p = ctypes.c_void_p(buf.data_ptr())
+    # 2^28 samples on a 64^3 grid with 8 coils: each window may meet 2 x 2 x 2
+    # tiles, so the 32-bit bin offsets could overflow -- refused before any
+    # launch (the pointers are never read)
+    with pytest.raises(N.MonalisaError, match="pairs"):
+        N.call("mlg_gridder_n2u_leight_noalloc", 3, p, p, p, p, p, p, 8, 1 << 28, 64, 64, 64, 3, 0.61, 10.0, p, p,
+               None)
