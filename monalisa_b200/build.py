@@ -4,7 +4,9 @@
   compiled for sm_100a only (``-gencode arch=compute_100a,code=sm_100a``);
 * ``_lib/libmexshim.so`` -- the project's MEX-API shim;
 * ``_lib/mex/<name>.so`` -- the drop-in MEX gateways (reference names and
-  argument layouts), linked against the shim and libmonalisa_gpu.so.
+  argument layouts), linked against the shim and libmonalisa_gpu.so;
+* ``driver/_bin/monalisa_driver`` -- the standalone C++ reconstruction driver
+  (driver/monalisa_driver.cpp) on the C ABI.
 
 Usage: ``python -m monalisa_b200.build`` (or ``build()`` from Python).
 Object files go to ``_build/`` (git-ignored).  Rebuilds only what changed.
@@ -103,6 +105,13 @@ def build(verbose: bool = False, jobs: int | None = None) -> str:
                       "-L", LIB, "-lmonalisa_gpu", "-lmexshim", "-Wl,-rpath,$ORIGIN/.."])
         with ThreadPoolExecutor(jobs or min(8, os.cpu_count() or 4)) as ex:
             list(ex.map(gw, GATEWAYS))
+    drv_src = os.path.join(ROOT, "driver", "monalisa_driver.cpp")
+    drv = os.path.join(ROOT, "driver", "_bin", "monalisa_driver")
+    if os.path.exists(drv_src) and _newer(drv, [drv_src, so] + headers):
+        os.makedirs(os.path.dirname(drv), exist_ok=True)
+        _run([CXX, "-O2", "-std=c++17", "-I", INCLUDE, "-I", os.path.join(CUDA_HOME, "include"), "-o", drv, drv_src,
+              "-L", LIB, "-lmonalisa_gpu", "-L", os.path.join(CUDA_HOME, "lib64"), "-lcudart",
+              "-Wl,-rpath,$ORIGIN/../../monalisa_b200/_lib", "-Wl,-rpath," + os.path.join(CUDA_HOME, "lib64")])
     if verbose:
         print("built", so)
     return so
