@@ -16,9 +16,10 @@
  *    (passed as void*, NULL = default stream) and are stream-ordered.  A
  *    handle may be used by one host thread at a time.
  *  - Device data layouts: complex64 = interleaved float2.  Images are
- *    [prod(n_u)] with x fastest (MATLAB column order).  Gridded data are
- *    coil-major [nCh][prod(N_u)].  k-space data on the device are
- *    coil-fastest [nPt][nCh] ("point layout").
+ *    [prod(n_u)] with x fastest (MATLAB column order).  Gridded data on the
+ *    device are coil-fastest [prod(N_u)][nCh] (one cell's coils adjacent).
+ *    k-space data on the device are coil-fastest [nPt][nCh] ("point
+ *    layout").
  *
  * Reference paths in the comments are relative to the Monalisa source tree.
  */
@@ -77,24 +78,33 @@ int mlg_gridder_n2u_leight(int imDim, const float* aReal, const float* aImag,
                            float kernelParam_2, float* bReal, float* bImag);
 
 /* The gridder of mlg_gridder_n2u_leight for callers that cannot allocate
- * device memory while they run (a program that reserved the GPU's memory for
- * its own pool at start-up, an embedding that forbids allocation after
- * initialisation, a real-time loop that cannot afford an allocation's
- * synchronisation).  No counterpart in the reference: it is an addition of
+ * device memory while they run: a program that reserved the GPU's memory for
+ * its own pool at start-up (an allocation would fail, or take memory the
+ * pool counts on), or an embedding that forbids allocation after
+ * initialisation.  No counterpart in the reference: it is an addition of
  * this library.
  *  - Inputs and outputs are device pointers owned by the caller, in the same
  *    layouts as mlg_gridder_n2u_leight: aReal/aImag [nCh, nPt], tx/ty/tz/Dn
  *    [nPt], bReal/bImag [nCh, Nx*Ny*Nz].  Work is ordered on `stream`
- *    (NULL = default stream); the call returns once the gridding kernels are
- *    queued, so the outputs are ready when the stream reaches that point.
+ *    (NULL = default stream).
+ *  - The call waits on the host once: after its counting kernels it
+ *    synchronises `stream` (so it also waits for all work queued there
+ *    before it) and reads seven bin totals into host memory, then queues the
+ *    gridding kernels and returns; the outputs are ready when the stream
+ *    reaches that point.
  *  - Nothing is allocated: all scratch comes from one fixed 32 MiB array in
  *    device memory that every GPU loading the library holds until exit.  A
- *    problem whose counters or bins do not fit is rejected with MLG_ERR_ARG
- *    and a message giving the bytes it would need.
- *  - The first call on a device looks up the array's device address; make it
- *    before any stream capture.
- *  - All calls share the array: calls that overlap on the GPU (other threads,
- *    other streams) race.  Each call clears the counters it relies on. */
+ *    problem whose counters or bins do not fit, or whose (tile, sample)
+ *    pairs could exceed 2^31 - 1, is rejected with MLG_ERR_ARG and a message
+ *    giving the bytes or pairs it would need, before anything is launched.
+ *  - The first call on a device does the set-up: it looks up the array's
+ *    device address and loads the gridding kernels (under CUDA's lazy module
+ *    loading the array and the kernels take their device memory then).  Make
+ *    that first call before any stream capture, and before reserving the
+ *    GPU's memory for a pool (or set CUDA_MODULE_LOADING=EAGER).
+ *  - All calls share the array, which keeps the last call's contents: calls
+ *    that overlap on the GPU (other threads, other streams) race.  Each call
+ *    clears the counters it relies on. */
 int mlg_gridder_n2u_leight_noalloc(int imDim, const float* aReal,
                                    const float* aImag, const float* tx,
                                    const float* ty, const float* tz,
@@ -289,6 +299,14 @@ int mlg_plan_create_sharing(mlg_plan_t base, mlg_matrix_t Gu, mlg_matrix_t Gut,
 int mlg_plan_set_dk(mlg_plan_t p, const double* dK_u);
 /* Device bytes held by the plan (excluding the caller's matrices). */
 int mlg_plan_device_bytes(mlg_plan_t p, long long* bytes);
+
+/* Synchronises the plan's stream and reports whether a bounded wait inside
+ * one of its device passes ran out since the last check (MLG_ERR_TIMEOUT;
+ * the results of that work are invalid) -- MLG_OK otherwise.  The flag is
+ * one per device and is cleared by the check; the synchronous host-buffer
+ * calls check it themselves.  No counterpart in the reference: the
+ * reference has no device code. */
+int mlg_plan_status(mlg_plan_t p);
 
 /* bmShanna (src/fourier123/map_function/nonCartesian/bmShanna_MATLAB.m:6-56)
  * on device buffers: x [prod(n_u)] (or [prod(n_u)][nCh], coil fastest, if

@@ -65,6 +65,7 @@ SIGNATURES = {
     "mlg_plan_destroy": [c_vp],
     "mlg_plan_set_dk": [c_vp, P_d],
     "mlg_plan_device_bytes": [c_vp, P_ll],
+    "mlg_plan_status": [c_vp],
     "mlg_shanna_dev": [c_vp, c_vp, c_int, c_vp, c_vp],
     "mlg_nakatsha_dev": [c_vp, c_vp, P_f, c_float, c_vp, c_vp],
     "mlg_shanna": [c_int, P_i, P_i, c_int, P_f, P_f, c_int, P_f, P_f, c_int, P_i, P_i, P_f, c_int, P_i, c_int,

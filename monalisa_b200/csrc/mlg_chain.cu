@@ -943,7 +943,7 @@ static int run_host(mlg_chain_t c, bool spatial, const float* yR, const float* y
   MLG_CUDA(cudaMemcpyAsync(xI, dx.p + ni, sizeof(float) * ni, cudaMemcpyDeviceToHost, s));
   if (cudaStreamSynchronize(s) != cudaSuccess)
     return fail(MLG_ERR_CUDA, "ADMM solver failed: %s", cudaGetErrorString(cudaGetLastError()));
-  return MLG_OK;
+  return mlg::fft_wait_status(c->fr[0]->wait_err, s);  // one flag per device: the frames share it
 }
 
 }  // namespace mlg

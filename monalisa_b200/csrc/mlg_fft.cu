@@ -1,12 +1,90 @@
 // Pruned, fused line-FFT passes (see mlg_fft.cuh): host side -- axis tables
 // and the per-pass dispatch into the instantiations of mlg_fft_pass_*.cu.
+#include <cudaTypedefs.h>
+
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "mlg_fft_kernels.cuh"
 
 namespace mlg {
+
+bool tma_passes_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("MLG_FFT_TMA");
+    return !(e && std::strcmp(e, "0") == 0);
+  }();
+  return on;
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against the driver library)
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  return fn;
+}
+
+int* fft_wait_word() {
+  static std::mutex mu;
+  static int* words[128] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 128) return nullptr;
+  std::lock_guard<std::mutex> lk(mu);
+  if (!words[dev]) {
+    int* w = nullptr;
+    if (cudaMalloc(&w, sizeof(int)) != cudaSuccess || cudaMemset(w, 0, sizeof(int)) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    words[dev] = w;
+  }
+  return words[dev];
+}
+
+int fft_wait_status(int* word, cudaStream_t s) {
+  if (!word) return MLG_OK;
+  int h = 0;
+  MLG_CUDA(cudaMemcpyAsync(&h, word, sizeof(int), cudaMemcpyDeviceToHost, s));
+  MLG_CUDA(cudaStreamSynchronize(s));
+  if (h == 0) return MLG_OK;
+  MLG_CUDA(cudaMemsetAsync(word, 0, sizeof(int), s));
+  MLG_CUDA(cudaStreamSynchronize(s));
+  return fail(MLG_ERR_TIMEOUT, "a bounded wait inside a line-FFT pass ran out; results of the work since the last "
+                               "check are invalid");
+}
+
+int tma_line_map(CUtensorMap* map, const void* base, int C, int dim_u, long long st_u, int len, long long st_ax,
+                 int dim_v, long long st_v, int box_L, int box_rows) {
+  auto enc = tensor_map_encoder();
+  MLG_CHECK(enc != nullptr, "cuTensorMapEncodeTiled is not available");
+  MLG_CHECK(((uintptr_t)base & 15) == 0, "TMA volume base not 16-byte aligned");
+  MLG_CHECK(C >= 1 && 2 * C <= 256 && box_L >= 1 && box_L <= 256 && box_rows >= 1 && box_rows <= 256,
+            "TMA box out of range");
+  const cuuint64_t dims[4] = {(cuuint64_t)2 * C, (cuuint64_t)dim_u, (cuuint64_t)len, (cuuint64_t)dim_v};
+  const cuuint64_t strides[3] = {(cuuint64_t)st_u * 8, (cuuint64_t)st_ax * 8, (cuuint64_t)st_v * 8};
+  for (int i = 0; i < 3; ++i)
+    MLG_CHECK(strides[i] % 16 == 0 && strides[i] < (1ull << 40), "TMA stride %llu not a multiple of 16 bytes",
+              (unsigned long long)strides[i]);
+  const cuuint32_t box[4] = {(cuuint32_t)(2 * C), (cuuint32_t)box_L, (cuuint32_t)box_rows, 1};
+  const cuuint32_t estr[4] = {1, 1, 1, 1};
+  const CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<void*>(base), dims, strides, box, estr,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  MLG_CHECK(r == CUDA_SUCCESS, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+  return MLG_OK;
+}
 
 int fft_axis_init(int N, FftAxisPlan& a) {
   a = FftAxisPlan();

@@ -63,7 +63,17 @@ struct PassDesc {
   // of 4); the pipelined pass fetches them ahead of the line copies
   const uint32_t* in_lmask = nullptr;
   int lmask_words = 0;
+  // device word set to 1 when a bounded wait inside a pass runs out (passes
+  // with such waits: the TMA passes), or NULL
+  int* wait_err = nullptr;
 };
+
+// The current device's wait flag (set by a pass whose bounded wait ran out),
+// allocated on first use -- call it outside stream capture.
+int* fft_wait_word();
+// Synchronises s, then reads and clears *word: MLG_OK, or MLG_ERR_TIMEOUT
+// when a pass's wait ran out since the last check.
+int fft_wait_status(int* word, cudaStream_t s);
 
 int fft_axis_init(int N, FftAxisPlan& a);
 void fft_axis_free(FftAxisPlan& a);

@@ -1001,6 +1001,12 @@ __global__ void __launch_bounds__(256, 2)
   }
 }
 
+}  // namespace mlg
+
+#include "mlg_fft_tma.cuh"
+
+namespace mlg {
+
 // ---- launch helpers ------------------------------------------------------------
 // Lines per CTA: 32 columns (256-byte row segments) for streaming passes; the
 // gathering pass uses 16 columns so that twice as many CTAs (and gathers)
@@ -1061,6 +1067,62 @@ static int launch_pipe(const FftAxisPlan& a, const PassDesc& d, int Lp, int thre
   fft_pass_pipe_kernel<N1, N2, DIR, MAXT, COLS><<<grid, threads, smem, s>>>(d, Lp, nb, a.tw);
   MLG_LAUNCHED();
   return MLG_OK;
+}
+
+// TMA pass (fft_pass_tma_kernel) for a plain pass without occupancy masks:
+// *launched stays false when the shape does not fit the TMA boxes (the
+// caller then takes the cp.async pipelined pass).
+template <int N1, int N2, int DIR, int COLS>
+static int launch_tma(const FftAxisPlan& a, const PassDesc& d, int Lp, cudaStream_t s, bool* launched) {
+  constexpr int N = N1 * N2, NT = cta_threads(COLS), NSLOT = 2;
+  *launched = false;
+  // register budget of step C: shapes beyond it are not instantiated
+  if constexpr (tma_step_c_iters<N1, N2, COLS, NT>() * N2 > 32) return MLG_OK;
+  else {
+  if (d.in_mask || d.in_lo < 0 || d.in_len < 1 || d.in_lo + d.in_len > N || d.out_lo < 0 || d.out_len < 1 ||
+      d.out_lo + d.out_len > N || Lp * d.C != COLS)
+    return MLG_OK;
+  const int u = d.ax == 0 ? 1 : 0, v = d.ax == 2 ? 1 : 2;
+  TmaPass t;
+  t.L = Lp;
+  t.gu = (d.dims[u] + Lp - 1) / Lp;
+  t.nbundles = blocks_for(d, Lp);
+  t.in_chunks = (N + 255) / 256;
+  t.out_chunks = (d.out_len + 255) / 256;
+  if (N % t.in_chunks || d.out_len % t.out_chunks) return MLG_OK;
+  t.in_rows = N / t.in_chunks;
+  t.out_rows = d.out_len / t.out_chunks;
+  t.in_lo = d.in_lo;
+  t.out_lo = d.out_lo;
+  t.err = d.wait_err;
+  const long long rowb = (long long)COLS * 8;  // shared-memory box starts on 128-byte boundaries
+  if ((t.in_rows * rowb) % 128 || (t.out_lo * rowb) % 128 || (t.out_rows * rowb) % 128) return MLG_OK;
+  CUtensorMap tin, tout;
+  if (tma_line_map(&tin, d.in, d.C, d.dims[u], d.in_stride[u], d.in_len, d.in_stride[d.ax], d.dims[v],
+                   d.in_stride[v], Lp, t.in_rows) != MLG_OK ||
+      tma_line_map(&tout, d.out, d.C, d.dims[u], d.out_stride[u], d.out_len, d.out_stride[d.ax], d.dims[v],
+                   d.out_stride[v], Lp, t.out_rows) != MLG_OK)
+    return MLG_OK;
+  const size_t smem = (size_t)NSLOT * N * COLS * 8 + 2 * NSLOT * sizeof(uint64_t) + 128;
+  thread_local int per_sm = 0, sms = 0;
+  thread_local size_t per_sm_smem = 0;
+  if (per_sm == 0 || per_sm_smem != smem) {
+    MLG_CUDA(cudaFuncSetAttribute(fft_pass_tma_kernel<N1, N2, DIR, COLS, NSLOT>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(200 * 1024)));
+    int dev = 0;
+    MLG_CUDA(cudaGetDevice(&dev));
+    MLG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    MLG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fft_pass_tma_kernel<N1, N2, DIR, COLS, NSLOT>,
+                                                           NT + 32, smem));
+    per_sm = std::max(1, per_sm);
+    per_sm_smem = smem;
+  }
+  const int grid = std::max(1, std::min(t.nbundles, per_sm * sms));
+  fft_pass_tma_kernel<N1, N2, DIR, COLS, NSLOT><<<grid, NT + 32, smem, s>>>(tin, tout, t, a.tw);
+  MLG_LAUNCHED();
+  *launched = true;
+  return MLG_OK;
+  }
 }
 
 static inline int pipe_lines(const FftAxisPlan& a, int C) {
@@ -1156,6 +1218,17 @@ static int launch_pass(const FftAxisPlan& a, const PassDesc& d, int L, cudaStrea
     const int Lp = pipe_lines(a, d.C);
     const int cols = Lp * d.C, tp = threads_for(cols);
     if ((d.C & 1) == 0 && tp % cols == 0 && 2 * (size_t)a.N * cols * sizeof(float2) <= kFftSmemCap) {
+      if (!d.in_mask && tma_passes_enabled()) {  // bundles moved by the TMA unit
+        bool done = false;
+        int st = MLG_OK;
+        switch (cols) {
+          case 16: st = launch_tma<N1, N2, DIR, 16>(a, d, Lp, s, &done); break;
+          case 24: st = launch_tma<N1, N2, DIR, 24>(a, d, Lp, s, &done); break;
+          case 32: st = launch_tma<N1, N2, DIR, 32>(a, d, Lp, s, &done); break;
+          default: break;
+        }
+        if (st != MLG_OK || done) return st;
+      }
       // the column counts of 2, 4, 8, 12, 16, 24 and 32 coils: compile-time
       switch (cols) {
         case 16: return launch_pipe<N1, N2, DIR, kFftThreads, 16>(a, d, Lp, tp, s);

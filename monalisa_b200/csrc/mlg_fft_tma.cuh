@@ -1,0 +1,308 @@
+// Line-FFT passes moved by the tensor memory accelerator (TMA): the plain
+// pipelined pass (zero-filled load, transform, cropped store) with its line
+// bundles copied global -> shared and shared -> global by
+// cp.async.bulk.tensor instead of per-thread 16-byte copies.  Included by
+// mlg_fft_kernels.cuh (it uses the register transforms defined there).
+//
+// A CTA = NT transform threads (a multiple of the bundle's columns, as in
+// fft_pass_pipe_kernel) + one producer warp.  The bundle of line group b
+// (L lines x C coils, N rows) is one 4-D box of the volume
+//   d0: the 2C floats of one cell, d1: line index u, d2: the FFT axis,
+//   d3: line index v
+// so one instruction loads it.  The input tensor's FFT-axis extent is the
+// stored range [in_lo, in_lo + in_len) and the box starts at -in_lo: rows
+// outside that range (and lines past the grid edge) arrive as zeros from the
+// TMA unit's out-of-bounds fill.  The transform leaves the line in natural
+// order, so the kept rows [out_lo, out_lo + out_len) are one contiguous box
+// for the store.  NSLOT shared buffers rotate: the producer loads bundle
+// it + NSLOT - 1 ahead while the transform threads work on bundle it; after
+// a bundle's transform it stores the bundle and, once the store has read the
+// buffer, loads the next bundle into it.
+//
+// Every wait is bounded (kTmaWaitNs of wall-clock time): a wait that runs out
+// sets *err, makes the CTA's other waits give up at once, and the CTA returns
+// after the copies it issued have finished.  No multicast form is used: each
+// CTA reads and writes this GPU's own buffers only.
+#pragma once
+
+#include <cuda.h>
+
+#include <cstdint>
+
+namespace mlg {
+
+constexpr unsigned long long kTmaWaitNs = 2000000000ull;  // 2 s per wait
+
+struct TmaPass {
+  int L = 1;          // lines per bundle
+  int gu = 1;         // bundles along u
+  int nbundles = 0;
+  int in_chunks = 1;  // load boxes per bundle
+  int in_rows = 0;    // rows per load box (in_chunks * in_rows = N)
+  int in_lo = 0;      // first stored input row
+  int out_lo = 0;     // first kept output row
+  int out_chunks = 1;
+  int out_rows = 0;   // rows per store box (out_chunks * out_rows = out_len)
+  int* err = nullptr; // set to 1 when a wait runs out (device word), or NULL
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(uint32_t addr, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(addr), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Waits for phase `parity` of *bar to complete.  Gives up (returns false)
+// when *abort is set or after kTmaWaitNs, in which case it sets *abort and
+// *err.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort, int* err) {
+  const uint32_t addr = smem_u32(bar);
+  if (mbar_try(addr, parity)) return true;
+  const unsigned long long t0 = global_ns();
+  for (;;) {
+    if (mbar_try(addr, parity)) return true;
+    if (*abort) return false;
+    if (global_ns() - t0 > kTmaWaitNs) {
+      *abort = 1;
+      if (err) atomicExch(err, 1);
+      return false;
+    }
+  }
+}
+
+// The same wait without the abort flag (draining copies already issued).
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+  const uint32_t addr = smem_u32(bar);
+  const unsigned long long t0 = global_ns();
+  while (!mbar_try(addr, parity))
+    if (global_ns() - t0 > kTmaWaitNs) return false;
+  return true;
+}
+
+__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,
+                                            uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+      "%5}], [%6];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void tma_store_4d(const CUtensorMap* map, int c0, int c1, int c2, int c3,
+                                             const void* src) {
+  asm volatile("cp.async.bulk.tensor.4d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3, %4}], [%5];" ::"l"(
+                   reinterpret_cast<uint64_t>(map)),
+               "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(src))
+               : "memory");
+}
+
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// barrier 1 over the NT transform threads (the producer warp never joins)
+template <int NT>
+__device__ __forceinline__ void bar_transform() {
+  asm volatile("bar.sync 1, %0;" ::"n"(NT) : "memory");
+}
+
+// barrier 1 over the NT transform threads returning the OR of v
+template <int NT>
+__device__ __forceinline__ bool bar_transform_or(bool v) {
+  uint32_t r;
+  asm volatile(
+      "{\n .reg .pred p, q;\n setp.ne.u32 q, %1, 0;\n bar.red.or.pred p, 1, %2, q;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(r)
+      : "r"((uint32_t)v), "n"(NT)
+      : "memory");
+  return r != 0;
+}
+
+// Sub-transforms of step C per thread: all of a thread's step-C inputs stay
+// in registers until every thread has read its own (KI * N2 values).
+template <int N1, int N2, int COLS, int NT>
+constexpr int tma_step_c_iters() {
+  return (N1 + NT / COLS - 1) / (NT / COLS);
+}
+
+// smem_fft_fixed with the result in natural order (X[k] at row k): step A
+// as there; step C reads all of a thread's rows, waits for every thread to
+// have read its own, then writes row k1 + N1 k2.  Barriers are over the NT
+// transform threads only.
+template <int N1, int N2, int DIR, int COLS, int NT>
+__device__ __forceinline__ void smem_fft_natural(float2* s, const float2* __restrict__ tw) {
+  constexpr int G = NT / COLS;
+  constexpr int KI = tma_step_c_iters<N1, N2, COLS, NT>();
+  const int col = threadIdx.x % COLS, g = threadIdx.x / COLS;
+  float2* const sc = s + col;
+#pragma unroll
+  for (int n2b = 0; n2b < N2; n2b += G) {
+    const int n2 = n2b + g;
+    if (N2 % G == 0 || n2 < N2) {
+      float2* const p = sc + n2 * COLS;
+      float2 r[N1];
+#pragma unroll
+      for (int n1 = 0; n1 < N1; ++n1) r[n1] = p[n1 * N2 * COLS];
+      reg_fft<N1, DIR>(r);
+      if (n2) {
+#pragma unroll
+        for (int k1 = 1; k1 < N1; ++k1) r[k1] = cmulf(r[k1], twid<DIR>(tw, n2 * k1));
+      }
+#pragma unroll
+      for (int k1 = 0; k1 < N1; ++k1) p[k1 * N2 * COLS] = r[k1];
+    }
+  }
+  bar_transform<NT>();
+  float2 r[KI][N2];
+#pragma unroll
+  for (int i = 0; i < KI; ++i) {
+    const int k1 = i * G + g;
+    if (N1 % G == 0 || k1 < N1) {
+      const float2* const p = sc + k1 * N2 * COLS;
+#pragma unroll
+      for (int n2 = 0; n2 < N2; ++n2) r[i][n2] = p[n2 * COLS];
+      reg_fft<N2, DIR>(r[i]);
+    }
+  }
+  bar_transform<NT>();
+#pragma unroll
+  for (int i = 0; i < KI; ++i) {
+    const int k1 = i * G + g;
+    if (N1 % G == 0 || k1 < N1) {
+#pragma unroll
+      for (int k2 = 0; k2 < N2; ++k2) sc[(k1 + N1 * k2) * COLS] = r[i][k2];
+    }
+  }
+}
+
+template <int N, int COLS, int NSLOT>
+constexpr int tma_min_blocks() {
+  const int per = NSLOT * N * COLS * 8 + 2048;
+  const int by_smem = (227 * 1024) / per;
+  return by_smem < 1 ? 1 : (by_smem > 3 ? 3 : by_smem);
+}
+
+template <int N1, int N2, int DIR, int COLS, int NSLOT>
+__global__ void __launch_bounds__(cta_threads(COLS) + 32, (tma_min_blocks<N1 * N2, COLS, NSLOT>()))
+    fft_pass_tma_kernel(const __grid_constant__ CUtensorMap tin, const __grid_constant__ CUtensorMap tout, TmaPass a,
+                        const float2* __restrict__ tw) {
+  constexpr int N = N1 * N2, NT = cta_threads(COLS);
+  constexpr unsigned kBuf = (unsigned)N * COLS * 8;  // bytes per bundle
+  extern __shared__ unsigned char tma_smem_raw[];
+  // 128-byte aligned buffers (TMA boxes in shared memory), then the barriers
+  unsigned char* base =
+      reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(tma_smem_raw) + 127) & ~uintptr_t(127));
+  uint64_t* full = reinterpret_cast<uint64_t*>(base + NSLOT * kBuf);
+  uint64_t* done = full + NSLOT;
+  __shared__ int abort_flag;
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    abort_flag = 0;
+#pragma unroll
+    for (int i = 0; i < NSLOT; ++i) {
+      mbar_init(full + i, 1);
+      mbar_init(done + i, NT);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  volatile int* abort = &abort_flag;
+  const int G = gridDim.x;
+  if (tid >= NT) {
+    if (tid != NT) return;
+    // producer: one thread
+    auto load = [&](int slot, int b) {
+      unsigned char* dst = base + slot * kBuf;
+      mbar_arrive_expect_tx(full + slot, kBuf);
+      const int c1 = (b % a.gu) * a.L, c3 = b / a.gu;
+      for (int k = 0; k < a.in_chunks; ++k)
+        tma_load_4d(dst + (size_t)k * a.in_rows * COLS * 8, &tin, 0, c1, k * a.in_rows - a.in_lo, c3, full + slot);
+    };
+    auto store = [&](int slot, int b) {
+      const unsigned char* src = base + slot * kBuf + (size_t)a.out_lo * COLS * 8;
+      const int c1 = (b % a.gu) * a.L, c3 = b / a.gu;
+      for (int k = 0; k < a.out_chunks; ++k)
+        tma_store_4d(&tout, 0, c1, k * a.out_rows, c3, src + (size_t)k * a.out_rows * COLS * 8);
+      bulk_commit();
+    };
+    int it = 0;
+    bool ok = true;
+    for (int b = blockIdx.x; b < a.nbundles; b += G, ++it) {
+      const int slot = it % NSLOT;
+      if (it >= NSLOT) {  // the slot held bundle it - NSLOT: store it first
+        if (!mbar_wait(done + slot, (unsigned)((it / NSLOT) - 1) & 1u, abort, a.err)) {
+          ok = false;
+          break;
+        }
+        store(slot, b - NSLOT * G);
+        bulk_wait_read_all();  // the store has read the buffer
+      }
+      load(slot, b);
+    }
+    const int issued = it;
+    if (ok) {  // the last NSLOT bundles
+      for (int k = issued > NSLOT ? issued - NSLOT : 0; k < issued; ++k) {
+        const int slot = k % NSLOT;
+        if (!mbar_wait(done + slot, (unsigned)(k / NSLOT) & 1u, abort, a.err)) {
+          ok = false;
+          break;
+        }
+        store(slot, blockIdx.x + k * G);
+      }
+    }
+    if (!ok) {  // let every load already issued land before the CTA leaves
+      for (int k = issued > NSLOT ? issued - NSLOT : 0; k < issued; ++k)
+        mbar_wait_bounded(full + k % NSLOT, (unsigned)(k / NSLOT) & 1u);
+    }
+    bulk_wait_all();
+    return;
+  }
+  // transform threads
+  int it = 0;
+  for (int b = blockIdx.x; b < a.nbundles; b += G, ++it) {
+    const int slot = it % NSLOT;
+    const bool ok = mbar_wait(full + slot, (unsigned)(it / NSLOT) & 1u, abort, a.err);
+    if (bar_transform_or<NT>(!ok)) return;  // all transform threads leave together
+    smem_fft_natural<N1, N2, DIR, COLS, NT>(reinterpret_cast<float2*>(base + slot * kBuf), tw);
+    fence_proxy_async_smem();  // the transform's writes become visible to the store
+    mbar_arrive(done + slot);
+  }
+}
+
+// Host: 4-D tensor map of a coil-fastest volume seen as the line boxes of
+// one pass (mlg_fft.cu).  Strides in float2 units; box = (2C floats, box_L
+// lines, box_rows rows, 1).
+int tma_line_map(CUtensorMap* map, const void* base, int C, int dim_u, long long st_u, int len, long long st_ax,
+                 int dim_v, long long st_v, int box_L, int box_rows);
+// Whether the TMA passes are enabled (MLG_FFT_TMA=0 turns them off).
+bool tma_passes_enabled();
+
+}  // namespace mlg

@@ -42,6 +42,7 @@ struct mlg_plan_s {
   uint32_t* line_mask = nullptr;
   int line_mask_words = 0;
   double* scalars = nullptr;      // solver scalars (device)
+  int* wait_err = nullptr;        // the device's pass wait flag (fft_wait_word, not owned)
   cudaStream_t stream = nullptr;  // internal non-blocking stream
   cudaEvent_t ev_in = nullptr, ev_out = nullptr;
   size_t bytes = 0;

@@ -429,7 +429,7 @@ int mlg_sensa(mlg_plan_t p, const float* yR, const float* yI, const float* ve, f
   MLG_CUDA(cudaMemcpyAsync(xR, dx.p, sizeof(float) * nx, cudaMemcpyDeviceToHost, s));
   MLG_CUDA(cudaMemcpyAsync(xI, dx.p + nx, sizeof(float) * nx, cudaMemcpyDeviceToHost, s));
   MLG_CUDA(cudaStreamSynchronize(s));
-  return MLG_OK;
+  return mlg::fft_wait_status(p->wait_err, s);
 }
 
 }  // extern "C"

@@ -215,6 +215,11 @@ class NufftPlan:
         N.call("mlg_plan_autotune", self._h, int(reps), N.dptr(ms))
         return {n: float(t) for n, t in zip(self.ADJOINT_MODES, ms) if t >= 0}
 
+    def status(self) -> None:
+        """Synchronises the plan's stream; raises MonalisaError (timeout) when
+        a bounded wait inside a device pass ran out since the last check."""
+        N.call("mlg_plan_status", self._h)
+
     def device_bytes(self) -> int:
         b = ctypes.c_longlong()
         N.call("mlg_plan_device_bytes", self._h, ctypes.byref(b))

@@ -153,7 +153,8 @@ def test_c2_leight_gridder_matches_oracle(c2):
            float(w.kernelParam[1]), N.tptr(bR), N.tptr(bI), N.stream_ptr())
     got = bR.cpu().numpy() + 1j * bI.cpu().numpy()
     del bR, bI
-    rR, rI = oracle.port_gridder_leight(3, aR, aI, tx[0], tx[1], tx[2], Dn, nCh, nPt, Ns[0], Ns[1], Ns[2],
+    # the restatement takes the MEX layout [nCh, nPt] (coil fastest in memory)
+    rR, rI = oracle.port_gridder_leight(3, aR.T, aI.T, tx[0], tx[1], tx[2], Dn, nCh, nPt, Ns[0], Ns[1], Ns[2],
                                         int(w.nWin), float(w.kernelParam[0]), float(w.kernelParam[1]))
     assert rel(got, (np.asarray(rR) + 1j * np.asarray(rI)).T) <= 1e-5  # [nCh, Nu] -> [Nu][nCh]
 
