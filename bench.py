@@ -16,8 +16,11 @@ GPUs), so `value` = (ranks x steps) / max-over-ranks time.
 The reference arm times the reference's CPU path on the host cores: its own
 C++ sparse-matrix kernel (compiled from source into oracle/_ref; the plain-C
 restatement when that is absent) inside the numpy/scipy restatement of the
-MATLAB operators, on a bounded sample (one forward + one adjoint operator
-application) extrapolated to a full reconstruction.
+MATLAB operators.  Each step is a bounded sample (one forward + one adjoint
+operator application on 8 of the 16 coils, about 12 s on 16 cores),
+extrapolated to a full reconstruction; `--ref-sample full` times whole
+reconstructions instead (about 12 minutes each), which validates the
+extrapolation.
 """
 from __future__ import annotations
 
@@ -141,7 +144,7 @@ class PlainGpuSensa:
     and bmSensa.m's CG loop with single-precision dot products and a host
     check of the stopping test each step.  Not part of the library."""
 
-    def __init__(self, w, Gu, Gut, KFC, KFCc, dev):
+    def __init__(self, w, Gu, Gut, KFC, KFCc, dev, dtype=None):
         import warnings
 
         import torch
@@ -149,6 +152,10 @@ class PlainGpuSensa:
         warnings.filterwarnings("ignore", message=".*[Ss]parse.*")
         self.t = torch
         self.dev = dev
+        # complex64 (the plain arm) or complex128: the same discrete
+        # reconstruction with every product in double (FP32 inputs promoted)
+        self.dtype = dtype or torch.complex64
+        rdt = torch.float64 if self.dtype == torch.complex128 else torch.float32
         self.n = [int(v) for v in w.n_u]
         self.N = [int(v) for v in w.N_u]
         self.nCh = int(w.nCh)
@@ -156,20 +163,20 @@ class PlainGpuSensa:
         def csr(D):
             indptr, indices, data = D.download().to_csr()
             return torch.sparse_csr_tensor(torch.from_numpy(indptr.astype(np.int32)).to(dev),
-                                           torch.from_numpy(indices).to(dev), torch.from_numpy(data).to(dev),
+                                           torch.from_numpy(indices).to(dev), torch.from_numpy(data).to(dev, rdt),
                                            size=(D.l_size, D.r_size))
 
         self.Gu, self.Gut = csr(Gu), csr(Gut)
         nu = int(np.prod(self.n))
-        self.KFC = torch.from_numpy(np.ascontiguousarray(np.asarray(KFC, np.complex64).reshape(nu, -1, order="F").T)).to(dev)
-        self.KFCc = torch.from_numpy(np.ascontiguousarray(np.asarray(KFCc, np.complex64).reshape(nu, -1, order="F").T)).to(dev)
+        self.KFC = torch.from_numpy(np.ascontiguousarray(np.asarray(KFC, np.complex64).reshape(nu, -1, order="F").T)).to(dev, self.dtype)
+        self.KFCc = torch.from_numpy(np.ascontiguousarray(np.asarray(KFCc, np.complex64).reshape(nu, -1, order="F").T)).to(dev, self.dtype)
         self.dims = tuple(range(1, 1 + len(self.n)))
         self.box = tuple(slice(N // 2 - n // 2, N // 2 - n // 2 + n) for N, n in zip(self.N[::-1], self.n[::-1]))
 
     def M(self, x):
         t, C = self.t, self.nCh
         v = (self.KFC * x[None, :]).reshape(C, *self.n[::-1])
-        g = t.zeros((C, *self.N[::-1]), dtype=t.complex64, device=self.dev)
+        g = t.zeros((C, *self.N[::-1]), dtype=self.dtype, device=self.dev)
         g[(slice(None),) + self.box] = v
         g = t.fft.fftshift(t.fft.fftn(t.fft.ifftshift(g, dim=self.dims), dim=self.dims), dim=self.dims)
         g = t.view_as_real(g.reshape(C, -1).T.contiguous()).reshape(-1, 2 * C)
@@ -187,8 +194,9 @@ class PlainGpuSensa:
     def sensa(self, y, ve, HX, nCGD):
         t = self.t
         eps = 10 * float(np.finfo(np.float32).eps)
-        HY = t.minimum(ve, ve.max())
-        x = t.zeros(int(np.prod(self.n)), dtype=t.complex64, device=self.dev)
+        y = y.to(self.dtype)
+        HY = t.minimum(ve, ve.max()).to(self.KFC.real.dtype)
+        x = t.zeros(int(np.prod(self.n)), dtype=self.dtype, device=self.dev)
         invHX = float(np.float32(1) / np.float32(HX))
         res = y - self.M(x)
         dagM = self.MH(res, HY, invHX)
@@ -210,6 +218,35 @@ class PlainGpuSensa:
         r = y - self.M(x)  # monitoring (bmSensa.m:82-83)
         float(t.vdot(r.reshape(-1), (HY[:, None] * r).reshape(-1)).real)
         return x
+
+
+def nudft_fp64(x, C, t, n_u, dK_u, N_u, dev):
+    """FP64 direct NUDFT of an image on the device: y_j = sum_r C(r) x(r)
+    exp(-2 pi i k_j . r) / prod(N_u) / prod(dK_u), pixel r of index i at
+    (i - n_u/2) / (dK_u N_u), k_j = t[:, j] in physical units -- what the
+    gridded forward operator approximates (no window, no deapodisation)."""
+    import torch
+
+    n_u = [int(v) for v in n_u]
+    N_u = np.asarray(N_u, np.float64)
+    dK_u = np.asarray(dK_u, np.float64)
+    dX = 1.0 / (dK_u * N_u)
+    nPix = int(np.prod(n_u))
+    idx = torch.arange(nPix, device=dev)
+    r, stride = [], 1
+    for d, n in enumerate(n_u):
+        r.append(((idx // stride) % n - n // 2).to(torch.float64) * float(dX[d]))
+        stride *= n
+    r = torch.stack(r, 0)  # [imDim, nPix]
+    Cx = torch.as_tensor(np.asarray(C, np.complex64), device=dev).to(torch.complex128) * \
+        torch.as_tensor(np.asarray(x, np.complex64), device=dev).to(torch.complex128)[:, None]
+    tt = torch.as_tensor(np.asarray(t, np.float64), device=dev)  # [imDim, nS]
+    out = torch.zeros((tt.shape[1], Cx.shape[1]), dtype=torch.complex128, device=dev)
+    for p0 in range(0, nPix, 65536):
+        ph = torch.exp(torch.complex(torch.zeros((), dtype=torch.float64, device=dev),
+                                     -2 * np.pi * (tt.T @ r[:, p0:p0 + 65536])))
+        out += ph @ Cx[p0:p0 + 65536]
+    return out * (1.0 / float(np.prod(N_u)) / float(np.prod(dK_u)))
 
 
 def run_gpu(args):
@@ -357,8 +394,12 @@ def run_gpu(args):
     adjoint_c2 = rec.plan.adjoint_mode
     if not args.no_extra:
         x_fp32 = x.clone()
+        ref64 = _c4_references(w, Gu, Gut, rec, y, ve, x_fp32, dev)
         extra["c4_mixed_precision"] = {
-            p: _mixed(w, Gu, Gut, y, ve, x_fp32, ms / args.steps, plain, stream, p) for p in ("mixed", "fp16_values")}
+            "fp32": {"rel_err_vs_fp64": ref64["fp32_vs_fp64"], "nudft_rel_err": ref64["nudft_fp32"]},
+            **{p: _mixed(w, Gu, Gut, y, ve, x_fp32, ms / args.steps, plain, stream, ref64, p)
+               for p in ("mixed", "fp16_values")},
+            "fp64_reference": ref64["about"]}
         rec.plan.close()
         extra["c1_radial2d"] = _c1(stream)
         from monalisa_b200.workloads import radial2d
@@ -376,9 +417,7 @@ def run_gpu(args):
         "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "c64 (fp32 data, fp64 CG scalars)",
         "data": "synthetic (seeded koosh-ball trajectory, random coil maps, ellipsoid phantom)",
-        "config": {"workload": "3D koosh-ball CG-SENSE: 128^3 image, 256^3 grid, 4096x256 samples, 16 coils, "
-                               "30 CG iterations", "parallelism": f"replicas x{ws}",
-                   "l2": "working set (2.1 GB grid) larger than L2 each step", **w.info},
+        "config": _config(w, ws),
         "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
         "recon_rel_err_vs_phantom": round(err, 5), "setup_s": round(setup_s, 2),
         "autotune": {"adjoint": adjoint_c2, "ms": {k: round(v, 4) for k, v in (rec.tuning or {}).items()}},
@@ -404,10 +443,64 @@ def _event_ms(fn, reps, stream):
     return e0.elapsed_time(e1) / reps
 
 
-def _mixed(w, Gu, Gut, y, ve, x_fp32, ms_fp32, plain, stream, precision="mixed"):
+def _HX(w):
+    """HX = prod((1/dK_u)/N_u) in single precision (bmSensa.m:26-27)."""
+    HX = np.float32(1)
+    for d in range(len(w.N_u)):
+        HX = np.float32(HX * np.float32(np.float32(1) / np.float32(w.dK_u[d]) / np.float32(w.N_u[d])))
+    return float(HX)
+
+
+def _forward_rounded(plan, x, half):
+    """The forward model of a plan, rounded as the mixed solver stores M p
+    (FP16 times the power of two that puts its largest component below
+    2^12) when `half`."""
+    import torch
+
+    y = plan.shanna(x)
+    if half:
+        yr = torch.view_as_real(y)
+        s = 2.0 ** (12 - np.frexp(float(yr.abs().max()))[1])
+        y = torch.view_as_complex(((yr * s).to(torch.float16).to(torch.float32) / s).contiguous())
+    return y
+
+
+def _c4_references(w, Gu, Gut, rec, y, ve, x_fp32, dev):
+    """c4's references at full size: (i) the FP64 restatement of the same
+    discrete reconstruction (bmSensa.m with every product in double: the
+    FP32 matrices, KFC and data promoted to FP64, torch.fft / torch.sparse
+    in complex128 on the device), and (iii) the FP64 direct NUDFT of the
+    phantom at 2048 seeded samples, against which each precision's forward
+    model is compared (the gridding approximation itself)."""
+    import torch
+
+    pg = PlainGpuSensa(w, Gu, Gut, rec.KFC, rec.KFC_conj, dev, dtype=torch.complex128)
+    x64 = pg.sensa(y, ve, _HX(w), w.nCGD)
+    del pg
+    torch.cuda.empty_cache()
+    idx = np.sort(np.random.default_rng(2048).choice(w.nPt, 2048, replace=False))
+    nud = nudft_fp64(w.x_true, w.C, w.t[:, idx], w.n_u, w.dK_u, w.N_u, dev)
+    xt = torch.from_numpy(w.x_true).to(dev)
+    idx_d = torch.from_numpy(idx).to(dev)
+
+    def nudft_err(plan, half):
+        yy = _forward_rounded(plan, xt, half)[idx_d].to(torch.complex128)
+        return float((yy - nud).norm() / nud.norm())
+
+    rel64 = lambda xx: float((xx.to(torch.complex128) - x64).norm() / x64.norm())
+    return {"x64": x64, "rel64": rel64, "nudft_err": nudft_err, "fp32_vs_fp64": rel64(x_fp32),
+            "nudft_fp32": nudft_err(rec.plan, False),
+            "about": "(i) FP64 restatement: bmSensa with FP32 inputs promoted to complex128, torch.fft/torch.sparse "
+                     "on the device, 30 CG; (iii) FP64 direct NUDFT of the phantom at 2048 seeded samples vs each "
+                     "precision's forward model (mixed: M p rounded to scaled FP16 as the solver stores it)"}
+
+
+def _mixed(w, Gu, Gut, y, ve, x_fp32, ms_fp32, plain, stream, ref64, precision="mixed"):
     """c4: the c2 reconstruction in reduced precision: 'mixed' (FP16 matrix
     values, M p stored in scaled FP16, FP32 residual and sums, FP64 scalars) or
-    'fp16_values' (FP16 matrix values only)."""
+    'fp16_values' (FP16 matrix values only).  Errors: against the FP64
+    restatement (gate 1e-3), the FP32 reconstruction, and the change of the
+    forward model's error against the FP64 NUDFT (at most 1e-3)."""
     import torch
 
     import monalisa_b200 as mb
@@ -427,16 +520,24 @@ def _mixed(w, Gu, Gut, y, ve, x_fp32, ms_fp32, plain, stream, precision="mixed")
            "speedup_vs_fp32": round(ms_fp32 / ms, 3),
            "speedup_vs_plain_gpu": round(plain["ms_per_recon"] / ms, 2) if plain else None,
            "rel_diff_vs_fp32_recon": float((x - x_fp32).norm() / x_fp32.norm()),
+           "rel_err_vs_fp64": ref64["rel64"](x),
+           "nudft_rel_err": ref64["nudft_err"](rec.plan, precision == "mixed"),
            "adjoint": rec.plan.adjoint_mode,
            "precision": {"mixed": "fp16 matrix values, M p in fp16 x 2^k per CG step, fp32 residual/sums/FFT, "
                                   "fp64 CG scalars",
                          "fp16_values": "fp16 matrix values, fp32 k-space/sums/FFT, fp64 CG scalars"}[precision]}
+    out["nudft_err_delta"] = out["nudft_rel_err"] - ref64["nudft_fp32"]
+    out["gates"] = {"rel_err_vs_fp64 <= 1e-3": out["rel_err_vs_fp64"] <= 1e-3,
+                    "nudft_err_delta <= 1e-3": out["nudft_err_delta"] <= 1e-3}
     rec.plan.close()
     return out
 
 
 def _c1(stream):
-    """c1: 2-D golden-angle radial CG-SENSE, 256^2 / 512^2, 1 coil, KB, 20 CG."""
+    """c1: 2-D golden-angle radial CG-SENSE, 256^2 / 512^2, 1 coil, KB, 20 CG;
+    beside it the plain-GPU arm and the reference CPU path (whole
+    reconstructions: bmSensa with the reference's SpMV kernel, which runs
+    2 x nCh = 2 OpenMP threads for one coil, as in the reference)."""
     import torch
 
     import monalisa_b200 as mb
@@ -457,10 +558,29 @@ def _c1(stream):
         step()
     ms = _event_ms(step, 10, stream)
     adjoint = rec.plan.adjoint_mode
+    pg = PlainGpuSensa(w, Gu, Gut, rec.KFC, rec.KFC_conj, torch.device("cuda"))
+    HX = _HX(w)
+    pg.sensa(y, ve, HX, w.nCGD)
+    box = {}
+    ms_plain = _event_ms(lambda: box.__setitem__("x", pg.sensa(y, ve, HX, w.nCGD)), 3, stream)
+    step()
+    torch.cuda.synchronize()
+    plain = {"recons_per_s": round(1000.0 / ms_plain, 3), "ms_per_recon": round(ms_plain, 3),
+             "speedup": round(ms_plain / ms, 2), "rel_diff": float((x - box["x"]).norm() / box["x"].norm())}
+    del pg, box
+    ref = ReferenceCpu(w, _to_oracle(w, Gu), _to_oracle(w, Gut), w.y, coils=w.nCh, kfc=(rec.KFC, rec.KFC_conj))
+    ref.recon()  # warm-up
+    t_cpu = statistics.median(ref.recon() for _ in range(3))
+    x_cpu = np.asarray(ref.last_image).ravel()
+    cpu = {"value": round(1.0 / t_cpu, 4), "unit": UNIT, "s_per_recon": round(t_cpu, 3), "cores": ref.cores,
+           "kind": ref.kind, "sample": "whole reconstructions (median of 3): bmSensa restatement with the "
+                                       "reference's bmSparseMat_cC_oBlock_omp_mex and scipy.fft",
+           "rel_diff_vs_gpu": float(np.linalg.norm(x.cpu().numpy() - x_cpu) / np.linalg.norm(x_cpu))}
     rec.plan.close()
     return {"workload": "2D golden-angle radial 256^2 image, 512^2 grid, 256x512 samples, 1 coil, KB nWin 3, "
                         "20 CG iterations from x = 0 (working set inside L2)",
-            "recons_per_s": round(1000.0 / ms, 3), "ms_per_recon": round(ms, 3), "adjoint": adjoint}
+            "recons_per_s": round(1000.0 / ms, 3), "ms_per_recon": round(ms, 3), "adjoint": adjoint,
+            "vs_plain_gpu": plain, "cpu_baseline": cpu, "speedup_vs_cpu": round(t_cpu * 1e3 / ms, 1)}
 
 
 def _gridder(w, stream, label, reps=5):
@@ -534,31 +654,126 @@ def _c3(stream):
     ms = _event_ms(recon, 1, stream)
     chain.close()
     ops = w.nFr * (w.nIter * (w.nCGD + 1) + 1), w.nFr * w.nIter * w.nCGD
+    per_bin = (w.nIter * (w.nCGD + 1) + 1, w.nIter * w.nCGD)
+    # plain-GPU operators (stock cuFFT / cuSPARSE per bin, nothing fused):
+    # every bin's forward and adjoint timed once, extrapolated to the
+    # reconstruction's operator count (the ADMM vector work is not counted)
+    from monalisa_b200.workloads import Workload
+
+    KFC = mb.bmKF(w.C, w.N_u, w.n_u, w.dK_u, w.nCh, w.kernelType, w.nWin, w.kernelParam)
+    KFCc = mb.bmKF_conj(np.conj(w.C), w.N_u, w.n_u, w.dK_u, w.nCh, w.kernelType, w.nWin, w.kernelParam)
+    wb = Workload("bin", 3, w.n_u, w.N_u, w.dK_u, w.nCh, w.nCGD, w.kernelType, w.nWin, w.kernelParam)
+    ve_all = np.concatenate(w.ve).astype(np.float32)
+    offs = np.concatenate([[0], np.cumsum(w.nPt)])
+    HX = _HX(wb)
+    fwd_ms = bwd_ms = 0.0
+    for f in range(w.nFr):
+        pg = PlainGpuSensa(wb, mats[f][0], mats[f][1], KFC, KFCc, torch.device("cuda"))
+        xf = torch.from_numpy(w.x_true[f]).cuda()
+        hy = torch.from_numpy(np.minimum(ve_all[offs[f]:offs[f + 1]], np.float32(10.0))).cuda()
+        pg.M(xf)
+        pg.MH(ys[f], hy, 1.0 / HX)
+        fwd_ms += _event_ms(lambda: pg.M(xf), 2, stream)
+        bwd_ms += _event_ms(lambda: pg.MH(ys[f], hy, 1.0 / HX), 2, stream)
+        del pg
+    plain_ms = per_bin[0] * fwd_ms + per_bin[1] * bwd_ms
+    # reference CPU path: one forward + one adjoint on 8 of the 12 coils for
+    # the bins with the fewest and the most samples, a line in the sample
+    # count through the two, summed over the bins and their operator counts
+    order = np.argsort(w.nPt)
+    pts, cost = [], []
+    ref = None
+    for f in (int(order[0]), int(order[-1])):
+        wf = Workload("bin", 3, w.n_u, w.N_u, w.dK_u, w.nCh, w.nCGD, w.kernelType, w.nWin, w.kernelParam)
+        wf.t, wf.ve, wf.C, wf.x_true = w.t[f], w.ve[f], w.C, w.x_true[f]
+        ref = ReferenceCpu(wf, _to_oracle(wf, mats[f][0]), _to_oracle(wf, mats[f][1]), ys[f].cpu().numpy(), coils=8,
+                           kfc=(KFC, KFCc))
+        fwd, adj = ref.sample()
+        sc = w.nCh / ref.coils
+        pts.append(w.nPt[f])
+        cost.append((fwd * sc, adj * sc))
+    slope = [(cost[1][k] - cost[0][k]) / max(pts[1] - pts[0], 1) for k in range(2)]
+    cpu_s = sum(per_bin[k] * (cost[0][k] + slope[k] * (n - pts[0])) for n in w.nPt for k in range(2))
     return {"workload": "20 koosh frame bins (200-1500 spokes x 256), 96^3 image, 192^3 grid, 12 coils, "
                         "temporal-TV ADMM 30 x 5 CG",
             "recons_per_s": round(1000.0 / ms, 4), "s_per_recon": round(ms / 1000.0, 3),
             "ms_per_admm_iteration": round(ms / w.nIter, 2), "shanna_nakatsha_per_recon": list(ops),
-            "objective_first_last": [hist[0][0], hist[-1][0]], "samples": int(sum(w.nPt))}
+            "objective_first_last": [hist[0][0], hist[-1][0]], "samples": int(sum(w.nPt)),
+            "vs_plain_gpu": {"s_per_recon": round(plain_ms / 1e3, 3), "speedup": round(plain_ms / ms, 2),
+                             "arm": "torch.fft + torch.sparse CSR operators per bin, each bin's forward and "
+                                    "adjoint timed once and multiplied by the operator counts (ADMM vector work "
+                                    "not counted)"},
+            "cpu_baseline": {"s_per_recon": round(cpu_s, 1), "value": round(1.0 / cpu_s, 6), "unit": UNIT,
+                             "cores": ref.cores, "kind": ref.kind,
+                             "sample": f"1 forward + 1 adjoint on 8 of 12 coils for the bins of {pts[0]} and "
+                                       f"{pts[1]} samples (x1.5 coils), linear in the sample count, summed over "
+                                       f"the 20 bins x {per_bin[0]} forward + {per_bin[1]} adjoint applications"},
+            "speedup_vs_cpu": round(cpu_s * 1e3 / ms, 1)}
 
 
 def _c5():
     """c5: the serving mix (60 % 2-D, 40 % 3-D, 8-16 coils, 20 CG), Poisson
-    arrivals at 50 requests/s, continuous admission on one GPU."""
+    arrivals, continuous admission on one GPU: 2000 requests at the
+    configuration's 50 requests/s and 1000 at 20 requests/s (below the GPU's
+    capacity for this mix, so latency there is mostly service time).  Beside
+    them, serial per-request latencies of the plain-GPU arm (whole
+    reconstructions with stock cuFFT / cuSPARSE calls) and of the reference
+    CPU path (one forward + one adjoint on up to 8 coils, extrapolated to 22
+    forward + 20 adjoint applications on all coils), averaged over the mix."""
+    import torch
+
+    import monalisa_b200 as mb
     from monalisa_b200 import serving
-    from monalisa_b200.workloads import serving_schedule, serving_templates
+    from monalisa_b200.workloads import Workload, serving_schedule, serving_templates
 
     templates = serving_templates()
     for k, tp in enumerate(templates):
         tp["y"] = serving.simulate_data(tp, seed=k)
     server = serving.ReconServer(workers=4)
     serving.run_poisson(server, templates, np.zeros(len(templates)), np.arange(len(templates)))
-    arrivals, tmpl = serving_schedule(150, 50.0)
-    reqs = serving.run_poisson(server, templates, arrivals, tmpl)
+    runs = {}
+    for rate, n in ((50.0, 2000), (20.0, 1000)):
+        arrivals, tmpl = serving_schedule(n, rate)
+        reqs = serving.run_poisson(server, templates, arrivals, tmpl)
+        runs[f"{rate:g}_req_per_s"] = {"offered_rate": rate, **{k: (round(v, 2) if isinstance(v, float) else v)
+                                                                 for k, v in serving.latency_stats(reqs).items()}}
     server.close()
-    return {"workload": "Poisson 50 req/s, 150 requests: 60% 2D 256^2/512^2 (128-512 spokes x 512), 40% 3D "
-                        "96^3-128^3 (1024-4096 spokes x 256), 8-16 coils, CG-SENSE 20",
-            "offered_rate": 50.0, **{k: (round(v, 2) if isinstance(v, float) else v)
-                                     for k, v in serving.latency_stats(reqs).items()}}
+    # serial latency per template: plain GPU and reference CPU
+    dev = torch.device("cuda")
+    stream = torch.cuda.current_stream()
+    plain_ms, cpu_s = [], []
+    ref = None
+    for k, tp in enumerate(templates):
+        nCh = tp["C"].shape[1]
+        kt, kp = ("kaiser", [1.95, 10, 10]) if tp["imDim"] == 2 else ("gauss", [0.61, 10])
+        wt = Workload(f"t{k}", tp["imDim"], tp["n_u"], tp["N_u"], np.ones(tp["imDim"]), nCh, 20, kt, 3, kp)
+        wt.t, wt.ve, wt.C, wt.x_true = tp["t"], tp["ve"], tp["C"], tp["x_true"]
+        Gu, Gut = mb.bmTraj2SparseMat(wt.t, wt.ve, wt.N_u, wt.dK_u, kt, 3, kp)
+        KFC = mb.bmKF(wt.C, wt.N_u, wt.n_u, wt.dK_u, nCh, kt, 3, kp)
+        KFCc = mb.bmKF_conj(np.conj(wt.C), wt.N_u, wt.n_u, wt.dK_u, nCh, kt, 3, kp)
+        pg = PlainGpuSensa(wt, Gu, Gut, KFC, KFCc, dev)
+        yd = torch.from_numpy(np.asarray(tp["y"], np.complex64)).to(dev)
+        ved = torch.from_numpy(np.asarray(wt.ve, np.float32)).to(dev)
+        pg.sensa(yd, ved, _HX(wt), 20)
+        plain_ms.append(_event_ms(lambda: pg.sensa(yd, ved, _HX(wt), 20), 1, stream))
+        del pg
+        ref = ReferenceCpu(wt, _to_oracle(wt, Gu), _to_oracle(wt, Gut), tp["y"], coils=8, kfc=(KFC, KFCc))
+        fwd, adj = ref.sample()
+        cpu_s.append(ref.recon_s(fwd, adj))
+    _, tmpl = serving_schedule(2000, 50.0)
+    mix = np.bincount(tmpl, minlength=len(templates)) / len(tmpl)
+    mean_plain = float(np.dot(mix, plain_ms))
+    mean_cpu = float(np.dot(mix, cpu_s))
+    return {"workload": "Poisson arrivals: 60% 2D 256^2/512^2 (128-512 spokes x 512), 40% 3D 96^3-128^3 "
+                        "(1024-4096 spokes x 256), 8-16 coils, CG-SENSE 20, 4 workers, admission by free HBM",
+            **runs,
+            "plain_gpu_serial": {"mean_ms_per_request": round(mean_plain, 1),
+                                 "recons_per_s": round(1e3 / mean_plain, 2),
+                                 "per_template_ms": [round(v, 1) for v in plain_ms]},
+            "cpu_serial": {"mean_s_per_request": round(mean_cpu, 2), "recons_per_s": round(1.0 / mean_cpu, 4),
+                           "per_template_s": [round(v, 2) for v in cpu_s], "cores": ref.cores, "kind": ref.kind,
+                           "sample": "per template: 1 forward + 1 adjoint on up to 8 coils, extrapolated to 22 "
+                                     "forward + 20 adjoint on all coils; averaged over the request mix"}}
 
 
 def _oracle():
@@ -577,31 +792,78 @@ def _to_oracle(w, D):
                             nWin=w.nWin, kernelParam=np.array(w.kernelParam))
 
 
+class ReferenceCpu:
+    """The reference CPU path on a workload's inputs: the reference's own
+    bmSparseMat_cC_oBlock_omp_mex (compiled from source into oracle/_ref;
+    the C restatement when that is absent) inside the numpy/scipy
+    restatement of bmShanna_MATLAB / bmNakatsha_MATLAB, scipy.fft with all
+    host threads.  A bounded sample (`sample`) is one forward and one
+    adjoint operator application on `coils` of the coils -- the operators are
+    per coil, and 8 coils already give the reference kernel's OpenMP loop
+    (2 x coils iterations) 16 threads -- extrapolated to one reconstruction of
+    (nCGD + 2) forward and nCGD adjoint applications on all coils; `recon`
+    times a whole reconstruction (bmSensa with its CG BLAS-1).  KFC /
+    KFC_conj may be given (set-up, not timed)."""
+
+    def __init__(self, w, gu, gut, y, coils=8, kfc=None):
+        oracle = _oracle()
+        self.o = oracle
+        self.w, self.gu, self.gut = w, gu, gut
+        self.kind = "reference" if oracle.ref_available() else "port"
+        self.cores = os.cpu_count() or 1
+        os.environ.setdefault("OMP_NUM_THREADS", str(self.cores))
+        self.coils = min(coils, w.nCh)
+        C = np.asarray(w.C, np.complex64)[:, :self.coils]
+        if kfc is not None:
+            self.KFC = np.ascontiguousarray(np.asarray(kfc[0])[:, :self.coils])
+            self.KFCc = np.ascontiguousarray(np.asarray(kfc[1])[:, :self.coils])
+        else:
+            self.KFC = oracle.bmKF(C, w.N_u, w.n_u, w.dK_u, self.coils, w.kernelType, w.nWin, w.kernelParam)
+            self.KFCc = oracle.bmKF_conj(np.conj(C), w.N_u, w.n_u, w.dK_u, self.coils, w.kernelType, w.nWin,
+                                         w.kernelParam)
+        self.y = np.ascontiguousarray(np.asarray(y, np.complex64)[:, :self.coils])
+        self.yfull = np.asarray(y, np.complex64)
+        self.spm = oracle.SpMV(self.kind)
+        self.last_image = None
+
+    def sample(self):
+        """Seconds of one forward and one adjoint application on the sample coils."""
+        o, w = self.o, self.w
+        x = w.x_true if w.x_true is not None else np.ones(int(np.prod(w.n_u)), np.complex64)
+        t0 = time.perf_counter()
+        o.bmShanna(x, self.gu, self.KFC, w.n_u, self.spm, workers=self.cores)
+        t1 = time.perf_counter()
+        o.bmNakatsha(self.y, self.gut, self.KFCc, True, w.n_u, self.spm, workers=self.cores)
+        t2 = time.perf_counter()
+        return t1 - t0, t2 - t1
+
+    def recon_s(self, fwd, adj):
+        w = self.w
+        return ((w.nCGD + 2) * fwd + w.nCGD * adj) * (w.nCh / self.coils)
+
+    def describe(self, fwd, adj):
+        w = self.w
+        spmv = ("reference bmSparseMat_cC_oBlock_omp_mex compiled from source" if self.kind == "reference"
+                else "C restatement")
+        return (f"1 forward ({fwd:.2f} s) + 1 adjoint ({adj:.2f} s) operator application on {self.coils} of "
+                f"{w.nCh} coils at full size, extrapolated x{w.nCh / self.coils:g} coils to {w.nCGD + 2} forward + "
+                f"{w.nCGD} adjoint applications per recon; SpMV = {spmv}, FFT = scipy.fft (workers={self.cores})")
+
+    def recon(self):
+        """Seconds of one whole reconstruction (all coils, nCGD CG updates)."""
+        o, w = self.o, self.w
+        t0 = time.perf_counter()
+        self.last_image = o.bmSensa(np.zeros(int(np.prod(w.n_u)), np.complex64), self.yfull, w.ve, w.C, self.gu,
+                                    self.gut, w.n_u, w.nCGD, spmv=self.spm, workers=self.cores)
+        return time.perf_counter() - t0
+
+
 def cpu_baseline(w, gu, gut, y):
-    """The reference CPU path on a bounded sample: one forward and one
-    adjoint operator application at full size (reference SpMV kernel +
-    scipy FFT with all host threads), extrapolated to one reconstruction of
-    (nCGD+2) forward and nCGD adjoint applications."""
-    oracle = _oracle()
-    kind = "reference" if oracle.ref_available() else "port"
-    cores = os.cpu_count() or 1
-    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
-    KFC = oracle.bmKF(w.C, w.N_u, w.n_u, w.dK_u, w.nCh, w.kernelType, w.nWin, w.kernelParam)
-    KFCc = oracle.bmKF_conj(np.conj(w.C), w.N_u, w.n_u, w.dK_u, w.nCh, w.kernelType, w.nWin, w.kernelParam)
-    spm = oracle.SpMV(kind)
-    x0 = w.x_true
-    t0 = time.perf_counter()
-    oracle.bmShanna(x0, gu, KFC, w.n_u, spm, workers=cores)
-    t1 = time.perf_counter()
-    oracle.bmNakatsha(y, gut, KFCc, True, w.n_u, spm, workers=cores)
-    t2 = time.perf_counter()
-    fwd, adj = t1 - t0, t2 - t1
-    recon_s = (w.nCGD + 2) * fwd + w.nCGD * adj
-    return {"value": round(1.0 / recon_s, 6), "unit": UNIT, "cores": cores, "kind": kind,
-            "sample": f"1 forward ({fwd:.2f} s) + 1 adjoint ({adj:.2f} s) operator application at full size, "
-                      f"extrapolated to {w.nCGD + 2} forward + {w.nCGD} adjoint per recon; SpMV = "
-                      f"{'reference bmSparseMat_cC_oBlock_omp_mex compiled from source' if kind == 'reference' else 'C restatement'}"
-                      f", FFT = scipy.fft (workers={cores})"}
+    """The reference CPU path on one bounded sample, for the GPU arm's line."""
+    ref = ReferenceCpu(w, gu, gut, y)
+    fwd, adj = ref.sample()
+    return {"value": round(1.0 / ref.recon_s(fwd, adj), 6), "unit": UNIT, "cores": ref.cores, "kind": ref.kind,
+            "sample": ref.describe(fwd, adj)}
 
 
 def run_reference(args):
@@ -617,21 +879,36 @@ def run_reference(args):
     G = oracle.traj2sparsemat(w.t, w.ve, w.N_u, w.dK_u, w.kernelType, w.nWin, w.kernelParam)
     rng = np.random.default_rng(5)
     y = (rng.standard_normal((w.nPt, w.nCh)) + 1j * rng.standard_normal((w.nPt, w.nCh))).astype(np.complex64)
-    samples = []
+    ref = ReferenceCpu(w, G["Gu"], G["Gut"], y)
+    step_s, recons = [], []
+    desc = ""
     for i in range(args.warmup + args.steps):
-        c = cpu_baseline(w, G["Gu"], G["Gut"], y)
+        if args.ref_sample == "full":
+            dt = ref.recon()
+            rs, desc = dt, f"one whole reconstruction ({w.nCGD} CG updates, all {w.nCh} coils) per step"
+        else:
+            fwd, adj = ref.sample()
+            dt, rs, desc = fwd + adj, ref.recon_s(fwd, adj), ref.describe(fwd, adj)
         if i >= args.warmup:
-            samples.append(c)
-    value = statistics.median(s["value"] for s in samples)
+            step_s.append(dt)
+            recons.append(rs)
+    value = round(1.0 / statistics.median(recons), 6)
     out = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
-           "warmup": args.warmup, "ms_per_step": round(1e3 / value, 1), "higher_is_better": True,
+           "warmup": args.warmup, "ms_per_step": round(1e3 * statistics.mean(step_s), 1),
+           "step": ("a bounded sample per step: " if args.ref_sample != "full" else "") + desc,
+           "recon_s_median": round(statistics.median(recons), 2), "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "c64", "data": "synthetic",
-           "config": {"workload": "3D koosh-ball CG-SENSE: 128^3 image, 256^3 grid, 4096x256 samples, 16 coils, "
-                                  "30 CG iterations", **w.info},
-           "cpu_baseline": {"value": value, "unit": UNIT, "kind": samples[0]["kind"], "cores": samples[0]["cores"],
-                            "sample": samples[0]["sample"]},
+           "config": _config(w, ws),
+           "cpu_baseline": {"value": value, "unit": UNIT, "kind": ref.kind, "cores": ref.cores, "sample": desc},
            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
+
+
+def _config(w, ws):
+    """The config of the headline line; the same dict in both arms."""
+    return {"workload": "3D koosh-ball CG-SENSE: 128^3 image, 256^3 grid, 4096x256 samples, 16 coils, "
+                        "30 CG iterations", "parallelism": f"replicas x{ws}",
+            "l2": "working set (2.1 GB grid) larger than L2 each step", **w.info}
 
 
 def main():
@@ -640,6 +917,8 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--ref-sample", default="sample", choices=["sample", "full"],
+                    help="reference arm: a bounded operator sample per step (default) or a whole reconstruction")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-GPU comparison arm")
     ap.add_argument("--no-extra", action="store_true", help="skip the c1 / c3 / c4 / c5 configurations")

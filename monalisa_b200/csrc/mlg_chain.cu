@@ -644,6 +644,7 @@ static int chain_monitor(mlg_chain_s* c, const float2* y, const float2* x, doubl
 static int chain_run(mlg_chain_s* c, bool spatial, const float2* y, const float* ve, float ve_max,
                      const float* delta, const float* rho, int adapt, int nIter, int nCGD, float2* x, float2* z,
                      float2* u, bool init_zu, double* history, cudaStream_t s) {
+  NvtxRange range(spatial ? "ADMM spatial TV (bmSteva)" : "ADMM temporal TV (bmTevaMorphosia_chain)");
   MLG_CHECK(nIter >= 0 && nCGD >= 0, "nIter / nCGD must be >= 0");
   MLG_CHECK(delta && rho, "NULL delta / rho");
   MLG_CHECK(!spatial || (c->nFr == 1 && !adapt), "the spatial solver runs on a chain of one frame, 'normal' mode");

@@ -92,6 +92,7 @@ void csr_free(Csr& c) {
   cudaFree(c.ord_rows);
   cudaFree(c.ord_bounds);
   cudaFree(c.val_h);
+  cudaFree(c.ord_rec);
   c = Csr();
 }
 

@@ -590,6 +590,7 @@ int leight_preload() {
 
 int leight_run(const LeightGeom& g, const LeightInputs& in, int nPt, const LeightOutput& out, LeightWorkspace& ws,
                cudaStream_t s) {
+  NvtxRange range("leight gridder (tile-binned)");
   MLG_CHECK(g.ntiles < (1LL << 31), "too many tiles");
   // the per-tile counts, their scan and the bin offsets are 32-bit: refuse
   // inputs whose (tile, sample) pairs could pass 2^31 before counting them
@@ -1210,6 +1211,7 @@ size_t leight_cells_bytes(const LeightGeom& g, int nPt) { return cells_layout(g,
 
 int leight_run_cells(const LeightGeom& g, const LeightInputs& in, int nPt, const LeightOutput& out, void* ws,
                      size_t ws_bytes, cudaStream_t s) {
+  NvtxRange range("leight gridder (cell-binned)");
   MLG_CHECK(in.layout == Layout::kPointSplit && out.layout == Layout::kPointSplit,
             "the cell-binned gridder takes split complex input and output");
   const CornerGrid e = corner_grid(g);

@@ -12,9 +12,22 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/monalisa_gpu.h"
 
 namespace mlg {
+
+// NVTX range over a host scope: profilers (Nsight Systems, ncu --nvtx) show
+// the operator stages and solver phases by name; without a tool attached the
+// calls return at once.
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
+
 
 // ---- status / error plumbing ----------------------------------------------
 void set_error(const char* fmt, ...);
@@ -146,10 +159,21 @@ struct Csr {
   int ord_short = -1;
   // FP16 copy of val for the mixed-precision solver (built on demand)
   __half* val_h = nullptr;
+  // Row records of the first ord_short ordered rows (sign-folded copies
+  // inside plans, csr_build_records): 16 words per row -- cell, entry count,
+  // then up to kRecInline (column, value bits) pairs; a longer row stores
+  // its first entry index in word 2 and keeps its entries in the CSR
+  uint32_t* ord_rec = nullptr;
 };
+constexpr int kRecInline = 7;
 constexpr int kSegLen = 512;
 
 void csr_free(Csr& c);
+// Builds ord_rec from ord_rows / ord_bounds and this matrix's values
+// (idempotent; needs the split non-empty order).
+int csr_build_records(Csr& c, cudaStream_t s);
+// Whether the record kernel serves the short rows (MLG_GUT_REC=0 turns it off).
+bool spmm_records_enabled();
 // Builds the segment tables of the long rows (call once the long-row list is
 // on the device).
 int csr_build_segments(Csr& c, cudaStream_t s);

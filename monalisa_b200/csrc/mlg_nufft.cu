@@ -55,6 +55,7 @@ static int forward_pass(mlg_plan_s* p, int ax, const float2* x, bool x_per_coil,
   pd.ax = ax;
   pd.dir = -1;
   pd.C = C;
+  pd.wait_err = p->wait_err;
   if (ax == 0) {
     pd.dims[1] = n[1];
     pd.dims[2] = n[2];
@@ -141,6 +142,7 @@ static int inverse_pass(mlg_plan_s* p, int ax, const float2* y, const float* HY,
   pd.ax = ax;
   pd.dir = 1;
   pd.C = C;
+  pd.wait_err = p->wait_err;
   const bool gut_in = fused_gut(p) && ax == d - 1;
   if (gut_in) set_gut_input(p, pd, y, HY);
   if (p->adjoint_mode == kAdjMasked && ax == d - 1) {
@@ -257,15 +259,25 @@ int nakatsha_stage(mlg_plan_s* p, int stage, const float2* y, const float* HY, f
 
 int shanna_run(mlg_plan_s* p, const float2* x, bool x_per_coil, float2* y, const float* sqn_w, double* partial,
                int* n_partial, cudaStream_t s) {
-  for (int st = 0; st < kShannaStages; ++st)
+  static const char* kNames[kShannaStages] = {"shanna: x pass (x.*KFC)", "shanna: y pass", "shanna: z pass",
+                                              "shanna: Gu"};
+  NvtxRange r("shanna");
+  for (int st = 0; st < kShannaStages; ++st) {
+    NvtxRange rs(kNames[st]);
     MLG_TRY(shanna_stage(p, st, x, x_per_coil, y, sqn_w, partial, n_partial, s));
+  }
   return MLG_OK;
 }
 
 int nakatsha_run(mlg_plan_s* p, const float2* y, const float* HY, float scale, float2* x, double* partial,
                  int* n_partial, cudaStream_t s) {
-  for (int st = 0; st < kNakatshaStages; ++st)
+  static const char* kNames[kNakatshaStages] = {"nakatsha: Gut", "nakatsha: last-axis pass", "nakatsha: middle pass",
+                                                "nakatsha: x pass (.*KFC_conj, coil sum)"};
+  NvtxRange r("nakatsha");
+  for (int st = 0; st < kNakatshaStages; ++st) {
+    NvtxRange rs(kNames[st]);
     MLG_TRY(nakatsha_stage(p, st, y, HY, scale, x, partial, n_partial, s));
+  }
   return MLG_OK;
 }
 
@@ -490,6 +502,8 @@ static int plan_create_impl(int imDim, const int* N_u, const int* n_u, int nCh, 
     }
   }
   cudaStream_t s = p->stream;
+  p->wait_err = fft_wait_word();
+  if (!p->wait_err) return bail(fail(MLG_ERR_OOM, "plan: the device wait flag could not be allocated"));
   // occupancy tables and the list of Gut's non-empty cells (in blocks of
   // nearby cells) live with the caller's matrix (built once, shared by the
   // sign-folded copy)
@@ -498,6 +512,7 @@ static int plan_create_impl(int imDim, const int* N_u, const int* n_u, int nCh, 
   if (Gut && (nCh % 2) == 0 && (st = csr_build_order(const_cast<Csr&>(*Gut), p->N, true, s)) != MLG_OK)
     return bail(st);
   if (Gut && (st = csr_sign_copy(*Gut, true, imDim, p->N, 1.0f, p->Gut_s, s)) != MLG_OK) return bail(st);
+  if (Gut && (nCh % 2) == 0 && nCh / 2 <= 16 && (st = csr_build_records(p->Gut_s, s)) != MLG_OK) return bail(st);
   if ((st = build_line_mask(p, s)) != MLG_OK) return bail(st);
   p->adjoint_mode = adjoint_mode_valid(p, kAdjMasked) ? kAdjMasked : (imDim >= 2 ? kAdjFused : kAdjFullGrid);
   const size_t kbytes = sizeof(float2) * (size_t)nu * nCh;
@@ -547,7 +562,7 @@ static int plan_create_impl(int imDim, const int* N_u, const int* n_u, int nCh, 
   if (cudaStreamSynchronize(s) != cudaSuccess) return bail(fail(MLG_ERR_CUDA, "plan creation failed"));
   p->bytes = (share ? 0 : 2 * kbytes + gbytes + abytes + bbytes) +
              sizeof(float) * (size_t)((Gu ? Gu->nnz : 0) + (Gut ? Gut->nnz : 0)) + sizeof(double) * (cap + 64) +
-             sizeof(float) * seg_floats;
+             sizeof(float) * seg_floats + (p->Gut_s.ord_rec ? 64 * (size_t)p->Gut_s.ord_short : 0);
   *out = p;
   return MLG_OK;
 }
@@ -602,6 +617,12 @@ int mlg_plan_create_sharing(mlg_plan_t base, mlg_matrix_t Gu, mlg_matrix_t Gut, 
   MLG_CHECK(Gu || Gut, "at least one of Gu / Gut is needed");
   MLG_CUDA(cudaSetDevice(base->device));
   return plan_create_sharing(base, Gu ? &Gu->csr : nullptr, Gut ? &Gut->csr : nullptr, out);
+}
+
+int mlg_plan_status(mlg_plan_t p) {
+  MLG_CHECK(p, "NULL plan");
+  MLG_CUDA(cudaSetDevice(p->device));
+  return fft_wait_status(p->wait_err, p->stream);
 }
 
 int mlg_plan_device_bytes(mlg_plan_t p, long long* bytes) {
@@ -663,6 +684,7 @@ int mlg_shanna(int imDim, const int* N_u, const int* n_u, int nCh, const float* 
     if (cudaStreamSynchronize(s) != cudaSuccess)
       st = fail(MLG_ERR_CUDA, "shanna failed: %s", cudaGetErrorString(cudaGetLastError()));
   }
+  if (st == MLG_OK) st = fft_wait_status(p->wait_err, s);
   dx.reset();
   dy.reset();
   x2.reset();
@@ -707,6 +729,7 @@ int mlg_nakatsha(int imDim, const int* N_u, const int* n_u, int nCh, const float
     if (cudaStreamSynchronize(s) != cudaSuccess)
       st = fail(MLG_ERR_CUDA, "nakatsha failed: %s", cudaGetErrorString(cudaGetLastError()));
   }
+  if (st == MLG_OK) st = fft_wait_status(p->wait_err, s);
   dx.reset();
   dy.reset();
   x2.reset();

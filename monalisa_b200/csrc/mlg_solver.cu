@@ -265,6 +265,7 @@ static int sensa_body(mlg_plan_s* p, const float2* y, const float* ve, float ve_
 
 int sensa_run(mlg_plan_s* p, const float2* y, const float* ve, float ve_max, int nIter, int nCGD, float2* x,
               double* residual, bool use_graph, cudaStream_t s) {
+  NvtxRange range("CG-SENSE (bmSensa)");
   MLG_CHECK(p->Gu && p->Gut, "CG-SENSE needs a plan with both Gu and Gut");
   MLG_CHECK(nIter >= 0 && nCGD >= 0, "nIter / nCGD must be >= 0");
   p->mixed_run = p->precision == MLG_PRECISION_MIXED;

@@ -16,6 +16,8 @@
 // (lanes = consecutive rows of one coil; used when the output is coil-major,
 // e.g. Gut -> grid), so the output side is always coalesced.
 #include <algorithm>
+#include <cstdlib>
+#include <cstring>
 #include <vector>
 
 #include "mlg_internal.cuh"
@@ -469,6 +471,120 @@ static void launch_pair(int ppt, bool out_h, bool contract, const SpmmParams& p,
   launch_pair_ppt<1>(out_h, contract, p, rows, rp, nrows, grid, mid, s);
 }
 
+// Short rows of an ordered non-empty product from their records (CONTRACT,
+// FP32 point layout in and out): a thread per (row, coil pair) reads the
+// row's 64-byte record -- cell, count and up to kRecInline (column, value)
+// pairs -- and issues every gather of the row at once, so a row costs two
+// dependent loads (record -> inputs) instead of three (bounds -> entry ->
+// input).  Rows with more entries loop over their CSR entries.  Per coil the
+// entries are summed in stored order with the same fused multiply-adds as
+// spmm_pair_kernel: the outputs are identical.  The first mid.blocks blocks
+// gather the mid rows a warp each, as there.
+constexpr int kRecMinBlocks = 4;
+
+__global__ void __launch_bounds__(256, kRecMinBlocks) spmm_rec_kernel(SpmmParams p, const uint4* __restrict__ rec,
+                                                                     int n_rows, MidRows mid) {
+  if ((int)blockIdx.x < mid.blocks) {
+    mid_rows_block(p, mid.rows, mid.bounds, mid.n, blockIdx.x, mid.blocks);
+    return;
+  }
+  const int bid = (int)blockIdx.x - mid.blocks;
+  const int P = p.nCh >> 1;
+  const long long i0 = (long long)bid * p.rows_per_block;
+  const int nr = (int)min((long long)p.rows_per_block, (long long)n_rows - i0);
+  const int total = nr * P;
+  const bool scale = p.in_row_scale != nullptr;
+  const float4* in = reinterpret_cast<const float4*>(p.in.a);
+  for (int it = threadIdx.x; it < total; it += blockDim.x) {
+    const int lr = it / P, pi = it - lr * P;
+    const uint4* rp = rec + (i0 + lr) * 4;
+    const uint4 h0 = __ldg(rp), h1 = __ldg(rp + 1), h2 = __ldg(rp + 2), h3 = __ldg(rp + 3);
+    const long long r = (int)h0.x;
+    const uint32_t n = h0.y;
+    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (n <= (uint32_t)kRecInline) {
+      const uint32_t cj[kRecInline] = {h0.z, h1.x, h1.z, h2.x, h2.z, h3.x, h3.z};
+      const uint32_t mv[kRecInline] = {h0.w, h1.y, h1.w, h2.y, h2.w, h3.y, h3.w};
+      float4 v[kRecInline];
+      float hy[kRecInline];
+#pragma unroll
+      for (int k = 0; k < kRecInline; ++k) {
+        if ((uint32_t)k < n) {
+          v[k] = __ldg(in + (long long)cj[k] * P + pi);
+          hy[k] = scale ? __ldg(p.in_row_scale + cj[k]) : 1.f;
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < kRecInline; ++k) {
+        if ((uint32_t)k < n) {
+          float m = __uint_as_float(mv[k]);
+          if (scale) m = __fmul_rn(m, hy[k]);
+          acc.x = __fmaf_rn(m, v[k].x, acc.x);
+          acc.y = __fmaf_rn(m, v[k].y, acc.y);
+          acc.z = __fmaf_rn(m, v[k].z, acc.z);
+          acc.w = __fmaf_rn(m, v[k].w, acc.w);
+        }
+      }
+    } else {
+      const uint32_t b = h0.z;
+#pragma unroll 4
+      for (uint32_t k = b; k < b + n; ++k) {
+        const int j = __ldg(p.col + k);
+        float m = __ldg(p.val + k);
+        const float4 v = __ldg(in + (long long)j * P + pi);
+        if (scale) m = __fmul_rn(m, __ldg(p.in_row_scale + j));
+        acc.x = __fmaf_rn(m, v.x, acc.x);
+        acc.y = __fmaf_rn(m, v.y, acc.y);
+        acc.z = __fmaf_rn(m, v.z, acc.z);
+        acc.w = __fmaf_rn(m, v.w, acc.w);
+      }
+    }
+    if (p.out_scale != 1.0f)
+      acc = make_float4(__fmul_rn(acc.x, p.out_scale), __fmul_rn(acc.y, p.out_scale), __fmul_rn(acc.z, p.out_scale),
+                        __fmul_rn(acc.w, p.out_scale));
+    reinterpret_cast<float4*>(p.out.a)[r * P + pi] = acc;
+  }
+}
+
+__global__ void rec_build_kernel(const int* __restrict__ rows, const uint2* __restrict__ bounds, int n,
+                                 const int* __restrict__ col, const float* __restrict__ val,
+                                 uint32_t* __restrict__ rec) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint2 be = bounds[i];
+    const uint32_t len = be.y - be.x;
+    uint32_t w[16] = {};
+    w[0] = (uint32_t)rows[i];
+    w[1] = len;
+    if (len <= (uint32_t)kRecInline) {
+      for (uint32_t k = 0; k < len; ++k) {
+        w[2 + 2 * k] = (uint32_t)col[be.x + k];
+        w[3 + 2 * k] = __float_as_uint(val[be.x + k]);
+      }
+    } else {
+      w[2] = be.x;
+    }
+    uint4* o = reinterpret_cast<uint4*>(rec) + 4 * (size_t)i;
+    for (int q = 0; q < 4; ++q) o[q] = make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
+  }
+}
+
+bool spmm_records_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("MLG_GUT_REC");
+    return !(e && std::strcmp(e, "0") == 0);
+  }();
+  return on;
+}
+
+int csr_build_records(Csr& c, cudaStream_t s) {
+  if (c.ord_rec || !c.ord_rows || !c.ord_nonempty || c.ord_short <= 0 || !c.val) return MLG_OK;
+  MLG_CUDA(cudaMalloc(&c.ord_rec, 64 * (size_t)c.ord_short));
+  const int g = std::max(1, std::min(148 * 16, (c.ord_short + 255) / 256));
+  rec_build_kernel<<<g, 256, 0, s>>>(c.ord_rows, c.ord_bounds, c.ord_short, c.col, c.val, c.ord_rec);
+  MLG_LAUNCHED();
+  return MLG_OK;
+}
+
 static bool use_pair_kernel(const SpmmArgs& a) {
   return a.in.layout == Layout::kPointC64 &&
          (a.out.layout == Layout::kPointC64 || a.out.layout == Layout::kPointF16) && (a.nCh % 2) == 0 &&
@@ -571,7 +687,11 @@ int spmm(const SpmmArgs& a, cudaStream_t s) {
         mid.blocks = (mid.n + 15) / 16;
       }
       const int grid_pair = split ? (n_pair + p.rows_per_block - 1) / p.rows_per_block : grid_short;
-      if (grid_pair + mid.blocks > 0) {
+      if (split && m.ord_rec && !a.half_values && spmm_records_enabled() && grid_pair + mid.blocks > 0) {
+        spmm_rec_kernel<<<grid_pair + mid.blocks, 256, 0, s>>>(p, reinterpret_cast<const uint4*>(m.ord_rec), n_pair,
+                                                               mid);
+        MLG_LAUNCHED();
+      } else if (grid_pair + mid.blocks > 0) {
         launch_pair(pair_ppt(a), oh, a.contract, p, ordered ? m.ord_rows : nullptr,
                     ordered ? m.ord_bounds : nullptr, n_pair, grid_pair, mid, s);
         MLG_LAUNCHED();
@@ -626,6 +746,7 @@ __global__ void sign_by_row_kernel(const uint32_t* __restrict__ row_ptr, const f
 void csr_free_sign_copy(Csr& c) {
   cudaFree(c.val);
   cudaFree(c.val_h);
+  cudaFree(c.ord_rec);
   c = Csr();
 }
 
@@ -648,6 +769,7 @@ int csr_sign_copy(const Csr& src, bool by_row, int imDim, const int* N, float gl
   dst = src;  // shares row_ptr / col / long_rows with src (not owned)
   dst.val = nullptr;
   dst.val_h = nullptr;
+  dst.ord_rec = nullptr;
   MLG_CUDA(cudaMalloc(&dst.val, sizeof(float) * (size_t)std::max<long long>(1, src.nnz)));
   const int Nx = N[0], Ny = imDim > 1 ? N[1] : 1;
   if (by_row) {

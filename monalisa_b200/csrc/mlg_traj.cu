@@ -521,6 +521,7 @@ static int build_sparsemats(const TrajGeom& g, int nPt, const double* t_host, Cs
 extern "C" int mlg_traj2sparsemat3(int imDim, int nPt, const double* t, const double* ve, const int* N_u,
                                    const double* dK_u, int kernelType, int nWin, const double* kernelParam,
                                    mlg_matrix_t* Gn, mlg_matrix_t* Gu, mlg_matrix_t* Gut) {
+  mlg::NvtxRange range("bmTraj2SparseMat (Gn, Gu, Gut)");
   MLG_CHECK(imDim >= 1 && imDim <= 3 && nPt >= 1 && t && N_u && dK_u && kernelParam, "invalid argument");
   MLG_CHECK(kernelType == MLG_KERNEL_GAUSS || kernelType == MLG_KERNEL_KAISER, "unknown kernel type");
   MLG_CHECK(nWin >= 1, "nWin must be >= 1");
