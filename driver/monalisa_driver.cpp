@@ -494,7 +494,7 @@ int main(int argc, char** argv) {
   std::printf("], \"nPt\": %d, \"nCh\": %d, \"nIter\": %d, \"nCGD\": %d, \"setup_ms\": %.3f, \"recon_ms\": %.3f, "
               "\"residual\": [",
               w.nPt, w.nCh, nIter, nCGD, setup_ms, best_ms);
-  for (int i = 0; i < nIter; ++i) std::printf("%s%.9g", i ? ", " : "", res[i]);
+  for (int i = 0; i < nIter; ++i) std::printf("%s%.17g", i ? ", " : "", res[i]);
   std::printf("]");
   if (err >= 0) std::printf(", \"rel_err_vs_phantom\": %.6f", err);
   std::printf("}\n");

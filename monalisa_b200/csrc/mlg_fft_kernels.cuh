@@ -627,7 +627,9 @@ __device__ __forceinline__ void cp_async_wait() {
 
 // The transform of smem_fft for a compile-time column count COLS and CTA
 // size NT (a multiple of COLS): every shared-memory offset is an immediate.
-template <int N1, int N2, int DIR, int COLS, int NT>
+// SMEM_TW: tw is the twiddle table copied into shared memory (a short
+// shared-memory load instead of a global one per twiddle).
+template <int N1, int N2, int DIR, int COLS, int NT, bool SMEM_TW = false>
 __device__ __forceinline__ void smem_fft_fixed(float2* s, const float2* __restrict__ tw) {
   static_assert(NT % COLS == 0, "CTA size must be a multiple of the columns");
   constexpr int G = NT / COLS;  // row groups
@@ -644,7 +646,16 @@ __device__ __forceinline__ void smem_fft_fixed(float2* s, const float2* __restri
       reg_fft<N1, DIR>(r);
       if (n2) {
 #pragma unroll
-        for (int k1 = 1; k1 < N1; ++k1) r[k1] = cmulf(r[k1], twid<DIR>(tw, n2 * k1));
+        for (int k1 = 1; k1 < N1; ++k1) {
+          float2 w;
+          if constexpr (SMEM_TW) {
+            w = tw[n2 * k1];
+            if (DIR > 0) w.y = -w.y;
+          } else {
+            w = twid<DIR>(tw, n2 * k1);
+          }
+          r[k1] = cmulf(r[k1], w);
+        }
       }
 #pragma unroll
       for (int k1 = 0; k1 < N1; ++k1) p[k1 * N2 * COLS] = r[k1];
@@ -839,9 +850,11 @@ __global__ void __launch_bounds__(cta_threads(COLS), pipe_min_blocks(N1 * N2, CO
   float4* const lb1 = s4all + N * CV;
   float2* const xb0 = reinterpret_cast<float2*>(s4all + 2 * N * CV);
   float2* const xb1 = xb0 + L * in_len;
+  float2* const tws = xb1 + L * in_len;  // twiddle table (N values), copied once
   const int vc = threadIdx.x % CV, r0 = threadIdx.x / CV;
   const int col = vc * 2, l = col / C, c = col - l * C;
   const int gu = (d.dims[1] + L - 1) / L;  // x pass: lines over (y, z)
+  for (int i = threadIdx.x; i < N; i += NT) tws[i] = __ldg(tw + i);  // visible after the loop's first barrier
 
   auto issue = [&](int b, float4* ldst, float2* xdst) {
     pipe_issue_lines<N, N % RSTEP == 0>(d, L, gu, l, c, vc, r0, CV, RSTEP, b, ldst, nullptr, 0);
@@ -884,7 +897,7 @@ __global__ void __launch_bounds__(cta_threads(COLS), pipe_min_blocks(N1 * N2, CO
       }
     }
     __syncthreads();
-    smem_fft_fixed<N1, N2, -1, COLS, NT>(reinterpret_cast<float2*>(cur), tw);  // ends with a barrier
+    smem_fft_fixed<N1, N2, -1, COLS, NT, true>(reinterpret_cast<float2*>(cur), tws);  // ends with a barrier
     if (ui < d.dims[1]) {
       float2* obase = d.out + (long long)ui * d.out_stride[1] + (long long)vi * d.out_stride[2] + c;
       const float4* const scol = cur + vc;
@@ -923,6 +936,8 @@ __global__ void __launch_bounds__(256, 2)
   float4* const lb1 = s4all + N * CV;
   float4* const kb0 = s4all + 2 * N * CV;
   float4* const kb1 = kb0 + out_len * CV;
+  float2* const tws = reinterpret_cast<float2*>(kb1 + out_len * CV);  // twiddle table (N values)
+  for (int i = threadIdx.x; i < N; i += NT) tws[i] = __ldg(tw + i);  // visible after the loop's first barrier
   const int vc = threadIdx.x % CV, r0 = threadIdx.x / CV;
   const int col = vc * 2, l = col / C, c = col - l * C;
   const int gu = (d.dims[1] + L - 1) / L;  // x pass: lines over (y, z)
@@ -953,7 +968,7 @@ __global__ void __launch_bounds__(256, 2)
       cp_async_wait<0>();
     }
     __syncthreads();
-    smem_fft_fixed<N1, N2, 1, COLS, NT>(reinterpret_cast<float2*>(cur), tw);  // ends with a barrier
+    smem_fft_fixed<N1, N2, 1, COLS, NT, true>(reinterpret_cast<float2*>(cur), tws);  // ends with a barrier
     const int u0 = (b % gu) * L, vi = b / gu;
     const int total = L * out_len;
     const int rounds = (total + G - 1) / G;  // uniform: every lane reaches the shuffles
@@ -1069,7 +1084,8 @@ static int launch_pipe(const FftAxisPlan& a, const PassDesc& d, int Lp, int thre
   return MLG_OK;
 }
 
-// TMA pass (fft_pass_tma_kernel) for a plain pass without occupancy masks:
+// TMA pass (fft_pass_tma_kernel) for a plain pass, with occupancy-masked
+// input (the first inverse pass of the masked adjoint) or without:
 // *launched stays false when the shape does not fit the TMA boxes (the
 // caller then takes the cp.async pipelined pass).
 template <int N1, int N2, int DIR, int COLS>
@@ -1079,9 +1095,12 @@ static int launch_tma(const FftAxisPlan& a, const PassDesc& d, int Lp, cudaStrea
   // register budget of step C: shapes beyond it are not instantiated
   if constexpr (tma_step_c_iters<N1, N2, COLS, NT>() * N2 > 32) return MLG_OK;
   else {
-  if (d.in_mask || d.in_lo < 0 || d.in_len < 1 || d.in_lo + d.in_len > N || d.out_lo < 0 || d.out_len < 1 ||
+  if (d.in_lo < 0 || d.in_len < 1 || d.in_lo + d.in_len > N || d.out_lo < 0 || d.out_len < 1 ||
       d.out_lo + d.out_len > N || Lp * d.C != COLS)
     return MLG_OK;
+  // occupancy-masked input: the line masks, the whole line stored
+  const bool masked = d.in_mask != nullptr;
+  if (masked && (DIR < 0 || !d.in_lmask || d.in_lo != 0 || d.in_len != N || d.lmask_words * 32 < N)) return MLG_OK;
   const int u = d.ax == 0 ? 1 : 0, v = d.ax == 2 ? 1 : 2;
   TmaPass t;
   t.L = Lp;
@@ -1095,6 +1114,14 @@ static int launch_tma(const FftAxisPlan& a, const PassDesc& d, int Lp, cudaStrea
   t.in_lo = d.in_lo;
   t.out_lo = d.out_lo;
   t.err = d.wait_err;
+  t.in = d.in;
+  t.st_u = d.in_stride[u];
+  t.st_v = d.in_stride[v];
+  t.st_ax = d.in_stride[d.ax];
+  t.C = d.C;
+  t.dim_u = d.dims[u];
+  t.lmask = d.in_lmask;
+  t.lw = d.lmask_words;
   const long long rowb = (long long)COLS * 8;  // shared-memory box starts on 128-byte boundaries
   if ((t.in_rows * rowb) % 128 || (t.out_lo * rowb) % 128 || (t.out_rows * rowb) % 128) return MLG_OK;
   CUtensorMap tin, tout;
@@ -1103,22 +1130,26 @@ static int launch_tma(const FftAxisPlan& a, const PassDesc& d, int Lp, cudaStrea
       tma_line_map(&tout, d.out, d.C, d.dims[u], d.out_stride[u], d.out_len, d.out_stride[d.ax], d.dims[v],
                    d.out_stride[v], Lp, t.out_rows) != MLG_OK)
     return MLG_OK;
-  const size_t smem = (size_t)NSLOT * N * COLS * 8 + 2 * NSLOT * sizeof(uint64_t) + 128;
-  thread_local int per_sm = 0, sms = 0;
-  thread_local size_t per_sm_smem = 0;
-  if (per_sm == 0 || per_sm_smem != smem) {
-    MLG_CUDA(cudaFuncSetAttribute(fft_pass_tma_kernel<N1, N2, DIR, COLS, NSLOT>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(200 * 1024)));
+  const size_t smem = (size_t)NSLOT * N * COLS * 8 + 2 * NSLOT * sizeof(uint64_t) + (size_t)N * 8 + 128;
+  auto kern = fft_pass_tma_kernel<N1, N2, DIR, COLS, NSLOT, false>;
+  if constexpr (DIR > 0) {
+    if (masked) kern = fft_pass_tma_kernel<N1, N2, DIR, COLS, NSLOT, true>;
+  }
+  // per instantiation, variant and host thread
+  thread_local int per_sm[2] = {0, 0}, sms = 0;
+  thread_local size_t per_sm_smem[2] = {0, 0};
+  const int vi = masked ? 1 : 0;
+  if (per_sm[vi] == 0 || per_sm_smem[vi] != smem) {
     int dev = 0;
     MLG_CUDA(cudaGetDevice(&dev));
     MLG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    MLG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fft_pass_tma_kernel<N1, N2, DIR, COLS, NSLOT>,
-                                                           NT + 32, smem));
-    per_sm = std::max(1, per_sm);
-    per_sm_smem = smem;
+    MLG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(200 * 1024)));
+    MLG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[vi], kern, NT + 32, smem));
+    per_sm[vi] = std::max(1, per_sm[vi]);
+    per_sm_smem[vi] = smem;
   }
-  const int grid = std::max(1, std::min(t.nbundles, per_sm * sms));
-  fft_pass_tma_kernel<N1, N2, DIR, COLS, NSLOT><<<grid, NT + 32, smem, s>>>(tin, tout, t, a.tw);
+  const int grid = std::max(1, std::min(t.nbundles, per_sm[vi] * sms));
+  kern<<<grid, NT + 32, smem, s>>>(tin, tout, t, a.tw);
   MLG_LAUNCHED();
   *launched = true;
   return MLG_OK;
@@ -1136,7 +1167,7 @@ static inline int pipe_lines(const FftAxisPlan& a, int C) {
 template <int N1, int N2, int CP>
 static int launch_nak_pipe(const FftAxisPlan& a, const PassDesc& d, int n_slots, cudaStream_t s) {
   const int Lp = 16 / (2 * CP);
-  const size_t smem = 2 * ((size_t)a.N + d.out_len) * 16 * sizeof(float2);
+  const size_t smem = 2 * ((size_t)a.N + d.out_len) * 16 * sizeof(float2) + (size_t)a.N * sizeof(float2);
   thread_local int per_sm = 0, sms = 0;
   thread_local size_t per_sm_smem = 0;
   if (per_sm == 0 || per_sm_smem != smem) {
@@ -1166,7 +1197,8 @@ static int launch_shanna_pipe(const FftAxisPlan& a, const PassDesc& d, int Lp, c
   k.in_stride[2] = (long long)d.in_len * d.dims[1] * d.C;
   k.in_mask = nullptr;
   k.in_lmask = nullptr;
-  const size_t smem = 2 * (size_t)a.N * COLS * sizeof(float2) + 2 * (size_t)Lp * d.in_len * sizeof(float2);
+  const size_t smem = 2 * (size_t)a.N * COLS * sizeof(float2) + 2 * (size_t)Lp * d.in_len * sizeof(float2) +
+                      (size_t)a.N * sizeof(float2);
   thread_local int per_sm = 0, sms = 0;
   thread_local size_t per_sm_smem = 0;
   if (per_sm == 0 || per_sm_smem != smem) {
@@ -1218,7 +1250,7 @@ static int launch_pass(const FftAxisPlan& a, const PassDesc& d, int L, cudaStrea
     const int Lp = pipe_lines(a, d.C);
     const int cols = Lp * d.C, tp = threads_for(cols);
     if ((d.C & 1) == 0 && tp % cols == 0 && 2 * (size_t)a.N * cols * sizeof(float2) <= kFftSmemCap) {
-      if (!d.in_mask && tma_passes_enabled()) {  // bundles moved by the TMA unit
+      if (tma_passes_enabled()) {  // bundles moved by the TMA unit (and bulk copies of masked rows)
         bool done = false;
         int st = MLG_OK;
         switch (cols) {

@@ -160,19 +160,19 @@ struct Csr {
   // FP16 copy of val for the mixed-precision solver (built on demand)
   __half* val_h = nullptr;
   // Row records of the first ord_short ordered rows (sign-folded copies
-  // inside plans, csr_build_records): 16 words per row -- cell, entry count,
+  // inside plans, csr_build_records): 8 words per row -- cell, entry count,
   // then up to kRecInline (column, value bits) pairs; a longer row stores
   // its first entry index in word 2 and keeps its entries in the CSR
   uint32_t* ord_rec = nullptr;
 };
-constexpr int kRecInline = 7;
+constexpr int kRecInline = 3;
 constexpr int kSegLen = 512;
 
 void csr_free(Csr& c);
 // Builds ord_rec from ord_rows / ord_bounds and this matrix's values
 // (idempotent; needs the split non-empty order).
 int csr_build_records(Csr& c, cudaStream_t s);
-// Whether the record kernel serves the short rows (MLG_GUT_REC=0 turns it off).
+// Whether the record kernel serves the short rows (MLG_GUT_REC=1 turns it on).
 bool spmm_records_enabled();
 // Builds the segment tables of the long rows (call once the long-row list is
 // on the device).

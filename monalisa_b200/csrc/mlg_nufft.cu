@@ -562,7 +562,7 @@ static int plan_create_impl(int imDim, const int* N_u, const int* n_u, int nCh, 
   if (cudaStreamSynchronize(s) != cudaSuccess) return bail(fail(MLG_ERR_CUDA, "plan creation failed"));
   p->bytes = (share ? 0 : 2 * kbytes + gbytes + abytes + bbytes) +
              sizeof(float) * (size_t)((Gu ? Gu->nnz : 0) + (Gut ? Gut->nnz : 0)) + sizeof(double) * (cap + 64) +
-             sizeof(float) * seg_floats + (p->Gut_s.ord_rec ? 64 * (size_t)p->Gut_s.ord_short : 0);
+             sizeof(float) * seg_floats + (p->Gut_s.ord_rec ? 32 * (size_t)p->Gut_s.ord_short : 0);
   *out = p;
   return MLG_OK;
 }

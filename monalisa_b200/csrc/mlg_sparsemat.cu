@@ -473,17 +473,17 @@ static void launch_pair(int ppt, bool out_h, bool contract, const SpmmParams& p,
 
 // Short rows of an ordered non-empty product from their records (CONTRACT,
 // FP32 point layout in and out): a thread per (row, coil pair) reads the
-// row's 64-byte record -- cell, count and up to kRecInline (column, value)
-// pairs -- and issues every gather of the row at once, so a row costs two
-// dependent loads (record -> inputs) instead of three (bounds -> entry ->
-// input).  Rows with more entries loop over their CSR entries.  Per coil the
-// entries are summed in stored order with the same fused multiply-adds as
-// spmm_pair_kernel: the outputs are identical.  The first mid.blocks blocks
-// gather the mid rows a warp each, as there.
-constexpr int kRecMinBlocks = 4;
-
-__global__ void __launch_bounds__(256, kRecMinBlocks) spmm_rec_kernel(SpmmParams p, const uint4* __restrict__ rec,
-                                                                     int n_rows, MidRows mid) {
+// row's 32-byte record -- cell, count and up to kRecInline (column, value)
+// pairs -- and issues every gather of the row at once, so such a row costs
+// two dependent loads (record -> inputs) instead of three (bounds -> entry ->
+// input), and the record stream is smaller than the bounds and entries it
+// replaces.  Rows with more entries loop over their CSR entries.  Per coil
+// the entries are summed in stored order with the same fused multiply-adds
+// as spmm_pair_kernel: the outputs are identical.  The first mid.blocks
+// blocks gather the mid rows a warp each, as there.  Eight blocks per SM, as
+// the pair kernel.
+__global__ void __launch_bounds__(256, 8) spmm_rec_kernel(SpmmParams p, const uint4* __restrict__ rec, int n_rows,
+                                                          MidRows mid) {
   if ((int)blockIdx.x < mid.blocks) {
     mid_rows_block(p, mid.rows, mid.bounds, mid.n, blockIdx.x, mid.blocks);
     return;
@@ -497,34 +497,32 @@ __global__ void __launch_bounds__(256, kRecMinBlocks) spmm_rec_kernel(SpmmParams
   const float4* in = reinterpret_cast<const float4*>(p.in.a);
   for (int it = threadIdx.x; it < total; it += blockDim.x) {
     const int lr = it / P, pi = it - lr * P;
-    const uint4* rp = rec + (i0 + lr) * 4;
-    const uint4 h0 = __ldg(rp), h1 = __ldg(rp + 1), h2 = __ldg(rp + 2), h3 = __ldg(rp + 3);
+    const uint4* rp = rec + (i0 + lr) * 2;
+    const uint4 h0 = __ldg(rp), h1 = __ldg(rp + 1);
     const long long r = (int)h0.x;
     const uint32_t n = h0.y;
     float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+    auto fma4 = [&](float m, float4 v) {
+      acc.x = __fmaf_rn(m, v.x, acc.x);
+      acc.y = __fmaf_rn(m, v.y, acc.y);
+      acc.z = __fmaf_rn(m, v.z, acc.z);
+      acc.w = __fmaf_rn(m, v.w, acc.w);
+    };
     if (n <= (uint32_t)kRecInline) {
-      const uint32_t cj[kRecInline] = {h0.z, h1.x, h1.z, h2.x, h2.z, h3.x, h3.z};
-      const uint32_t mv[kRecInline] = {h0.w, h1.y, h1.w, h2.y, h2.w, h3.y, h3.w};
-      float4 v[kRecInline];
-      float hy[kRecInline];
-#pragma unroll
-      for (int k = 0; k < kRecInline; ++k) {
-        if ((uint32_t)k < n) {
-          v[k] = __ldg(in + (long long)cj[k] * P + pi);
-          hy[k] = scale ? __ldg(p.in_row_scale + cj[k]) : 1.f;
-        }
+      const uint32_t c0 = h0.z, c1 = h1.x, c2 = h1.z;
+      float4 v0 = make_float4(0.f, 0.f, 0.f, 0.f), v1 = v0, v2 = v0;
+      float m0 = __uint_as_float(h0.w), m1 = __uint_as_float(h1.y), m2 = __uint_as_float(h1.w);
+      if (n > 0) v0 = __ldg(in + (long long)c0 * P + pi);
+      if (n > 1) v1 = __ldg(in + (long long)c1 * P + pi);
+      if (n > 2) v2 = __ldg(in + (long long)c2 * P + pi);
+      if (scale) {
+        if (n > 0) m0 = __fmul_rn(m0, __ldg(p.in_row_scale + c0));
+        if (n > 1) m1 = __fmul_rn(m1, __ldg(p.in_row_scale + c1));
+        if (n > 2) m2 = __fmul_rn(m2, __ldg(p.in_row_scale + c2));
       }
-#pragma unroll
-      for (int k = 0; k < kRecInline; ++k) {
-        if ((uint32_t)k < n) {
-          float m = __uint_as_float(mv[k]);
-          if (scale) m = __fmul_rn(m, hy[k]);
-          acc.x = __fmaf_rn(m, v[k].x, acc.x);
-          acc.y = __fmaf_rn(m, v[k].y, acc.y);
-          acc.z = __fmaf_rn(m, v[k].z, acc.z);
-          acc.w = __fmaf_rn(m, v[k].w, acc.w);
-        }
-      }
+      if (n > 0) fma4(m0, v0);
+      if (n > 1) fma4(m1, v1);
+      if (n > 2) fma4(m2, v2);
     } else {
       const uint32_t b = h0.z;
 #pragma unroll 4
@@ -533,10 +531,7 @@ __global__ void __launch_bounds__(256, kRecMinBlocks) spmm_rec_kernel(SpmmParams
         float m = __ldg(p.val + k);
         const float4 v = __ldg(in + (long long)j * P + pi);
         if (scale) m = __fmul_rn(m, __ldg(p.in_row_scale + j));
-        acc.x = __fmaf_rn(m, v.x, acc.x);
-        acc.y = __fmaf_rn(m, v.y, acc.y);
-        acc.z = __fmaf_rn(m, v.z, acc.z);
-        acc.w = __fmaf_rn(m, v.w, acc.w);
+        fma4(m, v);
       }
     }
     if (p.out_scale != 1.0f)
@@ -552,7 +547,7 @@ __global__ void rec_build_kernel(const int* __restrict__ rows, const uint2* __re
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const uint2 be = bounds[i];
     const uint32_t len = be.y - be.x;
-    uint32_t w[16] = {};
+    uint32_t w[8] = {};
     w[0] = (uint32_t)rows[i];
     w[1] = len;
     if (len <= (uint32_t)kRecInline) {
@@ -563,22 +558,23 @@ __global__ void rec_build_kernel(const int* __restrict__ rows, const uint2* __re
     } else {
       w[2] = be.x;
     }
-    uint4* o = reinterpret_cast<uint4*>(rec) + 4 * (size_t)i;
-    for (int q = 0; q < 4; ++q) o[q] = make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
+    uint4* o = reinterpret_cast<uint4*>(rec) + 2 * (size_t)i;
+    o[0] = make_uint4(w[0], w[1], w[2], w[3]);
+    o[1] = make_uint4(w[4], w[5], w[6], w[7]);
   }
 }
 
 bool spmm_records_enabled() {
   static const bool on = [] {
     const char* e = std::getenv("MLG_GUT_REC");
-    return !(e && std::strcmp(e, "0") == 0);
+    return e && std::strcmp(e, "1") == 0;
   }();
   return on;
 }
 
 int csr_build_records(Csr& c, cudaStream_t s) {
   if (c.ord_rec || !c.ord_rows || !c.ord_nonempty || c.ord_short <= 0 || !c.val) return MLG_OK;
-  MLG_CUDA(cudaMalloc(&c.ord_rec, 64 * (size_t)c.ord_short));
+  MLG_CUDA(cudaMalloc(&c.ord_rec, 32 * (size_t)c.ord_short));
   const int g = std::max(1, std::min(148 * 16, (c.ord_short + 255) / 256));
   rec_build_kernel<<<g, 256, 0, s>>>(c.ord_rows, c.ord_bounds, c.ord_short, c.col, c.val, c.ord_rec);
   MLG_LAUNCHED();

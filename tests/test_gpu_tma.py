@@ -7,7 +7,7 @@ a child process (the switches are read once per process):
   operators must agree bit for bit;
 * the Gut product over row records (cell, count and inline entries: two
   dependent loads per row) against the coil-pair kernel over the CSR
-  (MLG_GUT_REC=0), in the masked adjoint: bit for bit.  Shapes: 256-point lines x 16 coils
+  (MLG_GUT_REC=1 selects the records), in the masked adjoint: bit for bit.  Shapes: 256-point lines x 16 coils
 (16-column bundles), 192-point radix-3 lines x 12 coils (24 columns: two
 lines per bundle), 2-D 512-point lines (two load boxes of 256 rows), 8 coils
 (two lines per bundle), and a bundle count that leaves the last CTAs with
