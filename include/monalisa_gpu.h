@@ -364,6 +364,19 @@ int mlg_plan_get_adjoint(mlg_plan_t p, int* mode);
  * keeps the fastest.  ms (may be NULL) receives 3 times in milliseconds,
  * negative for strategies the plan cannot run. */
 int mlg_plan_autotune(mlg_plan_t p, int reps, double* ms);
+/* Kernel variants of a plan, with different launch shapes, that compute the
+ * same values bit for bit: pass_tma = 1 moves the line-FFT bundles with the
+ * TMA unit (a producer warp, tensor-map boxes, 2 bundles in flight per CTA),
+ * 0 with per-thread cp.async copies; gut_records = 1 reads Gut's short rows
+ * from 32-byte row records (masked adjoint, FP32, even coil count), 0 from
+ * the CSR.  Set them before a chain is created over the plan.
+ * mlg_plan_autotune_variants times both for the plan's adjoint strategy and
+ * keeps the fastest: ms[4] (may be NULL) = forward + adjoint with TMA /
+ * cp.async passes, adjoint with CSR / record Gut rows (-1: not timed).  No
+ * counterpart in the reference (its kernels are CPU code). */
+int mlg_plan_set_variant(mlg_plan_t p, int pass_tma, int gut_records);
+int mlg_plan_get_variant(mlg_plan_t p, int* pass_tma, int* gut_records);
+int mlg_plan_autotune_variants(mlg_plan_t p, int reps, double* ms);
 
 /* Precision of the plan's CG-SENSE solver (mlg_sensa_dev / mlg_sensa).
  * MLG_PRECISION_FP32: FP32 data and matrix values, FP64 scalars (the

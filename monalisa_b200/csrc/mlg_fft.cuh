@@ -66,6 +66,8 @@ struct PassDesc {
   // device word set to 1 when a bounded wait inside a pass runs out (passes
   // with such waits: the TMA passes), or NULL
   int* wait_err = nullptr;
+  // 1: take the cp.async passes even where a TMA pass exists (plan variant)
+  int no_tma = 0;
 };
 
 // The current device's wait flag (set by a pass whose bounded wait ran out),
@@ -74,6 +76,10 @@ int* fft_wait_word();
 // Synchronises s, then reads and clears *word: MLG_OK, or MLG_ERR_TIMEOUT
 // when a pass's wait ran out since the last check.
 int fft_wait_status(int* word, cudaStream_t s);
+
+// Whether the TMA passes may run at all (MLG_FFT_TMA=0 turns them off for
+// every plan; otherwise PassDesc::no_tma decides per pass).
+bool tma_passes_enabled();
 
 int fft_axis_init(int N, FftAxisPlan& a);
 void fft_axis_free(FftAxisPlan& a);

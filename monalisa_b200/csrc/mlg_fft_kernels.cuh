@@ -1250,7 +1250,7 @@ static int launch_pass(const FftAxisPlan& a, const PassDesc& d, int L, cudaStrea
     const int Lp = pipe_lines(a, d.C);
     const int cols = Lp * d.C, tp = threads_for(cols);
     if ((d.C & 1) == 0 && tp % cols == 0 && 2 * (size_t)a.N * cols * sizeof(float2) <= kFftSmemCap) {
-      if (tma_passes_enabled()) {  // bundles moved by the TMA unit (and bulk copies of masked rows)
+      if (tma_passes_enabled() && !d.no_tma) {  // bundles moved by the TMA unit (and bulk copies of masked rows)
         bool done = false;
         int st = MLG_OK;
         switch (cols) {

@@ -172,7 +172,8 @@ void csr_free(Csr& c);
 // Builds ord_rec from ord_rows / ord_bounds and this matrix's values
 // (idempotent; needs the split non-empty order).
 int csr_build_records(Csr& c, cudaStream_t s);
-// Whether the record kernel serves the short rows (MLG_GUT_REC=1 turns it on).
+// Whether the record kernel serves the short rows of every product that has
+// records (MLG_GUT_REC=1 forces it; otherwise SpmmArgs::records decides).
 bool spmm_records_enabled();
 // Builds the segment tables of the long rows (call once the long-row list is
 // on the device).
@@ -264,6 +265,9 @@ struct SpmmArgs {
   // Read the matrix values from m->val_h (FP16) instead of m->val; the sums
   // stay FP32.
   bool half_values = false;
+  // Short rows of an ordered non-empty product from the matrix's row
+  // records (ord_rec), when built; FP32 values only
+  bool records = false;
   // Optional: raised (atomicMax on the bits) to the largest |re| or |im| of
   // the values written, before any FP16 rounding (device, non-negative float)
   unsigned* absmax = nullptr;

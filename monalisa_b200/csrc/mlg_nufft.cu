@@ -56,6 +56,7 @@ static int forward_pass(mlg_plan_s* p, int ax, const float2* x, bool x_per_coil,
   pd.dir = -1;
   pd.C = C;
   pd.wait_err = p->wait_err;
+  pd.no_tma = p->pass_tma ? 0 : 1;
   if (ax == 0) {
     pd.dims[1] = n[1];
     pd.dims[2] = n[2];
@@ -143,6 +144,7 @@ static int inverse_pass(mlg_plan_s* p, int ax, const float2* y, const float* HY,
   pd.dir = 1;
   pd.C = C;
   pd.wait_err = p->wait_err;
+  pd.no_tma = p->pass_tma ? 0 : 1;
   const bool gut_in = fused_gut(p) && ax == d - 1;
   if (gut_in) set_gut_input(p, pd, y, HY);
   if (p->adjoint_mode == kAdjMasked && ax == d - 1) {
@@ -249,6 +251,7 @@ int nakatsha_stage(mlg_plan_s* p, int stage, const float2* y, const float* HY, f
     a.out.rows = p->Nu_tot;
     a.long_only = fused_gut(p);
     a.nonempty_only = p->adjoint_mode == kAdjMasked;
+    a.records = p->gut_records != 0;
     a.seg_scratch = p->seg_scratch;
     return spmm(a, s);
   }

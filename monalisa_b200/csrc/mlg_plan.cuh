@@ -43,6 +43,11 @@ struct mlg_plan_s {
   int line_mask_words = 0;
   double* scalars = nullptr;      // solver scalars (device)
   int* wait_err = nullptr;        // the device's pass wait flag (fft_wait_word, not owned)
+  // kernel variants chosen per plan (mlg_plan_autotune_variants): line-FFT
+  // bundles moved by the TMA unit (1) or by per-thread cp.async copies (0);
+  // Gut's short rows from row records (1) or from the CSR (0)
+  int pass_tma = 1;
+  int gut_records = 0;
   cudaStream_t stream = nullptr;  // internal non-blocking stream
   cudaEvent_t ev_in = nullptr, ev_out = nullptr;
   size_t bytes = 0;

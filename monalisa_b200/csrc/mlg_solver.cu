@@ -536,6 +536,87 @@ extern "C" int mlg_plan_autotune(mlg_plan_t p, int reps, double* ms) {
   return mlg_plan_set_adjoint(p, best);
 }
 
+extern "C" int mlg_plan_set_variant(mlg_plan_t p, int pass_tma, int gut_records) {
+  using namespace mlg;
+  MLG_CHECK(p, "NULL plan");
+  MLG_CHECK((pass_tma == 0 || pass_tma == 1) && (gut_records == 0 || gut_records == 1), "variants are 0 or 1");
+  MLG_CHECK(!gut_records || p->Gut_s.ord_rec, "this plan has no Gut row records (masked adjoint, even coil count)");
+  if (p->pass_tma != pass_tma || p->gut_records != gut_records) {
+    p->pass_tma = pass_tma;
+    p->gut_records = gut_records;
+    if (p->cg_graph) cudaGraphExecDestroy(p->cg_graph);  // captured with the old kernels
+    p->cg_graph = nullptr;
+    p->cg_graph_x = nullptr;
+  }
+  return MLG_OK;
+}
+
+extern "C" int mlg_plan_get_variant(mlg_plan_t p, int* pass_tma, int* gut_records) {
+  MLG_CHECK(p && pass_tma && gut_records, "NULL argument");
+  *pass_tma = p->pass_tma;
+  *gut_records = p->gut_records;
+  return MLG_OK;
+}
+
+// Times the kernel variants of the plan's current adjoint strategy and keeps
+// the fastest: ms[0..1] = forward + adjoint with TMA / cp.async passes,
+// ms[2..3] = adjoint with Gut from the CSR / from row records (-1: not
+// available).
+extern "C" int mlg_plan_autotune_variants(mlg_plan_t p, int reps, double* ms) {
+  using namespace mlg;
+  MLG_CHECK(p && reps >= 1, "invalid argument");
+  MLG_CHECK(p->Gu && p->Gut, "variant tuning needs a plan with Gu and Gut");
+  MLG_CUDA(cudaSetDevice(p->device));
+  MLG_TRY(ensure_solver_buffers(p));
+  cudaStream_t s = p->stream;
+  MLG_CUDA(cudaMemsetAsync(p->k_res, 0, sizeof(float2) * (size_t)p->nPt * p->nCh, s));
+  MLG_CUDA(cudaMemsetAsync(p->x_p, 0, sizeof(float2) * (size_t)p->nu_tot, s));
+  cudaEvent_t a, b;
+  MLG_CUDA(cudaEventCreate(&a));
+  MLG_CUDA(cudaEventCreate(&b));
+  int st = MLG_OK;
+  auto time_it = [&](bool fwd) {
+    auto once = [&] {
+      if (fwd && st == MLG_OK) st = shanna_run(p, p->x_p, false, p->k_Mp, nullptr, nullptr, nullptr, s);
+      if (st == MLG_OK) st = nakatsha_run(p, p->k_res, nullptr, 1.0f, p->x_dagM, nullptr, nullptr, s);
+    };
+    once();  // warm-up
+    cudaEventRecord(a, s);
+    for (int r = 0; r < reps && st == MLG_OK; ++r) once();
+    cudaEventRecord(b, s);
+    if (cudaEventSynchronize(b) != cudaSuccess) st = fail(MLG_ERR_CUDA, "variant tuning run failed");
+    float v = 0.f;
+    cudaEventElapsedTime(&v, a, b);
+    return (double)v / reps;
+  };
+  const int tma0 = p->pass_tma, rec0 = p->gut_records;
+  double t[4] = {-1.0, -1.0, -1.0, -1.0};
+  int best_tma = tma0, best_rec = rec0;
+  if (tma_passes_enabled()) {
+    for (int v = 1; v >= 0 && st == MLG_OK; --v) {
+      p->pass_tma = v;
+      t[1 - v] = time_it(true);
+    }
+    best_tma = t[0] <= t[1] ? 1 : 0;
+  }
+  p->pass_tma = best_tma;
+  if (st == MLG_OK && p->Gut_s.ord_rec && p->adjoint_mode == 2 && p->precision == MLG_PRECISION_FP32) {
+    for (int v = 0; v <= 1 && st == MLG_OK; ++v) {
+      p->gut_records = v;
+      t[2 + v] = time_it(false);
+    }
+    best_rec = t[3] < t[2] ? 1 : 0;
+  }
+  p->pass_tma = tma0;
+  p->gut_records = rec0;
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  if (ms)
+    for (int i = 0; i < 4; ++i) ms[i] = t[i];
+  if (st != MLG_OK) return st;
+  return mlg_plan_set_variant(p, best_tma, best_rec);
+}
+
 extern "C" int mlg_plan_set_precision(mlg_plan_t p, int precision) {
   using namespace mlg;
   MLG_CHECK(p, "NULL plan");

@@ -683,7 +683,7 @@ int spmm(const SpmmArgs& a, cudaStream_t s) {
         mid.blocks = (mid.n + 15) / 16;
       }
       const int grid_pair = split ? (n_pair + p.rows_per_block - 1) / p.rows_per_block : grid_short;
-      if (split && m.ord_rec && !a.half_values && spmm_records_enabled() && grid_pair + mid.blocks > 0) {
+      if (split && m.ord_rec && !a.half_values && (a.records || spmm_records_enabled()) && grid_pair + mid.blocks > 0) {
         spmm_rec_kernel<<<grid_pair + mid.blocks, 256, 0, s>>>(p, reinterpret_cast<const uint4*>(m.ord_rec), n_pair,
                                                                mid);
         MLG_LAUNCHED();

@@ -208,12 +208,33 @@ class NufftPlan:
         'fp16_values' (FP16 matrix values only)."""
         N.call("mlg_plan_set_precision", self._h, self.PRECISIONS.index(name))
 
-    def autotune(self, reps: int = 3) -> dict:
-        """Times the valid adjoint strategies and keeps the fastest; returns
-        {strategy: ms} (strategies the plan cannot run are omitted)."""
+    def autotune(self, reps: int = 3, variants: bool = True) -> dict:
+        """Times the valid adjoint strategies and keeps the fastest, then (with
+        `variants`) the kernel variants of that strategy (TMA or cp.async
+        line-FFT passes, Gut rows from the CSR or from row records); returns
+        {name: ms} (what the plan cannot run is omitted)."""
         ms = np.zeros(3)
         N.call("mlg_plan_autotune", self._h, int(reps), N.dptr(ms))
-        return {n: float(t) for n, t in zip(self.ADJOINT_MODES, ms) if t >= 0}
+        out = {n: float(t) for n, t in zip(self.ADJOINT_MODES, ms) if t >= 0}
+        if variants and self.nPt > 0:
+            mv = np.zeros(4)
+            N.call("mlg_plan_autotune_variants", self._h, int(reps), N.dptr(mv))
+            names = ("passes_tma", "passes_cp_async", "gut_csr", "gut_records")
+            out.update({n: float(t) for n, t in zip(names, mv) if t >= 0})
+        return out
+
+    @property
+    def variant(self) -> dict:
+        """The plan's kernel variants: {'pass_tma': 0/1, 'gut_records': 0/1}."""
+        a, b = ctypes.c_int(), ctypes.c_int()
+        N.call("mlg_plan_get_variant", self._h, ctypes.byref(a), ctypes.byref(b))
+        return {"pass_tma": a.value, "gut_records": b.value}
+
+    @variant.setter
+    def variant(self, v: dict):
+        cur = self.variant
+        cur.update(v)
+        N.call("mlg_plan_set_variant", self._h, int(cur["pass_tma"]), int(cur["gut_records"]))
 
     def status(self) -> None:
         """Synchronises the plan's stream; raises MonalisaError (timeout) when

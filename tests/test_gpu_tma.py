@@ -74,3 +74,37 @@ def test_gut_records_bit_identical_to_pair_kernel(tmp_path):
     a, b = _run(tmp_path, 1, 1), _run(tmp_path, 1, 0)
     for k in a.files:
         assert np.array_equal(a[k], b[k]), k
+
+
+def test_plan_variants_agree_and_the_tuner_picks_one():
+    """The per-plan kernel variants (TMA / cp.async passes, CSR / record Gut
+    rows) in one process: the same outputs bit for bit in every
+    combination; the variant tuner times them and keeps a valid one."""
+    import torch
+
+    import monalisa_b200 as mb
+    from monalisa_b200 import traj
+
+    n, N, nCh = 48, 96, 12
+    t = traj.bmTraj_fullRadial3_phyllotaxis_lineAssym2(96, 500, 1, 1.0)
+    Gu, Gut = mb.bmTraj2SparseMat(t, traj.bmVolumeElement_full_radial3(t), [N] * 3, [1, 1, 1])
+    rec = mb.SensaRecon(Gu, Gut, traj.coil_maps([n] * 3, nCh, 4), [n] * 3)
+    plan = rec.plan
+    plan.adjoint_mode = "masked"
+    rng = np.random.default_rng(2)
+    x = torch.from_numpy((rng.standard_normal(n ** 3) + 1j * rng.standard_normal(n ** 3)).astype(np.complex64)).cuda()
+    outs = []
+    for tma in (1, 0):
+        for recs in (0, 1):
+            plan.variant = {"pass_tma": tma, "gut_records": recs}
+            y = plan.shanna(x)
+            outs.append((y.cpu().numpy(), plan.nakatsha(y).cpu().numpy()))
+    for o in outs[1:]:
+        assert np.array_equal(o[0], outs[0][0]) and np.array_equal(o[1], outs[0][1])
+    times = plan.autotune(2)
+    assert {"passes_tma", "passes_cp_async"} <= set(times)
+    if plan.adjoint_mode == "masked":
+        assert {"gut_csr", "gut_records"} <= set(times)
+    assert plan.variant["pass_tma"] in (0, 1) and plan.variant["gut_records"] in (0, 1)
+    plan.status()
+    plan.close()
