@@ -365,17 +365,19 @@ int mlg_plan_get_adjoint(mlg_plan_t p, int* mode);
  * negative for strategies the plan cannot run. */
 int mlg_plan_autotune(mlg_plan_t p, int reps, double* ms);
 /* Kernel variants of a plan, with different launch shapes, that compute the
- * same values bit for bit: pass_tma = 1 moves the line-FFT bundles with the
- * TMA unit (a producer warp, tensor-map boxes, 2 bundles in flight per CTA),
+ * same values bit for bit: pass_buffers = 2 or 3 moves the line-FFT bundles
+ * with the TMA unit (a producer warp and that many bundle buffers per CTA:
+ * 3 CTAs per SM with 2 buffers, 2 with 3, at 256-point lines of 16 coils),
  * 0 with per-thread cp.async copies; gut_records = 1 reads Gut's short rows
  * from 32-byte row records (masked adjoint, FP32, even coil count), 0 from
- * the CSR.  Set them before a chain is created over the plan.
- * mlg_plan_autotune_variants times both for the plan's adjoint strategy and
- * keeps the fastest: ms[4] (may be NULL) = forward + adjoint with TMA /
- * cp.async passes, adjoint with CSR / record Gut rows (-1: not timed).  No
- * counterpart in the reference (its kernels are CPU code). */
-int mlg_plan_set_variant(mlg_plan_t p, int pass_tma, int gut_records);
-int mlg_plan_get_variant(mlg_plan_t p, int* pass_tma, int* gut_records);
+ * the CSR.  Defaults: 2 buffers, records where built.  Set them before a
+ * chain is created over the plan.  mlg_plan_autotune_variants times them for
+ * the plan's adjoint strategy and keeps the fastest: ms[5] (may be NULL) =
+ * forward + adjoint with 2 / 3 buffers and with cp.async passes, adjoint
+ * with CSR / record Gut rows (-1: not timed).  No counterpart in the
+ * reference (its kernels are CPU code). */
+int mlg_plan_set_variant(mlg_plan_t p, int pass_buffers, int gut_records);
+int mlg_plan_get_variant(mlg_plan_t p, int* pass_buffers, int* gut_records);
 int mlg_plan_autotune_variants(mlg_plan_t p, int reps, double* ms);
 
 /* Precision of the plan's CG-SENSE solver (mlg_sensa_dev / mlg_sensa).

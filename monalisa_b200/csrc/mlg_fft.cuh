@@ -66,8 +66,9 @@ struct PassDesc {
   // device word set to 1 when a bounded wait inside a pass runs out (passes
   // with such waits: the TMA passes), or NULL
   int* wait_err = nullptr;
-  // 1: take the cp.async passes even where a TMA pass exists (plan variant)
-  int no_tma = 0;
+  // bundle buffers of the TMA passes (2 or 3; the plan's variant), or 0:
+  // the cp.async passes even where a TMA pass exists
+  int tma_slots = 2;
 };
 
 // The current device's wait flag (set by a pass whose bounded wait ran out),
@@ -78,7 +79,7 @@ int* fft_wait_word();
 int fft_wait_status(int* word, cudaStream_t s);
 
 // Whether the TMA passes may run at all (MLG_FFT_TMA=0 turns them off for
-// every plan; otherwise PassDesc::no_tma decides per pass).
+// every plan; otherwise PassDesc::tma_slots decides per pass).
 bool tma_passes_enabled();
 
 int fft_axis_init(int N, FftAxisPlan& a);

@@ -1084,23 +1084,22 @@ static int launch_pipe(const FftAxisPlan& a, const PassDesc& d, int Lp, int thre
   return MLG_OK;
 }
 
-// TMA pass (fft_pass_tma_kernel) for a plain pass, with occupancy-masked
-// input (the first inverse pass of the masked adjoint) or without:
-// *launched stays false when the shape does not fit the TMA boxes (the
-// caller then takes the cp.async pipelined pass).
-template <int N1, int N2, int DIR, int COLS>
+// TMA pass (fft_pass_tma_kernel, NSLOT bundle buffers) for a plain pass
+// without occupancy masks: *launched stays false when the shape does not fit
+// the TMA boxes (the caller then takes the cp.async pipelined pass).  The
+// masked first inverse pass stays on cp.async: copying only its set rows
+// takes one small bulk copy per row, which measured slower (c2: 1.19 ms
+// against 0.69 ms) than per-thread copies.
+template <int N1, int N2, int DIR, int COLS, int NSLOT>
 static int launch_tma(const FftAxisPlan& a, const PassDesc& d, int Lp, cudaStream_t s, bool* launched) {
-  constexpr int N = N1 * N2, NT = cta_threads(COLS), NSLOT = 2;
+  constexpr int N = N1 * N2, NT = cta_threads(COLS);
   *launched = false;
   // register budget of step C: shapes beyond it are not instantiated
   if constexpr (tma_step_c_iters<N1, N2, COLS, NT>() * N2 > 32) return MLG_OK;
   else {
-  if (d.in_lo < 0 || d.in_len < 1 || d.in_lo + d.in_len > N || d.out_lo < 0 || d.out_len < 1 ||
+  if (d.in_mask || d.in_lo < 0 || d.in_len < 1 || d.in_lo + d.in_len > N || d.out_lo < 0 || d.out_len < 1 ||
       d.out_lo + d.out_len > N || Lp * d.C != COLS)
     return MLG_OK;
-  // occupancy-masked input: the line masks, the whole line stored
-  const bool masked = d.in_mask != nullptr;
-  if (masked && (DIR < 0 || !d.in_lmask || d.in_lo != 0 || d.in_len != N || d.lmask_words * 32 < N)) return MLG_OK;
   const int u = d.ax == 0 ? 1 : 0, v = d.ax == 2 ? 1 : 2;
   TmaPass t;
   t.L = Lp;
@@ -1114,14 +1113,6 @@ static int launch_tma(const FftAxisPlan& a, const PassDesc& d, int Lp, cudaStrea
   t.in_lo = d.in_lo;
   t.out_lo = d.out_lo;
   t.err = d.wait_err;
-  t.in = d.in;
-  t.st_u = d.in_stride[u];
-  t.st_v = d.in_stride[v];
-  t.st_ax = d.in_stride[d.ax];
-  t.C = d.C;
-  t.dim_u = d.dims[u];
-  t.lmask = d.in_lmask;
-  t.lw = d.lmask_words;
   const long long rowb = (long long)COLS * 8;  // shared-memory box starts on 128-byte boundaries
   if ((t.in_rows * rowb) % 128 || (t.out_lo * rowb) % 128 || (t.out_rows * rowb) % 128) return MLG_OK;
   CUtensorMap tin, tout;
@@ -1131,25 +1122,22 @@ static int launch_tma(const FftAxisPlan& a, const PassDesc& d, int Lp, cudaStrea
                    d.out_stride[v], Lp, t.out_rows) != MLG_OK)
     return MLG_OK;
   const size_t smem = (size_t)NSLOT * N * COLS * 8 + 2 * NSLOT * sizeof(uint64_t) + (size_t)N * 8 + 128;
-  auto kern = fft_pass_tma_kernel<N1, N2, DIR, COLS, NSLOT, false>;
-  if constexpr (DIR > 0) {
-    if (masked) kern = fft_pass_tma_kernel<N1, N2, DIR, COLS, NSLOT, true>;
-  }
-  // per instantiation, variant and host thread
-  thread_local int per_sm[2] = {0, 0}, sms = 0;
-  thread_local size_t per_sm_smem[2] = {0, 0};
-  const int vi = masked ? 1 : 0;
-  if (per_sm[vi] == 0 || per_sm_smem[vi] != smem) {
+  if (smem > 200 * 1024) return MLG_OK;
+  thread_local int per_sm = 0, sms = 0;
+  thread_local size_t per_sm_smem = 0;
+  if (per_sm == 0 || per_sm_smem != smem) {
+    MLG_CUDA(cudaFuncSetAttribute(fft_pass_tma_kernel<N1, N2, DIR, COLS, NSLOT>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(200 * 1024)));
     int dev = 0;
     MLG_CUDA(cudaGetDevice(&dev));
     MLG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    MLG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(200 * 1024)));
-    MLG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[vi], kern, NT + 32, smem));
-    per_sm[vi] = std::max(1, per_sm[vi]);
-    per_sm_smem[vi] = smem;
+    MLG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fft_pass_tma_kernel<N1, N2, DIR, COLS, NSLOT>,
+                                                           NT + 32, smem));
+    per_sm = std::max(1, per_sm);
+    per_sm_smem = smem;
   }
-  const int grid = std::max(1, std::min(t.nbundles, per_sm[vi] * sms));
-  kern<<<grid, NT + 32, smem, s>>>(tin, tout, t, a.tw);
+  const int grid = std::max(1, std::min(t.nbundles, per_sm * sms));
+  fft_pass_tma_kernel<N1, N2, DIR, COLS, NSLOT><<<grid, NT + 32, smem, s>>>(tin, tout, t, a.tw);
   MLG_LAUNCHED();
   *launched = true;
   return MLG_OK;
@@ -1250,13 +1238,20 @@ static int launch_pass(const FftAxisPlan& a, const PassDesc& d, int L, cudaStrea
     const int Lp = pipe_lines(a, d.C);
     const int cols = Lp * d.C, tp = threads_for(cols);
     if ((d.C & 1) == 0 && tp % cols == 0 && 2 * (size_t)a.N * cols * sizeof(float2) <= kFftSmemCap) {
-      if (tma_passes_enabled() && !d.no_tma) {  // bundles moved by the TMA unit (and bulk copies of masked rows)
+      if (tma_passes_enabled() && d.tma_slots >= 2) {  // bundles moved by the TMA unit
         bool done = false;
         int st = MLG_OK;
+        const bool three = d.tma_slots >= 3;
         switch (cols) {
-          case 16: st = launch_tma<N1, N2, DIR, 16>(a, d, Lp, s, &done); break;
-          case 24: st = launch_tma<N1, N2, DIR, 24>(a, d, Lp, s, &done); break;
-          case 32: st = launch_tma<N1, N2, DIR, 32>(a, d, Lp, s, &done); break;
+          case 16:
+            st = three ? launch_tma<N1, N2, DIR, 16, 3>(a, d, Lp, s, &done) : launch_tma<N1, N2, DIR, 16, 2>(a, d, Lp, s, &done);
+            break;
+          case 24:
+            st = three ? launch_tma<N1, N2, DIR, 24, 3>(a, d, Lp, s, &done) : launch_tma<N1, N2, DIR, 24, 2>(a, d, Lp, s, &done);
+            break;
+          case 32:
+            st = three ? launch_tma<N1, N2, DIR, 32, 3>(a, d, Lp, s, &done) : launch_tma<N1, N2, DIR, 32, 2>(a, d, Lp, s, &done);
+            break;
           default: break;
         }
         if (st != MLG_OK || done) return st;

@@ -44,15 +44,6 @@ struct TmaPass {
   int out_chunks = 1;
   int out_rows = 0;   // rows per store box (out_chunks * out_rows = out_len)
   int* err = nullptr; // set to 1 when a wait runs out (device word), or NULL
-  // occupancy-masked input (the first inverse pass after Gut wrote only its
-  // non-empty rows): row n of line (u, v) is copied only when bit n of the
-  // line's mask is set, otherwise written as zeros
-  const float2* in = nullptr;
-  long long st_u = 0, st_v = 0, st_ax = 0;  // float2 strides of the input
-  int C = 1;                                // coils per line
-  int dim_u = 1;                            // lines along u
-  const uint32_t* lmask = nullptr;          // lw words per line, line u + dim_u * v
-  int lw = 0;
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -127,22 +118,6 @@ __device__ __forceinline__ void tma_store_4d(const CUtensorMap* map, int c0, int
   asm volatile("cp.async.bulk.tensor.4d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3, %4}], [%5];" ::"l"(
                    reinterpret_cast<uint64_t>(map)),
                "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(src))
-               : "memory");
-}
-
-// Adds `bytes` to the transaction count of the barrier's current phase
-// (without an arrival).
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
-  asm volatile("mbarrier.expect_tx.relaxed.cta.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-               : "memory");
-}
-
-// Untiled bulk copy global -> shared completing on a barrier (16-byte
-// aligned addresses, size a multiple of 16).
-__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                   smem_u32(dst)),
-               "l"(src), "r"(bytes), "r"(smem_u32(bar))
                : "memory");
 }
 
@@ -239,11 +214,7 @@ constexpr int tma_min_blocks() {
   return by_smem < 1 ? 1 : (by_smem > 3 ? 3 : by_smem);
 }
 
-// MASKED: the load side reads only the rows set in the line masks -- the 32
-// lanes of the producer warp issue one untiled bulk copy per (row, line) on
-// the slot's barrier (expected bytes = the set rows) and write the unset rows
-// as zeros, then all arrive; the store side is the tensor-map box as above.
-template <int N1, int N2, int DIR, int COLS, int NSLOT, bool MASKED>
+template <int N1, int N2, int DIR, int COLS, int NSLOT>
 __global__ void __launch_bounds__(cta_threads(COLS) + 32, (tma_min_blocks<N1 * N2, COLS, NSLOT>()))
     fft_pass_tma_kernel(const __grid_constant__ CUtensorMap tin, const __grid_constant__ CUtensorMap tout, TmaPass a,
                         const float2* __restrict__ tw) {
@@ -263,7 +234,7 @@ __global__ void __launch_bounds__(cta_threads(COLS) + 32, (tma_min_blocks<N1 * N
     abort_flag = 0;
 #pragma unroll
     for (int i = 0; i < NSLOT; ++i) {
-      mbar_init(full + i, MASKED ? 32 : 1);
+      mbar_init(full + i, 1);
       mbar_init(done + i, NT);
     }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -272,51 +243,14 @@ __global__ void __launch_bounds__(cta_threads(COLS) + 32, (tma_min_blocks<N1 * N
   volatile int* abort = &abort_flag;
   const int G = gridDim.x;
   if (tid >= NT) {
-    const int lane = tid - NT;
-    if (!MASKED && lane != 0) return;
-    // producer: one thread (lane 0), or the whole warp for masked loads
+    if (tid != NT) return;
+    // producer: one thread
     auto load = [&](int slot, int b) {
       unsigned char* dst = base + slot * kBuf;
-      if constexpr (!MASKED) {
-        mbar_arrive_expect_tx(full + slot, kBuf);
-        const int c1 = (b % a.gu) * a.L, c3 = b / a.gu;
-        for (int k = 0; k < a.in_chunks; ++k)
-          tma_load_4d(dst + (size_t)k * a.in_rows * COLS * 8, &tin, 0, c1, k * a.in_rows - a.in_lo, c3, full + slot);
-      } else {
-        const int ui0 = (b % a.gu) * a.L, vi = b / a.gu;
-        constexpr int NW = (N + 31) / 32;
-        const unsigned row_bytes = (unsigned)a.C * 8;
-        unsigned cnt = 0;
-        for (int q = lane; q < a.L * NW; q += 32) {
-          const int l = q / NW, w = q - l * NW;
-          if (ui0 + l < a.dim_u) {
-            uint32_t m = __ldg(a.lmask + ((long long)(ui0 + l) + (long long)a.dim_u * vi) * a.lw + w);
-            if ((N & 31) && w == NW - 1) m &= (1u << (N & 31)) - 1u;
-            cnt += __popc(m);
-          }
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
-        if (lane == 0) mbar_expect_tx(full + slot, cnt * row_bytes);
-        __syncwarp();
-        for (int n = lane; n < N; n += 32) {
-          for (int l = 0; l < a.L; ++l) {
-            const int ui = ui0 + l;
-            float2* d = reinterpret_cast<float2*>(dst) + (size_t)n * COLS + l * a.C;
-            const bool set = ui < a.dim_u &&
-                             ((__ldg(a.lmask + ((long long)ui + (long long)a.dim_u * vi) * a.lw + (n >> 5)) >>
-                               (n & 31)) & 1u);
-            if (set) {
-              bulk_load(d, a.in + (long long)ui * a.st_u + (long long)vi * a.st_v + (long long)n * a.st_ax, row_bytes,
-                        full + slot);
-            } else {
-              for (int k = 0; k < a.C / 2; ++k) reinterpret_cast<float4*>(d)[k] = make_float4(0.f, 0.f, 0.f, 0.f);
-            }
-          }
-        }
-        __syncwarp();
-        mbar_arrive(full + slot);  // one arrival per lane
-      }
+      mbar_arrive_expect_tx(full + slot, kBuf);
+      const int c1 = (b % a.gu) * a.L, c3 = b / a.gu;
+      for (int k = 0; k < a.in_chunks; ++k)
+        tma_load_4d(dst + (size_t)k * a.in_rows * COLS * 8, &tin, 0, c1, k * a.in_rows - a.in_lo, c3, full + slot);
     };
     auto store = [&](int slot, int b) {
       const unsigned char* src = base + slot * kBuf + (size_t)a.out_lo * COLS * 8;
@@ -330,23 +264,15 @@ __global__ void __launch_bounds__(cta_threads(COLS) + 32, (tma_min_blocks<N1 * N
     for (int b = blockIdx.x; b < a.nbundles; b += G, ++it) {
       const int slot = it % NSLOT;
       if (it >= NSLOT) {  // the slot held bundle it - NSLOT: store it first
-        int okw = 1;
-        if (lane == 0) {
-          okw = mbar_wait(done + slot, (unsigned)((it / NSLOT) - 1) & 1u, abort, a.err) ? 1 : 0;
-          if (okw) {
-            store(slot, b - NSLOT * G);
-            bulk_wait_read_all();  // the store has read the buffer
-          }
-        }
-        if constexpr (MASKED) okw = __shfl_sync(0xffffffffu, okw, 0);
-        if (!okw) {
+        if (!mbar_wait(done + slot, (unsigned)((it / NSLOT) - 1) & 1u, abort, a.err)) {
           ok = false;
           break;
         }
+        store(slot, b - NSLOT * G);
+        bulk_wait_read_all();  // the store has read the buffer
       }
       load(slot, b);
     }
-    if (MASKED && lane != 0) return;  // lane 0 stores the last bundles and drains
     const int issued = it;
     if (ok) {  // the last NSLOT bundles
       for (int k = issued > NSLOT ? issued - NSLOT : 0; k < issued; ++k) {

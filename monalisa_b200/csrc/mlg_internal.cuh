@@ -172,9 +172,7 @@ void csr_free(Csr& c);
 // Builds ord_rec from ord_rows / ord_bounds and this matrix's values
 // (idempotent; needs the split non-empty order).
 int csr_build_records(Csr& c, cudaStream_t s);
-// Whether the record kernel serves the short rows of every product that has
-// records (MLG_GUT_REC=1 forces it; otherwise SpmmArgs::records decides).
-bool spmm_records_enabled();
+
 // Builds the segment tables of the long rows (call once the long-row list is
 // on the device).
 int csr_build_segments(Csr& c, cudaStream_t s);

@@ -44,9 +44,10 @@ struct mlg_plan_s {
   double* scalars = nullptr;      // solver scalars (device)
   int* wait_err = nullptr;        // the device's pass wait flag (fft_wait_word, not owned)
   // kernel variants chosen per plan (mlg_plan_autotune_variants): line-FFT
-  // bundles moved by the TMA unit (1) or by per-thread cp.async copies (0);
-  // Gut's short rows from row records (1) or from the CSR (0)
-  int pass_tma = 1;
+  // bundles moved by the TMA unit through 2 or 3 shared buffers per CTA
+  // (pass_buffers = 2, 3) or by per-thread cp.async copies (0); Gut's short
+  // rows from row records (1, when built) or from the CSR (0)
+  int pass_buffers = 2;
   int gut_records = 0;
   cudaStream_t stream = nullptr;  // internal non-blocking stream
   cudaEvent_t ev_in = nullptr, ev_out = nullptr;

@@ -536,13 +536,14 @@ extern "C" int mlg_plan_autotune(mlg_plan_t p, int reps, double* ms) {
   return mlg_plan_set_adjoint(p, best);
 }
 
-extern "C" int mlg_plan_set_variant(mlg_plan_t p, int pass_tma, int gut_records) {
+extern "C" int mlg_plan_set_variant(mlg_plan_t p, int pass_buffers, int gut_records) {
   using namespace mlg;
   MLG_CHECK(p, "NULL plan");
-  MLG_CHECK((pass_tma == 0 || pass_tma == 1) && (gut_records == 0 || gut_records == 1), "variants are 0 or 1");
+  MLG_CHECK((pass_buffers == 0 || pass_buffers == 2 || pass_buffers == 3) && (gut_records == 0 || gut_records == 1),
+            "variants: pass_buffers 0, 2 or 3; gut_records 0 or 1");
   MLG_CHECK(!gut_records || p->Gut_s.ord_rec, "this plan has no Gut row records (masked adjoint, even coil count)");
-  if (p->pass_tma != pass_tma || p->gut_records != gut_records) {
-    p->pass_tma = pass_tma;
+  if (p->pass_buffers != pass_buffers || p->gut_records != gut_records) {
+    p->pass_buffers = pass_buffers;
     p->gut_records = gut_records;
     if (p->cg_graph) cudaGraphExecDestroy(p->cg_graph);  // captured with the old kernels
     p->cg_graph = nullptr;
@@ -551,17 +552,17 @@ extern "C" int mlg_plan_set_variant(mlg_plan_t p, int pass_tma, int gut_records)
   return MLG_OK;
 }
 
-extern "C" int mlg_plan_get_variant(mlg_plan_t p, int* pass_tma, int* gut_records) {
-  MLG_CHECK(p && pass_tma && gut_records, "NULL argument");
-  *pass_tma = p->pass_tma;
+extern "C" int mlg_plan_get_variant(mlg_plan_t p, int* pass_buffers, int* gut_records) {
+  MLG_CHECK(p && pass_buffers && gut_records, "NULL argument");
+  *pass_buffers = p->pass_buffers;
   *gut_records = p->gut_records;
   return MLG_OK;
 }
 
 // Times the kernel variants of the plan's current adjoint strategy and keeps
-// the fastest: ms[0..1] = forward + adjoint with TMA / cp.async passes,
-// ms[2..3] = adjoint with Gut from the CSR / from row records (-1: not
-// available).
+// the fastest: ms[0..2] = forward + adjoint with TMA passes over 2 / 3
+// buffers and with cp.async passes, ms[3..4] = adjoint with Gut from the
+// CSR / from row records (-1: not available).
 extern "C" int mlg_plan_autotune_variants(mlg_plan_t p, int reps, double* ms) {
   using namespace mlg;
   MLG_CHECK(p && reps >= 1, "invalid argument");
@@ -589,32 +590,37 @@ extern "C" int mlg_plan_autotune_variants(mlg_plan_t p, int reps, double* ms) {
     cudaEventElapsedTime(&v, a, b);
     return (double)v / reps;
   };
-  const int tma0 = p->pass_tma, rec0 = p->gut_records;
-  double t[4] = {-1.0, -1.0, -1.0, -1.0};
-  int best_tma = tma0, best_rec = rec0;
+  const int buf0 = p->pass_buffers, rec0 = p->gut_records;
+  double t[5] = {-1.0, -1.0, -1.0, -1.0, -1.0};
+  int best_buf = buf0, best_rec = rec0;
   if (tma_passes_enabled()) {
-    for (int v = 1; v >= 0 && st == MLG_OK; --v) {
-      p->pass_tma = v;
-      t[1 - v] = time_it(true);
+    const int opts[3] = {2, 3, 0};
+    double best = 1e30;
+    for (int i = 0; i < 3 && st == MLG_OK; ++i) {
+      p->pass_buffers = opts[i];
+      t[i] = time_it(true);
+      if (t[i] < best) {
+        best = t[i];
+        best_buf = opts[i];
+      }
     }
-    best_tma = t[0] <= t[1] ? 1 : 0;
   }
-  p->pass_tma = best_tma;
+  p->pass_buffers = best_buf;
   if (st == MLG_OK && p->Gut_s.ord_rec && p->adjoint_mode == 2 && p->precision == MLG_PRECISION_FP32) {
     for (int v = 0; v <= 1 && st == MLG_OK; ++v) {
       p->gut_records = v;
-      t[2 + v] = time_it(false);
+      t[3 + v] = time_it(false);
     }
-    best_rec = t[3] < t[2] ? 1 : 0;
+    best_rec = t[4] < t[3] ? 1 : 0;
   }
-  p->pass_tma = tma0;
+  p->pass_buffers = buf0;
   p->gut_records = rec0;
   cudaEventDestroy(a);
   cudaEventDestroy(b);
   if (ms)
-    for (int i = 0; i < 4; ++i) ms[i] = t[i];
+    for (int i = 0; i < 5; ++i) ms[i] = t[i];
   if (st != MLG_OK) return st;
-  return mlg_plan_set_variant(p, best_tma, best_rec);
+  return mlg_plan_set_variant(p, best_buf, best_rec);
 }
 
 extern "C" int mlg_plan_set_precision(mlg_plan_t p, int precision) {

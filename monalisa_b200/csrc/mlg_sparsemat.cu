@@ -564,12 +564,14 @@ __global__ void rec_build_kernel(const int* __restrict__ rows, const uint2* __re
   }
 }
 
-bool spmm_records_enabled() {
-  static const bool on = [] {
+// MLG_GUT_REC=0 / 1 forces the CSR rows / the records in every product;
+// unset: SpmmArgs::records (the plan's variant) decides.
+static int records_forced() {
+  static const int v = [] {
     const char* e = std::getenv("MLG_GUT_REC");
-    return e && std::strcmp(e, "1") == 0;
+    return e ? (std::strcmp(e, "0") == 0 ? 0 : (std::strcmp(e, "1") == 0 ? 1 : -1)) : -1;
   }();
-  return on;
+  return v;
 }
 
 int csr_build_records(Csr& c, cudaStream_t s) {
@@ -683,7 +685,7 @@ int spmm(const SpmmArgs& a, cudaStream_t s) {
         mid.blocks = (mid.n + 15) / 16;
       }
       const int grid_pair = split ? (n_pair + p.rows_per_block - 1) / p.rows_per_block : grid_short;
-      if (split && m.ord_rec && !a.half_values && (a.records || spmm_records_enabled()) && grid_pair + mid.blocks > 0) {
+      if (split && m.ord_rec && !a.half_values && (records_forced() >= 0 ? records_forced() == 1 : a.records) && grid_pair + mid.blocks > 0) {
         spmm_rec_kernel<<<grid_pair + mid.blocks, 256, 0, s>>>(p, reinterpret_cast<const uint4*>(m.ord_rec), n_pair,
                                                                mid);
         MLG_LAUNCHED();

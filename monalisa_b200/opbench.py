@@ -26,6 +26,10 @@ def main(argv=None):
     ap.add_argument("--reps", type=int, default=3, help="forward + adjoint applications")
     ap.add_argument("--adjoint", default="masked", choices=["masked", "fused", "full_grid"])
     ap.add_argument("--precision", default="fp32", choices=["fp32", "mixed", "fp16_values"])
+    ap.add_argument("--buffers", type=int, default=None, choices=[0, 2, 3],
+                    help="line-FFT passes: TMA with 2 or 3 bundle buffers, or 0 (cp.async); default: the plan's")
+    ap.add_argument("--records", type=int, default=None, choices=[0, 1],
+                    help="Gut rows from row records (1) or the CSR (0); default: the plan's")
     ap.add_argument("--op", default="nufft", choices=["nufft", "gridder"],
                     help="nufft: operator stages; gridder: the leight adjoint gridder on the samples")
     args = ap.parse_args(argv)
@@ -57,6 +61,10 @@ def main(argv=None):
     Gu, Gut = mb.bmTraj2SparseMat(t, ve, [Ng] * 3, [1, 1, 1])
     rec = mb.SensaRecon(Gu, Gut, traj.coil_maps([n] * 3, args.coils, 1), [n] * 3, precision=args.precision)
     rec.plan.adjoint_mode = args.adjoint
+    if args.buffers is not None:
+        rec.plan.variant = {"pass_buffers": args.buffers}
+    if args.records is not None:
+        rec.plan.variant = {"gut_records": args.records}
     x = torch.from_numpy(traj.ellipsoid_phantom([n] * 3, 5, 2)).cuda()
     for _ in range(args.reps):
         y = rec.plan.shanna(x)
@@ -65,7 +73,7 @@ def main(argv=None):
     ms = np.zeros(len(STAGES))
     N.call("mlg_plan_profile", rec.plan.handle, max(1, args.reps), N.dptr(ms))
     print(f"{n}^3 image, {Ng}^3 grid, {args.spokes}x{args.samples} samples, {args.coils} coils, "
-          f"adjoint {rec.plan.adjoint_mode}, precision {args.precision}, Gu nnz {Gu.nnz}")
+          f"adjoint {rec.plan.adjoint_mode}, precision {args.precision}, variant {rec.plan.variant}, Gu nnz {Gu.nnz}")
     for name, v in zip(STAGES, ms):
         print(f"  {name:6s} {v:8.4f} ms")
     rec.plan.close()

@@ -7,7 +7,7 @@ a child process (the switches are read once per process):
   operators must agree bit for bit;
 * the Gut product over row records (cell, count and inline entries: two
   dependent loads per row) against the coil-pair kernel over the CSR
-  (MLG_GUT_REC=1 selects the records), in the masked adjoint: bit for bit.  Shapes: 256-point lines x 16 coils
+  (MLG_GUT_REC=0 / 1 forces either), in the masked adjoint: bit for bit.  Shapes: 256-point lines x 16 coils
 (16-column bundles), 192-point radix-3 lines x 12 coils (24 columns: two
 lines per bundle), 2-D 512-point lines (two load boxes of 256 rows), 8 coils
 (two lines per bundle), and a bundle count that leaves the last CTAs with
@@ -94,17 +94,17 @@ def test_plan_variants_agree_and_the_tuner_picks_one():
     rng = np.random.default_rng(2)
     x = torch.from_numpy((rng.standard_normal(n ** 3) + 1j * rng.standard_normal(n ** 3)).astype(np.complex64)).cuda()
     outs = []
-    for tma in (1, 0):
+    for bufs in (2, 3, 0):
         for recs in (0, 1):
-            plan.variant = {"pass_tma": tma, "gut_records": recs}
+            plan.variant = {"pass_buffers": bufs, "gut_records": recs}
             y = plan.shanna(x)
             outs.append((y.cpu().numpy(), plan.nakatsha(y).cpu().numpy()))
     for o in outs[1:]:
         assert np.array_equal(o[0], outs[0][0]) and np.array_equal(o[1], outs[0][1])
     times = plan.autotune(2)
-    assert {"passes_tma", "passes_cp_async"} <= set(times)
+    assert {"passes_tma_2buf", "passes_tma_3buf", "passes_cp_async"} <= set(times)
     if plan.adjoint_mode == "masked":
         assert {"gut_csr", "gut_records"} <= set(times)
-    assert plan.variant["pass_tma"] in (0, 1) and plan.variant["gut_records"] in (0, 1)
+    assert plan.variant["pass_buffers"] in (0, 2, 3) and plan.variant["gut_records"] in (0, 1)
     plan.status()
     plan.close()
