@@ -21,6 +21,14 @@ bool tma_passes_enabled() {
   return on;
 }
 
+bool tma_test_stall() {
+  static const bool on = [] {
+    const char* e = std::getenv("MLG_TEST_WAIT_TIMEOUT");
+    return e && std::strcmp(e, "1") == 0;
+  }();
+  return on;
+}
+
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no link
 // against the driver library)
 static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {

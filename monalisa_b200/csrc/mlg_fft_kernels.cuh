@@ -1113,6 +1113,7 @@ static int launch_tma(const FftAxisPlan& a, const PassDesc& d, int Lp, cudaStrea
   t.in_lo = d.in_lo;
   t.out_lo = d.out_lo;
   t.err = d.wait_err;
+  t.test_stall = tma_test_stall() ? 1 : 0;
   const long long rowb = (long long)COLS * 8;  // shared-memory box starts on 128-byte boundaries
   if ((t.in_rows * rowb) % 128 || (t.out_lo * rowb) % 128 || (t.out_rows * rowb) % 128) return MLG_OK;
   CUtensorMap tin, tout;

@@ -44,6 +44,9 @@ struct TmaPass {
   int out_chunks = 1;
   int out_rows = 0;   // rows per store box (out_chunks * out_rows = out_len)
   int* err = nullptr; // set to 1 when a wait runs out (device word), or NULL
+  // test hook (MLG_TEST_WAIT_TIMEOUT=1): CTA 0 never loads its first bundle,
+  // so its transform threads' bounded wait runs out and the timeout path runs
+  int test_stall = 0;
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -271,7 +274,7 @@ __global__ void __launch_bounds__(cta_threads(COLS) + 32, (tma_min_blocks<N1 * N
         store(slot, b - NSLOT * G);
         bulk_wait_read_all();  // the store has read the buffer
       }
-      load(slot, b);
+      if (!(a.test_stall && blockIdx.x == 0 && it == 0)) load(slot, b);
     }
     const int issued = it;
     if (ok) {  // the last NSLOT bundles
@@ -310,5 +313,7 @@ int tma_line_map(CUtensorMap* map, const void* base, int C, int dim_u, long long
                  int dim_v, long long st_v, int box_L, int box_rows);
 // Whether the TMA passes are enabled (MLG_FFT_TMA=0 turns them off).
 bool tma_passes_enabled();
+// The timeout test hook (MLG_TEST_WAIT_TIMEOUT=1), read once per process.
+bool tma_test_stall();
 
 }  // namespace mlg
