@@ -420,7 +420,8 @@ def run_gpu(args):
         "config": _config(w, ws),
         "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
         "recon_rel_err_vs_phantom": round(err, 5), "setup_s": round(setup_s, 2),
-        "autotune": {"adjoint": adjoint_c2, "ms": {k: round(v, 4) for k, v in (rec.tuning or {}).items()}},
+        "autotune": {"adjoint": adjoint_c2, "variant": rec.plan.variant,
+                     "ms": {k: round(v, 4) for k, v in (rec.tuning or {}).items()}},
         "vs_plain_gpu": plain,
         **extra,
     }
