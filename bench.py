@@ -498,7 +498,8 @@ def _c4_references(w, Gu, Gut, rec, y, ve, x_fp32, dev):
 
 def _mixed(w, Gu, Gut, y, ve, x_fp32, ms_fp32, plain, stream, ref64, precision="mixed"):
     """c4: the c2 reconstruction in reduced precision: 'mixed' (FP16 matrix
-    values, M p stored in scaled FP16, FP32 residual and sums, FP64 scalars) or
+    values, M p and the 3-D transforms' intermediate stored in scaled FP16
+    inside the CG steps, FP32 residual and sums, FP64 scalars) or
     'fp16_values' (FP16 matrix values only).  Errors: against the FP64
     restatement (gate 1e-3), the FP32 reconstruction, and the change of the
     forward model's error against the FP64 NUDFT (at most 1e-3)."""
@@ -523,9 +524,11 @@ def _mixed(w, Gu, Gut, y, ve, x_fp32, ms_fp32, plain, stream, ref64, precision="
            "rel_diff_vs_fp32_recon": float((x - x_fp32).norm() / x_fp32.norm()),
            "rel_err_vs_fp64": ref64["rel64"](x),
            "nudft_rel_err": ref64["nudft_err"](rec.plan, precision == "mixed"),
-           "adjoint": rec.plan.adjoint_mode,
-           "precision": {"mixed": "fp16 matrix values, M p in fp16 x 2^k per CG step, fp32 residual/sums/FFT, "
-                                  "fp64 CG scalars",
+           "adjoint": rec.plan.adjoint_mode, "variant": rec.plan.variant,
+           "half_intermediate": rec.plan.half_intermediate,
+           "precision": {"mixed": "fp16 matrix values, M p in fp16 x 2^k per CG step, 3-D transform intermediate "
+                                  "(after forward y / adjoint z pass) in fp16 x 2^k inside the CG steps where "
+                                  "half_intermediate, fp32 residual/sums/FFT arithmetic, fp64 CG scalars",
                          "fp16_values": "fp16 matrix values, fp32 k-space/sums/FFT, fp64 CG scalars"}[precision]}
     out["nudft_err_delta"] = out["nudft_rel_err"] - ref64["nudft_fp32"]
     out["gates"] = {"rel_err_vs_fp64 <= 1e-3": out["rel_err_vs_fp64"] <= 1e-3,

@@ -385,8 +385,11 @@ int mlg_plan_autotune_variants(mlg_plan_t p, int reps, double* ms);
  * reference's single-precision arithmetic).  MLG_PRECISION_MIXED: FP16 matrix
  * values (copies of Gu/Gut made once), 16-bit storage of the forward product
  * M p inside the CG steps (FP16 times a power of two chosen per step from the
- * previous step's largest value; the first step keeps FP32), an FP32
- * residual, FP32 sums and FFTs, FP64 scalars; the caller's y and x stay
+ * previous step's largest value; the first step keeps FP32), and, where the
+ * plan's passes support it (mlg_plan_get_half_intermediate), 16-bit storage
+ * of the 3-D transforms' intermediate inside the CG steps (FP16 times a power
+ * of two bounding it from its input's largest value); an FP32 residual, FP32
+ * sums and FFT arithmetic, FP64 scalars; the caller's y and x stay
  * complex64.  Mixed precision turns the fused-gather adjoint
  * strategy off (it reads FP32 k-space).  The operator entry points
  * (mlg_shanna_dev, mlg_nakatsha_dev) of a mixed plan read the FP16 values
@@ -397,13 +400,22 @@ int mlg_plan_autotune_variants(mlg_plan_t p, int reps, double* ms);
 #define MLG_PRECISION_FP16_VALUES 2
 int mlg_plan_set_precision(mlg_plan_t p, int precision);
 int mlg_plan_get_precision(mlg_plan_t p, int* precision);
+/* *on = 1 when a mixed solve of this plan keeps the intermediate of its 3-D
+ * transforms (after the forward y pass, after the adjoint z pass) in scaled
+ * FP16 inside the CG steps: MLG_PRECISION_MIXED, 3-D, a multiple of 4 coils,
+ * no fused adjoint gather, and TMA line passes for those shapes; 0
+ * otherwise.  No reference counterpart. */
+int mlg_plan_get_half_intermediate(mlg_plan_t p, int* on);
 
 /* Times the stages of one Shanna and one Nakatsha on the plan's stream with
  * CUDA events, averaged over `iters` repetitions after one warm-up:
  * ms[0..2] forward x, y, z FFT passes (x pass fused with x .* KFC),
  * ms[3] Gu product, ms[4] Gut product, ms[5..7] inverse z, y, x FFT passes
  * (x pass fused with .* KFC_conj and the coil sum).  Passes a 2-D / 1-D
- * plan does not run read 0.  Measurement helper; no reference counterpart. */
+ * plan does not run read 0.  A mixed-precision plan's stages run as inside
+ * its CG steps (FP16 M p, FP16 transform intermediate where
+ * mlg_plan_get_half_intermediate says so).  Inputs are zeros.  Measurement
+ * helper; no reference counterpart. */
 int mlg_plan_profile(mlg_plan_t p, int iters, double* ms);
 
 /* ---- reconstructions ---------------------------------------------------- */

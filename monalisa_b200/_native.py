@@ -57,6 +57,7 @@ SIGNATURES = {
     "mlg_plan_autotune_variants": [c_vp, c_int, P_d],
     "mlg_plan_set_precision": [c_vp, c_int],
     "mlg_plan_get_precision": [c_vp, P_i],
+    "mlg_plan_get_half_intermediate": [c_vp, P_i],
     "mlg_matrix_download": [c_vp, P_i, P_i, P_f, P_i, P_i],
     "mlg_matrix_spmm_dev": [c_vp, c_vp, c_int, c_vp, c_vp],
     "mlg_traj2sparsemat": [c_int, c_int, P_d, P_d, P_i, P_d, c_int, c_int, P_d, ctypes.POINTER(c_vp),

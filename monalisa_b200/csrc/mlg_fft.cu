@@ -74,20 +74,23 @@ int fft_wait_status(int* word, cudaStream_t s) {
 }
 
 int tma_line_map(CUtensorMap* map, const void* base, int C, int dim_u, long long st_u, int len, long long st_ax,
-                 int dim_v, long long st_v, int box_L, int box_rows) {
+                 int dim_v, long long st_v, int box_L, int box_rows, bool half) {
   auto enc = tensor_map_encoder();
   MLG_CHECK(enc != nullptr, "cuTensorMapEncodeTiled is not available");
   MLG_CHECK(((uintptr_t)base & 15) == 0, "TMA volume base not 16-byte aligned");
   MLG_CHECK(C >= 1 && 2 * C <= 256 && box_L >= 1 && box_L <= 256 && box_rows >= 1 && box_rows <= 256,
             "TMA box out of range");
   const cuuint64_t dims[4] = {(cuuint64_t)2 * C, (cuuint64_t)dim_u, (cuuint64_t)len, (cuuint64_t)dim_v};
-  const cuuint64_t strides[3] = {(cuuint64_t)st_u * 8, (cuuint64_t)st_ax * 8, (cuuint64_t)st_v * 8};
+  const cuuint64_t es = half ? 4 : 8;  // bytes per complex value
+  const cuuint64_t strides[3] = {(cuuint64_t)st_u * es, (cuuint64_t)st_ax * es, (cuuint64_t)st_v * es};
   for (int i = 0; i < 3; ++i)
     MLG_CHECK(strides[i] % 16 == 0 && strides[i] < (1ull << 40), "TMA stride %llu not a multiple of 16 bytes",
               (unsigned long long)strides[i]);
   const cuuint32_t box[4] = {(cuuint32_t)(2 * C), (cuuint32_t)box_L, (cuuint32_t)box_rows, 1};
   const cuuint32_t estr[4] = {1, 1, 1, 1};
-  const CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<void*>(base), dims, strides, box, estr,
+  MLG_CHECK(!half || (4 * C) % 16 == 0, "FP16 boxes need a multiple of 4 coils");
+  const CUresult r = enc(map, half ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4,
+                         const_cast<void*>(base), dims, strides, box, estr,
                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   MLG_CHECK(r == CUDA_SUCCESS, "cuTensorMapEncodeTiled failed (%d)", (int)r);

@@ -69,6 +69,19 @@ struct PassDesc {
   // bundle buffers of the TMA passes (2 or 3; the plan's variant), or 0:
   // the cp.async passes even where a TMA pass exists
   int tma_slots = 2;
+  // FP16 storage of a pass intermediate (mixed precision): the input
+  // (in_half, TMA passes) or output (out_half, TMA and cp.async plain passes)
+  // volume holds __half2 values times a power of two from h_amax / h_len
+  // (half_store_scale); out_absmax (optional, the pipelined forward x pass):
+  // raised to the largest component the pass stores (FP32 output).  A pass
+  // shape whose kernel lacks a requested one fails with MLG_ERR_UNSUPPORTED.
+  int in_half = 0, out_half = 0;
+  const unsigned* h_amax = nullptr;
+  int h_len = 1;
+  unsigned* out_absmax = nullptr;
+  // check only: MLG_OK when a kernel would run the pass with every field
+  // above honoured, MLG_ERR_UNSUPPORTED otherwise; nothing is launched
+  int dry = 0;
 };
 
 // The current device's wait flag (set by a pass whose bounded wait ran out),

@@ -53,6 +53,30 @@ __device__ __forceinline__ float2 cmulf(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 
+// Scale of a pass intermediate stored in FP16: a power of two s with
+// bound * s < 2^15 (< 65504), bound = 2 len amax >= any component of a
+// length-len transform of values whose components are at most amax (the
+// writer recorded amax; writer and reader compute the same s).
+__device__ __forceinline__ float half_store_scale(const unsigned* amax, int len) {
+  const float bound = __uint_as_float(__ldg(amax)) * (float)len * 2.0f;
+  if (!(bound > 0.f) || !(bound < 1e38f)) return 1.f;
+  int e;
+  frexpf(bound, &e);  // bound < 2^e
+  return ldexpf(1.f, 15 - e);
+}
+
+// Largest component magnitude of two complex values.
+__device__ __forceinline__ float absmax4(float4 v) {
+  return fmaxf(fmaxf(fabsf(v.x), fabsf(v.y)), fmaxf(fabsf(v.z), fabsf(v.w)));
+}
+
+// Raises *amax to the warp's largest v (every lane calls; v >= 0).
+__device__ __forceinline__ void warp_amax(unsigned* amax, float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(amax, __float_as_uint(v));
+}
+
 template <int DIR>
 __device__ __forceinline__ float2 twid(const float2* __restrict__ tw, int j) {
   const float2 w = __ldg(tw + j);
@@ -792,6 +816,7 @@ __global__ void __launch_bounds__(COLS > 0 ? cta_threads(COLS) : MAXT,
   int b = blockIdx.x;
   if (b >= nbundles) return;
   const int G = gridDim.x;
+  const float hs = d.out_half ? half_store_scale(d.h_amax, d.h_len) : 1.f;
   if (ring) {  // masks of the first three bundles
     for (int k = 0; k < 3; ++k)
       if (b + k * G < nbundles) fetch_masks(b + k * G, slot(k));
@@ -820,13 +845,28 @@ __global__ void __launch_bounds__(COLS > 0 ? cta_threads(COLS) : MAXT,
       smem_fft<N1, N2, DIR>(reinterpret_cast<float2*>(cur), cols, N1, N2, tw);
     const int ui = (b % gu) * L + l, vi = b / gu;
     if (ui < d.dims[u]) {
-      float2* obase = d.out + (long long)ui * d.out_stride[u] + (long long)vi * d.out_stride[v] + c;
+      const long long obase = (long long)ui * d.out_stride[u] + (long long)vi * d.out_stride[v] + c;
       const float4* const scol = cur + vc;
+      if (d.out_half) {  // FP16 intermediate (mixed precision): complex -> __half2, times hs
+        __half2* const hb = reinterpret_cast<__half2*>(d.out) + obase;
 #pragma unroll 4
-      for (int kk = r0; kk < d.out_len; kk += rstep) {
-        const int k = d.out_lo + kk;
-        const int pos = (k % N1) * N2 + k / N1;
-        *reinterpret_cast<float4*>(obase + (long long)kk * ost) = scol[pos * cv];
+        for (int kk = r0; kk < d.out_len; kk += rstep) {
+          const int k = d.out_lo + kk;
+          const float4 w = scol[((k % N1) * N2 + k / N1) * cv];
+          const __half2 h0 = __floats2half2_rn(w.x * hs, w.y * hs), h1 = __floats2half2_rn(w.z * hs, w.w * hs);
+          uint2 q;
+          q.x = *reinterpret_cast<const unsigned*>(&h0);
+          q.y = *reinterpret_cast<const unsigned*>(&h1);
+          *reinterpret_cast<uint2*>(hb + (long long)kk * ost) = q;
+        }
+      } else {
+        float2* const ob = d.out + obase;
+#pragma unroll 4
+        for (int kk = r0; kk < d.out_len; kk += rstep) {
+          const int k = d.out_lo + kk;
+          const int pos = (k % N1) * N2 + k / N1;
+          *reinterpret_cast<float4*>(ob + (long long)kk * ost) = scol[pos * cv];
+        }
       }
     }
     __syncthreads();  // cur is refilled by the copies issued in the next iteration
@@ -867,6 +907,7 @@ __global__ void __launch_bounds__(cta_threads(COLS), pipe_min_blocks(N1 * N2, CO
 
   int b = blockIdx.x;
   if (b >= nbundles) return;
+  float amax = 0.f;
   issue(b, lb0, xb0);
   for (int it = 0; b < nbundles; ++it, b += gridDim.x) {
     float4* const cur = (it & 1) ? lb1 : lb0;
@@ -906,11 +947,14 @@ __global__ void __launch_bounds__(cta_threads(COLS), pipe_min_blocks(N1 * N2, CO
       for (int kk = r0; kk < d.out_len; kk += RSTEP) {
         const int k = d.out_lo + kk;
         const int pos = (k % N1) * N2 + k / N1;
-        *reinterpret_cast<float4*>(obase + (long long)kk * ost) = scol[pos * CV];
+        const float4 w = scol[pos * CV];
+        *reinterpret_cast<float4*>(obase + (long long)kk * ost) = w;
+        amax = fmaxf(amax, absmax4(w));
       }
     }
     __syncthreads();  // both buffers are refilled by the next iteration's copies
   }
+  if (d.out_absmax) warp_amax(d.out_absmax, amax);  // the FP16 passes' scale (mixed precision)
 }
 
 // Pipelined inverse x pass fused with .* KFC_conj and the coil sum
@@ -1040,8 +1084,16 @@ static inline int blocks_for(const PassDesc& d, int L) {
 
 static inline int threads_for(int cols) { return cta_threads(cols); }
 
+// A pass descriptor asks for an FP16 intermediate or a recorded maximum that
+// the pass shape's kernel does not provide (no message for a dry run).
+static inline int half_unsupported(const PassDesc& d) {
+  if (d.dry) return MLG_ERR_UNSUPPORTED;
+  return fail(MLG_ERR_UNSUPPORTED, "FP16 pass intermediate / maximum not available for this pass shape");
+}
+
 template <int N1, int N2, int DIR, PassMode MODE, int MAXT>
 static int launch_bounded(const FftAxisPlan& a, const PassDesc& d, int L, int threads, cudaStream_t s) {
+  if (d.dry) return MLG_OK;
   const size_t smem = (size_t)a.N * L * d.C * sizeof(float2);
   static bool attr = false;  // per instantiation
   if (!attr) {
@@ -1059,6 +1111,7 @@ static int launch_bounded(const FftAxisPlan& a, const PassDesc& d, int L, int th
 // CTAs per SM) x SMs.
 template <int N1, int N2, int DIR, int MAXT, int COLS>
 static int launch_pipe(const FftAxisPlan& a, const PassDesc& d, int Lp, int threads, cudaStream_t s) {
+  if (d.dry) return MLG_OK;
   const size_t smem = 2 * (size_t)a.N * Lp * d.C * sizeof(float2) +
                       (d.in_lmask ? 4 * (size_t)Lp * d.lmask_words * sizeof(uint32_t) : 0);
   // per instantiation and host thread (serving workers launch concurrently);
@@ -1100,6 +1153,11 @@ static int launch_tma(const FftAxisPlan& a, const PassDesc& d, int Lp, cudaStrea
   if (d.in_mask || d.in_lo < 0 || d.in_len < 1 || d.in_lo + d.in_len > N || d.out_lo < 0 || d.out_len < 1 ||
       d.out_lo + d.out_len > N || Lp * d.C != COLS)
     return MLG_OK;
+  const bool ih = d.in_half != 0, oh = d.out_half != 0;
+  if (ih && oh) return MLG_OK;
+  if constexpr (N2 > NT / COLS) {  // FP16 input needs one step-A line per thread
+    if (ih) return MLG_OK;
+  }
   const int u = d.ax == 0 ? 1 : 0, v = d.ax == 2 ? 1 : 2;
   TmaPass t;
   t.L = Lp;
@@ -1114,31 +1172,46 @@ static int launch_tma(const FftAxisPlan& a, const PassDesc& d, int Lp, cudaStrea
   t.out_lo = d.out_lo;
   t.err = d.wait_err;
   t.test_stall = tma_test_stall() ? 1 : 0;
-  const long long rowb = (long long)COLS * 8;  // shared-memory box starts on 128-byte boundaries
-  if ((t.in_rows * rowb) % 128 || (t.out_lo * rowb) % 128 || (t.out_rows * rowb) % 128) return MLG_OK;
+  t.h_amax = d.h_amax;
+  t.h_len = d.h_len;
+  if ((ih || oh) && (!d.h_amax || (4 * d.C) % 16)) return MLG_OK;
+  // shared-memory box starts on 128-byte boundaries
+  const long long rowb_in = (long long)COLS * (ih ? 4 : 8), rowb_out = (long long)COLS * (oh ? 4 : 8);
+  if ((t.in_rows * rowb_in) % 128 || (t.out_lo * rowb_out) % 128 || (t.out_rows * rowb_out) % 128) return MLG_OK;
   CUtensorMap tin, tout;
   if (tma_line_map(&tin, d.in, d.C, d.dims[u], d.in_stride[u], d.in_len, d.in_stride[d.ax], d.dims[v],
-                   d.in_stride[v], Lp, t.in_rows) != MLG_OK ||
+                   d.in_stride[v], Lp, t.in_rows, ih) != MLG_OK ||
       tma_line_map(&tout, d.out, d.C, d.dims[u], d.out_stride[u], d.out_len, d.out_stride[d.ax], d.dims[v],
-                   d.out_stride[v], Lp, t.out_rows) != MLG_OK)
+                   d.out_stride[v], Lp, t.out_rows, oh) != MLG_OK)
     return MLG_OK;
+  // an FP16 bundle lands in the upper half of its buffer: 128-byte aligned
+  if (ih && ((size_t)N * COLS * 4) % 128) return MLG_OK;
   const size_t smem = (size_t)NSLOT * N * COLS * 8 + 2 * NSLOT * sizeof(uint64_t) + (size_t)N * 8 + 128;
   if (smem > 200 * 1024) return MLG_OK;
-  thread_local int per_sm = 0, sms = 0;
-  thread_local size_t per_sm_smem = 0;
-  if (per_sm == 0 || per_sm_smem != smem) {
-    MLG_CUDA(cudaFuncSetAttribute(fft_pass_tma_kernel<N1, N2, DIR, COLS, NSLOT>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(200 * 1024)));
+  if (d.dry) {
+    *launched = true;
+    return MLG_OK;
+  }
+  auto kern = fft_pass_tma_kernel<N1, N2, DIR, COLS, NSLOT, false, false>;
+  const int vi = ih ? 1 : (oh ? 2 : 0);
+  if constexpr (N2 <= NT / COLS) {
+    if (ih) kern = fft_pass_tma_kernel<N1, N2, DIR, COLS, NSLOT, true, false>;
+  }
+  if (oh) kern = fft_pass_tma_kernel<N1, N2, DIR, COLS, NSLOT, false, true>;
+  // per instantiation, FP16 variant and host thread
+  thread_local int per_sm[3] = {0, 0, 0}, sms = 0;
+  thread_local size_t per_sm_smem[3] = {0, 0, 0};
+  if (per_sm[vi] == 0 || per_sm_smem[vi] != smem) {
+    MLG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(200 * 1024)));
     int dev = 0;
     MLG_CUDA(cudaGetDevice(&dev));
     MLG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    MLG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fft_pass_tma_kernel<N1, N2, DIR, COLS, NSLOT>,
-                                                           NT + 32, smem));
-    per_sm = std::max(1, per_sm);
-    per_sm_smem = smem;
+    MLG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[vi], kern, NT + 32, smem));
+    per_sm[vi] = std::max(1, per_sm[vi]);
+    per_sm_smem[vi] = smem;
   }
-  const int grid = std::max(1, std::min(t.nbundles, per_sm * sms));
-  fft_pass_tma_kernel<N1, N2, DIR, COLS, NSLOT><<<grid, NT + 32, smem, s>>>(tin, tout, t, a.tw);
+  const int grid = std::max(1, std::min(t.nbundles, per_sm[vi] * sms));
+  kern<<<grid, NT + 32, smem, s>>>(tin, tout, t, a.tw);
   MLG_LAUNCHED();
   *launched = true;
   return MLG_OK;
@@ -1155,6 +1228,7 @@ static inline int pipe_lines(const FftAxisPlan& a, int C) {
 // pass (the partial-sum slots the caller reduces), an upper bound of the grid.
 template <int N1, int N2, int CP>
 static int launch_nak_pipe(const FftAxisPlan& a, const PassDesc& d, int n_slots, cudaStream_t s) {
+  if (d.dry) return MLG_OK;
   const int Lp = 16 / (2 * CP);
   const size_t smem = 2 * ((size_t)a.N + d.out_len) * 16 * sizeof(float2) + (size_t)a.N * sizeof(float2);
   thread_local int per_sm = 0, sms = 0;
@@ -1179,6 +1253,7 @@ static int launch_nak_pipe(const FftAxisPlan& a, const PassDesc& d, int n_slots,
 // Pipelined kShannaIn pass over COLS columns (Lp lines).
 template <int N1, int N2, int COLS>
 static int launch_shanna_pipe(const FftAxisPlan& a, const PassDesc& d, int Lp, cudaStream_t s) {
+  if (d.dry) return MLG_OK;
   PassDesc k = d;  // KFC as the copied input: rows of C values, lines of in_len rows
   k.in = d.kfc;
   k.in_stride[0] = d.C;
@@ -1210,6 +1285,7 @@ static int launch_shanna_pipe(const FftAxisPlan& a, const PassDesc& d, int Lp, c
 
 template <int N1, int N2, int DIR, PassMode MODE>
 static int launch_pass(const FftAxisPlan& a, const PassDesc& d, int L, cudaStream_t s) {
+  if ((d.in_half || d.out_half) && !d.h_amax) return half_unsupported(d);
   if constexpr (MODE == PassMode::kShannaIn && N1 > 0) {
     // one image shared by the coils, even C, 16 / 24 / 32 columns per bundle
     const int Lp = pipe_lines(a, d.C), cols = Lp * d.C;
@@ -1257,6 +1333,9 @@ static int launch_pass(const FftAxisPlan& a, const PassDesc& d, int L, cudaStrea
         }
         if (st != MLG_OK || done) return st;
       }
+      // FP16 input exists only on the TMA passes; the cp.async passes below
+      // store FP16 but load FP32 only
+      if (d.in_half) return half_unsupported(d);
       // the column counts of 2, 4, 8, 12, 16, 24 and 32 coils: compile-time
       switch (cols) {
         case 16: return launch_pipe<N1, N2, DIR, kFftThreads, 16>(a, d, Lp, tp, s);
@@ -1268,6 +1347,9 @@ static int launch_pass(const FftAxisPlan& a, const PassDesc& d, int L, cudaStrea
       return launch_pipe<N1, N2, DIR, kFftMaxThreads, 0>(a, d, Lp, tp, s);
     }
   }
+  // the FP16 intermediates and the recorded maximum exist only on the
+  // pipelined passes above
+  if (d.in_half || d.out_half || d.out_absmax) return half_unsupported(d);
   const int threads = threads_for(L * d.C);
   if (threads <= kFftThreads) return launch_bounded<N1, N2, DIR, MODE, kFftThreads>(a, d, L, threads, s);
   return launch_bounded<N1, N2, DIR, MODE, kFftMaxThreads>(a, d, L, threads, s);

@@ -44,6 +44,11 @@ struct TmaPass {
   int out_chunks = 1;
   int out_rows = 0;   // rows per store box (out_chunks * out_rows = out_len)
   int* err = nullptr; // set to 1 when a wait runs out (device word), or NULL
+  // FP16 input (IN_H) or output (OUT_H) bundles: the scale comes from the
+  // component maximum the writer of the first FP16 pass's input recorded
+  // (half_store_scale(h_amax, h_len))
+  const unsigned* h_amax = nullptr;
+  int h_len = 1;
   // test hook (MLG_TEST_WAIT_TIMEOUT=1): CTA 0 never loads its first bundle,
   // so its transform threads' bounded wait runs out and the timeout path runs
   int test_stall = 0;
@@ -161,20 +166,31 @@ constexpr int tma_step_c_iters() {
 // have read its own, then writes row k1 + N1 k2.  Barriers are over the NT
 // transform threads only.  tws: the axis' twiddle table exp(-2 pi i j/N)
 // copied into shared memory (the same values as the global table).
-template <int N1, int N2, int DIR, int COLS, int NT>
-__device__ __forceinline__ void smem_fft_natural(float2* s, const float2* tws) {
+// IN_H: the bundle arrived as FP16 in the upper half of the buffer; step A
+// reads its rows from there (times hs), waits for every thread to have read,
+// then writes FP32 (one n2 per thread: N2 <= NT / COLS).  OUT_H: step C
+// writes the rows as FP16 (times hs) into the lower half, row k at k.
+template <int N1, int N2, int DIR, int COLS, int NT, bool IN_H = false, bool OUT_H = false>
+__device__ __forceinline__ void smem_fft_natural(float2* s, const float2* tws, float hs) {
   constexpr int G = NT / COLS;
   constexpr int KI = tma_step_c_iters<N1, N2, COLS, NT>();
   const int col = threadIdx.x % COLS, g = threadIdx.x / COLS;
   float2* const sc = s + col;
+  if constexpr (IN_H) {
+    static_assert(N2 <= G, "FP16 input: one step-A line per thread");
+    const __half2* const hsrc = reinterpret_cast<const __half2*>(s + (size_t)N1 * N2 * COLS / 2) + col;
+    const int n2 = g;
+    float2 r[N1];
+    if (n2 < N2) {
 #pragma unroll
-  for (int n2b = 0; n2b < N2; n2b += G) {
-    const int n2 = n2b + g;
-    if (N2 % G == 0 || n2 < N2) {
+      for (int n1 = 0; n1 < N1; ++n1) {
+        const float2 v = __half22float2(hsrc[(n1 * N2 + n2) * COLS]);
+        r[n1] = make_float2(v.x * hs, v.y * hs);
+      }
+    }
+    bar_transform<NT>();  // every FP16 row read before FP32 rows overwrite them
+    if (n2 < N2) {
       float2* const p = sc + n2 * COLS;
-      float2 r[N1];
-#pragma unroll
-      for (int n1 = 0; n1 < N1; ++n1) r[n1] = p[n1 * N2 * COLS];
       reg_fft<N1, DIR>(r);
       if (n2) {
 #pragma unroll
@@ -185,6 +201,27 @@ __device__ __forceinline__ void smem_fft_natural(float2* s, const float2* tws) {
       }
 #pragma unroll
       for (int k1 = 0; k1 < N1; ++k1) p[k1 * N2 * COLS] = r[k1];
+    }
+  } else {
+#pragma unroll
+    for (int n2b = 0; n2b < N2; n2b += G) {
+      const int n2 = n2b + g;
+      if (N2 % G == 0 || n2 < N2) {
+        float2* const p = sc + n2 * COLS;
+        float2 r[N1];
+#pragma unroll
+        for (int n1 = 0; n1 < N1; ++n1) r[n1] = p[n1 * N2 * COLS];
+        reg_fft<N1, DIR>(r);
+        if (n2) {
+#pragma unroll
+          for (int k1 = 1; k1 < N1; ++k1) {
+            const float2 w = tws[n2 * k1];
+            r[k1] = cmulf(r[k1], DIR < 0 ? w : make_float2(w.x, -w.y));
+          }
+        }
+#pragma unroll
+        for (int k1 = 0; k1 < N1; ++k1) p[k1 * N2 * COLS] = r[k1];
+      }
     }
   }
   bar_transform<NT>();
@@ -205,7 +242,13 @@ __device__ __forceinline__ void smem_fft_natural(float2* s, const float2* tws) {
     const int k1 = i * G + g;
     if (N1 % G == 0 || k1 < N1) {
 #pragma unroll
-      for (int k2 = 0; k2 < N2; ++k2) sc[(k1 + N1 * k2) * COLS] = r[i][k2];
+      for (int k2 = 0; k2 < N2; ++k2) {
+        if constexpr (OUT_H)
+          reinterpret_cast<__half2*>(s)[(k1 + N1 * k2) * COLS + col] =
+              __floats2half2_rn(r[i][k2].x * hs, r[i][k2].y * hs);
+        else
+          sc[(k1 + N1 * k2) * COLS] = r[i][k2];
+      }
     }
   }
 }
@@ -217,7 +260,7 @@ constexpr int tma_min_blocks() {
   return by_smem < 1 ? 1 : (by_smem > 3 ? 3 : by_smem);
 }
 
-template <int N1, int N2, int DIR, int COLS, int NSLOT>
+template <int N1, int N2, int DIR, int COLS, int NSLOT, bool IN_H = false, bool OUT_H = false>
 __global__ void __launch_bounds__(cta_threads(COLS) + 32, (tma_min_blocks<N1 * N2, COLS, NSLOT>()))
     fft_pass_tma_kernel(const __grid_constant__ CUtensorMap tin, const __grid_constant__ CUtensorMap tout, TmaPass a,
                         const float2* __restrict__ tw) {
@@ -248,18 +291,20 @@ __global__ void __launch_bounds__(cta_threads(COLS) + 32, (tma_min_blocks<N1 * N
   if (tid >= NT) {
     if (tid != NT) return;
     // producer: one thread
+    constexpr int kInElem = IN_H ? 4 : 8, kOutElem = OUT_H ? 4 : 8;  // bytes per complex value
     auto load = [&](int slot, int b) {
-      unsigned char* dst = base + slot * kBuf;
-      mbar_arrive_expect_tx(full + slot, kBuf);
+      unsigned char* dst = base + slot * kBuf + (IN_H ? kBuf / 2 : 0);
+      mbar_arrive_expect_tx(full + slot, IN_H ? kBuf / 2 : kBuf);
       const int c1 = (b % a.gu) * a.L, c3 = b / a.gu;
       for (int k = 0; k < a.in_chunks; ++k)
-        tma_load_4d(dst + (size_t)k * a.in_rows * COLS * 8, &tin, 0, c1, k * a.in_rows - a.in_lo, c3, full + slot);
+        tma_load_4d(dst + (size_t)k * a.in_rows * COLS * kInElem, &tin, 0, c1, k * a.in_rows - a.in_lo, c3,
+                    full + slot);
     };
     auto store = [&](int slot, int b) {
-      const unsigned char* src = base + slot * kBuf + (size_t)a.out_lo * COLS * 8;
+      const unsigned char* src = base + slot * kBuf + (size_t)a.out_lo * COLS * kOutElem;
       const int c1 = (b % a.gu) * a.L, c3 = b / a.gu;
       for (int k = 0; k < a.out_chunks; ++k)
-        tma_store_4d(&tout, 0, c1, k * a.out_rows, c3, src + (size_t)k * a.out_rows * COLS * 8);
+        tma_store_4d(&tout, 0, c1, k * a.out_rows, c3, src + (size_t)k * a.out_rows * COLS * kOutElem);
       bulk_commit();
     };
     int it = 0;
@@ -295,22 +340,27 @@ __global__ void __launch_bounds__(cta_threads(COLS) + 32, (tma_min_blocks<N1 * N
     return;
   }
   // transform threads
+  float hs = 1.f;
+  if constexpr (IN_H || OUT_H) {
+    hs = half_store_scale(a.h_amax, a.h_len);
+    if (IN_H) hs = 1.f / hs;  // a power of two: exact
+  }
   int it = 0;
   for (int b = blockIdx.x; b < a.nbundles; b += G, ++it) {
     const int slot = it % NSLOT;
     const bool ok = mbar_wait(full + slot, (unsigned)(it / NSLOT) & 1u, abort, a.err);
     if (bar_transform_or<NT>(!ok)) return;  // all transform threads leave together
-    smem_fft_natural<N1, N2, DIR, COLS, NT>(reinterpret_cast<float2*>(base + slot * kBuf), tws);
+    smem_fft_natural<N1, N2, DIR, COLS, NT, IN_H, OUT_H>(reinterpret_cast<float2*>(base + slot * kBuf), tws, hs);
     fence_proxy_async_smem();  // the transform's writes become visible to the store
     mbar_arrive(done + slot);
   }
 }
 
 // Host: 4-D tensor map of a coil-fastest volume seen as the line boxes of
-// one pass (mlg_fft.cu).  Strides in float2 units; box = (2C floats, box_L
-// lines, box_rows rows, 1).
+// one pass (mlg_fft.cu).  Strides in complex units; box = (2C floats, box_L
+// lines, box_rows rows, 1); half: FP16 values (2C halves per cell).
 int tma_line_map(CUtensorMap* map, const void* base, int C, int dim_u, long long st_u, int len, long long st_ax,
-                 int dim_v, long long st_v, int box_L, int box_rows);
+                 int dim_v, long long st_v, int box_L, int box_rows, bool half = false);
 // Whether the TMA passes are enabled (MLG_FFT_TMA=0 turns them off).
 bool tma_passes_enabled();
 // The timeout test hook (MLG_TEST_WAIT_TIMEOUT=1), read once per process.

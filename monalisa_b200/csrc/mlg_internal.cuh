@@ -264,7 +264,8 @@ struct SpmmArgs {
   // stay FP32.
   bool half_values = false;
   // Short rows of an ordered non-empty product from the matrix's row
-  // records (ord_rec), when built; FP32 values only
+  // records (ord_rec), when built (FP32 values, rounded to FP16 as read with
+  // half_values)
   bool records = false;
   // Optional: raised (atomicMax on the bits) to the largest |re| or |im| of
   // the values written, before any FP16 rounding (device, non-negative float)

@@ -43,8 +43,12 @@ static void box_strides(const int e[3], int C, long long st[3]) {
 }
 
 // Forward passes: x (image -> A), y (A -> B), z (B -> grid).  The last pass
-// of the transform writes the grid.
-static int forward_pass(mlg_plan_s* p, int ax, const float2* x, bool x_per_coil, cudaStream_t s) {
+// of the transform writes the grid.  half (3-D): B in scaled FP16 -- the x
+// pass records max|A| in mix_amax[0], the y pass stores B times the power of
+// two that bounds a length-n[1] transform of it below 2^15, the z pass reads
+// it back; dry: check only (PassDesc::dry).
+static int forward_pass(mlg_plan_s* p, int ax, const float2* x, bool x_per_coil, cudaStream_t s, bool half = false,
+                        bool dry = false) {
   const int C = p->nCh, d = p->imDim;
   const int* N = p->N;
   const int* n = p->n;
@@ -57,7 +61,13 @@ static int forward_pass(mlg_plan_s* p, int ax, const float2* x, bool x_per_coil,
   pd.C = C;
   pd.wait_err = p->wait_err;
   pd.tma_slots = p->pass_buffers;
+  pd.dry = dry ? 1 : 0;
+  if (half) {
+    pd.h_amax = p->mix_amax;
+    pd.h_len = n[1];
+  }
   if (ax == 0) {
+    if (half) pd.out_absmax = p->mix_amax;
     pd.dims[1] = n[1];
     pd.dims[2] = n[2];
     pd.in_lo = p->off[0];
@@ -83,10 +93,12 @@ static int forward_pass(mlg_plan_s* p, int ax, const float2* x, bool x_per_coil,
     box_strides(d == 2 ? eG : eB, C, pd.out_stride);
     pd.out_lo = 0;
     pd.out_len = N[1];
+    pd.out_half = half ? 1 : 0;
     return fft_pass(p->ax[1], PassMode::kPlain, pd, nullptr, s);
   }
   pd.dims[0] = N[0];
   pd.dims[1] = N[1];
+  pd.in_half = half ? 1 : 0;
   pd.in = p->bufB;
   box_strides(eB, C, pd.in_stride);
   pd.in_lo = p->off[2];
@@ -131,8 +143,12 @@ static void set_gut_input(mlg_plan_s* p, PassDesc& pd, const float2* y, const fl
   pd.cell_stride[2] = (long long)p->N[0] * p->N[1];
 }
 
+// half (3-D): B in scaled FP16 -- the Gut product records max|grid| in
+// mix_amax[1], the z pass stores B times the power of two that bounds a
+// length-N[2] transform of it below 2^15, the y pass reads it back; dry:
+// check only (PassDesc::dry).
 static int inverse_pass(mlg_plan_s* p, int ax, const float2* y, const float* HY, float scale, float2* x,
-                        double* partial, int* n_partial, cudaStream_t s) {
+                        double* partial, int* n_partial, cudaStream_t s, bool half = false, bool dry = false) {
   const int C = p->nCh, d = p->imDim;
   const int* N = p->N;
   const int* n = p->n;
@@ -145,6 +161,11 @@ static int inverse_pass(mlg_plan_s* p, int ax, const float2* y, const float* HY,
   pd.C = C;
   pd.wait_err = p->wait_err;
   pd.tma_slots = p->pass_buffers;
+  pd.dry = dry ? 1 : 0;
+  if (half) {
+    pd.h_amax = p->mix_amax + 1;
+    pd.h_len = N[2];
+  }
   const bool gut_in = fused_gut(p) && ax == d - 1;
   if (gut_in) set_gut_input(p, pd, y, HY);
   if (p->adjoint_mode == kAdjMasked && ax == d - 1) {
@@ -167,6 +188,7 @@ static int inverse_pass(mlg_plan_s* p, int ax, const float2* y, const float* HY,
     box_strides(eB, C, pd.out_stride);
     pd.out_lo = p->off[2];
     pd.out_len = n[2];
+    pd.out_half = half ? 1 : 0;
     return fft_pass(p->ax[2], plain, pd, nullptr, s);
   }
   if (ax == 1) {
@@ -174,6 +196,7 @@ static int inverse_pass(mlg_plan_s* p, int ax, const float2* y, const float* HY,
     pd.dims[2] = n[2];
     pd.in = d == 2 ? p->grid : p->bufB;
     box_strides(d == 2 ? eG : eB, C, pd.in_stride);
+    pd.in_half = half ? 1 : 0;
     pd.in_lo = 0;
     pd.in_len = N[1];
     pd.out = p->bufA;
@@ -198,11 +221,38 @@ static int inverse_pass(mlg_plan_s* p, int ax, const float2* y, const float* HY,
   return fft_pass(p->ax[0], PassMode::kNakatshaOut, pd, n_partial, s);
 }
 
+// Whether the CG steps of a mixed solve keep bufB in FP16: a 3-D plan, a
+// coil count whose FP16 cells fill 16-byte TMA rows, no fused Gut gather (it
+// reads FP32), and a dry run of the four passes accepted by their kernels.
+// Cached per (pass_buffers, adjoint_mode), the plan state the pass kernels
+// depend on.
+bool half_intermediate_possible(mlg_plan_s* p) {
+  if (p->imDim != 3 || (p->nCh % 4) != 0 || fused_gut(p)) return false;
+  const int key = p->pass_buffers * 8 + p->adjoint_mode;
+  if (p->half_b_key == key) return p->half_b_ok;
+  // the maxima's words are not read by a dry run; any non-null address will do
+  unsigned* const words = p->mix_amax;
+  unsigned dummy[2];
+  if (!words) p->mix_amax = dummy;
+  bool ok = true;
+  for (int ax = 0; ax < 3 && ok; ++ax) ok = forward_pass(p, ax, nullptr, false, nullptr, true, true) == MLG_OK;
+  for (int ax = 2; ax >= 1 && ok; --ax)
+    ok = inverse_pass(p, ax, nullptr, nullptr, 1.f, nullptr, nullptr, nullptr, nullptr, true, true) == MLG_OK;
+  p->mix_amax = words;
+  p->half_b_key = key;
+  p->half_b_ok = ok;
+  return ok;
+}
+
+static bool half_b(mlg_plan_s* p) { return p->mp_half && p->mix_amax && half_intermediate_possible(p); }
+
 int shanna_stage(mlg_plan_s* p, int stage, const float2* x, bool x_per_coil, float2* y, const float* sqn_w,
                  double* partial, int* n_partial, cudaStream_t s) {
   if (stage < 3) {
     if (stage >= p->imDim) return MLG_OK;
-    return forward_pass(p, stage, x, x_per_coil, s);
+    const bool half = half_b(p);
+    if (half && stage == 0) MLG_CUDA(cudaMemsetAsync(p->mix_amax, 0, sizeof(unsigned), s));
+    return forward_pass(p, stage, x, x_per_coil, s, half);
   }
   SpmmArgs a;
   a.m = &p->Gu_s;
@@ -253,11 +303,15 @@ int nakatsha_stage(mlg_plan_s* p, int stage, const float2* y, const float* HY, f
     a.nonempty_only = p->adjoint_mode == kAdjMasked;
     a.records = p->gut_records != 0;
     a.seg_scratch = p->seg_scratch;
+    if (half_b(p)) {
+      MLG_CUDA(cudaMemsetAsync(p->mix_amax + 1, 0, sizeof(unsigned), s));
+      a.absmax = p->mix_amax + 1;
+    }
     return spmm(a, s);
   }
   const int ax = p->imDim - stage;
   if (ax < 0) return MLG_OK;
-  return inverse_pass(p, ax, y, HY, scale, x, partial, n_partial, s);
+  return inverse_pass(p, ax, y, HY, scale, x, partial, n_partial, s, ax >= 1 && half_b(p));
 }
 
 int shanna_run(mlg_plan_s* p, const float2* x, bool x_per_coil, float2* y, const float* sqn_w, double* partial,

@@ -77,6 +77,15 @@ struct mlg_plan_s {
   bool mp_half = false;
   float* kscale = nullptr;
   unsigned* kabsmax = nullptr;
+  // FP16 storage of bufB (the y / z pass intermediate of a 3-D transform)
+  // while mp_half is set, where every pass involved supports it: mix_amax[0]
+  // = largest component of the forward x pass's output, mix_amax[1] = of the
+  // Gut product (device words kscale + 4, + 5), the bounds of the FP16
+  // scales; half_b_key / half_b_ok cache the dry-run check of the four passes
+  // per (pass_buffers, adjoint_mode)
+  unsigned* mix_amax = nullptr;
+  int half_b_key = -1;
+  bool half_b_ok = false;
   int cg_graph_prec = -1;  // precision the captured CG step was built for
   mlg_plan_s* owner = nullptr;  // the plan whose buffers are borrowed
   int n_borrowers = 0;          // plans borrowing this one's buffers
@@ -92,6 +101,8 @@ int shanna_stage(mlg_plan_s* p, int stage, const float2* x, bool x_per_coil, flo
 int nakatsha_stage(mlg_plan_s* p, int stage, const float2* y, const float* HY, float scale, float2* x,
                    double* partial, int* n_partial, cudaStream_t s);
 bool adjoint_mode_valid(const mlg_plan_s* p, int mode);
+// whether the plan's passes take bufB in FP16 (mixed CG steps; host check)
+bool half_intermediate_possible(mlg_plan_s* p);
 int shanna_run(mlg_plan_s* p, const float2* x, bool x_per_coil, float2* y, const float* sqn_w, double* partial,
                int* n_partial, cudaStream_t s);
 int nakatsha_run(mlg_plan_s* p, const float2* y, const float* HY, float scale, float2* x, double* partial,

@@ -224,11 +224,12 @@ static int ensure_solver_buffers(mlg_plan_s* p) {
   if (cudaMalloc(&p->x_p, ni) != cudaSuccess || cudaMalloc(&p->x_dagM, ni) != cudaSuccess ||
       cudaMalloc(&p->k_res, nk) != cudaSuccess || cudaMalloc(&p->k_Mp, nk) != cudaSuccess ||
       cudaMalloc(&p->HY, sizeof(float) * (size_t)std::max(1, p->nPt)) != cudaSuccess ||
-      cudaMalloc(&p->kscale, 4 * sizeof(float)) != cudaSuccess) {
+      cudaMalloc(&p->kscale, 8 * sizeof(float)) != cudaSuccess) {
     cudaGetLastError();
     return fail(MLG_ERR_OOM, "solver work buffers: device allocation failed");
   }
   p->kabsmax = reinterpret_cast<unsigned*>(p->kscale + 2);
+  p->mix_amax = reinterpret_cast<unsigned*>(p->kscale + 4);
   p->solver_nPt = p->nPt;
   p->bytes += 2 * ni + 2 * nk + sizeof(float) * (size_t)p->nPt;
   return MLG_OK;
@@ -446,9 +447,14 @@ extern "C" int mlg_plan_profile(mlg_plan_t p, int iters, double* ms) {
   const long long nk = (long long)p->nPt * p->nCh;
   MLG_CUDA(cudaMemsetAsync(p->x_p, 0, sizeof(float2) * (size_t)p->nu_tot, s));
   MLG_CUDA(cudaMemsetAsync(p->k_res, 0, sizeof(float2) * (size_t)nk, s));
+  // a mixed plan's stages as they run inside its CG steps: FP16 M p (scale
+  // 1) and, where supported, the FP16 transform intermediate (maxima zeroed)
+  static const float k_init[8] = {1.f, 1.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  MLG_CUDA(cudaMemcpyAsync(p->kscale, k_init, sizeof(k_init), cudaMemcpyHostToDevice, s));
   constexpr int S = kShannaStages + kNakatshaStages;
   cudaEvent_t ev[S + 1];
   for (int k = 0; k <= S; ++k) MLG_CUDA(cudaEventCreate(&ev[k]));
+  p->mp_half = p->precision == MLG_PRECISION_MIXED;  // reset below on every path
   double acc[S] = {0};
   int st = MLG_OK;
   for (int it = 0; it <= iters && st == MLG_OK; ++it) {
@@ -469,6 +475,7 @@ extern "C" int mlg_plan_profile(mlg_plan_t p, int iters, double* ms) {
       acc[k] += v;
     }
   }
+  p->mp_half = false;
   for (int k = 0; k <= S; ++k) cudaEventDestroy(ev[k]);
   for (int k = 0; k < S; ++k) ms[k] = acc[k] / iters;
   return st;
@@ -606,7 +613,7 @@ extern "C" int mlg_plan_autotune_variants(mlg_plan_t p, int reps, double* ms) {
     }
   }
   p->pass_buffers = best_buf;
-  if (st == MLG_OK && p->Gut_s.ord_rec && p->adjoint_mode == 2 && p->precision == MLG_PRECISION_FP32) {
+  if (st == MLG_OK && p->Gut_s.ord_rec && p->adjoint_mode == 2) {
     for (int v = 0; v <= 1 && st == MLG_OK; ++v) {
       p->gut_records = v;
       t[3 + v] = time_it(false);
@@ -648,5 +655,11 @@ extern "C" int mlg_plan_set_precision(mlg_plan_t p, int precision) {
 extern "C" int mlg_plan_get_precision(mlg_plan_t p, int* precision) {
   MLG_CHECK(p && precision, "NULL argument");
   *precision = p->precision;
+  return MLG_OK;
+}
+
+extern "C" int mlg_plan_get_half_intermediate(mlg_plan_t p, int* on) {
+  MLG_CHECK(p && on, "NULL argument");
+  *on = p->precision == MLG_PRECISION_MIXED && half_intermediate_possible(p) ? 1 : 0;
   return MLG_OK;
 }

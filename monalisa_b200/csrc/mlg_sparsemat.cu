@@ -56,10 +56,21 @@ __device__ __forceinline__ float abs_max4(float4 v) {
   return fmaxf(fmaxf(fabsf(v.x), fabsf(v.y)), fmaxf(fabsf(v.z), fabsf(v.w)));
 }
 
-// One atomic per warp: the warp's largest value (all lanes must call).
-__device__ __forceinline__ void warp_absmax(unsigned* absmax, float v) {
+// The block's largest value (v >= 0) into *absmax: one atomic per block, and
+// none when the recorded value is already as large -- atomics on one word
+// serialise, and a product has thousands of blocks.  Every thread of the
+// block must call.
+__device__ __forceinline__ void block_absmax(unsigned* absmax, float v) {
+  __shared__ float wmax[32];
   for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
-  if ((threadIdx.x & 31) == 0) atomicMax(absmax, __float_as_uint(v));
+  if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float m = 0.f;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m = fmaxf(m, wmax[w]);
+    const unsigned u = __float_as_uint(m);
+    if (u > *reinterpret_cast<volatile const unsigned*>(absmax)) atomicMax(absmax, u);
+  }
 }
 
 template <Layout L>
@@ -304,6 +315,7 @@ __device__ __forceinline__ void mid_rows_block(const SpmmParams& p, const int* _
   const bool active = eg < EG;
   const bool scale = p.in_row_scale != nullptr;
   const float4* in = reinterpret_cast<const float4*>(p.in.a);
+  float amax = 0.f;
   for (int i = block * 8 + (int)(threadIdx.x >> 5); i < n_rows; i += nblocks * 8) {
     const uint2 be = __ldg(bounds + i);
     if (be.y - be.x > (uint32_t)kLongRow) continue;  // segment kernels own it (uniform in the warp)
@@ -333,8 +345,10 @@ __device__ __forceinline__ void mid_rows_block(const SpmmParams& p, const int* _
         s = make_float4(__fmul_rn(s.x, p.out_scale), __fmul_rn(s.y, p.out_scale), __fmul_rn(s.z, p.out_scale),
                         __fmul_rn(s.w, p.out_scale));
       reinterpret_cast<float4*>(p.out.a)[(long long)__ldg(rows + i) * P + pi] = s;
+      amax = fmaxf(amax, abs_max4(s));
     }
   }
+  if (p.absmax) block_absmax(p.absmax, amax);  // every thread of the block reaches it
 }
 
 // PPT coil pairs per thread: the row's bounds and each entry's column and
@@ -441,7 +455,7 @@ __global__ void __launch_bounds__(256, pair_min_blocks<PPT>()) spmm_pair_kernel(
 #pragma unroll
     for (int u = 0; u < PPT; ++u) finish_pair(r, pi + u, acc[u], w);
   }
-  if (p.absmax) warp_absmax(p.absmax, amax);
+  if (p.absmax) block_absmax(p.absmax, amax);
   if (p.partial) {
     const double t = block_sum(sq, sh);
     if (threadIdx.x == 0) p.partial[bid] = t;
@@ -479,9 +493,12 @@ static void launch_pair(int ppt, bool out_h, bool contract, const SpmmParams& p,
 // input), and the record stream is smaller than the bounds and entries it
 // replaces.  Rows with more entries loop over their CSR entries.  Per coil
 // the entries are summed in stored order with the same fused multiply-adds
-// as spmm_pair_kernel: the outputs are identical.  The first mid.blocks
-// blocks gather the mid rows a warp each, as there.  Eight blocks per SM, as
-// the pair kernel.
+// as spmm_pair_kernel: the outputs are identical.  With FP16 matrix values
+// (p.val_h) the inline FP32 values are rounded to FP16 as they are read,
+// which gives the values the CSR rows read from val_h.  The first mid.blocks
+// blocks gather the mid rows a warp each, as there.  p.absmax (optional) is
+// raised to the largest output component.  Eight blocks per SM, as the pair
+// kernel.
 __global__ void __launch_bounds__(256, 8) spmm_rec_kernel(SpmmParams p, const uint4* __restrict__ rec, int n_rows,
                                                           MidRows mid) {
   if ((int)blockIdx.x < mid.blocks) {
@@ -494,7 +511,9 @@ __global__ void __launch_bounds__(256, 8) spmm_rec_kernel(SpmmParams p, const ui
   const int nr = (int)min((long long)p.rows_per_block, (long long)n_rows - i0);
   const int total = nr * P;
   const bool scale = p.in_row_scale != nullptr;
+  const bool half_v = p.val_h != nullptr;  // FP16 matrix values: the inline FP32 values rounded alike
   const float4* in = reinterpret_cast<const float4*>(p.in.a);
+  float amax = 0.f;
   for (int it = threadIdx.x; it < total; it += blockDim.x) {
     const int lr = it / P, pi = it - lr * P;
     const uint4* rp = rec + (i0 + lr) * 2;
@@ -512,6 +531,11 @@ __global__ void __launch_bounds__(256, 8) spmm_rec_kernel(SpmmParams p, const ui
       const uint32_t c0 = h0.z, c1 = h1.x, c2 = h1.z;
       float4 v0 = make_float4(0.f, 0.f, 0.f, 0.f), v1 = v0, v2 = v0;
       float m0 = __uint_as_float(h0.w), m1 = __uint_as_float(h1.y), m2 = __uint_as_float(h1.w);
+      if (half_v) {
+        m0 = __half2float(__float2half_rn(m0));
+        m1 = __half2float(__float2half_rn(m1));
+        m2 = __half2float(__float2half_rn(m2));
+      }
       if (n > 0) v0 = __ldg(in + (long long)c0 * P + pi);
       if (n > 1) v1 = __ldg(in + (long long)c1 * P + pi);
       if (n > 2) v2 = __ldg(in + (long long)c2 * P + pi);
@@ -528,7 +552,7 @@ __global__ void __launch_bounds__(256, 8) spmm_rec_kernel(SpmmParams p, const ui
 #pragma unroll 4
       for (uint32_t k = b; k < b + n; ++k) {
         const int j = __ldg(p.col + k);
-        float m = __ldg(p.val + k);
+        float m = val_at(p, k);
         const float4 v = __ldg(in + (long long)j * P + pi);
         if (scale) m = __fmul_rn(m, __ldg(p.in_row_scale + j));
         fma4(m, v);
@@ -538,7 +562,9 @@ __global__ void __launch_bounds__(256, 8) spmm_rec_kernel(SpmmParams p, const ui
       acc = make_float4(__fmul_rn(acc.x, p.out_scale), __fmul_rn(acc.y, p.out_scale), __fmul_rn(acc.z, p.out_scale),
                         __fmul_rn(acc.w, p.out_scale));
     reinterpret_cast<float4*>(p.out.a)[r * P + pi] = acc;
+    amax = fmaxf(amax, abs_max4(acc));
   }
+  if (p.absmax) block_absmax(p.absmax, amax);
 }
 
 __global__ void rec_build_kernel(const int* __restrict__ rows, const uint2* __restrict__ bounds, int n,
@@ -674,8 +700,7 @@ int spmm(const SpmmArgs& a, cudaStream_t s) {
       MLG_CHECK(ordered || !a.nonempty_only, "non-empty-row products need the ordered row list");
       // operator products over a split order: the short rows by the pair
       // kernel, the longer ones by a warp each
-      const bool split = ordered && a.contract && m.ord_short >= 0 && !oh && !a.partial && !a.absmax &&
-                         a.nCh / 2 <= 16;
+      const bool split = ordered && a.contract && m.ord_short >= 0 && !oh && !a.partial && a.nCh / 2 <= 16;
       const int n_pair = split ? m.ord_short : (int)nrows;
       MidRows mid;
       if (split && nrows > n_pair) {  // about two mid rows per warp
@@ -685,7 +710,8 @@ int spmm(const SpmmArgs& a, cudaStream_t s) {
         mid.blocks = (mid.n + 15) / 16;
       }
       const int grid_pair = split ? (n_pair + p.rows_per_block - 1) / p.rows_per_block : grid_short;
-      if (split && m.ord_rec && !a.half_values && (records_forced() >= 0 ? records_forced() == 1 : a.records) && grid_pair + mid.blocks > 0) {
+      const bool recs = records_forced() >= 0 ? records_forced() == 1 : a.records;
+      if (split && m.ord_rec && recs && grid_pair + mid.blocks > 0) {
         spmm_rec_kernel<<<grid_pair + mid.blocks, 256, 0, s>>>(p, reinterpret_cast<const uint4*>(m.ord_rec), n_pair,
                                                                mid);
         MLG_LAUNCHED();

@@ -73,7 +73,8 @@ def main(argv=None):
     ms = np.zeros(len(STAGES))
     N.call("mlg_plan_profile", rec.plan.handle, max(1, args.reps), N.dptr(ms))
     print(f"{n}^3 image, {Ng}^3 grid, {args.spokes}x{args.samples} samples, {args.coils} coils, "
-          f"adjoint {rec.plan.adjoint_mode}, precision {args.precision}, variant {rec.plan.variant}, Gu nnz {Gu.nnz}")
+          f"adjoint {rec.plan.adjoint_mode}, precision {args.precision}, variant {rec.plan.variant}, "
+          f"fp16 intermediate {rec.plan.half_intermediate and args.precision == 'mixed'}, Gu nnz {Gu.nnz}")
     for name, v in zip(STAGES, ms):
         print(f"  {name:6s} {v:8.4f} ms")
     rec.plan.close()

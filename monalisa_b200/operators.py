@@ -204,9 +204,21 @@ class NufftPlan:
     @precision.setter
     def precision(self, name: str):
         """'fp32', 'mixed' (FP16 matrix values, the CG-SENSE solver's forward
-        product M p stored in scaled FP16, FP32 residual and sums, FP64 scalars) or
-        'fp16_values' (FP16 matrix values only)."""
+        product M p and, where the plan supports it, the 3-D transforms'
+        intermediate stored in scaled FP16 inside the CG steps; FP32 residual,
+        sums and FFT arithmetic, FP64 scalars) or 'fp16_values' (FP16 matrix
+        values only)."""
         N.call("mlg_plan_set_precision", self._h, self.PRECISIONS.index(name))
+
+    @property
+    def half_intermediate(self) -> bool:
+        """Whether the CG steps of a mixed solve keep the intermediate of the
+        3-D transforms (after the y pass of the forward, the z pass of the
+        adjoint) in scaled FP16: mixed precision on a plan whose passes support
+        it (3-D, a multiple of 4 coils, TMA line passes)."""
+        m = ctypes.c_int()
+        N.call("mlg_plan_get_half_intermediate", self._h, ctypes.byref(m))
+        return bool(m.value)
 
     def autotune(self, reps: int = 3, variants: bool = True) -> dict:
         """Times the valid adjoint strategies and keeps the fastest, then (with

@@ -55,6 +55,7 @@ def test_mixed_cg_sense_within_1e3_of_fp64(case):
     r32, x32 = _recon(case, "fp32")
     rm, xm = _recon(case, "mixed")
     assert rm.plan.precision == "mixed" and rm.plan.adjoint_mode != "fused"
+    assert rm.plan.half_intermediate  # 3-D, 8 coils, TMA passes: B in FP16 inside the CG steps
     rh, xh = _recon(case, "fp16_values")
     assert rh.plan.precision == "fp16_values"
     e32, em, eh = rel(x32, x64), rel(xm, x64), rel(xh, x64)
@@ -62,6 +63,29 @@ def test_mixed_cg_sense_within_1e3_of_fp64(case):
     assert em <= 1e-3, em
     assert eh <= 1e-3, eh
     assert em > e32 and eh > e32  # the reduced-precision paths really run in lower precision
+
+
+def test_mixed_fp16_intermediate_on_and_off(case):
+    """The same mixed solve with the 3-D transforms' intermediate in scaled
+    FP16 (TMA line passes) and in FP32 (cp.async passes, which cannot load
+    FP16): both within 1e-3 of the FP64 restatement, and different from each
+    other (the FP16 storage really runs); an FP32 plan reports it off."""
+    x64 = oracle.bmSensa(np.zeros(int(np.prod(case["n_u"]))), case["y"], case["ve"], case["C"], case["G"]["Gu"],
+                         case["G"]["Gut"], case["n_u"], 10, dtype=np.complex128)
+    r32, _ = _recon(case, "fp32")
+    assert not r32.plan.half_intermediate
+    out = {}
+    for buffers in (2, 0):
+        import monalisa_b200 as mb
+
+        Gu, Gut = mb.bmTraj2SparseMat(case["t"], case["ve"], case["N_u"], [1, 1, 1], "gauss", 3, [0.61, 10])
+        r = mb.SensaRecon(Gu, Gut, case["C"], case["n_u"], precision="mixed")
+        r.plan.variant = {"pass_buffers": buffers}
+        assert r.plan.half_intermediate == (buffers == 2)
+        out[buffers] = r.run_host(case["y"], case["ve"], nIter=1, nCGD=10)
+    e_on, e_off = rel(out[2], x64), rel(out[0], x64)
+    assert e_on <= 1e-3 and e_off <= 1e-3, (e_on, e_off)
+    assert rel(out[2], out[0]) > 0, "FP16 intermediate had no effect"
 
 
 def test_mixed_forward_model_vs_nudft(case):
