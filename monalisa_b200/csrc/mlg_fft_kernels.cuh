@@ -1137,12 +1137,13 @@ static int launch_pipe(const FftAxisPlan& a, const PassDesc& d, int Lp, int thre
   return MLG_OK;
 }
 
-// TMA pass (fft_pass_tma_kernel, NSLOT bundle buffers) for a plain pass
-// without occupancy masks: *launched stays false when the shape does not fit
-// the TMA boxes (the caller then takes the cp.async pipelined pass).  The
-// masked first inverse pass stays on cp.async: copying only its set rows
-// takes one small bulk copy per row, which measured slower (c2: 1.19 ms
-// against 0.69 ms) than per-thread copies.
+// TMA pass (fft_pass_tma_kernel, NSLOT bundle buffers) for a plain pass:
+// *launched stays false when the shape does not fit the TMA boxes (the
+// caller then takes the cp.async pipelined pass).  The masked first inverse
+// pass runs as MASKED (32-row chunk boxes loaded where the line masks have
+// occupied rows) when its line masks exist and a bundle's mask words fit one
+// slot; copying each occupied row by itself instead had measured slower than
+// the cp.async pass (c2: 1.19 against 0.69 ms).
 template <int N1, int N2, int DIR, int COLS, int NSLOT>
 static int launch_tma(const FftAxisPlan& a, const PassDesc& d, int Lp, cudaStream_t s, bool* launched) {
   constexpr int N = N1 * N2, NT = cta_threads(COLS);
@@ -1150,11 +1151,17 @@ static int launch_tma(const FftAxisPlan& a, const PassDesc& d, int Lp, cudaStrea
   // register budget of step C: shapes beyond it are not instantiated
   if constexpr (tma_step_c_iters<N1, N2, COLS, NT>() * N2 > 32) return MLG_OK;
   else {
-  if (d.in_mask || d.in_lo < 0 || d.in_len < 1 || d.in_lo + d.in_len > N || d.out_lo < 0 || d.out_len < 1 ||
+  if (d.in_lo < 0 || d.in_len < 1 || d.in_lo + d.in_len > N || d.out_lo < 0 || d.out_len < 1 ||
       d.out_lo + d.out_len > N || Lp * d.C != COLS)
     return MLG_OK;
   const bool ih = d.in_half != 0, oh = d.out_half != 0;
   if (ih && oh) return MLG_OK;
+  // masked: the first inverse pass over the whole stored line, with masks of
+  // N / 32 words per line for at most kTmaMaskWords words per bundle
+  const bool masked = d.in_mask != nullptr;
+  if (masked && (DIR < 0 || !d.in_lmask || N % 32 || ih || d.in_lo != 0 || d.in_len != N ||
+                 Lp * (N / 32) > kTmaMaskWords || d.lmask_words < N / 32))
+    return MLG_OK;
   if constexpr (N2 > NT / COLS) {  // FP16 input needs one step-A line per thread
     if (ih) return MLG_OK;
   }
@@ -1163,7 +1170,7 @@ static int launch_tma(const FftAxisPlan& a, const PassDesc& d, int Lp, cudaStrea
   t.L = Lp;
   t.gu = (d.dims[u] + Lp - 1) / Lp;
   t.nbundles = blocks_for(d, Lp);
-  t.in_chunks = (N + 255) / 256;
+  t.in_chunks = masked ? N / 32 : (N + 255) / 256;
   t.out_chunks = (d.out_len + 255) / 256;
   if (N % t.in_chunks || d.out_len % t.out_chunks) return MLG_OK;
   t.in_rows = N / t.in_chunks;
@@ -1174,6 +1181,11 @@ static int launch_tma(const FftAxisPlan& a, const PassDesc& d, int Lp, cudaStrea
   t.test_stall = tma_test_stall() ? 1 : 0;
   t.h_amax = d.h_amax;
   t.h_len = d.h_len;
+  if (masked) {
+    t.lmask = d.in_lmask;
+    t.lw = d.lmask_words;
+    t.du = d.dims[u];
+  }
   if ((ih || oh) && (!d.h_amax || (4 * d.C) % 16)) return MLG_OK;
   // shared-memory box starts on 128-byte boundaries
   const long long rowb_in = (long long)COLS * (ih ? 4 : 8), rowb_out = (long long)COLS * (oh ? 4 : 8);
@@ -1186,21 +1198,26 @@ static int launch_tma(const FftAxisPlan& a, const PassDesc& d, int Lp, cudaStrea
     return MLG_OK;
   // an FP16 bundle lands in the upper half of its buffer: 128-byte aligned
   if (ih && ((size_t)N * COLS * 4) % 128) return MLG_OK;
-  const size_t smem = (size_t)NSLOT * N * COLS * 8 + 2 * NSLOT * sizeof(uint64_t) + (size_t)N * 8 + 128;
+  const size_t smem = (size_t)NSLOT * N * COLS * 8 + 2 * NSLOT * sizeof(uint64_t) + (size_t)N * 8 + 128 +
+                      (masked ? (size_t)NSLOT * kTmaMaskWords * 4 : 0);
   if (smem > 200 * 1024) return MLG_OK;
   if (d.dry) {
     *launched = true;
     return MLG_OK;
   }
   auto kern = fft_pass_tma_kernel<N1, N2, DIR, COLS, NSLOT, false, false>;
-  const int vi = ih ? 1 : (oh ? 2 : 0);
+  const int vi = (ih ? 1 : (oh ? 2 : 0)) + (masked ? 3 : 0);
   if constexpr (N2 <= NT / COLS) {
     if (ih) kern = fft_pass_tma_kernel<N1, N2, DIR, COLS, NSLOT, true, false>;
   }
   if (oh) kern = fft_pass_tma_kernel<N1, N2, DIR, COLS, NSLOT, false, true>;
-  // per instantiation, FP16 variant and host thread
-  thread_local int per_sm[3] = {0, 0, 0}, sms = 0;
-  thread_local size_t per_sm_smem[3] = {0, 0, 0};
+  if constexpr (DIR > 0 && N % 32 == 0) {  // the masked first inverse pass
+    if (masked) kern = oh ? fft_pass_tma_kernel<N1, N2, DIR, COLS, NSLOT, false, true, true>
+                          : fft_pass_tma_kernel<N1, N2, DIR, COLS, NSLOT, false, false, true>;
+  }
+  // per instantiation, variant and host thread
+  thread_local int per_sm[6] = {0, 0, 0, 0, 0, 0}, sms = 0;
+  thread_local size_t per_sm_smem[6] = {0, 0, 0, 0, 0, 0};
   if (per_sm[vi] == 0 || per_sm_smem[vi] != smem) {
     MLG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(200 * 1024)));
     int dev = 0;

@@ -19,6 +19,16 @@
 // a bundle's transform it stores the bundle and, once the store has read the
 // buffer, loads the next bundle into it.
 //
+// MASKED (the first inverse pass of the masked adjoint, whose input grid
+// holds Gut's non-empty rows and stale values elsewhere): the load boxes are
+// 32-row chunks, and the producer loads only the chunks in which some line
+// of the bundle has an occupied cell -- its line-mask word for those 32 rows
+// is non-zero -- after copying the bundle's mask words into a per-slot
+// shared area; the transform threads read each row's occupancy bit there and
+// take zero for an unoccupied row (skipped chunks and stale cells alike).
+// The producer fetches the mask words before it waits for the slot, so their
+// latency overlaps that wait.
+//
 // Every wait is bounded (kTmaWaitNs of wall-clock time): a wait that runs out
 // sets *err, makes the CTA's other waits give up at once, and the CTA returns
 // after the copies it issued have finished.  No multicast form is used: each
@@ -32,6 +42,7 @@
 namespace mlg {
 
 constexpr unsigned long long kTmaWaitNs = 2000000000ull;  // 2 s per wait
+constexpr int kTmaMaskWords = 32;  // mask words per slot (lines x words per line)
 
 struct TmaPass {
   int L = 1;          // lines per bundle
@@ -49,6 +60,11 @@ struct TmaPass {
   // (half_store_scale(h_amax, h_len))
   const unsigned* h_amax = nullptr;
   int h_len = 1;
+  // MASKED: line masks (lw words per line; line = u index + du * v index;
+  // word w, bit j = occupancy of row 32 w + j)
+  const uint32_t* lmask = nullptr;
+  int lw = 0;
+  int du = 0;
   // test hook (MLG_TEST_WAIT_TIMEOUT=1): CTA 0 never loads its first bundle,
   // so its transform threads' bounded wait runs out and the timeout path runs
   int test_stall = 0;
@@ -170,8 +186,11 @@ constexpr int tma_step_c_iters() {
 // reads its rows from there (times hs), waits for every thread to have read,
 // then writes FP32 (one n2 per thread: N2 <= NT / COLS).  OUT_H: step C
 // writes the rows as FP16 (times hs) into the lower half, row k at k.
-template <int N1, int N2, int DIR, int COLS, int NT, bool IN_H = false, bool OUT_H = false>
-__device__ __forceinline__ void smem_fft_natural(float2* s, const float2* tws, float hs) {
+// MASKED: lbits = the thread's line's occupancy words; step A takes zero for
+// a row whose bit is clear.
+template <int N1, int N2, int DIR, int COLS, int NT, bool IN_H = false, bool OUT_H = false, bool MASKED = false>
+__device__ __forceinline__ void smem_fft_natural(float2* s, const float2* tws, float hs,
+                                                 const uint32_t* lbits = nullptr) {
   constexpr int G = NT / COLS;
   constexpr int KI = tma_step_c_iters<N1, N2, COLS, NT>();
   const int col = threadIdx.x % COLS, g = threadIdx.x / COLS;
@@ -210,7 +229,14 @@ __device__ __forceinline__ void smem_fft_natural(float2* s, const float2* tws, f
         float2* const p = sc + n2 * COLS;
         float2 r[N1];
 #pragma unroll
-        for (int n1 = 0; n1 < N1; ++n1) r[n1] = p[n1 * N2 * COLS];
+        for (int n1 = 0; n1 < N1; ++n1) {
+          if constexpr (MASKED) {
+            const int row = n1 * N2 + n2;
+            r[n1] = ((lbits[row >> 5] >> (row & 31)) & 1u) ? p[n1 * N2 * COLS] : make_float2(0.f, 0.f);
+          } else {
+            r[n1] = p[n1 * N2 * COLS];
+          }
+        }
         reg_fft<N1, DIR>(r);
         if (n2) {
 #pragma unroll
@@ -260,7 +286,7 @@ constexpr int tma_min_blocks() {
   return by_smem < 1 ? 1 : (by_smem > 3 ? 3 : by_smem);
 }
 
-template <int N1, int N2, int DIR, int COLS, int NSLOT, bool IN_H = false, bool OUT_H = false>
+template <int N1, int N2, int DIR, int COLS, int NSLOT, bool IN_H = false, bool OUT_H = false, bool MASKED = false>
 __global__ void __launch_bounds__(cta_threads(COLS) + 32, (tma_min_blocks<N1 * N2, COLS, NSLOT>()))
     fft_pass_tma_kernel(const __grid_constant__ CUtensorMap tin, const __grid_constant__ CUtensorMap tout, TmaPass a,
                         const float2* __restrict__ tw) {
@@ -273,6 +299,9 @@ __global__ void __launch_bounds__(cta_threads(COLS) + 32, (tma_min_blocks<N1 * N
   uint64_t* full = reinterpret_cast<uint64_t*>(base + NSLOT * kBuf);
   uint64_t* done = full + NSLOT;
   float2* tws = reinterpret_cast<float2*>(done + NSLOT);  // twiddle table, N values
+  uint32_t* masks = reinterpret_cast<uint32_t*>(tws + N);  // MASKED: NSLOT x kTmaMaskWords
+  constexpr int NW = (N + 31) / 32;                        // mask words per line
+  static_assert(!MASKED || (N % 32 == 0 && !IN_H), "masked passes: 32-row chunks of an FP32 input");
   __shared__ int abort_flag;
   const int tid = threadIdx.x;
   for (int i = tid; i < N; i += blockDim.x) tws[i] = __ldg(tw + i);
@@ -292,13 +321,41 @@ __global__ void __launch_bounds__(cta_threads(COLS) + 32, (tma_min_blocks<N1 * N
     if (tid != NT) return;
     // producer: one thread
     constexpr int kInElem = IN_H ? 4 : 8, kOutElem = OUT_H ? 4 : 8;  // bytes per complex value
+    // MASKED: the bundle's mask words (lines past the grid edge: zeros)
+    uint32_t mw[MASKED ? kTmaMaskWords : 1];
+    auto fetch_masks = [&](int b) {
+      if constexpr (MASKED) {
+        const int ui0 = (b % a.gu) * a.L, vi = b / a.gu;
+#pragma unroll
+        for (int i = 0; i < kTmaMaskWords; ++i) {
+          const int l = i / NW, w = i - (i / NW) * NW;
+          mw[i] = (l < a.L && ui0 + l < a.du)
+                      ? __ldg(a.lmask + ((long long)(ui0 + l) + (long long)a.du * vi) * a.lw + w)
+                      : 0u;
+        }
+      }
+    };
     auto load = [&](int slot, int b) {
       unsigned char* dst = base + slot * kBuf + (IN_H ? kBuf / 2 : 0);
-      mbar_arrive_expect_tx(full + slot, IN_H ? kBuf / 2 : kBuf);
       const int c1 = (b % a.gu) * a.L, c3 = b / a.gu;
-      for (int k = 0; k < a.in_chunks; ++k)
-        tma_load_4d(dst + (size_t)k * a.in_rows * COLS * kInElem, &tin, 0, c1, k * a.in_rows - a.in_lo, c3,
-                    full + slot);
+      if constexpr (MASKED) {
+        uint32_t any = 0;  // bit k: chunk k holds an occupied row of some line
+#pragma unroll
+        for (int i = 0; i < kTmaMaskWords; ++i) {
+          masks[slot * kTmaMaskWords + i] = mw[i];
+          if (mw[i]) any |= 1u << (i - (i / NW) * NW);
+        }
+        mbar_arrive_expect_tx(full + slot, (unsigned)__popc(any) * (unsigned)(a.in_rows * COLS * kInElem));
+        for (int k = 0; k < a.in_chunks; ++k)
+          if ((any >> k) & 1u)
+            tma_load_4d(dst + (size_t)k * a.in_rows * COLS * kInElem, &tin, 0, c1, k * a.in_rows - a.in_lo, c3,
+                        full + slot);
+      } else {
+        mbar_arrive_expect_tx(full + slot, IN_H ? kBuf / 2 : kBuf);
+        for (int k = 0; k < a.in_chunks; ++k)
+          tma_load_4d(dst + (size_t)k * a.in_rows * COLS * kInElem, &tin, 0, c1, k * a.in_rows - a.in_lo, c3,
+                      full + slot);
+      }
     };
     auto store = [&](int slot, int b) {
       const unsigned char* src = base + slot * kBuf + (size_t)a.out_lo * COLS * kOutElem;
@@ -311,6 +368,7 @@ __global__ void __launch_bounds__(cta_threads(COLS) + 32, (tma_min_blocks<N1 * N
     bool ok = true;
     for (int b = blockIdx.x; b < a.nbundles; b += G, ++it) {
       const int slot = it % NSLOT;
+      fetch_masks(b);  // in flight during the wait below
       if (it >= NSLOT) {  // the slot held bundle it - NSLOT: store it first
         if (!mbar_wait(done + slot, (unsigned)((it / NSLOT) - 1) & 1u, abort, a.err)) {
           ok = false;
@@ -350,7 +408,10 @@ __global__ void __launch_bounds__(cta_threads(COLS) + 32, (tma_min_blocks<N1 * N
     const int slot = it % NSLOT;
     const bool ok = mbar_wait(full + slot, (unsigned)(it / NSLOT) & 1u, abort, a.err);
     if (bar_transform_or<NT>(!ok)) return;  // all transform threads leave together
-    smem_fft_natural<N1, N2, DIR, COLS, NT, IN_H, OUT_H>(reinterpret_cast<float2*>(base + slot * kBuf), tws, hs);
+    const uint32_t* lbits = nullptr;
+    if constexpr (MASKED) lbits = masks + slot * kTmaMaskWords + ((tid % COLS) / (COLS / a.L)) * NW;
+    smem_fft_natural<N1, N2, DIR, COLS, NT, IN_H, OUT_H, MASKED>(reinterpret_cast<float2*>(base + slot * kBuf), tws,
+                                                                 hs, lbits);
     fence_proxy_async_smem();  // the transform's writes become visible to the store
     mbar_arrive(done + slot);
   }

@@ -301,7 +301,7 @@ int nakatsha_stage(mlg_plan_s* p, int stage, const float2* y, const float* HY, f
     a.out.rows = p->Nu_tot;
     a.long_only = fused_gut(p);
     a.nonempty_only = p->adjoint_mode == kAdjMasked;
-    a.records = p->gut_records != 0;
+    a.records = p->gut_records;
     a.seg_scratch = p->seg_scratch;
     if (half_b(p)) {
       MLG_CUDA(cudaMemsetAsync(p->mix_amax + 1, 0, sizeof(unsigned), s));

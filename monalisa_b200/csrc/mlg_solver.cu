@@ -546,8 +546,8 @@ extern "C" int mlg_plan_autotune(mlg_plan_t p, int reps, double* ms) {
 extern "C" int mlg_plan_set_variant(mlg_plan_t p, int pass_buffers, int gut_records) {
   using namespace mlg;
   MLG_CHECK(p, "NULL plan");
-  MLG_CHECK((pass_buffers == 0 || pass_buffers == 2 || pass_buffers == 3) && (gut_records == 0 || gut_records == 1),
-            "variants: pass_buffers 0, 2 or 3; gut_records 0 or 1");
+  MLG_CHECK((pass_buffers == 0 || pass_buffers == 2 || pass_buffers == 3) && gut_records >= 0 && gut_records <= 2,
+            "variants: pass_buffers 0, 2 or 3; gut_records 0, 1 or 2");
   MLG_CHECK(!gut_records || p->Gut_s.ord_rec, "this plan has no Gut row records (masked adjoint, even coil count)");
   if (p->pass_buffers != pass_buffers || p->gut_records != gut_records) {
     p->pass_buffers = pass_buffers;
@@ -568,8 +568,9 @@ extern "C" int mlg_plan_get_variant(mlg_plan_t p, int* pass_buffers, int* gut_re
 
 // Times the kernel variants of the plan's current adjoint strategy and keeps
 // the fastest: ms[0..2] = forward + adjoint with TMA passes over 2 / 3
-// buffers and with cp.async passes, ms[3..4] = adjoint with Gut from the
-// CSR / from row records (-1: not available).
+// buffers and with cp.async passes, ms[3..5] = adjoint with Gut from the
+// CSR / from row records / from row records two rows at a time (-1: not
+// available).
 extern "C" int mlg_plan_autotune_variants(mlg_plan_t p, int reps, double* ms) {
   using namespace mlg;
   MLG_CHECK(p && reps >= 1, "invalid argument");
@@ -598,7 +599,7 @@ extern "C" int mlg_plan_autotune_variants(mlg_plan_t p, int reps, double* ms) {
     return (double)v / reps;
   };
   const int buf0 = p->pass_buffers, rec0 = p->gut_records;
-  double t[5] = {-1.0, -1.0, -1.0, -1.0, -1.0};
+  double t[6] = {-1.0, -1.0, -1.0, -1.0, -1.0, -1.0};
   int best_buf = buf0, best_rec = rec0;
   if (tma_passes_enabled()) {
     const int opts[3] = {2, 3, 0};
@@ -614,18 +615,22 @@ extern "C" int mlg_plan_autotune_variants(mlg_plan_t p, int reps, double* ms) {
   }
   p->pass_buffers = best_buf;
   if (st == MLG_OK && p->Gut_s.ord_rec && p->adjoint_mode == 2) {
-    for (int v = 0; v <= 1 && st == MLG_OK; ++v) {
+    double best = 1e30;
+    for (int v = 0; v <= 2 && st == MLG_OK; ++v) {
       p->gut_records = v;
       t[3 + v] = time_it(false);
+      if (t[3 + v] < best) {
+        best = t[3 + v];
+        best_rec = v;
+      }
     }
-    best_rec = t[4] < t[3] ? 1 : 0;
   }
   p->pass_buffers = buf0;
   p->gut_records = rec0;
   cudaEventDestroy(a);
   cudaEventDestroy(b);
   if (ms)
-    for (int i = 0; i < 5; ++i) ms[i] = t[i];
+    for (int i = 0; i < 6; ++i) ms[i] = t[i];
   if (st != MLG_OK) return st;
   return mlg_plan_set_variant(p, best_buf, best_rec);
 }

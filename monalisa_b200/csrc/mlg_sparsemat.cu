@@ -306,7 +306,8 @@ struct MidRows {
 // a time, lane = (entry group eg, coil pair pi) for P <= 16 pairs, EG = 32 /
 // P groups; group eg takes entries eg, eg + EG, ... and the groups' sums are
 // added in group order (a fixed order: deterministic, but not the row's
-// stored order).
+// stored order).  AM: p.absmax is raised to the largest output component.
+template <bool AM>
 __device__ __forceinline__ void mid_rows_block(const SpmmParams& p, const int* __restrict__ rows,
                                                const uint2* __restrict__ bounds, int n_rows, int block,
                                                int nblocks) {
@@ -345,10 +346,10 @@ __device__ __forceinline__ void mid_rows_block(const SpmmParams& p, const int* _
         s = make_float4(__fmul_rn(s.x, p.out_scale), __fmul_rn(s.y, p.out_scale), __fmul_rn(s.z, p.out_scale),
                         __fmul_rn(s.w, p.out_scale));
       reinterpret_cast<float4*>(p.out.a)[(long long)__ldg(rows + i) * P + pi] = s;
-      amax = fmaxf(amax, abs_max4(s));
+      if constexpr (AM) amax = fmaxf(amax, abs_max4(s));
     }
   }
-  if (p.absmax) block_absmax(p.absmax, amax);  // every thread of the block reaches it
+  if constexpr (AM) block_absmax(p.absmax, amax);  // every thread of the block reaches it
 }
 
 // PPT coil pairs per thread: the row's bounds and each entry's column and
@@ -373,7 +374,12 @@ __global__ void __launch_bounds__(256, pair_min_blocks<PPT>()) spmm_pair_kernel(
                                                                                int n_rows, MidRows mid) {
   __shared__ double sh[32];
   if ((int)blockIdx.x < mid.blocks) {
-    if constexpr (CONTRACT && !OUT_H) mid_rows_block(p, mid.rows, mid.bounds, mid.n, blockIdx.x, mid.blocks);
+    if constexpr (CONTRACT && !OUT_H) {
+      if (p.absmax)
+        mid_rows_block<true>(p, mid.rows, mid.bounds, mid.n, blockIdx.x, mid.blocks);
+      else
+        mid_rows_block<false>(p, mid.rows, mid.bounds, mid.n, blockIdx.x, mid.blocks);
+    }
     return;
   }
   const int bid = (int)blockIdx.x - mid.blocks;
@@ -499,10 +505,22 @@ static void launch_pair(int ppt, bool out_h, bool contract, const SpmmParams& p,
 // blocks gather the mid rows a warp each, as there.  p.absmax (optional) is
 // raised to the largest output component.  Eight blocks per SM, as the pair
 // kernel.
-__global__ void __launch_bounds__(256, 8) spmm_rec_kernel(SpmmParams p, const uint4* __restrict__ rec, int n_rows,
-                                                          MidRows mid) {
+// U rows per iteration: the records of U (row, pair) items are loaded
+// before any of their gathers, so a thread has U rows' loads in flight (U = 2
+// at five blocks per SM, the registers of two records; the plan's variant
+// tuner picks U).  Items are still computed once each, by the same thread
+// arithmetic: the outputs do not depend on U.
+template <int U>
+constexpr int rec_min_blocks() {
+  return U == 1 ? 8 : 5;
+}
+
+template <bool HV, bool AM, int U>
+__global__ void __launch_bounds__(256, rec_min_blocks<U>()) spmm_rec_kernel(SpmmParams p,
+                                                                             const uint4* __restrict__ rec,
+                                                                             int n_rows, MidRows mid) {
   if ((int)blockIdx.x < mid.blocks) {
-    mid_rows_block(p, mid.rows, mid.bounds, mid.n, blockIdx.x, mid.blocks);
+    mid_rows_block<AM>(p, mid.rows, mid.bounds, mid.n, blockIdx.x, mid.blocks);
     return;
   }
   const int bid = (int)blockIdx.x - mid.blocks;
@@ -511,13 +529,9 @@ __global__ void __launch_bounds__(256, 8) spmm_rec_kernel(SpmmParams p, const ui
   const int nr = (int)min((long long)p.rows_per_block, (long long)n_rows - i0);
   const int total = nr * P;
   const bool scale = p.in_row_scale != nullptr;
-  const bool half_v = p.val_h != nullptr;  // FP16 matrix values: the inline FP32 values rounded alike
   const float4* in = reinterpret_cast<const float4*>(p.in.a);
   float amax = 0.f;
-  for (int it = threadIdx.x; it < total; it += blockDim.x) {
-    const int lr = it / P, pi = it - lr * P;
-    const uint4* rp = rec + (i0 + lr) * 2;
-    const uint4 h0 = __ldg(rp), h1 = __ldg(rp + 1);
+  auto row = [&](const uint4 h0, const uint4 h1, const int pi) {
     const long long r = (int)h0.x;
     const uint32_t n = h0.y;
     float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -531,7 +545,7 @@ __global__ void __launch_bounds__(256, 8) spmm_rec_kernel(SpmmParams p, const ui
       const uint32_t c0 = h0.z, c1 = h1.x, c2 = h1.z;
       float4 v0 = make_float4(0.f, 0.f, 0.f, 0.f), v1 = v0, v2 = v0;
       float m0 = __uint_as_float(h0.w), m1 = __uint_as_float(h1.y), m2 = __uint_as_float(h1.w);
-      if (half_v) {
+      if constexpr (HV) {  // FP16 matrix values: the inline FP32 values rounded alike
         m0 = __half2float(__float2half_rn(m0));
         m1 = __half2float(__float2half_rn(m1));
         m2 = __half2float(__float2half_rn(m2));
@@ -552,7 +566,7 @@ __global__ void __launch_bounds__(256, 8) spmm_rec_kernel(SpmmParams p, const ui
 #pragma unroll 4
       for (uint32_t k = b; k < b + n; ++k) {
         const int j = __ldg(p.col + k);
-        float m = val_at(p, k);
+        float m = HV ? __half2float(p.val_h[k]) : __ldg(p.val + k);
         const float4 v = __ldg(in + (long long)j * P + pi);
         if (scale) m = __fmul_rn(m, __ldg(p.in_row_scale + j));
         fma4(m, v);
@@ -562,9 +576,28 @@ __global__ void __launch_bounds__(256, 8) spmm_rec_kernel(SpmmParams p, const ui
       acc = make_float4(__fmul_rn(acc.x, p.out_scale), __fmul_rn(acc.y, p.out_scale), __fmul_rn(acc.z, p.out_scale),
                         __fmul_rn(acc.w, p.out_scale));
     reinterpret_cast<float4*>(p.out.a)[r * P + pi] = acc;
-    amax = fmaxf(amax, abs_max4(acc));
+    if constexpr (AM) amax = fmaxf(amax, abs_max4(acc));
+  };
+  for (int it0 = threadIdx.x; it0 < total; it0 += U * (int)blockDim.x) {
+    uint4 h0[U], h1[U];
+    int pis[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int it = it0 + u * (int)blockDim.x;
+      pis[u] = -1;
+      if (it < total) {
+        const int lr = it / P;
+        pis[u] = it - lr * P;
+        const uint4* rp = rec + (i0 + lr) * 2;
+        h0[u] = __ldg(rp);
+        h1[u] = __ldg(rp + 1);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+      if (pis[u] >= 0) row(h0[u], h1[u], pis[u]);
   }
-  if (p.absmax) block_absmax(p.absmax, amax);
+  if constexpr (AM) block_absmax(p.absmax, amax);
 }
 
 __global__ void rec_build_kernel(const int* __restrict__ rows, const uint2* __restrict__ bounds, int n,
@@ -590,12 +623,14 @@ __global__ void rec_build_kernel(const int* __restrict__ rows, const uint2* __re
   }
 }
 
-// MLG_GUT_REC=0 / 1 forces the CSR rows / the records in every product;
-// unset: SpmmArgs::records (the plan's variant) decides.
+// MLG_GUT_REC=0 / 1 / 2 forces the CSR rows / the records / the records two
+// rows at a time in every product; unset: SpmmArgs::records (the plan's
+// variant) decides.
 static int records_forced() {
   static const int v = [] {
     const char* e = std::getenv("MLG_GUT_REC");
-    return e ? (std::strcmp(e, "0") == 0 ? 0 : (std::strcmp(e, "1") == 0 ? 1 : -1)) : -1;
+    if (!e) return -1;
+    return std::strcmp(e, "0") == 0 ? 0 : std::strcmp(e, "1") == 0 ? 1 : std::strcmp(e, "2") == 0 ? 2 : -1;
   }();
   return v;
 }
@@ -710,10 +745,25 @@ int spmm(const SpmmArgs& a, cudaStream_t s) {
         mid.blocks = (mid.n + 15) / 16;
       }
       const int grid_pair = split ? (n_pair + p.rows_per_block - 1) / p.rows_per_block : grid_short;
-      const bool recs = records_forced() >= 0 ? records_forced() == 1 : a.records;
-      if (split && m.ord_rec && recs && grid_pair + mid.blocks > 0) {
-        spmm_rec_kernel<<<grid_pair + mid.blocks, 256, 0, s>>>(p, reinterpret_cast<const uint4*>(m.ord_rec), n_pair,
-                                                               mid);
+      const int recs = records_forced() >= 0 ? records_forced() : a.records;
+      if (split && m.ord_rec && recs > 0 && grid_pair + mid.blocks > 0) {
+        const uint4* rec = reinterpret_cast<const uint4*>(m.ord_rec);
+        const int g = grid_pair + mid.blocks;
+        if (recs >= 2) {
+          if (p.val_h)
+            p.absmax ? spmm_rec_kernel<true, true, 2><<<g, 256, 0, s>>>(p, rec, n_pair, mid)
+                     : spmm_rec_kernel<true, false, 2><<<g, 256, 0, s>>>(p, rec, n_pair, mid);
+          else
+            p.absmax ? spmm_rec_kernel<false, true, 2><<<g, 256, 0, s>>>(p, rec, n_pair, mid)
+                     : spmm_rec_kernel<false, false, 2><<<g, 256, 0, s>>>(p, rec, n_pair, mid);
+        } else {
+          if (p.val_h)
+            p.absmax ? spmm_rec_kernel<true, true, 1><<<g, 256, 0, s>>>(p, rec, n_pair, mid)
+                     : spmm_rec_kernel<true, false, 1><<<g, 256, 0, s>>>(p, rec, n_pair, mid);
+          else
+            p.absmax ? spmm_rec_kernel<false, true, 1><<<g, 256, 0, s>>>(p, rec, n_pair, mid)
+                     : spmm_rec_kernel<false, false, 1><<<g, 256, 0, s>>>(p, rec, n_pair, mid);
+        }
         MLG_LAUNCHED();
       } else if (grid_pair + mid.blocks > 0) {
         launch_pair(pair_ppt(a), oh, a.contract, p, ordered ? m.ord_rows : nullptr,
