@@ -369,14 +369,12 @@ int mlg_plan_autotune(mlg_plan_t p, int reps, double* ms);
  * with the TMA unit (a producer warp and that many bundle buffers per CTA:
  * 3 CTAs per SM with 2 buffers, 2 with 3, at 256-point lines of 16 coils),
  * 0 with per-thread cp.async copies; gut_records = 1 reads Gut's short rows
- * from 32-byte row records (masked adjoint, even coil count), 2 the same
- * with two rows' loads in flight per thread (five CTAs per SM instead of
- * eight), 0 from the CSR.  Defaults: 2 buffers, records where built.  Set
- * them before a chain is created over the plan.  mlg_plan_autotune_variants
- * times them for the plan's adjoint strategy and keeps the fastest: ms[6]
- * (may be NULL) = forward + adjoint with 2 / 3 buffers and with cp.async
- * passes, adjoint with CSR / record / two-row record Gut rows (-1: not
- * timed).  No counterpart in the reference (its kernels are CPU code). */
+ * from 32-byte row records (masked adjoint, even coil count), 0 from the
+ * CSR.  Defaults: 2 buffers, records where built.  Set them before a chain
+ * is created over the plan.  mlg_plan_autotune_variants times them for the
+ * plan's adjoint strategy and keeps the fastest: ms[5] (may be NULL) =
+ * forward + adjoint with 2 / 3 buffers and with cp.async passes, adjoint
+ * with CSR / record Gut rows (-1: not timed).  No counterpart in the reference (its kernels are CPU code). */
 int mlg_plan_set_variant(mlg_plan_t p, int pass_buffers, int gut_records);
 int mlg_plan_get_variant(mlg_plan_t p, int* pass_buffers, int* gut_records);
 int mlg_plan_autotune_variants(mlg_plan_t p, int reps, double* ms);

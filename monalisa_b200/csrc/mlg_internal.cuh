@@ -265,9 +265,8 @@ struct SpmmArgs {
   bool half_values = false;
   // Short rows of an ordered non-empty product from the matrix's row
   // records (ord_rec), when built (FP32 values, rounded to FP16 as read with
-  // half_values): 0 = the CSR rows, 1 = records, 2 = records with two rows'
-  // loads in flight per thread
-  int records = 0;
+  // half_values)
+  bool records = false;
   // Optional: raised (atomicMax on the bits) to the largest |re| or |im| of
   // the values written, before any FP16 rounding (device, non-negative float)
   unsigned* absmax = nullptr;

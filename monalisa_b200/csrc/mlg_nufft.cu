@@ -260,10 +260,9 @@ int shanna_stage(mlg_plan_s* p, int stage, const float2* x, bool x_per_coil, flo
   a.in.layout = Layout::kPointC64;
   a.in.a = p->grid;
   a.in.rows = p->Nu_tot;
-  if (p->mp_half) {  // M p of the mixed CG steps: scaled FP16, largest value recorded
+  if (p->mp_half) {  // M p of the mixed CG steps: scaled FP16 (the residual update records its maximum)
     a.out.layout = Layout::kPointF16;
     a.out.scale = p->kscale;
-    a.absmax = p->kabsmax;
   } else {
     a.out.layout = Layout::kPointC64;
   }
@@ -301,7 +300,7 @@ int nakatsha_stage(mlg_plan_s* p, int stage, const float2* y, const float* HY, f
     a.out.rows = p->Nu_tot;
     a.long_only = fused_gut(p);
     a.nonempty_only = p->adjoint_mode == kAdjMasked;
-    a.records = p->gut_records;
+    a.records = p->gut_records != 0;
     a.seg_scratch = p->seg_scratch;
     if (half_b(p)) {
       MLG_CUDA(cudaMemsetAsync(p->mix_amax + 1, 0, sizeof(unsigned), s));

@@ -70,8 +70,9 @@ struct mlg_plan_s {
   // MLG_PRECISION_FP32, _MIXED (the CG-SENSE solver then stores M p in
   // scaled FP16 and reads FP16 matrix values) or _FP16_VALUES; mixed_run is
   // set while a mixed solve runs, mp_half while its CG steps run (the forward
-  // product then writes Layout::kPointF16 with scale kscale[0..1] and raises
-  // *kabsmax, kscale + 2)
+  // product then writes Layout::kPointF16 with scale kscale[0..1]; the
+  // residual update that reads it raises *kabsmax, kscale + 2, for the next
+  // step's scale)
   int precision = 0;
   bool mixed_run = false;
   bool mp_half = false;

@@ -179,19 +179,36 @@ __global__ void cg_update_x_kernel(float2* __restrict__ x, const float2* __restr
   }
 }
 
-// res -= a Mp   (bmSensa.m:71); H: Mp in scaled FP16 (kscale = {s, 1/s})
+// res -= a Mp   (bmSensa.m:71); H: Mp in scaled FP16 (kscale = {s, 1/s}),
+// and the largest |component| of Mp is raised into *absmax (the next step's
+// scale; one atomic per block, none when the recorded value is as large)
 template <bool H>
 __global__ void cg_update_res_kernel(float2* __restrict__ res, const void* __restrict__ Mp, long long n,
-                                     const double* __restrict__ sc, const float* __restrict__ kscale) {
+                                     const double* __restrict__ sc, const float* __restrict__ kscale,
+                                     unsigned* __restrict__ absmax) {
   if (sc[S_DONE] != 0.0) return;
   const float a = (float)sc[S_A];
   const float s = H ? kscale[0] : 0.f, inv = H ? kscale[1] : 1.f;
+  float mx = 0.f;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     const float2 m = kld<H>(Mp, i, s, inv);
+    if (H) mx = fmaxf(mx, fmaxf(fabsf(m.x), fabsf(m.y)));
     float2 r = res[i];
     r.x = __fsub_rn(r.x, __fmul_rn(a, m.x));
     r.y = __fsub_rn(r.y, __fmul_rn(a, m.y));
     res[i] = r;
+  }
+  if constexpr (H) {  // every thread of the block reaches it (the early return above is block-uniform)
+    __shared__ float wm[kT / 32];
+    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = mx;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      float m = 0.f;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m = fmaxf(m, wm[w]);
+      const unsigned u = __float_as_uint(m);
+      if (u > *reinterpret_cast<volatile const unsigned*>(absmax)) atomicMax(absmax, u);
+    }
   }
 }
 
@@ -245,9 +262,9 @@ static int cg_step(mlg_plan_s* p, float2* x, double HX, double eps, cudaStream_t
   cg_update_x_kernel<<<grid1(p->nu_tot), kT, 0, s>>>(x, p->x_p, p->nu_tot, p->scalars);
   MLG_LAUNCHED();
   if (p->mp_half)
-    cg_update_res_kernel<true><<<grid1(nk), kT, 0, s>>>(p->k_res, p->k_Mp, nk, p->scalars, p->kscale);
+    cg_update_res_kernel<true><<<grid1(nk), kT, 0, s>>>(p->k_res, p->k_Mp, nk, p->scalars, p->kscale, p->kabsmax);
   else
-    cg_update_res_kernel<false><<<grid1(nk), kT, 0, s>>>(p->k_res, p->k_Mp, nk, p->scalars, nullptr);
+    cg_update_res_kernel<false><<<grid1(nk), kT, 0, s>>>(p->k_res, p->k_Mp, nk, p->scalars, nullptr, nullptr);
   MLG_LAUNCHED();
   MLG_TRY(nakatsha_run(p, p->k_res, p->HY, (float)(1.0 / HX), p->x_dagM, p->partial, &np, s));
   cg_beta_kernel<<<1, kT, 0, s>>>(p->partial, np, HX, eps, p->scalars);
@@ -546,8 +563,8 @@ extern "C" int mlg_plan_autotune(mlg_plan_t p, int reps, double* ms) {
 extern "C" int mlg_plan_set_variant(mlg_plan_t p, int pass_buffers, int gut_records) {
   using namespace mlg;
   MLG_CHECK(p, "NULL plan");
-  MLG_CHECK((pass_buffers == 0 || pass_buffers == 2 || pass_buffers == 3) && gut_records >= 0 && gut_records <= 2,
-            "variants: pass_buffers 0, 2 or 3; gut_records 0, 1 or 2");
+  MLG_CHECK((pass_buffers == 0 || pass_buffers == 2 || pass_buffers == 3) && (gut_records == 0 || gut_records == 1),
+            "variants: pass_buffers 0, 2 or 3; gut_records 0 or 1");
   MLG_CHECK(!gut_records || p->Gut_s.ord_rec, "this plan has no Gut row records (masked adjoint, even coil count)");
   if (p->pass_buffers != pass_buffers || p->gut_records != gut_records) {
     p->pass_buffers = pass_buffers;
@@ -568,9 +585,8 @@ extern "C" int mlg_plan_get_variant(mlg_plan_t p, int* pass_buffers, int* gut_re
 
 // Times the kernel variants of the plan's current adjoint strategy and keeps
 // the fastest: ms[0..2] = forward + adjoint with TMA passes over 2 / 3
-// buffers and with cp.async passes, ms[3..5] = adjoint with Gut from the
-// CSR / from row records / from row records two rows at a time (-1: not
-// available).
+// buffers and with cp.async passes, ms[3..4] = adjoint with Gut from the
+// CSR / from row records (-1: not available).
 extern "C" int mlg_plan_autotune_variants(mlg_plan_t p, int reps, double* ms) {
   using namespace mlg;
   MLG_CHECK(p && reps >= 1, "invalid argument");
@@ -599,7 +615,7 @@ extern "C" int mlg_plan_autotune_variants(mlg_plan_t p, int reps, double* ms) {
     return (double)v / reps;
   };
   const int buf0 = p->pass_buffers, rec0 = p->gut_records;
-  double t[6] = {-1.0, -1.0, -1.0, -1.0, -1.0, -1.0};
+  double t[5] = {-1.0, -1.0, -1.0, -1.0, -1.0};
   int best_buf = buf0, best_rec = rec0;
   if (tma_passes_enabled()) {
     const int opts[3] = {2, 3, 0};
@@ -616,7 +632,7 @@ extern "C" int mlg_plan_autotune_variants(mlg_plan_t p, int reps, double* ms) {
   p->pass_buffers = best_buf;
   if (st == MLG_OK && p->Gut_s.ord_rec && p->adjoint_mode == 2) {
     double best = 1e30;
-    for (int v = 0; v <= 2 && st == MLG_OK; ++v) {
+    for (int v = 0; v <= 1 && st == MLG_OK; ++v) {
       p->gut_records = v;
       t[3 + v] = time_it(false);
       if (t[3 + v] < best) {
@@ -630,7 +646,7 @@ extern "C" int mlg_plan_autotune_variants(mlg_plan_t p, int reps, double* ms) {
   cudaEventDestroy(a);
   cudaEventDestroy(b);
   if (ms)
-    for (int i = 0; i < 6; ++i) ms[i] = t[i];
+    for (int i = 0; i < 5; ++i) ms[i] = t[i];
   if (st != MLG_OK) return st;
   return mlg_plan_set_variant(p, best_buf, best_rec);
 }

@@ -505,20 +505,12 @@ static void launch_pair(int ppt, bool out_h, bool contract, const SpmmParams& p,
 // blocks gather the mid rows a warp each, as there.  p.absmax (optional) is
 // raised to the largest output component.  Eight blocks per SM, as the pair
 // kernel.
-// U rows per iteration: the records of U (row, pair) items are loaded
-// before any of their gathers, so a thread has U rows' loads in flight (U = 2
-// at five blocks per SM, the registers of two records; the plan's variant
-// tuner picks U).  Items are still computed once each, by the same thread
-// arithmetic: the outputs do not depend on U.
-template <int U>
-constexpr int rec_min_blocks() {
-  return U == 1 ? 8 : 5;
-}
-
-template <bool HV, bool AM, int U>
-__global__ void __launch_bounds__(256, rec_min_blocks<U>()) spmm_rec_kernel(SpmmParams p,
-                                                                             const uint4* __restrict__ rec,
-                                                                             int n_rows, MidRows mid) {
+// (Loading two rows' records before either row's gathers -- two rows in
+// flight per thread at five blocks per SM, the registers of two records --
+// measured slower on c2: 0.709 against 0.610 ms.)
+template <bool HV, bool AM>
+__global__ void __launch_bounds__(256, 8) spmm_rec_kernel(SpmmParams p, const uint4* __restrict__ rec, int n_rows,
+                                                          MidRows mid) {
   if ((int)blockIdx.x < mid.blocks) {
     mid_rows_block<AM>(p, mid.rows, mid.bounds, mid.n, blockIdx.x, mid.blocks);
     return;
@@ -578,24 +570,10 @@ __global__ void __launch_bounds__(256, rec_min_blocks<U>()) spmm_rec_kernel(Spmm
     reinterpret_cast<float4*>(p.out.a)[r * P + pi] = acc;
     if constexpr (AM) amax = fmaxf(amax, abs_max4(acc));
   };
-  for (int it0 = threadIdx.x; it0 < total; it0 += U * (int)blockDim.x) {
-    uint4 h0[U], h1[U];
-    int pis[U];
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const int it = it0 + u * (int)blockDim.x;
-      pis[u] = -1;
-      if (it < total) {
-        const int lr = it / P;
-        pis[u] = it - lr * P;
-        const uint4* rp = rec + (i0 + lr) * 2;
-        h0[u] = __ldg(rp);
-        h1[u] = __ldg(rp + 1);
-      }
-    }
-#pragma unroll
-    for (int u = 0; u < U; ++u)
-      if (pis[u] >= 0) row(h0[u], h1[u], pis[u]);
+  for (int it = threadIdx.x; it < total; it += blockDim.x) {
+    const int lr = it / P;
+    const uint4* rp = rec + (i0 + lr) * 2;
+    row(__ldg(rp), __ldg(rp + 1), it - lr * P);
   }
   if constexpr (AM) block_absmax(p.absmax, amax);
 }
@@ -623,14 +601,12 @@ __global__ void rec_build_kernel(const int* __restrict__ rows, const uint2* __re
   }
 }
 
-// MLG_GUT_REC=0 / 1 / 2 forces the CSR rows / the records / the records two
-// rows at a time in every product; unset: SpmmArgs::records (the plan's
-// variant) decides.
+// MLG_GUT_REC=0 / 1 forces the CSR rows / the records in every product;
+// unset: SpmmArgs::records (the plan's variant) decides.
 static int records_forced() {
   static const int v = [] {
     const char* e = std::getenv("MLG_GUT_REC");
-    if (!e) return -1;
-    return std::strcmp(e, "0") == 0 ? 0 : std::strcmp(e, "1") == 0 ? 1 : std::strcmp(e, "2") == 0 ? 2 : -1;
+    return e ? (std::strcmp(e, "0") == 0 ? 0 : (std::strcmp(e, "1") == 0 ? 1 : -1)) : -1;
   }();
   return v;
 }
@@ -745,25 +721,16 @@ int spmm(const SpmmArgs& a, cudaStream_t s) {
         mid.blocks = (mid.n + 15) / 16;
       }
       const int grid_pair = split ? (n_pair + p.rows_per_block - 1) / p.rows_per_block : grid_short;
-      const int recs = records_forced() >= 0 ? records_forced() : a.records;
-      if (split && m.ord_rec && recs > 0 && grid_pair + mid.blocks > 0) {
+      const bool recs = records_forced() >= 0 ? records_forced() == 1 : a.records;
+      if (split && m.ord_rec && recs && grid_pair + mid.blocks > 0) {
         const uint4* rec = reinterpret_cast<const uint4*>(m.ord_rec);
         const int g = grid_pair + mid.blocks;
-        if (recs >= 2) {
-          if (p.val_h)
-            p.absmax ? spmm_rec_kernel<true, true, 2><<<g, 256, 0, s>>>(p, rec, n_pair, mid)
-                     : spmm_rec_kernel<true, false, 2><<<g, 256, 0, s>>>(p, rec, n_pair, mid);
-          else
-            p.absmax ? spmm_rec_kernel<false, true, 2><<<g, 256, 0, s>>>(p, rec, n_pair, mid)
-                     : spmm_rec_kernel<false, false, 2><<<g, 256, 0, s>>>(p, rec, n_pair, mid);
-        } else {
-          if (p.val_h)
-            p.absmax ? spmm_rec_kernel<true, true, 1><<<g, 256, 0, s>>>(p, rec, n_pair, mid)
-                     : spmm_rec_kernel<true, false, 1><<<g, 256, 0, s>>>(p, rec, n_pair, mid);
-          else
-            p.absmax ? spmm_rec_kernel<false, true, 1><<<g, 256, 0, s>>>(p, rec, n_pair, mid)
-                     : spmm_rec_kernel<false, false, 1><<<g, 256, 0, s>>>(p, rec, n_pair, mid);
-        }
+        if (p.val_h)
+          p.absmax ? spmm_rec_kernel<true, true><<<g, 256, 0, s>>>(p, rec, n_pair, mid)
+                   : spmm_rec_kernel<true, false><<<g, 256, 0, s>>>(p, rec, n_pair, mid);
+        else
+          p.absmax ? spmm_rec_kernel<false, true><<<g, 256, 0, s>>>(p, rec, n_pair, mid)
+                   : spmm_rec_kernel<false, false><<<g, 256, 0, s>>>(p, rec, n_pair, mid);
         MLG_LAUNCHED();
       } else if (grid_pair + mid.blocks > 0) {
         launch_pair(pair_ppt(a), oh, a.contract, p, ordered ? m.ord_rows : nullptr,

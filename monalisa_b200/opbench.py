@@ -28,9 +28,8 @@ def main(argv=None):
     ap.add_argument("--precision", default="fp32", choices=["fp32", "mixed", "fp16_values"])
     ap.add_argument("--buffers", type=int, default=None, choices=[0, 2, 3],
                     help="line-FFT passes: TMA with 2 or 3 bundle buffers, or 0 (cp.async); default: the plan's")
-    ap.add_argument("--records", type=int, default=None, choices=[0, 1, 2],
-                    help="Gut rows from the CSR (0), row records (1) or row records two rows at a time (2); "
-                         "default: the plan's")
+    ap.add_argument("--records", type=int, default=None, choices=[0, 1],
+                    help="Gut rows from row records (1) or the CSR (0); default: the plan's")
     ap.add_argument("--op", default="nufft", choices=["nufft", "gridder"],
                     help="nufft: operator stages; gridder: the leight adjoint gridder on the samples")
     args = ap.parse_args(argv)

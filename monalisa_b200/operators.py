@@ -229,10 +229,9 @@ class NufftPlan:
         N.call("mlg_plan_autotune", self._h, int(reps), N.dptr(ms))
         out = {n: float(t) for n, t in zip(self.ADJOINT_MODES, ms) if t >= 0}
         if variants and self.nPt > 0:
-            mv = np.zeros(6)
+            mv = np.zeros(5)
             N.call("mlg_plan_autotune_variants", self._h, int(reps), N.dptr(mv))
-            names = ("passes_tma_2buf", "passes_tma_3buf", "passes_cp_async", "gut_csr", "gut_records",
-                     "gut_records_2row")
+            names = ("passes_tma_2buf", "passes_tma_3buf", "passes_cp_async", "gut_csr", "gut_records")
             out.update({n: float(t) for n, t in zip(names, mv) if t >= 0})
         return out
 
@@ -240,8 +239,7 @@ class NufftPlan:
     def variant(self) -> dict:
         """The plan's kernel variants: {'pass_buffers': 0 (cp.async passes),
         2 or 3 (TMA passes with that many bundle buffers), 'gut_records': 0 (CSR
-        rows), 1 (row records) or 2 (row records, two rows in flight per
-        thread)}."""
+        rows) or 1 (row records)}."""
         a, b = ctypes.c_int(), ctypes.c_int()
         N.call("mlg_plan_get_variant", self._h, ctypes.byref(a), ctypes.byref(b))
         return {"pass_buffers": a.value, "gut_records": b.value}

@@ -6,9 +6,8 @@ a child process (the switches are read once per process):
   (MLG_FFT_TMA=0): the arithmetic is the same, so forward and adjoint
   operators must agree bit for bit;
 * the Gut product over row records (cell, count and inline entries: two
-  dependent loads per row; one or two rows in flight per thread) against the
-  coil-pair kernel over the CSR (MLG_GUT_REC=0 / 1 / 2 forces each), in the
-  masked adjoint: bit for bit.  Shapes: 256-point lines x 16 coils
+  dependent loads per row) against the coil-pair kernel over the CSR
+  (MLG_GUT_REC=0 / 1 forces either), in the masked adjoint: bit for bit.  Shapes: 256-point lines x 16 coils
 (16-column bundles), 192-point radix-3 lines x 12 coils (24 columns: two
 lines per bundle), 2-D 512-point lines (two load boxes of 256 rows), 8 coils
 (two lines per bundle), and a bundle count that leaves the last CTAs with
@@ -72,16 +71,14 @@ def test_tma_passes_bit_identical_to_cp_async_passes(tmp_path):
 
 
 def test_gut_records_bit_identical_to_pair_kernel(tmp_path):
-    b = _run(tmp_path, 1, 0)
-    for level in (1, 2):  # records; records with two rows' loads in flight per thread
-        a = _run(tmp_path, 1, level)
-        for k in a.files:
-            assert np.array_equal(a[k], b[k]), (level, k)
+    a, b = _run(tmp_path, 1, 1), _run(tmp_path, 1, 0)
+    for k in a.files:
+        assert np.array_equal(a[k], b[k]), k
 
 
 def test_plan_variants_agree_and_the_tuner_picks_one():
-    """The per-plan kernel variants (TMA / cp.async passes, CSR / record /
-    two-row record Gut rows) in one process: the same outputs bit for bit in every
+    """The per-plan kernel variants (TMA / cp.async passes, CSR / record Gut
+    rows) in one process: the same outputs bit for bit in every
     combination; the variant tuner times them and keeps a valid one."""
     import torch
 
@@ -98,7 +95,7 @@ def test_plan_variants_agree_and_the_tuner_picks_one():
     x = torch.from_numpy((rng.standard_normal(n ** 3) + 1j * rng.standard_normal(n ** 3)).astype(np.complex64)).cuda()
     outs = []
     for bufs in (2, 3, 0):
-        for recs in (0, 1, 2):
+        for recs in (0, 1):
             plan.variant = {"pass_buffers": bufs, "gut_records": recs}
             y = plan.shanna(x)
             outs.append((y.cpu().numpy(), plan.nakatsha(y).cpu().numpy()))
@@ -107,7 +104,7 @@ def test_plan_variants_agree_and_the_tuner_picks_one():
     times = plan.autotune(2)
     assert {"passes_tma_2buf", "passes_tma_3buf", "passes_cp_async"} <= set(times)
     if plan.adjoint_mode == "masked":
-        assert {"gut_csr", "gut_records", "gut_records_2row"} <= set(times)
-    assert plan.variant["pass_buffers"] in (0, 2, 3) and plan.variant["gut_records"] in (0, 1, 2)
+        assert {"gut_csr", "gut_records"} <= set(times)
+    assert plan.variant["pass_buffers"] in (0, 2, 3) and plan.variant["gut_records"] in (0, 1)
     plan.status()
     plan.close()
