@@ -392,6 +392,7 @@ def run_gpu(args):
     # the other configurations of the benchmark, each timed with CUDA events
     extra = {}
     adjoint_c2 = rec.plan.adjoint_mode
+    variant_c2 = rec.plan.variant  # the headline plan closes before the JSON line
     if not args.no_extra:
         x_fp32 = x.clone()
         ref64 = _c4_references(w, Gu, Gut, rec, y, ve, x_fp32, dev)
@@ -420,7 +421,7 @@ def run_gpu(args):
         "config": _config(w, ws),
         "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
         "recon_rel_err_vs_phantom": round(err, 5), "setup_s": round(setup_s, 2),
-        "autotune": {"adjoint": adjoint_c2, "variant": rec.plan.variant,
+        "autotune": {"adjoint": adjoint_c2, "variant": variant_c2,
                      "ms": {k: round(v, 4) for k, v in (rec.tuning or {}).items()}},
         "vs_plain_gpu": plain,
         **extra,
