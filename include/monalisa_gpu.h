@@ -370,13 +370,19 @@ int mlg_plan_autotune(mlg_plan_t p, int reps, double* ms);
  * 3 CTAs per SM with 2 buffers, 2 with 3, at 256-point lines of 16 coils),
  * 0 with per-thread cp.async copies; gut_records = 1 reads Gut's short rows
  * from 32-byte row records (masked adjoint, even coil count), 0 from the
- * CSR.  Defaults: 2 buffers, records where built.  Set them before a chain
- * is created over the plan.  mlg_plan_autotune_variants times them for the
- * plan's adjoint strategy and keeps the fastest: ms[5] (may be NULL) =
- * forward + adjoint with 2 / 3 buffers and with cp.async passes, adjoint
- * with CSR / record Gut rows (-1: not timed).  No counterpart in the reference (its kernels are CPU code). */
-int mlg_plan_set_variant(mlg_plan_t p, int pass_buffers, int gut_records);
-int mlg_plan_get_variant(mlg_plan_t p, int* pass_buffers, int* gut_records);
+ * CSR; fwd_masked_store = 1 lets the last forward TMA pass store only the
+ * 32-row chunks of grid lines that hold cells Gu reads (the grid's other
+ * cells then keep stale values, which no operator reads; allowed when every
+ * Gu column is an occupied cell of Gut, checked at plan creation), 0 stores
+ * the whole grid.  Defaults: 2 buffers, records where built, masked stores
+ * where allowed.  Set them before a chain is created over the plan.
+ * mlg_plan_autotune_variants times them for the plan's adjoint strategy and
+ * keeps the fastest: ms[6] (may be NULL) = forward + adjoint with 2 / 3
+ * buffers and with cp.async passes, adjoint with CSR / record Gut rows,
+ * forward + adjoint storing the whole grid at the chosen buffer count (-1:
+ * not timed).  No counterpart in the reference (its kernels are CPU code). */
+int mlg_plan_set_variant(mlg_plan_t p, int pass_buffers, int gut_records, int fwd_masked_store);
+int mlg_plan_get_variant(mlg_plan_t p, int* pass_buffers, int* gut_records, int* fwd_masked_store);
 int mlg_plan_autotune_variants(mlg_plan_t p, int reps, double* ms);
 
 /* Precision of the plan's CG-SENSE solver (mlg_sensa_dev / mlg_sensa).

@@ -52,8 +52,8 @@ SIGNATURES = {
     "mlg_plan_set_adjoint": [c_vp, c_int],
     "mlg_plan_get_adjoint": [c_vp, P_i],
     "mlg_plan_autotune": [c_vp, c_int, P_d],
-    "mlg_plan_set_variant": [c_vp, c_int, c_int],
-    "mlg_plan_get_variant": [c_vp, P_i, P_i],
+    "mlg_plan_set_variant": [c_vp, c_int, c_int, c_int],
+    "mlg_plan_get_variant": [c_vp, P_i, P_i, P_i],
     "mlg_plan_autotune_variants": [c_vp, c_int, P_d],
     "mlg_plan_set_precision": [c_vp, c_int],
     "mlg_plan_get_precision": [c_vp, P_i],

@@ -82,6 +82,11 @@ struct PassDesc {
   // check only: MLG_OK when a kernel would run the pass with every field
   // above honoured, MLG_ERR_UNSUPPORTED otherwise; nothing is launched
   int dry = 0;
+  // optional, the last forward pass: line masks (the geometry of in_lmask,
+  // lmask_words words per line) of the output cells that will be read; a TMA
+  // pass then stores only the 32-row chunks that hold such a cell, other
+  // kernels store everything
+  const uint32_t* out_lmask = nullptr;
 };
 
 // The current device's wait flag (set by a pass whose bounded wait ran out),

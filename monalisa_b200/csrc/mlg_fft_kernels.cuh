@@ -1162,6 +1162,10 @@ static int launch_tma(const FftAxisPlan& a, const PassDesc& d, int Lp, cudaStrea
   if (masked && (DIR < 0 || !d.in_lmask || N % 32 || ih || d.in_lo != 0 || d.in_len != N ||
                  Lp * (N / 32) > kTmaMaskWords || d.lmask_words < N / 32))
     return MLG_OK;
+  // masked stores (optional: without them every chunk is stored): the last
+  // forward pass over the whole line, FP32 output, the same mask geometry
+  const bool mask_out = d.out_lmask != nullptr && DIR < 0 && N % 32 == 0 && !oh && !masked && d.out_lo == 0 &&
+                        d.out_len == N && Lp * (N / 32) <= kTmaMaskWords && d.lmask_words >= N / 32;
   if constexpr (N2 > NT / COLS) {  // FP16 input needs one step-A line per thread
     if (ih) return MLG_OK;
   }
@@ -1171,7 +1175,7 @@ static int launch_tma(const FftAxisPlan& a, const PassDesc& d, int Lp, cudaStrea
   t.gu = (d.dims[u] + Lp - 1) / Lp;
   t.nbundles = blocks_for(d, Lp);
   t.in_chunks = masked ? N / 32 : (N + 255) / 256;
-  t.out_chunks = (d.out_len + 255) / 256;
+  t.out_chunks = mask_out ? N / 32 : (d.out_len + 255) / 256;
   if (N % t.in_chunks || d.out_len % t.out_chunks) return MLG_OK;
   t.in_rows = N / t.in_chunks;
   t.out_rows = d.out_len / t.out_chunks;
@@ -1181,8 +1185,8 @@ static int launch_tma(const FftAxisPlan& a, const PassDesc& d, int Lp, cudaStrea
   t.test_stall = tma_test_stall() ? 1 : 0;
   t.h_amax = d.h_amax;
   t.h_len = d.h_len;
-  if (masked) {
-    t.lmask = d.in_lmask;
+  if (masked || mask_out) {
+    t.lmask = masked ? d.in_lmask : d.out_lmask;
     t.lw = d.lmask_words;
     t.du = d.dims[u];
   }
@@ -1199,14 +1203,14 @@ static int launch_tma(const FftAxisPlan& a, const PassDesc& d, int Lp, cudaStrea
   // an FP16 bundle lands in the upper half of its buffer: 128-byte aligned
   if (ih && ((size_t)N * COLS * 4) % 128) return MLG_OK;
   const size_t smem = (size_t)NSLOT * N * COLS * 8 + 2 * NSLOT * sizeof(uint64_t) + (size_t)N * 8 + 128 +
-                      (masked ? (size_t)NSLOT * kTmaMaskWords * 4 : 0);
+                      (masked || mask_out ? (size_t)NSLOT * kTmaMaskWords * 4 : 0);
   if (smem > 200 * 1024) return MLG_OK;
   if (d.dry) {
     *launched = true;
     return MLG_OK;
   }
   auto kern = fft_pass_tma_kernel<N1, N2, DIR, COLS, NSLOT, false, false>;
-  const int vi = (ih ? 1 : (oh ? 2 : 0)) + (masked ? 3 : 0);
+  const int vi = (ih ? 1 : (oh ? 2 : 0)) + (masked ? 3 : 0) + (mask_out ? 6 : 0);
   if constexpr (N2 <= NT / COLS) {
     if (ih) kern = fft_pass_tma_kernel<N1, N2, DIR, COLS, NSLOT, true, false>;
   }
@@ -1215,9 +1219,15 @@ static int launch_tma(const FftAxisPlan& a, const PassDesc& d, int Lp, cudaStrea
     if (masked) kern = oh ? fft_pass_tma_kernel<N1, N2, DIR, COLS, NSLOT, false, true, true>
                           : fft_pass_tma_kernel<N1, N2, DIR, COLS, NSLOT, false, false, true>;
   }
+  if constexpr (DIR < 0 && N % 32 == 0) {  // the last forward pass with masked stores
+    if (mask_out && !ih) kern = fft_pass_tma_kernel<N1, N2, DIR, COLS, NSLOT, false, false, false, true>;
+    if constexpr (N2 <= NT / COLS) {
+      if (mask_out && ih) kern = fft_pass_tma_kernel<N1, N2, DIR, COLS, NSLOT, true, false, false, true>;
+    }
+  }
   // per instantiation, variant and host thread
-  thread_local int per_sm[6] = {0, 0, 0, 0, 0, 0}, sms = 0;
-  thread_local size_t per_sm_smem[6] = {0, 0, 0, 0, 0, 0};
+  thread_local int per_sm[9] = {}, sms = 0;
+  thread_local size_t per_sm_smem[9] = {};
   if (per_sm[vi] == 0 || per_sm_smem[vi] != smem) {
     MLG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(200 * 1024)));
     int dev = 0;

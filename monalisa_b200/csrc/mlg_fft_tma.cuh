@@ -29,6 +29,12 @@
 // The producer fetches the mask words before it waits for the slot, so their
 // latency overlaps that wait.
 //
+// MASK_OUT (the last forward pass, whose output grid is read only at cells
+// Gut marks occupied): the store boxes are 32-row chunks, and the producer
+// stores only the chunks in which some line of the bundle has an occupied
+// cell (mask words kept in the slot's shared area since the bundle's load);
+// the other cells of the grid keep stale values, which no reader touches.
+//
 // Every wait is bounded (kTmaWaitNs of wall-clock time): a wait that runs out
 // sets *err, makes the CTA's other waits give up at once, and the CTA returns
 // after the copies it issued have finished.  No multicast form is used: each
@@ -286,7 +292,8 @@ constexpr int tma_min_blocks() {
   return by_smem < 1 ? 1 : (by_smem > 3 ? 3 : by_smem);
 }
 
-template <int N1, int N2, int DIR, int COLS, int NSLOT, bool IN_H = false, bool OUT_H = false, bool MASKED = false>
+template <int N1, int N2, int DIR, int COLS, int NSLOT, bool IN_H = false, bool OUT_H = false, bool MASKED = false,
+          bool MASK_OUT = false>
 __global__ void __launch_bounds__(cta_threads(COLS) + 32, (tma_min_blocks<N1 * N2, COLS, NSLOT>()))
     fft_pass_tma_kernel(const __grid_constant__ CUtensorMap tin, const __grid_constant__ CUtensorMap tout, TmaPass a,
                         const float2* __restrict__ tw) {
@@ -302,6 +309,8 @@ __global__ void __launch_bounds__(cta_threads(COLS) + 32, (tma_min_blocks<N1 * N
   uint32_t* masks = reinterpret_cast<uint32_t*>(tws + N);  // MASKED: NSLOT x kTmaMaskWords
   constexpr int NW = (N + 31) / 32;                        // mask words per line
   static_assert(!MASKED || (N % 32 == 0 && !IN_H), "masked passes: 32-row chunks of an FP32 input");
+  static_assert(!MASK_OUT || (N % 32 == 0 && !OUT_H && !MASKED), "masked stores: 32-row chunks of an FP32 output");
+  constexpr bool kMasks = MASKED || MASK_OUT;  // the producer fetches the bundles' mask words
   __shared__ int abort_flag;
   const int tid = threadIdx.x;
   for (int i = tid; i < N; i += blockDim.x) tws[i] = __ldg(tw + i);
@@ -322,9 +331,9 @@ __global__ void __launch_bounds__(cta_threads(COLS) + 32, (tma_min_blocks<N1 * N
     // producer: one thread
     constexpr int kInElem = IN_H ? 4 : 8, kOutElem = OUT_H ? 4 : 8;  // bytes per complex value
     // MASKED: the bundle's mask words (lines past the grid edge: zeros)
-    uint32_t mw[MASKED ? kTmaMaskWords : 1];
+    uint32_t mw[kMasks ? kTmaMaskWords : 1];
     auto fetch_masks = [&](int b) {
-      if constexpr (MASKED) {
+      if constexpr (kMasks) {
         const int ui0 = (b % a.gu) * a.L, vi = b / a.gu;
 #pragma unroll
         for (int i = 0; i < kTmaMaskWords; ++i) {
@@ -351,6 +360,10 @@ __global__ void __launch_bounds__(cta_threads(COLS) + 32, (tma_min_blocks<N1 * N
             tma_load_4d(dst + (size_t)k * a.in_rows * COLS * kInElem, &tin, 0, c1, k * a.in_rows - a.in_lo, c3,
                         full + slot);
       } else {
+        if constexpr (MASK_OUT) {
+#pragma unroll
+          for (int i = 0; i < kTmaMaskWords; ++i) masks[slot * kTmaMaskWords + i] = mw[i];
+        }
         mbar_arrive_expect_tx(full + slot, IN_H ? kBuf / 2 : kBuf);
         for (int k = 0; k < a.in_chunks; ++k)
           tma_load_4d(dst + (size_t)k * a.in_rows * COLS * kInElem, &tin, 0, c1, k * a.in_rows - a.in_lo, c3,
@@ -360,8 +373,15 @@ __global__ void __launch_bounds__(cta_threads(COLS) + 32, (tma_min_blocks<N1 * N
     auto store = [&](int slot, int b) {
       const unsigned char* src = base + slot * kBuf + (size_t)a.out_lo * COLS * kOutElem;
       const int c1 = (b % a.gu) * a.L, c3 = b / a.gu;
+      uint32_t keep = ~0u;  // MASK_OUT: bit k = chunk k holds an occupied row of some line
+      if constexpr (MASK_OUT) {
+        keep = 0;
+        for (int i = 0; i < kTmaMaskWords; ++i)
+          if (masks[slot * kTmaMaskWords + i]) keep |= 1u << (i - (i / NW) * NW);
+      }
       for (int k = 0; k < a.out_chunks; ++k)
-        tma_store_4d(&tout, 0, c1, k * a.out_rows, c3, src + (size_t)k * a.out_rows * COLS * kOutElem);
+        if ((keep >> k) & 1u)
+          tma_store_4d(&tout, 0, c1, k * a.out_rows, c3, src + (size_t)k * a.out_rows * COLS * kOutElem);
       bulk_commit();
     };
     int it = 0;

@@ -42,6 +42,16 @@ static void box_strides(const int e[3], int C, long long st[3]) {
   st[2] = (long long)C * e[0] * e[1];
 }
 
+// The last forward pass may store only the chunks of grid lines that hold
+// cells Gu reads (plan variant fwd_masked_store; the line masks of the
+// masked adjoint cover every Gu column when gu_covered).
+static void set_masked_store(const mlg_plan_s* p, PassDesc& pd) {
+  if (p->fwd_masked_store && p->gu_covered && p->line_mask) {
+    pd.out_lmask = p->line_mask;
+    pd.lmask_words = p->line_mask_words;
+  }
+}
+
 // Forward passes: x (image -> A), y (A -> B), z (B -> grid).  The last pass
 // of the transform writes the grid.  half (3-D): B in scaled FP16 -- the x
 // pass records max|A| in mix_amax[0], the y pass stores B times the power of
@@ -94,6 +104,7 @@ static int forward_pass(mlg_plan_s* p, int ax, const float2* x, bool x_per_coil,
     pd.out_lo = 0;
     pd.out_len = N[1];
     pd.out_half = half ? 1 : 0;
+    if (d == 2) set_masked_store(p, pd);
     return fft_pass(p->ax[1], PassMode::kPlain, pd, nullptr, s);
   }
   pd.dims[0] = N[0];
@@ -107,6 +118,7 @@ static int forward_pass(mlg_plan_s* p, int ax, const float2* x, bool x_per_coil,
   box_strides(eG, C, pd.out_stride);
   pd.out_lo = 0;
   pd.out_len = N[2];
+  set_masked_store(p, pd);
   return fft_pass(p->ax[2], PassMode::kPlain, pd, nullptr, s);
 }
 
@@ -417,6 +429,33 @@ __global__ void line_mask_kernel(const uint32_t* __restrict__ nz, int du, int dv
   }
 }
 
+// 1 in *miss when a Gu column (a grid cell Gu reads) is not an occupied cell
+// of Gut's occupancy bits.
+__global__ void cover_check_kernel(const int* __restrict__ col, long long nnz, const uint32_t* __restrict__ nz,
+                                   int* miss) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nnz; k += (long long)gridDim.x * blockDim.x) {
+    const int c = __ldg(col + k);
+    if (!((__ldg(nz + (c >> 5)) >> (c & 31)) & 1u)) *miss = 1;
+  }
+}
+
+// Whether the line masks cover every cell Gu reads (Gu and Gut of one
+// trajectory are transposes, so they do; matrices from elsewhere may not).
+static int check_gu_covered(mlg_plan_s* p, cudaStream_t s) {
+  p->gu_covered = false;
+  if (!p->line_mask || !p->Gu || !p->Gut_s.nz_mask || p->Gu_s.nnz == 0) return MLG_OK;
+  DevBuf<int> miss;
+  MLG_TRY(miss.alloc(1, s));
+  MLG_CUDA(cudaMemsetAsync(miss.p, 0, sizeof(int), s));
+  cover_check_kernel<<<ew_grid(p->Gu_s.nnz), kEwThreads, 0, s>>>(p->Gu_s.col, p->Gu_s.nnz, p->Gut_s.nz_mask, miss.p);
+  MLG_LAUNCHED();
+  int h = 1;
+  MLG_CUDA(cudaMemcpyAsync(&h, miss.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+  MLG_CUDA(cudaStreamSynchronize(s));
+  p->gu_covered = h == 0;
+  return MLG_OK;
+}
+
 // Geometry as inverse_pass sets it for axis imDim - 1 (2-D and 3-D; in 1-D
 // that pass is the fused x pass, which reads the occupancy mask itself).
 static int build_line_mask(mlg_plan_s* p, cudaStream_t s) {
@@ -571,6 +610,8 @@ static int plan_create_impl(int imDim, const int* N_u, const int* n_u, int nCh, 
   if (Gut && (nCh % 2) == 0 && nCh / 2 <= 16 && (st = csr_build_records(p->Gut_s, s)) != MLG_OK) return bail(st);
   p->gut_records = p->Gut_s.ord_rec ? 1 : 0;  // measured faster on c2 (0.607 vs 0.671 ms)
   if ((st = build_line_mask(p, s)) != MLG_OK) return bail(st);
+  if ((st = check_gu_covered(p, s)) != MLG_OK) return bail(st);
+  p->fwd_masked_store = p->gu_covered ? 1 : 0;
   p->adjoint_mode = adjoint_mode_valid(p, kAdjMasked) ? kAdjMasked : (imDim >= 2 ? kAdjFused : kAdjFullGrid);
   const size_t kbytes = sizeof(float2) * (size_t)nu * nCh;
   const size_t gbytes = sizeof(float2) * (size_t)Nu * nCh;

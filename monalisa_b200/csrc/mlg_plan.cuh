@@ -46,9 +46,14 @@ struct mlg_plan_s {
   // kernel variants chosen per plan (mlg_plan_autotune_variants): line-FFT
   // bundles moved by the TMA unit through 2 or 3 shared buffers per CTA
   // (pass_buffers = 2, 3) or by per-thread cp.async copies (0); Gut's short
-  // rows from row records (1, when built) or from the CSR (0)
+  // rows from row records (1, when built) or from the CSR (0); the last
+  // forward pass storing only the 32-row chunks that hold cells Gu reads
+  // (fwd_masked_store = 1; allowed when gu_covered: every Gu column is an
+  // occupied cell of the line masks, checked once at plan creation)
   int pass_buffers = 2;
   int gut_records = 0;
+  int fwd_masked_store = 0;
+  bool gu_covered = false;
   cudaStream_t stream = nullptr;  // internal non-blocking stream
   cudaEvent_t ev_in = nullptr, ev_out = nullptr;
   size_t bytes = 0;

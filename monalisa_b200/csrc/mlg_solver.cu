@@ -560,15 +560,19 @@ extern "C" int mlg_plan_autotune(mlg_plan_t p, int reps, double* ms) {
   return mlg_plan_set_adjoint(p, best);
 }
 
-extern "C" int mlg_plan_set_variant(mlg_plan_t p, int pass_buffers, int gut_records) {
+extern "C" int mlg_plan_set_variant(mlg_plan_t p, int pass_buffers, int gut_records, int fwd_masked_store) {
   using namespace mlg;
   MLG_CHECK(p, "NULL plan");
-  MLG_CHECK((pass_buffers == 0 || pass_buffers == 2 || pass_buffers == 3) && (gut_records == 0 || gut_records == 1),
-            "variants: pass_buffers 0, 2 or 3; gut_records 0 or 1");
+  MLG_CHECK((pass_buffers == 0 || pass_buffers == 2 || pass_buffers == 3) && (gut_records == 0 || gut_records == 1) &&
+                (fwd_masked_store == 0 || fwd_masked_store == 1),
+            "variants: pass_buffers 0, 2 or 3; gut_records 0 or 1; fwd_masked_store 0 or 1");
   MLG_CHECK(!gut_records || p->Gut_s.ord_rec, "this plan has no Gut row records (masked adjoint, even coil count)");
-  if (p->pass_buffers != pass_buffers || p->gut_records != gut_records) {
+  MLG_CHECK(!fwd_masked_store || p->gu_covered,
+            "this plan cannot mask its forward stores (no line masks, or a Gu column outside Gut's occupied cells)");
+  if (p->pass_buffers != pass_buffers || p->gut_records != gut_records || p->fwd_masked_store != fwd_masked_store) {
     p->pass_buffers = pass_buffers;
     p->gut_records = gut_records;
+    p->fwd_masked_store = fwd_masked_store;
     if (p->cg_graph) cudaGraphExecDestroy(p->cg_graph);  // captured with the old kernels
     p->cg_graph = nullptr;
     p->cg_graph_x = nullptr;
@@ -576,17 +580,20 @@ extern "C" int mlg_plan_set_variant(mlg_plan_t p, int pass_buffers, int gut_reco
   return MLG_OK;
 }
 
-extern "C" int mlg_plan_get_variant(mlg_plan_t p, int* pass_buffers, int* gut_records) {
-  MLG_CHECK(p && pass_buffers && gut_records, "NULL argument");
+extern "C" int mlg_plan_get_variant(mlg_plan_t p, int* pass_buffers, int* gut_records, int* fwd_masked_store) {
+  MLG_CHECK(p && pass_buffers && gut_records && fwd_masked_store, "NULL argument");
   *pass_buffers = p->pass_buffers;
   *gut_records = p->gut_records;
+  *fwd_masked_store = p->fwd_masked_store;
   return MLG_OK;
 }
 
 // Times the kernel variants of the plan's current adjoint strategy and keeps
 // the fastest: ms[0..2] = forward + adjoint with TMA passes over 2 / 3
-// buffers and with cp.async passes, ms[3..4] = adjoint with Gut from the
-// CSR / from row records (-1: not available).
+// buffers and with cp.async passes (masked forward stores where the plan
+// allows them), ms[3..4] = adjoint with Gut from the CSR / from row records,
+// ms[5] = forward + adjoint storing every chunk of the grid, at the chosen
+// buffer count (-1: not available).
 extern "C" int mlg_plan_autotune_variants(mlg_plan_t p, int reps, double* ms) {
   using namespace mlg;
   MLG_CHECK(p && reps >= 1, "invalid argument");
@@ -614,9 +621,11 @@ extern "C" int mlg_plan_autotune_variants(mlg_plan_t p, int reps, double* ms) {
     cudaEventElapsedTime(&v, a, b);
     return (double)v / reps;
   };
-  const int buf0 = p->pass_buffers, rec0 = p->gut_records;
-  double t[5] = {-1.0, -1.0, -1.0, -1.0, -1.0};
-  int best_buf = buf0, best_rec = rec0;
+  const int buf0 = p->pass_buffers, rec0 = p->gut_records, mask0 = p->fwd_masked_store;
+  double t[6] = {-1.0, -1.0, -1.0, -1.0, -1.0, -1.0};
+  int best_buf = buf0, best_rec = rec0, best_mask = mask0;
+  p->fwd_masked_store = p->gu_covered ? 1 : 0;
+  double best_fwd = -1.0;
   if (tma_passes_enabled()) {
     const int opts[3] = {2, 3, 0};
     double best = 1e30;
@@ -628,8 +637,16 @@ extern "C" int mlg_plan_autotune_variants(mlg_plan_t p, int reps, double* ms) {
         best_buf = opts[i];
       }
     }
+    best_fwd = best;
   }
   p->pass_buffers = best_buf;
+  best_mask = p->fwd_masked_store;
+  if (st == MLG_OK && p->gu_covered && best_buf >= 2 && best_fwd > 0.0) {
+    p->fwd_masked_store = 0;
+    t[5] = time_it(true);
+    best_mask = t[5] < best_fwd ? 0 : 1;
+  }
+  p->fwd_masked_store = best_mask;
   if (st == MLG_OK && p->Gut_s.ord_rec && p->adjoint_mode == 2) {
     double best = 1e30;
     for (int v = 0; v <= 1 && st == MLG_OK; ++v) {
@@ -643,12 +660,13 @@ extern "C" int mlg_plan_autotune_variants(mlg_plan_t p, int reps, double* ms) {
   }
   p->pass_buffers = buf0;
   p->gut_records = rec0;
+  p->fwd_masked_store = mask0;
   cudaEventDestroy(a);
   cudaEventDestroy(b);
   if (ms)
-    for (int i = 0; i < 5; ++i) ms[i] = t[i];
+    for (int i = 0; i < 6; ++i) ms[i] = t[i];
   if (st != MLG_OK) return st;
-  return mlg_plan_set_variant(p, best_buf, best_rec);
+  return mlg_plan_set_variant(p, best_buf, best_rec, best_mask);
 }
 
 extern "C" int mlg_plan_set_precision(mlg_plan_t p, int precision) {

@@ -28,6 +28,8 @@ def main(argv=None):
     ap.add_argument("--precision", default="fp32", choices=["fp32", "mixed", "fp16_values"])
     ap.add_argument("--buffers", type=int, default=None, choices=[0, 2, 3],
                     help="line-FFT passes: TMA with 2 or 3 bundle buffers, or 0 (cp.async); default: the plan's")
+    ap.add_argument("--masked-store", type=int, default=None, choices=[0, 1],
+                    help="last forward pass stores only grid chunks Gu reads (1) or the whole grid (0)")
     ap.add_argument("--records", type=int, default=None, choices=[0, 1],
                     help="Gut rows from row records (1) or the CSR (0); default: the plan's")
     ap.add_argument("--op", default="nufft", choices=["nufft", "gridder"],
@@ -65,6 +67,8 @@ def main(argv=None):
         rec.plan.variant = {"pass_buffers": args.buffers}
     if args.records is not None:
         rec.plan.variant = {"gut_records": args.records}
+    if args.masked_store is not None:
+        rec.plan.variant = {"fwd_masked_store": args.masked_store}
     x = torch.from_numpy(traj.ellipsoid_phantom([n] * 3, 5, 2)).cuda()
     for _ in range(args.reps):
         y = rec.plan.shanna(x)

@@ -229,9 +229,10 @@ class NufftPlan:
         N.call("mlg_plan_autotune", self._h, int(reps), N.dptr(ms))
         out = {n: float(t) for n, t in zip(self.ADJOINT_MODES, ms) if t >= 0}
         if variants and self.nPt > 0:
-            mv = np.zeros(5)
+            mv = np.zeros(6)
             N.call("mlg_plan_autotune_variants", self._h, int(reps), N.dptr(mv))
-            names = ("passes_tma_2buf", "passes_tma_3buf", "passes_cp_async", "gut_csr", "gut_records")
+            names = ("passes_tma_2buf", "passes_tma_3buf", "passes_cp_async", "gut_csr", "gut_records",
+                     "fwd_full_store")
             out.update({n: float(t) for n, t in zip(names, mv) if t >= 0})
         return out
 
@@ -239,16 +240,18 @@ class NufftPlan:
     def variant(self) -> dict:
         """The plan's kernel variants: {'pass_buffers': 0 (cp.async passes),
         2 or 3 (TMA passes with that many bundle buffers), 'gut_records': 0 (CSR
-        rows) or 1 (row records)}."""
-        a, b = ctypes.c_int(), ctypes.c_int()
-        N.call("mlg_plan_get_variant", self._h, ctypes.byref(a), ctypes.byref(b))
-        return {"pass_buffers": a.value, "gut_records": b.value}
+        rows) or 1 (row records), 'fwd_masked_store': 1 (the last forward pass
+        stores only the grid chunks holding cells Gu reads) or 0}."""
+        a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        N.call("mlg_plan_get_variant", self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c))
+        return {"pass_buffers": a.value, "gut_records": b.value, "fwd_masked_store": c.value}
 
     @variant.setter
     def variant(self, v: dict):
         cur = self.variant
         cur.update(v)
-        N.call("mlg_plan_set_variant", self._h, int(cur["pass_buffers"]), int(cur["gut_records"]))
+        N.call("mlg_plan_set_variant", self._h, int(cur["pass_buffers"]), int(cur["gut_records"]),
+               int(cur["fwd_masked_store"]))
 
     def status(self) -> None:
         """Synchronises the plan's stream; raises MonalisaError (timeout) when

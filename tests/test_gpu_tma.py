@@ -78,7 +78,7 @@ def test_gut_records_bit_identical_to_pair_kernel(tmp_path):
 
 def test_plan_variants_agree_and_the_tuner_picks_one():
     """The per-plan kernel variants (TMA / cp.async passes, CSR / record Gut
-    rows) in one process: the same outputs bit for bit in every
+    rows, whole / chunk-masked forward grid stores) in one process: the same outputs bit for bit in every
     combination; the variant tuner times them and keeps a valid one."""
     import torch
 
@@ -94,15 +94,19 @@ def test_plan_variants_agree_and_the_tuner_picks_one():
     rng = np.random.default_rng(2)
     x = torch.from_numpy((rng.standard_normal(n ** 3) + 1j * rng.standard_normal(n ** 3)).astype(np.complex64)).cuda()
     outs = []
+    assert plan.variant["fwd_masked_store"] == 1  # Gu and Gut of one trajectory: covered
     for bufs in (2, 3, 0):
         for recs in (0, 1):
-            plan.variant = {"pass_buffers": bufs, "gut_records": recs}
-            y = plan.shanna(x)
-            outs.append((y.cpu().numpy(), plan.nakatsha(y).cpu().numpy()))
+            for masked_store in (1, 0):
+                plan.variant = {"pass_buffers": bufs, "gut_records": recs, "fwd_masked_store": masked_store}
+                y = plan.shanna(x)
+                outs.append((y.cpu().numpy(), plan.nakatsha(y).cpu().numpy()))
     for o in outs[1:]:
         assert np.array_equal(o[0], outs[0][0]) and np.array_equal(o[1], outs[0][1])
     times = plan.autotune(2)
     assert {"passes_tma_2buf", "passes_tma_3buf", "passes_cp_async"} <= set(times)
+    if plan.variant["pass_buffers"] >= 2:
+        assert "fwd_full_store" in times
     if plan.adjoint_mode == "masked":
         assert {"gut_csr", "gut_records"} <= set(times)
     assert plan.variant["pass_buffers"] in (0, 2, 3) and plan.variant["gut_records"] in (0, 1)
