@@ -1203,7 +1203,7 @@ static int launch_tma(const FftAxisPlan& a, const PassDesc& d, int Lp, cudaStrea
   // an FP16 bundle lands in the upper half of its buffer: 128-byte aligned
   if (ih && ((size_t)N * COLS * 4) % 128) return MLG_OK;
   const size_t smem = (size_t)NSLOT * N * COLS * 8 + 2 * NSLOT * sizeof(uint64_t) + (size_t)N * 8 + 128 +
-                      (masked || mask_out ? (size_t)NSLOT * kTmaMaskWords * 4 : 0);
+                      (masked || mask_out ? (size_t)NSLOT * (kTmaMaskWords + 1) * 4 : 0);
   if (smem > 200 * 1024) return MLG_OK;
   if (d.dry) {
     *launched = true;

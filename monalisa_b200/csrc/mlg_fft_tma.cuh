@@ -35,6 +35,13 @@
 // cell (mask words kept in the slot's shared area since the bundle's load);
 // the other cells of the grid keep stale values, which no reader touches.
 //
+// Empty bundles (lines outside the occupied region: no chunk holds an
+// occupied cell): the producer publishes the bundle's chunk bits in the
+// slot's word `slot_any`; with MASK_OUT such a bundle is neither loaded nor
+// transformed (nothing of it is stored), with MASKED its input is all zero,
+// so the transform threads write zeros for its kept rows instead of
+// transforming it.
+//
 // Every wait is bounded (kTmaWaitNs of wall-clock time): a wait that runs out
 // sets *err, makes the CTA's other waits give up at once, and the CTA returns
 // after the copies it issued have finished.  No multicast form is used: each
@@ -307,6 +314,7 @@ __global__ void __launch_bounds__(cta_threads(COLS) + 32, (tma_min_blocks<N1 * N
   uint64_t* done = full + NSLOT;
   float2* tws = reinterpret_cast<float2*>(done + NSLOT);  // twiddle table, N values
   uint32_t* masks = reinterpret_cast<uint32_t*>(tws + N);  // MASKED: NSLOT x kTmaMaskWords
+  uint32_t* slot_any = masks + NSLOT * kTmaMaskWords;      // MASKED / MASK_OUT: chunk bits per slot
   constexpr int NW = (N + 31) / 32;                        // mask words per line
   static_assert(!MASKED || (N % 32 == 0 && !IN_H), "masked passes: 32-row chunks of an FP32 input");
   static_assert(!MASK_OUT || (N % 32 == 0 && !OUT_H && !MASKED), "masked stores: 32-row chunks of an FP32 output");
@@ -354,6 +362,7 @@ __global__ void __launch_bounds__(cta_threads(COLS) + 32, (tma_min_blocks<N1 * N
           masks[slot * kTmaMaskWords + i] = mw[i];
           if (mw[i]) any |= 1u << (i - (i / NW) * NW);
         }
+        slot_any[slot] = any;
         mbar_arrive_expect_tx(full + slot, (unsigned)__popc(any) * (unsigned)(a.in_rows * COLS * kInElem));
         for (int k = 0; k < a.in_chunks; ++k)
           if ((any >> k) & 1u)
@@ -361,8 +370,15 @@ __global__ void __launch_bounds__(cta_threads(COLS) + 32, (tma_min_blocks<N1 * N
                         full + slot);
       } else {
         if constexpr (MASK_OUT) {
+          uint32_t keep = 0;  // bit k: output chunk k holds an occupied row of some line
 #pragma unroll
-          for (int i = 0; i < kTmaMaskWords; ++i) masks[slot * kTmaMaskWords + i] = mw[i];
+          for (int i = 0; i < kTmaMaskWords; ++i)
+            if (mw[i]) keep |= 1u << (i - (i / NW) * NW);
+          slot_any[slot] = keep;
+          if (keep == 0) {  // nothing of this bundle is stored: no load, no transform
+            mbar_arrive(full + slot);
+            return;
+          }
         }
         mbar_arrive_expect_tx(full + slot, IN_H ? kBuf / 2 : kBuf);
         for (int k = 0; k < a.in_chunks; ++k)
@@ -374,11 +390,7 @@ __global__ void __launch_bounds__(cta_threads(COLS) + 32, (tma_min_blocks<N1 * N
       const unsigned char* src = base + slot * kBuf + (size_t)a.out_lo * COLS * kOutElem;
       const int c1 = (b % a.gu) * a.L, c3 = b / a.gu;
       uint32_t keep = ~0u;  // MASK_OUT: bit k = chunk k holds an occupied row of some line
-      if constexpr (MASK_OUT) {
-        keep = 0;
-        for (int i = 0; i < kTmaMaskWords; ++i)
-          if (masks[slot * kTmaMaskWords + i]) keep |= 1u << (i - (i / NW) * NW);
-      }
+      if constexpr (MASK_OUT) keep = slot_any[slot];
       for (int k = 0; k < a.out_chunks; ++k)
         if ((keep >> k) & 1u)
           tma_store_4d(&tout, 0, c1, k * a.out_rows, c3, src + (size_t)k * a.out_rows * COLS * kOutElem);
@@ -430,8 +442,20 @@ __global__ void __launch_bounds__(cta_threads(COLS) + 32, (tma_min_blocks<N1 * N
     if (bar_transform_or<NT>(!ok)) return;  // all transform threads leave together
     const uint32_t* lbits = nullptr;
     if constexpr (MASKED) lbits = masks + slot * kTmaMaskWords + ((tid % COLS) / (COLS / a.L)) * NW;
-    smem_fft_natural<N1, N2, DIR, COLS, NT, IN_H, OUT_H, MASKED>(reinterpret_cast<float2*>(base + slot * kBuf), tws,
-                                                                 hs, lbits);
+    // an empty bundle (uniform over the CTA: one slot word)
+    const bool empty = (MASKED || MASK_OUT) && slot_any[slot] == 0;
+    if (!empty) {
+      smem_fft_natural<N1, N2, DIR, COLS, NT, IN_H, OUT_H, MASKED>(reinterpret_cast<float2*>(base + slot * kBuf),
+                                                                   tws, hs, lbits);
+    } else if constexpr (MASKED) {  // all-zero input: its kept rows are zeros
+      const int col = tid % COLS;
+      for (int k = a.out_lo + tid / COLS; k < a.out_lo + a.out_rows * a.out_chunks; k += NT / COLS) {
+        if constexpr (OUT_H)
+          reinterpret_cast<__half2*>(base + slot * kBuf)[k * COLS + col] = __floats2half2_rn(0.f, 0.f);
+        else
+          reinterpret_cast<float2*>(base + slot * kBuf)[k * COLS + col] = make_float2(0.f, 0.f);
+      }
+    }
     fence_proxy_async_smem();  // the transform's writes become visible to the store
     mbar_arrive(done + slot);
   }
