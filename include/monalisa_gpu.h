@@ -388,14 +388,12 @@ int mlg_plan_autotune_variants(mlg_plan_t p, int reps, double* ms);
 /* Precision of the plan's CG-SENSE solver (mlg_sensa_dev / mlg_sensa).
  * MLG_PRECISION_FP32: FP32 data and matrix values, FP64 scalars (the
  * reference's single-precision arithmetic).  MLG_PRECISION_MIXED: FP16 matrix
- * values (copies of Gu/Gut made once), 16-bit storage of the forward product
- * M p inside the CG steps (FP16 times a power of two chosen per step from the
- * previous step's largest value; the first step keeps FP32), and, where the
- * plan's passes support it (mlg_plan_get_half_intermediate), 16-bit storage
- * of the 3-D transforms' intermediate inside the CG steps (FP16 times a power
- * of two bounding it from its input's largest value); an FP32 residual, FP32
- * sums and FFT arithmetic, FP64 scalars; the caller's y and x stay
- * complex64.  Mixed precision turns the fused-gather adjoint
+ * values (copies of Gu/Gut made once) and, where the plan's passes support
+ * it (mlg_plan_get_half_intermediate), 16-bit storage of the 3-D
+ * transforms' intermediate inside the CG steps (FP16 times a power of two
+ * bounding it from its input's largest value); FP32 k-space vectors (M p and
+ * the residual), FP32 sums and FFT arithmetic, FP64 scalars; the caller's y
+ * and x stay complex64.  Mixed precision turns the fused-gather adjoint
  * strategy off (it reads FP32 k-space).  The operator entry points
  * (mlg_shanna_dev, mlg_nakatsha_dev) of a mixed plan read the FP16 values
  * but keep their complex64 k-space buffers.  No reference counterpart. */
@@ -418,7 +416,7 @@ int mlg_plan_get_half_intermediate(mlg_plan_t p, int* on);
  * ms[3] Gu product, ms[4] Gut product, ms[5..7] inverse z, y, x FFT passes
  * (x pass fused with .* KFC_conj and the coil sum).  Passes a 2-D / 1-D
  * plan does not run read 0.  A mixed-precision plan's stages run as inside
- * its CG steps (FP16 M p, FP16 transform intermediate where
+ * its CG steps (the FP16 transform intermediate where
  * mlg_plan_get_half_intermediate says so).  Inputs are zeros.  Measurement
  * helper; no reference counterpart. */
 int mlg_plan_profile(mlg_plan_t p, int iters, double* ms);

@@ -223,10 +223,6 @@ enum class Layout : int {
   kPointSplit = 3, // float re[rows][nCh], im[...] (MATLAB point layout)
   kCoilReal = 4,   // float [nCh][rows]           (real, column layout)
   kPointReal = 5,  // float [rows][nCh]           (real, row layout)
-  // complex [rows][nCh] in FP16, scaled: __half2(v * scale[0]) saturated at
-  // +-65504, read back as __half2 * scale[1] (scale[0] a power of two); while
-  // scale[0] == 0 the buffer holds plain float2 [rows][nCh] instead
-  kPointF16 = 6,
 };
 
 struct Operand {
@@ -234,7 +230,6 @@ struct Operand {
   void* a = nullptr;        // float2* or float* (re)
   void* b = nullptr;        // im (split layouts)
   long long rows = 0;       // leading dimension for coil-major layouts
-  const float* scale = nullptr;  // kPointF16: device {store factor, load factor}
 };
 
 struct SpmmArgs {

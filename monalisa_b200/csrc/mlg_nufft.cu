@@ -256,7 +256,7 @@ bool half_intermediate_possible(mlg_plan_s* p) {
   return ok;
 }
 
-static bool half_b(mlg_plan_s* p) { return p->mp_half && p->mix_amax && half_intermediate_possible(p); }
+static bool half_b(mlg_plan_s* p) { return p->cg_half && p->mix_amax && half_intermediate_possible(p); }
 
 int shanna_stage(mlg_plan_s* p, int stage, const float2* x, bool x_per_coil, float2* y, const float* sqn_w,
                  double* partial, int* n_partial, cudaStream_t s) {
@@ -272,12 +272,7 @@ int shanna_stage(mlg_plan_s* p, int stage, const float2* x, bool x_per_coil, flo
   a.in.layout = Layout::kPointC64;
   a.in.a = p->grid;
   a.in.rows = p->Nu_tot;
-  if (p->mp_half) {  // M p of the mixed CG steps: scaled FP16 (the residual update records its maximum)
-    a.out.layout = Layout::kPointF16;
-    a.out.scale = p->kscale;
-  } else {
-    a.out.layout = Layout::kPointC64;
-  }
+  a.out.layout = Layout::kPointC64;
   a.half_values = p->precision != MLG_PRECISION_FP32;
   a.contract = true;  // operator-internal product: fused multiply-adds
   a.out.a = y;
@@ -498,7 +493,7 @@ static void plan_free(mlg_plan_s* p) {
   cudaFree(p->partial);
   cudaFree(p->seg_scratch);
   cudaFree(p->line_mask);
-  cudaFree(p->kscale);
+  cudaFree(p->mix_amax);
   cudaFree(p->scalars);
   cudaFree(p->x_p);
   cudaFree(p->x_dagM);

@@ -72,23 +72,18 @@ struct mlg_plan_s {
   // matrices) borrows that plan's KFC, KFCc, grid, bufA, bufB, FFT tables,
   // stream and events; both then run in the order of that one stream.
   bool borrowed = false;
-  // MLG_PRECISION_FP32, _MIXED (the CG-SENSE solver then stores M p in
-  // scaled FP16 and reads FP16 matrix values) or _FP16_VALUES; mixed_run is
-  // set while a mixed solve runs, mp_half while its CG steps run (the forward
-  // product then writes Layout::kPointF16 with scale kscale[0..1]; the
-  // residual update that reads it raises *kabsmax, kscale + 2, for the next
-  // step's scale)
+  // MLG_PRECISION_FP32, _MIXED (FP16 matrix values and, inside the CG
+  // steps, the FP16 transform intermediate) or _FP16_VALUES; mixed_run is set
+  // while a mixed solve runs, cg_half while its CG steps run
   int precision = 0;
   bool mixed_run = false;
-  bool mp_half = false;
-  float* kscale = nullptr;
-  unsigned* kabsmax = nullptr;
+  bool cg_half = false;
   // FP16 storage of bufB (the y / z pass intermediate of a 3-D transform)
-  // while mp_half is set, where every pass involved supports it: mix_amax[0]
+  // while cg_half is set, where every pass involved supports it: mix_amax[0]
   // = largest component of the forward x pass's output, mix_amax[1] = of the
-  // Gut product (device words kscale + 4, + 5), the bounds of the FP16
-  // scales; half_b_key / half_b_ok cache the dry-run check of the four passes
-  // per (pass_buffers, adjoint_mode)
+  // Gut product (two device words, allocated with the solver buffers), the
+  // bounds of the FP16 scales; half_b_key / half_b_ok cache the dry-run check
+  // of the four passes per (pass_buffers, adjoint_mode)
   unsigned* mix_amax = nullptr;
   int half_b_key = -1;
   bool half_b_ok = false;

@@ -77,35 +77,6 @@ __global__ void max_kernel(const float* __restrict__ v, int n, float* out) {
   if (threadIdx.x == 0) out[blockIdx.x] = sh[0];
 }
 
-// k-space work vectors: the residual is FP32 complex; M p (recomputed from p
-// every step, so its rounding does not accumulate) is FP32 or, in mixed
-// precision, scaled FP16 (Layout::kPointF16: __half2 * scale[1], or float2
-// while scale[0] == 0)
-template <bool H>
-__device__ __forceinline__ float2 kld(const void* v, long long i, float s, float inv) {
-  if (H && s != 0.f) {
-    const float2 h = __half22float2(reinterpret_cast<const __half2*>(v)[i]);
-    return make_float2(h.x * inv, h.y * inv);
-  }
-  return reinterpret_cast<const float2*>(v)[i];
-}
-
-// Scale of the next FP16 M p: the power of two that maps this step's largest
-// |component| just below 2^12 (16x headroom before saturation at 65504, the
-// smallest normal half 2^-26 of that maximum); absmax is reset.
-__global__ void f16_scale_kernel(unsigned* absmax, float* scale) {
-  const float m = __uint_as_float(*absmax);
-  float s = 1.f;
-  if (m > 0.f && isfinite(m)) {
-    int e = 0;
-    frexpf(m, &e);  // m < 2^e
-    s = ldexpf(1.f, max(-120, min(120, 12 - e)));
-  }
-  scale[0] = s;
-  scale[1] = 1.f / s;  // exact: a power of two
-  *absmax = 0u;
-}
-
 // res = y - Mx (k-space), optional partials of sum HY |res|^2; y is the
 // caller's FP32 data, Mx and res (FP32) the work vectors
 __global__ void residual_kernel(const float2* __restrict__ y, const float2* __restrict__ Mx, long long n, int nCh,
@@ -179,36 +150,20 @@ __global__ void cg_update_x_kernel(float2* __restrict__ x, const float2* __restr
   }
 }
 
-// res -= a Mp   (bmSensa.m:71); H: Mp in scaled FP16 (kscale = {s, 1/s}),
-// and the largest |component| of Mp is raised into *absmax (the next step's
-// scale; one atomic per block, none when the recorded value is as large)
-template <bool H>
-__global__ void cg_update_res_kernel(float2* __restrict__ res, const void* __restrict__ Mp, long long n,
-                                     const double* __restrict__ sc, const float* __restrict__ kscale,
-                                     unsigned* __restrict__ absmax) {
+// res -= a Mp   (bmSensa.m:71); the residual and M p are FP32 complex in
+// every precision (M p in scaled FP16 was measured: the store slowed the
+// latency-bound Gu gather by more than the halved k-space traffic saved, c2
+// mixed 97.3 against 95.6 ms, and raised the image error 1.06e-4 -> 1.33e-4)
+__global__ void cg_update_res_kernel(float2* __restrict__ res, const float2* __restrict__ Mp, long long n,
+                                     const double* __restrict__ sc) {
   if (sc[S_DONE] != 0.0) return;
   const float a = (float)sc[S_A];
-  const float s = H ? kscale[0] : 0.f, inv = H ? kscale[1] : 1.f;
-  float mx = 0.f;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-    const float2 m = kld<H>(Mp, i, s, inv);
-    if (H) mx = fmaxf(mx, fmaxf(fabsf(m.x), fabsf(m.y)));
+    const float2 m = Mp[i];
     float2 r = res[i];
     r.x = __fsub_rn(r.x, __fmul_rn(a, m.x));
     r.y = __fsub_rn(r.y, __fmul_rn(a, m.y));
     res[i] = r;
-  }
-  if constexpr (H) {  // every thread of the block reaches it (the early return above is block-uniform)
-    __shared__ float wm[kT / 32];
-    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-    if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = mx;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      float m = 0.f;
-      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m = fmaxf(m, wm[w]);
-      const unsigned u = __float_as_uint(m);
-      if (u > *reinterpret_cast<volatile const unsigned*>(absmax)) atomicMax(absmax, u);
-    }
   }
 }
 
@@ -236,17 +191,15 @@ static int ensure_solver_buffers(mlg_plan_s* p) {
   cudaFree(p->k_Mp);
   cudaFree(p->HY);
   const size_t ni = sizeof(float2) * (size_t)p->nu_tot, nk = sizeof(float2) * (size_t)p->nPt * p->nCh;
-  cudaFree(p->kscale);
-  p->kscale = nullptr;
+  cudaFree(p->mix_amax);
+  p->mix_amax = nullptr;
   if (cudaMalloc(&p->x_p, ni) != cudaSuccess || cudaMalloc(&p->x_dagM, ni) != cudaSuccess ||
       cudaMalloc(&p->k_res, nk) != cudaSuccess || cudaMalloc(&p->k_Mp, nk) != cudaSuccess ||
       cudaMalloc(&p->HY, sizeof(float) * (size_t)std::max(1, p->nPt)) != cudaSuccess ||
-      cudaMalloc(&p->kscale, 8 * sizeof(float)) != cudaSuccess) {
+      cudaMalloc(&p->mix_amax, 2 * sizeof(unsigned)) != cudaSuccess) {
     cudaGetLastError();
     return fail(MLG_ERR_OOM, "solver work buffers: device allocation failed");
   }
-  p->kabsmax = reinterpret_cast<unsigned*>(p->kscale + 2);
-  p->mix_amax = reinterpret_cast<unsigned*>(p->kscale + 4);
   p->solver_nPt = p->nPt;
   p->bytes += 2 * ni + 2 * nk + sizeof(float) * (size_t)p->nPt;
   return MLG_OK;
@@ -261,20 +214,13 @@ static int cg_step(mlg_plan_s* p, float2* x, double HX, double eps, cudaStream_t
   MLG_LAUNCHED();
   cg_update_x_kernel<<<grid1(p->nu_tot), kT, 0, s>>>(x, p->x_p, p->nu_tot, p->scalars);
   MLG_LAUNCHED();
-  if (p->mp_half)
-    cg_update_res_kernel<true><<<grid1(nk), kT, 0, s>>>(p->k_res, p->k_Mp, nk, p->scalars, p->kscale, p->kabsmax);
-  else
-    cg_update_res_kernel<false><<<grid1(nk), kT, 0, s>>>(p->k_res, p->k_Mp, nk, p->scalars, nullptr, nullptr);
+  cg_update_res_kernel<<<grid1(nk), kT, 0, s>>>(p->k_res, p->k_Mp, nk, p->scalars);
   MLG_LAUNCHED();
   MLG_TRY(nakatsha_run(p, p->k_res, p->HY, (float)(1.0 / HX), p->x_dagM, p->partial, &np, s));
   cg_beta_kernel<<<1, kT, 0, s>>>(p->partial, np, HX, eps, p->scalars);
   MLG_LAUNCHED();
   cg_update_p_kernel<<<grid1(p->nu_tot), kT, 0, s>>>(p->x_p, p->x_dagM, p->nu_tot, p->scalars);
   MLG_LAUNCHED();
-  if (p->mp_half) {  // the next step's FP16 scale, from this step's M p
-    f16_scale_kernel<<<1, 1, 0, s>>>(p->kabsmax, p->kscale);
-    MLG_LAUNCHED();
-  }
   return MLG_OK;
 }
 
@@ -289,7 +235,7 @@ int sensa_run(mlg_plan_s* p, const float2* y, const float* ve, float ve_max, int
   p->mixed_run = p->precision == MLG_PRECISION_MIXED;
   const int st = sensa_body(p, y, ve, ve_max, nIter, nCGD, x, residual, use_graph, s);
   p->mixed_run = false;
-  p->mp_half = false;
+  p->cg_half = false;
   return st;
 }
 
@@ -345,7 +291,7 @@ static int sensa_body(mlg_plan_s* p, const float2* y, const float* ve, float ve_
   for (int it = 0; it < nIter; ++it) {
     // res = y - M x; dagM = (1/HX) M*(HY res); sqn = HX |dagM|^2; p = dagM
     int np = 0;
-    p->mp_half = false;  // M x of the residual and of the monitoring stay FP32
+    p->cg_half = false;  // M x of the residual and of the monitoring: FP32 transforms
     MLG_TRY(shanna_run(p, x, false, p->k_Mp, nullptr, nullptr, nullptr, s));
     launch_residual(grid1(nk), y, p->k_Mp, nk, p->nCh, p->HY, p->k_res, nullptr, s);
     MLG_LAUNCHED();
@@ -353,10 +299,7 @@ static int sensa_body(mlg_plan_s* p, const float2* y, const float* ve, float ve_
     cg_init_kernel<<<1, kT, 0, s>>>(p->partial, np, HX, eps, p->scalars);
     MLG_LAUNCHED();
     MLG_CUDA(cudaMemcpyAsync(p->x_p, p->x_dagM, sizeof(float2) * (size_t)p->nu_tot, cudaMemcpyDeviceToDevice, s));
-    if (p->mixed_run) {  // the first CG step keeps M p in FP32 and measures it
-      MLG_CUDA(cudaMemsetAsync(p->kscale, 0, 4 * sizeof(float), s));
-      p->mp_half = true;
-    }
+    p->cg_half = p->mixed_run;  // the CG steps: FP16 transform intermediate where supported
     if (full > 0) MLG_TRY(ensure_graph());
     for (int i = 0; i < full; ++i) {
       if (use_graph) {
@@ -374,7 +317,7 @@ static int sensa_body(mlg_plan_s* p, const float2* y, const float* ve, float ve_
       MLG_LAUNCHED();
     }
     // monitoring: R = |y - Mx|^2_HY   (bmSensa.m:82-83)
-    p->mp_half = false;
+    p->cg_half = false;
     MLG_TRY(shanna_run(p, x, false, p->k_Mp, nullptr, nullptr, nullptr, s));
     const int g = grid1(nk);
     launch_residual(g, y, p->k_Mp, nk, p->nCh, p->HY, nullptr, p->partial, s);
@@ -464,14 +407,12 @@ extern "C" int mlg_plan_profile(mlg_plan_t p, int iters, double* ms) {
   const long long nk = (long long)p->nPt * p->nCh;
   MLG_CUDA(cudaMemsetAsync(p->x_p, 0, sizeof(float2) * (size_t)p->nu_tot, s));
   MLG_CUDA(cudaMemsetAsync(p->k_res, 0, sizeof(float2) * (size_t)nk, s));
-  // a mixed plan's stages as they run inside its CG steps: FP16 M p (scale
-  // 1) and, where supported, the FP16 transform intermediate (maxima zeroed)
-  static const float k_init[8] = {1.f, 1.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-  MLG_CUDA(cudaMemcpyAsync(p->kscale, k_init, sizeof(k_init), cudaMemcpyHostToDevice, s));
+  // a mixed plan's stages as they run inside its CG steps (the FP16
+  // transform intermediate, where supported)
   constexpr int S = kShannaStages + kNakatshaStages;
   cudaEvent_t ev[S + 1];
   for (int k = 0; k <= S; ++k) MLG_CUDA(cudaEventCreate(&ev[k]));
-  p->mp_half = p->precision == MLG_PRECISION_MIXED;  // reset below on every path
+  p->cg_half = p->precision == MLG_PRECISION_MIXED;  // reset below on every path
   double acc[S] = {0};
   int st = MLG_OK;
   for (int it = 0; it <= iters && st == MLG_OK; ++it) {
@@ -492,7 +433,7 @@ extern "C" int mlg_plan_profile(mlg_plan_t p, int iters, double* ms) {
       acc[k] += v;
     }
   }
-  p->mp_half = false;
+  p->cg_half = false;
   for (int k = 0; k <= S; ++k) cudaEventDestroy(ev[k]);
   for (int k = 0; k < S; ++k) ms[k] = acc[k] / iters;
   return st;

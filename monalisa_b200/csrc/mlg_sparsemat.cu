@@ -45,13 +45,6 @@ struct SpmmParams {
   unsigned* absmax;
 };
 
-// Scaled FP16 complex values (Layout::kPointF16): saturating conversion so
-// that a scale chosen from an earlier maximum never produces infinities.
-__device__ __forceinline__ __half2 to_f16_sat(float2 v, float s) {
-  constexpr float kMax = 65504.f;
-  return __floats2half2_rn(fminf(fmaxf(v.x * s, -kMax), kMax), fminf(fmaxf(v.y * s, -kMax), kMax));
-}
-
 __device__ __forceinline__ float abs_max4(float4 v) {
   return fmaxf(fmaxf(fabsf(v.x), fabsf(v.y)), fmaxf(fabsf(v.z), fabsf(v.w)));
 }
@@ -87,11 +80,6 @@ __device__ __forceinline__ float2 ld(const Operand& o, long long row, int c, int
     return make_float2(__ldg(reinterpret_cast<const float*>(o.a) + i), __ldg(reinterpret_cast<const float*>(o.b) + i));
   } else if constexpr (L == Layout::kPointReal) {
     return make_float2(__ldg(reinterpret_cast<const float*>(o.a) + row * nCh + c), 0.f);
-  } else if constexpr (L == Layout::kPointF16) {
-    if (__ldg(o.scale) == 0.f) return __ldg(reinterpret_cast<const float2*>(o.a) + row * nCh + c);
-    const float2 v = __half22float2(reinterpret_cast<const __half2*>(o.a)[row * nCh + c]);
-    const float inv = __ldg(o.scale + 1);
-    return make_float2(v.x * inv, v.y * inv);
   } else {
     return make_float2(__ldg(reinterpret_cast<const float*>(o.a) + (long long)c * o.rows + row), 0.f);
   }
@@ -113,12 +101,6 @@ __device__ __forceinline__ void st(const Operand& o, long long row, int c, int n
     reinterpret_cast<float*>(o.b)[i] = v.y;
   } else if constexpr (L == Layout::kPointReal) {
     reinterpret_cast<float*>(o.a)[row * nCh + c] = v.x;
-  } else if constexpr (L == Layout::kPointF16) {
-    const float s = __ldg(o.scale);
-    if (s == 0.f)
-      reinterpret_cast<float2*>(o.a)[row * nCh + c] = v;
-    else
-      reinterpret_cast<__half2*>(o.a)[row * nCh + c] = to_f16_sat(v, s);
   } else {
     reinterpret_cast<float*>(o.a)[(long long)c * o.rows + row] = v.x;
   }
@@ -279,20 +261,7 @@ __global__ void __launch_bounds__(256) spmm_seg_combine_kernel(SpmmParams p, con
 // CONTRACT (operators inside plans), with the row scale folded into the
 // matrix value and fused multiply-adds: 9 instead of 16 arithmetic and load
 // instructions per entry and coil pair.
-// A coil pair: two complex values; the input is FP32 (float4), the output
-// FP32 or, with OUT_H, scaled FP16 (Layout::kPointF16: 2 x __half2 = uint2).
-template <bool OUT_H>
-__device__ __forceinline__ void st_pair(void* base, long long i, float4 v, float s) {
-  if (OUT_H && s != 0.f) {
-    const __half2 a = to_f16_sat(make_float2(v.x, v.y), s), b = to_f16_sat(make_float2(v.z, v.w), s);
-    uint2 r;
-    r.x = *reinterpret_cast<const unsigned int*>(&a);
-    r.y = *reinterpret_cast<const unsigned int*>(&b);
-    reinterpret_cast<uint2*>(base)[i] = r;
-  } else {
-    reinterpret_cast<float4*>(base)[i] = v;
-  }
-}
+// A coil pair: two complex values (float4) in and out.
 
 struct MidRows {
   const int* rows = nullptr;
@@ -367,14 +336,14 @@ constexpr int pair_min_blocks() {
 // With mid_blocks > 0 (CONTRACT, FP32 output) the first mid_blocks blocks
 // gather the mid rows, a warp per row (mid_rows_block), and the others the
 // listed short rows: one launch, the long-running mid rows started first.
-template <bool OUT_H, bool CONTRACT, int PPT>
+template <bool CONTRACT, int PPT>
 __global__ void __launch_bounds__(256, pair_min_blocks<PPT>()) spmm_pair_kernel(SpmmParams p,
                                                                                const int* __restrict__ rows,
                                                                                const uint2* __restrict__ bounds,
                                                                                int n_rows, MidRows mid) {
   __shared__ double sh[32];
   if ((int)blockIdx.x < mid.blocks) {
-    if constexpr (CONTRACT && !OUT_H) {
+    if constexpr (CONTRACT) {
       if (p.absmax)
         mid_rows_block<true>(p, mid.rows, mid.bounds, mid.n, blockIdx.x, mid.blocks);
       else
@@ -388,7 +357,6 @@ __global__ void __launch_bounds__(256, pair_min_blocks<PPT>()) spmm_pair_kernel(
   const int nr = (int)min((long long)p.rows_per_block, (long long)n_rows - i0);
   const int total = nr * G;
   const bool scale = p.in_row_scale != nullptr;
-  const float so = OUT_H ? __ldg(p.out.scale) : 0.f;
   float amax = 0.f;
   double sq = 0.0;
   // item -> row, first coil pair and entry range (empty for rows the segment kernels own)
@@ -441,7 +409,7 @@ __global__ void __launch_bounds__(256, pair_min_blocks<PPT>()) spmm_pair_kernel(
     if (p.out_scale != 1.0f)
       acc = make_float4(__fmul_rn(acc.x, p.out_scale), __fmul_rn(acc.y, p.out_scale), __fmul_rn(acc.z, p.out_scale),
                         __fmul_rn(acc.w, p.out_scale));
-    st_pair<OUT_H>(p.out.a, r * P + pi, acc, so);
+    reinterpret_cast<float4*>(p.out.a)[r * P + pi] = acc;
     amax = fmaxf(amax, abs_max4(acc));
     if (p.partial)
       sq += w * ((double)acc.x * acc.x + (double)acc.y * acc.y + (double)acc.z * acc.z + (double)acc.w * acc.w);
@@ -469,26 +437,19 @@ __global__ void __launch_bounds__(256, pair_min_blocks<PPT>()) spmm_pair_kernel(
 }
 
 template <int PPT>
-static void launch_pair_ppt(bool out_h, bool contract, const SpmmParams& p, const int* rows, const uint2* rp,
-                            int nrows, int grid, const MidRows& mid, cudaStream_t s) {
+static void launch_pair_ppt(bool contract, const SpmmParams& p, const int* rows, const uint2* rp, int nrows, int grid,
+                            const MidRows& mid, cudaStream_t s) {
   grid += mid.blocks;
-  if (contract) {
-    if (out_h)
-      spmm_pair_kernel<true, true, PPT><<<grid, 256, 0, s>>>(p, rows, rp, nrows, mid);
-    else
-      spmm_pair_kernel<false, true, PPT><<<grid, 256, 0, s>>>(p, rows, rp, nrows, mid);
-  } else {
-    if (out_h)
-      spmm_pair_kernel<true, false, PPT><<<grid, 256, 0, s>>>(p, rows, rp, nrows, mid);
-    else
-      spmm_pair_kernel<false, false, PPT><<<grid, 256, 0, s>>>(p, rows, rp, nrows, mid);
-  }
+  if (contract)
+    spmm_pair_kernel<true, PPT><<<grid, 256, 0, s>>>(p, rows, rp, nrows, mid);
+  else
+    spmm_pair_kernel<false, PPT><<<grid, 256, 0, s>>>(p, rows, rp, nrows, mid);
 }
 
-static void launch_pair(int ppt, bool out_h, bool contract, const SpmmParams& p, const int* rows, const uint2* rp,
-                        int nrows, int grid, const MidRows& mid, cudaStream_t s) {
+static void launch_pair(int ppt, bool contract, const SpmmParams& p, const int* rows, const uint2* rp, int nrows,
+                        int grid, const MidRows& mid, cudaStream_t s) {
   (void)ppt;  // one pair per thread (pair_ppt)
-  launch_pair_ppt<1>(out_h, contract, p, rows, rp, nrows, grid, mid, s);
+  launch_pair_ppt<1>(contract, p, rows, rp, nrows, grid, mid, s);
 }
 
 // Short rows of an ordered non-empty product from their records (CONTRACT,
@@ -622,7 +583,7 @@ int csr_build_records(Csr& c, cudaStream_t s) {
 
 static bool use_pair_kernel(const SpmmArgs& a) {
   return a.in.layout == Layout::kPointC64 &&
-         (a.out.layout == Layout::kPointC64 || a.out.layout == Layout::kPointF16) && (a.nCh % 2) == 0 &&
+         a.out.layout == Layout::kPointC64 && (a.nCh % 2) == 0 &&
          !a.normalize;
 }
 
@@ -701,17 +662,14 @@ int spmm(const SpmmArgs& a, cudaStream_t s) {
   float3* sc3 = reinterpret_cast<float3*>(scratch);
   using L = Layout;
   const L i = a.in.layout, o = a.out.layout;
-  MLG_CHECK(i != L::kPointF16, "scaled FP16 is an output layout only");
-  MLG_CHECK(o != L::kPointF16 || a.out.scale, "scaled FP16 output needs its scale");
   if (use_pair_kernel(a)) {
-    const bool oh = o == L::kPointF16;
     if (grid_short > 0) {
       // the matrix's processing order when it covers the requested rows
       const bool ordered = m.ord_rows && m.ord_nonempty == a.nonempty_only;
       MLG_CHECK(ordered || !a.nonempty_only, "non-empty-row products need the ordered row list");
       // operator products over a split order: the short rows by the pair
       // kernel, the longer ones by a warp each
-      const bool split = ordered && a.contract && m.ord_short >= 0 && !oh && !a.partial && a.nCh / 2 <= 16;
+      const bool split = ordered && a.contract && m.ord_short >= 0 && !a.partial && a.nCh / 2 <= 16;
       const int n_pair = split ? m.ord_short : (int)nrows;
       MidRows mid;
       if (split && nrows > n_pair) {  // about two mid rows per warp
@@ -733,21 +691,18 @@ int spmm(const SpmmArgs& a, cudaStream_t s) {
                    : spmm_rec_kernel<false, false><<<g, 256, 0, s>>>(p, rec, n_pair, mid);
         MLG_LAUNCHED();
       } else if (grid_pair + mid.blocks > 0) {
-        launch_pair(pair_ppt(a), oh, a.contract, p, ordered ? m.ord_rows : nullptr,
+        launch_pair(pair_ppt(a), a.contract, p, ordered ? m.ord_rows : nullptr,
                     ordered ? m.ord_bounds : nullptr, n_pair, grid_pair, mid, s);
         MLG_LAUNCHED();
       }
     }
     // long rows (segment kernels) with the same element types
-    if (oh) return launch<L::kPointC64, L::kPointF16, false>(p, m, sc3, 0, s);
     return launch<L::kPointC64, L::kPointC64, false>(p, m, sc3, 0, s);
   }
   if (i == L::kCoilC64 && o == L::kPointC64) return launch<L::kCoilC64, L::kPointC64, false>(p, m, sc3, grid_short, s);
   if (i == L::kPointC64 && o == L::kCoilC64) return launch<L::kPointC64, L::kCoilC64, true>(p, m, sc3, grid_short, s);
   if (i == L::kPointC64 && o == L::kPointC64)
     return launch<L::kPointC64, L::kPointC64, false>(p, m, sc3, grid_short, s);
-  if (i == L::kPointC64 && o == L::kPointF16)
-    return launch<L::kPointC64, L::kPointF16, false>(p, m, sc3, grid_short, s);
   if (i == L::kCoilSplit && o == L::kCoilSplit)
     return launch<L::kCoilSplit, L::kCoilSplit, true>(p, m, sc3, grid_short, s);
   if (i == L::kPointSplit && o == L::kPointSplit)

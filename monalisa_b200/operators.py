@@ -203,11 +203,11 @@ class NufftPlan:
 
     @precision.setter
     def precision(self, name: str):
-        """'fp32', 'mixed' (FP16 matrix values, the CG-SENSE solver's forward
-        product M p and, where the plan supports it, the 3-D transforms'
-        intermediate stored in scaled FP16 inside the CG steps; FP32 residual,
-        sums and FFT arithmetic, FP64 scalars) or 'fp16_values' (FP16 matrix
-        values only)."""
+        """'fp32', 'mixed' (FP16 matrix values and, where the plan supports
+        it, the 3-D transforms' intermediate stored in scaled FP16 inside the
+        CG-SENSE solver's steps; FP32 k-space vectors, sums and FFT
+        arithmetic, FP64 scalars) or 'fp16_values' (FP16 matrix values
+        only)."""
         N.call("mlg_plan_set_precision", self._h, self.PRECISIONS.index(name))
 
     @property

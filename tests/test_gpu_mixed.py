@@ -1,5 +1,6 @@
-"""Mixed precision (FP16 matrix values, scaled-FP16 forward products M p, FP32 sums
-and FFTs, FP64 CG scalars) against the FP64 restatement of the same
+"""Mixed precision (FP16 matrix values, the 3-D transforms' intermediate in
+scaled FP16 inside the CG steps, FP32 k-space vectors, sums and FFT arithmetic,
+FP64 CG scalars) against the FP64 restatement of the same
 discrete reconstruction, and the forward model against the FP64 direct
 NUDFT.
 
@@ -90,8 +91,8 @@ def test_mixed_fp16_intermediate_on_and_off(case):
 
 def test_mixed_forward_model_vs_nudft(case):
     """Forward model error against the FP64 NUDFT at 2048 samples: FP32 and
-    mixed (FP16 values; the result rounded as the solver stores M p: FP16
-    times the power of two that puts its largest component below 2^12)."""
+    mixed (the plan's forward operator: FP16 matrix values; the CG steps'
+    FP16 transform intermediate is covered by the image test above)."""
     import monalisa_b200 as mb
     import torch
 
@@ -102,10 +103,6 @@ def test_mixed_forward_model_vs_nudft(case):
     for prec in ("fp32", "mixed"):
         r, _ = _recon(case, prec)
         y = r.plan.shanna(x)
-        if prec == "mixed":
-            yr = torch.view_as_real(y)
-            s = 2.0 ** (12 - np.frexp(float(yr.abs().max()))[1])
-            y = torch.view_as_complex(((yr * s).to(torch.float16).to(torch.float32) / s).contiguous())
         errs[prec] = rel(y.cpu().numpy()[idx], ref)
     assert errs["fp32"] < 0.2  # the gridding approximation (Gaussian window, nWin 3)
     assert errs["mixed"] - errs["fp32"] <= 1e-3, errs
