@@ -106,11 +106,12 @@ class ClockSampler:
 STAGES = ["fwd_x", "fwd_y", "fwd_z", "gu", "gut", "inv_z", "inv_y", "inv_x"]
 
 
-def algorithmic_bytes(w, Gu, Gut, nCh, adjoint):
+def algorithmic_bytes(w, Gu, Gut, nCh, adjoint, masked_store=False):
     """Bytes each stage must move at least, for one operator application
     (forward passes read the non-zero part only and write what the next pass
     needs; the inverse passes keep only the cropped lines).  The Gut / inverse
-    z split depends on the adjoint strategy the plan runs."""
+    z split depends on the adjoint strategy the plan runs; with masked
+    forward stores the forward z pass must write only the cells Gu reads."""
     nnz = Gu.nnz
     nPt = Gu.l_size
     N0, N1, N2 = (int(v) for v in w.N_u)
@@ -129,7 +130,7 @@ def algorithmic_bytes(w, Gu, Gut, nCh, adjoint):
     else:
         gut, inv_z = ysrc + 4 * (Nu + 1) + G, G + B
     return {
-        "fwd_x": nu * 8 + nu * nCh * 8 + A, "fwd_y": A + B, "fwd_z": B + G,
+        "fwd_x": nu * 8 + nu * nCh * 8 + A, "fwd_y": A + B, "fwd_z": B + (T if masked_store else G),
         "gu": nnz * 8 + 4 * (nPt + 1) + T + nPt * nCh * 8,
         "gut": gut, "inv_z": inv_z, "inv_y": B + A, "inv_x": A + nu * nCh * 8 + nu * 8,
     }
@@ -344,7 +345,8 @@ def run_gpu(args):
     # plan's stream) -> roofline of the dominant kernel of this library
     st = np.zeros(len(STAGES))
     N.call("mlg_plan_profile", rec.plan.handle, 5, N.dptr(st))
-    B = algorithmic_bytes(w, Gu, Gut, w.nCh, rec.plan.adjoint_mode)
+    B = algorithmic_bytes(w, Gu, Gut, w.nCh, rec.plan.adjoint_mode,
+                          masked_store=bool(rec.plan.variant["fwd_masked_store"]))
     peak, peak_kind = _peaks()
     stages = {}
     for i, nm in enumerate(STAGES):
