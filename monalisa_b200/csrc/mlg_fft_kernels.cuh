@@ -1253,6 +1253,78 @@ static inline int pipe_lines(const FftAxisPlan& a, int C) {
 
 // Pipelined kNakatshaOut pass; n_slots = the CTA count of the unpipelined
 // pass (the partial-sum slots the caller reduces), an upper bound of the grid.
+// TMA forward x pass (fft_pass_tma_kernel SHANNA): the bundle's KFC rows
+// are the loaded box (the coil-map volume seen as x lines, zero outside the
+// stored x range), the lines' image values one bulk copy; AMAX when the
+// pass records its largest output component.  *launched stays false when
+// the shape does not fit (the caller then takes the cp.async pass).
+template <int N1, int N2, int COLS, int NSLOT>
+static int launch_tma_shanna(const FftAxisPlan& a, const PassDesc& d, int Lp, cudaStream_t s, bool* launched) {
+  constexpr int N = N1 * N2, NT = cta_threads(COLS);
+  *launched = false;
+  if constexpr (tma_step_c_iters<N1, N2, COLS, NT>() * N2 > 32) return MLG_OK;
+  else {
+  // the image bulk copy: an even line length and a 16-byte aligned image
+  if (d.img_per_coil || !d.img || !d.kfc || d.in_lo < 0 || d.in_len < 2 || (d.in_len & 1) ||
+      d.in_lo + d.in_len > N || d.out_lo < 0 || d.out_len < 1 || d.out_lo + d.out_len > N || Lp * d.C != COLS ||
+      d.out_half || ((uintptr_t)d.img & 15))
+    return MLG_OK;
+  TmaPass t;
+  t.L = Lp;
+  t.gu = (d.dims[1] + Lp - 1) / Lp;
+  t.nbundles = blocks_for(d, Lp);
+  t.in_chunks = (N + 255) / 256;
+  t.out_chunks = (d.out_len + 255) / 256;
+  if (N % t.in_chunks || d.out_len % t.out_chunks) return MLG_OK;
+  t.in_rows = N / t.in_chunks;
+  t.out_rows = d.out_len / t.out_chunks;
+  t.in_lo = d.in_lo;
+  t.out_lo = d.out_lo;
+  t.err = d.wait_err;
+  t.test_stall = tma_test_stall() ? 1 : 0;
+  t.du = d.dims[1];
+  t.img = d.img;
+  t.img_len = d.in_len;
+  t.par0 = (d.coord_off[1] + d.coord_off[2]) & 1;
+  t.amax = d.out_absmax;
+  const long long rowb = (long long)COLS * 8;  // shared-memory box starts on 128-byte boundaries
+  if ((t.in_rows * rowb) % 128 || (t.out_lo * rowb) % 128 || (t.out_rows * rowb) % 128) return MLG_OK;
+  CUtensorMap tin, tout;
+  // KFC [pixel][coil] as a volume of x lines: lines along y (u) and z (v)
+  if (tma_line_map(&tin, d.kfc, d.C, d.dims[1], (long long)d.in_len * d.C, d.in_len, d.C, d.dims[2],
+                   (long long)d.in_len * d.dims[1] * d.C, Lp, t.in_rows) != MLG_OK ||
+      tma_line_map(&tout, d.out, d.C, d.dims[1], d.out_stride[1], d.out_len, d.out_stride[0], d.dims[2],
+                   d.out_stride[2], Lp, t.out_rows) != MLG_OK)
+    return MLG_OK;
+  const size_t smem = (size_t)NSLOT * N * COLS * 8 + 2 * NSLOT * sizeof(uint64_t) + (size_t)N * 8 + 128 +
+                      (size_t)NSLOT * Lp * d.in_len * 8;
+  if (smem > 200 * 1024) return MLG_OK;
+  if (d.dry) {
+    *launched = true;
+    return MLG_OK;
+  }
+  auto kern = d.out_absmax ? fft_pass_tma_kernel<N1, N2, -1, COLS, NSLOT, false, false, false, false, true, true>
+                           : fft_pass_tma_kernel<N1, N2, -1, COLS, NSLOT, false, false, false, false, true, false>;
+  const int vi = d.out_absmax ? 1 : 0;
+  thread_local int per_sm[2] = {}, sms = 0;
+  thread_local size_t per_sm_smem[2] = {};
+  if (per_sm[vi] == 0 || per_sm_smem[vi] != smem) {
+    MLG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(200 * 1024)));
+    int dev = 0;
+    MLG_CUDA(cudaGetDevice(&dev));
+    MLG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    MLG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[vi], kern, NT + 32, smem));
+    per_sm[vi] = std::max(1, per_sm[vi]);
+    per_sm_smem[vi] = smem;
+  }
+  const int grid = std::max(1, std::min(t.nbundles, per_sm[vi] * sms));
+  kern<<<grid, NT + 32, smem, s>>>(tin, tout, t, a.tw);
+  MLG_LAUNCHED();
+  *launched = true;
+  return MLG_OK;
+  }
+}
+
 template <int N1, int N2, int CP>
 static int launch_nak_pipe(const FftAxisPlan& a, const PassDesc& d, int n_slots, cudaStream_t s) {
   if (d.dry) return MLG_OK;
@@ -1316,6 +1388,27 @@ static int launch_pass(const FftAxisPlan& a, const PassDesc& d, int L, cudaStrea
   if constexpr (MODE == PassMode::kShannaIn && N1 > 0) {
     // one image shared by the coils, even C, 16 / 24 / 32 columns per bundle
     const int Lp = pipe_lines(a, d.C), cols = Lp * d.C;
+    if (!d.img_per_coil && (d.C & 1) == 0 && tma_passes_enabled() && d.tma_slots >= 2) {  // TMA x pass
+      bool done = false;
+      int st = MLG_OK;
+      const bool three = d.tma_slots >= 3;
+      switch (cols) {
+        case 16:
+          st = three ? launch_tma_shanna<N1, N2, 16, 3>(a, d, Lp, s, &done)
+                     : launch_tma_shanna<N1, N2, 16, 2>(a, d, Lp, s, &done);
+          break;
+        case 24:
+          st = three ? launch_tma_shanna<N1, N2, 24, 3>(a, d, Lp, s, &done)
+                     : launch_tma_shanna<N1, N2, 24, 2>(a, d, Lp, s, &done);
+          break;
+        case 32:
+          st = three ? launch_tma_shanna<N1, N2, 32, 3>(a, d, Lp, s, &done)
+                     : launch_tma_shanna<N1, N2, 32, 2>(a, d, Lp, s, &done);
+          break;
+        default: break;
+      }
+      if (st != MLG_OK || done) return st;
+    }
     if (!d.img_per_coil && (d.C & 1) == 0 && 2 * (size_t)a.N * cols * sizeof(float2) <= kFftSmemCap) {
       switch (cols) {
         case 16: return launch_shanna_pipe<N1, N2, 16>(a, d, Lp, s);

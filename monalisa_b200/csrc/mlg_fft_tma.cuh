@@ -42,6 +42,14 @@
 // so the transform threads write zeros for its kept rows instead of
 // transforming it.
 //
+// SHANNA (the forward x pass of the forward operator, bmShanna's x .* KFC,
+// zero-fill and first FFT): the loaded box holds the bundle's KFC rows (the
+// coil-map volume seen as x lines, zero outside the stored x range), one
+// untiled bulk copy brings the lines' image values onto the same barrier,
+// and the transform threads form x .* KFC with the centring modulation in
+// place before the transform.  AMAX: the transform threads record the
+// largest output component (the scale of the mixed-precision intermediate).
+//
 // Every wait is bounded (kTmaWaitNs of wall-clock time): a wait that runs out
 // sets *err, makes the CTA's other waits give up at once, and the CTA returns
 // after the copies it issued have finished.  No multicast form is used: each
@@ -77,7 +85,13 @@ struct TmaPass {
   // word w, bit j = occupancy of row 32 w + j)
   const uint32_t* lmask = nullptr;
   int lw = 0;
-  int du = 0;
+  int du = 0;  // (also SHANNA) lines along u in the volume
+  // SHANNA: the image (img_len pixels per x line, shared by the coils) and
+  // the parity of the modulation's line offset; AMAX: the recorded maximum
+  const float2* img = nullptr;
+  int img_len = 0;
+  int par0 = 0;
+  unsigned* amax = nullptr;
   // test hook (MLG_TEST_WAIT_TIMEOUT=1): CTA 0 never loads its first bundle,
   // so its transform threads' bounded wait runs out and the timeout path runs
   int test_stall = 0;
@@ -150,6 +164,15 @@ __device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, i
       : "memory");
 }
 
+// Untiled bulk copy global -> shared onto an mbarrier (no multicast); both
+// addresses 16-byte aligned, bytes a multiple of 16.
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(reinterpret_cast<uint64_t>(src)), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
 __device__ __forceinline__ void tma_store_4d(const CUtensorMap* map, int c0, int c1, int c2, int c3,
                                              const void* src) {
   asm volatile("cp.async.bulk.tensor.4d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3, %4}], [%5];" ::"l"(
@@ -201,9 +224,11 @@ constexpr int tma_step_c_iters() {
 // writes the rows as FP16 (times hs) into the lower half, row k at k.
 // MASKED: lbits = the thread's line's occupancy words; step A takes zero for
 // a row whose bit is clear.
-template <int N1, int N2, int DIR, int COLS, int NT, bool IN_H = false, bool OUT_H = false, bool MASKED = false>
+// AMAX: *amax is raised to the largest component the thread writes.
+template <int N1, int N2, int DIR, int COLS, int NT, bool IN_H = false, bool OUT_H = false, bool MASKED = false,
+          bool AMAX = false>
 __device__ __forceinline__ void smem_fft_natural(float2* s, const float2* tws, float hs,
-                                                 const uint32_t* lbits = nullptr) {
+                                                 const uint32_t* lbits = nullptr, float* amax = nullptr) {
   constexpr int G = NT / COLS;
   constexpr int KI = tma_step_c_iters<N1, N2, COLS, NT>();
   const int col = threadIdx.x % COLS, g = threadIdx.x / COLS;
@@ -287,6 +312,7 @@ __device__ __forceinline__ void smem_fft_natural(float2* s, const float2* tws, f
               __floats2half2_rn(r[i][k2].x * hs, r[i][k2].y * hs);
         else
           sc[(k1 + N1 * k2) * COLS] = r[i][k2];
+        if constexpr (AMAX) *amax = fmaxf(*amax, fmaxf(fabsf(r[i][k2].x), fabsf(r[i][k2].y)));
       }
     }
   }
@@ -300,7 +326,7 @@ constexpr int tma_min_blocks() {
 }
 
 template <int N1, int N2, int DIR, int COLS, int NSLOT, bool IN_H = false, bool OUT_H = false, bool MASKED = false,
-          bool MASK_OUT = false>
+          bool MASK_OUT = false, bool SHANNA = false, bool AMAX = false>
 __global__ void __launch_bounds__(cta_threads(COLS) + 32, (tma_min_blocks<N1 * N2, COLS, NSLOT>()))
     fft_pass_tma_kernel(const __grid_constant__ CUtensorMap tin, const __grid_constant__ CUtensorMap tout, TmaPass a,
                         const float2* __restrict__ tw) {
@@ -315,6 +341,8 @@ __global__ void __launch_bounds__(cta_threads(COLS) + 32, (tma_min_blocks<N1 * N
   float2* tws = reinterpret_cast<float2*>(done + NSLOT);  // twiddle table, N values
   uint32_t* masks = reinterpret_cast<uint32_t*>(tws + N);  // MASKED: NSLOT x kTmaMaskWords
   uint32_t* slot_any = masks + NSLOT * kTmaMaskWords;      // MASKED / MASK_OUT: chunk bits per slot
+  float2* xbuf = tws + N;  // SHANNA: NSLOT x (L x img_len) image values (in place of the masks)
+  static_assert(!SHANNA || (!MASKED && !MASK_OUT && !IN_H && DIR < 0), "the forward x pass");
   constexpr int NW = (N + 31) / 32;                        // mask words per line
   static_assert(!MASKED || (N % 32 == 0 && !IN_H), "masked passes: 32-row chunks of an FP32 input");
   static_assert(!MASK_OUT || (N % 32 == 0 && !OUT_H && !MASKED), "masked stores: 32-row chunks of an FP32 output");
@@ -368,6 +396,16 @@ __global__ void __launch_bounds__(cta_threads(COLS) + 32, (tma_min_blocks<N1 * N
           if ((any >> k) & 1u)
             tma_load_4d(dst + (size_t)k * a.in_rows * COLS * kInElem, &tin, 0, c1, k * a.in_rows - a.in_lo, c3,
                         full + slot);
+      } else if constexpr (SHANNA) {
+        const int u0 = (b % a.gu) * a.L, vi = b / a.gu;
+        const int nl = min(a.L, a.du - u0);  // lines inside the volume (>= 1)
+        const unsigned xbytes = (unsigned)(nl * a.img_len) * 8u;
+        mbar_arrive_expect_tx(full + slot, kBuf + xbytes);
+        for (int k = 0; k < a.in_chunks; ++k)
+          tma_load_4d(dst + (size_t)k * a.in_rows * COLS * kInElem, &tin, 0, c1, k * a.in_rows - a.in_lo, c3,
+                      full + slot);
+        bulk_load(xbuf + (size_t)slot * a.L * a.img_len, a.img + (long long)a.img_len * (u0 + (long long)a.du * vi),
+                  xbytes, full + slot);
       } else {
         if constexpr (MASK_OUT) {
           uint32_t keep = 0;  // bit k: output chunk k holds an occupied row of some line
@@ -435,6 +473,7 @@ __global__ void __launch_bounds__(cta_threads(COLS) + 32, (tma_min_blocks<N1 * N
     hs = half_store_scale(a.h_amax, a.h_len);
     if (IN_H) hs = 1.f / hs;  // a power of two: exact
   }
+  float amax = 0.f;  // AMAX: largest output component this thread wrote
   int it = 0;
   for (int b = blockIdx.x; b < a.nbundles; b += G, ++it) {
     const int slot = it % NSLOT;
@@ -442,11 +481,26 @@ __global__ void __launch_bounds__(cta_threads(COLS) + 32, (tma_min_blocks<N1 * N
     if (bar_transform_or<NT>(!ok)) return;  // all transform threads leave together
     const uint32_t* lbits = nullptr;
     if constexpr (MASKED) lbits = masks + slot * kTmaMaskWords + ((tid % COLS) / (COLS / a.L)) * NW;
+    if constexpr (SHANNA) {  // x .* KFC with the modulation, in place (bmShanna_MATLAB.m:28-54)
+      const int col = tid % COLS, l = col / (COLS / a.L);
+      const int ui = (b % a.gu) * a.L + l, vi = b / a.gu;
+      if (ui < a.du) {  // lines past the volume edge: zero KFC rows, no image values
+        const int par = (a.par0 + ui + vi) & 1;
+        const float2* const xl = xbuf + (size_t)slot * a.L * a.img_len + l * a.img_len - a.in_lo;
+        float2* const sb = reinterpret_cast<float2*>(base + slot * kBuf);
+        for (int n = a.in_lo + tid / COLS; n < a.in_lo + a.img_len; n += NT / COLS) {
+          float2 p = cmulf(xl[n], sb[n * COLS + col]);
+          if ((n + par) & 1) p = make_float2(-p.x, -p.y);
+          sb[n * COLS + col] = p;
+        }
+      }
+      bar_transform<NT>();  // every product written before the transform reads it
+    }
     // an empty bundle (uniform over the CTA: one slot word)
     const bool empty = (MASKED || MASK_OUT) && slot_any[slot] == 0;
     if (!empty) {
-      smem_fft_natural<N1, N2, DIR, COLS, NT, IN_H, OUT_H, MASKED>(reinterpret_cast<float2*>(base + slot * kBuf),
-                                                                   tws, hs, lbits);
+      smem_fft_natural<N1, N2, DIR, COLS, NT, IN_H, OUT_H, MASKED, AMAX>(
+          reinterpret_cast<float2*>(base + slot * kBuf), tws, hs, lbits, &amax);
     } else if constexpr (MASKED) {  // all-zero input: its kept rows are zeros
       const int col = tid % COLS;
       for (int k = a.out_lo + tid / COLS; k < a.out_lo + a.out_rows * a.out_chunks; k += NT / COLS) {
@@ -459,6 +513,7 @@ __global__ void __launch_bounds__(cta_threads(COLS) + 32, (tma_min_blocks<N1 * N
     fence_proxy_async_smem();  // the transform's writes become visible to the store
     mbar_arrive(done + slot);
   }
+  if constexpr (AMAX) warp_amax(a.amax, amax);  // the transform threads are whole warps
 }
 
 // Host: 4-D tensor map of a coil-fastest volume seen as the line boxes of
