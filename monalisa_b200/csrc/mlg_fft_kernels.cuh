@@ -53,6 +53,15 @@ __device__ __forceinline__ float2 cmulf(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 
+// The same product with every rounding explicit (no contraction into fused
+// multiply-adds, which the compiler may choose differently at each call
+// site): the forward x passes' x .* KFC, so that their TMA, pipelined and
+// unpipelined kernels agree bit for bit.
+__device__ __forceinline__ float2 cmulf_rn(float2 a, float2 b) {
+  return make_float2(__fsub_rn(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y)),
+                     __fadd_rn(__fmul_rn(a.x, b.y), __fmul_rn(a.y, b.x)));
+}
+
 // Scale of a pass intermediate stored in FP16: a power of two s with
 // bound * s < 2^15 (< 65504), bound = 2 len amax >= any component of a
 // length-len transform of values whose components are at most amax (the
@@ -264,7 +273,7 @@ __device__ __forceinline__ float2 load_elem(const PassDesc& d, const Lines& ln, 
     // axis x: pixel (n - in_lo, ui, vi) of the n_x * n_y * n_z image
     const long long m = (n - d.in_lo) + (long long)d.in_len * (ui + (long long)d.dims[1] * ln.vi);
     const float2 xv = __ldg(d.img + (d.img_per_coil ? m * d.C + c : m));
-    float2 v = cmulf(xv, __ldg(d.kfc + m * d.C + c));
+    float2 v = cmulf_rn(xv, __ldg(d.kfc + m * d.C + c));
     if ((n + d.coord_off[1] + ui + d.coord_off[2] + ln.vi) & 1) v = make_float2(-v.x, -v.y);
     return v;
   } else {
@@ -928,7 +937,7 @@ __global__ void __launch_bounds__(cta_threads(COLS), pipe_min_blocks(N1 * N2, CO
         if (n >= in_lo && n < in_hi) {
           const float4 k = cur[n * CV + vc];
           const float2 a = xl[n];
-          float2 p0 = cmulf(a, make_float2(k.x, k.y)), p1 = cmulf(a, make_float2(k.z, k.w));
+          float2 p0 = cmulf_rn(a, make_float2(k.x, k.y)), p1 = cmulf_rn(a, make_float2(k.z, k.w));
           if ((n + par) & 1) {
             p0 = make_float2(-p0.x, -p0.y);
             p1 = make_float2(-p1.x, -p1.y);

@@ -489,7 +489,7 @@ __global__ void __launch_bounds__(cta_threads(COLS) + 32, (tma_min_blocks<N1 * N
         const float2* const xl = xbuf + (size_t)slot * a.L * a.img_len + l * a.img_len - a.in_lo;
         float2* const sb = reinterpret_cast<float2*>(base + slot * kBuf);
         for (int n = a.in_lo + tid / COLS; n < a.in_lo + a.img_len; n += NT / COLS) {
-          float2 p = cmulf(xl[n], sb[n * COLS + col]);
+          float2 p = cmulf_rn(xl[n], sb[n * COLS + col]);
           if ((n + par) & 1) p = make_float2(-p.x, -p.y);
           sb[n * COLS + col] = p;
         }
