@@ -566,9 +566,15 @@ __global__ void __launch_bounds__(MAXT) fft_pass_kernel(PassDesc d, int L, int r
   // X[k] sits at position (k % n1s) * n2s + k / n1s
   if constexpr (MODE == PassMode::kNakatshaOut) {
     __shared__ double red[MAXT / 32];
-    // group of gc lanes per output pixel, lanes over coils, fixed-order tree
+    // group of gc lanes per output pixel, lanes over coils, fixed-order tree;
+    // with a power-of-two number of coil pairs, a lane per pair summed as the
+    // pipelined and TMA inverse x passes sum (nak_pair_term, then the tree)
+    const bool pairs = (C & 1) == 0 && ((C / 2) & (C / 2 - 1)) == 0 && C / 2 <= 32;
     int gc = 1;
-    while (gc < C && gc < 32) gc <<= 1;
+    if (pairs)
+      gc = C / 2;
+    else
+      while (gc < C && gc < 32) gc <<= 1;
     const int groups = blockDim.x / gc;
     const int lane = threadIdx.x % gc, grp = threadIdx.x / gc;
     double sq = 0.0;
@@ -586,7 +592,11 @@ __global__ void __launch_bounds__(MAXT) fft_pass_kernel(PassDesc d, int L, int r
       const int pos = (k % n1s) * n2s + k / n1s;
       const float sg = ((k + d.coord_off[1] + ui + d.coord_off[2] + ln.vi) & 1) ? -d.sfac : d.sfac;
       float2 acc = make_float2(0.f, 0.f);
-      if (ok) {
+      if (ok && pairs) {
+        const float4 sv = *reinterpret_cast<const float4*>(s + pos * cols + l * C + 2 * lane);
+        const float4 kv = __ldg(reinterpret_cast<const float4*>(d.kfc + m * C + 2 * lane));
+        acc = nak_pair_term(sv, kv, sg);
+      } else if (ok) {
         for (int c = lane; c < C; c += gc) {
           float2 v = s[pos * cols + l * C + c];
           v = make_float2(v.x * sg, v.y * sg);
@@ -596,8 +606,8 @@ __global__ void __launch_bounds__(MAXT) fft_pass_kernel(PassDesc d, int L, int r
         }
       }
       for (int w = gc / 2; w > 0; w >>= 1) {
-        acc.x += __shfl_xor_sync(0xffffffffu, acc.x, w, gc);
-        acc.y += __shfl_xor_sync(0xffffffffu, acc.y, w, gc);
+        acc.x = __fadd_rn(acc.x, __shfl_xor_sync(0xffffffffu, acc.x, w, gc));
+        acc.y = __fadd_rn(acc.y, __shfl_xor_sync(0xffffffffu, acc.y, w, gc));
       }
       if (ok && lane == 0) {
         d.img_out[m] = acc;
