@@ -64,7 +64,8 @@ __device__ __forceinline__ float2 cmulf_rn(float2 a, float2 b) {
 
 // One coil pair's share of the inverse x pass's coil sum: the two coils'
 // values times the modulation-and-scale factor sg, times their KFC_conj
-// values, added (explicit roundings, shared by the TMA and cp.async kernels).
+// values, added (explicit roundings; the pipelined and unpipelined kernels
+// share it, so they give the same image bit for bit).
 __device__ __forceinline__ float2 nak_pair_term(float4 sv, float4 kv, float sg) {
   const float2 t0 = cmulf_rn(make_float2(__fmul_rn(sv.x, sg), __fmul_rn(sv.y, sg)), make_float2(kv.x, kv.y));
   const float2 t1 = cmulf_rn(make_float2(__fmul_rn(sv.z, sg), __fmul_rn(sv.w, sg)), make_float2(kv.z, kv.w));
@@ -1351,75 +1352,6 @@ static int launch_tma_shanna(const FftAxisPlan& a, const PassDesc& d, int Lp, cu
   }
 }
 
-// TMA inverse x pass (fft_pass_tma_kernel NAK) for 2, 4, 8 or 16 coils (16
-// columns, 16 / C lines per bundle): the A lines are the loaded box, their
-// KFC_conj rows one bulk copy.  *launched stays false when the shape does
-// not fit (the caller then takes the cp.async pass).  The per-CTA partial
-// sums cover the same pixels in another grouping than the cp.async pass's,
-// so their sum agrees to rounding, not bit for bit; the image does.
-template <int N1, int N2, int NSLOT>
-static int launch_tma_nak(const FftAxisPlan& a, const PassDesc& d, int n_slots, cudaStream_t s, bool* launched) {
-  constexpr int COLS = 16, N = N1 * N2, NT = cta_threads(COLS);
-  *launched = false;
-  if constexpr (tma_step_c_iters<N1, N2, COLS, NT>() * N2 > 32) return MLG_OK;
-  else {
-  const int C = d.C;
-  if (C < 2 || C > 16 || (16 % C) || !d.img_out || !d.kfc || d.in_lo != 0 || d.in_len != N || d.out_lo < 0 ||
-      d.out_len < 1 || d.out_lo + d.out_len > N || d.in_half || d.out_half || ((uintptr_t)d.kfc & 15))
-    return MLG_OK;
-  const int Lp = 16 / C;
-  TmaPass t;
-  t.L = Lp;
-  t.gu = (d.dims[1] + Lp - 1) / Lp;
-  t.nbundles = blocks_for(d, Lp);
-  t.in_chunks = (N + 255) / 256;
-  if (N % t.in_chunks) return MLG_OK;
-  t.in_rows = N / t.in_chunks;
-  t.in_lo = 0;
-  t.out_lo = d.out_lo;
-  t.out_rows = d.out_len;
-  t.err = d.wait_err;
-  t.test_stall = tma_test_stall() ? 1 : 0;
-  t.du = d.dims[1];
-  t.img_len = d.out_len;
-  t.par0 = (d.coord_off[1] + d.coord_off[2]) & 1;
-  t.img_out = d.img_out;
-  t.kfcc = d.kfc;
-  t.sfac = d.sfac;
-  t.partial = d.partial;
-  t.n_slots = n_slots;
-  if ((t.in_rows * (long long)COLS * 8) % 128) return MLG_OK;
-  CUtensorMap tin;
-  if (tma_line_map(&tin, d.in, C, d.dims[1], d.in_stride[1], d.in_len, d.in_stride[0], d.dims[2], d.in_stride[2],
-                   Lp, t.in_rows) != MLG_OK)
-    return MLG_OK;
-  const size_t smem = (size_t)NSLOT * N * COLS * 8 + 2 * NSLOT * sizeof(uint64_t) + (size_t)N * 8 + 128 +
-                      (size_t)NSLOT * d.out_len * COLS * 8;
-  if (smem > 200 * 1024) return MLG_OK;
-  if (d.dry) {
-    *launched = true;
-    return MLG_OK;
-  }
-  auto kern = fft_pass_tma_kernel<N1, N2, 1, COLS, NSLOT, false, false, false, false, false, false, true>;
-  thread_local int per_sm = 0, sms = 0;
-  thread_local size_t per_sm_smem = 0;
-  if (per_sm == 0 || per_sm_smem != smem) {
-    MLG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(200 * 1024)));
-    int dev = 0;
-    MLG_CUDA(cudaGetDevice(&dev));
-    MLG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    MLG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT + 32, smem));
-    per_sm = std::max(1, per_sm);
-    per_sm_smem = smem;
-  }
-  const int grid = std::max(1, std::min(std::min(t.nbundles, per_sm * sms), n_slots));
-  kern<<<grid, NT + 32, smem, s>>>(tin, tin, t, a.tw);
-  MLG_LAUNCHED();
-  *launched = true;
-  return MLG_OK;
-  }
-}
-
 template <int N1, int N2, int CP>
 static int launch_nak_pipe(const FftAxisPlan& a, const PassDesc& d, int n_slots, cudaStream_t s) {
   if (d.dry) return MLG_OK;
@@ -1514,13 +1446,6 @@ static int launch_pass(const FftAxisPlan& a, const PassDesc& d, int L, cudaStrea
     }
   }
   if constexpr (MODE == PassMode::kNakatshaOut && N1 > 0) {
-    if (tma_passes_enabled() && d.tma_slots >= 2) {  // TMA inverse x pass
-      bool done = false;
-      const int n_slots = blocks_for(d, L);
-      const int st = d.tma_slots >= 3 ? launch_tma_nak<N1, N2, 3>(a, d, n_slots, s, &done)
-                                       : launch_tma_nak<N1, N2, 2>(a, d, n_slots, s, &done);
-      if (st != MLG_OK || done) return st;
-    }
     // 2, 4, 8 or 16 coils, two bundles of lines and KFC rows within ~100 KB
     if (2 * ((size_t)a.N + d.out_len) * 16 * sizeof(float2) <= 104 * 1024) {
       const int n_slots = blocks_for(d, L);

@@ -50,13 +50,6 @@
 // place before the transform.  AMAX: the transform threads record the
 // largest output component (the scale of the mixed-precision intermediate).
 //
-// NAK (the inverse x pass of the adjoint, bmNakatsha's last FFT, crop,
-// .* KFC_conj and coil sum): the loaded box holds the bundle's A lines, one
-// untiled bulk copy brings their KFC_conj rows onto the same barrier, and
-// after the transform groups of C/2 transform threads form each kept
-// pixel's coil sum, store it and add |x|^2 to an FP64 per-CTA partial sum;
-// nothing is stored by TMA.
-//
 // Every wait is bounded (kTmaWaitNs of wall-clock time): a wait that runs out
 // sets *err, makes the CTA's other waits give up at once, and the CTA returns
 // after the copies it issued have finished.  No multicast form is used: each
@@ -96,17 +89,9 @@ struct TmaPass {
   // SHANNA: the image (img_len pixels per x line, shared by the coils) and
   // the parity of the modulation's line offset; AMAX: the recorded maximum
   const float2* img = nullptr;
-  int img_len = 0;  // (also NAK) kept pixels per x line
-  int par0 = 0;     // (also NAK)
+  int img_len = 0;
+  int par0 = 0;
   unsigned* amax = nullptr;
-  // NAK: the image written, KFC_conj [pixel][coil], the output factor
-  // (1/prod N with the modulation's constant sign), the per-CTA partial sums
-  // of |x|^2 (n_slots slots, those past the grid zeroed by CTA 0; optional)
-  float2* img_out = nullptr;
-  const float2* kfcc = nullptr;
-  float sfac = 1.f;
-  double* partial = nullptr;
-  int n_slots = 0;
   // test hook (MLG_TEST_WAIT_TIMEOUT=1): CTA 0 never loads its first bundle,
   // so its transform threads' bounded wait runs out and the timeout path runs
   int test_stall = 0;
@@ -341,7 +326,7 @@ constexpr int tma_min_blocks() {
 }
 
 template <int N1, int N2, int DIR, int COLS, int NSLOT, bool IN_H = false, bool OUT_H = false, bool MASKED = false,
-          bool MASK_OUT = false, bool SHANNA = false, bool AMAX = false, bool NAK = false>
+          bool MASK_OUT = false, bool SHANNA = false, bool AMAX = false>
 __global__ void __launch_bounds__(cta_threads(COLS) + 32, (tma_min_blocks<N1 * N2, COLS, NSLOT>()))
     fft_pass_tma_kernel(const __grid_constant__ CUtensorMap tin, const __grid_constant__ CUtensorMap tout, TmaPass a,
                         const float2* __restrict__ tw) {
@@ -358,9 +343,6 @@ __global__ void __launch_bounds__(cta_threads(COLS) + 32, (tma_min_blocks<N1 * N
   uint32_t* slot_any = masks + NSLOT * kTmaMaskWords;      // MASKED / MASK_OUT: chunk bits per slot
   float2* xbuf = tws + N;  // SHANNA: NSLOT x (L x img_len) image values (in place of the masks)
   static_assert(!SHANNA || (!MASKED && !MASK_OUT && !IN_H && DIR < 0), "the forward x pass");
-  float2* kbuf = tws + N;  // NAK: NSLOT x (L x img_len x C) KFC_conj values
-  static_assert(!NAK || (!MASKED && !MASK_OUT && !IN_H && !OUT_H && !SHANNA && DIR > 0 && COLS == 16),
-                "the inverse x pass, 16 columns");
   constexpr int NW = (N + 31) / 32;                        // mask words per line
   static_assert(!MASKED || (N % 32 == 0 && !IN_H), "masked passes: 32-row chunks of an FP32 input");
   static_assert(!MASK_OUT || (N % 32 == 0 && !OUT_H && !MASKED), "masked stores: 32-row chunks of an FP32 output");
@@ -414,17 +396,6 @@ __global__ void __launch_bounds__(cta_threads(COLS) + 32, (tma_min_blocks<N1 * N
           if ((any >> k) & 1u)
             tma_load_4d(dst + (size_t)k * a.in_rows * COLS * kInElem, &tin, 0, c1, k * a.in_rows - a.in_lo, c3,
                         full + slot);
-      } else if constexpr (NAK) {
-        const int u0 = (b % a.gu) * a.L, vi = b / a.gu;
-        const int nl = min(a.L, a.du - u0);  // lines inside the volume (>= 1)
-        const int C = COLS / a.L;
-        const unsigned kbytes = (unsigned)(nl * a.img_len * C) * 8u;
-        mbar_arrive_expect_tx(full + slot, kBuf + kbytes);
-        for (int k = 0; k < a.in_chunks; ++k)
-          tma_load_4d(dst + (size_t)k * a.in_rows * COLS * kInElem, &tin, 0, c1, k * a.in_rows - a.in_lo, c3,
-                      full + slot);
-        bulk_load(kbuf + (size_t)slot * a.img_len * COLS, a.kfcc + (long long)a.img_len * (u0 + (long long)a.du * vi) * C,
-                  kbytes, full + slot);
       } else if constexpr (SHANNA) {
         const int u0 = (b % a.gu) * a.L, vi = b / a.gu;
         const int nl = min(a.L, a.du - u0);  // lines inside the volume (>= 1)
@@ -454,7 +425,6 @@ __global__ void __launch_bounds__(cta_threads(COLS) + 32, (tma_min_blocks<N1 * N
       }
     };
     auto store = [&](int slot, int b) {
-      if constexpr (NAK) return;  // the transform threads store the pixels themselves
       const unsigned char* src = base + slot * kBuf + (size_t)a.out_lo * COLS * kOutElem;
       const int c1 = (b % a.gu) * a.L, c3 = b / a.gu;
       uint32_t keep = ~0u;  // MASK_OUT: bit k = chunk k holds an occupied row of some line
@@ -504,7 +474,6 @@ __global__ void __launch_bounds__(cta_threads(COLS) + 32, (tma_min_blocks<N1 * N
     if (IN_H) hs = 1.f / hs;  // a power of two: exact
   }
   float amax = 0.f;  // AMAX: largest output component this thread wrote
-  double sq = 0.0;   // NAK: sum of |x|^2 of the pixels this thread stored
   int it = 0;
   for (int b = blockIdx.x; b < a.nbundles; b += G, ++it) {
     const int slot = it % NSLOT;
@@ -541,57 +510,10 @@ __global__ void __launch_bounds__(cta_threads(COLS) + 32, (tma_min_blocks<N1 * N
           reinterpret_cast<float2*>(base + slot * kBuf)[k * COLS + col] = make_float2(0.f, 0.f);
       }
     }
-    if constexpr (NAK) {  // crop, modulation and scale, .* KFC_conj, coil sum (bmNakatsha_MATLAB.m:32-56)
-      bar_transform<NT>();  // every transformed row written
-      const int C = COLS / a.L, CP = C / 2, GP = NT / CP;
-      const int q = tid % CP, grp = tid / CP;
-      const int u0 = (b % a.gu) * a.L, vi = b / a.gu;
-      const float4* const cur = reinterpret_cast<const float4*>(base + slot * kBuf);
-      const float4* const kcur = reinterpret_cast<const float4*>(kbuf + (size_t)slot * a.img_len * COLS);
-      const int total = a.L * a.img_len;
-      const int rounds = (total + GP - 1) / GP;  // uniform: every lane reaches the shuffles
-      for (int rd = 0; rd < rounds; ++rd) {
-        const int o = rd * GP + grp;
-        const bool live = o < total;
-        const int ll = live ? o / a.img_len : 0;
-        const int kk = live ? o - ll * a.img_len : 0;
-        const int ui = u0 + ll;
-        const bool okp = live && ui < a.du;
-        const int k = a.out_lo + kk;
-        float2 acc = make_float2(0.f, 0.f);
-        if (okp) {
-          const float sg = ((k + a.par0 + ui + vi) & 1) ? -a.sfac : a.sfac;
-          acc = nak_pair_term(cur[k * (COLS / 2) + ll * CP + q], kcur[(ll * a.img_len + kk) * CP + q], sg);
-        }
-        for (int w = CP / 2; w > 0; w >>= 1) {
-          acc.x = __fadd_rn(acc.x, __shfl_xor_sync(0xffffffffu, acc.x, w, CP));
-          acc.y = __fadd_rn(acc.y, __shfl_xor_sync(0xffffffffu, acc.y, w, CP));
-        }
-        if (okp && q == 0) {
-          a.img_out[kk + (long long)a.img_len * (ui + (long long)a.du * vi)] = acc;
-          sq += (double)acc.x * acc.x + (double)acc.y * acc.y;
-        }
-      }
-    }
     fence_proxy_async_smem();  // the transform's writes become visible to the store
     mbar_arrive(done + slot);
   }
   if constexpr (AMAX) warp_amax(a.amax, amax);  // the transform threads are whole warps
-  if constexpr (NAK) {
-    if (a.partial) {  // per-CTA sum in a fixed order
-      __shared__ double red[NT / 32];
-      for (int o = 16; o > 0; o >>= 1) sq += __shfl_down_sync(0xffffffffu, sq, o);
-      if ((tid & 31) == 0) red[tid >> 5] = sq;
-      bar_transform<NT>();
-      if (tid == 0) {
-        double t = 0.0;
-        for (int i = 0; i < NT / 32; ++i) t += red[i];
-        a.partial[blockIdx.x] = t;
-      }
-      if (blockIdx.x == 0)
-        for (int i = G + tid; i < a.n_slots; i += NT) a.partial[i] = 0.0;
-    }
-  }
 }
 
 // Host: 4-D tensor map of a coil-fastest volume seen as the line boxes of
