@@ -5,7 +5,7 @@ behind every bench number, against the oracle, at the bench's own sizes.
   the device-built Gu/Gut against the restatement of bmTraj2SparseMat.m
   (structure exact, values within 2.5e-7); one Shanna (bmShanna_MATLAB.m:28-54)
   and one Nakatsha (bmNakatsha_MATLAB.m:32-56) in every adjoint strategy --
-  256-point lines, 16-column pipelined passes -- relative L2 <= 1e-5 against
+  256-point lines, 16-column TMA passes (the default variant) -- relative L2 <= 1e-5 against
   the FP32 oracle on the same matrices; the leight gridder
   (bmGridder_n2u_leight3_mex.cpp:226-351) on the c2 samples against the
   bit-pinned C restatement, relative L2 <= 1e-5.
@@ -14,7 +14,7 @@ behind every bench number, against the oracle, at the bench's own sizes.
   (bmSensa.m:39-85) against the FP32 oracle <= 1e-4 (FP64 scalars on both
   sides).
 * c3 bins and the 3-D serving requests with 12 coils (96^3 / 192^3): the
-  24-column pipelined passes on radix-3 192-point lines, <= 1e-5.
+  24-column passes on radix-3 192-point lines, <= 1e-5.
 * 2-D serving requests (512^2 grid, 12 coils): 512-point lines in 24-column
   passes, <= 1e-5.
 
