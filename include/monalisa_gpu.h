@@ -390,8 +390,9 @@ int mlg_plan_autotune_variants(mlg_plan_t p, int reps, double* ms);
  * reference's single-precision arithmetic).  MLG_PRECISION_MIXED: FP16 matrix
  * values (copies of Gu/Gut made once) and, where the plan's passes support
  * it (mlg_plan_get_half_intermediate), 16-bit storage of the 3-D
- * transforms' intermediate inside the CG steps (FP16 times a power of two
- * bounding it from its input's largest value); FP32 k-space vectors (M p and
+ * transforms' intermediate and of the forward grid inside the CG steps (FP16
+ * times a power of two bounding it from the forward x pass's or the Gut
+ * product's largest value); FP32 k-space vectors (M p and
  * the residual), FP32 sums and FFT arithmetic, FP64 scalars; the caller's y
  * and x stay complex64.  Mixed precision turns the fused-gather adjoint
  * strategy off (it reads FP32 k-space).  The operator entry points
@@ -403,11 +404,13 @@ int mlg_plan_autotune_variants(mlg_plan_t p, int reps, double* ms);
 #define MLG_PRECISION_FP16_VALUES 2
 int mlg_plan_set_precision(mlg_plan_t p, int precision);
 int mlg_plan_get_precision(mlg_plan_t p, int* precision);
-/* *on = 1 when a mixed solve of this plan keeps the intermediate of its 3-D
- * transforms (after the forward y pass, after the adjoint z pass) in scaled
- * FP16 inside the CG steps: MLG_PRECISION_MIXED, 3-D, a multiple of 4 coils,
- * no fused adjoint gather, and TMA line passes for those shapes; 0
- * otherwise.  No reference counterpart. */
+/* *on != 0 when a mixed solve of this plan keeps the intermediate of its
+ * 3-D transforms (after the forward y pass, after the adjoint z pass) in
+ * scaled FP16 inside the CG steps: MLG_PRECISION_MIXED, 3-D, a multiple of 4
+ * coils, no fused adjoint gather, and TMA line passes for those shapes (bit
+ * 0); bit 1 set when the forward grid is stored in scaled FP16 as well (the
+ * last forward pass writes it, Gu's gathers read it: even coil count, no Gu
+ * row longer than 256 entries); 0 otherwise.  No reference counterpart. */
 int mlg_plan_get_half_intermediate(mlg_plan_t p, int* on);
 
 /* Times the stages of one Shanna and one Nakatsha on the plan's stream with

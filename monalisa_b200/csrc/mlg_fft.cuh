@@ -78,6 +78,7 @@ struct PassDesc {
   int in_half = 0, out_half = 0;
   const unsigned* h_amax = nullptr;
   int h_len = 1;
+  int h_len_out = 0;  // with both in_half and out_half: the output's h_len (0: h_len)
   unsigned* out_absmax = nullptr;
   // check only: MLG_OK when a kernel would run the pass with every field
   // above honoured, MLG_ERR_UNSUPPORTED otherwise; nothing is launched

@@ -72,18 +72,6 @@ __device__ __forceinline__ float2 nak_pair_term(float4 sv, float4 kv, float sg) 
   return make_float2(__fadd_rn(t0.x, t1.x), __fadd_rn(t0.y, t1.y));
 }
 
-// Scale of a pass intermediate stored in FP16: a power of two s with
-// bound * s < 2^15 (< 65504), bound = 2 len amax >= any component of a
-// length-len transform of values whose components are at most amax (the
-// writer recorded amax; writer and reader compute the same s).
-__device__ __forceinline__ float half_store_scale(const unsigned* amax, int len) {
-  const float bound = __uint_as_float(__ldg(amax)) * (float)len * 2.0f;
-  if (!(bound > 0.f) || !(bound < 1e38f)) return 1.f;
-  int e;
-  frexpf(bound, &e);  // bound < 2^e
-  return ldexpf(1.f, 15 - e);
-}
-
 // Largest component magnitude of two complex values.
 __device__ __forceinline__ float absmax4(float4 v) {
   return fmaxf(fmaxf(fabsf(v.x), fabsf(v.y)), fmaxf(fabsf(v.z), fabsf(v.w)));
@@ -1182,7 +1170,6 @@ static int launch_tma(const FftAxisPlan& a, const PassDesc& d, int Lp, cudaStrea
       d.out_lo + d.out_len > N || Lp * d.C != COLS)
     return MLG_OK;
   const bool ih = d.in_half != 0, oh = d.out_half != 0;
-  if (ih && oh) return MLG_OK;
   // masked: the first inverse pass over the whole stored line, with masks of
   // N / 32 words per line for at most kTmaMaskWords words per bundle
   const bool masked = d.in_mask != nullptr;
@@ -1190,8 +1177,8 @@ static int launch_tma(const FftAxisPlan& a, const PassDesc& d, int Lp, cudaStrea
                  Lp * (N / 32) > kTmaMaskWords || d.lmask_words < N / 32))
     return MLG_OK;
   // masked stores (optional: without them every chunk is stored): the last
-  // forward pass over the whole line, FP32 output, the same mask geometry
-  const bool mask_out = d.out_lmask != nullptr && DIR < 0 && N % 32 == 0 && !oh && !masked && d.out_lo == 0 &&
+  // forward pass over the whole line, the same mask geometry
+  const bool mask_out = d.out_lmask != nullptr && DIR < 0 && N % 32 == 0 && !masked && d.out_lo == 0 &&
                         d.out_len == N && Lp * (N / 32) <= kTmaMaskWords && d.lmask_words >= N / 32;
   if constexpr (N2 > NT / COLS) {  // FP16 input needs one step-A line per thread
     if (ih) return MLG_OK;
@@ -1212,6 +1199,7 @@ static int launch_tma(const FftAxisPlan& a, const PassDesc& d, int Lp, cudaStrea
   t.test_stall = tma_test_stall() ? 1 : 0;
   t.h_amax = d.h_amax;
   t.h_len = d.h_len;
+  t.h_len_out = d.h_len_out;
   if (masked || mask_out) {
     t.lmask = masked ? d.in_lmask : d.out_lmask;
     t.lw = d.lmask_words;
@@ -1237,24 +1225,29 @@ static int launch_tma(const FftAxisPlan& a, const PassDesc& d, int Lp, cudaStrea
     return MLG_OK;
   }
   auto kern = fft_pass_tma_kernel<N1, N2, DIR, COLS, NSLOT, false, false>;
-  const int vi = (ih ? 1 : (oh ? 2 : 0)) + (masked ? 3 : 0) + (mask_out ? 6 : 0);
+  const int vi = (ih ? 1 : 0) + (oh ? 2 : 0) + (masked ? 4 : 0) + (mask_out ? 8 : 0);
   if constexpr (N2 <= NT / COLS) {
-    if (ih) kern = fft_pass_tma_kernel<N1, N2, DIR, COLS, NSLOT, true, false>;
+    if (ih) kern = oh ? fft_pass_tma_kernel<N1, N2, DIR, COLS, NSLOT, true, true>
+                      : fft_pass_tma_kernel<N1, N2, DIR, COLS, NSLOT, true, false>;
   }
-  if (oh) kern = fft_pass_tma_kernel<N1, N2, DIR, COLS, NSLOT, false, true>;
+  if (oh && !ih) kern = fft_pass_tma_kernel<N1, N2, DIR, COLS, NSLOT, false, true>;
   if constexpr (DIR > 0 && N % 32 == 0) {  // the masked first inverse pass
     if (masked) kern = oh ? fft_pass_tma_kernel<N1, N2, DIR, COLS, NSLOT, false, true, true>
                           : fft_pass_tma_kernel<N1, N2, DIR, COLS, NSLOT, false, false, true>;
   }
   if constexpr (DIR < 0 && N % 32 == 0) {  // the last forward pass with masked stores
-    if (mask_out && !ih) kern = fft_pass_tma_kernel<N1, N2, DIR, COLS, NSLOT, false, false, false, true>;
+    if (mask_out && !ih)
+      kern = oh ? fft_pass_tma_kernel<N1, N2, DIR, COLS, NSLOT, false, true, false, true>
+                : fft_pass_tma_kernel<N1, N2, DIR, COLS, NSLOT, false, false, false, true>;
     if constexpr (N2 <= NT / COLS) {
-      if (mask_out && ih) kern = fft_pass_tma_kernel<N1, N2, DIR, COLS, NSLOT, true, false, false, true>;
+      if (mask_out && ih)
+        kern = oh ? fft_pass_tma_kernel<N1, N2, DIR, COLS, NSLOT, true, true, false, true>
+                  : fft_pass_tma_kernel<N1, N2, DIR, COLS, NSLOT, true, false, false, true>;
     }
   }
   // per instantiation, variant and host thread
-  thread_local int per_sm[9] = {}, sms = 0;
-  thread_local size_t per_sm_smem[9] = {};
+  thread_local int per_sm[16] = {}, sms = 0;
+  thread_local size_t per_sm_smem[16] = {};
   if (per_sm[vi] == 0 || per_sm_smem[vi] != smem) {
     MLG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(200 * 1024)));
     int dev = 0;

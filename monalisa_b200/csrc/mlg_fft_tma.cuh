@@ -81,6 +81,7 @@ struct TmaPass {
   // (half_store_scale(h_amax, h_len))
   const unsigned* h_amax = nullptr;
   int h_len = 1;
+  int h_len_out = 0;  // FP16 input and output: the output's length (0: h_len)
   // MASKED: line masks (lw words per line; line = u index + du * v index;
   // word w, bit j = occupancy of row 32 w + j)
   const uint32_t* lmask = nullptr;
@@ -219,15 +220,15 @@ constexpr int tma_step_c_iters() {
 // transform threads only.  tws: the axis' twiddle table exp(-2 pi i j/N)
 // copied into shared memory (the same values as the global table).
 // IN_H: the bundle arrived as FP16 in the upper half of the buffer; step A
-// reads its rows from there (times hs), waits for every thread to have read,
+// reads its rows from there (times hs_in), waits for every thread to have read,
 // then writes FP32 (one n2 per thread: N2 <= NT / COLS).  OUT_H: step C
-// writes the rows as FP16 (times hs) into the lower half, row k at k.
+// writes the rows as FP16 (times hs_out) into the lower half, row k at k.
 // MASKED: lbits = the thread's line's occupancy words; step A takes zero for
 // a row whose bit is clear.
 // AMAX: *amax is raised to the largest component the thread writes.
 template <int N1, int N2, int DIR, int COLS, int NT, bool IN_H = false, bool OUT_H = false, bool MASKED = false,
           bool AMAX = false>
-__device__ __forceinline__ void smem_fft_natural(float2* s, const float2* tws, float hs,
+__device__ __forceinline__ void smem_fft_natural(float2* s, const float2* tws, float hs_in, float hs_out,
                                                  const uint32_t* lbits = nullptr, float* amax = nullptr) {
   constexpr int G = NT / COLS;
   constexpr int KI = tma_step_c_iters<N1, N2, COLS, NT>();
@@ -242,7 +243,7 @@ __device__ __forceinline__ void smem_fft_natural(float2* s, const float2* tws, f
 #pragma unroll
       for (int n1 = 0; n1 < N1; ++n1) {
         const float2 v = __half22float2(hsrc[(n1 * N2 + n2) * COLS]);
-        r[n1] = make_float2(v.x * hs, v.y * hs);
+        r[n1] = make_float2(v.x * hs_in, v.y * hs_in);
       }
     }
     bar_transform<NT>();  // every FP16 row read before FP32 rows overwrite them
@@ -309,7 +310,7 @@ __device__ __forceinline__ void smem_fft_natural(float2* s, const float2* tws, f
       for (int k2 = 0; k2 < N2; ++k2) {
         if constexpr (OUT_H)
           reinterpret_cast<__half2*>(s)[(k1 + N1 * k2) * COLS + col] =
-              __floats2half2_rn(r[i][k2].x * hs, r[i][k2].y * hs);
+              __floats2half2_rn(r[i][k2].x * hs_out, r[i][k2].y * hs_out);
         else
           sc[(k1 + N1 * k2) * COLS] = r[i][k2];
         if constexpr (AMAX) *amax = fmaxf(*amax, fmaxf(fabsf(r[i][k2].x), fabsf(r[i][k2].y)));
@@ -345,7 +346,7 @@ __global__ void __launch_bounds__(cta_threads(COLS) + 32, (tma_min_blocks<N1 * N
   static_assert(!SHANNA || (!MASKED && !MASK_OUT && !IN_H && DIR < 0), "the forward x pass");
   constexpr int NW = (N + 31) / 32;                        // mask words per line
   static_assert(!MASKED || (N % 32 == 0 && !IN_H), "masked passes: 32-row chunks of an FP32 input");
-  static_assert(!MASK_OUT || (N % 32 == 0 && !OUT_H && !MASKED), "masked stores: 32-row chunks of an FP32 output");
+  static_assert(!MASK_OUT || (N % 32 == 0 && !MASKED), "masked stores: 32-row chunks");
   constexpr bool kMasks = MASKED || MASK_OUT;  // the producer fetches the bundles' mask words
   __shared__ int abort_flag;
   const int tid = threadIdx.x;
@@ -468,11 +469,9 @@ __global__ void __launch_bounds__(cta_threads(COLS) + 32, (tma_min_blocks<N1 * N
     return;
   }
   // transform threads
-  float hs = 1.f;
-  if constexpr (IN_H || OUT_H) {
-    hs = half_store_scale(a.h_amax, a.h_len);
-    if (IN_H) hs = 1.f / hs;  // a power of two: exact
-  }
+  float hs_in = 1.f, hs_out = 1.f;  // FP16 load / store factors (powers of two)
+  if constexpr (IN_H) hs_in = 1.f / half_store_scale(a.h_amax, a.h_len);
+  if constexpr (OUT_H) hs_out = half_store_scale(a.h_amax, a.h_len_out > 0 ? a.h_len_out : a.h_len);
   float amax = 0.f;  // AMAX: largest output component this thread wrote
   int it = 0;
   for (int b = blockIdx.x; b < a.nbundles; b += G, ++it) {
@@ -500,7 +499,7 @@ __global__ void __launch_bounds__(cta_threads(COLS) + 32, (tma_min_blocks<N1 * N
     const bool empty = (MASKED || MASK_OUT) && slot_any[slot] == 0;
     if (!empty) {
       smem_fft_natural<N1, N2, DIR, COLS, NT, IN_H, OUT_H, MASKED, AMAX>(
-          reinterpret_cast<float2*>(base + slot * kBuf), tws, hs, lbits, &amax);
+          reinterpret_cast<float2*>(base + slot * kBuf), tws, hs_in, hs_out, lbits, &amax);
     } else if constexpr (MASKED) {  // all-zero input: its kept rows are zeros
       const int col = tid % COLS;
       for (int k = a.out_lo + tid / COLS; k < a.out_lo + a.out_rows * a.out_chunks; k += NT / COLS) {

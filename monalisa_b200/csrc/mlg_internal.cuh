@@ -166,6 +166,21 @@ struct Csr {
   uint32_t* ord_rec = nullptr;
 };
 constexpr int kRecInline = 3;
+
+#ifdef __CUDACC__
+// Scale of a mixed-precision intermediate stored in FP16: a power of two s
+// with bound * s < 2^15 (< 65504), bound = 2 len amax >= any component of a
+// length-len transform (or of a product of transforms whose lengths
+// multiply to len) of values whose components are at most amax (the writer
+// of those values recorded amax; writer and reader compute the same s).
+__device__ __forceinline__ float half_store_scale(const unsigned* amax, int len) {
+  const float bound = __uint_as_float(__ldg(amax)) * (float)len * 2.0f;
+  if (!(bound > 0.f) || !(bound < 1e38f)) return 1.f;
+  int e;
+  frexpf(bound, &e);  // bound < 2^e
+  return ldexpf(1.f, 15 - e);
+}
+#endif
 constexpr int kSegLen = 512;
 
 void csr_free(Csr& c);
@@ -265,6 +280,11 @@ struct SpmmArgs {
   // Optional: raised (atomicMax on the bits) to the largest |re| or |im| of
   // the values written, before any FP16 rounding (device, non-negative float)
   unsigned* absmax = nullptr;
+  // Optional: the input (point layout, even nCh) holds __half2 values times
+  // half_store_scale(in_half_amax, in_half_len) (the mixed-precision forward
+  // grid); coil-pair products of rows without long rows only
+  const unsigned* in_half_amax = nullptr;
+  int in_half_len = 0;
   // Contracted arithmetic for the coil-pair rows (operators inside plans):
   // the row scale folded into the matrix value (m * HY_j) and fused
   // multiply-adds.  Off (the default): separate round-to-nearest multiply and

@@ -58,7 +58,7 @@ static void set_masked_store(const mlg_plan_s* p, PassDesc& pd) {
 // two that bounds a length-n[1] transform of it below 2^15, the z pass reads
 // it back; dry: check only (PassDesc::dry).
 static int forward_pass(mlg_plan_s* p, int ax, const float2* x, bool x_per_coil, cudaStream_t s, bool half = false,
-                        bool dry = false) {
+                        bool dry = false, bool half_grid = false) {
   const int C = p->nCh, d = p->imDim;
   const int* N = p->N;
   const int* n = p->n;
@@ -110,6 +110,10 @@ static int forward_pass(mlg_plan_s* p, int ax, const float2* x, bool x_per_coil,
   pd.dims[0] = N[0];
   pd.dims[1] = N[1];
   pd.in_half = half ? 1 : 0;
+  if (half_grid) {  // the grid in FP16 too: |grid| <= 2 n_y n_z max|A|
+    pd.out_half = 1;
+    pd.h_len_out = n[1] * n[2];
+  }
   pd.in = p->bufB;
   box_strides(eB, C, pd.in_stride);
   pd.in_lo = p->off[2];
@@ -250,9 +254,14 @@ bool half_intermediate_possible(mlg_plan_s* p) {
   for (int ax = 0; ax < 3 && ok; ++ax) ok = forward_pass(p, ax, nullptr, false, nullptr, true, true) == MLG_OK;
   for (int ax = 2; ax >= 1 && ok; --ax)
     ok = inverse_pass(p, ax, nullptr, nullptr, 1.f, nullptr, nullptr, nullptr, nullptr, true, true) == MLG_OK;
+  // the forward grid in FP16 as well: the z pass storing FP16, Gu's coil-pair
+  // gathers reading it (even coil count, no long rows)
+  const bool ok_g = ok && (p->nCh % 2) == 0 && p->Gu && p->Gu_s.n_long == 0 &&
+                    forward_pass(p, 2, nullptr, false, nullptr, true, true, true) == MLG_OK;
   p->mix_amax = words;
   p->half_b_key = key;
   p->half_b_ok = ok;
+  p->half_g_ok = ok_g;
   return ok;
 }
 
@@ -264,7 +273,7 @@ int shanna_stage(mlg_plan_s* p, int stage, const float2* x, bool x_per_coil, flo
     if (stage >= p->imDim) return MLG_OK;
     const bool half = half_b(p);
     if (half && stage == 0) MLG_CUDA(cudaMemsetAsync(p->mix_amax, 0, sizeof(unsigned), s));
-    return forward_pass(p, stage, x, x_per_coil, s, half);
+    return forward_pass(p, stage, x, x_per_coil, s, half, false, half && p->half_g_ok);
   }
   SpmmArgs a;
   a.m = &p->Gu_s;
@@ -273,6 +282,10 @@ int shanna_stage(mlg_plan_s* p, int stage, const float2* x, bool x_per_coil, flo
   a.in.a = p->grid;
   a.in.rows = p->Nu_tot;
   a.out.layout = Layout::kPointC64;
+  if (half_b(p) && p->half_g_ok) {  // the forward grid stored in FP16 by the z pass
+    a.in_half_amax = p->mix_amax;
+    a.in_half_len = p->n[1] * p->n[2];
+  }
   a.half_values = p->precision != MLG_PRECISION_FP32;
   a.contract = true;  // operator-internal product: fused multiply-adds
   a.out.a = y;

@@ -87,6 +87,9 @@ struct mlg_plan_s {
   unsigned* mix_amax = nullptr;
   int half_b_key = -1;
   bool half_b_ok = false;
+  // with half_b_ok: the forward grid in FP16 too (the last forward pass
+  // stores it, Gu reads it; the same key)
+  bool half_g_ok = false;
   int cg_graph_prec = -1;  // precision the captured CG step was built for
   mlg_plan_s* owner = nullptr;  // the plan whose buffers are borrowed
   int n_borrowers = 0;          // plans borrowing this one's buffers

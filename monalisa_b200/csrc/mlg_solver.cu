@@ -640,6 +640,7 @@ extern "C" int mlg_plan_get_precision(mlg_plan_t p, int* precision) {
 
 extern "C" int mlg_plan_get_half_intermediate(mlg_plan_t p, int* on) {
   MLG_CHECK(p && on, "NULL argument");
-  *on = p->precision == MLG_PRECISION_MIXED && half_intermediate_possible(p) ? 1 : 0;
+  *on = 0;
+  if (p->precision == MLG_PRECISION_MIXED && half_intermediate_possible(p)) *on = 1 | (p->half_g_ok ? 2 : 0);
   return MLG_OK;
 }

@@ -43,6 +43,9 @@ struct SpmmParams {
   double* partial;
   int partial_long_offset;
   unsigned* absmax;
+  // FP16 point-layout input (pair kernel, IN_H): scale from this word and length
+  const unsigned* in_h_amax;
+  int in_h_len;
 };
 
 __device__ __forceinline__ float abs_max4(float4 v) {
@@ -336,7 +339,10 @@ constexpr int pair_min_blocks() {
 // With mid_blocks > 0 (CONTRACT, FP32 output) the first mid_blocks blocks
 // gather the mid rows, a warp per row (mid_rows_block), and the others the
 // listed short rows: one launch, the long-running mid rows started first.
-template <bool CONTRACT, int PPT>
+// IN_H: the input holds __half2 values times a power of two (the
+// mixed-precision forward grid; the scale as its writer computed it from
+// p.in_h_amax / p.in_h_len), read as 8 bytes per coil pair.
+template <bool CONTRACT, int PPT, bool IN_H = false>
 __global__ void __launch_bounds__(256, pair_min_blocks<PPT>()) spmm_pair_kernel(SpmmParams p,
                                                                                const int* __restrict__ rows,
                                                                                const uint2* __restrict__ bounds,
@@ -357,6 +363,7 @@ __global__ void __launch_bounds__(256, pair_min_blocks<PPT>()) spmm_pair_kernel(
   const int nr = (int)min((long long)p.rows_per_block, (long long)n_rows - i0);
   const int total = nr * G;
   const bool scale = p.in_row_scale != nullptr;
+  const float hin = IN_H ? 1.f / half_store_scale(p.in_h_amax, p.in_h_len) : 1.f;  // a power of two
   float amax = 0.f;
   double sq = 0.0;
   // item -> row, first coil pair and entry range (empty for rows the segment kernels own)
@@ -379,10 +386,21 @@ __global__ void __launch_bounds__(256, pair_min_blocks<PPT>()) spmm_pair_kernel(
   auto entry = [&](uint32_t k, int pi, float4* acc) {
     const int j = __ldg(p.col + k);
     float m = val_at(p, k);
-    const float4* src = reinterpret_cast<const float4*>(p.in.a) + (long long)j * P + pi;
     float4 v[PPT];
+    if constexpr (IN_H) {
+      const uint2* src = reinterpret_cast<const uint2*>(p.in.a) + (long long)j * P + pi;
 #pragma unroll
-    for (int u = 0; u < PPT; ++u) v[u] = __ldg(src + u);
+      for (int u = 0; u < PPT; ++u) {
+        const uint2 q = __ldg(src + u);
+        const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&q.x));
+        const float2 b = __half22float2(*reinterpret_cast<const __half2*>(&q.y));
+        v[u] = make_float4(a.x * hin, a.y * hin, b.x * hin, b.y * hin);
+      }
+    } else {
+      const float4* src = reinterpret_cast<const float4*>(p.in.a) + (long long)j * P + pi;
+#pragma unroll
+      for (int u = 0; u < PPT; ++u) v[u] = __ldg(src + u);
+    }
     if constexpr (CONTRACT) {
       if (scale) m = __fmul_rn(m, __ldg(p.in_row_scale + j));
 #pragma unroll
@@ -440,7 +458,9 @@ template <int PPT>
 static void launch_pair_ppt(bool contract, const SpmmParams& p, const int* rows, const uint2* rp, int nrows, int grid,
                             const MidRows& mid, cudaStream_t s) {
   grid += mid.blocks;
-  if (contract)
+  if (p.in_h_amax)  // FP16 input: contracted operator products only (checked by spmm)
+    spmm_pair_kernel<true, PPT, true><<<grid, 256, 0, s>>>(p, rows, rp, nrows, mid);
+  else if (contract)
     spmm_pair_kernel<true, PPT><<<grid, 256, 0, s>>>(p, rows, rp, nrows, mid);
   else
     spmm_pair_kernel<false, PPT><<<grid, 256, 0, s>>>(p, rows, rp, nrows, mid);
@@ -646,6 +666,10 @@ int spmm(const SpmmArgs& a, cudaStream_t s) {
   p.sqn_w = a.sqn_row_weight;
   p.partial = a.partial;
   p.absmax = a.absmax;
+  p.in_h_amax = a.in_half_amax;
+  p.in_h_len = a.in_half_len;
+  MLG_CHECK(!a.in_half_amax || (use_pair_kernel(a) && a.contract && m.n_long == 0 && !a.nonempty_only),
+            "FP16 input: contracted coil-pair products without long rows only");
   MLG_CHECK(!a.nonempty_only || (m.ord_rows && m.ord_nonempty && use_pair_kernel(a)),
             "non-empty-row products need the ordered row list and the coil-pair kernel");
   const long long nrows = spmm_rows(a);

@@ -218,7 +218,15 @@ class NufftPlan:
         it (3-D, a multiple of 4 coils, TMA line passes)."""
         m = ctypes.c_int()
         N.call("mlg_plan_get_half_intermediate", self._h, ctypes.byref(m))
-        return bool(m.value)
+        return bool(m.value & 1)
+
+    @property
+    def half_grid(self) -> bool:
+        """Whether the CG steps of a mixed solve also store the forward grid
+        in scaled FP16 (written by the last forward pass, read by Gu)."""
+        m = ctypes.c_int()
+        N.call("mlg_plan_get_half_intermediate", self._h, ctypes.byref(m))
+        return bool(m.value & 2)
 
     def autotune(self, reps: int = 3, variants: bool = True) -> dict:
         """Times the valid adjoint strategies and keeps the fastest, then (with

@@ -67,9 +67,9 @@ def test_mixed_cg_sense_within_1e3_of_fp64(case):
 
 
 def test_mixed_fp16_intermediate_on_and_off(case):
-    """The same mixed solve with the 3-D transforms' intermediate in scaled
-    FP16 (TMA line passes) and in FP32 (cp.async passes, which cannot load
-    FP16): both within 1e-3 of the FP64 restatement, and different from each
+    """The same mixed solve with the 3-D transforms' intermediate and the
+    forward grid in scaled FP16 (TMA line passes) and in FP32 (cp.async
+    passes, which cannot load FP16): both within 1e-3 of the FP64 restatement, and different from each
     other (the FP16 storage really runs); an FP32 plan reports it off."""
     x64 = oracle.bmSensa(np.zeros(int(np.prod(case["n_u"]))), case["y"], case["ve"], case["C"], case["G"]["Gu"],
                          case["G"]["Gut"], case["n_u"], 10, dtype=np.complex128)
@@ -83,6 +83,7 @@ def test_mixed_fp16_intermediate_on_and_off(case):
         r = mb.SensaRecon(Gu, Gut, case["C"], case["n_u"], precision="mixed")
         r.plan.variant = {"pass_buffers": buffers}
         assert r.plan.half_intermediate == (buffers == 2)
+        assert r.plan.half_grid == (buffers == 2)  # 8 coils, 27-entry Gu rows: the grid in FP16 too
         out[buffers] = r.run_host(case["y"], case["ve"], nIter=1, nCGD=10)
     e_on, e_off = rel(out[2], x64), rel(out[0], x64)
     assert e_on <= 1e-3 and e_off <= 1e-3, (e_on, e_off)
