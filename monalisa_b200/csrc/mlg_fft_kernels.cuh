@@ -1155,7 +1155,7 @@ static int launch_pipe(const FftAxisPlan& a, const PassDesc& d, int Lp, int thre
 // TMA pass (fft_pass_tma_kernel, NSLOT bundle buffers) for a plain pass:
 // *launched stays false when the shape does not fit the TMA boxes (the
 // caller then takes the cp.async pipelined pass).  The masked first inverse
-// pass runs as MASKED (32-row chunk boxes loaded where the line masks have
+// pass runs as MASKED (16-row chunk boxes loaded where the line masks have
 // occupied rows) when its line masks exist and a bundle's mask words fit one
 // slot; copying each occupied row by itself instead had measured slower than
 // the cp.async pass (c2: 1.19 against 0.69 ms).
@@ -1173,13 +1173,14 @@ static int launch_tma(const FftAxisPlan& a, const PassDesc& d, int Lp, cudaStrea
   // masked: the first inverse pass over the whole stored line, with masks of
   // N / 32 words per line for at most kTmaMaskWords words per bundle
   const bool masked = d.in_mask != nullptr;
-  if (masked && (DIR < 0 || !d.in_lmask || N % 32 || ih || d.in_lo != 0 || d.in_len != N ||
-                 Lp * (N / 32) > kTmaMaskWords || d.lmask_words < N / 32))
+  if (masked && (DIR < 0 || !d.in_lmask || N % 32 || N / kTmaChunkRows > 32 || ih || d.in_lo != 0 ||
+                 d.in_len != N || Lp * (N / 32) > kTmaMaskWords || d.lmask_words < N / 32))
     return MLG_OK;
   // masked stores (optional: without them every chunk is stored): the last
   // forward pass over the whole line, the same mask geometry
-  const bool mask_out = d.out_lmask != nullptr && DIR < 0 && N % 32 == 0 && !masked && d.out_lo == 0 &&
-                        d.out_len == N && Lp * (N / 32) <= kTmaMaskWords && d.lmask_words >= N / 32;
+  const bool mask_out = d.out_lmask != nullptr && DIR < 0 && N % 32 == 0 && N / kTmaChunkRows <= 32 && !masked &&
+                        d.out_lo == 0 && d.out_len == N && Lp * (N / 32) <= kTmaMaskWords &&
+                        d.lmask_words >= N / 32;
   if constexpr (N2 > NT / COLS) {  // FP16 input needs one step-A line per thread
     if (ih) return MLG_OK;
   }
@@ -1188,8 +1189,8 @@ static int launch_tma(const FftAxisPlan& a, const PassDesc& d, int Lp, cudaStrea
   t.L = Lp;
   t.gu = (d.dims[u] + Lp - 1) / Lp;
   t.nbundles = blocks_for(d, Lp);
-  t.in_chunks = masked ? N / 32 : (N + 255) / 256;
-  t.out_chunks = mask_out ? N / 32 : (d.out_len + 255) / 256;
+  t.in_chunks = masked ? N / kTmaChunkRows : (N + 255) / 256;
+  t.out_chunks = mask_out ? N / kTmaChunkRows : (d.out_len + 255) / 256;
   if (N % t.in_chunks || d.out_len % t.out_chunks) return MLG_OK;
   t.in_rows = N / t.in_chunks;
   t.out_rows = d.out_len / t.out_chunks;

@@ -21,16 +21,16 @@
 //
 // MASKED (the first inverse pass of the masked adjoint, whose input grid
 // holds Gut's non-empty rows and stale values elsewhere): the load boxes are
-// 32-row chunks, and the producer loads only the chunks in which some line
-// of the bundle has an occupied cell -- its line-mask word for those 32 rows
-// is non-zero -- after copying the bundle's mask words into a per-slot
+// chunks of kTmaChunkRows rows, and the producer loads only the chunks in
+// which some line of the bundle has an occupied cell -- its line-mask bits
+// for those rows are not all zero -- after copying the bundle's mask words into a per-slot
 // shared area; the transform threads read each row's occupancy bit there and
 // take zero for an unoccupied row (skipped chunks and stale cells alike).
 // The producer fetches the mask words before it waits for the slot, so their
 // latency overlaps that wait.
 //
 // MASK_OUT (the last forward pass, whose output grid is read only at cells
-// Gut marks occupied): the store boxes are 32-row chunks, and the producer
+// Gut marks occupied): the store boxes are kTmaChunkRows-row chunks, and the producer
 // stores only the chunks in which some line of the bundle has an occupied
 // cell (mask words kept in the slot's shared area since the bundle's load);
 // the other cells of the grid keep stale values, which no reader touches.
@@ -64,6 +64,22 @@ namespace mlg {
 
 constexpr unsigned long long kTmaWaitNs = 2000000000ull;  // 2 s per wait
 constexpr int kTmaMaskWords = 32;  // mask words per slot (lines x words per line)
+constexpr int kTmaChunkRows = 16;  // rows per load / store box of the masked passes
+static_assert(32 % kTmaChunkRows == 0, "a mask word covers whole chunks");
+
+// Chunk bits of mask word w of a line: bit w * (32 / kTmaChunkRows) + q set
+// when rows [q * kTmaChunkRows, (q + 1) * kTmaChunkRows) of the word hold an
+// occupied cell.
+__device__ __forceinline__ uint32_t tma_chunk_bits(uint32_t word, int w) {
+  constexpr int CPW = 32 / kTmaChunkRows;
+  uint32_t r = 0;
+#pragma unroll
+  for (int q = 0; q < CPW; ++q) {
+    const uint32_t part = CPW == 1 ? word : (word >> (q * kTmaChunkRows)) & ((1u << (kTmaChunkRows % 32)) - 1u);
+    if (part) r |= 1u << (w * CPW + q);
+  }
+  return r;
+}
 
 struct TmaPass {
   int L = 1;          // lines per bundle
@@ -345,8 +361,8 @@ __global__ void __launch_bounds__(cta_threads(COLS) + 32, (tma_min_blocks<N1 * N
   float2* xbuf = tws + N;  // SHANNA: NSLOT x (L x img_len) image values (in place of the masks)
   static_assert(!SHANNA || (!MASKED && !MASK_OUT && !IN_H && DIR < 0), "the forward x pass");
   constexpr int NW = (N + 31) / 32;                        // mask words per line
-  static_assert(!MASKED || (N % 32 == 0 && !IN_H), "masked passes: 32-row chunks of an FP32 input");
-  static_assert(!MASK_OUT || (N % 32 == 0 && !MASKED), "masked stores: 32-row chunks");
+  static_assert(!MASKED || (N % 32 == 0 && !IN_H), "masked passes: whole mask words of an FP32 input");
+  static_assert(!MASK_OUT || (N % 32 == 0 && !MASKED), "masked stores: whole mask words");
   constexpr bool kMasks = MASKED || MASK_OUT;  // the producer fetches the bundles' mask words
   __shared__ int abort_flag;
   const int tid = threadIdx.x;
@@ -389,7 +405,7 @@ __global__ void __launch_bounds__(cta_threads(COLS) + 32, (tma_min_blocks<N1 * N
 #pragma unroll
         for (int i = 0; i < kTmaMaskWords; ++i) {
           masks[slot * kTmaMaskWords + i] = mw[i];
-          if (mw[i]) any |= 1u << (i - (i / NW) * NW);
+          any |= tma_chunk_bits(mw[i], i - (i / NW) * NW);
         }
         slot_any[slot] = any;
         mbar_arrive_expect_tx(full + slot, (unsigned)__popc(any) * (unsigned)(a.in_rows * COLS * kInElem));
@@ -412,7 +428,7 @@ __global__ void __launch_bounds__(cta_threads(COLS) + 32, (tma_min_blocks<N1 * N
           uint32_t keep = 0;  // bit k: output chunk k holds an occupied row of some line
 #pragma unroll
           for (int i = 0; i < kTmaMaskWords; ++i)
-            if (mw[i]) keep |= 1u << (i - (i / NW) * NW);
+            keep |= tma_chunk_bits(mw[i], i - (i / NW) * NW);
           slot_any[slot] = keep;
           if (keep == 0) {  // nothing of this bundle is stored: no load, no transform
             mbar_arrive(full + slot);
