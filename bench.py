@@ -447,6 +447,24 @@ def _event_ms(fn, reps, stream):
     return e0.elapsed_time(e1) / reps
 
 
+def _event_ms_median(fn, reps, stream):
+    """Median of `reps` separately timed calls (CUDA events on `stream`): for
+    the plain-GPU arms, whose host-side stopping test each CG step makes a
+    single run sensitive to host scheduling."""
+    import torch
+
+    out = []
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        out.append(e0.elapsed_time(e1))
+    return float(np.median(out))
+
+
 def _HX(w):
     """HX = prod((1/dK_u)/N_u) in single precision (bmSensa.m:26-27)."""
     HX = np.float32(1)
@@ -556,7 +574,7 @@ def _c1(stream):
     HX = _HX(w)
     pg.sensa(y, ve, HX, w.nCGD)
     box = {}
-    ms_plain = _event_ms(lambda: box.__setitem__("x", pg.sensa(y, ve, HX, w.nCGD)), 3, stream)
+    ms_plain = _event_ms_median(lambda: box.__setitem__("x", pg.sensa(y, ve, HX, w.nCGD)), 5, stream)
     step()
     torch.cuda.synchronize()
     plain = {"recons_per_s": round(1000.0 / ms_plain, 3), "ms_per_recon": round(ms_plain, 3),
