@@ -1,4 +1,7 @@
-"""Frame bins of one temporal-TV reconstruction sharded over ranks.
+"""Frame bins of one temporal-TV reconstruction, or the coils of one
+CG-SENSE reconstruction, sharded over ranks.
+
+Frame bins:
 
 bmTevaMorphosia_chain (src/fourier123/solver_function/imDim_morphosia/
 nonCartesian/bmTevaMorphosia_chain.m:6-195) couples its frames in two ways
@@ -19,6 +22,17 @@ object with the same methods works (the tests run the restatement on CPU
 tensors over gloo).  Images are complex64 torch tensors [prod(n_u)], k-space
 [nPt_i, nCh].  Deformation fields (Tu/Tut) are not supported here; the
 single-GPU chain (solvers.TevaMorphosiaChain) has them.
+
+Coils (bmSensa, src/fourier123/solver_function/imDim/nonCartesian/
+bmSensa.m:6-96): the forward model of each coil is independent, and coils
+meet only in the coil sum of the adjoint (bmNakatsha_MATLAB.m:55) and in the
+k-space norms of the CG steps (bmSensa.m:59, :83).  Each rank holds a run of
+coils (its k-space columns and coil maps); an adjoint is the rank's partial
+coil sum followed by one all-reduce of a prod(n_u) complex64 image, and each
+k-space norm one all-reduce of an FP64 scalar.  The image-space quantities
+(x, p, the adjoint residual and its norm, bmSensa.m:45, :73) are then the
+same on every rank, so the CG recurrences run redundantly without further
+exchange.
 """
 from __future__ import annotations
 
@@ -233,3 +247,152 @@ def _prox_one_norm(v, s):
     re = torch.sign(v.real) * torch.clamp(v.real.abs() - s, min=0)
     im = torch.sign(v.imag) * torch.clamp(v.imag.abs() - s, min=0)
     return torch.complex(re, im)
+
+
+def shard_coils(nCh: int, world: int):
+    """Contiguous runs of coils, one per rank: rank r gets coils
+    [bounds[r], bounds[r+1]).  Runs are whole coil pairs where every rank can
+    have one (the coil-pair kernels and the Gut row records want even coil
+    counts); an odd last coil goes to the last rank."""
+    if world < 1 or world > nCh:
+        raise ValueError(f"{nCh} coils cannot be split over {world} ranks")
+    unit = 2 if nCh >= 2 * world else 1
+    units, spare = divmod(nCh, unit)
+    q, rem = divmod(units, world)
+    sizes = [(q + (1 if r < rem else 0)) * unit for r in range(world)]
+    sizes[-1] += spare
+    bounds = [0]
+    for s in sizes:
+        bounds.append(bounds[-1] + s)
+    return bounds
+
+
+class CoilPlanEngine:
+    """The operators of the coils [lo, hi) on this rank's GPU: a NUFFT plan
+    whose KFC / KFC_conj hold those coils only.  Gu / Gut may be device
+    matrices shared by several engines on one GPU (a plan keeps what it
+    derives from them, e.g. Gut's row records, to itself)."""
+
+    def __init__(self, Gu, Gut, C, n_u, lo: int, hi: int, dK_u=None):
+        from .solvers import SensaRecon
+
+        nu = int(np.prod(np.ravel(n_u)))
+        C = np.asarray(C, np.complex64).reshape(nu, -1, order="F")
+        if not (0 <= lo < hi <= C.shape[1]):
+            raise ValueError(f"coils [{lo}, {hi}) outside the {C.shape[1]} coil maps")
+        self._recon = SensaRecon(Gu, Gut, np.ascontiguousarray(C[:, lo:hi]), n_u, dK_u)
+        self.plan = self._recon.plan
+        self.lo, self.hi = lo, hi
+        r = self._recon
+        # HX = prod((1/dK_u)/N_u) in single precision (bmSensa.m:26-27)
+        dX = (np.float32(1) / r.dK_u.astype(np.float32)) / r.N_u.astype(np.float32)
+        self.HX = float(np.prod(dX.astype(np.float32)))
+
+    def M(self, x):
+        return self.plan.shanna(x)
+
+    def MH(self, r, HY, scale):
+        return self.plan.nakatsha(r, HY, scale)
+
+    def close(self):
+        self.plan.close()
+
+
+class CoilShardedSensa:
+    """bmSensa.m:6-96 over the coils held by this rank.  `engines` are this
+    rank's coil groups in coil order (one or more; each has M(x) -> k-space
+    [nPt, nCh_g], MH(r, HY, scale) -> scale * its partial coil sum of the
+    adjoint of HY .* r, and HX); `group` is a torch.distributed process group
+    (None: one process, no collectives).  Several groups on one rank are
+    summed in order before the all-reduce."""
+
+    def __init__(self, engines, group=None):
+        self.engines = list(engines)
+        if not self.engines:
+            raise ValueError("at least one coil group per rank")
+        self.HX = self.engines[0].HX
+        self.group = group
+        if group is not None:
+            import torch.distributed as dist
+
+            self.dist = dist
+        else:
+            self.dist = None
+
+    def _allreduce(self, vals, dev):
+        import torch
+
+        t = torch.tensor(vals, dtype=torch.float64, device=dev)
+        if self.dist is not None:
+            self.dist.all_reduce(t, group=self.group)
+        return [float(v) for v in t.cpu()]
+
+    def _coil_sum(self, parts):
+        """Partial coil sums of this rank's groups, then one all-reduce of the
+        image (the coil sum of bmNakatsha_MATLAB.m:55 across ranks)."""
+        import torch
+
+        img = parts[0]
+        for q in parts[1:]:
+            img = img + q
+        if self.dist is not None:
+            buf = torch.view_as_real(img.contiguous()).contiguous()
+            self.dist.all_reduce(buf, group=self.group)
+            img = torch.view_as_complex(buf)
+        return img
+
+    @staticmethod
+    def _dot(v, h=None):
+        vr, vi = v.real.double(), v.imag.double()
+        s = vr * vr + vi * vi
+        if h is not None:
+            s = s * (h.double()[:, None] if s.dim() == 2 else h.double())
+        return float(s.sum())
+
+    def run(self, y, ve, x, nIter=1, nCGD=20, ve_max=None, history=None):
+        """y: list over this rank's coil groups of k-space [nPt, nCh_g]; ve
+        [nPt] float32; x [prod(n_u)] initial image, the same on every rank.
+        Returns the image (the same on every rank).  ``history`` receives the
+        monitored residual ||y - M x||^2_HY of each outer iteration
+        (bmSensa.m:82-84), summed over all coils."""
+        import torch
+
+        E = self.engines
+        if len(y) != len(E):
+            raise ValueError("y needs one k-space block per coil group")
+        dev = x.device
+        myEps = 10 * float(np.finfo(np.float32).eps)
+        HX = self.HX
+        if ve_max is None:
+            ve_max = float(ve.max())  # bmSensa.m:29-31 (the same ve on every rank)
+        HY = torch.clamp(ve.to(torch.float32), max=float(np.float32(ve_max)))  # bmSensa.m:32
+        invHX = 1.0 / HX
+        M = lambda v: [e.M(v) for e in E]
+        dagM = lambda r: self._coil_sum([e.MH(r[g], HY, invHX) for g, e in enumerate(E)])
+        kdot = lambda v: self._allreduce([sum(self._dot(b, HY) for b in v)], dev)[0]
+        for _ in range(nIter):
+            Mx = M(x)
+            res = [y[g] - Mx[g] for g in range(len(E))]  # bmSensa.m:43
+            g_img = dagM(res)  # :44
+            sq_next = HX * self._dot(g_img)  # :45
+            p = g_img
+            for i in range(1, nCGD + 1):
+                res_c, sq_c, p_c = res, sq_next, p
+                if sq_c < myEps:  # :54-56
+                    break
+                Mp = M(p_c)
+                a = sq_c / kdot(Mp)  # :58-61
+                af = float(np.float32(a))
+                x = x + af * p_c  # :63
+                if i == nCGD:
+                    break
+                res = [res_c[g] - af * Mp[g] for g in range(len(E))]  # :71
+                g_img = dagM(res)  # :72
+                sq_next = HX * self._dot(g_img)  # :73
+                bf = float(np.float32(sq_next / sq_c))  # :75
+                p = g_img + bf * p_c  # :77
+            Mx = M(x)
+            R = kdot([y[g] - Mx[g] for g in range(len(E))])  # :82-83
+            if history is not None:
+                history.append(R)
+        return x
