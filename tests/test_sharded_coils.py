@@ -1,7 +1,8 @@
 """Coil sharding of one CG-SENSE reconstruction on CPU ranks (gloo): the
-coils split over 2 and 3 ranks (and over two coil groups in one process),
-with the adjoint's coil sum all-reduced as an image and the k-space norms as
-FP64 scalars, give the single-process restatement of bmSensa.m (oracle) --
+coils split over 2 and 3 ranks (one or two coil groups per rank, and two
+coil groups in one process), with the adjoint's coil sum all-reduced as an
+image and the k-space norms as FP64 scalars, give the single-process
+restatement of bmSensa.m (oracle) --
 image relative L2 <= 1e-5, monitored residuals within 1e-5 -- and every rank
 ends with the same image.  The per-group operators are the restatement's
 Shanna / Nakatsha over the group's columns of KFC / KFC_conj on CPU tensors
@@ -89,7 +90,7 @@ def _check(x, hist, ref):
     np.testing.assert_allclose(np.array(hist), hist_ref, rtol=1e-5)
 
 
-def _rank(rank, world, port, out):
+def _rank(rank, world, port, out, split=False):
     import sys
 
     for p in (ROOT, os.path.join(ROOT, "oracle")):
@@ -107,17 +108,20 @@ def _rank(rank, world, port, out):
     case = _case()
     bounds = shard_coils(case["nCh"], world)
     lo, hi = bounds[rank], bounds[rank + 1]
-    sh = CoilShardedSensa([OracleCoilEngine(case, lo, hi)], group=dist.group.WORLD)
+    # split: the rank's coils as two groups (summed locally before the all-reduce)
+    groups = [(lo, lo + 1), (lo + 1, hi)] if split and hi - lo > 1 else [(lo, hi)]
+    sh = CoilShardedSensa([OracleCoilEngine(case, a, b) for a, b in groups], group=dist.group.WORLD)
     hist = []
-    x = sh.run([torch.from_numpy(np.ascontiguousarray(case["y"][:, lo:hi]))], torch.from_numpy(case["ve"]),
-               torch.from_numpy(case["x0"].copy()), nIter=N_ITER, nCGD=N_CGD, history=hist)
+    x = sh.run([torch.from_numpy(np.ascontiguousarray(case["y"][:, a:b])) for a, b in groups],
+               torch.from_numpy(case["ve"]), torch.from_numpy(case["x0"].copy()), nIter=N_ITER, nCGD=N_CGD,
+               history=hist)
     out[rank] = (lo, hi, x.numpy(), hist)
     dist.barrier()
     dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("world", [2, 3])
-def test_coil_sharded_sensa_matches_single_process_restatement(world):
+@pytest.mark.parametrize("world,split", [(2, False), (3, False), (2, True)])
+def test_coil_sharded_sensa_matches_single_process_restatement(world, split):
     import sys
 
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -126,7 +130,7 @@ def test_coil_sharded_sensa_matches_single_process_restatement(world):
     port = _free_port()
     ctx = mp.get_context("spawn")
     out = ctx.Manager().dict()
-    procs = [ctx.Process(target=_rank, args=(r, world, port, out)) for r in range(world)]
+    procs = [ctx.Process(target=_rank, args=(r, world, port, out, split)) for r in range(world)]
     for p in procs:
         p.start()
     for p in procs:
